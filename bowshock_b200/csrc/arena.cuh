@@ -1,0 +1,111 @@
+// Device layout of a case arena: every case of a sweep (one or many, uneven grid sizes) packed into the same
+// structure-of-arrays buffers, so one launch of each kernel serves all cases. A single-case solver is an arena of one.
+//
+// Per case (ni x nj cells, row-major with i fastest, as the reference's grid.rs:1-4):
+//   cells     U, R, X, DU, RR, U0, FORCE (float4 = 4 conserved vars), dt, geometry cellg = {V, A, xc, rc}
+//   padded    W = primitives with 2 ghost layers, (ni+4) x (nj+4)            (solver.rs:200-203)
+//   i-faces   iface = {nx, nr, len, w = len*r_mid}, (ni+1) x nj                (grid.rs:22-47)
+//   j-faces   jface, ni x (nj+1)
+// Case descriptors, iteration counters and convergence masks live in device memory so that an iteration launched
+// from a CUDA graph reads everything it needs on the device.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bk {
+
+enum { SCHEME_EXPLICIT = 0, SCHEME_IMPLICIT = 3 };
+enum { DT_SUM = 0, DT_MIN_DIRECTION = 1 };
+
+struct CaseDev {
+  int ni, nj;
+  long long cell_off, pad_off, if_off, jf_off;
+  int tile_off, ntx, nty;           // residual tiles (TI x TJ cells)
+  int iline_off, jline_off;         // first global i-line / j-line of this case
+  int pblk_off;                     // first block of the padded-cell kernels
+  int has_block, i_end, j_end, j_sting;
+  int has_nozzle, nz_j_end;
+  float nz_state[4], nz_turb[2];
+  int bc[4];
+  double fs[4];
+  float cfl;
+  int limiter, first_order_iters, low_mach;
+  int scheme;
+  float cfl0, cfl_max, growth, eps_fix;
+  int dt_mode, lines, implicit_bc, sub_iters, roe;
+  int viscous, sst, wall_i_start;
+  double re_c, sutherland, roughness;
+  int n_active;
+};
+
+struct Arena {
+  int ncases;
+  const CaseDev* cases;
+  int* iter;    // per case: iterations since the last reset (first-order phase, solver.rs:477)
+  int* ramp_k;  // per case: CFL-ramp counter (implicit.rs:602-603)
+  int* active;  // per case: 1 = iterate, 0 = frozen (converged or stopped)
+  float4 *U, *W, *R, *X, *DU, *RR, *U0, *FORCE;
+  float* dt;
+  const float4 *iface, *jface, *cellg;
+  const float2 *ifc, *jfc;  // face centres (mean of the end nodes)
+  float* scratch;  // line solves: 36 floats per cell
+  double* rsum;    // sum of R_rho^2, [slot * ncases + case]
+  const int* tile_case;
+  int ntiles;
+  const int* iline_case;
+  int nilines;
+  const int* jline_case;
+  int njlines;
+  const int* pblk_case;
+  int npblk;
+  // viscous / SST fields (null for an inviscid arena)
+  float4* grad4;   // (u_x, u_r, v_x, v_r)
+  float2* gradT;   // (T_x, T_r)
+  float* mu;
+  float* mu_t;
+  float4* fvi;     // viscous i-face fluxes
+  float4* fvj;     // viscous j-face fluxes
+  float2* turb;    // (k, omega)
+  float2* turb_new;
+  float* dwall;
+  float* mflux_i;  // inviscid mass flux F[0] of the i-faces (turbulence convection)
+  float* mflux_j;
+  double* tsum;    // sum of (rho dk/dt)^2, [slot * ncases + case]
+  float4* tcoef;   // SST line coefficients, 3 per cell
+  float2* trhs;    // SST right-hand side / solution per cell
+  float4* grad_kw; // (k_x, k_r, omega_x, omega_r)
+  float2* blend;   // (F1, X)
+  // FP64-derived stencil of every face: (|d|, e_x, e_r, 0) between the two side positions (viscous.rs:233-250)
+  const float4 *ifs, *jfs;
+};
+
+constexpr int TI = 32, TJ = 8;  // residual tile
+
+__device__ __forceinline__ bool is_solid(const CaseDev& c, int i, int j) {
+  if (!c.has_block) return false;
+  return i < c.i_end ? j < c.j_end : j < c.j_sting;
+}
+__device__ __forceinline__ int col_start(const CaseDev& c, int i) { return c.has_block ? (i < c.i_end ? c.j_end : c.j_sting) : 0; }
+// first fluid cell of row j; ni when the whole row is solid (implicit.rs:471-477)
+__device__ __forceinline__ int row_start(const CaseDev& c, int j) {
+  if (!c.has_block) return 0;
+  if (j < c.j_sting) return c.ni;
+  return j < c.j_end ? c.i_end : 0;
+}
+// viscous.rs:97-127
+__device__ __forceinline__ bool noslip_jface(const CaseDev& c, int i, int j) {
+  if (!c.viscous) return false;
+  if (!c.has_block) return j == 0 && c.bc[2] == 2 && i >= c.wall_i_start;
+  return (j == c.j_end && i >= c.wall_i_start && i < c.i_end) || (j == c.j_sting && c.j_sting > 0 && i >= c.i_end);
+}
+__device__ __forceinline__ bool noslip_iface(const CaseDev& c, int i, int j) {
+  return c.viscous && c.has_block && i == c.i_end && j >= c.j_sting && j < c.j_end && !(c.has_nozzle && j < c.nz_j_end);
+}
+__device__ __forceinline__ bool jet_iface(const CaseDev& c, int i, int j) { return c.has_block && i == c.i_end && c.has_nozzle && j < c.nz_j_end; }
+
+__device__ __forceinline__ long long cidx(const CaseDev& c, int i, int j) { return c.cell_off + (long long)j * c.ni + i; }
+__device__ __forceinline__ long long pidx(const CaseDev& c, int i, int j) { return c.pad_off + (long long)(j + 2) * (c.ni + 4) + (i + 2); }
+__device__ __forceinline__ long long ifidx(const CaseDev& c, int i, int j) { return c.if_off + (long long)j * (c.ni + 1) + i; }
+__device__ __forceinline__ long long jfidx(const CaseDev& c, int i, int j) { return c.jf_off + (long long)j * c.ni + i; }
+
+}  // namespace bk

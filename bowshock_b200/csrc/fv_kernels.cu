@@ -1,0 +1,686 @@
+// Mean-flow kernels of one iteration over a case arena (sm_100a):
+//   k_prims     conserved -> primitive with both ghost layers and the block ghosts     (solver.rs:423-498)
+//   k_residual  32x8 cell tiles staged in shared memory: every i/j face flux of the tile computed once (MUSCL + limiter,
+//               HLLC blended to Rusanov, low-Mach correction), the cell residual with the axisymmetric source, the local
+//               time step, and the FP64 density-residual norm (block reduce + one atomic per block)   (solver.rs:474-654)
+//   k_stage     SSP-RK3 stage update                                                   (solver.rs:694-720)
+//   k_lines     line-implicit solve of (I - dt J_dir) x = b along every i or j line: one warp per line, a partitioned
+//               block-tridiagonal (4x4) solver — each lane eliminates its own segment in registers, the separator
+//               unknowns form a reduced block-tridiagonal system solved by parallel cyclic reduction across the warp
+//               through shared memory, then each lane back-substitutes its segment       (implicit.rs:528-563)
+//   k_defect    defect r = dt R - (A_i du + A_j du - du) of the unfactored operator     (implicit.rs:622-630)
+// The Jacobian blocks are assembled in registers from W, the face metrics and dt wherever they are needed
+// (implicit.rs:284-467); they are never stored.
+#include "arena.cuh"
+#include "device_math.cuh"
+#include "viscous.cuh"
+
+namespace bk {
+
+__device__ __forceinline__ V4<float> Wat(const Arena& A, const CaseDev& c, int i, int j) { return from_f4(A.W[pidx(c, i, j)]); }
+__device__ __forceinline__ V4<float> prim_of(const Arena& A, const CaseDev& c, int i, int j) { return cons_to_prim(from_f4(A.U[cidx(c, i, j)])); }
+__device__ __forceinline__ V4<double> fs_of(const CaseDev& c) { return mk4<double>(c.fs[0], c.fs[1], c.fs[2], c.fs[3]); }
+
+// ==================================================================================== primitives + ghosts
+__global__ void k_prims(Arena A) {
+  int b = blockIdx.x;
+  int ci = A.pblk_case[b];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  int p = (b - c.pblk_off) * blockDim.x + threadIdx.x;
+  int pw = c.ni + 4;
+  if (p >= pw * (c.nj + 4)) return;
+  int i = p % pw - 2, j = p / pw - 2;
+  int ni = c.ni, nj = c.nj;
+  V4<float> out;
+  bool in_i = i >= 0 && i < ni, in_j = j >= 0 && j < nj;
+  if (in_i && in_j) {
+    int j0 = col_start(c, i);
+    if (c.has_block && j0 > 0 && j < j0 && j >= j0 - 2) {
+      // block ghost below a body / sting surface (solver.rs:457-471)
+      int src = j0 + (j0 - 1 - j);
+      float4 f = A.jface[jfidx(c, i, j0)];
+      out = wall_ghost(prim_of(A, c, i, src), f.x, f.y, noslip_jface(c, i, j0));
+    } else {
+      out = prim_of(A, c, i, j);
+    }
+  } else if (in_j && !in_i) {
+    // i ghosts (solver.rs:429-439), in FP64
+    V4<double> fs = fs_of(c);
+    if (i < 0) {
+      int k = -i;
+      float4 f = A.iface[ifidx(c, 0, j)];
+      V4<double> edge = cvt4<double>(prim_of(A, c, 0, j)), mir = cvt4<double>(prim_of(A, c, k - 1, j));
+      V4<double> g = ghost_state<double>(c.bc[0], fs, edge, mir, f.x, f.y, -1.0);
+      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+    } else {
+      int k = i - ni + 1;
+      float4 f = A.iface[ifidx(c, ni, j)];
+      V4<double> edge = cvt4<double>(prim_of(A, c, ni - 1, j)), mir = cvt4<double>(prim_of(A, c, ni - k, j));
+      V4<double> g = ghost_state<double>(c.bc[1], fs, edge, mir, f.x, f.y, 1.0);
+      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+    }
+  } else if (in_i && !in_j) {
+    // j ghosts (solver.rs:440-451)
+    V4<double> fs = fs_of(c);
+    if (j < 0) {
+      int k = -j;
+      float4 f = A.jface[jfidx(c, i, 0)];
+      V4<double> mir = cvt4<double>(prim_of(A, c, i, k - 1));
+      V4<double> g;
+      if (noslip_jface(c, i, 0))
+        g = wall_ghost<double>(mir, f.x, f.y, true);
+      else
+        g = ghost_state<double>(c.bc[2], fs, cvt4<double>(prim_of(A, c, i, 0)), mir, f.x, f.y, -1.0);
+      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+    } else {
+      int k = j - nj + 1;
+      float4 f = A.jface[jfidx(c, i, nj)];
+      V4<double> edge = cvt4<double>(prim_of(A, c, i, nj - 1)), mir = cvt4<double>(prim_of(A, c, i, nj - k));
+      V4<double> g = ghost_state<double>(c.bc[3], fs, edge, mir, f.x, f.y, 1.0);
+      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+    }
+  } else {
+    out = mk4<float>((float)c.fs[0], (float)c.fs[1], (float)c.fs[2], (float)c.fs[3]);  // corners: never read
+  }
+  A.W[pidx(c, i, j)] = to_f4(out);
+}
+
+// ==================================================================================== residual
+// Inviscid flux of i-face (i, j) from the shared-memory stencil (solver.rs:505-542), with the base-wall stencils of a block.
+__device__ __forceinline__ V4<float> iface_flux(const Arena& A, const CaseDev& c, int i, int j, const V4<float>& m2_, const V4<float>& m1_,
+                                                const V4<float>& p0, const V4<float>& p1, int lim, float4 f) {
+  V4<float> m2 = m2_, m1 = m1_;
+  if (c.has_block && j < c.j_end) {
+    if (j < c.j_sting || i < c.i_end) return mk4<float>(0, 0, 0, 0);
+    if (i <= c.i_end + 1) {
+      float4 fb = A.iface[ifidx(c, c.i_end, j)];
+      if (jet_iface(c, c.i_end, j)) {
+        V4<float> jw = mk4<float>(c.nz_state[0], c.nz_state[1], c.nz_state[2], c.nz_state[3]);
+        m2 = jw;
+        if (i == c.i_end) m1 = jw;
+      } else if (i == c.i_end) {
+        bool ns = noslip_iface(c, i, j);
+        m2 = wall_ghost(p1, fb.x, fb.y, ns);
+        m1 = wall_ghost(p0, fb.x, fb.y, ns);
+      } else {
+        m2 = wall_ghost(m1, fb.x, fb.y, noslip_iface(c, c.i_end, j));
+      }
+    }
+  }
+  return face_flux_lm(m2, m1, p0, p1, lim, f.x, f.y, c.low_mach != 0);
+}
+
+__device__ __forceinline__ float diffusion_rate(float mu_c, float mu_t_c, float rho_c, float len, float area) {  // viscous.rs:421-424
+  float lv = 1.4f * (mu_c / 0.72f + mu_t_c / 0.9f) / rho_c;
+  return 2.0f * lv * len * len / area;
+}
+__device__ __forceinline__ float hoop_stress(float mue, float4 g4, float v_c, float r_c) {  // viscous.rs:413-416
+  float div = g4.x + g4.w + v_c / r_c;
+  return mue * (2.0f * v_c / r_c - 2.0f / 3.0f * div);
+}
+
+// dt_kind: 0 = keep dt, 1 = explicit local time step (solver.rs:614-643), 2 = implicit pseudo-time step (implicit.rs:666-695)
+__global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int slot) {
+  __shared__ float4 sW[TJ + 4][TI + 4];
+  __shared__ float4 sFI[TJ][TI + 1];
+  __shared__ float4 sFJ[TJ + 1][TI];
+  __shared__ double sred[TI * TJ / 32];
+  __shared__ float s_cfl;
+  const int t = blockIdx.x;
+  const int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  const int lt = t - c.tile_off;
+  const int i0 = (lt % c.ntx) * TI, j0 = (lt / c.ntx) * TJ;
+  const int ni = c.ni, nj = c.nj;
+  const int tid = threadIdx.x;
+  const int iter = A.iter[ci];
+  const int lim = iter < c.first_order_iters ? LIM_FIRST : c.limiter;
+  if (tid == 0) {
+    if (dt_kind == 2) {
+      int k = A.ramp_k[ci];
+      double cfl = (double)c.cfl0 * pow((double)c.growth, (double)(k < 10000 ? k : 10000));
+      s_cfl = (float)fmin(cfl, (double)c.cfl_max);
+    } else {
+      s_cfl = c.cfl;
+    }
+  }
+  // stage the padded primitives of the tile and its 2-cell halo
+  for (int idx = tid; idx < (TJ + 4) * (TI + 4); idx += blockDim.x) {
+    int r = idx / (TI + 4), q = idx % (TI + 4);
+    int gi = i0 - 2 + q, gj = j0 - 2 + r;
+    sW[r][q] = (gi < ni + 2 && gj < nj + 2) ? A.W[pidx(c, gi, gj)] : make_float4(1.f, 0.f, 0.f, 1.f);
+  }
+  __syncthreads();
+  // i faces (TI+1 per row) and j faces (TJ+1 per column)
+  for (int idx = tid; idx < TJ * (TI + 1) + (TJ + 1) * TI; idx += blockDim.x) {
+    if (idx < TJ * (TI + 1)) {
+      int r = idx / (TI + 1), q = idx % (TI + 1);
+      int i = i0 + q, j = j0 + r;
+      if (i <= ni && j < nj) {
+        V4<float> fl = iface_flux(A, c, i, j, from_f4(sW[r + 2][q]), from_f4(sW[r + 2][q + 1]), from_f4(sW[r + 2][q + 2]),
+                                  from_f4(sW[r + 2][q + 3]), lim, A.iface[ifidx(c, i, j)]);
+        sFI[r][q] = to_f4(fl);
+      }
+    } else {
+      int k = idx - TJ * (TI + 1);
+      int r = k / TI, q = k % TI;
+      int i = i0 + q, j = j0 + r;
+      if (i < ni && j <= nj) {
+        V4<float> fl;
+        if (c.has_block && j < col_start(c, i)) {
+          fl = mk4<float>(0, 0, 0, 0);
+        } else {
+          float4 f = A.jface[jfidx(c, i, j)];
+          fl = face_flux_lm(from_f4(sW[r][q + 2]), from_f4(sW[r + 1][q + 2]), from_f4(sW[r + 2][q + 2]), from_f4(sW[r + 3][q + 2]), lim, f.x,
+                            f.y, c.low_mach != 0);
+        }
+        sFJ[r][q] = to_f4(fl);
+        // inviscid mass flux of the face for the turbulence convection (turbulence.rs:445-456)
+        if (A.mflux_j && c.sst) A.mflux_j[jfidx(c, i, j)] = fl[0];
+      }
+    }
+  }
+  __syncthreads();
+  if (A.mflux_i && c.sst) {
+    for (int idx = tid; idx < TJ * (TI + 1); idx += blockDim.x) {
+      int r = idx / (TI + 1), q = idx % (TI + 1);
+      int i = i0 + q, j = j0 + r;
+      if (i <= ni && j < nj && (q < TI || i == ni)) A.mflux_i[ifidx(c, i, j)] = sFI[r][q].x;
+    }
+  }
+  const int q = tid % TI, r = tid / TI;
+  const int i = i0 + q, j = j0 + r;
+  double rr = 0.0;
+  if (i < ni && j < nj) {
+    long long cc = cidx(c, i, j);
+    if (is_solid(c, i, j)) {
+      A.R[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (dt_kind) A.dt[cc] = 0.f;
+    } else {
+      float4 fl = A.iface[ifidx(c, i, j)], fr = A.iface[ifidx(c, i + 1, j)];
+      float4 fb = A.jface[jfidx(c, i, j)], ft = A.jface[jfidx(c, i, j + 1)];
+      float4 g = A.cellg[cc];  // (V, A, xc, rc)
+      V4<float> gl = from_f4(sFI[r][q]), gr = from_f4(sFI[r][q + 1]), gb = from_f4(sFJ[r][q]), gt = from_f4(sFJ[r + 1][q]);
+      V4<float> wc = from_f4(sW[r + 2][q + 2]);
+      float inv_v = 1.0f / g.x;
+      V4<float> out;
+      float mu_c = 0.f, mut_c = 0.f;
+      if (c.viscous) {
+        V4<float> hl = from_f4(A.fvi[ifidx(c, i, j)]), hr = from_f4(A.fvi[ifidx(c, i + 1, j)]);
+        V4<float> hb = from_f4(A.fvj[jfidx(c, i, j)]), ht = from_f4(A.fvj[jfidx(c, i, j + 1)]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          out[k] = -((gr[k] - hr[k]) * fr.w - (gl[k] - hl[k]) * fl.w + (gt[k] - ht[k]) * ft.w - (gb[k] - hb[k]) * fb.w) * inv_v;
+        mu_c = A.mu[cc];
+        mut_c = A.mu_t[cc];
+        float t_tt = hoop_stress(mu_c + mut_c, A.grad4[cc], wc[2], g.w);
+        out[2] += (wc[3] - t_tt) * g.y * inv_v;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) out[k] = -(gr[k] * fr.w - gl[k] * fl.w + gt[k] * ft.w - gb[k] * fb.w) * inv_v;
+        out[2] += wc[3] * g.y * inv_v;
+      }
+      if (A.FORCE) {
+        float4 fo = A.FORCE[cc];
+        out[0] += fo.x;
+        out[1] += fo.y;
+        out[2] += fo.z;
+        out[3] += fo.w;
+      }
+      A.R[cc] = to_f4(out);
+      rr = (double)out[0] * (double)out[0];
+      if (dt_kind) {
+        float cs = sqrtf(1.4f * wc[3] / wc[0]);
+        auto lam = [&](float4 f) { return (fabsf(wc[1] * f.x + wc[2] * f.y) + cs) * f.z; };
+        float xi = 0.f, xj = 0.f;
+        if (c.viscous) {
+          xi = diffusion_rate(mu_c, mut_c, wc[0], 0.5f * (fl.z + fr.z), g.y);
+          xj = diffusion_rate(mu_c, mut_c, wc[0], 0.5f * (fb.z + ft.z), g.y);
+        }
+        float cfl = s_cfl, d;
+        if (dt_kind == 1) {
+          float sum = lam(fl) + lam(fr) + lam(fb) + lam(ft);
+          d = c.viscous ? cfl * g.y / (0.5f * sum + xi + xj) : cfl * g.y / (0.5f * sum);
+        } else {
+          float li = 0.5f * (lam(fl) + lam(fr)) + xi, lj = 0.5f * (lam(fb) + lam(ft)) + xj;
+          d = c.dt_mode == DT_SUM ? cfl * g.y / (li + lj) : cfl * g.y / (2.0f * fminf(li, lj));
+        }
+        A.dt[cc] = d;
+      }
+    }
+  }
+  if (slot >= 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rr += __shfl_down_sync(0xffffffffu, rr, o);
+    if ((tid & 31) == 0) sred[tid >> 5] = rr;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sred[k];
+      atomicAdd(&A.rsum[(long long)slot * A.ncases + ci], s);
+    }
+  }
+}
+
+// ==================================================================================== explicit stage
+// u = a (u + dt R) + b u0 on the fluid cells; `copy` first saves u0 = u; `last` advances the iteration counter.
+__global__ void k_stage(Arena A, float a, float b, int copy, int last) {
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (last && lt == 0 && threadIdx.x == 0) A.iter[ci] += 1;
+  if (i >= c.ni || j >= c.nj || is_solid(c, i, j)) return;
+  long long cc = cidx(c, i, j);
+  float4 u = A.U[cc];
+  if (copy) A.U0[cc] = u;
+  float4 u0 = copy ? u : A.U0[cc];
+  float4 r = A.R[cc];
+  float d = A.dt[cc];
+  u.x = a * (u.x + d * r.x) + b * u0.x;
+  u.y = a * (u.y + d * r.y) + b * u0.y;
+  u.z = a * (u.z + d * r.z) + b * u0.z;
+  u.w = a * (u.w + d * r.w) + b * u0.w;
+  A.U[cc] = u;
+}
+
+// ==================================================================================== implicit operator
+
+// Blocks (lo, d, up) of I - dt J_dir for fluid cell (i, j) of a line (implicit.rs:379-467).
+__device__ void assemble(const Arena& A, const CaseDev& c, bool dir_i, int i, int j, M4<float>& lo, M4<float>& d, M4<float>& up) {
+  const int k = dir_i ? i : j, n = dir_i ? c.ni : c.nj;
+  const int k0 = dir_i ? row_start(c, j) : col_start(c, i);
+  const long long cc = cidx(c, i, j);
+  V4<float> wk = Wat(A, c, i, j);
+  float4 fl = dir_i ? A.iface[ifidx(c, i, j)] : A.jface[jfidx(c, i, j)];
+  float4 fr = dir_i ? A.iface[ifidx(c, i + 1, j)] : A.jface[jfidx(c, i, j + 1)];
+  float4 g = A.cellg[cc];
+  float src = dir_i ? 0.f : g.y / g.x;
+  bool wall_lower = k == k0 && k0 > 0;
+  bool jet = wall_lower && dir_i && jet_iface(c, k0, j);
+  V4<float> wm;
+  if (jet) {
+    wm = mk4<float>(c.nz_state[0], c.nz_state[1], c.nz_state[2], c.nz_state[3]);
+  } else if (wall_lower && dir_i) {
+    float4 fb = A.iface[ifidx(c, k0, j)];
+    wm = wall_ghost(wk, fb.x, fb.y, noslip_iface(c, k0, j));
+  } else {
+    wm = dir_i ? Wat(A, c, i - 1, j) : Wat(A, c, i, j - 1);
+  }
+  V4<float> wp = dir_i ? Wat(A, c, i + 1, j) : Wat(A, c, i, j + 1);
+  float lam_l = 0.f, lam_r = 0.f;
+  if (c.viscous) {
+    lam_l = dir_i ? face_lambda_dev(A, c, true, i, j) : face_lambda_dev(A, c, false, i, j);
+    lam_r = dir_i ? face_lambda_dev(A, c, true, i + 1, j) : face_lambda_dev(A, c, false, i, j + 1);
+  }
+  cell_blocks<float>(wk, wm, wp, fl.x, fl.y, fl.w, fr.x, fr.y, fr.w, g.x, A.dt[cc], c.lines != 0, src, c.roe != 0, c.eps_fix, lam_l, lam_r,
+                     lo, d, up);
+  if (k == k0) {
+    M4<float> T;
+    if (jet) {
+      T = zero4<float>();
+    } else if (wall_lower) {
+      bool ns = dir_i ? noslip_iface(c, k0, j) : noslip_jface(c, i, k0);
+      T = ns ? noslip4<float>() : reflection<float>(fl.x, fl.y);
+    } else if (!c.implicit_bc) {
+      T = zero4<float>();
+    } else {
+      int bc = dir_i ? c.bc[0] : c.bc[2];
+      if (!dir_i && noslip_jface(c, i, 0) && bc == BC_SLIPWALL) {
+        T = noslip4<float>();
+      } else {
+        M4<double> Td = ghost_jacobian(bc, fs_of(c), cvt4<double>(wk), fl.x, fl.y, -1.0);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
+      }
+    }
+    axpy(d, 1.f, mm(lo, T));
+    lo = zero4<float>();
+  }
+  if (k == n - 1) {
+    M4<float> T;
+    if (!c.implicit_bc) {
+      T = zero4<float>();
+    } else {
+      M4<double> Td = ghost_jacobian(dir_i ? c.bc[1] : c.bc[3], fs_of(c), cvt4<double>(wk), fr.x, fr.y, 1.0);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
+    }
+    axpy(d, 1.f, mm(up, T));
+    up = zero4<float>();
+  }
+}
+
+// right-hand side of a line solve for cell cc: dt R (first pass) or the stored vector
+__device__ __forceinline__ V4<float> rhs_of(const Arena& A, const float4* in, bool from_res, long long cc) {
+  V4<float> r = from_f4(in[cc]);
+  if (from_res) {
+    float d = A.dt[cc];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r[k] *= d;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void st_scratch(float* s, const M4<float>& Y, const V4<float>& g, const M4<float>& GE) {
+  float4* p = reinterpret_cast<float4*>(s);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) p[q] = make_float4(Y[4 * q], Y[4 * q + 1], Y[4 * q + 2], Y[4 * q + 3]);
+  p[4] = to_f4(g);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) p[5 + q] = make_float4(GE[4 * q], GE[4 * q + 1], GE[4 * q + 2], GE[4 * q + 3]);
+}
+__device__ __forceinline__ void ld_scratch(const float* s, M4<float>& Y, V4<float>& g, M4<float>& GE) {
+  const float4* p = reinterpret_cast<const float4*>(s);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 a = p[q];
+    Y[4 * q] = a.x, Y[4 * q + 1] = a.y, Y[4 * q + 2] = a.z, Y[4 * q + 3] = a.w;
+  }
+  g = from_f4(p[4]);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 a = p[5 + q];
+    GE[4 * q] = a.x, GE[4 * q + 1] = a.y, GE[4 * q + 2] = a.z, GE[4 * q + 3] = a.w;
+  }
+}
+
+// Positivity-damped update u += alpha du, alpha halved up to 8 times (implicit.rs:641-660).
+__device__ __forceinline__ void damped_update(float4* U, long long cc, const V4<float>& dq) {
+  float4 u4 = U[cc];
+  V4<float> u = from_f4(u4);
+  float alpha = 1.f;
+  for (int t = 0; t < 8; ++t) {
+    V4<float> q = mk4<float>(u[0] + alpha * dq[0], u[1] + alpha * dq[1], u[2] + alpha * dq[2], u[3] + alpha * dq[3]);
+    V4<float> w = cons_to_prim(q);
+    if (w[0] > 0.f && w[3] > 0.f && isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]) && isfinite(q[3])) {
+      U[cc] = to_f4(q);
+      return;
+    }
+    alpha *= 0.5f;
+  }
+}
+
+constexpr int LINE_WARPS = 4;
+struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
+  float a[16], b[16], c[16], d[4];
+};
+
+// epilogue: 0 = out[c] = x; 1 = DU[c] = x (+ damped update if `update`); 2 = DU[c] += x (+ update)
+__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out, int epilogue, int update) {
+  __shared__ PcrSlot sp[LINE_WARPS][32];
+  __shared__ float4 sl[LINE_WARPS][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * LINE_WARPS + warp;
+  const int nl = dir_i ? A.nilines : A.njlines;
+  if (gw >= nl) return;
+  const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  const int L = gw - (dir_i ? c.iline_off : c.jline_off);
+  const int n = dir_i ? c.ni : c.nj;
+  const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
+  const int len = n - k0;
+  if (len <= 0) return;
+  int m = (len + 31) / 32;
+  if (m < 2) m = 2;
+  const int P = (len + m - 1) / m;
+  const int s = lane;
+  const bool act = s < P;
+  const int a = k0 + s * m;
+  const int e = act ? min(a + m, n) : a;
+  const bool has_sep = act && s < P - 1;
+  const int ke = has_sep ? e - 2 : e - 1;  // last interior cell
+  auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
+  auto ij = [&](int k, int& i, int& j) {
+    i = dir_i ? k : L;
+    j = dir_i ? L : k;
+  };
+  float* scr = A.scratch;
+  // ---- forward elimination of the segment interior
+  M4<float> Y = zero4<float>(), GE = zero4<float>();
+  V4<float> g = mk4<float>(0, 0, 0, 0);
+  if (act) {
+    for (int k = a; k <= ke; ++k) {
+      int i, j;
+      ij(k, i, j);
+      M4<float> Ak, Bk, Ck;
+      assemble(A, c, dir_i != 0, i, j, Ak, Bk, Ck);
+      long long cc = cell(k);
+      V4<float> r = rhs_of(A, in, from_res != 0, cc);
+      M4<float> M = Bk;
+      M4<float> GEr;
+      if (k > a) {
+        axpy(M, -1.f, mm(Ak, Y));
+        V4<float> t = mv(Ak, g);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r[q] -= t[q];
+        GEr = mm(Ak, GE);
+      } else {
+        GEr = Ak;
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) GEr[q] = -GEr[q];
+      M4<float> Minv = inv4(M);
+      g = mv(Minv, r);
+      GE = mm(Minv, GEr);
+      Y = mm(Minv, Ck);
+      st_scratch(scr + 36 * cc, Y, g, GE);
+    }
+  }
+  // ---- (v, E, F) at the last interior cell and, by a backward pass, at the first
+  V4<float> v_l = g;
+  M4<float> E_l = GE, F_l;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) F_l[q] = -Y[q];
+  V4<float> v_f = v_l;
+  M4<float> E_f = E_l, F_f = F_l;
+  if (act) {
+    for (int k = ke - 1; k >= a; --k) {
+      M4<float> Yk, GEk;
+      V4<float> gk;
+      ld_scratch(scr + 36 * cell(k), Yk, gk, GEk);
+      V4<float> t = mv(Yk, v_f);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v_f[q] = gk[q] - t[q];
+      M4<float> tE = mm(Yk, E_f), tF = mm(Yk, F_f);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        E_f[q] = GEk[q] - tE[q];
+        F_f[q] = -tF[q];
+      }
+    }
+  }
+  // publish (v, E, F) of the first interior cell for the lane on the left
+  PcrSlot* my = &sp[warp][s];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    my->a[q] = E_f[q];
+    my->c[q] = F_f[q];
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) my->d[q] = v_f[q];
+  __syncwarp();
+  // ---- reduced row of the separator (the last cell of the segment)
+  const int N = P - 1;
+  M4<float> ra = zero4<float>(), rb = eye4<float>(), rc = zero4<float>();
+  V4<float> rd = mk4<float>(0, 0, 0, 0);
+  if (has_sep) {
+    int i, j;
+    ij(e - 1, i, j);
+    M4<float> As, Bs, Cs;
+    assemble(A, c, dir_i != 0, i, j, As, Bs, Cs);
+    V4<float> r = rhs_of(A, in, from_res != 0, cell(e - 1));
+    const PcrSlot* nx = &sp[warp][s + 1];
+    M4<float> En, Fn;
+    V4<float> vn;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      En[q] = nx->a[q];
+      Fn[q] = nx->c[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) vn[q] = nx->d[q];
+    ra = mm(As, E_l);
+    rb = Bs;
+    axpy(rb, 1.f, mm(As, F_l));
+    axpy(rb, 1.f, mm(Cs, En));
+    rc = mm(Cs, Fn);
+    V4<float> t1 = mv(As, v_l), t2 = mv(Cs, vn);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rd[q] = r[q] - t1[q] - t2[q];
+  }
+  __syncwarp();
+  // ---- parallel cyclic reduction of the N separator rows across the warp
+  for (int h = 1; h < N; h <<= 1) {
+    M4<float> binv = inv4(rb);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      my->a[q] = ra[q];
+      my->b[q] = binv[q];
+      my->c[q] = rc[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) my->d[q] = rd[q];
+    __syncwarp();
+    if (s < N) {
+      M4<float> na = zero4<float>(), nc = zero4<float>(), nb = rb;
+      V4<float> nd = rd;
+      if (s - h >= 0) {
+        const PcrSlot* o = &sp[warp][s - h];
+        M4<float> oa, ob, oc;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          oa[q] = o->a[q];
+          ob[q] = o->b[q];
+          oc[q] = o->c[q];
+        }
+        M4<float> al = mm(ra, ob);  // alpha = -a_i b_{i-h}^-1
+#pragma unroll
+        for (int q = 0; q < 16; ++q) al[q] = -al[q];
+        na = mm(al, oa);
+        axpy(nb, 1.f, mm(al, oc));
+        V4<float> od = mk4<float>(o->d[0], o->d[1], o->d[2], o->d[3]);
+        V4<float> t = mv(al, od);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nd[q] += t[q];
+      }
+      if (s + h < N) {
+        const PcrSlot* o = &sp[warp][s + h];
+        M4<float> oa, ob, oc;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          oa[q] = o->a[q];
+          ob[q] = o->b[q];
+          oc[q] = o->c[q];
+        }
+        M4<float> ga = mm(rc, ob);  // gamma = -c_i b_{i+h}^-1
+#pragma unroll
+        for (int q = 0; q < 16; ++q) ga[q] = -ga[q];
+        nc = mm(ga, oc);
+        axpy(nb, 1.f, mm(ga, oa));
+        V4<float> od = mk4<float>(o->d[0], o->d[1], o->d[2], o->d[3]);
+        V4<float> t = mv(ga, od);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nd[q] += t[q];
+      }
+      ra = na;
+      rb = nb;
+      rc = nc;
+      rd = nd;
+    }
+    __syncwarp();
+  }
+  V4<float> lsep = mk4<float>(0, 0, 0, 0);
+  if (s < N) lsep = mv(inv4(rb), rd);
+  sl[warp][s] = to_f4(lsep);
+  __syncwarp();
+  if (!act) return;
+  // ---- back substitution of the segment
+  V4<float> lprev = s > 0 ? from_f4(sl[warp][s - 1]) : mk4<float>(0, 0, 0, 0);
+  V4<float> xn = has_sep ? lsep : mk4<float>(0, 0, 0, 0);
+  auto emit = [&](long long cc, const V4<float>& x) {
+    if (epilogue == 0) {
+      out[cc] = to_f4(x);
+      return;
+    }
+    V4<float> du = x;
+    if (epilogue == 2) {
+      V4<float> o = from_f4(A.DU[cc]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) du[q] += o[q];
+    }
+    A.DU[cc] = to_f4(du);
+    if (update) damped_update(A.U, cc, du);
+  };
+  if (has_sep) emit(cell(e - 1), lsep);
+  for (int k = ke; k >= a; --k) {
+    M4<float> Yk, GEk;
+    V4<float> gk;
+    long long cc = cell(k);
+    ld_scratch(scr + 36 * cc, Yk, gk, GEk);
+    V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
+    V4<float> x;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
+    emit(cc, x);
+    xn = x;
+  }
+  // the line through cell 0 of the case advances its iteration counters after the update
+  if (update && L == 0 && lane == 0) {
+    A.iter[ci] += 1;
+    A.ramp_k[ci] += 1;
+  }
+}
+
+// Defect of the unfactored operator (implicit.rs:622-630): rr = dt R - (A_i du + A_j du - du), per fluid cell.
+__global__ void k_defect(Arena A) {
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (i >= c.ni || j >= c.nj) return;
+  long long cc = cidx(c, i, j);
+  if (is_solid(c, i, j)) {
+    A.RR[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  V4<float> du = from_f4(A.DU[cc]);
+  V4<float> acc = mk4<float>(0, 0, 0, 0);
+  for (int dir = 0; dir < 2; ++dir) {
+    bool di = dir == 0;
+    M4<float> lo, d, up;
+    assemble(A, c, di, i, j, lo, d, up);
+    V4<float> v = mv(d, du);
+    int k = di ? i : j, kn = di ? c.ni : c.nj;
+    int k0 = di ? row_start(c, j) : col_start(c, i);
+    if (k > k0) {
+      V4<float> t2 = mv(lo, from_f4(A.DU[di ? cidx(c, i - 1, j) : cidx(c, i, j - 1)]));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] += t2[q];
+    }
+    if (k + 1 < kn) {
+      V4<float> t2 = mv(up, from_f4(A.DU[di ? cidx(c, i + 1, j) : cidx(c, i, j + 1)]));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] += t2[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] += v[q];
+  }
+  float4 r = A.R[cc];
+  float d = A.dt[cc];
+  float4 o;
+  o.x = r.x * d - (acc[0] - du[0]);
+  o.y = r.y * d - (acc[1] - du[1]);
+  o.z = r.z * d - (acc[2] - du[2]);
+  o.w = r.w * d - (acc[3] - du[3]);
+  A.RR[cc] = o;
+}
+
+}  // namespace bk

@@ -1,0 +1,708 @@
+// Host side of a case arena: FP64 grid metrics (grid.rs:65-119), device buffers, launch tables, the launch sequence of
+// one iteration (solver.rs:658-676 with implicit.rs:601-663 or solver.rs:694-720), chunked residual read-back, and the
+// state / turbulence transfers. One arena serves one case (the GpuSolver C ABI) or many (the batched sweep).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "arena.cuh"
+
+namespace bk {
+
+struct HostCase {
+  int ni = 0, nj = 0;
+  std::vector<double> x, r;                       // nodes
+  std::vector<double> if_nx, if_nr, if_len, if_rm;  // (ni+1)*nj
+  std::vector<double> jf_nx, jf_nr, jf_len, jf_rm;  // ni*(nj+1)
+  std::vector<double> area, vol, xc, rc;
+  // configuration (doubles as given by the caller)
+  double cfl = 0.5;
+  int limiter = 1;
+  double fs[4] = {1, 0, 0, 1.0 / 1.4};
+  int bc[4] = {3, 3, 2, 3};
+  long long first_order_iters = 0;
+  int low_mach = 0;
+  int scheme = SCHEME_EXPLICIT;
+  double cfl0 = 1, cfl_max = 30, growth = 1.02, eps_fix = 0.1;
+  int dt_mode = 0, lines = 1, implicit_bc = 1, sub_iters = 2, roe = 1;
+  bool has_block = false;
+  long long i_end = 0, j_end = 0, j_sting = 0;
+  bool has_nozzle = false;
+  long long nz_j_end = 0;
+  double nz_state[4] = {0, 0, 0, 0}, nz_turb[2] = {0, 0};
+  bool viscous = false;
+  int turbulence = 0;
+  long long wall_i_start = 0;
+  double re_c = 1e6, sutherland = 0.368, roughness = 0;
+  long long n_active() const {
+    long long n = (long long)ni * nj;
+    if (has_block) n -= i_end * j_end + ((long long)ni - i_end) * j_sting;
+    return n;
+  }
+  bool solid(int i, int j) const { return has_block && (i < i_end ? j < j_end : j < j_sting); }
+  int col_start(int i) const { return has_block ? (int)(i < i_end ? j_end : j_sting) : 0; }
+  // viscous.rs:97-109 (host side: wall distance)
+  bool noslip_jface(int i, int j) const {
+    if (!viscous) return false;
+    if (!has_block) return j == 0 && bc[2] == 2 && i >= wall_i_start;
+    return (j == j_end && i >= wall_i_start && i < i_end) || (j == j_sting && j_sting > 0 && i >= i_end);
+  }
+  bool noslip_iface(int i, int j) const {
+    return viscous && has_block && i == i_end && j >= j_sting && j < j_end && !(has_nozzle && j < nz_j_end);
+  }
+};
+
+// Stencil (|d|, e_x, e_r) of every face between the positions of its two sides (a cell centroid, or for a ghost its
+// mirror image in the face centre), viscous.rs:150-250, in FP64. Faces inside the block get |d| = 1 (never read).
+inline void face_stencils(const HostCase& h, std::vector<float4>& fis, std::vector<float4>& fjs) {
+  const int ni = h.ni, nj = h.nj;
+  auto node = [&](int i, int j) { return std::make_pair(h.x[(size_t)j * (ni + 1) + i], h.r[(size_t)j * (ni + 1) + i]); };
+  auto st = [&](int cl, bool gl, int cr, bool gr, double xf, double rf) {
+    double xl = h.xc[cl], rl = h.rc[cl], xr = h.xc[cr], rr = h.rc[cr];
+    if (gl) xl = 2.0 * xf - xl, rl = 2.0 * rf - rl;
+    if (gr) xr = 2.0 * xf - xr, rr = 2.0 * rf - rr;
+    double dx = xr - xl, dr = rr - rl, dd = std::hypot(dx, dr);
+    return make_float4((float)dd, (float)(dx / dd), (float)(dr / dd), 0.f);
+  };
+  fis.assign((size_t)(ni + 1) * nj, make_float4(1.f, 1.f, 0.f, 0.f));
+  fjs.assign((size_t)ni * (nj + 1), make_float4(1.f, 0.f, 1.f, 0.f));
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i <= ni; ++i) {
+      auto a = node(i, j), b = node(i, j + 1);
+      double xf = 0.5 * (a.first + b.first), rf = 0.5 * (a.second + b.second);
+      float4& o = fis[(size_t)j * (ni + 1) + i];
+      if (h.has_block && j < h.j_end) {
+        if (j < h.j_sting || i < h.i_end) continue;
+        if (i == h.i_end) {
+          int c = j * ni + i;
+          o = st(c, true, c, false, xf, rf);
+          continue;
+        }
+      }
+      if (i == 0)
+        o = st(j * ni, true, j * ni, false, xf, rf);
+      else if (i == ni)
+        o = st(j * ni + ni - 1, false, j * ni + ni - 1, true, xf, rf);
+      else
+        o = st(j * ni + i - 1, false, j * ni + i, false, xf, rf);
+    }
+  for (int j = 0; j <= nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+      auto a = node(i, j), b = node(i + 1, j);
+      double xf = 0.5 * (a.first + b.first), rf = 0.5 * (a.second + b.second);
+      float4& o = fjs[(size_t)j * ni + i];
+      int j0 = h.col_start(i);
+      if (h.has_block) {
+        if (j < j0) continue;
+        if (j == j0 && j0 > 0) {
+          int c = j * ni + i;
+          o = st(c, true, c, false, xf, rf);
+          continue;
+        }
+      }
+      if (j == 0)
+        o = st(i, true, i, false, xf, rf);
+      else if (j == nj)
+        o = st((nj - 1) * ni + i, false, (nj - 1) * ni + i, true, xf, rf);
+      else
+        o = st((j - 1) * ni + i, false, j * ni + i, false, xf, rf);
+    }
+}
+
+// Distance of every cell centroid to the nearest no-slip wall face segment (turbulence.rs:91-125), FP64, brute force.
+inline std::vector<double> wall_distance(const HostCase& h) {
+  const int ni = h.ni, nj = h.nj;
+  std::vector<double> segs;
+  auto node = [&](int i, int j) { return std::make_pair(h.x[(size_t)j * (ni + 1) + i], h.r[(size_t)j * (ni + 1) + i]); };
+  for (int j = 0; j <= nj; ++j)
+    for (int i = 0; i < ni; ++i)
+      if (h.noslip_jface(i, j)) {
+        auto a = node(i, j), b = node(i + 1, j);
+        segs.insert(segs.end(), {a.first, a.second, b.first, b.second});
+      }
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i <= ni; ++i)
+      if (h.noslip_iface(i, j)) {
+        auto a = node(i, j), b = node(i, j + 1);
+        segs.insert(segs.end(), {a.first, a.second, b.first, b.second});
+      }
+  std::vector<double> d((size_t)ni * nj, std::numeric_limits<double>::infinity());
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+      if (h.solid(i, j)) continue;
+      size_t c = (size_t)j * ni + i;
+      double px = h.xc[c], pr = h.rc[c], best = d[c];
+      for (size_t s = 0; s + 3 < segs.size(); s += 4) {
+        double ex = segs[s + 2] - segs[s], er = segs[s + 3] - segs[s + 1];
+        double t = ((px - segs[s]) * ex + (pr - segs[s + 1]) * er) / (ex * ex + er * er);
+        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        best = std::fmin(best, std::hypot(px - (segs[s] + t * ex), pr - (segs[s + 1] + t * er)));
+      }
+      d[c] = best;
+    }
+  return d;
+}
+
+// grid.rs:65-119 in FP64; false (and a message) on a non-positive cell area
+inline bool compute_metrics(HostCase& h, std::string& err) {
+  const int ni = h.ni, nj = h.nj;
+  auto nn = [&](int i, int j) { return (size_t)j * (ni + 1) + i; };
+  const std::vector<double>&x = h.x, &r = h.r;
+  h.if_nx.assign((size_t)(ni + 1) * nj, 0);
+  h.if_nr = h.if_len = h.if_rm = h.if_nx;
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i <= ni; ++i) {
+      size_t a = nn(i, j), b = nn(i, j + 1), f = (size_t)j * (ni + 1) + i;
+      double dx = x[b] - x[a], dr = r[b] - r[a], len = std::hypot(dx, dr);
+      h.if_nx[f] = dr / len;
+      h.if_nr[f] = -dx / len;
+      h.if_len[f] = len;
+      h.if_rm[f] = 0.5 * (r[a] + r[b]);
+    }
+  h.jf_nx.assign((size_t)ni * (nj + 1), 0);
+  h.jf_nr = h.jf_len = h.jf_rm = h.jf_nx;
+  for (int j = 0; j <= nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+      size_t a = nn(i, j), b = nn(i + 1, j), f = (size_t)j * ni + i;
+      double dx = x[b] - x[a], dr = r[b] - r[a], len = std::hypot(dx, dr);
+      h.jf_nx[f] = -dr / len;
+      h.jf_nr[f] = dx / len;
+      h.jf_len[f] = len;
+      h.jf_rm[f] = 0.5 * (r[a] + r[b]);
+    }
+  size_t n = (size_t)ni * nj;
+  h.area.assign(n, 0);
+  h.vol = h.xc = h.rc = h.area;
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+      size_t p[4] = {nn(i, j), nn(i + 1, j), nn(i + 1, j + 1), nn(i, j + 1)};
+      double a = 0, v = 0, sx = 0, sr = 0;
+      const int tri[2][3] = {{0, 1, 2}, {0, 2, 3}};
+      for (auto& t : tri) {
+        size_t k0 = p[t[0]], k1 = p[t[1]], k2 = p[t[2]];
+        double at = 0.5 * ((x[k1] - x[k0]) * (r[k2] - r[k0]) - (x[k2] - x[k0]) * (r[k1] - r[k0]));
+        double cx = (x[k0] + x[k1] + x[k2]) / 3.0, cr = (r[k0] + r[k1] + r[k2]) / 3.0;
+        a += at;
+        v += at * cr;
+        sx += at * cx;
+        sr += at * cr;
+      }
+      if (!(a > 0.0)) {
+        err = "non-positive cell area at (" + std::to_string(i) + "," + std::to_string(j) + ")";
+        return false;
+      }
+      size_t c = (size_t)j * ni + i;
+      h.area[c] = a;
+      h.vol[c] = v;
+      h.xc[c] = sx / a;
+      h.rc[c] = sr / a;
+    }
+  return true;
+}
+
+#define BK_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                          \
+      return 3;                                                                          \
+    }                                                                                    \
+  } while (0)
+
+template <class T>
+inline int dalloc(T** p, size_t n, std::string& err) {
+  *p = nullptr;
+  if (n == 0) return 0;
+  BK_CUDA(cudaMalloc((void**)p, n * sizeof(T)));
+  return 0;
+}
+
+struct ArenaHost {
+  std::vector<HostCase> cases;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  bool ready = false;
+  int slots = 256;  // residual history slots per chunk
+  // host copies of the tables
+  std::vector<CaseDev> desc;
+  long long ncell = 0, npad = 0, nif = 0, njf = 0;
+  int ntiles = 0, nil = 0, njl = 0, npblk = 0;
+  bool any_viscous = false, any_sst = false;
+  // device buffers
+  Arena A{};
+  CaseDev* d_cases = nullptr;
+  int *d_iter = nullptr, *d_ramp = nullptr, *d_active = nullptr;
+  int *d_tile_case = nullptr, *d_iline = nullptr, *d_jline = nullptr, *d_pblk = nullptr;
+  std::vector<double> h_rsum;
+  cudaGraphExec_t graph = nullptr;
+  int graph_len = 0;
+  std::vector<int> h_active;
+
+  ~ArenaHost() { release(); }
+
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0,
+                    A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
+                    A.grad4, A.gradT, A.mu, A.mu_t, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
+                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+    d_cases = nullptr;
+    d_iter = d_ramp = d_active = d_tile_case = d_iline = d_jline = d_pblk = nullptr;
+    A = Arena{};
+    if (stream) cudaStreamDestroy(stream), stream = nullptr;
+    ready = false;
+  }
+
+  CaseDev make_desc(const HostCase& h) const {
+    CaseDev c{};
+    c.ni = h.ni;
+    c.nj = h.nj;
+    c.has_block = h.has_block;
+    c.i_end = (int)h.i_end;
+    c.j_end = (int)h.j_end;
+    c.j_sting = (int)h.j_sting;
+    c.has_nozzle = h.has_nozzle;
+    c.nz_j_end = (int)h.nz_j_end;
+    for (int k = 0; k < 4; ++k) c.nz_state[k] = (float)h.nz_state[k];
+    c.nz_turb[0] = (float)h.nz_turb[0];
+    c.nz_turb[1] = (float)h.nz_turb[1];
+    for (int k = 0; k < 4; ++k) {
+      c.bc[k] = h.bc[k];
+      c.fs[k] = h.fs[k];
+    }
+    c.cfl = (float)h.cfl;
+    c.limiter = h.limiter;
+    c.first_order_iters = (int)std::min<long long>(h.first_order_iters, 1 << 30);
+    c.low_mach = h.low_mach;
+    c.scheme = h.scheme;
+    c.cfl0 = (float)h.cfl0;
+    c.cfl_max = (float)h.cfl_max;
+    c.growth = (float)h.growth;
+    c.eps_fix = (float)h.eps_fix;
+    c.dt_mode = h.dt_mode;
+    c.lines = h.lines;
+    c.implicit_bc = h.implicit_bc;
+    c.sub_iters = h.sub_iters;
+    c.roe = h.roe;
+    c.viscous = h.viscous;
+    c.sst = h.viscous && h.turbulence == 1;
+    c.wall_i_start = (int)h.wall_i_start;
+    c.re_c = h.re_c;
+    c.sutherland = h.sutherland;
+    c.roughness = h.roughness;
+    c.n_active = (int)h.n_active();
+    return c;
+  }
+
+  // Lay out the arena, allocate and upload geometry (once; the case dimensions are fixed afterwards).
+  int setup() {
+    release();
+    BK_CUDA(cudaSetDevice(device));
+    BK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    const int nc = (int)cases.size();
+    desc.resize(nc);
+    ncell = npad = nif = njf = 0;
+    ntiles = nil = njl = npblk = 0;
+    std::vector<int> tile_case, iline, jline, pblk;
+    for (int k = 0; k < nc; ++k) {
+      HostCase& h = cases[k];
+      CaseDev c = make_desc(h);
+      c.cell_off = ncell;
+      c.pad_off = npad;
+      c.if_off = nif;
+      c.jf_off = njf;
+      c.ntx = (h.ni + TI - 1) / TI;
+      c.nty = (h.nj + TJ - 1) / TJ;
+      c.tile_off = ntiles;
+      c.iline_off = nil;
+      c.jline_off = njl;
+      c.pblk_off = npblk;
+      int nt = c.ntx * c.nty, nb = (int)(((long long)(h.ni + 4) * (h.nj + 4) + 255) / 256);
+      tile_case.insert(tile_case.end(), nt, k);
+      iline.insert(iline.end(), h.nj, k);
+      jline.insert(jline.end(), h.ni, k);
+      pblk.insert(pblk.end(), nb, k);
+      ntiles += nt;
+      nil += h.nj;
+      njl += h.ni;
+      npblk += nb;
+      ncell += (long long)h.ni * h.nj;
+      npad += (long long)(h.ni + 4) * (h.nj + 4);
+      nif += (long long)(h.ni + 1) * h.nj;
+      njf += (long long)h.ni * (h.nj + 1);
+      desc[k] = c;
+    }
+    int rc = 0;
+#define ALLOC(p, n) \
+  if ((rc = dalloc(&(p), (size_t)(n), err))) return rc
+    ALLOC(d_cases, nc);
+    ALLOC(d_iter, nc);
+    ALLOC(d_ramp, nc);
+    ALLOC(d_active, nc);
+    ALLOC(d_tile_case, ntiles);
+    ALLOC(d_iline, nil);
+    ALLOC(d_jline, njl);
+    ALLOC(d_pblk, npblk);
+    ALLOC(A.U, ncell);
+    ALLOC(A.W, npad);
+    ALLOC(A.R, ncell);
+    ALLOC(A.X, ncell);
+    ALLOC(A.DU, ncell);
+    ALLOC(A.RR, ncell);
+    ALLOC(A.U0, ncell);
+    ALLOC(A.dt, ncell);
+    float4 *fi, *fj, *cg;
+    float2 *ic, *jc;
+    ALLOC(fi, nif);
+    ALLOC(fj, njf);
+    ALLOC(cg, ncell);
+    ALLOC(ic, nif);
+    ALLOC(jc, njf);
+    A.iface = fi;
+    A.jface = fj;
+    A.cellg = cg;
+    A.ifc = ic;
+    A.jfc = jc;
+    ALLOC(A.scratch, ncell * 36);
+    ALLOC(A.rsum, (size_t)slots * nc);
+    ALLOC(A.tsum, (size_t)slots * nc);
+    float4 *fis, *fjs;
+    ALLOC(fis, nif);
+    ALLOC(fjs, njf);
+    A.ifs = fis;
+    A.jfs = fjs;
+    BK_CUDA(cudaMemcpy(d_tile_case, tile_case.data(), tile_case.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_iline, iline.data(), iline.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_jline, jline.data(), jline.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_pblk, pblk.data(), pblk.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // geometry
+    std::vector<float4> hfi(nif), hfj(njf), hcg(ncell);
+    std::vector<float2> hic(nif), hjc(njf);
+    for (int k = 0; k < nc; ++k) {
+      const HostCase& h = cases[k];
+      const CaseDev& c = desc[k];
+      for (int j = 0; j < h.nj; ++j)
+        for (int i = 0; i <= h.ni; ++i) {
+          size_t f = (size_t)j * (h.ni + 1) + i;
+          hfi[c.if_off + f] = make_float4((float)h.if_nx[f], (float)h.if_nr[f], (float)h.if_len[f], (float)(h.if_len[f] * h.if_rm[f]));
+          size_t a = (size_t)j * (h.ni + 1) + i, b = (size_t)(j + 1) * (h.ni + 1) + i;
+          hic[c.if_off + f] = make_float2((float)(0.5 * (h.x[a] + h.x[b])), (float)(0.5 * (h.r[a] + h.r[b])));
+        }
+      for (int j = 0; j <= h.nj; ++j)
+        for (int i = 0; i < h.ni; ++i) {
+          size_t f = (size_t)j * h.ni + i;
+          hfj[c.jf_off + f] = make_float4((float)h.jf_nx[f], (float)h.jf_nr[f], (float)h.jf_len[f], (float)(h.jf_len[f] * h.jf_rm[f]));
+          size_t a = (size_t)j * (h.ni + 1) + i, b = a + 1;
+          hjc[c.jf_off + f] = make_float2((float)(0.5 * (h.x[a] + h.x[b])), (float)(0.5 * (h.r[a] + h.r[b])));
+        }
+      for (int j = 0; j < h.nj; ++j)
+        for (int i = 0; i < h.ni; ++i) {
+          size_t cc = (size_t)j * h.ni + i;
+          hcg[c.cell_off + cc] = make_float4((float)h.vol[cc], (float)h.area[cc], (float)h.xc[cc], (float)h.rc[cc]);
+        }
+    }
+    BK_CUDA(cudaMemcpy(fi, hfi.data(), nif * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(fj, hfj.data(), njf * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(cg, hcg.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(ic, hic.data(), nif * sizeof(float2), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(jc, hjc.data(), njf * sizeof(float2), cudaMemcpyHostToDevice));
+    A.ncases = nc;
+    A.cases = d_cases;
+    A.iter = d_iter;
+    A.ramp_k = d_ramp;
+    A.active = d_active;
+    A.tile_case = d_tile_case;
+    A.ntiles = ntiles;
+    A.iline_case = d_iline;
+    A.nilines = nil;
+    A.jline_case = d_jline;
+    A.njlines = njl;
+    A.pblk_case = d_pblk;
+    A.npblk = npblk;
+    std::vector<int> zero(nc, 0);
+    h_active.assign(nc, 1);
+    BK_CUDA(cudaMemcpy(d_iter, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_ramp, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_active, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    ready = true;
+    if ((rc = upload_desc())) return rc;
+    for (int k = 0; k < nc; ++k)
+      if ((rc = reset_case(k))) return rc;
+    return 0;
+  }
+
+  // Re-derive the descriptors from the host configuration (config, scheme, block, viscous changes).
+  int upload_desc() {
+    any_viscous = any_sst = false;
+    for (size_t k = 0; k < cases.size(); ++k) {
+      CaseDev c = make_desc(cases[k]);
+      CaseDev& d = desc[k];
+      c.cell_off = d.cell_off;
+      c.pad_off = d.pad_off;
+      c.if_off = d.if_off;
+      c.jf_off = d.jf_off;
+      c.tile_off = d.tile_off;
+      c.ntx = d.ntx;
+      c.nty = d.nty;
+      c.iline_off = d.iline_off;
+      c.jline_off = d.jline_off;
+      c.pblk_off = d.pblk_off;
+      d = c;
+      any_viscous |= c.viscous != 0;
+      any_sst |= c.sst != 0;
+    }
+    int rc = 0;
+    if (any_viscous && !A.mu) {
+      ALLOC(A.grad4, ncell);
+      ALLOC(A.gradT, ncell);
+      ALLOC(A.mu, ncell);
+      ALLOC(A.mu_t, ncell);
+      ALLOC(A.fvi, nif);
+      ALLOC(A.fvj, njf);
+      BK_CUDA(cudaMemset(A.mu_t, 0, ncell * sizeof(float)));
+      BK_CUDA(cudaMemset(A.fvi, 0, nif * sizeof(float4)));
+      BK_CUDA(cudaMemset(A.fvj, 0, njf * sizeof(float4)));
+    }
+    if (any_sst && !A.turb) {
+      ALLOC(A.turb, ncell);
+      ALLOC(A.dwall, ncell);
+      ALLOC(A.mflux_i, nif);
+      ALLOC(A.mflux_j, njf);
+      ALLOC(A.tcoef, 3 * ncell);
+      ALLOC(A.trhs, ncell);
+      ALLOC(A.grad_kw, ncell);
+      ALLOC(A.blend, ncell);
+      BK_CUDA(cudaMemset(A.mflux_i, 0, nif * sizeof(float)));
+      BK_CUDA(cudaMemset(A.mflux_j, 0, njf * sizeof(float)));
+    }
+    if ((rc = upload_stencils())) return rc;
+    BK_CUDA(cudaMemcpy(d_cases, desc.data(), desc.size() * sizeof(CaseDev), cudaMemcpyHostToDevice));
+    if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    return 0;
+  }
+#undef ALLOC
+
+  int upload_stencils() {
+    std::vector<float4> fis, fjs;
+    for (size_t k = 0; k < cases.size(); ++k) {
+      face_stencils(cases[k], fis, fjs);
+      BK_CUDA(cudaMemcpy((void*)(A.ifs + desc[k].if_off), fis.data(), fis.size() * sizeof(float4), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy((void*)(A.jfs + desc[k].jf_off), fjs.data(), fjs.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    }
+    return 0;
+  }
+
+  // turbulence.rs:128-138: free-stream (k, omega) everywhere, the wall distance, mu_t = rho k / omega on fluid cells
+  std::vector<double> last_turb_residual;
+  int turb_init(int k) {
+    const HostCase& h = cases[k];
+    const CaseDev& c = desc[k];
+    size_t n = (size_t)h.ni * h.nj;
+    double winf = 1e-6 * h.re_c, kinf = 9e-9;
+    std::vector<double> d = wall_distance(h);
+    std::vector<float> df(n), mt(n);
+    std::vector<float2> t(n, make_float2((float)kinf, (float)winf));
+    std::vector<double> u(4 * n);
+    int rc = get_state(k, u.data());
+    if (rc) return rc;
+    for (size_t cc = 0; cc < n; ++cc) {
+      df[cc] = std::isfinite(d[cc]) ? (float)d[cc] : 3.0e38f;
+      mt[cc] = h.solid((int)(cc % h.ni), (int)(cc / h.ni)) ? 0.f : (float)(u[4 * cc] * kinf / winf);
+    }
+    BK_CUDA(cudaMemcpy(A.dwall + c.cell_off, df.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(A.turb + c.cell_off, t.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(A.mu_t + c.cell_off, mt.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int turb_upload(int k, const double* turb, const double* mu_t) {
+    const CaseDev& c = desc[k];
+    size_t n = (size_t)c.ni * c.nj;
+    if (turb) {
+      std::vector<float2> t(n);
+      for (size_t i = 0; i < n; ++i) t[i] = make_float2((float)turb[2 * i], (float)turb[2 * i + 1]);
+      BK_CUDA(cudaMemcpy(A.turb + c.cell_off, t.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    if (mu_t) {
+      std::vector<float> m(n);
+      for (size_t i = 0; i < n; ++i) m[i] = (float)mu_t[i];
+      BK_CUDA(cudaMemcpy(A.mu_t + c.cell_off, m.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return 0;
+  }
+
+  int reset_case(int k) {
+    const HostCase& h = cases[k];
+    double w[4] = {h.fs[0], h.fs[1], h.fs[2], h.fs[3]};
+    double q[4] = {w[0], w[0] * w[1], w[0] * w[2], w[3] / 0.4 + 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2])};
+    std::vector<double> u((size_t)h.ni * h.nj * 4);
+    for (size_t c = 0; c < (size_t)h.ni * h.nj; ++c)
+      for (int m = 0; m < 4; ++m) u[4 * c + m] = q[m];
+    return set_state(k, u.data());
+  }
+
+  int set_state(int k, const double* u) {
+    const CaseDev& c = desc[k];
+    size_t n = (size_t)c.ni * c.nj;
+    std::vector<float4> h(n);
+    for (size_t i = 0; i < n; ++i) h[i] = make_float4((float)u[4 * i], (float)u[4 * i + 1], (float)u[4 * i + 2], (float)u[4 * i + 3]);
+    BK_CUDA(cudaMemcpy(A.U + c.cell_off, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    int z = 0;
+    BK_CUDA(cudaMemcpy(d_iter + k, &z, sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_ramp + k, &z, sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+  }
+
+  int get_state(int k, double* u) {
+    const CaseDev& c = desc[k];
+    size_t n = (size_t)c.ni * c.nj;
+    std::vector<float4> h(n);
+    BK_CUDA(cudaStreamSynchronize(stream));
+    BK_CUDA(cudaMemcpy(h.data(), A.U + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) {
+      u[4 * i] = h[i].x;
+      u[4 * i + 1] = h[i].y;
+      u[4 * i + 2] = h[i].z;
+      u[4 * i + 3] = h[i].w;
+    }
+    return 0;
+  }
+
+  int set_counter(int* d, int k, int v) {
+    BK_CUDA(cudaMemcpy(d + k, &v, sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int get_counter(const int* d, int k, int& v) {
+    BK_CUDA(cudaStreamSynchronize(stream));
+    BK_CUDA(cudaMemcpy(&v, d + k, sizeof(int), cudaMemcpyDeviceToHost));
+    return 0;
+  }
+  int set_active(const int* act) {
+    for (size_t k = 0; k < cases.size(); ++k) h_active[k] = act[k] ? 1 : 0;
+    BK_CUDA(cudaMemcpyAsync(d_active, h_active.data(), cases.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    BK_CUDA(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  // ---------------------------------------------------------------- one iteration (stream-ordered launches)
+  void launch_mean_flow_prep() {
+    k_prims<<<npblk, 256, 0, stream>>>(A);
+    if (any_viscous) {
+      k_visc_cell<<<ntiles, TI * TJ, 0, stream>>>(A);
+      k_visc_face<<<ntiles, TI * TJ, 0, stream>>>(A);
+    }
+  }
+  int scheme_of_arena() const { return desc.empty() ? 0 : desc[0].scheme; }
+  int sub_iters_of_arena() const {
+    int s = 1;
+    for (auto& d : desc) s = std::max(s, d.sub_iters);
+    return s;
+  }
+  void launch_iteration(int slot) {
+    const int lb_i = (nil + LINE_WARPS - 1) / LINE_WARPS, lb_j = (njl + LINE_WARPS - 1) / LINE_WARPS;
+    if (scheme_of_arena() == SCHEME_IMPLICIT) {
+      launch_mean_flow_prep();
+      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot);
+      const int s = sub_iters_of_arena();
+      k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X, 0, 0);
+      k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, 1, s == 1 ? 1 : 0);
+      for (int p = 1; p < s; ++p) {
+        k_defect<<<ntiles, TI * TJ, 0, stream>>>(A);
+        k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, 0, A.X, 0, 0);
+        k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, 2, p == s - 1 ? 1 : 0);
+      }
+      if (any_sst) {
+        // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step
+        k_turb_grad<<<ntiles, TI * TJ, 0, stream>>>(A);
+        k_turb_blend<<<ntiles, TI * TJ, 0, stream>>>(A);
+        k_turb_cell<<<ntiles, TI * TJ, 0, stream>>>(A, slot);
+        k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1);
+        k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0);
+        k_turb_update<<<ntiles, TI * TJ, 0, stream>>>(A);
+      }
+    } else {
+      launch_mean_flow_prep();
+      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot);
+      k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0);
+      launch_mean_flow_prep();
+      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1);
+      k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0);
+      launch_mean_flow_prep();
+      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1);
+      k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1);
+    }
+  }
+
+  // n iterations; residual (n x ncases, iteration-major) may be null
+  int run(long long n, double* residual) {
+    const int nc = (int)cases.size();
+    long long done = 0;
+    while (done < n) {
+      int chunk = (int)std::min<long long>(n - done, slots);
+      BK_CUDA(cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream));
+      if (any_sst) BK_CUDA(cudaMemsetAsync(A.tsum, 0, (size_t)chunk * nc * sizeof(double), stream));
+      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      BK_CUDA(cudaGetLastError());
+      if (residual) {
+        h_rsum.resize((size_t)chunk * nc);
+        BK_CUDA(cudaMemcpyAsync(h_rsum.data(), A.rsum, h_rsum.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      }
+      std::vector<double> ht;
+      if (any_sst) {
+        ht.resize(nc);
+        BK_CUDA(cudaMemcpyAsync(ht.data(), A.tsum + (size_t)(chunk - 1) * nc, nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      }
+      BK_CUDA(cudaStreamSynchronize(stream));
+      if (any_sst) {
+        last_turb_residual.resize(nc);
+        for (int c = 0; c < nc; ++c) last_turb_residual[c] = std::sqrt(ht[c] / (double)desc[c].n_active);
+      }
+      if (residual)
+        for (int k = 0; k < chunk; ++k)
+          for (int c = 0; c < nc; ++c)
+            residual[(done + k) * nc + c] = std::sqrt(h_rsum[(size_t)k * nc + c] / (double)desc[c].n_active);
+      done += chunk;
+    }
+    return 0;
+  }
+
+  // Solver::eval_residual of the current state (no update): dt_kind 1 = explicit dt, 2 = implicit dt
+  int eval_residual(int dt_kind, std::vector<double>* dens) {
+    const int nc = (int)cases.size();
+    BK_CUDA(cudaMemsetAsync(A.rsum, 0, nc * sizeof(double), stream));
+    launch_mean_flow_prep();
+    k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, dt_kind, 0);
+    BK_CUDA(cudaGetLastError());
+    std::vector<double> h(nc);
+    BK_CUDA(cudaMemcpyAsync(h.data(), A.rsum, nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    BK_CUDA(cudaStreamSynchronize(stream));
+    if (dens) {
+      dens->resize(nc);
+      for (int c = 0; c < nc; ++c) (*dens)[c] = std::sqrt(h[c] / (double)desc[c].n_active);
+    }
+    return 0;
+  }
+
+  template <class T, class D>
+  int download_cells(int k, const T* dptr, std::vector<D>& out, int comps) {
+    const CaseDev& c = desc[k];
+    size_t n = (size_t)c.ni * c.nj;
+    std::vector<T> h(n);
+    BK_CUDA(cudaStreamSynchronize(stream));
+    BK_CUDA(cudaMemcpy(h.data(), dptr + c.cell_off, n * sizeof(T), cudaMemcpyDeviceToHost));
+    out.resize(n * comps);
+    const float* f = reinterpret_cast<const float*>(h.data());
+    for (size_t i = 0; i < n * comps; ++i) out[i] = f[i];
+    return 0;
+  }
+};
+
+}  // namespace bk

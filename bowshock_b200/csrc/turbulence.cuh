@@ -1,0 +1,345 @@
+// Menter SST k-omega update (crates/bowshock-cfd/src/turbulence.rs:542-611) on the arena, loosely coupled after each
+// mean-flow iteration as in the reference:
+//   k_turb_grad   Green-Gauss gradients of k and omega with the boundary states of the two scalars (turbulence.rs:337-372)
+//   k_turb_blend  F1 and the cross-diffusion X (turbulence.rs:375-397)
+//   k_turb_cell   face convection / diffusion data of the four faces (turbulence.rs:413-435) and the cell terms: residual,
+//                 diag0 and the coefficients of the i- and j-line systems (turbulence.rs:477-519, 559-579)
+//   k_turb_lines  the two scalar tridiagonal line systems, i then j, one thread per (line, scalar) (turbulence.rs:580-581)
+//   k_turb_update clipped update and the new eddy viscosity (turbulence.rs:584-603)
+// Host helpers: the turbulence initialisation (free stream, wall distance in FP64, mu_t; turbulence.rs:128-138).
+#pragma once
+#include "arena.cuh"
+#include "device_math.cuh"
+#include "viscous.cuh"
+
+namespace bk {
+
+constexpr float K_INF = 9e-9f;
+constexpr float A1 = 0.31f, BETA_STAR = 0.09f, SIGMA_K1 = 0.85f, SIGMA_K2 = 1.0f, SIGMA_W1 = 0.5f, SIGMA_W2 = 0.856f, BETA1 = 0.075f,
+                BETA2 = 0.0828f, GAMMA1 = 5.0f / 9.0f, GAMMA2 = 0.44f;
+
+enum { KIND_CELL = 0, KIND_INF = 1, KIND_FIXED = 2, KIND_WALL = 3 };
+__device__ __forceinline__ int bc_kind(int bc) { return (bc == BC_FREESTREAM || bc == BC_CHARACTERISTIC || bc == BC_PRESSURE_OUTFLOW) ? KIND_INF : KIND_CELL; }
+__device__ __forceinline__ float omega_inf(const CaseDev& c) { return (float)(1e-6 * c.re_c); }
+
+// Ctx::iface / jface (turbulence.rs:188-221): the origin of the ghost state of the two scalars
+__device__ __forceinline__ int ikind(const CaseDev& c, int i, const SidesD& s) {
+  if (i == 0) return bc_kind(c.bc[0]);
+  if (i == c.ni) return bc_kind(c.bc[1]);
+  if (s.l.ghost && s.l.fixed && c.has_nozzle) return KIND_FIXED;
+  if (s.l.ghost && s.noslip) return KIND_WALL;
+  return KIND_CELL;
+}
+__device__ __forceinline__ int jkind(const CaseDev& c, int j, const SidesD& s) {
+  if (s.l.ghost) {
+    if (s.noslip) return KIND_WALL;
+    if (j == 0) return bc_kind(c.bc[2]);
+    return KIND_CELL;
+  }
+  if (s.r.ghost) return bc_kind(c.bc[3]);
+  return KIND_CELL;
+}
+// Ctx::kw (turbulence.rs:224-245), smooth walls
+__device__ __forceinline__ float2 kw_side(const Arena& A, const CaseDev& c, const SideD& s, int kind) {
+  float2 t = A.turb[s.cell];
+  if (!s.ghost || kind == KIND_CELL) return t;
+  if (kind == KIND_INF) return make_float2(K_INF, omega_inf(c));
+  if (kind == KIND_FIXED) return make_float2(c.nz_turb[0], c.nz_turb[1]);
+  long long cc = s.cell;
+  int i = (int)((cc - c.cell_off) % c.ni), j = (int)((cc - c.cell_off) / c.ni);
+  float rho = A.W[pidx(c, i, j)].x;
+  float nu = A.mu[cc] / rho;
+  float d = A.dwall[cc];
+  return make_float2(-t.x, 2.f * (60.f * nu / (BETA1 * d * d)) - t.y);
+}
+
+__global__ void k_turb_grad(Arena A) {  // turbulence.rs:337-372
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (i >= c.ni || j >= c.nj) return;
+  long long cc = cidx(c, i, j);
+  if (is_solid(c, i, j)) {
+    A.grad_kw[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  float2 pc = A.turb[cc];
+  SidesD sl, sr, sb, st;
+  iface_sides_d(A, c, i, j, sl);
+  iface_sides_d(A, c, i + 1, j, sr);
+  jface_sides_d(A, c, i, j, sb);
+  jface_sides_d(A, c, i, j + 1, st);
+  float2 nb[4] = {kw_side(A, c, sr.r, ikind(c, i + 1, sr)), kw_side(A, c, sl.l, ikind(c, i, sl)), kw_side(A, c, st.r, jkind(c, j + 1, st)),
+                  kw_side(A, c, sb.l, jkind(c, j, sb))};
+  float4 fs4[4] = {A.iface[ifidx(c, i + 1, j)], A.iface[ifidx(c, i, j)], A.jface[jfidx(c, i, j + 1)], A.jface[jfidx(c, i, j)]};
+  const float sg[4] = {1.f, -1.f, 1.f, -1.f};
+  float g[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    float pk = 0.5f * (pc.x + nb[f].x), pw = 0.5f * (pc.y + nb[f].y);
+    g[0] += sg[f] * pk * fs4[f].x * fs4[f].z;
+    g[1] += sg[f] * pk * fs4[f].y * fs4[f].z;
+    g[2] += sg[f] * pw * fs4[f].x * fs4[f].z;
+    g[3] += sg[f] * pw * fs4[f].y * fs4[f].z;
+  }
+  float inv_a = 1.f / A.cellg[cc].y;
+  A.grad_kw[cc] = make_float4(g[0] * inv_a, g[1] * inv_a, g[2] * inv_a, g[3] * inv_a);
+}
+
+__global__ void k_turb_blend(Arena A) {  // turbulence.rs:375-397
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (i >= c.ni || j >= c.nj) return;
+  long long cc = cidx(c, i, j);
+  if (is_solid(c, i, j)) {
+    A.blend[cc] = make_float2(0.f, 0.f);
+    return;
+  }
+  float rho = A.W[pidx(c, i, j)].x;
+  float nu = A.mu[cc] / rho;
+  float2 kw = A.turb[cc];
+  float d = A.dwall[cc];
+  float4 g = A.grad_kw[cc];
+  float x = 2.f * rho * SIGMA_W2 * (g.x * g.z + g.y * g.w) / kw.y;
+  float cd = fmaxf(x, 1e-20f);
+  float t1 = sqrtf(kw.x) / (BETA_STAR * kw.y * d), t2 = 500.f * nu / (d * d * kw.y);
+  float t3 = 4.f * rho * SIGMA_W2 * kw.x / (cd * d * d);
+  float a = fminf(fmaxf(t1, t2), t3);
+  float a2 = a * a;
+  A.blend[cc] = make_float2(tanhf(a2 * a2), x);
+}
+
+struct TFaceD {
+  float m, g0, g1, f0, f1;
+  float2 l, r;
+};
+
+// turbulence.rs:413-435
+__device__ TFaceD tface_d(const Arena& A, const CaseDev& c, const SidesD& s, int kind, float4 f, float4 st, float m) {
+  TFaceD o;
+  o.m = m;
+  o.l = kw_side(A, c, s.l, kind);
+  o.r = kw_side(A, c, s.r, kind);
+  o.g0 = o.g1 = o.f0 = o.f1 = 0.f;
+  if (f.w == 0.f) return o;
+  float dd = st.x, ex = st.y, er = st.z;
+  float4 gl = A.grad_kw[s.l.cell], gr = A.grad_kw[s.r.cell];
+  float mu_f, mut_f;
+  face_mu_d(A, s, mu_f, mut_f);
+  float f1l = A.blend[s.l.cell].x, f1r = A.blend[s.r.cell].x;
+  {
+    float sigma = 0.5f * (f1l * SIGMA_K1 + (1.f - f1l) * SIGMA_K2 + f1r * SIGMA_K1 + (1.f - f1r) * SIGMA_K2);
+    float coef = mu_f + sigma * mut_f;
+    float gbx = 0.5f * (gl.x + gr.x), gbr = 0.5f * (gl.y + gr.y);
+    float corr = (o.r.x - o.l.x) / dd - (gbx * ex + gbr * er);
+    float gn = (gbx + corr * ex) * f.x + (gbr + corr * er) * f.y;
+    o.f0 = coef * gn * f.w;
+    o.g0 = coef * f.w / dd;
+  }
+  {
+    float sigma = 0.5f * (f1l * SIGMA_W1 + (1.f - f1l) * SIGMA_W2 + f1r * SIGMA_W1 + (1.f - f1r) * SIGMA_W2);
+    float coef = mu_f + sigma * mut_f;
+    float gbx = 0.5f * (gl.z + gr.z), gbr = 0.5f * (gl.w + gr.w);
+    float corr = (o.r.y - o.l.y) / dd - (gbx * ex + gbr * er);
+    float gn = (gbx + corr * ex) * f.x + (gbr + corr * er) * f.y;
+    o.f1 = coef * gn * f.w;
+    o.g1 = coef * f.w / dd;
+  }
+  return o;
+}
+
+__device__ __forceinline__ float strain2(float4 g, float v, float r) {  // turbulence.rs:250-255
+  float vr = v / r;
+  float div = g.x + g.w + vr;
+  float shear = g.y + g.z;
+  return 2.f * (g.x * g.x + g.w * g.w + vr * vr) + shear * shear - 2.f / 3.f * div * div;
+}
+
+// Cell terms and line coefficients (turbulence.rs:477-519, 559-579). Coefficients per cell:
+//   tcoef[3c+0] = (lo_i k, lo_i w, up_i k, up_i w), [3c+1] = (d_i k, d_i w, lo_j k / d0k, lo_j w / d0w),
+//   [3c+2] = (up_j k / d0k, up_j w / d0w, d_j k, d_j w); trhs[c] = V R (the i-line right-hand side).
+__global__ void k_turb_cell(Arena A, int slot) {
+  __shared__ double sred[TI * TJ / 32];
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  double rr = 0.0;
+  if (i < c.ni && j < c.nj) {
+    long long cc = cidx(c, i, j);
+    if (is_solid(c, i, j)) {
+      A.tcoef[3 * cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+      A.tcoef[3 * cc + 1] = make_float4(1.f, 1.f, 0.f, 0.f);
+      A.tcoef[3 * cc + 2] = make_float4(0.f, 0.f, 1.f, 1.f);
+      A.trhs[cc] = make_float2(0.f, 0.f);
+    } else {
+      float4 g = A.cellg[cc];
+      float vol = g.x;
+      float4 wc = A.W[pidx(c, i, j)];
+      float rho = wc.x;
+      float2 kw = A.turb[cc];
+      float2 bl = A.blend[cc];
+      float f1 = bl.x;
+      float s2 = strain2(A.grad4[cc], wc.z, g.w);
+      float mut_c = A.mu_t[cc];
+      float prod = fminf(mut_c * s2, 10.f * BETA_STAR * rho * kw.x * kw.y);
+      float beta = f1 * BETA1 + (1.f - f1) * BETA2;
+      float gamma = f1 * GAMMA1 + (1.f - f1) * GAMMA2;
+      float src0 = prod - BETA_STAR * rho * kw.y * kw.x;
+      float src1 = gamma * rho * prod / fmaxf(mut_c, 1e-30f) - beta * rho * kw.y * kw.y + (1.f - f1) * bl.y;
+      float dest0 = BETA_STAR * kw.y, dest1 = 2.f * beta * kw.y;
+      // the four faces
+      TFaceD fa[4];
+      {
+        SidesD s;
+        iface_sides_d(A, c, i, j, s);
+        fa[0] = tface_d(A, c, s, ikind(c, i, s), A.iface[ifidx(c, i, j)], A.ifs[ifidx(c, i, j)], A.mflux_i[ifidx(c, i, j)] * A.iface[ifidx(c, i, j)].w);
+        iface_sides_d(A, c, i + 1, j, s);
+        fa[1] = tface_d(A, c, s, ikind(c, i + 1, s), A.iface[ifidx(c, i + 1, j)], A.ifs[ifidx(c, i + 1, j)],
+                        A.mflux_i[ifidx(c, i + 1, j)] * A.iface[ifidx(c, i + 1, j)].w);
+        jface_sides_d(A, c, i, j, s);
+        fa[2] = tface_d(A, c, s, jkind(c, j, s), A.jface[jfidx(c, i, j)], A.jfs[jfidx(c, i, j)], A.mflux_j[jfidx(c, i, j)] * A.jface[jfidx(c, i, j)].w);
+        jface_sides_d(A, c, i, j + 1, s);
+        fa[3] = tface_d(A, c, s, jkind(c, j + 1, s), A.jface[jfidx(c, i, j + 1)], A.jfs[jfidx(c, i, j + 1)],
+                        A.mflux_j[jfidx(c, i, j + 1)] * A.jface[jfidx(c, i, j + 1)].w);
+      }
+      bool ends_lo[2] = {i == row_start(c, j), j == col_start(c, i)};
+      bool ends_up[2] = {i == c.ni - 1, j == c.nj - 1};
+      float rate0 = 0.f, rate1 = 0.f;
+      float lo[2][2], dd[2][2], up[2][2];
+#pragma unroll
+      for (int dir = 0; dir < 2; ++dir) {
+        const TFaceD& lf = fa[2 * dir];
+        const TFaceD& uf = fa[2 * dir + 1];
+        float a_lo = fmaxf(lf.m, 0.f), a_up = fmaxf(-uf.m, 0.f);
+        rate0 += a_lo * (lf.l.x - kw.x) + a_up * (uf.r.x - kw.x) + uf.f0 - lf.f0;
+        rate1 += a_lo * (lf.l.y - kw.y) + a_up * (uf.r.y - kw.y) + uf.f1 - lf.f1;
+        lo[dir][0] = ends_lo[dir] ? 0.f : -(a_lo + lf.g0);
+        lo[dir][1] = ends_lo[dir] ? 0.f : -(a_lo + lf.g1);
+        up[dir][0] = ends_up[dir] ? 0.f : -(a_up + uf.g0);
+        up[dir][1] = ends_up[dir] ? 0.f : -(a_up + uf.g1);
+        dd[dir][0] = a_lo + a_up + lf.g0 + uf.g0;
+        dd[dir][1] = a_lo + a_up + lf.g1 + uf.g1;
+      }
+      float r0 = rate0 / vol + src0, r1 = rate1 / vol + src1;
+      float dtc = A.dt[cc];
+      float d00 = rho * vol / dtc + rho * vol * dest0, d01 = rho * vol / dtc + rho * vol * dest1;
+      A.tcoef[3 * cc] = make_float4(lo[0][0], lo[0][1], up[0][0], up[0][1]);
+      A.tcoef[3 * cc + 1] = make_float4(d00 + dd[0][0], d01 + dd[0][1], lo[1][0] / d00, lo[1][1] / d01);
+      A.tcoef[3 * cc + 2] = make_float4(up[1][0] / d00, up[1][1] / d01, 1.f + dd[1][0] / d00, 1.f + dd[1][1] / d01);
+      A.trhs[cc] = make_float2(vol * r0, vol * r1);
+      rr = (double)r0 * (double)r0;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) rr += __shfl_down_sync(0xffffffffu, rr, o);
+  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = rr;
+  __syncthreads();
+  if (threadIdx.x == 0 && slot >= 0) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sred[k];
+    atomicAdd(&A.tsum[(long long)slot * A.ncases + ci], s);
+  }
+}
+
+// Scalar tridiagonal solve along every i (dir 1) or j (dir 0) line, one thread per (line, scalar): x <- A^-1 x in place
+// in trhs (turbulence.rs:580-581 with the block solver's diagonal blocks, implicit.rs:179-204).
+__global__ void k_turb_lines(Arena A, int dir_i) {
+  int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  int nl = dir_i ? A.nilines : A.njlines;
+  if (gt >= 2 * nl) return;
+  int line = gt >> 1, e = gt & 1;
+  int ci = dir_i ? A.iline_case[line] : A.jline_case[line];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  int L = line - (dir_i ? c.iline_off : c.jline_off);
+  int n = dir_i ? c.ni : c.nj;
+  int k0 = dir_i ? row_start(c, L) : col_start(c, L);
+  if (n - k0 <= 0) return;
+  float* cp = A.scratch;  // 36 floats per cell: slots 0 / 1 hold the Thomas c' of the two scalars
+  float xprev = 0.f, cprev = 0.f;
+  for (int k = k0; k < n; ++k) {
+    long long cc = dir_i ? cidx(c, k, L) : cidx(c, L, k);
+    float4 t0 = A.tcoef[3 * cc], t1 = A.tcoef[3 * cc + 1], t2 = A.tcoef[3 * cc + 2];
+    float lo, d, up;
+    if (dir_i) {
+      lo = e ? t0.y : t0.x;
+      up = e ? t0.w : t0.z;
+      d = e ? t1.y : t1.x;
+    } else {
+      lo = e ? t1.w : t1.z;
+      up = e ? t2.y : t2.x;
+      d = e ? t2.w : t2.z;
+    }
+    float2 r2 = A.trhs[cc];
+    float r = e ? r2.y : r2.x;
+    float m = d, rhs = r;
+    if (k > k0) {
+      m -= lo * cprev;
+      rhs -= lo * xprev;
+    }
+    float minv = 1.f / m;
+    float x = minv * rhs;
+    float cpk = minv * up;
+    cp[36 * cc + e] = cpk;
+    if (e)
+      A.trhs[cc].y = x;
+    else
+      A.trhs[cc].x = x;
+    xprev = x;
+    cprev = cpk;
+  }
+  for (int k = n - 2; k >= k0; --k) {
+    long long cc = dir_i ? cidx(c, k, L) : cidx(c, L, k);
+    long long cn = dir_i ? cidx(c, k + 1, L) : cidx(c, L, k + 1);
+    float xn = e ? A.trhs[cn].y : A.trhs[cn].x;
+    float v = (e ? A.trhs[cc].y : A.trhs[cc].x) - cp[36 * cc + e] * xn;
+    if (e)
+      A.trhs[cc].y = v;
+    else
+      A.trhs[cc].x = v;
+  }
+}
+
+__global__ void k_turb_update(Arena A) {  // turbulence.rs:584-603
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (i >= c.ni || j >= c.nj) return;
+  long long cc = cidx(c, i, j);
+  if (is_solid(c, i, j)) {
+    A.turb[cc] = make_float2(0.f, 0.f);
+    A.mu_t[cc] = 0.f;
+    return;
+  }
+  float2 kw0 = A.turb[cc];
+  float2 x = A.trhs[cc];
+  float winf = omega_inf(c);
+  float k = fmaxf(fmaxf(kw0.x + x.x, 0.1f * kw0.x), 1e-3f * K_INF);
+  float om = fmaxf(fmaxf(kw0.y + x.y, 0.1f * kw0.y), 1e-3f * winf);
+  float4 wc = A.W[pidx(c, i, j)];
+  float rho = wc.x;
+  float nu = A.mu[cc] / rho;
+  float strain = sqrtf(fmaxf(strain2(A.grad4[cc], wc.z, A.cellg[cc].w), 0.f));
+  float d = A.dwall[cc];
+  float t1 = sqrtf(k) / (BETA_STAR * om * d), t2 = 500.f * nu / (d * d * om);
+  float b = fmaxf(2.f * t1, t2);
+  float f2 = tanhf(b * b);
+  float mut = fminf(rho * A1 * k / fmaxf(A1 * om, strain * f2), (float)(1e5 / c.re_c));
+  A.turb[cc] = make_float2(k, om);
+  A.mu_t[cc] = mut;
+}
+
+}  // namespace bk

@@ -1,0 +1,224 @@
+"""`GpuSolver` over the B200 backend: the host-side mirror of the reference's GPU solver interface
+(crates/bowshock-cfd/src/gpu/mod.rs:233-414), same method names, argument meaning and errors, calling the C ABI.
+
+    s = GpuSolver.new(ni, nj, x, r, Config(...))        # GpuSolver::new
+    s.set_block(...); s.set_scheme(...); s.set_viscous(...)
+    residuals = s.run(50)                                # GpuSolver::run
+    u = s.state_f64()                                    # GpuSolver::state_f64
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import BowshockError
+
+GAMMA = 1.4
+LIM_FIRST_ORDER, LIM_MINMOD, LIM_VAN_ALBADA, LIM_VENKATAKRISHNAN = 0, 1, 2, 3
+BC_FREESTREAM, BC_EXTRAPOLATE, BC_SLIPWALL, BC_CHARACTERISTIC, BC_PRESSURE_OUTFLOW = 0, 1, 2, 3, 4
+SCHEME_EXPLICIT, SCHEME_IMPLICIT = 0, 3
+DT_SUM, DT_MIN_DIRECTION = 0, 1
+TURB_LAMINAR, TURB_SST = 0, 1
+
+
+def freestream(mach: float):
+    """gas.rs:41-43: rho = 1, c = 1, p = 1/gamma, u = Mach."""
+    return (1.0, float(mach), 0.0, 1.0 / GAMMA)
+
+
+@dataclass
+class Config:  # solver.rs:40-48
+    cfl: float = 0.5
+    limiter: int = LIM_MINMOD
+    freestream: tuple = freestream(0.5)
+    bc: tuple = (BC_CHARACTERISTIC, BC_CHARACTERISTIC, BC_SLIPWALL, BC_CHARACTERISTIC)
+    first_order_iters: int = 0
+
+    def c(self):
+        return _ffi.Config(self.cfl, self.limiter, (C.c_double * 4)(*self.freestream), (C.c_int32 * 4)(*self.bc),
+                           int(self.first_order_iters))
+
+
+@dataclass
+class ImplicitParams:  # implicit.rs:59-84 (DEFAULT)
+    cfl0: float = 1.0
+    cfl_max: float = 30.0
+    growth: float = 1.02
+    dt_mode: int = DT_SUM
+    lines: bool = True
+    implicit_bc: bool = True
+    sub_iters: int = 2
+    roe: bool = True
+    eps_fix: float = 0.1
+
+    @staticmethod
+    def viscous():  # implicit.rs:83
+        return ImplicitParams(dt_mode=DT_MIN_DIRECTION, cfl_max=10.0, sub_iters=3)
+
+    @staticmethod
+    def rans():  # numerics.rs:245 (RANS_IMPLICIT)
+        return ImplicitParams(dt_mode=DT_SUM, cfl_max=50.0, sub_iters=3)
+
+
+EXPLICIT = "explicit"
+
+
+@dataclass
+class Viscous:  # solver.rs:164-176
+    re_c: float
+    sutherland: float
+    turbulence: int = TURB_LAMINAR
+    wall_i_start: int = 0
+    roughness: float = 0.0
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class GpuSolver:
+    """One case on the B200 backend (a case arena of one)."""
+
+    def __init__(self, handle, ni, nj):
+        self._h = handle
+        self.ni, self.nj = ni, nj
+        self._viscous = None
+
+    # -------------------------------------------------------------- construction
+    @classmethod
+    def new(cls, ni: int, nj: int, x, r, cfg: Config, device: int = 0) -> "GpuSolver":
+        lib = _ffi.load()
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
+        if x.size != (ni + 1) * (nj + 1) or r.size != x.size:
+            raise BowshockError(_ffi.INVALID, "node arrays must hold (ni+1)*(nj+1) entries")
+        h = C.c_void_p()
+        c = cfg.c()
+        rc = lib.bowshock_solver_create(ni, nj, _dp(x), _dp(r), C.byref(c), device, C.byref(h))
+        if rc:
+            raise BowshockError(rc, "bowshock_solver_create failed (invalid grid / config, or no usable CUDA device)")
+        return cls(h, ni, nj)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _ffi.load().bowshock_solver_destroy(h)
+            self._h = None
+
+    def _check(self, rc):
+        if rc:
+            msg = _ffi.load().bowshock_solver_last_error(self._h)
+            raise BowshockError(rc, msg.decode() if msg else "")
+
+    # -------------------------------------------------------------- configuration (gpu/mod.rs:279-362)
+    def set_config(self, cfg: Config):
+        c = cfg.c()
+        self._check(_ffi.load().bowshock_solver_set_config(self._h, C.byref(c)))
+
+    def set_low_mach(self, on: bool):
+        self._check(_ffi.load().bowshock_solver_set_low_mach(self._h, int(bool(on))))
+
+    def set_block(self, block):
+        """`block`: None or (i_end, j_end, j_sting)."""
+        if block is None:
+            self._check(_ffi.load().bowshock_solver_set_block(self._h, None))
+        else:
+            b = _ffi.Block(*[int(v) for v in block])
+            self._check(_ffi.load().bowshock_solver_set_block(self._h, C.byref(b)))
+
+    def set_nozzle(self, nozzle):
+        """`nozzle`: None or (j_end, state[4], turb[2])."""
+        if nozzle is None:
+            self._check(_ffi.load().bowshock_solver_set_nozzle(self._h, None))
+        else:
+            j_end, state, turb = nozzle
+            n = _ffi.Nozzle(int(j_end), (C.c_double * 4)(*state), (C.c_double * 2)(*turb))
+            self._check(_ffi.load().bowshock_solver_set_nozzle(self._h, C.byref(n)))
+
+    def set_scheme(self, scheme):
+        """`scheme`: EXPLICIT or an ImplicitParams."""
+        if scheme == EXPLICIT:
+            s = _ffi.Scheme(kind=SCHEME_EXPLICIT)
+        else:
+            p = scheme
+            s = _ffi.Scheme(SCHEME_IMPLICIT, p.cfl0, p.cfl_max, p.growth, p.dt_mode, int(p.lines), int(p.implicit_bc),
+                            int(p.sub_iters), int(p.roe), p.eps_fix)
+        self._check(_ffi.load().bowshock_solver_set_scheme(self._h, C.byref(s)))
+
+    def set_viscous(self, v: Viscous | None):
+        if v is None:
+            self._check(_ffi.load().bowshock_solver_set_viscous(self._h, None))
+        else:
+            c = _ffi.Viscous(v.re_c, v.sutherland, v.turbulence, int(v.wall_i_start), v.roughness)
+            self._check(_ffi.load().bowshock_solver_set_viscous(self._h, C.byref(c)))
+        self._viscous = v
+
+    # -------------------------------------------------------------- state (gpu/mod.rs:365-392)
+    def set_state(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(-1)
+        if u.size != 4 * self.ni * self.nj:
+            raise BowshockError(_ffi.INVALID, "state must hold ni*nj*4 values")
+        self._check(_ffi.load().bowshock_solver_set_state(self._h, _dp(u)))
+
+    def reset(self):
+        self._check(_ffi.load().bowshock_solver_reset(self._h))
+
+    def state_f64(self) -> np.ndarray:
+        u = np.zeros(4 * self.ni * self.nj)
+        self._check(_ffi.load().bowshock_solver_state(self._h, _dp(u)))
+        return u.reshape(-1, 4)
+
+    def turb_state(self):
+        t = np.zeros(2 * self.ni * self.nj)
+        m = np.zeros(self.ni * self.nj)
+        self._check(_ffi.load().bowshock_solver_turb_state(self._h, _dp(t), _dp(m)))
+        return t.reshape(-1, 2), m
+
+    def set_turb(self, turb, mu_t):
+        t = np.ascontiguousarray(turb, dtype=np.float64).reshape(-1)
+        m = np.ascontiguousarray(mu_t, dtype=np.float64).reshape(-1)
+        self._check(_ffi.load().bowshock_solver_set_turb(self._h, _dp(t), _dp(m)))
+
+    @property
+    def iter(self) -> int:
+        v = C.c_uint64()
+        self._check(_ffi.load().bowshock_solver_iter(self._h, C.byref(v)))
+        return v.value
+
+    def set_iter(self, it: int):
+        self._check(_ffi.load().bowshock_solver_set_iter(self._h, int(it)))
+
+    def restart_ramp(self):
+        self._check(_ffi.load().bowshock_solver_restart_ramp(self._h))
+
+    # -------------------------------------------------------------- iteration (gpu/mod.rs:396-413)
+    def run(self, n: int) -> np.ndarray:
+        out = np.zeros(n)
+        self._check(_ffi.load().bowshock_solver_run(self._h, int(n), _dp(out)))
+        return out
+
+    def eval_residual(self, compute_dt: bool = True):
+        """`Solver::eval_residual` + `density_residual` of the current state: (res (n,4), dt (n), density residual)."""
+        res = np.zeros(4 * self.ni * self.nj)
+        dt = np.zeros(self.ni * self.nj)
+        d = C.c_double()
+        self._check(_ffi.load().bowshock_solver_eval_residual(self._h, int(compute_dt), _dp(res), _dp(dt), C.byref(d)))
+        return res.reshape(-1, 4), dt, d.value
+
+    def turb_residual(self) -> float:
+        d = C.c_double()
+        self._check(_ffi.load().bowshock_solver_turb_residual(self._h, C.byref(d)))
+        return d.value
+
+    def read_boundary_into(self, u: np.ndarray):
+        buf = np.ascontiguousarray(u, dtype=np.float64).reshape(-1)
+        self._check(_ffi.load().bowshock_solver_read_boundary(self._h, _dp(buf)))
+        u.reshape(-1)[:] = buf
+
+    def base_cells(self, j_rows: int) -> np.ndarray:
+        out = np.zeros(8 * j_rows)
+        self._check(_ffi.load().bowshock_solver_base_cells(self._h, _dp(out)))
+        return out.reshape(j_rows, 2, 4)

@@ -1,0 +1,282 @@
+/* bowshock_b200 — C ABI of the B200 finite-volume backend.
+ *
+ * Drop-in boundary: these entry points are the reference's GPU solver interface `GpuSolver`
+ * (crates/bowshock-cfd/src/gpu/mod.rs:233-414), which the engine's `GpuRunner` (crates/bowshock-core/src/engine/gpu.rs:28-169)
+ * and the facade's `GpuBackend` runner (crates/bowshock-core/src/analysis.rs:1186-1253) drive, restated as plain C so a
+ * Rust `B200Backend` can bind them with `extern "C"`. Each declaration names the reference method it replaces.
+ * Plus the batched case arena (many uneven cases per launch), which has no counterpart in the reference.
+ *
+ * Conventions
+ *  - Every call returns a status (BOWSHOCK_OK = 0) and never aborts the process; the message of the last failure of a
+ *    handle is returned by bowshock_solver_last_error / bowshock_arena_last_error (reference: GpuError, gpu/mod.rs:29-56).
+ *  - Arrays are row-major with i fastest: cell (i, j) at j*ni + i, node (i, j) at j*(ni+1) + i (reference grid.rs:1-4).
+ *    Conserved state u = (rho, rho u, rho v, E) per cell, 4 doubles; turbulence (k, omega) per cell, 2 doubles.
+ *  - Units are the reference's: rho_inf = c_inf = 1, p_inf = 1/gamma, lengths in nose diameters (gas.rs:41-43).
+ *  - The handle owns all device memory; the caller owns host arrays, which are copied in and out; no pointer is kept
+ *    past a call. Handles are not thread-safe; distinct handles may be used from distinct threads.
+ *  - There is no CPU fallback: without a usable CUDA device, creation fails with BOWSHOCK_CUDA_ERROR.
+ */
+#ifndef BOWSHOCK_B200_H
+#define BOWSHOCK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (reference error convention: gpu/mod.rs:29-56, bowshock-core error.rs:7-45) */
+#define BOWSHOCK_OK 0
+#define BOWSHOCK_UNSUPPORTED 1
+#define BOWSHOCK_INVALID 2
+#define BOWSHOCK_CUDA_ERROR 3
+#define BOWSHOCK_NONFINITE 4
+#define BOWSHOCK_TIMEOUT 5
+#define BOWSHOCK_CANCELLED 6
+
+/* limiter (flux.rs:5-13) */
+#define BOWSHOCK_LIM_FIRST_ORDER 0
+#define BOWSHOCK_LIM_MINMOD 1
+#define BOWSHOCK_LIM_VAN_ALBADA 2
+#define BOWSHOCK_LIM_VENKATAKRISHNAN 3
+/* boundary conditions [imin, imax, jmin, jmax] (solver.rs:21-37) */
+#define BOWSHOCK_BC_FREESTREAM 0
+#define BOWSHOCK_BC_EXTRAPOLATE 1
+#define BOWSHOCK_BC_SLIPWALL 2
+#define BOWSHOCK_BC_CHARACTERISTIC 3
+#define BOWSHOCK_BC_PRESSURE_OUTFLOW 4
+/* scheme kinds (solver.rs:143-153): the GPU implements Explicit and Implicit, like the reference's GPU solver */
+#define BOWSHOCK_SCHEME_EXPLICIT 0
+#define BOWSHOCK_SCHEME_IMPLICIT 3
+#define BOWSHOCK_DT_SUM 0
+#define BOWSHOCK_DT_MIN_DIRECTION 1
+#define BOWSHOCK_TURB_LAMINAR 0
+#define BOWSHOCK_TURB_SST 1
+
+/* solver.rs:40-48 `Config` */
+typedef struct {
+  double cfl;
+  int32_t limiter;
+  double freestream[4]; /* primitive (rho, u, v, p) */
+  int32_t bc[4];
+  uint64_t first_order_iters;
+} bowshock_config;
+
+/* implicit.rs:59-84 `ImplicitParams` (kind = BOWSHOCK_SCHEME_IMPLICIT) or the explicit SSP-RK3 scheme */
+typedef struct {
+  int32_t kind;
+  double cfl0, cfl_max, growth;
+  int32_t dt_mode, lines, implicit_bc;
+  uint64_t sub_iters;
+  int32_t roe;
+  double eps_fix;
+} bowshock_scheme;
+
+/* solver.rs:59-102 `Block` */
+typedef struct {
+  uint64_t i_end, j_end, j_sting;
+} bowshock_block;
+
+/* solver.rs:164-176 `Viscous` (smooth walls: roughness must be 0 on this backend) */
+typedef struct {
+  double re_c, sutherland;
+  int32_t turbulence;
+  uint64_t wall_i_start;
+  double roughness;
+} bowshock_viscous;
+
+/* solver.rs:186-193 `Nozzle` */
+typedef struct {
+  uint64_t j_end;
+  double state[4];
+  double turb[2];
+} bowshock_nozzle;
+
+typedef struct bowshock_solver bowshock_solver;
+
+/* GpuSolver::new (gpu/mod.rs:243-249): grid from node coordinates (ni+1)*(nj+1), state at the free stream, iteration 0.
+ * `device` is the CUDA device ordinal. Metrics are computed in FP64 on the host (grid.rs:65-119) and stored as FP32. */
+int bowshock_solver_create(uint64_t ni, uint64_t nj, const double* x, const double* r, const bowshock_config* cfg, int device,
+                           bowshock_solver** out);
+/* drop (gpu/mod.rs, Drop of LazySolver) */
+void bowshock_solver_destroy(bowshock_solver* s);
+/* GpuError text of the last failed call on this handle */
+const char* bowshock_solver_last_error(const bowshock_solver* s);
+/* GpuSolver::ni / nj fields (gpu/mod.rs:237-238) */
+int bowshock_solver_dims(const bowshock_solver* s, uint64_t* ni, uint64_t* nj);
+/* GpuSolver::set_config (gpu/mod.rs:279-285): a boundary-condition change on a viscous run is refused (UNSUPPORTED) */
+int bowshock_solver_set_config(bowshock_solver* s, const bowshock_config* cfg);
+/* GpuSolver::set_low_mach (gpu/mod.rs:297-299) */
+int bowshock_solver_set_low_mach(bowshock_solver* s, int on);
+/* GpuSolver::set_block (gpu/mod.rs:302-308): NULL = no block; refused after set_viscous */
+int bowshock_solver_set_block(bowshock_solver* s, const bowshock_block* block);
+/* GpuSolver::set_nozzle (gpu/mod.rs:316-322): NULL = none; must follow set_block and precede set_viscous */
+int bowshock_solver_set_nozzle(bowshock_solver* s, const bowshock_nozzle* nozzle);
+/* GpuSolver::set_scheme (gpu/mod.rs:331-337): explicit or implicit; the CFL ramp restarts */
+int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* scheme);
+/* GpuSolver::set_viscous (gpu/mod.rs:351-357): NULL = Euler; the turbulence state restarts at the free stream, the wall
+ * distance is computed on the device; roughness > 0 is UNSUPPORTED */
+int bowshock_solver_set_viscous(bowshock_solver* s, const bowshock_viscous* v);
+/* GpuSolver::set_state (gpu/mod.rs:378-381): overwrite the conserved state, restart the iteration counter and the ramp */
+int bowshock_solver_set_state(bowshock_solver* s, const double* u);
+/* GpuSolver::reset (gpu/mod.rs:384-387) */
+int bowshock_solver_reset(bowshock_solver* s);
+/* GpuSolver::state_f64 (gpu/mod.rs:390-392) */
+int bowshock_solver_state(const bowshock_solver* s, double* u);
+/* GpuSolver::turb_state (gpu/mod.rs:365-370): (k, omega) per cell and mu_t per cell; UNSUPPORTED without SST */
+int bowshock_solver_turb_state(const bowshock_solver* s, double* turb, double* mu_t);
+/* LazySolver::from_host's copy of the host turbulence state (gpu/mod.rs:251-263): set (k, omega) and mu_t */
+int bowshock_solver_set_turb(bowshock_solver* s, const double* turb, const double* mu_t);
+/* GpuSolver::iter / set_iter / restart_ramp (gpu/mod.rs:288-294, 344-347) */
+int bowshock_solver_iter(const bowshock_solver* s, uint64_t* iter);
+int bowshock_solver_set_iter(bowshock_solver* s, uint64_t iter);
+int bowshock_solver_restart_ramp(bowshock_solver* s);
+/* GpuSolver::run (gpu/mod.rs:396-398): n iterations; residual[k] = density residual (L2 of d rho/dt over sqrt(n_active))
+ * at the start of iteration k, accumulated in FP64 on the device. residual may be NULL. */
+int bowshock_solver_run(bowshock_solver* s, uint64_t n, double* residual);
+/* Solver::eval_residual + density_residual (solver.rs:474-654) of the current state without advancing it: the per-cell
+ * residual (ni*nj*4) and local time step (ni*nj; explicit definition when compute_dt = 1), either output may be NULL */
+int bowshock_solver_eval_residual(bowshock_solver* s, int compute_dt, double* res, double* dt, double* density_residual);
+/* GpuSolver::turb_residual (gpu/mod.rs:373-375) */
+int bowshock_solver_turb_residual(const bowshock_solver* s, double* r);
+/* GpuSolver::read_boundary_into (gpu/mod.rs:401-404): the wall / base stencil cells (rows col_start(i), col_start(i)+1
+ * and the two columns behind the base) of the conserved state into u (ni*nj*4); other cells are left untouched */
+int bowshock_solver_read_boundary(const bowshock_solver* s, double* u);
+/* GpuSolver::base_cells (gpu/mod.rs:408-413): [(i_end, j), (i_end+1, j)] conserved states for j in j_sting..j_end */
+int bowshock_solver_base_cells(const bowshock_solver* s, double* out);
+
+/* ---------------------------------------------------------------------------------------------- bodies and forces */
+#define BOWSHOCK_NOSE_TANGENT_OGIVE 0
+#define BOWSHOCK_NOSE_CONE 1
+#define BOWSHOCK_NOSE_POWER 2
+#define BOWSHOCK_NOSE_PARABOLIC 3
+#define BOWSHOCK_NOSE_HAACK 4
+#define BOWSHOCK_MAX_SEGMENTS 8
+
+/* body_grid.rs:31-43, 233-251 `Nose`, `Segment`, `BaseBody` (lengths in nose diameters; param = power n, parabolic K or
+ * Haack C) */
+typedef struct {
+  int32_t nose_kind;
+  double fineness, half_angle, param;
+  int32_t nseg;
+  double seg_length[BOWSHOCK_MAX_SEGMENTS], seg_slope[BOWSHOCK_MAX_SEGMENTS];
+  double sting_radius;
+} bowshock_body;
+
+/* Force integration of the current state (engine/run.rs:188-313), computed in FP64 on the device. */
+typedef struct {
+  double cd_nose, cd_nose_cell, cd_base, cp_base, cp_base_cell, cd_friction, y_plus_max;
+  double cd_aft[BOWSHOCK_MAX_SEGMENTS];
+  double cd_total; /* nose + aft segments + friction + base */
+} bowshock_forces;
+
+/* engine/run.rs:188-313 (wall_distribution, aft_drag, base_state, friction) on the device, in FP64 */
+int bowshock_solver_forces(bowshock_solver* s, const bowshock_body* body, bowshock_forces* out);
+
+/* ---------------------------------------------------------------------------------------------- run to a stop rule */
+#define BOWSHOCK_WAKE_STING 0
+#define BOWSHOCK_WAKE_BASE 1
+#define BOWSHOCK_STOP_MAX_ITERATIONS 0
+#define BOWSHOCK_STOP_RESIDUAL_DROP 1
+#define BOWSHOCK_STOP_CD_STATIONARY 2
+#define BOWSHOCK_STOP_BASE_PRESSURE_STATIONARY 3
+#define BOWSHOCK_STOP_MEAN_STATIONARY 4
+#define BOWSHOCK_STOP_NON_FINITE 5
+#define BOWSHOCK_STOP_CANCELLED 6
+
+/* The stop-rule part of numerics.rs:261-287 `Numerics` and the arguments of engine/run.rs:44 `run_on`. */
+typedef struct {
+  uint64_t max_iter, min_iter;
+  double drop_orders;
+  uint64_t monitor_window;
+  int32_t has_monitor_tol;
+  double monitor_tol;
+  int32_t has_mean_window;
+  uint64_t mean_window;
+  int32_t has_drag_rel_tol;
+  double drag_rel_tol;
+  int32_t wake;    /* BOWSHOCK_WAKE_* */
+  int32_t warm;    /* keep the state; no first-order start-up (run.rs:54-63) */
+  double r_ref;    /* residual reference of the drop rule; < 0: the run's own peak */
+} bowshock_run_params;
+
+/* engine/result.rs `PointResult` (the scalar fields) */
+typedef struct {
+  uint64_t iters;
+  double residual_peak, drop_orders;
+  int32_t stop_reason;
+  bowshock_forces forces;
+  double last_monitor;
+} bowshock_point_result;
+
+/* Progress callback, called between chunks of 50 iterations (progress.rs:1-8); return non-zero to cancel. */
+typedef int (*bowshock_progress_fn)(void* user, uint64_t case_index, uint64_t iteration, double residual, double monitor);
+
+/* engine/gpu.rs:86-169 `GpuRunner::run_on`: iterate in chunks of 50 to the stop rules of engine/run.rs:105-170 (stop
+ * iteration CPU-equivalent inside a chunk), the monitor sampled every 50 iterations by the FP64 force pass, then the
+ * forces of the final state. residual (cap entries) may be NULL. */
+int bowshock_solver_run_to_stop(bowshock_solver* s, const bowshock_body* body, const bowshock_run_params* p, bowshock_point_result* out,
+                                double* residual, uint64_t cap, bowshock_progress_fn progress, void* user);
+
+/* ---------------------------------------------------------------------------------------------- mesher */
+/* body_grid.rs:330-355 `BaseGridParams` (power-off) and body_grid.rs:112-131 `LargeGridParams` */
+typedef struct {
+  double x_up, x_down, r_far;
+  uint64_t n_up, n_nose, n_seg[BOWSHOCK_MAX_SEGMENTS], n_wake, n_sting, n_gap, nj_out;
+  double dx_tip, dr_wall;
+  int32_t gap_one_sided;
+} bowshock_base_grid;
+typedef struct {
+  double x_up, x_down, r_far;
+  uint64_t n_up, n_nose, n_seg[BOWSHOCK_MAX_SEGMENTS], n_ext, nj;
+  double dx_tip, dr_wall;
+} bowshock_sting_grid;
+
+/* body_grid.rs:360-452 `base_domain_grid`: node coordinates and the solid block. Call with x = r = NULL to get ni, nj. */
+int bowshock_base_domain_grid(const bowshock_body* body, const bowshock_base_grid* p, uint64_t* ni, uint64_t* nj, double* x, double* r,
+                              bowshock_block* block);
+/* body_grid.rs:213-231 `large_domain_grid` (sting wake). Call with x = r = NULL to get ni, nj. */
+int bowshock_large_domain_grid(const bowshock_body* body, const bowshock_sting_grid* p, uint64_t* ni, uint64_t* nj, double* x, double* r);
+
+/* ---------------------------------------------------------------------------------------------- batched case arena
+ * No counterpart in the reference (it runs Mach points one at a time, analysis.rs:727-797): many cases with uneven grids
+ * packed into one structure-of-arrays arena, every kernel launched once per iteration for all of them, per-case
+ * convergence masks. The per-case numerics are those of the single-case solver. */
+typedef struct {
+  uint64_t ni, nj;
+  const double *x, *r;
+  bowshock_config cfg;
+  int32_t low_mach;
+  int32_t has_block;
+  bowshock_block block;
+  bowshock_scheme scheme; /* implicit for every case of an arena */
+  int32_t has_viscous;
+  bowshock_viscous viscous;
+  bowshock_body body;
+  bowshock_run_params run;
+} bowshock_case_desc;
+
+typedef struct bowshock_arena bowshock_arena;
+int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int device, bowshock_arena** out);
+void bowshock_arena_destroy(bowshock_arena* a);
+const char* bowshock_arena_last_error(const bowshock_arena* a);
+/* cells of all cases */
+int bowshock_arena_cells(const bowshock_arena* a, uint64_t* ncells);
+/* n iterations of every active case; residual (n x ncases, iteration-major) may be NULL */
+int bowshock_arena_run(bowshock_arena* a, uint64_t n, double* residual);
+/* cold-start every case and iterate each to its stop rule, masking converged cases out; results per case */
+int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bowshock_progress_fn progress, void* user);
+/* FP64 forces of every case's current state (ncases entries) */
+int bowshock_arena_forces(bowshock_arena* a, bowshock_forces* out);
+int bowshock_arena_state(const bowshock_arena* a, uint64_t k, double* u);
+int bowshock_arena_set_state(bowshock_arena* a, uint64_t k, const double* u);
+/* per-case activity mask (1 = iterate), ncases entries */
+int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active);
+/* mean device time of one arena iteration over the last bowshock_arena_run, in milliseconds (CUDA events) */
+int bowshock_arena_last_ms_per_iter(const bowshock_arena* a, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BOWSHOCK_B200_H */

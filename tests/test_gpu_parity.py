@@ -1,0 +1,104 @@
+"""B200 backend against the oracle, through the C ABI, with the reference's GPU-vs-CPU protocol and tolerances
+(crates/bowshock-gpu-cases/tests/{explicit,implicit,viscous}.rs): the same start state, N iterations, state and residual
+history compared. The FP32 tolerances are the reference's own for its f32 GPU path: explicit state 1e-5 / residual 1e-4
+(explicit.rs:10-12), implicit state 1e-3 (implicit.rs:6-8, viscous.rs body check)."""
+import numpy as np
+import pytest
+
+import oracle_ffi as o
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _per_cell_residual_check(spec, tol):
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    cpu.eval_residual(True)
+    rc, dc = cpu.res, cpu.dt
+    rg, dg, dens = gpu.eval_residual(True)
+    # per component, relative to the component's largest magnitude over the grid (FP32 flux differences)
+    for k in range(4):
+        scale = np.max(np.abs(rc[:, k])) + 1e-30
+        err = np.max(np.abs(rg[:, k] - rc[:, k])) / scale
+        assert err < tol, f"{spec.label}: residual component {k} max rel err {err:.3e}"
+    fluid = dc > 0
+    assert np.max(np.abs(dg[fluid] - dc[fluid]) / dc[fluid]) < 1e-5
+    assert abs(dens - cpu.density_residual()) / cpu.density_residual() < 1e-4
+
+
+def test_residual_per_cell_far_field_box():
+    spec = cases.far_field_box(0.5)
+    spec.u0 = cases.perturbed_state(spec)
+    spec.first_order_iters = 0
+    _per_cell_residual_check(spec, 1e-5)
+
+
+def test_residual_per_cell_base_block():
+    spec = cases.subsonic_base(0.5)
+    rng = np.random.default_rng(7)
+    u = np.tile(o.prim_to_cons(np.array(spec.fs)), (spec.ni * spec.nj, 1))
+    w = o.cons_to_prim(u)
+    w[:, 0] *= 1 + 0.05 * rng.standard_normal(len(w))
+    w[:, 1] += 0.05 * rng.standard_normal(len(w))
+    w[:, 2] += 0.05 * rng.standard_normal(len(w))
+    w[:, 3] *= 1 + 0.05 * rng.standard_normal(len(w))
+    spec.u0 = o.prim_to_cons(w)
+    spec.first_order_iters = 0
+    _per_cell_residual_check(spec, 2e-5)
+
+
+@pytest.mark.parametrize("mach,outflow", [(0.5, o.BC_CHARACTERISTIC), (1.3, o.BC_CHARACTERISTIC), (0.5, o.BC_PRESSURE_OUTFLOW)])
+def test_explicit_state_matches_oracle(mach, outflow):  # explicit.rs protocol, f32 tolerances
+    spec = cases.far_field_box(mach, outflow)
+    spec.u0 = cases.perturbed_state(spec)
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)
+    assert cases.state_diff(gpu.state_f64(), cpu.u) < 1e-5
+    assert cases.residual_diff(rg, rc) < 1e-4
+
+
+@pytest.mark.parametrize("maker", [cases.subsonic_sting, cases.subsonic_base])
+def test_implicit_state_matches_oracle(maker):  # implicit.rs:11-35 protocol
+    spec = maker(0.5)
+    spec.first_order_iters = 5
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)
+    d = cases.state_diff(gpu.state_f64(), cpu.u)
+    assert d < 1e-3, f"{spec.label}: state diff {d:.3e}"
+    assert np.all(np.isfinite(rg))
+    assert cases.residual_diff(rg[:5], rc[:5]) < 1e-3
+
+
+def test_implicit_box_with_perturbation_matches_oracle():
+    spec = cases.far_field_box(0.5)
+    spec.u0 = cases.perturbed_state(spec)
+    spec.scheme = dict(cfl0=1.0, cfl_max=30.0, growth=1.02, dt_mode=0, lines=True, implicit_bc=True, sub_iters=2, roe=True, eps_fix=0.1)
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)
+    assert cases.state_diff(gpu.state_f64(), cpu.u) < 1e-3
+    assert cases.residual_diff(rg, rc) < 1e-2
+
+
+def test_g3_body_sst_matches_oracle():  # viscous.rs body check: 30 implicit iterations, first 5 first order
+    spec = cases.g3_body()
+    spec.first_order_iters = 5
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)
+    d = cases.state_diff(gpu.state_f64(), cpu.u)
+    assert d < 1e-3, f"G3 state diff {d:.3e}"
+    t_g, m_g = gpu.turb_state()
+    t_c = cpu.turb
+    fluid = t_c[:, 0] > 0
+    for e, name in ((0, "k"), (1, "omega")):
+        err = np.max(np.abs(t_g[fluid, e] - t_c[fluid, e]) / np.abs(t_c[fluid, e]))
+        assert err < 1e-2, f"G3 {name} max rel diff {err:.3e}"
+    assert np.max(np.abs(m_g[fluid] - cpu.mu_t[fluid]) / np.abs(cpu.mu_t[fluid])) < 1e-2
