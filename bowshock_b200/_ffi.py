@@ -29,7 +29,8 @@ class Config(C.Structure):  # bowshock_config
 class Scheme(C.Structure):  # bowshock_scheme
     _fields_ = [("kind", C.c_int32), ("cfl0", C.c_double), ("cfl_max", C.c_double), ("growth", C.c_double),
                 ("dt_mode", C.c_int32), ("lines", C.c_int32), ("implicit_bc", C.c_int32), ("sub_iters", C.c_uint64),
-                ("roe", C.c_int32), ("eps_fix", C.c_double)]
+                ("roe", C.c_int32), ("eps_fix", C.c_double), ("mg_levels", C.c_uint64), ("mg_pre", C.c_uint64),
+                ("mg_post", C.c_uint64), ("mg_gamma", C.c_uint64), ("mg_coarsest", C.c_uint64)]
 
 
 class Block(C.Structure):  # bowshock_block
@@ -43,6 +44,53 @@ class Viscous(C.Structure):  # bowshock_viscous
 
 class Nozzle(C.Structure):  # bowshock_nozzle
     _fields_ = [("j_end", C.c_uint64), ("state", C.c_double * 4), ("turb", C.c_double * 2)]
+
+
+class BowshockBody(C.Structure):  # bowshock_body
+    _fields_ = [("nose_kind", C.c_int32), ("fineness", C.c_double), ("half_angle", C.c_double), ("param", C.c_double),
+                ("nseg", C.c_int32), ("seg_length", C.c_double * 8), ("seg_slope", C.c_double * 8), ("sting_radius", C.c_double)]
+
+
+class Forces(C.Structure):  # bowshock_forces
+    _fields_ = [("cd_nose", C.c_double), ("cd_nose_cell", C.c_double), ("cd_base", C.c_double), ("cp_base", C.c_double),
+                ("cp_base_cell", C.c_double), ("cd_friction", C.c_double), ("y_plus_max", C.c_double), ("cd_aft", C.c_double * 8),
+                ("cd_total", C.c_double)]
+
+
+class RunParams(C.Structure):  # bowshock_run_params
+    _fields_ = [("max_iter", C.c_uint64), ("min_iter", C.c_uint64), ("drop_orders", C.c_double), ("monitor_window", C.c_uint64),
+                ("has_monitor_tol", C.c_int32), ("monitor_tol", C.c_double), ("has_mean_window", C.c_int32),
+                ("mean_window", C.c_uint64), ("has_drag_rel_tol", C.c_int32), ("drag_rel_tol", C.c_double), ("wake", C.c_int32),
+                ("warm", C.c_int32), ("r_ref", C.c_double)]
+
+
+class PointResult(C.Structure):  # bowshock_point_result
+    _fields_ = [("iters", C.c_uint64), ("residual_peak", C.c_double), ("drop_orders", C.c_double), ("stop_reason", C.c_int32),
+                ("forces", Forces), ("last_monitor", C.c_double)]
+
+
+class BaseGridC(C.Structure):  # bowshock_base_grid
+    _fields_ = [("x_up", C.c_double), ("x_down", C.c_double), ("r_far", C.c_double), ("n_up", C.c_uint64), ("n_nose", C.c_uint64),
+                ("n_seg", C.c_uint64 * 8), ("n_wake", C.c_uint64), ("n_sting", C.c_uint64), ("n_gap", C.c_uint64),
+                ("nj_out", C.c_uint64), ("dx_tip", C.c_double), ("dr_wall", C.c_double), ("gap_one_sided", C.c_int32)]
+
+
+class StingGridC(C.Structure):  # bowshock_sting_grid
+    _fields_ = [("x_up", C.c_double), ("x_down", C.c_double), ("r_far", C.c_double), ("n_up", C.c_uint64), ("n_nose", C.c_uint64),
+                ("n_seg", C.c_uint64 * 8), ("n_ext", C.c_uint64), ("nj", C.c_uint64), ("dx_tip", C.c_double), ("dr_wall", C.c_double)]
+
+
+class CaseDesc(C.Structure):  # bowshock_case_desc
+    _fields_ = [("ni", C.c_uint64), ("nj", C.c_uint64), ("x", C.POINTER(C.c_double)), ("r", C.POINTER(C.c_double)), ("cfg", Config),
+                ("low_mach", C.c_int32), ("has_block", C.c_int32), ("block", Block), ("scheme", Scheme), ("has_viscous", C.c_int32),
+                ("viscous", Viscous), ("body", BowshockBody), ("run", RunParams)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_double, C.c_double)
+
+
+def dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
 # every symbol the header declares, with its ctypes signature
@@ -72,6 +120,24 @@ SIGNATURES = {
     "bowshock_solver_turb_residual": (_I, [_P, _dp]),
     "bowshock_solver_read_boundary": (_I, [_P, _dp]),
     "bowshock_solver_base_cells": (_I, [_P, _dp]),
+    "bowshock_solver_forces": (_I, [_P, C.POINTER(BowshockBody), C.POINTER(Forces)]),
+    "bowshock_solver_run_to_stop": (_I, [_P, C.POINTER(BowshockBody), C.POINTER(RunParams), C.POINTER(PointResult), _dp, _U,
+                                         PROGRESS_FN, _P]),
+    "bowshock_base_domain_grid": (_I, [C.POINTER(BowshockBody), C.POINTER(BaseGridC), C.POINTER(_U), C.POINTER(_U), _dp, _dp,
+                                       C.POINTER(Block)]),
+    "bowshock_large_domain_grid": (_I, [C.POINTER(BowshockBody), C.POINTER(StingGridC), C.POINTER(_U), C.POINTER(_U), _dp, _dp]),
+    "bowshock_arena_create": (_I, [_U, C.POINTER(CaseDesc), _I, C.POINTER(_P)]),
+    "bowshock_arena_destroy": (None, [_P]),
+    "bowshock_arena_last_error": (C.c_char_p, [_P]),
+    "bowshock_arena_cells": (_I, [_P, C.POINTER(_U)]),
+    "bowshock_arena_run": (_I, [_P, _U, _dp]),
+    "bowshock_arena_solve": (_I, [_P, C.POINTER(PointResult), PROGRESS_FN, _P]),
+    "bowshock_arena_forces": (_I, [_P, C.POINTER(Forces)]),
+    "bowshock_arena_state": (_I, [_P, _U, _dp]),
+    "bowshock_arena_set_state": (_I, [_P, _U, _dp]),
+    "bowshock_arena_set_active": (_I, [_P, C.POINTER(C.c_int32)]),
+    "bowshock_arena_last_ms_per_iter": (_I, [_P, _dp]),
+    "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
 }
 
 _lib = None

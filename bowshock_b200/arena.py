@@ -1,0 +1,94 @@
+"""Batched case arena: many cases with uneven grids in one set of launches, with per-case convergence masks
+(include/bowshock_b200.h, `bowshock_arena_*`). No counterpart in the reference, which runs Mach points one at a time
+(crates/bowshock-core/src/analysis.rs:727-797); each case's numerics are those of the single-case solver."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import BowshockError
+from .solver import point_dict, forces_dict
+
+
+class Arena:
+    def __init__(self, cases, device=0, grids=None):
+        """`cases`: list of case.Case; `grids`: optional precomputed (ni, nj, x, r, block) per case."""
+        lib = _ffi.load()
+        self.cases = list(cases)
+        self._descs = (_ffi.CaseDesc * len(self.cases))()
+        self._keep = []
+        for k, c in enumerate(self.cases):
+            d = c.case_desc(grids[k] if grids is not None else None)
+            self._keep.append((d._x, d._r))
+            self._descs[k] = d
+        h = C.c_void_p()
+        rc = lib.bowshock_arena_create(len(self.cases), self._descs, device, C.byref(h))
+        if rc:
+            raise BowshockError(rc, "bowshock_arena_create failed (invalid case, or no usable CUDA device)")
+        self._h = h
+        self.ncases = len(self.cases)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _ffi.load().bowshock_arena_destroy(h)
+            self._h = None
+
+    def _check(self, rc):
+        if rc:
+            m = _ffi.load().bowshock_arena_last_error(self._h)
+            raise BowshockError(rc, m.decode() if m else "")
+
+    @property
+    def cells(self) -> int:
+        n = C.c_uint64()
+        self._check(_ffi.load().bowshock_arena_cells(self._h, C.byref(n)))
+        return n.value
+
+    def run(self, n: int) -> np.ndarray:
+        """n iterations of every active case: the density residual history, shape (n, ncases)."""
+        out = np.zeros(n * self.ncases)
+        self._check(_ffi.load().bowshock_arena_run(self._h, int(n), _ffi.dptr(out)))
+        return out.reshape(n, self.ncases)
+
+    def ms_per_iter(self) -> float:
+        d = C.c_double()
+        self._check(_ffi.load().bowshock_arena_last_ms_per_iter(self._h, C.byref(d)))
+        return d.value
+
+    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage")
+
+    def profile(self, n: int):
+        """Per-kernel-group device time over n iterations launched one kernel at a time: {group: (ms, launches)}."""
+        ms = np.zeros(8)
+        cnt = (C.c_uint64 * 8)()
+        self._check(_ffi.load().bowshock_arena_profile(self._h, int(n), _ffi.dptr(ms), cnt))
+        return {g: (float(ms[k]), int(cnt[k])) for k, g in enumerate(self.PROFILE_GROUPS)}
+
+    def solve(self, progress=None):
+        """Cold-start every case and iterate each to its stop rule (converged cases are masked out)."""
+        res = (_ffi.PointResult * self.ncases)()
+        cb = _ffi.PROGRESS_FN(lambda u, k, it, r, m: 0 if progress(k, it, r, m) else 1) if progress else _ffi.PROGRESS_FN(0)
+        self._check(_ffi.load().bowshock_arena_solve(self._h, res, cb, None))
+        return [point_dict(res[k], len(self.cases[k].body.segments)) for k in range(self.ncases)]
+
+    def forces(self):
+        out = (_ffi.Forces * self.ncases)()
+        self._check(_ffi.load().bowshock_arena_forces(self._h, out))
+        return [forces_dict(out[k], len(self.cases[k].body.segments)) for k in range(self.ncases)]
+
+    def state(self, k: int) -> np.ndarray:
+        ni, nj = self._descs[k].ni, self._descs[k].nj
+        u = np.zeros(4 * ni * nj)
+        self._check(_ffi.load().bowshock_arena_state(self._h, k, _ffi.dptr(u)))
+        return u.reshape(-1, 4)
+
+    def set_state(self, k: int, u):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(-1)
+        self._check(_ffi.load().bowshock_arena_set_state(self._h, k, _ffi.dptr(u)))
+
+    def set_active(self, mask):
+        m = (C.c_int32 * self.ncases)(*[int(bool(v)) for v in mask])
+        self._check(_ffi.load().bowshock_arena_set_active(self._h, m))

@@ -9,8 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libbowshock_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "capi.cu"), os.path.join(HERE, "csrc", "arena_capi.cu")]
-HEADERS = ["arena.cuh", "device_math.cuh", "viscous.cuh", "turbulence.cuh", "host_arena.cuh", "fv_kernels.cu", "forces.cuh"]
+SOURCES = [os.path.join(HERE, "csrc", "capi.cu")]
+HEADERS = ["arena.cuh", "device_math.cuh", "viscous.cuh", "turbulence.cuh", "host_arena.cuh", "fv_kernels.cu", "forces.cuh", "mesher.cuh", "runner.cuh"]
 
 
 def nvcc():

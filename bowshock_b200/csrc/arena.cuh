@@ -14,7 +14,7 @@
 
 namespace bk {
 
-enum { SCHEME_EXPLICIT = 0, SCHEME_IMPLICIT = 3 };
+enum { SCHEME_EXPLICIT = 0, SCHEME_MULTIGRID = 2, SCHEME_IMPLICIT = 3 };
 enum { DT_SUM = 0, DT_MIN_DIRECTION = 1 };
 
 struct CaseDev {
@@ -36,6 +36,8 @@ struct CaseDev {
   int viscous, sst, wall_i_start;
   double re_c, sutherland, roughness;
   int n_active;
+  // FAS multigrid: level of this case (0 = fine) and the arena indices of its finer / coarser level (-1: none)
+  int level, fine_case, coarse_case;
 };
 
 struct Arena {
@@ -77,6 +79,9 @@ struct Arena {
   float2* blend;   // (F1, X)
   // FP64-derived stencil of every face: (|d|, e_x, e_r, 0) between the two side positions (viscous.rs:233-250)
   const float4 *ifs, *jfs;
+  // FAS multigrid: the restricted state at the start of a coarse cycle, and the user's mask the level masks derive from
+  float4* MG0;
+  int* enabled;
 };
 
 constexpr int TI = 32, TJ = 8;  // residual tile

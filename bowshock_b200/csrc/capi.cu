@@ -6,7 +6,9 @@
 #include "../../include/bowshock_b200.h"
 #include "fv_kernels.cu"
 #include "turbulence.cuh"
+#include "multigrid.cuh"
 #include "host_arena.cuh"
+#include "mesher.cuh"
 
 using namespace bk;
 
@@ -81,7 +83,11 @@ int bowshock_solver_create(uint64_t ni, uint64_t nj, const double* x, const doub
   return BOWSHOCK_OK;
 }
 
-void bowshock_solver_destroy(bowshock_solver* s) { delete s; }
+static void solver_forces_drop(bowshock_solver* s);
+void bowshock_solver_destroy(bowshock_solver* s) {
+  if (s) solver_forces_drop(s);
+  delete s;
+}
 
 const char* bowshock_solver_last_error(const bowshock_solver* s) { return s ? s->last_error.c_str() : "null handle"; }
 
@@ -150,12 +156,75 @@ int bowshock_solver_set_nozzle(bowshock_solver* s, const bowshock_nozzle* n) {
   return from_arena(s, s->ar.upload_desc());
 }
 
+// Rebuild the arena of a solver with its FAS hierarchy (multigrid.rs:29-64): the fine grid, then grids with every second
+// node line removed while both dimensions are even and the coarse one stays >= 8, and the block halves; coarse levels are
+// first order with the fine level's BCs, free stream and CFL. nlev = 1 removes the hierarchy. The state is kept.
+static int rebuild_levels(bowshock_solver* s, int nlev) {
+  ArenaHost& ar = s->ar;
+  HostCase fine = ar.cases[0];
+  std::vector<double> u((size_t)fine.ni * fine.nj * 4);
+  int rc = ar.get_state(0, u.data());
+  if (rc) return from_arena(s, rc);
+  std::vector<HostCase> lv{fine};
+  lv[0].level = 0;
+  lv[0].fine_case = lv[0].coarse_case = -1;
+  while ((int)lv.size() < nlev) {
+    const HostCase& f = lv.back();
+    if (f.ni % 2 || f.nj % 2 || f.ni / 2 < 8 || f.nj / 2 < 8) break;
+    if (f.has_block && (f.i_end % 2 || f.j_end % 2 || f.j_sting % 2)) break;
+    HostCase c = f;
+    c.ni = f.ni / 2;
+    c.nj = f.nj / 2;
+    c.x.clear();
+    c.r.clear();
+    for (int j = 0; j <= c.nj; ++j)
+      for (int i = 0; i <= c.ni; ++i) {
+        size_t k = (size_t)2 * j * (f.ni + 1) + 2 * i;
+        c.x.push_back(f.x[k]);
+        c.r.push_back(f.r[k]);
+      }
+    std::string e;
+    if (!compute_metrics(c, e)) return fail(s, BOWSHOCK_INVALID, e);
+    if (f.has_block) c.i_end = f.i_end / 2, c.j_end = f.j_end / 2, c.j_sting = f.j_sting / 2;
+    c.limiter = 0;
+    c.first_order_iters = 0;
+    c.level = (int)lv.size();
+    c.fine_case = (int)lv.size() - 1;
+    c.coarse_case = -1;
+    lv.back().coarse_case = (int)lv.size();
+    lv.push_back(std::move(c));
+  }
+  ar.cases = std::move(lv);
+  ar.mg_levels = (int)ar.cases.size();
+  if ((rc = ar.setup())) return from_arena(s, rc);
+  return from_arena(s, ar.set_state(0, u.data()));
+}
+
 int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
   if (!s || !sc) return BOWSHOCK_INVALID;
-  if (sc->kind != BOWSHOCK_SCHEME_EXPLICIT && sc->kind != BOWSHOCK_SCHEME_IMPLICIT)
-    return fail(s, BOWSHOCK_UNSUPPORTED, "only Scheme::Explicit and Scheme::Implicit are implemented on the GPU");
+  if (sc->kind != BOWSHOCK_SCHEME_EXPLICIT && sc->kind != BOWSHOCK_SCHEME_IMPLICIT && sc->kind != BOWSHOCK_SCHEME_MULTIGRID)
+    return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
   if (sc->kind == BOWSHOCK_SCHEME_IMPLICIT && (sc->sub_iters < 1 || sc->sub_iters > 16 || !(sc->cfl0 > 0) || !(sc->cfl_max > 0)))
     return fail(s, BOWSHOCK_INVALID, "implicit parameters out of range");
+  if (sc->kind == BOWSHOCK_SCHEME_MULTIGRID) {
+    // multigrid.rs:29-31: refused with viscous terms and with a nozzle
+    if (s->ar.cases[0].viscous) return fail(s, BOWSHOCK_UNSUPPORTED, "viscous terms need Scheme::Explicit or Scheme::Implicit");
+    if (s->ar.cases[0].has_nozzle) return fail(s, BOWSHOCK_UNSUPPORTED, "nozzle needs Scheme::Explicit or Scheme::Implicit");
+    if (sc->mg_levels < 1 || sc->mg_levels > 16 || sc->mg_coarsest > 1000 || sc->mg_pre > 100 || sc->mg_post > 100 || sc->mg_gamma > 4)
+      return fail(s, BOWSHOCK_INVALID, "multigrid parameters out of range");
+  }
+  int want_levels = sc->kind == BOWSHOCK_SCHEME_MULTIGRID ? (int)sc->mg_levels : 1;
+  if (want_levels != s->ar.mg_levels || (int)s->ar.cases.size() != want_levels) {
+    s->ar.cases[0].scheme = sc->kind;
+    int rc = rebuild_levels(s, want_levels);
+    if (rc) return rc;
+  }
+  ArenaHost& ar = s->ar;
+  ar.mg_pre = (int)sc->mg_pre;
+  ar.mg_post = (int)sc->mg_post;
+  ar.mg_gamma = (int)sc->mg_gamma;
+  ar.mg_coarsest = (int)sc->mg_coarsest;
+  for (auto& hc : ar.cases) hc.scheme = sc->kind;
   HostCase& h = s->ar.cases[0];
   h.scheme = sc->kind;
   h.cfl0 = sc->cfl0;
@@ -250,8 +319,12 @@ int bowshock_solver_restart_ramp(bowshock_solver* s) {
 
 int bowshock_solver_run(bowshock_solver* s, uint64_t n, double* residual) {
   if (!s) return BOWSHOCK_INVALID;
-  int rc = s->ar.run((long long)n, residual);
+  const size_t nc = s->ar.cases.size();  // > 1 with a multigrid hierarchy: report the fine level only
+  std::vector<double> all(residual && nc > 1 ? n * nc : 0);
+  int rc = s->ar.run((long long)n, nc > 1 ? (residual ? all.data() : nullptr) : residual);
   if (rc) return from_arena(s, rc);
+  if (residual && nc > 1)
+    for (uint64_t k = 0; k < n; ++k) residual[k] = all[k * nc];
   if (residual)
     for (uint64_t k = 0; k < n; ++k)
       if (!std::isfinite(residual[k])) return fail(s, BOWSHOCK_NONFINITE, "non-finite residual at iteration " + std::to_string(k));
@@ -333,3 +406,340 @@ int bowshock_solver_base_cells(const bowshock_solver* s, double* out) {
 }
 
 }  // extern "C"
+
+// ==================================================================================== forces, runner, mesher, arena
+#include "runner.cuh"
+
+struct bowshock_solver_ext {
+  ForcePass fp;
+  bool ready = false;
+};
+static std::vector<std::pair<bowshock_solver*, bowshock_solver_ext*>>& ext_table() {
+  static std::vector<std::pair<bowshock_solver*, bowshock_solver_ext*>> t;
+  return t;
+}
+
+static RunParams to_params(const bowshock_run_params* p) {
+  RunParams r;
+  r.max_iter = (long long)p->max_iter;
+  r.min_iter = (long long)p->min_iter;
+  r.drop_orders = p->drop_orders;
+  r.monitor_window = (long long)p->monitor_window;
+  r.has_monitor_tol = p->has_monitor_tol != 0;
+  r.monitor_tol = p->monitor_tol;
+  r.has_mean_window = p->has_mean_window != 0;
+  r.mean_window = (long long)p->mean_window;
+  r.has_drag_rel_tol = p->has_drag_rel_tol != 0;
+  r.drag_rel_tol = p->drag_rel_tol;
+  r.wake = p->wake;
+  r.warm = p->warm != 0;
+  r.r_ref = p->r_ref;
+  return r;
+}
+
+static bool valid_body(const bowshock_body* b, std::string& m) {
+  if (!b) return m = "null body", false;
+  if (b->nseg < 1 || b->nseg > BOWSHOCK_MAX_SEGMENTS) return m = "a body needs 1 to 8 aft segments", false;
+  if (b->nose_kind < 0 || b->nose_kind > 4) return m = "unknown nose shape", false;
+  return true;
+}
+
+static mesh::Body to_mesh_body(const bowshock_body* b) {
+  mesh::Body mb;
+  mb.nose = b->nose_kind;
+  mb.fineness = b->fineness;
+  mb.half_angle = b->half_angle;
+  mb.param = b->param;
+  for (int s = 0; s < b->nseg; ++s) mb.seg_len.push_back(b->seg_length[s]), mb.seg_slope.push_back(b->seg_slope[s]);
+  mb.sting_radius = b->sting_radius;
+  return mb;
+}
+
+// One ForcePass per solver handle, created on first use.
+static ForcePass* solver_forces(bowshock_solver* s, int& rc) {
+  rc = 0;
+  for (auto& e : ext_table())
+    if (e.first == s) return &e.second->fp;
+  auto* x = new bowshock_solver_ext();
+  rc = x->fp.setup(s->ar);
+  if (rc) {
+    delete x;
+    return nullptr;
+  }
+  ext_table().push_back({s, x});
+  return &x->fp;
+}
+static void solver_forces_drop(bowshock_solver* s) {
+  auto& t = ext_table();
+  for (size_t k = 0; k < t.size(); ++k)
+    if (t[k].first == s) {
+      delete t[k].second;
+      t.erase(t.begin() + k);
+      return;
+    }
+}
+
+static void fill_forces(const Forces& f, int nseg, bowshock_forces* o) {
+  o->cd_nose = f.f[F_CD_NOSE];
+  o->cd_nose_cell = f.f[F_CD_NOSE_CELL];
+  o->cd_base = f.f[F_CD_BASE];
+  o->cp_base = f.f[F_CP_BASE];
+  o->cp_base_cell = f.f[F_CP_BASE_CELL];
+  o->cd_friction = f.f[F_CD_FRICTION];
+  o->y_plus_max = f.f[F_YPLUS];
+  for (int k = 0; k < BOWSHOCK_MAX_SEGMENTS; ++k) o->cd_aft[k] = k < nseg ? f.f[F_CD_AFT0 + k] : 0.0;
+  o->cd_total = f.cd_total(nseg);
+}
+
+extern "C" {
+
+int bowshock_solver_forces(bowshock_solver* s, const bowshock_body* body, bowshock_forces* out) {
+  if (!s || !out) return BOWSHOCK_INVALID;
+  std::string m;
+  if (!valid_body(body, m)) return fail(s, BOWSHOCK_INVALID, m);
+  int rc = 0;
+  ForcePass* fp = solver_forces(s, rc);
+  if (!fp) return from_arena(s, rc);
+  if ((rc = fp->set_body(s->ar, 0, body))) return from_arena(s, rc);
+  std::vector<Forces> f;
+  if ((rc = fp->run(s->ar, f))) return from_arena(s, rc);
+  fill_forces(f[0], body->nseg, out);
+  return BOWSHOCK_OK;
+}
+
+int bowshock_solver_run_to_stop(bowshock_solver* s, const bowshock_body* body, const bowshock_run_params* p, bowshock_point_result* out,
+                                double* residual, uint64_t cap, bowshock_progress_fn progress, void* user) {
+  if (!s || !p || !out) return BOWSHOCK_INVALID;
+  std::string m;
+  if (!valid_body(body, m)) return fail(s, BOWSHOCK_INVALID, m);
+  if (s->ar.cases[0].scheme != BOWSHOCK_SCHEME_IMPLICIT && s->ar.cases[0].scheme != BOWSHOCK_SCHEME_EXPLICIT)
+    return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
+  int rc = 0;
+  ForcePass* fp = solver_forces(s, rc);
+  if (!fp) return from_arena(s, rc);
+  if ((rc = fp->set_body(s->ar, 0, body))) return from_arena(s, rc);
+  std::vector<CaseRun> runs(1);
+  runs[0].p = to_params(p);
+  runs[0].nseg = body->nseg;
+  runs[0].skip = runs[0].p.warm ? 0 : 20;
+  if ((rc = start_case(s->ar, 0, runs[0].p, s->ar.cases[0].first_order_iters))) return from_arena(s, rc);
+  std::function<bool(int, long long, double, double)> cb;
+  if (progress) cb = [&](int k, long long it, double r, double mon) { return progress(user, (uint64_t)k, (uint64_t)it, r, mon) == 0; };
+  if ((rc = solve_arena(s->ar, *fp, runs, cb))) return from_arena(s, rc);
+  std::vector<Forces> f;
+  if ((rc = fp->run(s->ar, f))) return from_arena(s, rc);
+  fill_point(runs[0], f[0], out);
+  if (residual)
+    for (size_t k = 0; k < runs[0].residual.size() && k < cap; ++k) residual[k] = runs[0].residual[k];
+  int one = 1;
+  s->ar.set_active(&one);
+  return runs[0].reason == 5 ? fail(s, BOWSHOCK_NONFINITE, "non-finite residual or monitor") : BOWSHOCK_OK;
+}
+
+int bowshock_base_domain_grid(const bowshock_body* body, const bowshock_base_grid* p, uint64_t* ni, uint64_t* nj, double* x, double* r,
+                              bowshock_block* block) {
+  std::string m;
+  if (!valid_body(body, m) || !p || !ni || !nj) return BOWSHOCK_INVALID;
+  mesh::Body mb = to_mesh_body(body);
+  mesh::BaseGrid g{p->x_up, p->x_down, p->r_far, p->n_up, p->n_nose, {}, p->n_wake, p->n_sting, p->n_gap, p->nj_out, p->dx_tip, p->dr_wall,
+                   p->gap_one_sided != 0};
+  for (int k = 0; k < body->nseg; ++k) g.n_seg.push_back(p->n_seg[k]);
+  size_t a, b, blk[3];
+  std::vector<double> X, R;
+  if (!mesh::base_domain_grid(mb, g, a, b, X, R, blk, m)) return BOWSHOCK_INVALID;
+  *ni = a;
+  *nj = b;
+  if (x) std::memcpy(x, X.data(), X.size() * sizeof(double));
+  if (r) std::memcpy(r, R.data(), R.size() * sizeof(double));
+  if (block) *block = bowshock_block{blk[0], blk[1], blk[2]};
+  return BOWSHOCK_OK;
+}
+
+int bowshock_large_domain_grid(const bowshock_body* body, const bowshock_sting_grid* p, uint64_t* ni, uint64_t* nj, double* x, double* r) {
+  std::string m;
+  if (!valid_body(body, m) || !p || !ni || !nj) return BOWSHOCK_INVALID;
+  mesh::Body mb = to_mesh_body(body);
+  mesh::StingGrid g{p->x_up, p->x_down, p->r_far, p->n_up, p->n_nose, {}, p->n_ext, p->nj, p->dx_tip, p->dr_wall};
+  for (int k = 0; k < body->nseg; ++k) g.n_seg.push_back(p->n_seg[k]);
+  size_t a, b;
+  std::vector<double> X, R;
+  if (!mesh::large_domain_grid(mb, g, a, b, X, R, m)) return BOWSHOCK_INVALID;
+  *ni = a;
+  *nj = b;
+  if (x) std::memcpy(x, X.data(), X.size() * sizeof(double));
+  if (r) std::memcpy(r, R.data(), R.size() * sizeof(double));
+  return BOWSHOCK_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batched arena
+struct bowshock_arena {
+  ArenaHost ar;
+  ForcePass fp;
+  std::vector<bowshock_case_desc> descs;
+  std::vector<int> nseg;
+  std::string last_error;
+};
+
+static int afail(bowshock_arena* a, int code, const std::string& m) {
+  if (a) a->last_error = m;
+  return code;
+}
+static int afrom(bowshock_arena* a, int rc) {
+  if (rc) a->last_error = a->ar.err;
+  return rc;
+}
+
+extern "C" {
+
+int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int device, bowshock_arena** out) {
+  if (!out || !cases || ncases == 0) return BOWSHOCK_INVALID;
+  *out = nullptr;
+  bowshock_arena* a = new (std::nothrow) bowshock_arena();
+  if (!a) return BOWSHOCK_INVALID;
+  std::string m;
+  for (uint64_t k = 0; k < ncases; ++k) {
+    const bowshock_case_desc& d = cases[k];
+    if (d.ni < 4 || d.nj < 2 || !d.x || !d.r || !valid_config(&d.cfg, m) || !valid_body(&d.body, m) ||
+        d.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT || d.scheme.sub_iters < 1 || d.scheme.sub_iters > 16 ||
+        (d.has_viscous && d.viscous.roughness != 0.0)) {
+      delete a;
+      return BOWSHOCK_INVALID;
+    }
+    HostCase h;
+    h.ni = (int)d.ni;
+    h.nj = (int)d.nj;
+    h.x.assign(d.x, d.x + (d.ni + 1) * (d.nj + 1));
+    h.r.assign(d.r, d.r + (d.ni + 1) * (d.nj + 1));
+    apply_config(h, &d.cfg);
+    h.low_mach = d.low_mach ? 1 : 0;
+    h.scheme = BOWSHOCK_SCHEME_IMPLICIT;
+    h.cfl0 = d.scheme.cfl0;
+    h.cfl_max = d.scheme.cfl_max;
+    h.growth = d.scheme.growth;
+    h.dt_mode = d.scheme.dt_mode;
+    h.lines = d.scheme.lines;
+    h.implicit_bc = d.scheme.implicit_bc;
+    h.sub_iters = (int)d.scheme.sub_iters;
+    h.roe = d.scheme.roe;
+    h.eps_fix = d.scheme.eps_fix;
+    if (d.has_block) {
+      const bowshock_block& b = d.block;
+      if (!(b.i_end >= 1 && b.i_end + 2 <= d.ni && b.j_end >= 2 && b.j_end + 2 <= d.nj && b.j_end > b.j_sting && (b.j_sting == 0 || b.j_sting >= 2))) {
+        delete a;
+        return BOWSHOCK_INVALID;
+      }
+      h.has_block = true;
+      h.i_end = (long long)b.i_end;
+      h.j_end = (long long)b.j_end;
+      h.j_sting = (long long)b.j_sting;
+    }
+    if (d.has_viscous) {
+      h.viscous = true;
+      h.turbulence = d.viscous.turbulence;
+      h.wall_i_start = (long long)d.viscous.wall_i_start;
+      h.re_c = d.viscous.re_c;
+      h.sutherland = d.viscous.sutherland;
+    }
+    if (!compute_metrics(h, m)) {
+      delete a;
+      return BOWSHOCK_INVALID;
+    }
+    a->ar.cases.push_back(std::move(h));
+    a->descs.push_back(d);
+    a->nseg.push_back(d.body.nseg);
+  }
+  a->ar.device = device;
+  int rc = a->ar.setup();
+  if (!rc) rc = a->fp.setup(a->ar);
+  for (uint64_t k = 0; !rc && k < ncases; ++k) rc = a->fp.set_body(a->ar, (int)k, &cases[k].body);
+  for (uint64_t k = 0; !rc && k < ncases; ++k)
+    if (a->ar.cases[k].viscous && a->ar.cases[k].turbulence == 1) rc = a->ar.turb_init((int)k);
+  if (rc) {
+    delete a;
+    return BOWSHOCK_CUDA_ERROR;
+  }
+  *out = a;
+  return BOWSHOCK_OK;
+}
+
+void bowshock_arena_destroy(bowshock_arena* a) { delete a; }
+const char* bowshock_arena_last_error(const bowshock_arena* a) { return a ? a->last_error.c_str() : "null handle"; }
+
+int bowshock_arena_cells(const bowshock_arena* a, uint64_t* ncells) {
+  if (!a || !ncells) return BOWSHOCK_INVALID;
+  *ncells = (uint64_t)a->ar.ncell;
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_run(bowshock_arena* a, uint64_t n, double* residual) {
+  if (!a) return BOWSHOCK_INVALID;
+  return afrom(a, a->ar.run((long long)n, residual));
+}
+
+int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bowshock_progress_fn progress, void* user) {
+  if (!a || !results) return BOWSHOCK_INVALID;
+  const int nc = (int)a->ar.cases.size();
+  std::vector<CaseRun> runs(nc);
+  int rc = 0;
+  for (int k = 0; k < nc; ++k) {
+    runs[k].p = to_params(&a->descs[k].run);
+    runs[k].nseg = a->nseg[k];
+    runs[k].skip = runs[k].p.warm ? 0 : 20;
+    if ((rc = start_case(a->ar, k, runs[k].p, a->ar.cases[k].first_order_iters))) return afrom(a, rc);
+  }
+  std::function<bool(int, long long, double, double)> cb;
+  if (progress) cb = [&](int k, long long it, double r, double mon) { return progress(user, (uint64_t)k, (uint64_t)it, r, mon) == 0; };
+  if ((rc = solve_arena(a->ar, a->fp, runs, cb))) return afrom(a, rc);
+  std::vector<Forces> f;
+  if ((rc = a->fp.run(a->ar, f))) return afrom(a, rc);
+  for (int k = 0; k < nc; ++k) fill_point(runs[k], f[k], &results[k]);
+  std::vector<int> all(nc, 1);
+  return afrom(a, a->ar.set_active(all.data()));
+}
+
+int bowshock_arena_forces(bowshock_arena* a, bowshock_forces* out) {
+  if (!a || !out) return BOWSHOCK_INVALID;
+  std::vector<Forces> f;
+  int rc = a->fp.run(a->ar, f);
+  if (rc) return afrom(a, rc);
+  for (size_t k = 0; k < f.size(); ++k) fill_forces(f[k], a->nseg[k], &out[k]);
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_state(const bowshock_arena* a, uint64_t k, double* u) {
+  if (!a || !u || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
+  bowshock_arena* m = const_cast<bowshock_arena*>(a);
+  return afrom(m, m->ar.get_state((int)k, u));
+}
+
+int bowshock_arena_set_state(bowshock_arena* a, uint64_t k, const double* u) {
+  if (!a || !u || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
+  return afrom(a, a->ar.set_state((int)k, u));
+}
+
+int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active) {
+  if (!a || !active) return BOWSHOCK_INVALID;
+  std::vector<int> v(active, active + a->ar.cases.size());
+  return afrom(a, a->ar.set_active(v.data()));
+}
+
+int bowshock_arena_last_ms_per_iter(const bowshock_arena* a, double* ms) {
+  if (!a || !ms) return BOWSHOCK_INVALID;
+  *ms = a->ar.last_ms_per_iter;
+  return BOWSHOCK_OK;
+}
+
+}  // extern "C"
+
+extern "C" int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches) {
+  if (!a || !ms || !launches) return BOWSHOCK_INVALID;
+  int rc = a->ar.profile((long long)n);
+  if (rc) return afrom(a, rc);
+  for (int g = 0; g < ArenaHost::G_N; ++g) {
+    ms[g] = a->ar.prof_ms[g];
+    launches[g] = (uint64_t)a->ar.prof_launches[g];
+  }
+  return BOWSHOCK_OK;
+}

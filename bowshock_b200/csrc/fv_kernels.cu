@@ -410,8 +410,10 @@ struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
   float a[16], b[16], c[16], d[4];
 };
 
-// epilogue: 0 = out[c] = x; 1 = DU[c] = x (+ damped update if `update`); 2 = DU[c] += x (+ update)
-__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out, int epilogue, int update) {
+// Factorisation pass `pass` (0 = the first solve, p >= 1 = the p-th defect correction) of each case with more than `pass`
+// passes (implicit.rs:619-639). i-sweeps write x to `out`; j-sweeps write du (pass 0) or add the correction to du, and
+// the last pass of a case applies the positivity-damped update.
+__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out, int pass) {
   __shared__ PcrSlot sp[LINE_WARPS][32];
   __shared__ float4 sl[LINE_WARPS][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -420,7 +422,9 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   if (gw >= nl) return;
   const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
   const CaseDev& c = A.cases[ci];
-  if (!A.active[ci]) return;
+  if (!A.active[ci] || pass >= c.sub_iters) return;
+  const int epilogue = dir_i ? 0 : (pass == 0 ? 1 : 2);
+  const bool update = !dir_i && pass == c.sub_iters - 1;
   const int L = gw - (dir_i ? c.iline_off : c.jline_off);
   const int n = dir_i ? c.ni : c.nj;
   const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
@@ -638,11 +642,11 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
 }
 
 // Defect of the unfactored operator (implicit.rs:622-630): rr = dt R - (A_i du + A_j du - du), per fluid cell.
-__global__ void k_defect(Arena A) {
+__global__ void k_defect(Arena A, int pass) {
   int t = blockIdx.x;
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
-  if (!A.active[ci]) return;
+  if (!A.active[ci] || pass >= c.sub_iters) return;
   int lt = t - c.tile_off;
   int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
   if (i >= c.ni || j >= c.nj) return;

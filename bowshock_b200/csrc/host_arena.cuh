@@ -9,6 +9,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "arena.cuh"
@@ -40,6 +41,7 @@ struct HostCase {
   int turbulence = 0;
   long long wall_i_start = 0;
   double re_c = 1e6, sutherland = 0.368, roughness = 0;
+  int level = 0, fine_case = -1, coarse_case = -1;  // FAS multigrid hierarchy inside the arena
   long long n_active() const {
     long long n = (long long)ni * nj;
     if (has_block) n -= i_end * j_end + ((long long)ni - i_end) * j_sting;
@@ -133,19 +135,26 @@ inline std::vector<double> wall_distance(const HostCase& h) {
         segs.insert(segs.end(), {a.first, a.second, b.first, b.second});
       }
   std::vector<double> d((size_t)ni * nj, std::numeric_limits<double>::infinity());
-  for (int j = 0; j < nj; ++j)
-    for (int i = 0; i < ni; ++i) {
-      if (h.solid(i, j)) continue;
-      size_t c = (size_t)j * ni + i;
-      double px = h.xc[c], pr = h.rc[c], best = d[c];
-      for (size_t s = 0; s + 3 < segs.size(); s += 4) {
-        double ex = segs[s + 2] - segs[s], er = segs[s + 3] - segs[s + 1];
-        double t = ((px - segs[s]) * ex + (pr - segs[s + 1]) * er) / (ex * ex + er * er);
-        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
-        best = std::fmin(best, std::hypot(px - (segs[s] + t * ex), pr - (segs[s + 1] + t * er)));
+  auto rows = [&](int j0, int j1) {
+    for (int j = j0; j < j1; ++j)
+      for (int i = 0; i < ni; ++i) {
+        if (h.solid(i, j)) continue;
+        size_t c = (size_t)j * ni + i;
+        double px = h.xc[c], pr = h.rc[c], best = d[c];
+        for (size_t s = 0; s + 3 < segs.size(); s += 4) {
+          double ex = segs[s + 2] - segs[s], er = segs[s + 3] - segs[s + 1];
+          double t = ((px - segs[s]) * ex + (pr - segs[s + 1]) * er) / (ex * ex + er * er);
+          t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+          best = std::fmin(best, std::hypot(px - (segs[s] + t * ex), pr - (segs[s + 1] + t * er)));
+        }
+        d[c] = best;
       }
-      d[c] = best;
-    }
+  };
+  // rows are independent: split them over the host threads
+  int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) th.emplace_back(rows, (int)((long long)nj * t / nt), (int)((long long)nj * (t + 1) / nt));
+  for (auto& x : th) x.join();
   return d;
 }
 
@@ -249,10 +258,15 @@ struct ArenaHost {
 
   void release() {
     if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    if (ev0) cudaEventDestroy(ev0), ev0 = nullptr;
+    if (ev1) cudaEventDestroy(ev1), ev1 = nullptr;
+    if (pe0) cudaEventDestroy(pe0), pe0 = nullptr;
+    if (pe1) cudaEventDestroy(pe1), pe1 = nullptr;
     void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0,
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
                     A.grad4, A.gradT, A.mu, A.mu_t, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
-                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs};
+                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled};
+    d_enabled = nullptr;
     for (void* p : ptrs)
       if (p) cudaFree(p);
     d_cases = nullptr;
@@ -300,6 +314,9 @@ struct ArenaHost {
     c.sutherland = h.sutherland;
     c.roughness = h.roughness;
     c.n_active = (int)h.n_active();
+    c.level = h.level;
+    c.fine_case = h.fine_case;
+    c.coarse_case = h.coarse_case;
     return c;
   }
 
@@ -375,6 +392,13 @@ struct ArenaHost {
     ALLOC(A.scratch, ncell * 36);
     ALLOC(A.rsum, (size_t)slots * nc);
     ALLOC(A.tsum, (size_t)slots * nc);
+    ALLOC(d_enabled, nc);
+    A.enabled = d_enabled;
+    if (mg_levels > 1) {
+      ALLOC(A.MG0, ncell);
+      ALLOC(A.FORCE, ncell);
+      BK_CUDA(cudaMemset(A.FORCE, 0, ncell * sizeof(float4)));
+    }
     float4 *fis, *fjs;
     ALLOC(fis, nif);
     ALLOC(fjs, njf);
@@ -433,6 +457,7 @@ struct ArenaHost {
     BK_CUDA(cudaMemcpy(d_iter, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(d_ramp, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(d_active, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_enabled, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
     ready = true;
     if ((rc = upload_desc())) return rc;
     for (int k = 0; k < nc; ++k)
@@ -587,17 +612,82 @@ struct ArenaHost {
   }
   int set_active(const int* act) {
     for (size_t k = 0; k < cases.size(); ++k) h_active[k] = act[k] ? 1 : 0;
-    BK_CUDA(cudaMemcpyAsync(d_active, h_active.data(), cases.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    BK_CUDA(cudaMemcpyAsync(d_enabled, h_active.data(), cases.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    if (mg_levels > 1)
+      k_level_mask<<<((int)cases.size() + 127) / 128, 128, 0, stream>>>(A, 0);
+    else
+      BK_CUDA(cudaMemcpyAsync(d_active, h_active.data(), cases.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
     BK_CUDA(cudaStreamSynchronize(stream));
     return 0;
   }
 
+  // ---------------------------------------------------------------- FAS multigrid (multigrid.rs:72-112)
+  int mg_levels = 1, mg_pre = 1, mg_post = 1, mg_gamma = 1, mg_coarsest = 4;
+  int* d_enabled = nullptr;
+  void set_level(int l) { k_level_mask<<<((int)cases.size() + 127) / 128, 128, 0, stream>>>(A, l); }
+  // one SSP-RK3 step of the active level (solver.rs:694-710); `slot` records the first stage's density residual
+  void rk3(int slot, int last) {
+    launch_mean_flow_prep();
+    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot); });
+    L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
+    launch_mean_flow_prep();
+    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
+    launch_mean_flow_prep();
+    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, last); });
+  }
+  void mg_level(int l, int slot) {  // multigrid.rs:87-112
+    const bool coarsest = l == mg_levels - 1;
+    const int n_pre = coarsest ? mg_coarsest : mg_pre;
+    set_level(l);
+    for (int k = 0; k < n_pre; ++k) rk3(l == 0 && k == 0 ? slot : -1, 0);
+    if (coarsest) return;
+    launch_mean_flow_prep();
+    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, (l == 0 && n_pre == 0) ? slot : -1); });
+    L(G_STAGE, [&] { k_restrict_state<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+    set_level(l + 1);
+    launch_mean_flow_prep();
+    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    L(G_STAGE, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+    for (int g = 0; g < std::max(mg_gamma, 1); ++g) mg_level(l + 1, -1);
+    L(G_STAGE, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l); });
+    set_level(l);
+    for (int k = 0; k < mg_post; ++k) rk3(-1, l == 0 && k == mg_post - 1 ? 1 : 0);
+    if (l == 0 && mg_post == 0) {  // the cycle still counts one iteration
+      launch_mean_flow_prep();
+      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 0, 1); });
+    }
+  }
+
   // ---------------------------------------------------------------- one iteration (stream-ordered launches)
+  // Kernel groups of the per-kernel profile (CUDA events around every launch when `profiling` is set).
+  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_N };
+  bool profiling = false;
+  double prof_ms[G_N] = {0};
+  long long prof_launches[G_N] = {0};
+  cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+  template <class F>
+  void L(int g, F&& launch) {
+    if (!profiling) {
+      launch();
+      return;
+    }
+    if (!pe0) cudaEventCreate(&pe0), cudaEventCreate(&pe1);
+    cudaEventRecord(pe0, stream);
+    launch();
+    cudaEventRecord(pe1, stream);
+    cudaEventSynchronize(pe1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, pe0, pe1);
+    prof_ms[g] += ms;
+    prof_launches[g] += 1;
+  }
   void launch_mean_flow_prep() {
-    k_prims<<<npblk, 256, 0, stream>>>(A);
+    L(G_PRIMS, [&] { k_prims<<<npblk, 256, 0, stream>>>(A); });
     if (any_viscous) {
-      k_visc_cell<<<ntiles, TI * TJ, 0, stream>>>(A);
-      k_visc_face<<<ntiles, TI * TJ, 0, stream>>>(A);
+      L(G_VISC, [&] { k_visc_cell<<<ntiles, TI * TJ, 0, stream>>>(A); });
+      L(G_VISC, [&] { k_visc_face<<<ntiles, TI * TJ, 0, stream>>>(A); });
     }
   }
   int scheme_of_arena() const { return desc.empty() ? 0 : desc[0].scheme; }
@@ -608,49 +698,108 @@ struct ArenaHost {
   }
   void launch_iteration(int slot) {
     const int lb_i = (nil + LINE_WARPS - 1) / LINE_WARPS, lb_j = (njl + LINE_WARPS - 1) / LINE_WARPS;
-    if (scheme_of_arena() == SCHEME_IMPLICIT) {
+    if (scheme_of_arena() == SCHEME_MULTIGRID) {
+      mg_level(0, slot);
+      set_level(0);
+    } else if (scheme_of_arena() == SCHEME_IMPLICIT) {
       launch_mean_flow_prep();
-      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot);
+      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot); });
       const int s = sub_iters_of_arena();
-      k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X, 0, 0);
-      k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, 1, s == 1 ? 1 : 0);
+      L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X, 0); });
+      L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, 0); });
       for (int p = 1; p < s; ++p) {
-        k_defect<<<ntiles, TI * TJ, 0, stream>>>(A);
-        k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, 0, A.X, 0, 0);
-        k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, 2, p == s - 1 ? 1 : 0);
+        L(G_DEFECT, [&] { k_defect<<<ntiles, TI * TJ, 0, stream>>>(A, p); });
+        L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, 0, A.X, p); });
+        L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, p); });
       }
       if (any_sst) {
         // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step
-        k_turb_grad<<<ntiles, TI * TJ, 0, stream>>>(A);
-        k_turb_blend<<<ntiles, TI * TJ, 0, stream>>>(A);
-        k_turb_cell<<<ntiles, TI * TJ, 0, stream>>>(A, slot);
-        k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1);
-        k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0);
-        k_turb_update<<<ntiles, TI * TJ, 0, stream>>>(A);
+        L(G_TURB, [&] { k_turb_grad<<<ntiles, TI * TJ, 0, stream>>>(A); });
+        L(G_TURB, [&] { k_turb_blend<<<ntiles, TI * TJ, 0, stream>>>(A); });
+        L(G_TURB, [&] { k_turb_cell<<<ntiles, TI * TJ, 0, stream>>>(A, slot); });
+        L(G_TURB, [&] { k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1); });
+        L(G_TURB, [&] { k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0); });
+        L(G_TURB, [&] { k_turb_update<<<ntiles, TI * TJ, 0, stream>>>(A); });
       }
     } else {
       launch_mean_flow_prep();
-      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot);
-      k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0);
+      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot); });
+      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
       launch_mean_flow_prep();
-      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1);
-      k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0);
+      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
       launch_mean_flow_prep();
-      k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1);
-      k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1);
+      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1); });
     }
+  }
+  // n iterations with CUDA events around every launch (no graph); per-group totals in prof_ms / prof_launches
+  int profile(long long n) {
+    for (int g = 0; g < G_N; ++g) prof_ms[g] = 0, prof_launches[g] = 0;
+    bool g0 = use_graphs;
+    use_graphs = false;
+    profiling = true;
+    int rc = run(n, nullptr);
+    profiling = false;
+    use_graphs = g0;
+    return rc;
+  }
+
+  bool use_graphs = true;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms_per_iter = 0.0;
+  // one chunk of `chunk` iterations: captured once into a CUDA graph, replayed afterwards
+  int launch_chunk(int chunk) {
+    const int nc = (int)cases.size();
+    if (!use_graphs) {
+      BK_CUDA(cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream));
+      if (any_sst) BK_CUDA(cudaMemsetAsync(A.tsum, 0, (size_t)chunk * nc * sizeof(double), stream));
+      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      BK_CUDA(cudaGetLastError());
+      return 0;
+    }
+    if (!graph || graph_len != chunk) {
+      if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+      cudaGraph_t g;
+      BK_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream);
+      if (any_sst) cudaMemsetAsync(A.tsum, 0, (size_t)chunk * nc * sizeof(double), stream);
+      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      cudaError_t le = cudaGetLastError();
+      BK_CUDA(cudaStreamEndCapture(stream, &g));
+      if (le != cudaSuccess) {
+        cudaGraphDestroy(g);
+        err = std::string("launch during capture: ") + cudaGetErrorString(le);
+        return 3;
+      }
+      cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        graph = nullptr;
+        err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie);
+        return 3;
+      }
+      graph_len = chunk;
+    }
+    BK_CUDA(cudaGraphLaunch(graph, stream));
+    return 0;
   }
 
   // n iterations; residual (n x ncases, iteration-major) may be null
   int run(long long n, double* residual) {
     const int nc = (int)cases.size();
     long long done = 0;
+    if (!ev0) {
+      BK_CUDA(cudaEventCreate(&ev0));
+      BK_CUDA(cudaEventCreate(&ev1));
+    }
+    double ms_total = 0.0;
     while (done < n) {
       int chunk = (int)std::min<long long>(n - done, slots);
-      BK_CUDA(cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream));
-      if (any_sst) BK_CUDA(cudaMemsetAsync(A.tsum, 0, (size_t)chunk * nc * sizeof(double), stream));
-      for (int k = 0; k < chunk; ++k) launch_iteration(k);
-      BK_CUDA(cudaGetLastError());
+      BK_CUDA(cudaEventRecord(ev0, stream));
+      int rc_ = launch_chunk(chunk);
+      if (rc_) return rc_;
+      BK_CUDA(cudaEventRecord(ev1, stream));
       if (residual) {
         h_rsum.resize((size_t)chunk * nc);
         BK_CUDA(cudaMemcpyAsync(h_rsum.data(), A.rsum, h_rsum.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -661,6 +810,9 @@ struct ArenaHost {
         BK_CUDA(cudaMemcpyAsync(ht.data(), A.tsum + (size_t)(chunk - 1) * nc, nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
       }
       BK_CUDA(cudaStreamSynchronize(stream));
+      float ms = 0.f;
+      BK_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      ms_total += ms;
       if (any_sst) {
         last_turb_residual.resize(nc);
         for (int c = 0; c < nc; ++c) last_turb_residual[c] = std::sqrt(ht[c] / (double)desc[c].n_active);
@@ -671,6 +823,7 @@ struct ArenaHost {
             residual[(done + k) * nc + c] = std::sqrt(h_rsum[(size_t)k * nc + c] / (double)desc[c].n_active);
       done += chunk;
     }
+    last_ms_per_iter = n > 0 ? ms_total / (double)n : 0.0;
     return 0;
   }
 

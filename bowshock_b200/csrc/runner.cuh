@@ -1,0 +1,261 @@
+// Run control above the arena: the FP64 force pass (forces.cuh) used as the convergence monitor, the stop rules of
+// crates/bowshock-core/src/engine/run.rs:105-170, the chunked run of engine/gpu.rs:86-169 (SYNC = 50 iterations per
+// device->host exchange, the stop iteration found CPU-equivalently inside a chunk) and, for the batched arena, the
+// per-case convergence masks. Each chunk of iterations is captured once into a CUDA graph and replayed.
+#pragma once
+#include <functional>
+
+#include "forces.cuh"
+#include "host_arena.cuh"
+
+namespace bk {
+
+constexpr int SYNC = 50;  // engine/gpu.rs:24-25, numerics.rs:236 (MONITOR_EVERY)
+constexpr size_t DRAG_REL_WINDOW = 500;
+
+struct RunParams {
+  long long max_iter = 10000, min_iter = 0;
+  double drop_orders = 6.0;
+  long long monitor_window = 2000;
+  bool has_monitor_tol = false;
+  double monitor_tol = 0;
+  bool has_mean_window = false;
+  long long mean_window = 0;
+  bool has_drag_rel_tol = false;
+  double drag_rel_tol = 0;
+  int wake = 0;
+  bool warm = false;
+  double r_ref = -1;
+};
+
+struct Forces {
+  double f[F_NF];
+  double cd_total(int nseg) const {
+    double fore = f[F_CD_NOSE];
+    for (int k = 0; k < nseg; ++k) fore = fore + f[F_CD_AFT0 + k];
+    return fore + f[F_CD_FRICTION] + f[F_CD_BASE];
+  }
+};
+
+// run.rs:157-170
+inline bool mean_stationary(const std::vector<std::pair<long long, double>>& hist, size_t k) {
+  size_t from = 0;
+  while (from < hist.size() && hist[from].first <= 2000) ++from;
+  if (k == 0 || hist.size() - from < 2 * k) return false;
+  const auto* w = &hist[hist.size() - 2 * k];
+  double m0 = 0, m1 = 0;
+  for (size_t t = 0; t < k; ++t) m0 += w[t].second;
+  for (size_t t = k; t < 2 * k; ++t) m1 += w[t].second;
+  m0 /= (double)k;
+  m1 /= (double)k;
+  double m = 0.5 * (m0 + m1), lo = INFINITY, hi = -INFINITY;
+  for (size_t t = 0; t < 2 * k; ++t) lo = std::fmin(lo, w[t].second), hi = std::fmax(hi, w[t].second);
+  double a = w[2 * k - 2].second - m, b = w[2 * k - 1].second - m;
+  return std::fabs(m1 - m0) <= 2e-3 * std::fabs(m) && hi - lo <= 0.05 * std::fabs(m) && a * b < 0.0;
+}
+
+// run.rs:105-150; returns true with `why` set when iteration `it` (0-based) ends the run
+inline bool stop_reason(const RunParams& n, bool viscous, long long it, double r, double reference, long long skip,
+                        const std::vector<std::pair<long long, double>>& hist, int& why) {
+  if (!std::isfinite(r) || (!hist.empty() && hist.back().first == it + 1 && (!std::isfinite(hist.back().second) || std::fabs(hist.back().second) > 1e3))) {
+    why = 5;
+    return true;
+  }
+  if (it + 1 < n.min_iter) return false;
+  if (it > skip && reference / r >= std::pow(10.0, n.drop_orders)) {
+    why = 1;
+    return true;
+  }
+  if (n.has_drag_rel_tol) {
+    size_t k = DRAG_REL_WINDOW / SYNC;
+    if (viscous && !hist.empty() && hist.back().first == it + 1 && it + 1 >= (long long)DRAG_REL_WINDOW && reference / r >= 100.0 &&
+        hist.size() >= k) {
+      double lo = INFINITY, hi = -INFINITY, mean = 0;
+      for (size_t t = hist.size() - k; t < hist.size(); ++t) lo = std::fmin(lo, hist[t].second), hi = std::fmax(hi, hist[t].second), mean += hist[t].second;
+      mean /= (double)k;
+      if (hi - lo < n.drag_rel_tol * std::fabs(mean)) {
+        why = 2;
+        return true;
+      }
+    }
+  }
+  if (n.has_monitor_tol && it % 500 == 499 && it + 1 >= 2 * n.monitor_window && reference / r >= 100.0) {
+    size_t k = (size_t)(n.monitor_window / SYNC);
+    if (hist.size() >= k) {
+      double lo = INFINITY, hi = -INFINITY;
+      for (size_t t = hist.size() - k; t < hist.size(); ++t) lo = std::fmin(lo, hist[t].second), hi = std::fmax(hi, hist[t].second);
+      if (hi - lo < n.monitor_tol) {
+        why = (!viscous && n.wake == 1) ? 3 : 2;
+        return true;
+      }
+    }
+  }
+  if (viscous && n.has_mean_window && !hist.empty() && hist.back().first == it + 1 && mean_stationary(hist, (size_t)(n.mean_window / SYNC))) {
+    why = 4;
+    return true;
+  }
+  return false;
+}
+
+// per-case run state of the chunked runner
+struct CaseRun {
+  RunParams p;
+  int nseg = 0;
+  long long it = 0, skip = 20;
+  double rmax = 0;
+  std::vector<double> residual;
+  std::vector<std::pair<long long, double>> hist;
+  bool done = false;
+  int reason = 0;
+  double last_monitor = NAN;
+};
+
+struct ForcePass {
+  double *nx = nullptr, *nr = nullptr, *xc = nullptr, *rc = nullptr, *out = nullptr;
+  long long* node_off = nullptr;
+  BodyDev* bodies = nullptr;
+  std::vector<BodyDev> hb;
+  int nc = 0;
+  ~ForcePass() {
+    for (void* p : {(void*)nx, (void*)nr, (void*)xc, (void*)rc, (void*)out, (void*)node_off, (void*)bodies})
+      if (p) cudaFree(p);
+  }
+  int setup(ArenaHost& ar) {
+    std::string& err = ar.err;
+    nc = (int)ar.cases.size();
+    long long nn = 0;
+    std::vector<long long> off(nc);
+    for (int k = 0; k < nc; ++k) off[k] = nn, nn += (long long)(ar.cases[k].ni + 1) * (ar.cases[k].nj + 1);
+    int rc_ = 0;
+    if ((rc_ = dalloc(&nx, nn, err)) || (rc_ = dalloc(&nr, nn, err)) || (rc_ = dalloc(&xc, ar.ncell, err)) || (rc_ = dalloc(&rc, ar.ncell, err)) ||
+        (rc_ = dalloc(&out, (size_t)nc * F_NF, err)) || (rc_ = dalloc(&node_off, nc, err)) || (rc_ = dalloc(&bodies, nc, err)))
+      return rc_;
+    for (int k = 0; k < nc; ++k) {
+      const HostCase& h = ar.cases[k];
+      BK_CUDA(cudaMemcpy(nx + off[k], h.x.data(), h.x.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(nr + off[k], h.r.data(), h.r.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(xc + ar.desc[k].cell_off, h.xc.data(), h.xc.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(rc + ar.desc[k].cell_off, h.rc.data(), h.rc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    BK_CUDA(cudaMemcpy(node_off, off.data(), nc * sizeof(long long), cudaMemcpyHostToDevice));
+    hb.assign(nc, BodyDev{});
+    return 0;
+  }
+  int set_body(ArenaHost& ar, int k, const bowshock_body* b) {
+    std::string& err = ar.err;
+    BodyDev d{};
+    mesh::Body mb;
+    mb.nose = b->nose_kind;
+    mb.fineness = b->fineness;
+    mb.half_angle = b->half_angle;
+    mb.param = b->param;
+    for (int s = 0; s < b->nseg && s < MAX_SEG; ++s) mb.seg_len.push_back(b->seg_length[s]), mb.seg_slope.push_back(b->seg_slope[s]);
+    d.nose_length = mb.nose_length();
+    d.rb2 = 0.25;
+    d.x_base = mb.x_base();
+    d.nseg = (int)mb.seg_len.size();
+    for (int s = 0; s <= d.nseg; ++s) d.stations[s] = mb.station(s).first;
+    d.has_body = 1;
+    hb[k] = d;
+    BK_CUDA(cudaMemcpy(bodies + k, &d, sizeof(BodyDev), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int run(ArenaHost& ar, std::vector<Forces>& res) {
+    std::string& err = ar.err;
+    k_forces<<<nc, 256, 0, ar.stream>>>(ar.A, bodies, nx, nr, node_off, xc, rc, out);
+    BK_CUDA(cudaGetLastError());
+    std::vector<double> h((size_t)nc * F_NF);
+    BK_CUDA(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ar.stream));
+    BK_CUDA(cudaStreamSynchronize(ar.stream));
+    res.resize(nc);
+    for (int k = 0; k < nc; ++k) std::memcpy(res[k].f, &h[(size_t)k * F_NF], F_NF * sizeof(double));
+    return 0;
+  }
+};
+
+// run.rs:174-185: total CD of a viscous case, else the nose CD (sting) or the area-mean base Cp (base wake)
+inline double monitor_of(const HostCase& h, const RunParams& p, const Forces& f, int nseg) {
+  if (h.viscous) return f.cd_total(nseg);
+  return p.wake == 0 ? f.f[F_CD_NOSE] : f.f[F_CP_BASE];
+}
+
+inline void fill_point(const CaseRun& cr, const Forces& f, bowshock_point_result* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->iters = (uint64_t)cr.residual.size();
+  o->residual_peak = cr.rmax;
+  double last = cr.residual.empty() ? cr.rmax : cr.residual.back();
+  o->drop_orders = (cr.rmax > 0 && last > 0) ? std::log10(cr.rmax / last) : 0.0;
+  o->stop_reason = cr.reason;
+  o->forces.cd_nose = f.f[F_CD_NOSE];
+  o->forces.cd_nose_cell = f.f[F_CD_NOSE_CELL];
+  o->forces.cd_base = f.f[F_CD_BASE];
+  o->forces.cp_base = f.f[F_CP_BASE];
+  o->forces.cp_base_cell = f.f[F_CP_BASE_CELL];
+  o->forces.cd_friction = f.f[F_CD_FRICTION];
+  o->forces.y_plus_max = f.f[F_YPLUS];
+  for (int k = 0; k < MAX_SEG; ++k) o->forces.cd_aft[k] = k < cr.nseg ? f.f[F_CD_AFT0 + k] : 0.0;
+  o->forces.cd_total = f.cd_total(cr.nseg);
+  o->last_monitor = cr.last_monitor;
+}
+
+// Cold (or warm) start of case k for a run: free stream, turbulence re-initialised, counters reset (run.rs:44-63).
+inline int start_case(ArenaHost& ar, int k, const RunParams& p, long long first_order_iters) {
+  int rc = 0;
+  if (!p.warm) {
+    if ((rc = ar.reset_case(k))) return rc;
+    if (ar.cases[k].viscous && ar.cases[k].turbulence == 1 && (rc = ar.turb_init(k))) return rc;
+  }
+  if ((rc = ar.set_counter(ar.d_iter, k, p.warm ? (int)first_order_iters : 0))) return rc;
+  return ar.set_counter(ar.d_ramp, k, 0);
+}
+
+// Iterate every active case of the arena to its stop rule in chunks of SYNC iterations.
+inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
+                       const std::function<bool(int, long long, double, double)>& progress) {
+  const int nc = (int)ar.cases.size();
+  std::vector<int> act(nc);
+  for (int k = 0; k < nc; ++k) act[k] = runs[k].done ? 0 : 1;
+  int rc = ar.set_active(act.data());
+  if (rc) return rc;
+  std::vector<double> res((size_t)SYNC * nc);
+  std::vector<Forces> f;
+  while (true) {
+    int left = 0;
+    for (int k = 0; k < nc; ++k) left += !runs[k].done;
+    if (!left) break;
+    if ((rc = ar.run(SYNC, res.data()))) return rc;
+    if ((rc = fp.run(ar, f))) return rc;
+    bool mask_changed = false;
+    for (int k = 0; k < nc; ++k) {
+      CaseRun& cr = runs[k];
+      if (cr.done) continue;
+      double mon = monitor_of(ar.cases[k], cr.p, f[k], cr.nseg);
+      bool sample = cr.p.wake == 1 || cr.p.has_monitor_tol || cr.p.has_drag_rel_tol;
+      for (int t = 0; t < SYNC && !cr.done; ++t) {
+        long long it = cr.it;
+        double r = res[(size_t)t * nc + k];
+        cr.residual.push_back(r);
+        if (it >= cr.skip) cr.rmax = std::fmax(cr.rmax, r);
+        if (sample && it % SYNC == SYNC - 1) cr.hist.emplace_back(it + 1, mon), cr.last_monitor = mon;
+        int why = 0;
+        if (stop_reason(cr.p, ar.cases[k].viscous, it, r, cr.p.r_ref >= 0 ? cr.p.r_ref : cr.rmax, cr.skip, cr.hist, why)) {
+          cr.done = true;
+          cr.reason = why;
+        } else if (it + 1 >= cr.p.max_iter) {
+          cr.done = true;
+          cr.reason = 0;
+        }
+        cr.it += 1;
+      }
+      if (!cr.done && progress && !progress(k, cr.it, cr.residual.back(), mon)) {
+        cr.done = true;
+        cr.reason = 6;
+      }
+      if (cr.done) act[k] = 0, mask_changed = true;
+    }
+    if (mask_changed && (rc = ar.set_active(act.data()))) return rc;
+  }
+  return 0;
+}
+
+}  // namespace bk

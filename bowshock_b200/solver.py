@@ -67,6 +67,15 @@ EXPLICIT = "explicit"
 
 
 @dataclass
+class MgParams:  # solver.rs:123-140 (DEFAULT): FAS multigrid with the SSP-RK3 smoother
+    levels: int = 6
+    pre: int = 1
+    post: int = 1
+    gamma: int = 1
+    coarsest: int = 4
+
+
+@dataclass
 class Viscous:  # solver.rs:164-176
     re_c: float
     sutherland: float
@@ -142,6 +151,9 @@ class GpuSolver:
         """`scheme`: EXPLICIT or an ImplicitParams."""
         if scheme == EXPLICIT:
             s = _ffi.Scheme(kind=SCHEME_EXPLICIT)
+        elif isinstance(scheme, MgParams):
+            s = _ffi.Scheme(kind=2, mg_levels=scheme.levels, mg_pre=scheme.pre, mg_post=scheme.post, mg_gamma=scheme.gamma,
+                            mg_coarsest=scheme.coarsest)
         else:
             p = scheme
             s = _ffi.Scheme(SCHEME_IMPLICIT, p.cfl0, p.cfl_max, p.growth, p.dt_mode, int(p.lines), int(p.implicit_bc),
@@ -222,3 +234,41 @@ class GpuSolver:
         out = np.zeros(8 * j_rows)
         self._check(_ffi.load().bowshock_solver_base_cells(self._h, _dp(out)))
         return out.reshape(j_rows, 2, 4)
+
+    # -------------------------------------------------------------- FP64 forces and the runner (engine/run.rs, gpu.rs)
+    def forces(self, body) -> dict:
+        """Force integration of the current state (engine/run.rs:188-313), FP64 on the device. `body`: case.Body."""
+        f = _ffi.Forces()
+        b = body.c()
+        self._check(_ffi.load().bowshock_solver_forces(self._h, C.byref(b), C.byref(f)))
+        return forces_dict(f, len(body.segments))
+
+    def run_to_stop(self, body, numerics, wake, warm=False, r_ref=None, progress=None):
+        """`GpuRunner::run_on` (engine/gpu.rs:86-169): iterate to the stop rules of engine/run.rs:105-170 in chunks of 50,
+        then the forces of the final state. `progress(case, iteration, residual, monitor) -> bool` (False cancels)."""
+        p = numerics.run_params(wake, warm, r_ref)
+        out = _ffi.PointResult()
+        hist = np.zeros(int(numerics.max_iter) + 64)
+        b = body.c()
+        cb = _ffi.PROGRESS_FN(lambda u, k, it, r, m: 0 if progress is None or progress(k, it, r, m) else 1)
+        self._check(_ffi.load().bowshock_solver_run_to_stop(self._h, C.byref(b), C.byref(p), C.byref(out), _dp(hist), hist.size,
+                                                            cb if progress else _ffi.PROGRESS_FN(0), None))
+        return point_dict(out, len(body.segments), hist[: out.iters].copy())
+
+
+STOP_REASONS = ["max iterations", "residual drop", "CD stationary", "base pressure stationary", "mean stationary",
+                "non-finite residual", "cancelled"]
+
+
+def forces_dict(f, nseg):
+    return dict(cd_nose=f.cd_nose, cd_nose_cell=f.cd_nose_cell, cd_aft=list(f.cd_aft)[:nseg], cd_base=f.cd_base, cp_base=f.cp_base,
+                cp_base_cell=f.cp_base_cell, cd_friction=f.cd_friction, y_plus_max=f.y_plus_max, cd_total=f.cd_total)
+
+
+def point_dict(p, nseg, residual=None):
+    d = dict(iters=p.iters, residual_peak=p.residual_peak, drop_orders=p.drop_orders, stop_reason=STOP_REASONS[p.stop_reason],
+             last_monitor=p.last_monitor)
+    d.update(forces_dict(p.forces, nseg))
+    if residual is not None:
+        d["residual"] = residual
+    return d

@@ -48,6 +48,7 @@ extern "C" {
 #define BOWSHOCK_BC_PRESSURE_OUTFLOW 4
 /* scheme kinds (solver.rs:143-153): the GPU implements Explicit and Implicit, like the reference's GPU solver */
 #define BOWSHOCK_SCHEME_EXPLICIT 0
+#define BOWSHOCK_SCHEME_MULTIGRID 2
 #define BOWSHOCK_SCHEME_IMPLICIT 3
 #define BOWSHOCK_DT_SUM 0
 #define BOWSHOCK_DT_MIN_DIRECTION 1
@@ -63,7 +64,8 @@ typedef struct {
   uint64_t first_order_iters;
 } bowshock_config;
 
-/* implicit.rs:59-84 `ImplicitParams` (kind = BOWSHOCK_SCHEME_IMPLICIT) or the explicit SSP-RK3 scheme */
+/* implicit.rs:59-84 `ImplicitParams` (kind = BOWSHOCK_SCHEME_IMPLICIT), the explicit SSP-RK3 scheme, or FAS multigrid
+ * with the SSP-RK3 smoother, solver.rs:123-140 `MgParams` (kind = BOWSHOCK_SCHEME_MULTIGRID; Euler only, as the reference) */
 typedef struct {
   int32_t kind;
   double cfl0, cfl_max, growth;
@@ -71,6 +73,7 @@ typedef struct {
   uint64_t sub_iters;
   int32_t roe;
   double eps_fix;
+  uint64_t mg_levels, mg_pre, mg_post, mg_gamma, mg_coarsest;
 } bowshock_scheme;
 
 /* solver.rs:59-102 `Block` */
@@ -275,6 +278,12 @@ int bowshock_arena_set_state(bowshock_arena* a, uint64_t k, const double* u);
 int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active);
 /* mean device time of one arena iteration over the last bowshock_arena_run, in milliseconds (CUDA events) */
 int bowshock_arena_last_ms_per_iter(const bowshock_arena* a, double* ms);
+
+/* Per-kernel profile (the reference's Profile of gpu/mod.rs:533-542): n iterations launched one kernel at a time with CUDA
+ * events around each launch; per kernel group (prims, viscous, residual, i-lines, j-lines, defect, turbulence, stage) the
+ * total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
+#define BOWSHOCK_PROFILE_GROUPS 8
+int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
 
 #ifdef __cplusplus
 }

@@ -102,3 +102,58 @@ def test_g3_body_sst_matches_oracle():  # viscous.rs body check: 30 implicit ite
         err = np.max(np.abs(t_g[fluid, e] - t_c[fluid, e]) / np.abs(t_c[fluid, e]))
         assert err < 1e-2, f"G3 {name} max rel diff {err:.3e}"
     assert np.max(np.abs(m_g[fluid] - cpu.mu_t[fluid]) / np.abs(cpu.mu_t[fluid])) < 1e-2
+
+
+def _mg_spec(ni, nj, mach, limiter, cfl, u_scale=None):
+    from tests.test_oracle_solver import mg_grid
+    x, r = mg_grid(ni, nj)
+    spec = cases.Spec(ni, nj, x, r, cfl, limiter, tuple(o.freestream(mach)),
+                      (o.BC_CHARACTERISTIC, o.BC_CHARACTERISTIC, o.BC_SLIPWALL, o.BC_CHARACTERISTIC), 0, label="mg grid")
+    if u_scale is not None:
+        fs = o.freestream(mach)
+        w = np.array([fs[0] * u_scale[0], fs[1], fs[2], fs[3] * u_scale[1]])
+        spec.u0 = np.tile(o.prim_to_cons(w), (ni * nj, 1))
+    return spec
+
+
+def _mg_pair(spec):
+    import bowshock_b200 as bk
+    cpu = cases.oracle_solver(spec)
+    levels = cpu.set_scheme(o.multigrid_scheme())
+    gpu = cases.gpu_solver(spec)
+    gpu.set_scheme(bk.solver.MgParams())
+    if spec.u0 is not None:
+        gpu.set_state(spec.u0)
+    return cpu, gpu, levels
+
+
+def test_multigrid_hierarchy_preserves_the_free_stream():  # multigrid.rs:239-258
+    spec = _mg_spec(64, 32, 0.5, o.VAN_ALBADA, 0.5)
+    cpu, gpu, levels = _mg_pair(spec)
+    assert levels == 3
+    gpu.run(30)
+    assert np.max(np.abs(gpu.state_f64() - o.prim_to_cons(o.freestream(0.5)))) < 1e-6
+
+
+def test_multigrid_cycles_match_the_oracle():  # cycle-by-cycle FAS state, perturbed start of multigrid.rs:274-276
+    spec = _mg_spec(32, 16, 0.4, o.FIRST_ORDER, 0.8, u_scale=(1.02, 1.03))
+    cpu, gpu, _ = _mg_pair(spec)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)
+    assert cases.state_diff(gpu.state_f64(), cpu.u) < 1e-5
+    assert cases.residual_diff(rg[:10], rc[:10]) < 1e-3
+
+
+def test_multigrid_reaches_the_explicit_fixed_point():  # multigrid.rs:260-291, to FP32 round-off
+    spec = _mg_spec(32, 16, 0.4, o.FIRST_ORDER, 0.8, u_scale=(1.02, 1.03))
+    cpu = cases.oracle_solver(spec)
+    for _ in range(4000):
+        if cpu.step() < 1e-11:
+            break
+    import bowshock_b200 as bk
+    gpu = cases.gpu_solver(spec)
+    gpu.set_scheme(bk.solver.MgParams())
+    gpu.set_state(spec.u0)
+    r = gpu.run(1500)
+    assert r[-1] < 1e-6 * r[0]
+    assert np.max(np.abs(gpu.state_f64() - cpu.u)) < 2e-6

@@ -1,0 +1,61 @@
+"""Whole runs on the B200 backend: the FP64 device force pass against the oracle's post-processing of the same state,
+converged drag of the reference's G3 body against the FP64 oracle (|dCD| <= 1e-4, the target of the sweep metric), and
+the batched arena against single-case solvers."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_ffi as o
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def g3_cases():
+    from bowshock_b200.case import Body, Case, WAKE_BASE, rans_params
+    from tests.golden.g3_case import g3_case
+    re_c, suth = rans_params(0.0, 0.1)
+    pc = Case.viscous_case(0.5, Body(0, fineness=3.0, segments=((6.0, 0.0),)), 0, WAKE_BASE, re_c, suth, 0.5)
+    return pc, g3_case()
+
+
+def test_device_forces_match_the_oracle_post_processing():  # engine/run.rs:188-313 on the same state
+    pc, oc = g3_cases()
+    s = pc.build_solver()
+    s.run(300)
+    f = s.forces(pc.body)
+    cpu = o.Solver.from_case(oc)
+    cpu.u = s.state_f64()
+    r = o.finish(oc, cpu)
+    for k in ("cd_nose", "cd_base", "cd_friction", "cp_base", "y_plus_max", "cd_total"):
+        a, b = f[k], getattr(r, k)
+        assert abs(a - b) <= 1e-10 * max(1.0, abs(b)), (k, a, b)
+
+
+def test_g3_converged_drag_matches_the_fp64_oracle():
+    pc, _ = g3_cases()
+    ref = json.load(open(os.path.join(HERE, "golden", "g3_oracle.json")))
+    s = pc.build_solver()
+    r = s.run_to_stop(pc.body, pc.numerics, pc.wake)
+    print("G3 on B200:", {k: r[k] for k in ("iters", "stop_reason", "cd_total", "cd_friction", "cd_base", "cp_base", "y_plus_max")})
+    assert r["stop_reason"] in ("CD stationary", "residual drop", "mean stationary")
+    for k in ("cd_total", "cd_friction", "cd_base"):
+        assert abs(r[k] - ref[k]) <= 1e-4, (k, r[k], ref[k])
+
+
+def test_arena_cases_match_single_case_solvers():
+    from bowshock_b200.arena import Arena
+    from bowshock_b200.case import Body, Case, WAKE_BASE, WAKE_STING
+    pc, _ = g3_cases()
+    cases = [Case.new(0.5, Body(0, 3.0, segments=((6.0, 0.0),)), 0, WAKE_STING), Case.new(1.5, Body(0, 3.0, segments=((6.0, 0.0),)), 0, WAKE_BASE), pc]
+    for c in cases:
+        c.numerics.first_order_iters = 5
+    a = Arena(cases)
+    ra = a.run(40)
+    for k, c in enumerate(cases):
+        s = c.build_solver()
+        rs = s.run(40)
+        assert np.array_equal(a.state(k), s.state_f64()), f"case {k} differs from its single-case solver"
+        assert np.allclose(ra[:, k], rs, rtol=1e-12)
