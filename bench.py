@@ -1,18 +1,20 @@
 """Benchmark of the B200 backend on the seeded 32-case mixed sweep (Euler + RANS SST, grids 96x48 to 320x160).
 
-Metric: converged cases per hour on one B200 for the batched line-implicit backend. One step = one line-implicit iteration
-of the whole 32-case arena (all cases active). `value` is the steady-state throughput of a persistent arena that is kept
-full (converged cases replaced by new ones):
+Metric: converged cases per hour on one B200 at |dCD| <= 1e-4 against the FP64 oracle's converged CD of the same case
+(tests/golden/sweep_census.json, made by tests/golden/make_sweep_census.py).
 
-    cases/s = n_cases * sum_k cells_k / (t_step * sum_k cells_k * N_k)
-
-with t_step the device time of one arena iteration (CUDA events, the timed region: K steps replayed from CUDA graphs) and
-N_k the iterations case k needs to reach its stop rule, measured in the same run by the census (every case cold-started and
-iterated to the reference's stop rules, converged cases masked out). `e2e` is the census itself measured by the wall clock
-through the public API (meshing, arena creation with the host->device copies, the solve, the device->host read-back of
-residual histories and forces). `cpu_baseline` times the oracle (the f64 C++ restatement of the reference CPU solver, all
-host threads) on a bounded sample of iterations of every case and applies the same N_k. The plain single-case backend is
-timed the same way (one case per arena, one after another) and reported as `config.plain_single_case_cases_per_hr`.
+  timed region  K line-implicit iterations of the whole 32-case arena (every case active), replayed from CUDA graphs,
+                CUDA events on the launching stream: `ms_per_step`, the roofline of the dominant kernel group, the launch
+                count. 760,692 cells x ~0.5-1.6 KB per cell-update is far above the 126 MB L2, so no flush is needed.
+  value         the census: every case cold-started from the free stream and iterated to the reference's stop rules in one
+                arena (converged cases masked out), the device time of all its iterations and FP64 force passes (CUDA
+                events): value = 3600 * (cases within |dCD| <= 1e-4) / census device seconds.
+  e2e           the same census through the public API by the wall clock: meshing, arena creation with the host->device
+                copies, the solve with its chunked read-backs, the forces.
+  plain         the plain single-case backend: each case alone through GpuSolver.run_to_stop (same kernels, one case per
+                launch), wall clock, reported as config.plain_single_case_cases_per_hr.
+  cpu_baseline  the oracle (f64 C++ restatement of the reference CPU path, all host threads) timed on a bounded sample of
+                iterations of every case, times the oracle's own iteration counts to its stop rules.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -96,8 +98,31 @@ class Clocks:
 
 
 def build_cases(rank=0):
+    """The 32-case sweep; every rank solves the same seeded sweep (replicas: the cases shard across GPUs with no exchange,
+    and the oracle's census of this seed checks every rank's CDs)."""
     from bowshock_b200.sweep import SEED, sweep_cases
-    return sweep_cases(32, SEED + rank)
+    return sweep_cases(32, SEED)
+
+
+def h2d_bytes(cases, grids):
+    """Bytes the census copies host->device per case: face metrics (float4 + centres float2, + FP64-derived face stencils for
+    viscous cases), cell geometry, the FP64 nodes and cell centres of the force pass, wall distance and turbulence start for
+    SST, and the free-stream start state (float pair)."""
+    total = 0
+    for c, g in zip(cases, grids):
+        ni, nj = g[0], g[1]
+        fi, fj, nc, nn = (ni + 1) * nj, ni * (nj + 1), ni * nj, (ni + 1) * (nj + 1)
+        b = 24 * (fi + fj) + 16 * nc + 16 * nn + 16 * nc + 32 * nc
+        if c.viscous is not None:
+            b += 16 * (fi + fj) + 4 * nc + 8 * nc
+        total += b
+    return total
+
+
+def d2h_bytes(ncases, iters):
+    """Bytes read back per 50-iteration chunk (density residuals, turbulence residual, FP64 forces), over the census."""
+    chunks = (max(iters) + 49) // 50
+    return int(chunks * (50 * ncases * 8 + ncases * 8 + ncases * 15 * 8))
 
 
 def combine_ranks(dist, ms_step, value, e2e):
@@ -113,66 +138,87 @@ def combine_ranks(dist, ms_step, value, e2e):
     return float(t.item()), float(s[0]), float(s[1])
 
 
-def cpu_sample(cases, grids, n_iter, census):
-    """The oracle on `n_iter` iterations of every case (all host threads): cases/hr with the census iteration counts."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_ffi as o
-    from tests import cases as tc
-    t_case = []
-    for k, c in enumerate(cases):
-        ni, nj, x, r, blk = grids[k]
-        cfg = c.config()
-        spec = tc.Spec(ni, nj, np.asarray(x).reshape(nj + 1, ni + 1), np.asarray(r).reshape(nj + 1, ni + 1), cfg.cfl, cfg.limiter,
-                       tuple(cfg.freestream), tuple(cfg.bc), cfg.first_order_iters, c.numerics.low_mach, blk,
-                       dict(cfl0=c.numerics.scheme.cfl0, cfl_max=c.numerics.scheme.cfl_max, growth=c.numerics.scheme.growth,
-                            dt_mode=c.numerics.scheme.dt_mode, lines=True, implicit_bc=True, sub_iters=c.numerics.scheme.sub_iters,
-                            roe=True, eps_fix=0.1),
-                       None if c.viscous is None else dict(re_c=c.viscous.re_c, sutherland=c.viscous.sutherland, turbulence=1,
-                                                           wall_i_start=c.viscous.wall_i_start, roughness=0.0))
-        s = tc.oracle_solver(spec)
-        s.step()  # warm-up
-        t0 = time.perf_counter()
-        s.steps(n_iter)
-        t_case.append((time.perf_counter() - t0) / n_iter)
-    n = np.array([census[k] for k in range(len(cases))], dtype=float)
-    total_s = float(np.sum(np.array(t_case) * n))
-    return 3600.0 * len(cases) / total_s, t_case
-
-
 def census_fixture():
+    """The oracle's census of the sweep: {case index: {iters, cd_total, ...}} (cases it has not finished are absent)."""
     p = os.path.join(ROOT, "tests", "golden", "sweep_census.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f)
-    return None
+            return {int(k): v for k, v in json.load(f)["cases"].items()}
+    return {}
+
+
+class OracleSample:
+    """The oracle solver of every case of the sweep, built once; `step(k)` times one iteration of case k."""
+
+    def __init__(self, cases):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+        import oracle_ffi as o
+        from sweep_oracle import oracle_case
+        self.o = o
+        self.solvers = []
+        for c in cases:
+            oc = oracle_case(c)
+            s = o.Solver.from_case(oc)
+            cfg = s.config
+            cfg.cfl, cfg.limiter, cfg.first_order_iters = oc.numerics.cfl, oc.numerics.limiter, oc.numerics.first_order_iters
+            s.set_config(cfg)
+            s.set_low_mach(bool(oc.numerics.low_mach))
+            s.set_scheme(oc.numerics.scheme)
+            self.solvers.append(s)
+        self.t = [[] for _ in cases]
+
+    def step(self, k):
+        t0 = time.perf_counter()
+        self.solvers[k].step()
+        self.t[k].append(time.perf_counter() - t0)
+
+    def cases_per_hr(self, iters):
+        """3600 n / sum_k (seconds per iteration of case k x its iterations to the stop rule)."""
+        total = sum(float(np.mean(self.t[k])) * iters[k] for k in range(len(self.solvers)))
+        return 3600.0 * len(self.solvers) / total
+
+
+def oracle_iters(fx, cases):
+    """The oracle's iterations to its stop rule per case; a case it has not finished takes the mean of its kind."""
+    out, filled = [], []
+    for k, c in enumerate(cases):
+        if k in fx:
+            out.append(fx[k]["iters"])
+        else:
+            same = [v["iters"] for v in fx.values() if v["viscous"] == (c.viscous is not None)]
+            out.append(int(np.mean(same)) if same else int(c.numerics.max_iter))
+            filled.append(k)
+    return out, filled
 
 
 def run_reference(args, rank, world):
-    """The reference arm: the reference CPU path (its f64 restatement, the oracle) on the same workload and metric."""
+    """The reference arm: the reference CPU path (its f64 restatement, the oracle) on the same workload and metric. One step
+    = one iteration of one case, rotating through the 32 cases; cases/hr from the mean seconds per iteration of each case
+    and the oracle's own iteration counts to its stop rules."""
     if rank != 0:
         return None
     cases = build_cases(0)
-    grids = [c.grid() for c in cases]
     fx = census_fixture()
-    census = fx["iters"] if fx else [4000] * len(cases)
-    n_iter = 2
-    vals, t_case = [], None
-    for _ in range(args.warmup):
-        cpu_sample(cases[:2], grids[:2], 1, census)
+    iters, filled = oracle_iters(fx, cases)
+    smp = OracleSample(cases)
+    for s in range(max(args.warmup, len(cases))):  # at least one untimed iteration of every case
+        smp.solvers[s % len(cases)].step()
+    steps = max(args.steps, len(cases))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, t_case = cpu_sample(cases, grids, n_iter, census)
-        vals.append(v)
+    for s in range(steps):
+        smp.step(s % len(cases))
     wall = time.perf_counter() - t0
-    value = float(np.mean(vals))
-    threads = os.cpu_count()
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+    value = smp.cases_per_hr(iters)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    sample = f"{steps} oracle iterations, one case per step rotating through the 32 cases, x the oracle's iterations to its stop rules"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * wall / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 32-case sweep, SplitMix64 seed 0x0B05C0C2)",
-            "config": {"workload": "32-case mixed Euler/SST sweep, reference CPU path (f64 restatement), line-implicit",
-                       "cases": len(cases), "census": "tests/golden/sweep_census.json" if fx else "4000 iterations per case (no census)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{n_iter} iterations of each of the 32 cases per step, x the census iterations to converge"},
+            "config": {"workload": "32-case mixed Euler/RANS-SST sweep, grids 96x48..320x160, reference CPU path (f64 C++ restatement "
+                                   "of crates/bowshock-cfd, OpenMP over lines), reference numerics presets",
+                       "cases": len(cases), "oracle_iters": iters, "iters_estimated_for_cases": filled},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 
@@ -186,42 +232,50 @@ def run_ours(args, rank, world, dist):
     cells = np.array([g[0] * g[1] for g in grids], dtype=float)
     arena = Arena(cases, device=device, grids=grids)
     ncell = arena.cells
-    # warm-up (also builds and instantiates the CUDA graph of the step chunk)
-    arena.run(max(args.warmup, 1))
+    # warm-up (also captures and instantiates the CUDA graph of the step chunk)
+    arena.run(max(args.warmup, 3))
     if dist:
         dist.barrier()
     clocks = Clocks(device)
     clocks.start()
-    t0 = time.perf_counter()
     arena.run(args.steps)
-    wall_timed = time.perf_counter() - t0
-    ms_step = arena.ms_per_iter()
-    clk = clocks.stop()
-    ms_local = ms_step
-    # per-kernel profile (CUDA events around every launch) for the roofline of the dominant kernel
-    prof = arena.profile(5)
-    hbm, peak_kind = peaks()
-    # census: every case to its stop rule, through the public API, timed by the wall clock (e2e)
+    ms_local = arena.ms_per_iter()
+    # census: every case to its stop rule, through the public API (wall clock = e2e; device time = value)
     cen_cases = build_cases(rank)
     t1 = time.perf_counter()
     cen_grids = [c.grid() for c in cen_cases]
     cen = Arena(cen_cases, device=device, grids=cen_grids)
     results = cen.solve()
     wall_census = time.perf_counter() - t1
+    clk = clocks.stop()
+    census_dev_s = cen.last_solve_ms() / 1000.0
+    del cen
     iters = [r["iters"] for r in results]
     n_k = np.array(iters, dtype=float)
-    cases_per_s = len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * n_k)))
-    value_rank = 3600.0 * cases_per_s
-    # plain single-case backend: one case per arena, one after another, same iteration counts
-    t_plain = []
+    fx = census_fixture()
+    dcd = {k: results[k]["cd_total"] - fx[k]["cd_total"] for k in range(len(cases)) if k in fx}
+    ok = [k for k, d in dcd.items() if abs(d) <= 1e-4]
+    n_ok = len(ok)
+    value_rank = 3600.0 * n_ok / census_dev_s
+    e2e_rank = 3600.0 * n_ok / wall_census
+    steady = 3600.0 * len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * n_k)))
+    # per-kernel profile (CUDA events around every launch) for the roofline of the dominant kernel group
+    prof = arena.profile(5)
+    del arena
+    hbm, peak_kind = peaks()
+    # plain single-case backend: each case alone, to its stop rule, wall clock
+    t_plain = 0.0
+    plain_ok = 0
     for k, c in enumerate(cases):
-        a1 = Arena([c], device=device, grids=[grids[k]])
-        a1.run(3)
-        a1.run(20)
-        t_plain.append(a1.ms_per_iter() / 1000.0)
-        del a1
-    plain_cases_per_hr = 3600.0 * len(cases) / float(np.sum(np.array(t_plain) * n_k))
-    ms_step, total_value, e2e_value = combine_ranks(dist, ms_local, value_rank, 3600.0 * len(cases) / wall_census)
+        s1 = c.build_solver(device, grid=grids[k])
+        t0 = time.perf_counter()
+        r1 = s1.run_to_stop(c.body, c.numerics, c.wake)
+        t_plain += time.perf_counter() - t0
+        if k in fx and abs(r1["cd_total"] - fx[k]["cd_total"]) <= 1e-4:
+            plain_ok += 1
+        del s1
+    plain_cases_per_hr = 3600.0 * plain_ok / t_plain
+    ms_step, total_value, e2e_value = combine_ranks(dist, ms_local, value_rank, e2e_rank)
     if rank != 0:
         return None
     # roofline of the dominant kernel group
@@ -233,62 +287,85 @@ def run_ours(args, rank, world, dist):
         words = np.where(viscous, SWEEP_WORDS[True], SWEEP_WORDS[False])
         sub = np.array([c.numerics.scheme.sub_iters for c in cases])
         # one launch sweeps every case that has a pass at that position; average over the passes of an iteration
-        passes = sub.max()
-        bytes_iter = float(np.sum(cells * words * 4 * sub)) / passes
+        bytes_iter = float(np.sum(cells * words * 4 * sub)) / sub.max()
     else:
         bytes_iter = float(np.sum(cells * (42 + np.where(viscous, 21, 0)) * 4))  # residual pass: 2 nv + g + v + 1 words
     ms_launch = ms_top / launches_top
     achieved = bytes_iter / (ms_launch / 1000.0) / 1e9
-    fx_traffic = None
+    traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            fx_traffic = json.load(open(tpath)).get(top)
+            traffic = json.load(open(tpath)).get(top)
         except Exception:
-            fx_traffic = None
-    # CPU baseline: the oracle on a bounded sample with the same census iteration counts
-    cpu_val, t_cpu = cpu_sample(cases, grids, 2, iters) if rank == 0 else (None, None)
+            traffic = None
+    # CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
+    smp = OracleSample(cases)
+    for k in range(len(cases)):
+        smp.solvers[k].step()
+    for _ in range(3):
+        for k in range(len(cases)):
+            smp.step(k)
+    o_iters, filled = oracle_iters(fx, cases)
+    cpu_val = smp.cases_per_hr(o_iters)
     stops = {}
     for r in results:
         stops[r["stop_reason"]] = stops.get(r["stop_reason"], 0) + 1
     launches_per_iter = sum(v[1] for v in prof.values()) / 5.0
-    h2d = int(sum(16 * (g[0] + 1) * (g[1] + 1) + 32 * g[0] * g[1] for g in cen_grids))
-    d2h = int(len(cases) * (8 * 50 + 8 * 16))
+    h2d = h2d_bytes(cen_cases, cen_grids)
+    d2h = d2h_bytes(len(cases), iters)
     line = {
         "metric": METRIC, "value": total_value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-        "data": "synthetic (seeded 32-case sweep per GPU, SplitMix64 seed 0x0B05C0C2 + rank)",
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
+        "data": "synthetic (seeded 32-case sweep, SplitMix64 seed 0x0B05C0C2, the same sweep on every GPU)",
         "config": {
             "workload": "32-case mixed Euler/RANS-SST sweep, grids 96x48..320x160, line-implicit, batched arena (one launch per kernel "
-                        "for all cases), CUDA graph per chunk",
+                        "for all cases), CUDA graph per 50-iteration chunk; state FP32 pair, lines FP32, residual/forces/norms FP64",
             "cases": len(cases), "cells": int(ncell), "cell_updates_per_s": float(ncell / (ms_step / 1000.0)),
-            "l2": "working set larger than L2 (no flush needed): ~%.0f MB per iteration" % (ncell * 420 / 1e6),
-            "census_iters_mean": float(n_k.mean()), "census_iters": iters, "census_stop_reasons": stops,
-            "census_wall_s": wall_census, "value_rule": "n * sum(cells) / (t_step * sum(cells * N_k))",
-            "plain_single_case_cases_per_hr": plain_cases_per_hr, "batched_vs_plain": total_value / world / plain_cases_per_hr,
+            "l2": "no flush: the step's working set (~%.0f MB) is larger than the 126 MB L2" % (ncell * 600 / 1e6),
+            "converged_within_1e-4": n_ok, "checked_against_oracle": len(dcd),
+            "dcd": {str(k): float(f"{d:.3e}") for k, d in dcd.items()},
+            "census_device_s": census_dev_s, "census_wall_s": wall_census, "census_iters": iters, "census_stop_reasons": stops,
+            "steady_state_cases_per_hr": steady,
+            "plain_single_case_cases_per_hr": plain_cases_per_hr, "plain_wall_s": t_plain, "plain_converged_within_1e-4": plain_ok,
+            "batched_vs_plain_e2e": e2e_value / world / plain_cases_per_hr if plain_cases_per_hr else None,
             "learned_warm_start": "not built: cold (free-stream) starts",
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "parallelism": f"cases-per-GPU replicas x{world}",
         },
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_iter, "ms_per_launch": ms_launch,
-                     "traffic": fx_traffic},
-        "cpu_baseline": {"value": cpu_val, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                         "sample": "2 iterations of each of the 32 cases (oracle, all host threads) x the census iterations to converge"},
+                     "traffic": traffic},
+        "cpu_baseline": {"value": cpu_val, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "kind": "port",
+                         "sample": "3 oracle iterations of each of the 32 cases (all host threads) x the oracle's iterations to its stop rules"
+                                   + (f" (cases {filled} not in the census fixture: mean of their kind)" if filled else "")},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "what": "wall clock of meshing + arena creation + solve to the stop rules + read-back, through the public API"},
+                "what": "census by the wall clock through the public API: meshing, arena creation (host->device), solve with chunked "
+                        "read-backs (device->host), forces"},
         "clocks": clk,
         "gpu_launches": int(round(launches_per_iter * args.steps)),
     }
     return line
 
 
+def run_kernels(args):
+    """The timed region alone (arena, warm-up, K iterations): the command the ncu captures of the kernels run."""
+    import bowshock_b200  # noqa: F401
+    from bowshock_b200.arena import Arena
+    cases = build_cases(0)
+    arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
+    arena.run(max(args.warmup, 3))
+    arena.run(args.steps)
+    return {"kernels_only": True, "cells": arena.cells, "steps": args.steps, "ms_per_step": arena.ms_per_iter()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--kernels-only", action="store_true", help="only the timed arena iterations (for ncu captures)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -299,7 +376,9 @@ def main():
         import torch.distributed as td
         td.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
         dist = td
-    if args.impl == "reference":
+    if args.kernels_only:
+        line = run_kernels(args)
+    elif args.impl == "reference":
         line = run_reference(args, rank, world)
     else:
         line = run_ours(args, rank, world, dist)

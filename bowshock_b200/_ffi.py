@@ -138,6 +138,7 @@ SIGNATURES = {
     "bowshock_arena_set_state": (_I, [_P, _U, _dp]),
     "bowshock_arena_set_active": (_I, [_P, C.POINTER(C.c_int32)]),
     "bowshock_arena_last_ms_per_iter": (_I, [_P, _dp]),
+    "bowshock_arena_last_solve_ms": (_I, [_P, _dp]),
     "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
 }
 

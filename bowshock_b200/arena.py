@@ -58,6 +58,12 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_last_ms_per_iter(self._h, C.byref(d)))
         return d.value
 
+    def last_solve_ms(self) -> float:
+        """Device time of the last solve() (iterations and force passes, CUDA events), in milliseconds."""
+        d = C.c_double()
+        self._check(_ffi.load().bowshock_arena_last_solve_ms(self._h, C.byref(d)))
+        return d.value
+
     PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage")
 
     def profile(self, n: int):

@@ -79,8 +79,12 @@ class Numerics:
         return Numerics(max_iter=10000 << level, monitor_tol=1e-3 if wake == WAKE_BASE else None)
 
     @staticmethod
-    def transonic():  # numerics.rs:313-329, with the line-implicit scheme in place of SSP-RK3 (same fixed point)
-        return Numerics(limiter=LIM_MINMOD, low_mach=False, first_order_iters=300, max_iter=60000, monitor_tol=2e-4)
+    def transonic():
+        """numerics.rs:313-329 with the line-implicit scheme in place of SSP-RK3 (the same spatial operator, so the same
+        fixed point). The implicit scheme converges the 300-iteration first-order phase by itself, which SSP-RK3 at CFL 0.5
+        never does, so the stop rules are held until the first second-order residual (min_iter = first_order_iters + 1):
+        otherwise a run would stop on the first-order solution."""
+        return Numerics(limiter=LIM_MINMOD, low_mach=False, first_order_iters=300, max_iter=60000, min_iter=301, monitor_tol=2e-4)
 
     @staticmethod
     def auto(mach, level, wake):  # numerics.rs:332-339
@@ -227,8 +231,8 @@ class Case:
         return Config(n.cfl, n.limiter, freestream(self.mach), (BC_CHARACTERISTIC, n.outflow, BC_SLIPWALL, BC_CHARACTERISTIC),
                       n.first_order_iters)
 
-    def build_solver(self, device=0) -> GpuSolver:  # case.rs:147-176
-        ni, nj, x, r, blk = self.grid()
+    def build_solver(self, device=0, grid=None) -> GpuSolver:  # case.rs:147-176
+        ni, nj, x, r, blk = grid if grid is not None else self.grid()
         s = GpuSolver.new(ni, nj, x, r, self.config(), device)
         if blk is not None:
             s.set_block(blk)

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "device_math.cuh"
+
 namespace bk {
 
 enum { SCHEME_EXPLICIT = 0, SCHEME_MULTIGRID = 2, SCHEME_IMPLICIT = 3 };
@@ -47,6 +49,10 @@ struct Arena {
   int* ramp_k;  // per case: CFL-ramp counter (implicit.rs:602-603)
   int* active;  // per case: 1 = iterate, 0 = frozen (converged or stopped)
   float4 *U, *W, *R, *X, *DU, *RR, *U0, *FORCE;
+  // Low words of the state and of the primitives: the state is the unevaluated pair U + Ulo (about 48 significant bits),
+  // so that the FP64 residual, not FP32 rounding of the state, decides the converged state. Everything that only
+  // preconditions (Jacobians, line solves, turbulence, viscous gradients) reads the high words alone.
+  float4 *Ulo, *Wlo, *U0lo;
   float* dt;
   const float4 *iface, *jface, *cellg;
   const float2 *ifc, *jfc;  // face centres (mean of the end nodes)
@@ -80,7 +86,7 @@ struct Arena {
   // FP64-derived stencil of every face: (|d|, e_x, e_r, 0) between the two side positions (viscous.rs:233-250)
   const float4 *ifs, *jfs;
   // FAS multigrid: the restricted state at the start of a coarse cycle, and the user's mask the level masks derive from
-  float4* MG0;
+  float4 *MG0, *MG0lo;
   int* enabled;
 };
 
@@ -107,6 +113,17 @@ __device__ __forceinline__ bool noslip_iface(const CaseDev& c, int i, int j) {
   return c.viscous && c.has_block && i == c.i_end && j >= c.j_sting && j < c.j_end && !(c.has_nozzle && j < c.nz_j_end);
 }
 __device__ __forceinline__ bool jet_iface(const CaseDev& c, int i, int j) { return c.has_block && i == c.i_end && c.has_nozzle && j < c.nz_j_end; }
+
+// a pair (hi, lo) as one double, and a double split into the nearest float and its remainder
+__device__ __forceinline__ V4<double> pair_ld(float4 h, float4 l) {
+  return mk4<double>((double)h.x + (double)l.x, (double)h.y + (double)l.y, (double)h.z + (double)l.z, (double)h.w + (double)l.w);
+}
+__device__ __forceinline__ void pair_st(float4* hi, float4* lo, long long k, const V4<double>& q) {
+  float4 h = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+  hi[k] = h;
+  lo[k] = make_float4((float)(q[0] - (double)h.x), (float)(q[1] - (double)h.y), (float)(q[2] - (double)h.z), (float)(q[3] - (double)h.w));
+}
+__device__ __forceinline__ V4<double> state_of(const Arena& A, long long k) { return pair_ld(A.U[k], A.Ulo[k]); }
 
 __device__ __forceinline__ long long cidx(const CaseDev& c, int i, int j) { return c.cell_off + (long long)j * c.ni + i; }
 __device__ __forceinline__ long long pidx(const CaseDev& c, int i, int j) { return c.pad_off + (long long)(j + 2) * (c.ni + 4) + (i + 2); }

@@ -580,6 +580,7 @@ struct bowshock_arena {
   std::vector<bowshock_case_desc> descs;
   std::vector<int> nseg;
   std::string last_error;
+  double last_solve_ms = 0.0;
 };
 
 static int afail(bowshock_arena* a, int code, const std::string& m) {
@@ -691,7 +692,8 @@ int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bows
   }
   std::function<bool(int, long long, double, double)> cb;
   if (progress) cb = [&](int k, long long it, double r, double mon) { return progress(user, (uint64_t)k, (uint64_t)it, r, mon) == 0; };
-  if ((rc = solve_arena(a->ar, a->fp, runs, cb))) return afrom(a, rc);
+  a->last_solve_ms = 0.0;
+  if ((rc = solve_arena(a->ar, a->fp, runs, cb, &a->last_solve_ms))) return afrom(a, rc);
   std::vector<Forces> f;
   if ((rc = a->fp.run(a->ar, f))) return afrom(a, rc);
   for (int k = 0; k < nc; ++k) fill_point(runs[k], f[k], &results[k]);
@@ -728,6 +730,12 @@ int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active) {
 int bowshock_arena_last_ms_per_iter(const bowshock_arena* a, double* ms) {
   if (!a || !ms) return BOWSHOCK_INVALID;
   *ms = a->ar.last_ms_per_iter;
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms) {
+  if (!a || !ms) return BOWSHOCK_INVALID;
+  *ms = a->last_solve_ms;
   return BOWSHOCK_OK;
 }
 

@@ -30,9 +30,9 @@ enum {
 };
 
 __device__ __forceinline__ double dpress(const Arena& A, const CaseDev& c, int i, int j) {
-  float4 q = A.U[cidx(c, i, j)];
-  double rho = q.x, u = q.y / rho, v = q.z / rho;
-  return 0.4 * ((double)q.w - 0.5 * rho * (u * u + v * v));
+  V4<double> q = state_of(A, cidx(c, i, j));
+  double rho = q[0], u = q[1] / rho, v = q[2] / rho;
+  return 0.4 * (q[3] - 0.5 * rho * (u * u + v * v));
 }
 
 __global__ void k_forces(Arena A, const BodyDev* bodies, const double* nx, const double* nr, const long long* node_off, const double* dxc,
@@ -106,9 +106,9 @@ __global__ void k_forces(Arena A, const BodyDev* bodies, const double* nx, const
         double dx = x1 - x0, dr = r1 - r0, len = hypot(dx, dr);
         double fnx = -dr / len, fnr = dx / len, frm = 0.5 * (r0 + r1);
         long long cc = c.cell_off + (long long)j * ni + i;
-        float4 q = A.U[cc];
-        double rho = q.x, u = q.y / rho, v = q.z / rho;
-        double p = 0.4 * ((double)q.w - 0.5 * rho * (u * u + v * v));
+        V4<double> q = state_of(A, cc);
+        double rho = q[0], u = q[1] / rho, v = q[2] / rho;
+        double p = 0.4 * (q[3] - 0.5 * rho * (u * u + v * v));
         double tx = fnr, tr = -fnx;
         double u_t = u * tx + v * tr;
         double d_n = fabs((dxc[cc] - xm) * fnx + (drc[cc] - frm) * fnr);

@@ -18,10 +18,11 @@
 namespace bk {
 
 __device__ __forceinline__ V4<float> Wat(const Arena& A, const CaseDev& c, int i, int j) { return from_f4(A.W[pidx(c, i, j)]); }
-__device__ __forceinline__ V4<float> prim_of(const Arena& A, const CaseDev& c, int i, int j) { return cons_to_prim(from_f4(A.U[cidx(c, i, j)])); }
+__device__ __forceinline__ V4<double> prim_of(const Arena& A, const CaseDev& c, int i, int j) { return cons_to_prim(state_of(A, cidx(c, i, j))); }
 __device__ __forceinline__ V4<double> fs_of(const CaseDev& c) { return mk4<double>(c.fs[0], c.fs[1], c.fs[2], c.fs[3]); }
 
 // ==================================================================================== primitives + ghosts
+// FP64 from the state pair, stored as the pair (W, Wlo); the ghosts in FP64 as well.
 __global__ void k_prims(Arena A) {
   int b = blockIdx.x;
   int ci = A.pblk_case[b];
@@ -32,7 +33,7 @@ __global__ void k_prims(Arena A) {
   if (p >= pw * (c.nj + 4)) return;
   int i = p % pw - 2, j = p / pw - 2;
   int ni = c.ni, nj = c.nj;
-  V4<float> out;
+  V4<double> out;
   bool in_i = i >= 0 && i < ni, in_j = j >= 0 && j < nj;
   if (in_i && in_j) {
     int j0 = col_start(c, i);
@@ -40,25 +41,21 @@ __global__ void k_prims(Arena A) {
       // block ghost below a body / sting surface (solver.rs:457-471)
       int src = j0 + (j0 - 1 - j);
       float4 f = A.jface[jfidx(c, i, j0)];
-      out = wall_ghost(prim_of(A, c, i, src), f.x, f.y, noslip_jface(c, i, j0));
+      out = wall_ghost<double>(prim_of(A, c, i, src), f.x, f.y, noslip_jface(c, i, j0));
     } else {
       out = prim_of(A, c, i, j);
     }
   } else if (in_j && !in_i) {
-    // i ghosts (solver.rs:429-439), in FP64
+    // i ghosts (solver.rs:429-439)
     V4<double> fs = fs_of(c);
     if (i < 0) {
       int k = -i;
       float4 f = A.iface[ifidx(c, 0, j)];
-      V4<double> edge = cvt4<double>(prim_of(A, c, 0, j)), mir = cvt4<double>(prim_of(A, c, k - 1, j));
-      V4<double> g = ghost_state<double>(c.bc[0], fs, edge, mir, f.x, f.y, -1.0);
-      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+      out = ghost_state<double>(c.bc[0], fs, prim_of(A, c, 0, j), prim_of(A, c, k - 1, j), f.x, f.y, -1.0);
     } else {
       int k = i - ni + 1;
       float4 f = A.iface[ifidx(c, ni, j)];
-      V4<double> edge = cvt4<double>(prim_of(A, c, ni - 1, j)), mir = cvt4<double>(prim_of(A, c, ni - k, j));
-      V4<double> g = ghost_state<double>(c.bc[1], fs, edge, mir, f.x, f.y, 1.0);
-      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+      out = ghost_state<double>(c.bc[1], fs, prim_of(A, c, ni - 1, j), prim_of(A, c, ni - k, j), f.x, f.y, 1.0);
     }
   } else if (in_i && !in_j) {
     // j ghosts (solver.rs:440-451)
@@ -66,24 +63,20 @@ __global__ void k_prims(Arena A) {
     if (j < 0) {
       int k = -j;
       float4 f = A.jface[jfidx(c, i, 0)];
-      V4<double> mir = cvt4<double>(prim_of(A, c, i, k - 1));
-      V4<double> g;
+      V4<double> mir = prim_of(A, c, i, k - 1);
       if (noslip_jface(c, i, 0))
-        g = wall_ghost<double>(mir, f.x, f.y, true);
+        out = wall_ghost<double>(mir, f.x, f.y, true);
       else
-        g = ghost_state<double>(c.bc[2], fs, cvt4<double>(prim_of(A, c, i, 0)), mir, f.x, f.y, -1.0);
-      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+        out = ghost_state<double>(c.bc[2], fs, prim_of(A, c, i, 0), mir, f.x, f.y, -1.0);
     } else {
       int k = j - nj + 1;
       float4 f = A.jface[jfidx(c, i, nj)];
-      V4<double> edge = cvt4<double>(prim_of(A, c, i, nj - 1)), mir = cvt4<double>(prim_of(A, c, i, nj - k));
-      V4<double> g = ghost_state<double>(c.bc[3], fs, edge, mir, f.x, f.y, 1.0);
-      out = mk4<float>((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+      out = ghost_state<double>(c.bc[3], fs, prim_of(A, c, i, nj - 1), prim_of(A, c, i, nj - k), f.x, f.y, 1.0);
     }
   } else {
-    out = mk4<float>((float)c.fs[0], (float)c.fs[1], (float)c.fs[2], (float)c.fs[3]);  // corners: never read
+    out = fs_of(c);  // corners: never read
   }
-  A.W[pidx(c, i, j)] = to_f4(out);
+  pair_st(A.W, A.Wlo, pidx(c, i, j), out);
 }
 
 // ==================================================================================== residual
@@ -128,7 +121,7 @@ __device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(
 
 // dt_kind: 0 = keep dt, 1 = explicit local time step (solver.rs:614-643), 2 = implicit pseudo-time step (implicit.rs:666-695)
 __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int slot) {
-  __shared__ float4 sW[TJ + 4][TI + 4];
+  __shared__ float4 sW[TJ + 4][TI + 4], sWl[TJ + 4][TI + 4];
   __shared__ double4 sFI[TJ][TI + 1];
   __shared__ double4 sFJ[TJ + 1][TI];
   __shared__ double sred[TI * TJ / 32];
@@ -156,16 +149,19 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
   for (int idx = tid; idx < (TJ + 4) * (TI + 4); idx += blockDim.x) {
     int r = idx / (TI + 4), q = idx % (TI + 4);
     int gi = i0 - 2 + q, gj = j0 - 2 + r;
-    sW[r][q] = (gi < ni + 2 && gj < nj + 2) ? A.W[pidx(c, gi, gj)] : make_float4(1.f, 0.f, 0.f, 1.f);
+    bool in = gi < ni + 2 && gj < nj + 2;
+    sW[r][q] = in ? A.W[pidx(c, gi, gj)] : make_float4(1.f, 0.f, 0.f, 1.f);
+    sWl[r][q] = in ? A.Wlo[pidx(c, gi, gj)] : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
+  auto wd = [&](int r, int q) { return pair_ld(sW[r][q], sWl[r][q]); };
   // i faces (TI+1 per row) and j faces (TJ+1 per column), FP64
   for (int idx = tid; idx < TJ * (TI + 1) + (TJ + 1) * TI; idx += blockDim.x) {
     if (idx < TJ * (TI + 1)) {
       int r = idx / (TI + 1), q = idx % (TI + 1);
       int i = i0 + q, j = j0 + r;
       if (i <= ni && j < nj) {
-        V4<double> fl = iface_flux(A, c, i, j, f2d(sW[r + 2][q]), f2d(sW[r + 2][q + 1]), f2d(sW[r + 2][q + 2]), f2d(sW[r + 2][q + 3]), lim,
+        V4<double> fl = iface_flux(A, c, i, j, wd(r + 2, q), wd(r + 2, q + 1), wd(r + 2, q + 2), wd(r + 2, q + 3), lim,
                                    A.iface[ifidx(c, i, j)]);
         sFI[r][q] = to_d4(fl);
       }
@@ -179,7 +175,7 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
           fl = mk4<double>(0, 0, 0, 0);
         } else {
           float4 f = A.jface[jfidx(c, i, j)];
-          fl = face_flux_lm<double>(f2d(sW[r][q + 2]), f2d(sW[r + 1][q + 2]), f2d(sW[r + 2][q + 2]), f2d(sW[r + 3][q + 2]), lim, f.x, f.y,
+          fl = face_flux_lm<double>(wd(r, q + 2), wd(r + 1, q + 2), wd(r + 2, q + 2), wd(r + 3, q + 2), lim, f.x, f.y,
                                     c.low_mach != 0);
         }
         sFJ[r][q] = to_d4(fl);
@@ -210,6 +206,7 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
       float4 g = A.cellg[cc];  // (V, A, xc, rc)
       V4<double> gl = d4(sFI[r][q]), gr = d4(sFI[r][q + 1]), gb = d4(sFJ[r][q]), gt = d4(sFJ[r + 1][q]);
       V4<float> wc = from_f4(sW[r + 2][q + 2]);
+      const V4<double> wcd = wd(r + 2, q + 2);
       const double wl = fl.w, wr = fr.w, wb = fb.w, wt = ft.w, inv_v = 1.0 / (double)g.x;
       V4<double> out;
       float mu_c = 0.f, mut_c = 0.f;
@@ -220,12 +217,12 @@ __global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int s
         for (int k = 0; k < 4; ++k) out[k] = -((gr[k] - hr[k]) * wr - (gl[k] - hl[k]) * wl + (gt[k] - ht[k]) * wt - (gb[k] - hb[k]) * wb) * inv_v;
         mu_c = A.mu[cc];
         mut_c = A.mu_t[cc];
-        double t_tt = hoop_stress((double)mu_c + (double)mut_c, A.grad4[cc], wc[2], g.w);
-        out[2] += ((double)wc[3] - t_tt) * (double)g.y * inv_v;
+        double t_tt = hoop_stress((double)mu_c + (double)mut_c, A.grad4[cc], wcd[2], g.w);
+        out[2] += (wcd[3] - t_tt) * (double)g.y * inv_v;
       } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k) out[k] = -(gr[k] * wr - gl[k] * wl + gt[k] * wt - gb[k] * wb) * inv_v;
-        out[2] += (double)wc[3] * (double)g.y * inv_v;
+        out[2] += wcd[3] * (double)g.y * inv_v;
       }
       if (A.FORCE) {
         float4 fo = A.FORCE[cc];
@@ -281,16 +278,15 @@ __global__ void k_stage(Arena A, float a, float b, int copy, int last) {
   if (last && lt == 0 && threadIdx.x == 0) A.iter[ci] += 1;
   if (i >= c.ni || j >= c.nj || is_solid(c, i, j)) return;
   long long cc = cidx(c, i, j);
-  float4 u = A.U[cc];
-  if (copy) A.U0[cc] = u;
-  float4 u0 = copy ? u : A.U0[cc];
+  float4 uh = A.U[cc], ul = A.Ulo[cc];
+  if (copy) A.U0[cc] = uh, A.U0lo[cc] = ul;
+  V4<double> u = pair_ld(uh, ul), u0 = copy ? u : pair_ld(A.U0[cc], A.U0lo[cc]);
   float4 r = A.R[cc];
-  float d = A.dt[cc];
-  u.x = a * (u.x + d * r.x) + b * u0.x;
-  u.y = a * (u.y + d * r.y) + b * u0.y;
-  u.z = a * (u.z + d * r.z) + b * u0.z;
-  u.w = a * (u.w + d * r.w) + b * u0.w;
-  A.U[cc] = u;
+  double d = A.dt[cc];
+  V4<double> rd = f2d(r);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) u[k] = (double)a * (u[k] + d * rd[k]) + (double)b * u0[k];
+  pair_st(A.U, A.Ulo, cc, u);
 }
 
 // ==================================================================================== implicit operator
@@ -394,19 +390,18 @@ __device__ __forceinline__ void ld_scratch(const float* s, M4<float>& Y, V4<floa
   }
 }
 
-// Positivity-damped update u += alpha du, alpha halved up to 8 times (implicit.rs:641-660).
-__device__ __forceinline__ void damped_update(float4* U, long long cc, const V4<float>& dq) {
-  float4 u4 = U[cc];
-  V4<float> u = from_f4(u4);
-  float alpha = 1.f;
+// Positivity-damped update u += alpha du, alpha halved up to 8 times (implicit.rs:641-660), on the state pair in FP64.
+__device__ __forceinline__ void damped_update(const Arena& A, long long cc, const V4<float>& dq) {
+  V4<double> u = state_of(A, cc);
+  double alpha = 1.0;
   for (int t = 0; t < 8; ++t) {
-    V4<float> q = mk4<float>(u[0] + alpha * dq[0], u[1] + alpha * dq[1], u[2] + alpha * dq[2], u[3] + alpha * dq[3]);
-    V4<float> w = cons_to_prim(q);
-    if (w[0] > 0.f && w[3] > 0.f && isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]) && isfinite(q[3])) {
-      U[cc] = to_f4(q);
+    V4<double> q = mk4<double>(u[0] + alpha * dq[0], u[1] + alpha * dq[1], u[2] + alpha * dq[2], u[3] + alpha * dq[3]);
+    V4<double> w = cons_to_prim(q);
+    if (w[0] > 0.0 && w[3] > 0.0 && isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]) && isfinite(q[3])) {
+      pair_st(A.U, A.Ulo, cc, q);
       return;
     }
-    alpha *= 0.5f;
+    alpha *= 0.5;
   }
 }
 
@@ -624,7 +619,7 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
       for (int q = 0; q < 4; ++q) du[q] += o[q];
     }
     A.DU[cc] = to_f4(du);
-    if (update) damped_update(A.U, cc, du);
+    if (update) damped_update(A, cc, du);
   };
   if (has_sep) emit(cell(e - 1), lsep);
   for (int k = ke; k >= a; --k) {

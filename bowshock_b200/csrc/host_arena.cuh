@@ -262,7 +262,7 @@ struct ArenaHost {
     if (ev1) cudaEventDestroy(ev1), ev1 = nullptr;
     if (pe0) cudaEventDestroy(pe0), pe0 = nullptr;
     if (pe1) cudaEventDestroy(pe1), pe1 = nullptr;
-    void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0,
+    void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0, A.Ulo, A.Wlo, A.U0lo, A.MG0lo,
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
                     A.grad4, A.gradT, A.mu, A.mu_t, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
                     A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled};
@@ -376,6 +376,10 @@ struct ArenaHost {
     ALLOC(A.DU, ncell);
     ALLOC(A.RR, ncell);
     ALLOC(A.U0, ncell);
+    ALLOC(A.Ulo, ncell);
+    ALLOC(A.Wlo, npad);
+    ALLOC(A.U0lo, ncell);
+    BK_CUDA(cudaMemset(A.Ulo, 0, ncell * sizeof(float4)));
     ALLOC(A.dt, ncell);
     float4 *fi, *fj, *cg;
     float2 *ic, *jc;
@@ -396,6 +400,7 @@ struct ArenaHost {
     A.enabled = d_enabled;
     if (mg_levels > 1) {
       ALLOC(A.MG0, ncell);
+      ALLOC(A.MG0lo, ncell);
       ALLOC(A.FORCE, ncell);
       BK_CUDA(cudaMemset(A.FORCE, 0, ncell * sizeof(float4)));
     }
@@ -577,9 +582,15 @@ struct ArenaHost {
   int set_state(int k, const double* u) {
     const CaseDev& c = desc[k];
     size_t n = (size_t)c.ni * c.nj;
-    std::vector<float4> h(n);
-    for (size_t i = 0; i < n; ++i) h[i] = make_float4((float)u[4 * i], (float)u[4 * i + 1], (float)u[4 * i + 2], (float)u[4 * i + 3]);
+    std::vector<float4> h(n), l(n);
+    for (size_t i = 0; i < n; ++i) {
+      const double* q = u + 4 * i;
+      h[i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+      l[i] = make_float4((float)(q[0] - (double)h[i].x), (float)(q[1] - (double)h[i].y), (float)(q[2] - (double)h[i].z),
+                         (float)(q[3] - (double)h[i].w));
+    }
     BK_CUDA(cudaMemcpy(A.U + c.cell_off, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(A.Ulo + c.cell_off, l.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
     int z = 0;
     BK_CUDA(cudaMemcpy(d_iter + k, &z, sizeof(int), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(d_ramp + k, &z, sizeof(int), cudaMemcpyHostToDevice));
@@ -589,14 +600,15 @@ struct ArenaHost {
   int get_state(int k, double* u) {
     const CaseDev& c = desc[k];
     size_t n = (size_t)c.ni * c.nj;
-    std::vector<float4> h(n);
+    std::vector<float4> h(n), l(n);
     BK_CUDA(cudaStreamSynchronize(stream));
     BK_CUDA(cudaMemcpy(h.data(), A.U + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    BK_CUDA(cudaMemcpy(l.data(), A.Ulo + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) {
-      u[4 * i] = h[i].x;
-      u[4 * i + 1] = h[i].y;
-      u[4 * i + 2] = h[i].z;
-      u[4 * i + 3] = h[i].w;
+      u[4 * i] = (double)h[i].x + (double)l[i].x;
+      u[4 * i + 1] = (double)h[i].y + (double)l[i].y;
+      u[4 * i + 2] = (double)h[i].z + (double)l[i].z;
+      u[4 * i + 3] = (double)h[i].w + (double)l[i].w;
     }
     return 0;
   }

@@ -34,13 +34,14 @@ __global__ void k_restrict_state(Arena A, int level) {
     if (is_solid(f, fi, fj)) continue;
     long long fc = cidx(f, fi, fj);
     double vol = A.cellg[fc].x;
-    float4 u = A.U[fc];
-    s[0] += vol * u.x, s[1] += vol * u.y, s[2] += vol * u.z, s[3] += vol * u.w;
+    V4<double> u = state_of(A, fc);
+    s[0] += vol * u[0], s[1] += vol * u[1], s[2] += vol * u[2], s[3] += vol * u[3];
     v += vol;
   }
   long long cc = cidx(c, i, j);
-  if (v > 0.0) A.U[cc] = make_float4((float)(s[0] / v), (float)(s[1] / v), (float)(s[2] / v), (float)(s[3] / v));
+  if (v > 0.0) pair_st(A.U, A.Ulo, cc, mk4<double>(s[0] / v, s[1] / v, s[2] / v, s[3] / v));
   A.MG0[cc] = A.U[cc];
+  A.MG0lo[cc] = A.Ulo[cc];
   A.FORCE[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -84,27 +85,27 @@ __global__ void k_prolong(Arena A, int level) {
   int ci2 = (i % 2 == 0) ? (ci > 0 ? ci - 1 : 0) : min(ci + 1, c.ni - 1);
   int cj2 = (j % 2 == 0) ? (cj > 0 ? cj - 1 : 0) : min(cj + 1, c.nj - 1);
   const int ca[4] = {ci, ci2, ci, ci2}, cb[4] = {cj, cj, cj2, cj2};
-  const float wt[4] = {9.f, 3.f, 3.f, 1.f};
-  float d[4] = {0, 0, 0, 0}, wsum = 0.f;
+  const double wt[4] = {9.0, 3.0, 3.0, 1.0};
+  double d[4] = {0, 0, 0, 0}, wsum = 0.0;
   for (int q = 0; q < 4; ++q) {
     if (is_solid(c, ca[q], cb[q])) continue;
     long long cc = cidx(c, ca[q], cb[q]);
-    float4 u = A.U[cc], u0 = A.MG0[cc];
-    d[0] += wt[q] * (u.x - u0.x), d[1] += wt[q] * (u.y - u0.y), d[2] += wt[q] * (u.z - u0.z), d[3] += wt[q] * (u.w - u0.w);
+    V4<double> u = state_of(A, cc), u0 = pair_ld(A.MG0[cc], A.MG0lo[cc]);
+    for (int k = 0; k < 4; ++k) d[k] += wt[q] * (u[k] - u0[k]);
     wsum += wt[q];
   }
   for (int q = 0; q < 4; ++q) d[q] /= wsum;
   long long fc = cidx(f, i, j);
-  float4 u = A.U[fc];
-  float alpha = 1.f;
+  V4<double> u = state_of(A, fc);
+  double alpha = 1.0;
   for (int it = 0; it < 6; ++it) {
-    V4<float> q = mk4<float>(u.x + alpha * d[0], u.y + alpha * d[1], u.z + alpha * d[2], u.w + alpha * d[3]);
-    V4<float> w = cons_to_prim(q);
-    if (w[0] > 0.f && w[3] > 0.f) {
-      A.U[fc] = to_f4(q);
+    V4<double> q = mk4<double>(u[0] + alpha * d[0], u[1] + alpha * d[1], u[2] + alpha * d[2], u[3] + alpha * d[3]);
+    V4<double> w = cons_to_prim(q);
+    if (w[0] > 0.0 && w[3] > 0.0) {
+      pair_st(A.U, A.Ulo, fc, q);
       return;
     }
-    alpha *= 0.5f;
+    alpha *= 0.5;
   }
 }
 

@@ -116,9 +116,13 @@ struct ForcePass {
   BodyDev* bodies = nullptr;
   std::vector<BodyDev> hb;
   int nc = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double last_ms = 0.0;  // device time of the last pass (kernel + read-back)
   ~ForcePass() {
     for (void* p : {(void*)nx, (void*)nr, (void*)xc, (void*)rc, (void*)out, (void*)node_off, (void*)bodies})
       if (p) cudaFree(p);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
   }
   int setup(ArenaHost& ar) {
     std::string& err = ar.err;
@@ -162,11 +166,20 @@ struct ForcePass {
   }
   int run(ArenaHost& ar, std::vector<Forces>& res) {
     std::string& err = ar.err;
+    if (!e0) {
+      BK_CUDA(cudaEventCreate(&e0));
+      BK_CUDA(cudaEventCreate(&e1));
+    }
+    BK_CUDA(cudaEventRecord(e0, ar.stream));
     k_forces<<<nc, 256, 0, ar.stream>>>(ar.A, bodies, nx, nr, node_off, xc, rc, out);
     BK_CUDA(cudaGetLastError());
     std::vector<double> h((size_t)nc * F_NF);
     BK_CUDA(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ar.stream));
+    BK_CUDA(cudaEventRecord(e1, ar.stream));
     BK_CUDA(cudaStreamSynchronize(ar.stream));
+    float ms = 0.f;
+    BK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    last_ms = ms;
     res.resize(nc);
     for (int k = 0; k < nc; ++k) std::memcpy(res[k].f, &h[(size_t)k * F_NF], F_NF * sizeof(double));
     return 0;
@@ -210,8 +223,10 @@ inline int start_case(ArenaHost& ar, int k, const RunParams& p, long long first_
 }
 
 // Iterate every active case of the arena to its stop rule in chunks of SYNC iterations.
+// `device_ms` (optional) receives the device time of the iterations and force passes (CUDA events around each).
 inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
-                       const std::function<bool(int, long long, double, double)>& progress) {
+                       const std::function<bool(int, long long, double, double)>& progress, double* device_ms = nullptr) {
+  double dev_ms = 0.0;
   const int nc = (int)ar.cases.size();
   std::vector<int> act(nc);
   for (int k = 0; k < nc; ++k) act[k] = runs[k].done ? 0 : 1;
@@ -225,6 +240,8 @@ inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
     if (!left) break;
     if ((rc = ar.run(SYNC, res.data()))) return rc;
     if ((rc = fp.run(ar, f))) return rc;
+    dev_ms += ar.last_ms_per_iter * SYNC + fp.last_ms;
+    if (device_ms) *device_ms = dev_ms;
     bool mask_changed = false;
     for (int k = 0; k < nc; ++k) {
       CaseRun& cr = runs[k];

@@ -89,6 +89,7 @@ def make_case(p) -> Case:
             g.n_wake -= 1
         gap = max(4, _even_round(nj * g.n_gap / (g.n_gap + g.nj_out)))
         g.n_gap, g.nj_out = gap, nj - gap
+        c.viscous.wall_i_start = g.n_up  # the no-slip wall starts at the nose tip (case.rs:96-97)
     else:
         c = Case.new(p["mach"], body, 0, WAKE_STING, Numerics.auto(p["mach"], 0, WAKE_STING))
         g = c.grid_sting

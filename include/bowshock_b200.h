@@ -281,6 +281,9 @@ int bowshock_arena_set_state(bowshock_arena* a, uint64_t k, const double* u);
 int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active);
 /* mean device time of one arena iteration over the last bowshock_arena_run, in milliseconds (CUDA events) */
 int bowshock_arena_last_ms_per_iter(const bowshock_arena* a, double* ms);
+/* device time of the last bowshock_arena_solve in milliseconds: every iteration chunk and FP64 force pass, CUDA events
+ * around each (host-side stop-rule checks between chunks excluded) */
+int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
 
 /* Per-kernel profile (the reference's Profile of gpu/mod.rs:533-542): n iterations launched one kernel at a time with CUDA
  * events around each launch; per kernel group (prims, viscous, residual, i-lines, j-lines, defect, turbulence, stage) the
