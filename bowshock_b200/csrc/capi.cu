@@ -2,6 +2,7 @@
 // backed by a case arena of one. Unity build: the kernels and the host arena are compiled into this translation unit.
 #include <cstdio>
 #include <exception>
+#include <mutex>
 
 #include "../../include/bowshock_b200.h"
 #include "fv_kernels.cu"
@@ -755,4 +756,87 @@ extern "C" int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms,
 extern "C" int bowshock_solver_set_ramp(bowshock_solver* s, uint64_t ramp_k) {
   if (!s) return BOWSHOCK_INVALID;
   return from_arena(s, s->ar.set_counter(s->ar.d_ramp, 0, (int)std::min<uint64_t>(ramp_k, 1u << 30)));
+}
+
+// ============================================================================ allocation-free iteration
+// bowshock_solver_run_noalloc: the iterations of bowshock_solver_run without a single device allocation. Who needs it:
+// a host that sets its solvers up once and then steps them from code that must not allocate device memory, because the
+// free memory of the GPU already belongs to that host's own pool (another framework's caching allocator sharing the
+// device) or because the step runs in a loop that cannot take the device-wide synchronisation an allocation can bring.
+// bowshock_solver_run allocates on its first call (it instantiates a CUDA graph of the iteration chunk and creates timing
+// events); this variant launches the same kernels directly on the solver's stream, and the spike storage of its line
+// solves (k_lines, 36 floats per cell) comes from the static array below instead of the solver's own buffer.
+//
+// The array: BOWSHOCK_NOALLOC_SCRATCH_BYTES (16 MiB) in this file's device module, so every GPU that loads the library
+// holds it until the process exits. Host code cannot use its name as a device address: the address is looked up once per
+// device, with that device current, by the first call on that device (cudaGetSymbolAddress). Every call on a device
+// shares the array and it keeps the last call's contents; nothing in it has to start at zero (each line solve writes every
+// spike entry before it reads it). Calls whose kernels overlap on one GPU (solvers on different streams or host threads)
+// race on the array and corrupt each other: the caller must serialise them.
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) float g_noalloc_scratch[BOWSHOCK_NOALLOC_SCRATCH_BYTES / sizeof(float)];
+float* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+cudaError_t g_noalloc_err[NOALLOC_MAX_DEVICES];
+std::once_flag g_noalloc_once[NOALLOC_MAX_DEVICES];
+
+void noalloc_setup(int device) {
+  int prev = -1;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e == cudaSuccess && prev != device) e = cudaSetDevice(device);
+  void* p = nullptr;
+  if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (prev >= 0 && prev != device) cudaSetDevice(prev);
+  g_noalloc_err[device] = e;
+  g_noalloc_ptr[device] = e == cudaSuccess ? static_cast<float*>(p) : nullptr;
+}
+
+// n iterations of the solver's arena with `scratch` as the line solves' spike storage; errors in ar.err
+int noalloc_iterate(ArenaHost& ar, float* scratch, uint64_t n, double* residual) {
+  std::string& err = ar.err;
+  BK_CUDA(cudaSetDevice(ar.device));
+  const int nc = (int)ar.cases.size();  // > 1 with a multigrid hierarchy: the fine level is case 0
+  const double n_active = (double)ar.desc[0].n_active;
+  uint64_t done = 0;
+  while (done < n) {
+    const int chunk = (int)std::min<uint64_t>(n - done, (uint64_t)ar.slots);
+    BK_CUDA(cudaMemsetAsync(ar.A.rsum, 0, (size_t)chunk * nc * sizeof(double), ar.stream));
+    if (ar.any_sst) BK_CUDA(cudaMemsetAsync(ar.A.tsum, 0, (size_t)chunk * nc * sizeof(double), ar.stream));
+    float* own = ar.A.scratch;
+    ar.A.scratch = scratch;  // the kernels take the arena by value at launch
+    for (int k = 0; k < chunk; ++k) ar.launch_iteration(k);
+    ar.A.scratch = own;
+    BK_CUDA(cudaGetLastError());
+    if (residual)  // case 0's column of the [slot][case] sums of R_rho^2
+      BK_CUDA(cudaMemcpy2DAsync(residual + done, sizeof(double), ar.A.rsum, (size_t)nc * sizeof(double), sizeof(double), chunk,
+                                cudaMemcpyDeviceToHost, ar.stream));
+    BK_CUDA(cudaStreamSynchronize(ar.stream));
+    if (residual)
+      for (int k = 0; k < chunk; ++k) residual[done + k] = std::sqrt(residual[done + k] / n_active);
+    done += chunk;
+  }
+  return 0;
+}
+}  // namespace
+
+extern "C" int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, double* residual) {
+  if (!s) return BOWSHOCK_INVALID;
+  ArenaHost& ar = s->ar;
+  const int dev = ar.device;
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(s, BOWSHOCK_INVALID, "device index out of range for the static scratch");
+  const uint64_t need = (uint64_t)ar.ncell * 36u * sizeof(float);
+  if (need > (uint64_t)BOWSHOCK_NOALLOC_SCRATCH_BYTES)
+    return fail(s, BOWSHOCK_INVALID,
+                "the solver's " + std::to_string((long long)ar.ncell) + " cells need " + std::to_string(need) +
+                    " bytes of line-solve scratch, more than the static maximum of " + std::to_string(BOWSHOCK_NOALLOC_SCRATCH_BYTES) +
+                    " bytes (" + std::to_string(BOWSHOCK_NOALLOC_MAX_CELLS) + " cells)");
+  std::call_once(g_noalloc_once[dev], noalloc_setup, dev);
+  if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev])
+    return fail(s, BOWSHOCK_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(g_noalloc_err[dev]));
+  int rc = noalloc_iterate(ar, g_noalloc_ptr[dev], n, residual);
+  if (rc) return from_arena(s, rc);
+  if (residual)
+    for (uint64_t k = 0; k < n; ++k)
+      if (!std::isfinite(residual[k])) return fail(s, BOWSHOCK_NONFINITE, "non-finite residual at iteration " + std::to_string(k));
+  return BOWSHOCK_OK;
 }

@@ -216,6 +216,14 @@ class GpuSolver:
         self._check(_ffi.load().bowshock_solver_run(self._h, int(n), _dp(out)))
         return out
 
+    def run_noalloc(self, n: int) -> np.ndarray:
+        """`run` without device allocation (bowshock_solver_run_noalloc): for stepping from code that may not allocate
+        device memory once the solver exists. The line solves use the library's static 16 MiB scratch array, shared by
+        all calls on the device, so calls overlapping on one GPU must be serialised."""
+        out = np.zeros(n)
+        self._check(_ffi.load().bowshock_solver_run_noalloc(self._h, int(n), _dp(out)))
+        return out
+
     def eval_residual(self, compute_dt: bool = True):
         """`Solver::eval_residual` + `density_residual` of the current state: (res (n,4), dt (n), density residual)."""
         res = np.zeros(4 * self.ni * self.nj)
