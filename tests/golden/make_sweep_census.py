@@ -1,7 +1,7 @@
 """Regenerates tests/golden/sweep_census.json: the oracle's run of every case of the seeded 32-case sweep to the
 reference's stop rule (run.rs:44-170), with its converged CD components, iteration count and wall time.
 
-Usage: python tests/golden/make_sweep_census.py [case indices...]   (default: all 32, cheapest first)
+Usage: python tests/golden/make_sweep_census.py [case indices...]   (default: the cases not yet in the JSON, cheapest first)
 Results are merged into the existing JSON after each case, so an interrupted run keeps what finished. The oracle's
 OpenMP thread count (OMP_NUM_THREADS) is recorded beside each time. Several hours of CPU time for all 32 cases."""
 import json
@@ -24,8 +24,10 @@ OUT = os.path.join(HERE, "sweep_census.json")
 
 def main():
     cases = sweep_cases()
-    idx = [int(a) for a in sys.argv[1:]] or sorted(range(len(cases)), key=lambda k: (cases[k].viscous is not None, np.prod(cases[k].cells())))
     data = json.load(open(OUT)) if os.path.exists(OUT) else dict(made_by="tests/golden/make_sweep_census.py", cases={})
+    # explicit indices are (re)run; by default the cases not yet in the JSON, cheapest first
+    idx = [int(a) for a in sys.argv[1:]] or sorted((k for k in range(len(cases)) if str(k) not in data["cases"]),
+                                                   key=lambda k: (cases[k].viscous is not None, np.prod(cases[k].cells())))
     for k in idx:
         c = cases[k]
         oc = oracle_case(c)
