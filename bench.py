@@ -356,7 +356,9 @@ def run_kernels(args):
     arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
     arena.run(max(args.warmup, 3))
     arena.run(args.steps)
-    return {"kernels_only": True, "cells": arena.cells, "steps": args.steps, "ms_per_step": arena.ms_per_iter()}
+    ms = arena.ms_per_iter()
+    prof = {g: round(v[0] / v[1], 4) for g, v in arena.profile(3).items() if v[1]} if args.steps >= 10 else None
+    return {"kernels_only": True, "cells": arena.cells, "steps": args.steps, "ms_per_step": ms, "ms_per_launch": prof}
 
 
 def main():

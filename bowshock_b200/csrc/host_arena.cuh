@@ -243,6 +243,7 @@ struct ArenaHost {
   std::vector<CaseDev> desc;
   long long ncell = 0, npad = 0, nif = 0, njf = 0;
   int ntiles = 0, nil = 0, njl = 0, npblk = 0;
+  int max_line = 0;  // longest i or j line of any case
   bool any_viscous = false, any_sst = false;
   // device buffers
   Arena A{};
@@ -329,6 +330,7 @@ struct ArenaHost {
     desc.resize(nc);
     ncell = npad = nif = njf = 0;
     ntiles = nil = njl = npblk = 0;
+    max_line = 0;
     std::vector<int> tile_case, iline, jline, pblk;
     for (int k = 0; k < nc; ++k) {
       HostCase& h = cases[k];
@@ -351,6 +353,7 @@ struct ArenaHost {
       ntiles += nt;
       nil += h.nj;
       njl += h.ni;
+      max_line = std::max(max_line, std::max(h.ni, h.nj));
       npblk += nb;
       ncell += (long long)h.ni * h.nj;
       npad += (long long)(h.ni + 4) * (h.nj + 4);
@@ -729,8 +732,13 @@ struct ArenaHost {
         L(G_TURB, [&] { k_turb_grad<<<ntiles, TI * TJ, 0, stream>>>(A); });
         L(G_TURB, [&] { k_turb_blend<<<ntiles, TI * TJ, 0, stream>>>(A); });
         L(G_TURB, [&] { k_turb_cell<<<ntiles, TI * TJ, 0, stream>>>(A, slot); });
-        L(G_TURB, [&] { k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1); });
-        L(G_TURB, [&] { k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0); });
+        if (max_line <= 32 * TL_MAXM) {
+          L(G_TURB, [&] { k_turb_lines_w<<<(nil + TL_WARPS - 1) / TL_WARPS, 32 * TL_WARPS, 0, stream>>>(A, 1); });
+          L(G_TURB, [&] { k_turb_lines_w<<<(njl + TL_WARPS - 1) / TL_WARPS, 32 * TL_WARPS, 0, stream>>>(A, 0); });
+        } else {
+          L(G_TURB, [&] { k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1); });
+          L(G_TURB, [&] { k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0); });
+        }
         L(G_TURB, [&] { k_turb_update<<<ntiles, TI * TJ, 0, stream>>>(A); });
       }
     } else {

@@ -4,7 +4,8 @@
 //   k_turb_blend  F1 and the cross-diffusion X (turbulence.rs:375-397)
 //   k_turb_cell   face convection / diffusion data of the four faces (turbulence.rs:413-435) and the cell terms: residual,
 //                 diag0 and the coefficients of the i- and j-line systems (turbulence.rs:477-519, 559-579)
-//   k_turb_lines  the two scalar tridiagonal line systems, i then j, one thread per (line, scalar) (turbulence.rs:580-581)
+//   k_turb_lines  the two scalar tridiagonal line systems, i then j, one thread per (line, scalar) (turbulence.rs:580-581);
+//                 k_turb_lines_w the same with one warp per line (partitioned Thomas), used for lines up to 512 cells
 //   k_turb_update clipped update and the new eddy viscosity (turbulence.rs:584-603)
 // Host helpers: the turbulence initialisation (free stream, wall distance in FP64, mu_t; turbulence.rs:128-138).
 #pragma once
@@ -307,6 +308,141 @@ __global__ void k_turb_lines(Arena A, int dir_i) {
       A.trhs[cc].y = v;
     else
       A.trhs[cc].x = v;
+  }
+}
+
+// The same two scalar line systems, one warp per line and both scalars per lane (partitioned Thomas): lane s eliminates
+// its segment of m = max(2, ceil(len/32)) cells (m <= TL_MAXM, so the spikes stay in registers), expressing every interior
+// unknown through the separators on either side (the last cell of each segment but the last); the separator rows form a
+// tridiagonal system solved by parallel cyclic reduction with warp shuffles; each lane then back-substitutes its segment.
+// Coefficient reads per cell are the same as the thread-per-line kernel's, but 32 lanes share a line, so the grid has
+// 32x the threads and every read is used once.
+constexpr int TL_WARPS = 4, TL_MAXM = 16;  // lines of up to 32 * TL_MAXM = 512 cells
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 f2rcp(float2 a) { return make_float2(1.f / a.x, 1.f / a.y); }
+__device__ __forceinline__ float2 shfl_up2(float2 v, int h) {
+  return make_float2(__shfl_up_sync(0xffffffffu, v.x, h), __shfl_up_sync(0xffffffffu, v.y, h));
+}
+__device__ __forceinline__ float2 shfl_down2(float2 v, int h) {
+  return make_float2(__shfl_down_sync(0xffffffffu, v.x, h), __shfl_down_sync(0xffffffffu, v.y, h));
+}
+
+__global__ void __launch_bounds__(32 * TL_WARPS) k_turb_lines_w(Arena A, int dir_i) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int line = blockIdx.x * TL_WARPS + warp;
+  const int nl = dir_i ? A.nilines : A.njlines;
+  if (line >= nl) return;  // uniform per warp
+  const int ci = dir_i ? A.iline_case[line] : A.jline_case[line];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  const int L = line - (dir_i ? c.iline_off : c.jline_off);
+  const int n = dir_i ? c.ni : c.nj;
+  const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
+  const int len = n - k0;
+  if (len <= 0) return;
+  int m = (len + 31) / 32;
+  if (m < 2) m = 2;
+  const int P = (len + m - 1) / m, N = P - 1;
+  const int s = lane;
+  const bool act = s < P;
+  const int a = k0 + s * m;
+  const int e = act ? min(a + m, n) : a;
+  const bool has_sep = act && s < N;
+  const int cnt = act ? (has_sep ? e - 1 - a : e - a) : 0;  // interior cells of the segment
+  auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
+  auto coef = [&](long long cc, float2& lo, float2& d, float2& up) {
+    if (dir_i) {
+      float4 t0 = A.tcoef[3 * cc], t1 = A.tcoef[3 * cc + 1];
+      lo = make_float2(t0.x, t0.y), up = make_float2(t0.z, t0.w), d = make_float2(t1.x, t1.y);
+    } else {
+      float4 t1 = A.tcoef[3 * cc + 1], t2 = A.tcoef[3 * cc + 2];
+      lo = make_float2(t1.z, t1.w), up = make_float2(t2.x, t2.y), d = make_float2(t2.z, t2.w);
+    }
+  };
+  float2 Y[TL_MAXM], G[TL_MAXM], GE[TL_MAXM];
+  const float2 z2 = make_float2(0.f, 0.f);
+  float2 yl = z2, gl = z2, gel = z2;
+#pragma unroll
+  for (int t = 0; t < TL_MAXM; ++t) {
+    if (t < cnt) {
+      long long cc = cell(a + t);
+      float2 lo, d, up;
+      coef(cc, lo, d, up);
+      float2 r = A.trhs[cc];
+      float2 M = d, GEr = f2neg(lo);
+      if (t > 0) {
+        M = f2sub(M, f2mul(lo, yl));
+        r = f2sub(r, f2mul(lo, gl));
+        GEr = f2neg(f2mul(lo, gel));
+      }
+      float2 inv = f2rcp(M);
+      gl = f2mul(inv, r);
+      gel = f2mul(inv, GEr);
+      yl = f2mul(inv, up);
+      Y[t] = yl, G[t] = gl, GE[t] = gel;
+    }
+  }
+  // x at the last interior cell = v_l + E_l l_{s-1} + F_l l_s; at the first, by the backward recurrence, v_f + E_f .. + F_f ..
+  const float2 v_l = gl, E_l = gel, F_l = f2neg(yl);
+  float2 v_f = v_l, E_f = E_l, F_f = F_l;
+#pragma unroll
+  for (int t = TL_MAXM - 2; t >= 0; --t) {
+    if (t < cnt - 1) {
+      v_f = f2sub(G[t], f2mul(Y[t], v_f));
+      E_f = f2sub(GE[t], f2mul(Y[t], E_f));
+      F_f = f2neg(f2mul(Y[t], F_f));
+    }
+  }
+  const float2 v_n = shfl_down2(v_f, 1), E_n = shfl_down2(E_f, 1), F_n = shfl_down2(F_f, 1);
+  // separator row: lo x_{last interior} + d x_sep + up x_{first of the next segment}
+  float2 ra = z2, rb = make_float2(1.f, 1.f), rc = z2, rd = z2;
+  if (has_sep) {
+    long long cs = cell(e - 1);
+    float2 lo, d, up;
+    coef(cs, lo, d, up);
+    float2 r = A.trhs[cs];
+    ra = f2mul(lo, E_l);
+    rb = f2add(f2add(d, f2mul(lo, F_l)), f2mul(up, E_n));
+    rc = f2mul(up, F_n);
+    rd = f2sub(f2sub(r, f2mul(lo, v_l)), f2mul(up, v_n));
+  }
+  // parallel cyclic reduction of the N separator rows
+  for (int h = 1; h < N; h <<= 1) {
+    float2 am = shfl_up2(ra, h), bm = shfl_up2(rb, h), cm = shfl_up2(rc, h), dm = shfl_up2(rd, h);
+    float2 ap = shfl_down2(ra, h), bp = shfl_down2(rb, h), cp = shfl_down2(rc, h), dp = shfl_down2(rd, h);
+    if (s < N) {
+      float2 na = z2, nc = z2, nb = rb, nd = rd;
+      if (s - h >= 0) {
+        float2 al = f2neg(f2mul(ra, f2rcp(bm)));
+        na = f2mul(al, am);
+        nb = f2add(nb, f2mul(al, cm));
+        nd = f2add(nd, f2mul(al, dm));
+      }
+      if (s + h < N) {
+        float2 ga = f2neg(f2mul(rc, f2rcp(bp)));
+        nc = f2mul(ga, cp);
+        nb = f2add(nb, f2mul(ga, ap));
+        nd = f2add(nd, f2mul(ga, dp));
+      }
+      ra = na, rb = nb, rc = nc, rd = nd;
+    }
+  }
+  const float2 lsep = s < N ? f2mul(rd, f2rcp(rb)) : z2;
+  float2 lprev = shfl_up2(lsep, 1);
+  if (s == 0) lprev = z2;
+  if (!act) return;
+  if (has_sep) A.trhs[cell(e - 1)] = lsep;
+  float2 xn = has_sep ? lsep : z2;
+#pragma unroll
+  for (int t = TL_MAXM - 1; t >= 0; --t) {
+    if (t < cnt) {
+      float2 x = f2sub(f2add(G[t], f2mul(GE[t], lprev)), f2mul(Y[t], xn));
+      A.trhs[cell(a + t)] = x;
+      xn = x;
+    }
   }
 }
 
