@@ -56,7 +56,8 @@ struct Arena {
   float* dt;
   const float4 *iface, *jface, *cellg;
   const float2 *ifc, *jfc;  // face centres (mean of the end nodes)
-  float* scratch;  // line solves: 36 floats per cell
+  float* scratch;  // line-solve records (fv_kernels.cu: line_rec, pcr_rec)
+  long long ncell;
   double* rsum;    // sum of R_rho^2, [slot * ncases + case]
   const int* tile_case;
   int ntiles;

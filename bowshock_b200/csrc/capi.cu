@@ -765,13 +765,14 @@ extern "C" int bowshock_solver_set_ramp(bowshock_solver* s, uint64_t ramp_k) {
 // device) or because the step runs in a loop that cannot take the device-wide synchronisation an allocation can bring.
 // bowshock_solver_run allocates on its first call (it instantiates a CUDA graph of the iteration chunk and creates timing
 // events); this variant launches the same kernels directly on the solver's stream, and the spike storage of its line
-// solves (k_lines, 36 floats per cell) comes from the static array below instead of the solver's own buffer.
+// solves (the records of k_lines / k_lines_subst / k_defect: blocks, factors and reduction multipliers) comes from the
+// static array below instead of the solver's own buffer.
 //
-// The array: BOWSHOCK_NOALLOC_SCRATCH_BYTES (16 MiB) in this file's device module, so every GPU that loads the library
+// The array: BOWSHOCK_NOALLOC_SCRATCH_BYTES (64 MiB) in this file's device module, so every GPU that loads the library
 // holds it until the process exits. Host code cannot use its name as a device address: the address is looked up once per
 // device, with that device current, by the first call on that device (cudaGetSymbolAddress). Every call on a device
-// shares the array and it keeps the last call's contents; nothing in it has to start at zero (each line solve writes every
-// spike entry before it reads it). Calls whose kernels overlap on one GPU (solvers on different streams or host threads)
+// shares the array and it keeps the last call's contents; nothing in it has to start at zero (the first line pass of
+// every iteration writes every record entry before any kernel reads it). Calls whose kernels overlap on one GPU (solvers on different streams or host threads)
 // race on the array and corrupt each other: the caller must serialise them.
 namespace {
 constexpr int NOALLOC_MAX_DEVICES = 64;
@@ -824,12 +825,12 @@ extern "C" int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, doubl
   ArenaHost& ar = s->ar;
   const int dev = ar.device;
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(s, BOWSHOCK_INVALID, "device index out of range for the static scratch");
-  const uint64_t need = (uint64_t)ar.ncell * 36u * sizeof(float);
+  const uint64_t need = (uint64_t)ar.scratch_floats() * sizeof(float);
   if (need > (uint64_t)BOWSHOCK_NOALLOC_SCRATCH_BYTES)
     return fail(s, BOWSHOCK_INVALID,
-                "the solver's " + std::to_string((long long)ar.ncell) + " cells need " + std::to_string(need) +
-                    " bytes of line-solve scratch, more than the static maximum of " + std::to_string(BOWSHOCK_NOALLOC_SCRATCH_BYTES) +
-                    " bytes (" + std::to_string(BOWSHOCK_NOALLOC_MAX_CELLS) + " cells)");
+                "the solver's " + std::to_string((long long)ar.ncell) + " cells and " + std::to_string(ar.nil + ar.njl) + " lines need " +
+                    std::to_string(need) + " bytes of line-solve records, more than the static maximum of " +
+                    std::to_string(BOWSHOCK_NOALLOC_SCRATCH_BYTES) + " bytes");
   std::call_once(g_noalloc_once[dev], noalloc_setup, dev);
   if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev])
     return fail(s, BOWSHOCK_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(g_noalloc_err[dev]));

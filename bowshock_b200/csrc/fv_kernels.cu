@@ -367,27 +367,33 @@ __device__ __forceinline__ V4<float> rhs_of(const Arena& A, const float4* in, bo
   return r;
 }
 
-__device__ __forceinline__ void st_scratch(float* s, const M4<float>& Y, const V4<float>& g, const M4<float>& GE) {
-  float4* p = reinterpret_cast<float4*>(s);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) p[q] = make_float4(Y[4 * q], Y[4 * q + 1], Y[4 * q + 2], Y[4 * q + 3]);
-  p[4] = to_f4(g);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) p[5 + q] = make_float4(GE[4 * q], GE[4 * q + 1], GE[4 * q + 2], GE[4 * q + 3]);
+// Line-solve records in A.scratch (float4 units): for every cell and direction (i first, then j) 25 float4 =
+//   [0..3] lo, [4..7] d, [8..11] up  (the assembled blocks of I - dt J_dir, line ends folded in)
+//   [12..15] M^-1, [16..19] Y = M^-1 up, [20..23] GE (the left spike), [24] g (the right-hand side's forward sweep);
+// then for every line and lane of the reduced separator system 44 float4 = 5 PCR levels x (alpha, gamma) + b^-1.
+// The first pass of an iteration assembles and factorises (k_lines); later passes (k_lines_subst) and the defect (k_defect)
+// only read them.
+constexpr int REC = 25, PREC = 44, PCR_LEVELS = 5;
+__device__ __forceinline__ float4* line_rec(const Arena& A, bool dir_i, long long cc) {
+  return reinterpret_cast<float4*>(A.scratch) + ((dir_i ? 0 : A.ncell) + cc) * REC;
 }
-__device__ __forceinline__ void ld_scratch(const float* s, M4<float>& Y, V4<float>& g, M4<float>& GE) {
-  const float4* p = reinterpret_cast<const float4*>(s);
+__device__ __forceinline__ float4* pcr_rec(const Arena& A, bool dir_i, int gw, int lane) {
+  float4* base = reinterpret_cast<float4*>(A.scratch) + 2 * A.ncell * REC;
+  if (!dir_i) base += (long long)A.nilines * 32 * PREC;
+  return base + ((long long)gw * 32 + lane) * PREC;
+}
+__device__ __forceinline__ void st_m4(float4* p, const M4<float>& m) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) p[q] = make_float4(m[4 * q], m[4 * q + 1], m[4 * q + 2], m[4 * q + 3]);
+}
+__device__ __forceinline__ M4<float> ld_m4(const float4* p) {
+  M4<float> m;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    float4 a = p[q];
-    Y[4 * q] = a.x, Y[4 * q + 1] = a.y, Y[4 * q + 2] = a.z, Y[4 * q + 3] = a.w;
+    float4 v = p[q];
+    m[4 * q] = v.x, m[4 * q + 1] = v.y, m[4 * q + 2] = v.z, m[4 * q + 3] = v.w;
   }
-  g = from_f4(p[4]);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    float4 a = p[5 + q];
-    GE[4 * q] = a.x, GE[4 * q + 1] = a.y, GE[4 * q + 2] = a.z, GE[4 * q + 3] = a.w;
-  }
+  return m;
 }
 
 // Positivity-damped update u += alpha du, alpha halved up to 8 times (implicit.rs:641-660), on the state pair in FP64.
@@ -410,41 +416,78 @@ struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
   float a[16], b[16], c[16], d[4];
 };
 
-// Factorisation pass `pass` (0 = the first solve, p >= 1 = the p-th defect correction) of each case with more than `pass`
-// passes (implicit.rs:619-639). i-sweeps write x to `out`; j-sweeps write du (pass 0) or add the correction to du, and
-// the last pass of a case applies the positivity-damped update.
-__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out, int pass) {
+// Line geometry shared by the factorisation and substitution kernels: warp `gw` solves line L of case c; lane s owns the
+// segment [a, e) of m = max(2, ceil(len/32)) cells, the last cell of every segment but the last is a separator.
+struct LineSeg {
+  int ci, L, n, k0, len, m, P, N, a, e, ke;
+  bool act, has_sep;
+};
+__device__ __forceinline__ bool line_seg(const Arena& A, int dir_i, int gw, int lane, LineSeg& g) {
+  const int nl = dir_i ? A.nilines : A.njlines;
+  if (gw >= nl) return false;
+  g.ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  const CaseDev& c = A.cases[g.ci];
+  g.L = gw - (dir_i ? c.iline_off : c.jline_off);
+  g.n = dir_i ? c.ni : c.nj;
+  g.k0 = dir_i ? row_start(c, g.L) : col_start(c, g.L);
+  g.len = g.n - g.k0;
+  if (g.len <= 0) return false;
+  g.m = (g.len + 31) / 32;
+  if (g.m < 2) g.m = 2;
+  g.P = (g.len + g.m - 1) / g.m;
+  g.N = g.P - 1;
+  g.act = lane < g.P;
+  g.a = g.k0 + lane * g.m;
+  g.e = g.act ? min(g.a + g.m, g.n) : g.a;
+  g.has_sep = g.act && lane < g.P - 1;
+  g.ke = g.has_sep ? g.e - 2 : g.e - 1;  // last interior cell
+  return true;
+}
+
+// Result x of cell cc of a line solve: i-sweeps write x to `out`; j-sweeps write du (pass 0) or add the correction to
+// du, and the last pass of a case applies the positivity-damped update.
+__device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool update, float4* out, long long cc, const V4<float>& x) {
+  if (epilogue == 0) {
+    out[cc] = to_f4(x);
+    return;
+  }
+  V4<float> du = x;
+  if (epilogue == 2) {
+    V4<float> o = from_f4(A.DU[cc]);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) du[q] += o[q];
+  }
+  A.DU[cc] = to_f4(du);
+  if (update) damped_update(A, cc, du);
+}
+
+// First pass of an iteration (implicit.rs:619-621): assemble the blocks of I - dt J_dir of every cell of the line in
+// registers, factorise with the partitioned solver (each lane eliminates its segment, the separator unknowns form a
+// reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
+// back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line
+// records for the later passes and the defect.
+__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out) {
   __shared__ PcrSlot sp[LINE_WARPS][32];
   __shared__ float4 sl[LINE_WARPS][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * LINE_WARPS + warp;
-  const int nl = dir_i ? A.nilines : A.njlines;
-  if (gw >= nl) return;
-  const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  LineSeg G;
+  if (!line_seg(A, dir_i, gw, lane, G)) return;
+  const int ci = G.ci;
   const CaseDev& c = A.cases[ci];
-  if (!A.active[ci] || pass >= c.sub_iters) return;
-  const int epilogue = dir_i ? 0 : (pass == 0 ? 1 : 2);
-  const bool update = !dir_i && pass == c.sub_iters - 1;
-  const int L = gw - (dir_i ? c.iline_off : c.jline_off);
-  const int n = dir_i ? c.ni : c.nj;
-  const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
-  const int len = n - k0;
-  if (len <= 0) return;
-  int m = (len + 31) / 32;
-  if (m < 2) m = 2;
-  const int P = (len + m - 1) / m;
+  if (!A.active[ci]) return;
+  const int epilogue = dir_i ? 0 : 1;
+  const bool update = !dir_i && c.sub_iters <= 1;
+  const int L = G.L, n = G.n, P = G.P, N = G.N, a = G.a, e = G.e, ke = G.ke;
   const int s = lane;
-  const bool act = s < P;
-  const int a = k0 + s * m;
-  const int e = act ? min(a + m, n) : a;
-  const bool has_sep = act && s < P - 1;
-  const int ke = has_sep ? e - 2 : e - 1;  // last interior cell
+  const bool act = G.act, has_sep = G.has_sep;
   auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
   auto ij = [&](int k, int& i, int& j) {
     i = dir_i ? k : L;
     j = dir_i ? L : k;
   };
-  float* scr = A.scratch;
+  (void)n;
+  (void)P;
   // ---- forward elimination of the segment interior
   M4<float> Y = zero4<float>(), GE = zero4<float>();
   V4<float> g = mk4<float>(0, 0, 0, 0);
@@ -455,6 +498,10 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
       M4<float> Ak, Bk, Ck;
       assemble(A, c, dir_i != 0, i, j, Ak, Bk, Ck);
       long long cc = cell(k);
+      float4* rec = line_rec(A, dir_i != 0, cc);
+      st_m4(rec, Ak);
+      st_m4(rec + 4, Bk);
+      st_m4(rec + 8, Ck);
       V4<float> r = rhs_of(A, in, from_res != 0, cc);
       M4<float> M = Bk;
       M4<float> GEr;
@@ -473,7 +520,10 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
       g = mv(Minv, r);
       GE = mm(Minv, GEr);
       Y = mm(Minv, Ck);
-      st_scratch(scr + 36 * cc, Y, g, GE);
+      st_m4(rec + 12, Minv);
+      st_m4(rec + 16, Y);
+      st_m4(rec + 20, GE);
+      rec[24] = to_f4(g);
     }
   }
   // ---- (v, E, F) at the last interior cell and, by a backward pass, at the first
@@ -485,9 +535,9 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   M4<float> E_f = E_l, F_f = F_l;
   if (act) {
     for (int k = ke - 1; k >= a; --k) {
-      M4<float> Yk, GEk;
-      V4<float> gk;
-      ld_scratch(scr + 36 * cell(k), Yk, gk, GEk);
+      const float4* rec = line_rec(A, dir_i != 0, cell(k));
+      M4<float> Yk = ld_m4(rec + 16), GEk = ld_m4(rec + 20);
+      V4<float> gk = from_f4(rec[24]);
       V4<float> t = mv(Yk, v_f);
 #pragma unroll
       for (int q = 0; q < 4; ++q) v_f[q] = gk[q] - t[q];
@@ -510,7 +560,6 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   for (int q = 0; q < 4; ++q) my->d[q] = v_f[q];
   __syncwarp();
   // ---- reduced row of the separator (the last cell of the segment)
-  const int N = P - 1;
   M4<float> ra = zero4<float>(), rb = eye4<float>(), rc = zero4<float>();
   V4<float> rd = mk4<float>(0, 0, 0, 0);
   if (has_sep) {
@@ -518,6 +567,10 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
     ij(e - 1, i, j);
     M4<float> As, Bs, Cs;
     assemble(A, c, dir_i != 0, i, j, As, Bs, Cs);
+    float4* rec = line_rec(A, dir_i != 0, cell(e - 1));
+    st_m4(rec, As);
+    st_m4(rec + 4, Bs);
+    st_m4(rec + 8, Cs);
     V4<float> r = rhs_of(A, in, from_res != 0, cell(e - 1));
     const PcrSlot* nx = &sp[warp][s + 1];
     M4<float> En, Fn;
@@ -539,8 +592,10 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
     for (int q = 0; q < 4; ++q) rd[q] = r[q] - t1[q] - t2[q];
   }
   __syncwarp();
-  // ---- parallel cyclic reduction of the N separator rows across the warp
-  for (int h = 1; h < N; h <<= 1) {
+  // ---- parallel cyclic reduction of the N separator rows across the warp; multipliers kept per level
+  float4* prec = pcr_rec(A, dir_i != 0, gw, s);
+  int lvl = 0;
+  for (int h = 1; h < N; h <<= 1, ++lvl) {
     M4<float> binv = inv4(rb);
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
@@ -553,6 +608,7 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
     __syncwarp();
     if (s < N) {
       M4<float> na = zero4<float>(), nc = zero4<float>(), nb = rb;
+      M4<float> al = zero4<float>(), ga = zero4<float>();
       V4<float> nd = rd;
       if (s - h >= 0) {
         const PcrSlot* o = &sp[warp][s - h];
@@ -563,7 +619,7 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
           ob[q] = o->b[q];
           oc[q] = o->c[q];
         }
-        M4<float> al = mm(ra, ob);  // alpha = -a_i b_{i-h}^-1
+        al = mm(ra, ob);  // alpha = -a_i b_{i-h}^-1
 #pragma unroll
         for (int q = 0; q < 16; ++q) al[q] = -al[q];
         na = mm(al, oa);
@@ -582,7 +638,7 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
           ob[q] = o->b[q];
           oc[q] = o->c[q];
         }
-        M4<float> ga = mm(rc, ob);  // gamma = -c_i b_{i+h}^-1
+        ga = mm(rc, ob);  // gamma = -c_i b_{i+h}^-1
 #pragma unroll
         for (int q = 0; q < 16; ++q) ga[q] = -ga[q];
         nc = mm(ga, oc);
@@ -592,6 +648,8 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
 #pragma unroll
         for (int q = 0; q < 4; ++q) nd[q] += t[q];
       }
+      st_m4(prec + 8 * lvl, al);
+      st_m4(prec + 8 * lvl + 4, ga);
       ra = na;
       rb = nb;
       rc = nc;
@@ -600,38 +658,28 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
     __syncwarp();
   }
   V4<float> lsep = mk4<float>(0, 0, 0, 0);
-  if (s < N) lsep = mv(inv4(rb), rd);
+  if (s < N) {
+    M4<float> binv = inv4(rb);
+    st_m4(prec + 8 * PCR_LEVELS, binv);
+    lsep = mv(binv, rd);
+  }
   sl[warp][s] = to_f4(lsep);
   __syncwarp();
   if (!act) return;
   // ---- back substitution of the segment
   V4<float> lprev = s > 0 ? from_f4(sl[warp][s - 1]) : mk4<float>(0, 0, 0, 0);
   V4<float> xn = has_sep ? lsep : mk4<float>(0, 0, 0, 0);
-  auto emit = [&](long long cc, const V4<float>& x) {
-    if (epilogue == 0) {
-      out[cc] = to_f4(x);
-      return;
-    }
-    V4<float> du = x;
-    if (epilogue == 2) {
-      V4<float> o = from_f4(A.DU[cc]);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) du[q] += o[q];
-    }
-    A.DU[cc] = to_f4(du);
-    if (update) damped_update(A, cc, du);
-  };
-  if (has_sep) emit(cell(e - 1), lsep);
+  if (has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
   for (int k = ke; k >= a; --k) {
-    M4<float> Yk, GEk;
-    V4<float> gk;
     long long cc = cell(k);
-    ld_scratch(scr + 36 * cc, Yk, gk, GEk);
+    const float4* rec = line_rec(A, dir_i != 0, cc);
+    M4<float> Yk = ld_m4(rec + 16), GEk = ld_m4(rec + 20);
+    V4<float> gk = from_f4(rec[24]);
     V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
     V4<float> x;
 #pragma unroll
     for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
-    emit(cc, x);
+    line_emit(A, epilogue, update, out, cc, x);
     xn = x;
   }
   // the line through cell 0 of the case advances its iteration counters after the update
@@ -641,7 +689,116 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   }
 }
 
-// Defect of the unfactored operator (implicit.rs:622-630): rr = dt R - (A_i du + A_j du - du), per fluid cell.
+__device__ __forceinline__ V4<float> shfl_up4(const V4<float>& v, int h) {
+  V4<float> r;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) r[q] = __shfl_up_sync(0xffffffffu, v[q], h);
+  return r;
+}
+__device__ __forceinline__ V4<float> shfl_down4(const V4<float>& v, int h) {
+  V4<float> r;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) r[q] = __shfl_down_sync(0xffffffffu, v[q], h);
+  return r;
+}
+
+// Defect-correction pass `pass` >= 1 (implicit.rs:622-639) of every case with more than `pass` passes: the same solve
+// with the factors of the first pass. Per cell: g = M^-1 (r - lo g_prev) forward, the separators' right-hand sides, the
+// reduction of the right-hand side alone with the kept multipliers (warp shuffles), x = g + GE l_left - Y x_next backward.
+__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines_subst(Arena A, int dir_i, const float4* in, float4* out, int pass) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * LINE_WARPS + warp;
+  LineSeg G;
+  if (!line_seg(A, dir_i, gw, lane, G)) return;
+  const int ci = G.ci;
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || pass >= c.sub_iters) return;
+  const int epilogue = dir_i ? 0 : 2;
+  const bool update = !dir_i && pass == c.sub_iters - 1;
+  const int L = G.L, N = G.N, a = G.a, e = G.e, ke = G.ke;
+  const int s = lane;
+  auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
+  V4<float> g = mk4<float>(0, 0, 0, 0);
+  if (G.act) {
+    for (int k = a; k <= ke; ++k) {
+      long long cc = cell(k);
+      float4* rec = line_rec(A, dir_i != 0, cc);
+      V4<float> r = from_f4(in[cc]);
+      if (k > a) {
+        V4<float> t = mv(ld_m4(rec), g);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r[q] -= t[q];
+      }
+      g = mv(ld_m4(rec + 12), r);
+      rec[24] = to_f4(g);
+    }
+  }
+  const V4<float> v_l = g;
+  V4<float> v_f = v_l;
+  if (G.act) {
+    for (int k = ke - 1; k >= a; --k) {
+      const float4* rec = line_rec(A, dir_i != 0, cell(k));
+      V4<float> t = mv(ld_m4(rec + 16), v_f);
+      V4<float> gk = from_f4(rec[24]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v_f[q] = gk[q] - t[q];
+    }
+  }
+  const V4<float> vn = shfl_down4(v_f, 1);
+  V4<float> rd = mk4<float>(0, 0, 0, 0);
+  if (G.has_sep) {
+    long long cs = cell(e - 1);
+    const float4* rec = line_rec(A, dir_i != 0, cs);
+    V4<float> r = from_f4(in[cs]);
+    V4<float> t1 = mv(ld_m4(rec), v_l), t2 = mv(ld_m4(rec + 8), vn);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rd[q] = r[q] - t1[q] - t2[q];
+  }
+  const float4* prec = pcr_rec(A, dir_i != 0, gw, s);
+  int lvl = 0;
+  for (int h = 1; h < N; h <<= 1, ++lvl) {
+    V4<float> dm = shfl_up4(rd, h), dp = shfl_down4(rd, h);
+    if (s < N) {
+      V4<float> nd = rd;
+      if (s - h >= 0) {
+        V4<float> t = mv(ld_m4(prec + 8 * lvl), dm);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nd[q] += t[q];
+      }
+      if (s + h < N) {
+        V4<float> t = mv(ld_m4(prec + 8 * lvl + 4), dp);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nd[q] += t[q];
+      }
+      rd = nd;
+    }
+  }
+  V4<float> lsep = mk4<float>(0, 0, 0, 0);
+  if (s < N) lsep = mv(ld_m4(prec + 8 * PCR_LEVELS), rd);
+  V4<float> lprev = shfl_up4(lsep, 1);
+  if (s == 0) lprev = mk4<float>(0, 0, 0, 0);
+  if (!G.act) return;
+  V4<float> xn = G.has_sep ? lsep : mk4<float>(0, 0, 0, 0);
+  if (G.has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
+  for (int k = ke; k >= a; --k) {
+    long long cc = cell(k);
+    const float4* rec = line_rec(A, dir_i != 0, cc);
+    V4<float> t1 = mv(ld_m4(rec + 20), lprev), t2 = mv(ld_m4(rec + 16), xn);
+    V4<float> gk = from_f4(rec[24]);
+    V4<float> x;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
+    line_emit(A, epilogue, update, out, cc, x);
+    xn = x;
+  }
+  if (update && L == 0 && lane == 0) {
+    A.iter[ci] += 1;
+    A.ramp_k[ci] += 1;
+  }
+}
+
+// Defect of the unfactored operator (implicit.rs:622-630): rr = dt R - (A_i du + A_j du - du), per fluid cell, with the
+// blocks the first pass kept in the line records.
 __global__ void k_defect(Arena A, int pass) {
   int t = blockIdx.x;
   int ci = A.tile_case[t];
@@ -659,18 +816,17 @@ __global__ void k_defect(Arena A, int pass) {
   V4<float> acc = mk4<float>(0, 0, 0, 0);
   for (int dir = 0; dir < 2; ++dir) {
     bool di = dir == 0;
-    M4<float> lo, d, up;
-    assemble(A, c, di, i, j, lo, d, up);
-    V4<float> v = mv(d, du);
+    const float4* rec = line_rec(A, di, cc);
+    V4<float> v = mv(ld_m4(rec + 4), du);
     int k = di ? i : j, kn = di ? c.ni : c.nj;
     int k0 = di ? row_start(c, j) : col_start(c, i);
     if (k > k0) {
-      V4<float> t2 = mv(lo, from_f4(A.DU[di ? cidx(c, i - 1, j) : cidx(c, i, j - 1)]));
+      V4<float> t2 = mv(ld_m4(rec), from_f4(A.DU[di ? cidx(c, i - 1, j) : cidx(c, i, j - 1)]));
 #pragma unroll
       for (int q = 0; q < 4; ++q) v[q] += t2[q];
     }
     if (k + 1 < kn) {
-      V4<float> t2 = mv(up, from_f4(A.DU[di ? cidx(c, i + 1, j) : cidx(c, i, j + 1)]));
+      V4<float> t2 = mv(ld_m4(rec + 8), from_f4(A.DU[di ? cidx(c, i + 1, j) : cidx(c, i, j + 1)]));
 #pragma unroll
       for (int q = 0; q < 4; ++q) v[q] += t2[q];
     }

@@ -244,6 +244,8 @@ struct ArenaHost {
   long long ncell = 0, npad = 0, nif = 0, njf = 0;
   int ntiles = 0, nil = 0, njl = 0, npblk = 0;
   int max_line = 0;  // longest i or j line of any case
+  // floats of the line-solve records: 25 float4 per cell and direction, 44 float4 per lane of every line
+  size_t scratch_floats() const { return 4 * ((size_t)2 * ncell * 25 + (size_t)(nil + njl) * 32 * 44); }
   bool any_viscous = false, any_sst = false;
   // device buffers
   Arena A{};
@@ -396,7 +398,7 @@ struct ArenaHost {
     A.cellg = cg;
     A.ifc = ic;
     A.jfc = jc;
-    ALLOC(A.scratch, ncell * 36);
+    ALLOC(A.scratch, scratch_floats());
     ALLOC(A.rsum, (size_t)slots * nc);
     ALLOC(A.tsum, (size_t)slots * nc);
     ALLOC(d_enabled, nc);
@@ -456,6 +458,7 @@ struct ArenaHost {
     A.ntiles = ntiles;
     A.iline_case = d_iline;
     A.nilines = nil;
+    A.ncell = ncell;
     A.jline_case = d_jline;
     A.njlines = njl;
     A.pblk_case = d_pblk;
@@ -720,12 +723,12 @@ struct ArenaHost {
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot); });
       const int s = sub_iters_of_arena();
-      L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X, 0); });
-      L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, 0); });
+      L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X); });
+      L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
         L(G_DEFECT, [&] { k_defect<<<ntiles, TI * TJ, 0, stream>>>(A, p); });
-        L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, 0, A.X, p); });
-        L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr, p); });
+        L(G_LINES_I, [&] { k_lines_subst<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, A.X, p); });
+        L(G_LINES_J, [&] { k_lines_subst<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, nullptr, p); });
       }
       if (any_sst) {
         // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step

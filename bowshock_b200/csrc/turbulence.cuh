@@ -266,7 +266,7 @@ __global__ void k_turb_lines(Arena A, int dir_i) {
   int n = dir_i ? c.ni : c.nj;
   int k0 = dir_i ? row_start(c, L) : col_start(c, L);
   if (n - k0 <= 0) return;
-  float* cp = A.scratch;  // 36 floats per cell: slots 0 / 1 hold the Thomas c' of the two scalars
+  float* cp = A.scratch;  // the mean-flow line records are spent by now: floats 36 c + 0 / 1 hold the Thomas c' of the scalars
   float xprev = 0.f, cprev = 0.f;
   for (int k = k0; k < n; ++k) {
     long long cc = dir_i ? cidx(c, k, L) : cidx(c, L, k);

@@ -218,8 +218,8 @@ class GpuSolver:
 
     def run_noalloc(self, n: int) -> np.ndarray:
         """`run` without device allocation (bowshock_solver_run_noalloc): for stepping from code that may not allocate
-        device memory once the solver exists. The line solves use the library's static 16 MiB scratch array, shared by
-        all calls on the device, so calls overlapping on one GPU must be serialised."""
+        device memory once the solver exists. The line solves keep their records in the library's static 64 MiB array,
+        shared by all calls on the device, so calls overlapping on one GPU must be serialised."""
         out = np.zeros(n)
         self._check(_ffi.load().bowshock_solver_run_noalloc(self._h, int(n), _dp(out)))
         return out

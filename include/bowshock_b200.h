@@ -296,14 +296,15 @@ int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* 
  * own pool (another framework's caching allocator on the same device), or the stepping loop cannot take the device-wide
  * synchronisation an allocation may cause. bowshock_solver_run allocates on its first call (CUDA graph instantiation,
  * timing events); this variant launches the same kernels directly on the solver's stream and takes the line solves'
- * spike storage (36 floats per cell) from a static 16 MiB device array of the library, so solvers of at most
- * BOWSHOCK_NOALLOC_MAX_CELLS cells (all multigrid levels counted) are accepted; larger ones get BOWSHOCK_INVALID with a
- * message and nothing is launched. Same residual semantics and results as bowshock_solver_run.
+ * records (blocks, factors, reduction multipliers) from a static 64 MiB device array of the library. A solver needs
+ * BOWSHOCK_NOALLOC_BYTES(cells, lines) of it, cells and i + j lines of all multigrid levels counted (about 80,000 cells
+ * for a grid of aspect 2); a larger one gets BOWSHOCK_INVALID with a message and nothing is launched. Same residual
+ * semantics and results as bowshock_solver_run.
  * The first call on a device looks the array's device address up (cudaGetSymbolAddress with that device current); make
  * that first call before any stream capture. Every call on a device shares the array (nothing in it needs to start at
  * zero); calls that overlap on one GPU, from solvers on other streams or threads, race on it and must be serialised. */
-#define BOWSHOCK_NOALLOC_SCRATCH_BYTES (16u << 20)
-#define BOWSHOCK_NOALLOC_MAX_CELLS (BOWSHOCK_NOALLOC_SCRATCH_BYTES / 144u)
+#define BOWSHOCK_NOALLOC_SCRATCH_BYTES (64u << 20)
+#define BOWSHOCK_NOALLOC_BYTES(cells, lines) (400ull * 2ull * (unsigned long long)(cells) + 22528ull * (unsigned long long)(lines))
 int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, double* residual);
 
 #ifdef __cplusplus
