@@ -283,11 +283,13 @@ def run_ours(args, rank, world, dist):
     top = max(groups, key=lambda g: groups[g][0])
     ms_top, launches_top = groups[top]
     viscous = np.array([c.viscous is not None for c in cases])
-    if top in ("lines_i", "lines_j"):
+    if top in ("lines_i", "lines_j", "subst_i", "subst_j"):
         words = np.where(viscous, SWEEP_WORDS[True], SWEEP_WORDS[False])
         sub = np.array([c.numerics.scheme.sub_iters for c in cases])
-        # one launch sweeps every case that has a pass at that position; average over the passes of an iteration
-        bytes_iter = float(np.sum(cells * words * 4 * sub)) / sub.max()
+        if top.startswith("lines"):  # the factorising first pass sweeps every case once
+            bytes_iter = float(np.sum(cells * words * 4))
+        else:  # a substitution launch sweeps the cases with a pass at that position: the mean over the launches
+            bytes_iter = float(np.sum(cells * words * 4 * (sub - 1))) / max(sub.max() - 1, 1)
     else:
         bytes_iter = float(np.sum(cells * (42 + np.where(viscous, 21, 0)) * 4))  # residual pass: 2 nv + g + v + 1 words
     ms_launch = ms_top / launches_top

@@ -64,12 +64,12 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_last_solve_ms(self._h, C.byref(d)))
         return d.value
 
-    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage")
+    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage", "subst_i", "subst_j", "assemble")
 
     def profile(self, n: int):
         """Per-kernel-group device time over n iterations launched one kernel at a time: {group: (ms, launches)}."""
-        ms = np.zeros(8)
-        cnt = (C.c_uint64 * 8)()
+        ms = np.zeros(len(self.PROFILE_GROUPS))
+        cnt = (C.c_uint64 * len(self.PROFILE_GROUPS))()
         self._check(_ffi.load().bowshock_arena_profile(self._h, int(n), _ffi.dptr(ms), cnt))
         return {g: (float(ms[k]), int(cnt[k])) for k, g in enumerate(self.PROFILE_GROUPS)}
 

@@ -461,8 +461,30 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
   if (update) damped_update(A, cc, du);
 }
 
-// First pass of an iteration (implicit.rs:619-621): assemble the blocks of I - dt J_dir of every cell of the line in
-// registers, factorise with the partitioned solver (each lane eliminates its segment, the separator unknowns form a
+// Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
+// one thread per cell: the assembly is the arithmetic-heavy part of the operator and has no dependence along the lines.
+__global__ void __launch_bounds__(TI* TJ) k_assemble(Arena A) {
+  int t = blockIdx.x;
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (i >= c.ni || j >= c.nj || is_solid(c, i, j)) return;
+  long long cc = cidx(c, i, j);
+#pragma unroll 1
+  for (int dir = 0; dir < 2; ++dir) {
+    M4<float> lo, d, up;
+    assemble(A, c, dir == 0, i, j, lo, d, up);
+    float4* rec = line_rec(A, dir == 0, cc);
+    st_m4(rec, lo);
+    st_m4(rec + 4, d);
+    st_m4(rec + 8, up);
+  }
+}
+
+// First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble left in the line records, factorise
+// with the partitioned solver (each lane eliminates its segment, the separator unknowns form a
 // reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
 // back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line
 // records for the later passes and the defect.
@@ -482,10 +504,6 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   const int s = lane;
   const bool act = G.act, has_sep = G.has_sep;
   auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
-  auto ij = [&](int k, int& i, int& j) {
-    i = dir_i ? k : L;
-    j = dir_i ? L : k;
-  };
   (void)n;
   (void)P;
   // ---- forward elimination of the segment interior
@@ -493,15 +511,9 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   V4<float> g = mk4<float>(0, 0, 0, 0);
   if (act) {
     for (int k = a; k <= ke; ++k) {
-      int i, j;
-      ij(k, i, j);
-      M4<float> Ak, Bk, Ck;
-      assemble(A, c, dir_i != 0, i, j, Ak, Bk, Ck);
       long long cc = cell(k);
       float4* rec = line_rec(A, dir_i != 0, cc);
-      st_m4(rec, Ak);
-      st_m4(rec + 4, Bk);
-      st_m4(rec + 8, Ck);
+      M4<float> Ak = ld_m4(rec), Bk = ld_m4(rec + 4), Ck = ld_m4(rec + 8);
       V4<float> r = rhs_of(A, in, from_res != 0, cc);
       M4<float> M = Bk;
       M4<float> GEr;
@@ -563,14 +575,8 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, c
   M4<float> ra = zero4<float>(), rb = eye4<float>(), rc = zero4<float>();
   V4<float> rd = mk4<float>(0, 0, 0, 0);
   if (has_sep) {
-    int i, j;
-    ij(e - 1, i, j);
-    M4<float> As, Bs, Cs;
-    assemble(A, c, dir_i != 0, i, j, As, Bs, Cs);
-    float4* rec = line_rec(A, dir_i != 0, cell(e - 1));
-    st_m4(rec, As);
-    st_m4(rec + 4, Bs);
-    st_m4(rec + 8, Cs);
+    const float4* rec = line_rec(A, dir_i != 0, cell(e - 1));
+    M4<float> As = ld_m4(rec), Bs = ld_m4(rec + 4), Cs = ld_m4(rec + 8);
     V4<float> r = rhs_of(A, in, from_res != 0, cell(e - 1));
     const PcrSlot* nx = &sp[warp][s + 1];
     M4<float> En, Fn;

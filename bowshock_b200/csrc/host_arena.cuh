@@ -680,7 +680,7 @@ struct ArenaHost {
 
   // ---------------------------------------------------------------- one iteration (stream-ordered launches)
   // Kernel groups of the per-kernel profile (CUDA events around every launch when `profiling` is set).
-  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_N };
+  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_SUBST_I, G_SUBST_J, G_ASSEMBLE, G_N };
   bool profiling = false;
   double prof_ms[G_N] = {0};
   long long prof_launches[G_N] = {0};
@@ -723,12 +723,13 @@ struct ArenaHost {
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot); });
       const int s = sub_iters_of_arena();
+      L(G_ASSEMBLE, [&] { k_assemble<<<ntiles, TI * TJ, 0, stream>>>(A); });
       L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
         L(G_DEFECT, [&] { k_defect<<<ntiles, TI * TJ, 0, stream>>>(A, p); });
-        L(G_LINES_I, [&] { k_lines_subst<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, A.X, p); });
-        L(G_LINES_J, [&] { k_lines_subst<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, nullptr, p); });
+        L(G_SUBST_I, [&] { k_lines_subst<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, A.X, p); });
+        L(G_SUBST_J, [&] { k_lines_subst<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, nullptr, p); });
       }
       if (any_sst) {
         // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step

@@ -286,9 +286,10 @@ int bowshock_arena_last_ms_per_iter(const bowshock_arena* a, double* ms);
 int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
 
 /* Per-kernel profile (the reference's Profile of gpu/mod.rs:533-542): n iterations launched one kernel at a time with CUDA
- * events around each launch; per kernel group (prims, viscous, residual, i-lines, j-lines, defect, turbulence, stage) the
+ * events around each launch; per kernel group (prims, viscous, residual, i-lines, j-lines (the factorising first pass),
+ * defect, turbulence, stage, i- and j-substitution passes, block assembly) the
  * total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
-#define BOWSHOCK_PROFILE_GROUPS 8
+#define BOWSHOCK_PROFILE_GROUPS 11
 int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
 
 /* bowshock_solver_run without any device allocation. No counterpart in the reference. For hosts that create their solvers
