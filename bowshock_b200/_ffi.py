@@ -66,7 +66,7 @@ class RunParams(C.Structure):  # bowshock_run_params
 
 class PointResult(C.Structure):  # bowshock_point_result
     _fields_ = [("iters", C.c_uint64), ("residual_peak", C.c_double), ("drop_orders", C.c_double), ("stop_reason", C.c_int32),
-                ("forces", Forces), ("last_monitor", C.c_double)]
+                ("forces", Forces), ("last_monitor", C.c_double), ("cd_window", C.c_double)]
 
 
 class BaseGridC(C.Structure):  # bowshock_base_grid

@@ -320,40 +320,6 @@ __device__ void assemble(const Arena& A, const CaseDev& c, bool dir_i, int i, in
   }
   cell_blocks<float>(wk, wm, wp, fl.x, fl.y, fl.w, fr.x, fr.y, fr.w, g.x, A.dt[cc], c.lines != 0, src, c.roe != 0, c.eps_fix, lam_l, lam_r,
                      lo, d, up);
-  if (k == k0) {
-    M4<float> T;
-    if (jet) {
-      T = zero4<float>();
-    } else if (wall_lower) {
-      bool ns = dir_i ? noslip_iface(c, k0, j) : noslip_jface(c, i, k0);
-      T = ns ? noslip4<float>() : reflection<float>(fl.x, fl.y);
-    } else if (!c.implicit_bc) {
-      T = zero4<float>();
-    } else {
-      int bc = dir_i ? c.bc[0] : c.bc[2];
-      if (!dir_i && noslip_jface(c, i, 0) && bc == BC_SLIPWALL) {
-        T = noslip4<float>();
-      } else {
-        M4<double> Td = ghost_jacobian(bc, fs_of(c), cvt4<double>(wk), fl.x, fl.y, -1.0);
-#pragma unroll
-        for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
-      }
-    }
-    axpy(d, 1.f, mm(lo, T));
-    lo = zero4<float>();
-  }
-  if (k == n - 1) {
-    M4<float> T;
-    if (!c.implicit_bc) {
-      T = zero4<float>();
-    } else {
-      M4<double> Td = ghost_jacobian(dir_i ? c.bc[1] : c.bc[3], fs_of(c), cvt4<double>(wk), fr.x, fr.y, 1.0);
-#pragma unroll
-      for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
-    }
-    axpy(d, 1.f, mm(up, T));
-    up = zero4<float>();
-  }
 }
 
 // right-hand side of a line solve for cell cc: dt R (first pass) or the stored vector
@@ -463,7 +429,7 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
 
 // Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
 // one thread per cell: the assembly is the arithmetic-heavy part of the operator and has no dependence along the lines.
-__global__ void __launch_bounds__(TI* TJ) k_assemble(Arena A) {
+__global__ void __launch_bounds__(TI* TJ, 2) k_assemble(Arena A) {
   int t = blockIdx.x;
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
@@ -483,7 +449,76 @@ __global__ void __launch_bounds__(TI* TJ) k_assemble(Arena A) {
   }
 }
 
-// First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble left in the line records, factorise
+// Ghost Jacobians of the two ends of line `L` folded into the diagonal blocks (implicit.rs:440-467): at the first cell
+// d += lo T and lo = 0, with T the wall reflection / no-slip, the jet's zero, or the far-field ghost Jacobian (FP64 finite
+// differences); at the last cell d += up T and up = 0. One thread per line, after k_assemble.
+__device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int L) {
+  const int n = dir_i ? c.ni : c.nj;
+  const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
+  if (k0 >= n) return;
+  {
+    const int i = dir_i ? k0 : L, j = dir_i ? L : k0;
+    const long long cc = cidx(c, i, j);
+    float4 fl = dir_i ? A.iface[ifidx(c, i, j)] : A.jface[jfidx(c, i, j)];
+    bool wall_lower = k0 > 0;
+    bool jet = wall_lower && dir_i && jet_iface(c, k0, j);
+    M4<float> T;
+    if (jet) {
+      T = zero4<float>();
+    } else if (wall_lower) {
+      bool ns = dir_i ? noslip_iface(c, k0, j) : noslip_jface(c, i, k0);
+      T = ns ? noslip4<float>() : reflection<float>(fl.x, fl.y);
+    } else if (!c.implicit_bc) {
+      T = zero4<float>();
+    } else {
+      int bc = dir_i ? c.bc[0] : c.bc[2];
+      if (!dir_i && noslip_jface(c, i, 0) && bc == BC_SLIPWALL) {
+        T = noslip4<float>();
+      } else {
+        M4<double> Td = ghost_jacobian(bc, fs_of(c), cvt4<double>(Wat(A, c, i, j)), fl.x, fl.y, -1.0);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
+      }
+    }
+    float4* rec = line_rec(A, dir_i, cc);
+    M4<float> d = ld_m4(rec + 4);
+    axpy(d, 1.f, mm(ld_m4(rec), T));
+    st_m4(rec, zero4<float>());
+    st_m4(rec + 4, d);
+  }
+  {
+    const int i = dir_i ? n - 1 : L, j = dir_i ? L : n - 1;
+    const long long cc = cidx(c, i, j);
+    float4 fr = dir_i ? A.iface[ifidx(c, i + 1, j)] : A.jface[jfidx(c, i, j + 1)];
+    M4<float> T;
+    if (!c.implicit_bc) {
+      T = zero4<float>();
+    } else {
+      M4<double> Td = ghost_jacobian(dir_i ? c.bc[1] : c.bc[3], fs_of(c), cvt4<double>(Wat(A, c, i, j)), fr.x, fr.y, 1.0);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
+    }
+    float4* rec = line_rec(A, dir_i, cc);
+    M4<float> d = ld_m4(rec + 4);
+    axpy(d, 1.f, mm(ld_m4(rec + 8), T));
+    st_m4(rec + 8, zero4<float>());
+    st_m4(rec + 4, d);
+  }
+}
+
+// every i line, then every j line, of the active cases
+__global__ void k_line_ends(Arena A) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool dir_i = t < A.nilines;
+  int gw = dir_i ? t : t - A.nilines;
+  if (!dir_i && gw >= A.njlines) return;
+  int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  fold_line_ends(A, c, dir_i, gw - (dir_i ? c.iline_off : c.jline_off));
+}
+
+// First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble and k_line_ends left in the line records, factorise
 // with the partitioned solver (each lane eliminates its segment, the separator unknowns form a
 // reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
 // back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line

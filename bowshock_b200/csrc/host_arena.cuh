@@ -724,6 +724,7 @@ struct ArenaHost {
       L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot); });
       const int s = sub_iters_of_arena();
       L(G_ASSEMBLE, [&] { k_assemble<<<ntiles, TI * TJ, 0, stream>>>(A); });
+      L(G_ASSEMBLE, [&] { k_line_ends<<<(nil + njl + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {

@@ -209,6 +209,15 @@ inline void fill_point(const CaseRun& cr, const Forces& f, bowshock_point_result
   for (int k = 0; k < MAX_SEG; ++k) o->forces.cd_aft[k] = k < cr.nseg ? f.f[F_CD_AFT0 + k] : 0.0;
   o->forces.cd_total = f.cd_total(cr.nseg);
   o->last_monitor = cr.last_monitor;
+  o->cd_window = o->forces.cd_total;
+  if (cr.reason == 4 && cr.p.mean_window >= SYNC) {  // mean stationary: the two windows mean_stationary compared
+    size_t k = 2 * (size_t)(cr.p.mean_window / SYNC);
+    if (cr.hist.size() >= k) {
+      double m = 0.0;
+      for (size_t t = cr.hist.size() - k; t < cr.hist.size(); ++t) m += cr.hist[t].second;
+      o->cd_window = m / (double)k;
+    }
+  }
 }
 
 // Cold (or warm) start of case k for a run: free stream, turbulence re-initialised, counters reset (run.rs:44-63).

@@ -279,7 +279,7 @@ def forces_dict(f, nseg):
 
 def point_dict(p, nseg, residual=None):
     d = dict(iters=p.iters, residual_peak=p.residual_peak, drop_orders=p.drop_orders, stop_reason=STOP_REASONS[p.stop_reason],
-             last_monitor=p.last_monitor)
+             last_monitor=p.last_monitor, cd_window=p.cd_window)
     d.update(forces_dict(p.forces, nseg))
     if residual is not None:
         d["residual"] = residual

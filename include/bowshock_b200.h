@@ -214,6 +214,9 @@ typedef struct {
   int32_t stop_reason;
   bowshock_forces forces;
   double last_monitor;
+  /* a run stopped on a limit cycle (mean stationary): the mean of the monitored CD over the two windows the rule compared;
+   * otherwise the final total CD. Not in the reference: the instantaneous CD of a limit cycle depends on the phase. */
+  double cd_window;
 } bowshock_point_result;
 
 /* Progress callback, called between chunks of 50 iterations (progress.rs:1-8); return non-zero to cancel. */

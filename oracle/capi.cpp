@@ -87,6 +87,7 @@ typedef struct {
   int stop_reason;
   double cd_nose, cd_nose_cell, cd_aft[8], cd_base, cd_friction, cd_total, cp_base, cp_base_cell, y_plus_max, farfield_dp, min_rho, min_p,
       m_max, m_wall_max;
+  double cd_window;  // mean stationary: mean monitored CD over the two compared windows; otherwise cd_total
 } OrcPointResult;
 
 }  // extern "C"
@@ -703,6 +704,13 @@ int orc_run_on(const OrcCase* c, void* h, int warm, double r_ref, OrcPointResult
   Solver* s = static_cast<Solver*>(h);
   PointResult p = run_on(cc, *s, warm != 0, r_ref >= 0 ? &r_ref : nullptr);
   fill_result(p, out);
+  out->cd_window = p.cd_total;
+  size_t k = 2 * (cc.numerics.mean_window / MONITOR_EVERY);
+  if (p.stop_reason == STOP_MEAN_STATIONARY && k > 0 && p.monitor_history.size() >= k) {
+    double m = 0.0;
+    for (size_t t = p.monitor_history.size() - k; t < p.monitor_history.size(); ++t) m += p.monitor_history[t].second;
+    out->cd_window = m / (double)k;
+  }
   if (residual)
     for (size_t k = 0; k < p.residual.size() && k < cap; ++k) residual[k] = p.residual[k];
   return 0;

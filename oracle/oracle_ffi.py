@@ -85,7 +85,7 @@ class OrcPointResult(C.Structure):
                 ("cd_aft", C.c_double * 8), ("cd_base", C.c_double), ("cd_friction", C.c_double),
                 ("cd_total", C.c_double), ("cp_base", C.c_double), ("cp_base_cell", C.c_double),
                 ("y_plus_max", C.c_double), ("farfield_dp", C.c_double), ("min_rho", C.c_double),
-                ("min_p", C.c_double), ("m_max", C.c_double), ("m_wall_max", C.c_double)]
+                ("min_p", C.c_double), ("m_max", C.c_double), ("m_wall_max", C.c_double), ("cd_window", C.c_double)]
 
 
 def build():
@@ -559,6 +559,7 @@ class PointResult:
     min_rho: float
     min_p: float
     m_max: float
+    cd_window: float = float("nan")
 
 
 def _result(p: OrcPointResult, residual, nseg):
@@ -566,7 +567,7 @@ def _result(p: OrcPointResult, residual, nseg):
                        stop_reason=STOP_REASONS[p.stop_reason], cd_nose=p.cd_nose, cd_aft=list(p.cd_aft)[:nseg],
                        cd_base=p.cd_base, cd_friction=p.cd_friction, cd_total=p.cd_total, cp_base=p.cp_base,
                        y_plus_max=p.y_plus_max, farfield_dp=p.farfield_dp, min_rho=p.min_rho, min_p=p.min_p,
-                       m_max=p.m_max)
+                       m_max=p.m_max, cd_window=p.cd_window)
 
 
 def run_on(case: OrcCase, s: Solver, warm=False, r_ref=None) -> PointResult:

@@ -42,7 +42,8 @@ def main():
         sec = time.time() - t0
         data["cases"][str(k)] = dict(ni=ni, nj=nj, viscous=c.viscous is not None, mach=c.mach, iters=res.iters, stop=res.stop_reason,
                                      drop=res.drop_orders, cd_total=res.cd_total, cd_nose=res.cd_nose, cd_aft=res.cd_aft,
-                                     cd_friction=res.cd_friction, cd_base=res.cd_base, cp_base=res.cp_base, seconds=round(sec, 2),
+                                     cd_friction=res.cd_friction, cd_base=res.cd_base, cp_base=res.cp_base, cd_window=res.cd_window,
+                                     seconds=round(sec, 2),
                                      threads=int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())))
         json.dump(data, open(OUT + ".tmp", "w"), indent=1)
         os.replace(OUT + ".tmp", OUT)
