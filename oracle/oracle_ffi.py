@@ -588,3 +588,222 @@ def finish(case: OrcCase, s: Solver) -> PointResult:
 
 def monitor(case: OrcCase, s: Solver) -> float:
     return lib().orc_monitor(C.byref(case), s.handle)
+
+
+# ------------------------------------------------------------------ 3D Euler (solver3.cpp)
+class OrcImplicitParams(C.Structure):  # orc::ImplicitParams
+    _fields_ = [("cfl0", C.c_double), ("cfl_max", C.c_double), ("growth", C.c_double), ("dt_mode", C.c_int), ("lines", C.c_bool),
+                ("implicit_bc", C.c_bool), ("sub_iters", C.c_size_t), ("roe", C.c_bool), ("eps_fix", C.c_double)]
+
+
+class Orc3Result(C.Structure):
+    _fields_ = [("cn", C.c_double), ("ca", C.c_double), ("x_cp", C.c_double), ("iterations", C.c_uint64), ("stop_reason", C.c_int32),
+                ("drop_orders", C.c_double)]
+
+
+STOP3 = {0: "max iterations", 1: "residual drop", 2: "CN stationary", 5: "non-finite residual"}
+_lib3_ready = False
+
+
+def lib3():
+    global _lib3_ready
+    L = lib()
+    if not _lib3_ready:
+        D, P, S, I, U = C.c_double, C.c_void_p, C.c_size_t, C.c_int, C.c_uint64
+        dp = C.POINTER(C.c_double)
+        sig = {
+            "orc3_new": (P, [U, U, dp, dp, U, dp, U, D, D, I, U, I, I, C.POINTER(OrcImplicitParams), D, C.c_char_p, U]),
+            "orc3_free": (None, [P]),
+            "orc3_dims": (None, [P, C.POINTER(U), C.POINTER(U), C.POINTER(U)]),
+            "orc3_get": (U, [P, I, dp]),
+            "orc3_set_state": (None, [P, dp]),
+            "orc3_set_iter": (None, [P, U, U]),
+            "orc3_eval_residual": (D, [P, D]),
+            "orc3_steps": (None, [P, U, dp]),
+            "orc3_forces": (None, [P, D, D, dp]),
+            "orc3_run": (None, [P, D, D, U, D, U, C.POINTER(Orc3Result)]),
+            "orc3_face_flux": (None, [dp, dp, dp, dp, I, dp, dp, I, dp]),
+            "orc3_hllc": (None, [dp, dp, dp, dp]),
+            "orc3_physical_flux": (None, [dp, dp, dp]),
+            "orc3_char_ghost": (None, [dp, dp, dp, dp]),
+            "orc3_flux_jacobian": (None, [dp, dp, dp]),
+            "orc3_abs_jacobian": (None, [dp, dp, dp, D, dp]),
+            "orc3_inv5": (None, [dp, dp]),
+            "orc3_block_thomas5": (None, [U, dp, dp, dp, dp]),
+            "orc3_reflection": (None, [dp, dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib3_ready = True
+    return L
+
+
+def face_flux3(m2, m1, p0, p1, lim, n, rot, low_mach=False):
+    out = np.zeros(5)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (m2, m1, p0, p1, n, rot)]
+    lib3().orc3_face_flux(_dp(a[0]), _dp(a[1]), _dp(a[2]), _dp(a[3]), int(lim), _dp(a[4]), _dp(a[5]), int(low_mach), _dp(out))
+    return out
+
+
+def hllc3(wl, wr, n):
+    out = np.zeros(5)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (wl, wr, n)]
+    lib3().orc3_hllc(_dp(a[0]), _dp(a[1]), _dp(a[2]), _dp(out))
+    return out
+
+
+def physical_flux3(w, n):
+    out = np.zeros(5)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (w, n)]
+    lib3().orc3_physical_flux(_dp(a[0]), _dp(a[1]), _dp(out))
+    return out
+
+
+def characteristic_ghost3(fs, interior, n):
+    out = np.zeros(5)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (fs, interior, n)]
+    lib3().orc3_char_ghost(_dp(a[0]), _dp(a[1]), _dp(a[2]), _dp(out))
+    return out
+
+
+def flux_jacobian3(w, n):
+    out = np.zeros(25)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (w, n)]
+    lib3().orc3_flux_jacobian(_dp(a[0]), _dp(a[1]), _dp(out))
+    return out.reshape(5, 5)
+
+
+def abs_jacobian3(wl, wr, n, eps_fix):
+    out = np.zeros(25)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (wl, wr, n)]
+    lib3().orc3_abs_jacobian(_dp(a[0]), _dp(a[1]), _dp(a[2]), eps_fix, _dp(out))
+    return out.reshape(5, 5)
+
+
+def inv5(m):
+    out = np.zeros(25)
+    a = np.ascontiguousarray(m, dtype=np.float64)
+    lib3().orc3_inv5(_dp(a), _dp(out))
+    return out.reshape(5, 5)
+
+
+def reflection3(n):
+    out = np.zeros(25)
+    a = np.ascontiguousarray(n, dtype=np.float64)
+    lib3().orc3_reflection(_dp(a), _dp(out))
+    return out.reshape(5, 5)
+
+
+def block_thomas5(lo, d, up, rhs):
+    lo, d, up = (np.ascontiguousarray(a, dtype=np.float64) for a in (lo, d, up))
+    x = np.ascontiguousarray(rhs, dtype=np.float64).copy()
+    lib3().orc3_block_thomas5(x.shape[0], _dp(lo), _dp(d), _dp(up), _dp(x))
+    return x
+
+
+def prim_to_cons3(w):
+    w = np.asarray(w, dtype=np.float64)
+    rho, u, v, ww, p = (w[..., k] for k in range(5))
+    return np.stack([rho, rho * u, rho * v, rho * ww, p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + ww * ww)], axis=-1)
+
+
+def cons_to_prim3(q):
+    q = np.asarray(q, dtype=np.float64)
+    rho = q[..., 0]
+    u, v, ww = q[..., 1] / rho, q[..., 2] / rho, q[..., 3] / rho
+    p = (GAMMA - 1.0) * (q[..., 4] - 0.5 * rho * (u * u + v * v + ww * ww))
+    return np.stack([rho, u, v, ww, p], axis=-1)
+
+
+def freestream3(mach, alpha):
+    return np.array([1.0, mach * np.cos(alpha), 0.0, mach * np.sin(alpha), 1.0 / GAMMA])
+
+
+def implicit3_params(**kw):
+    """`ImplicitParams::DEFAULT` (implicit.rs:79-80) with overrides."""
+    p = OrcImplicitParams(cfl0=1.0, cfl_max=30.0, growth=1.02, dt_mode=DT_SUM, lines=True, implicit_bc=True, sub_iters=2, roe=True, eps_fix=0.1)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Solver3:
+    """`Solver3` on a revolved 2D grid (grid3.rs:189-206): nodes (ni+1)(nj+1) of x, r; theta: nk+1 angles in [0, pi]."""
+
+    def __init__(self, ni, nj, x2, r2, nk, theta, axis_cells, mach, alpha, limiter=MINMOD, first_order_iters=0, low_mach=False,
+                 implicit=True, params=None, cfl=0.5):
+        x2 = np.ascontiguousarray(x2, dtype=np.float64).reshape(-1)
+        r2 = np.ascontiguousarray(r2, dtype=np.float64).reshape(-1)
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        err = C.create_string_buffer(256)
+        p = params if params is not None else implicit3_params()
+        self._h = lib3().orc3_new(ni, nj, _dp(x2), _dp(r2), nk, _dp(th), axis_cells, mach, alpha, int(limiter), first_order_iters,
+                                  int(low_mach), int(implicit), C.byref(p), cfl, err, 256)
+        if not self._h:
+            raise ValueError(err.value.decode())
+        self.mach, self.alpha = mach, alpha
+        self.dims = (ni, nj, nk)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib3().orc3_free(self._h)
+            self._h = None
+
+    def _get(self, field):
+        n = lib3().orc3_get(self._h, field, None)
+        out = np.zeros(n)
+        lib3().orc3_get(self._h, field, _dp(out))
+        return out
+
+    @property
+    def u(self):
+        return self._get(0).reshape(-1, 5)
+
+    @u.setter
+    def u(self, v):
+        a = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        lib3().orc3_set_state(self._h, _dp(a))
+
+    @property
+    def res(self):
+        return self._get(1).reshape(-1, 5)
+
+    @property
+    def dt(self):
+        return self._get(2)
+
+    @property
+    def vol(self):
+        return self._get(3)
+
+    @property
+    def xc(self):
+        return self._get(4).reshape(-1, 3)
+
+    def faces(self, fam):
+        """(n, area, centroid) per face of family 0 / 1 / 2 (i / j / k)."""
+        f = self._get(5 + fam).reshape(-1, 7)
+        return f[:, :3], f[:, 3], f[:, 4:]
+
+    def set_iter(self, it, ramp=None):
+        lib3().orc3_set_iter(self._h, it, it if ramp is None else ramp)
+
+    def eval_residual(self, cfl=0.5):
+        return lib3().orc3_eval_residual(self._h, cfl)
+
+    def steps(self, n):
+        r = np.zeros(n)
+        lib3().orc3_steps(self._h, n, _dp(r))
+        return r
+
+    def forces(self, x_max):
+        out = np.zeros(3)
+        lib3().orc3_forces(self._h, self.mach, x_max, _dp(out))
+        return dict(cn=out[0], ca=out[1], x_cp=out[2])
+
+    def run(self, x_max, max_iter=8000, rel_tol=0.002, window=500):
+        r = Orc3Result()
+        lib3().orc3_run(self._h, self.mach, x_max, max_iter, rel_tol, window, C.byref(r))
+        return dict(cn=r.cn, ca=r.ca, x_cp=r.x_cp, iterations=r.iterations, stop_reason=STOP3.get(r.stop_reason, "?"), drop_orders=r.drop_orders)

@@ -25,6 +25,8 @@ def oracle_case(c):
     for k, n in enumerate(g.n_seg):
         og.n_seg[k] = n
     n, on = c.numerics, oc.numerics
+    if on.scheme.kind == o.SCHEME_IMPLICIT and n.scheme.cfl_max != on.scheme.cfl_max:  # a preset whose CFL limit was changed
+        on.scheme.cfl_max = n.scheme.cfl_max
     assert (on.max_iter, on.first_order_iters, on.limiter, bool(on.low_mach)) == (n.max_iter, n.first_order_iters, n.limiter,
                                                                                   bool(n.low_mach))
     return oc
