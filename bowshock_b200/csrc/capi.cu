@@ -10,6 +10,7 @@
 #include "multigrid.cuh"
 #include "host_arena.cuh"
 #include "mesher.cuh"
+#include "host3.cuh"
 
 using namespace bk;
 
@@ -841,3 +842,128 @@ extern "C" int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, doubl
       if (!std::isfinite(residual[k])) return fail(s, BOWSHOCK_NONFINITE, "non-finite residual at iteration " + std::to_string(k));
   return BOWSHOCK_OK;
 }
+
+// ============================================================================ 3D Euler batch
+struct bowshock3_batch {
+  bk3::Batch3 b;
+  std::string last_error;
+};
+static int b3from(bowshock3_batch* h, int rc) {
+  if (rc) h->last_error = h->b.err;
+  return rc;
+}
+extern "C" {
+int bowshock3_create(uint64_t ni, uint64_t nj, uint64_t nk, const double* x, const double* y, const double* z, uint64_t axis_cells,
+                     uint64_t ncases, const bowshock3_config* cfg, int device, bowshock3_batch** out) {
+  if (!x || !y || !z || !cfg || !out || ncases == 0) return BOWSHOCK_INVALID;
+  *out = nullptr;
+  std::vector<bk3::Case3Host> cs(ncases);
+  for (uint64_t k = 0; k < ncases; ++k) {
+    const bowshock3_config& c = cfg[k];
+    if (c.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT && c.scheme.kind != BOWSHOCK_SCHEME_EXPLICIT) return BOWSHOCK_UNSUPPORTED;
+    if (c.scheme.kind != cfg[0].scheme.kind) return BOWSHOCK_UNSUPPORTED;  // one scheme per batch
+    if (!(c.mach > 0.0) || c.limiter < 0 || c.limiter > 3) return BOWSHOCK_INVALID;
+    bk3::Case3Host& h = cs[k];
+    h.mach = c.mach, h.alpha = c.alpha, h.cfl = c.cfl, h.limiter = c.limiter, h.low_mach = c.low_mach != 0;
+    h.first_order_iters = (long long)c.first_order_iters;
+    h.implicit = c.scheme.kind == BOWSHOCK_SCHEME_IMPLICIT;
+    h.cfl0 = c.scheme.cfl0, h.cfl_max = c.scheme.cfl_max, h.growth = c.scheme.growth, h.eps_fix = c.scheme.eps_fix;
+    h.dt_mode = c.scheme.dt_mode, h.sub_iters = (int)std::max<uint64_t>(c.scheme.sub_iters, 1), h.roe = c.scheme.roe != 0;
+    h.implicit_bc = c.scheme.implicit_bc != 0, h.lines = c.scheme.lines != 0;
+  }
+  auto* h = new bowshock3_batch();
+  int rc = h->b.create(ni, nj, nk, x, y, z, axis_cells, cs, device);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return BOWSHOCK_OK;
+}
+void bowshock3_destroy(bowshock3_batch* b) { delete b; }
+const char* bowshock3_last_error(const bowshock3_batch* b) { return b ? b->last_error.c_str() : "null handle"; }
+int bowshock3_reset(bowshock3_batch* b) { return b ? b3from(b, b->b.reset()) : BOWSHOCK_INVALID; }
+int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp) {
+  return b ? b3from(b, b->b.set_counters((int)std::min<uint64_t>(iter, 1u << 30), (int)std::min<uint64_t>(ramp, 1u << 30))) : BOWSHOCK_INVALID;
+}
+int bowshock3_set_state(bowshock3_batch* b, uint64_t k, const double* u) {
+  if (!b || !u || k >= (uint64_t)b->b.B.nb) return BOWSHOCK_INVALID;
+  return b3from(b, b->b.set_state((int)k, u));
+}
+int bowshock3_state(bowshock3_batch* b, uint64_t k, double* u) {
+  if (!b || !u || k >= (uint64_t)b->b.B.nb) return BOWSHOCK_INVALID;
+  return b3from(b, b->b.get_state((int)k, u));
+}
+int bowshock3_run(bowshock3_batch* b, uint64_t n, double* residual) {
+  if (!b) return BOWSHOCK_INVALID;
+  int rc = b->b.run((long long)n, residual);
+  if (rc) return b3from(b, rc);
+  return BOWSHOCK_OK;
+}
+int bowshock3_eval_residual(bowshock3_batch* b, uint64_t k, double* res, double* dt, double* density_residual) {
+  if (!b || k >= (uint64_t)b->b.B.nb) return BOWSHOCK_INVALID;
+  std::vector<double> dens;
+  int rc = b->b.eval_residual(dens);
+  if (!rc) rc = b->b.read_residual((int)k, res, dt);
+  if (rc) return b3from(b, rc);
+  if (density_residual) *density_residual = dens[k];
+  return BOWSHOCK_OK;
+}
+int bowshock3_forces(bowshock3_batch* b, double x_max, double* out) {
+  if (!b || !out) return BOWSHOCK_INVALID;
+  std::vector<double> f;
+  int rc = b->b.forces(x_max, f);
+  if (rc) return b3from(b, rc);
+  std::memcpy(out, f.data(), f.size() * sizeof(double));
+  return BOWSHOCK_OK;
+}
+int bowshock3_solve(bowshock3_batch* b, const bowshock3_run_params* p, bowshock3_result* out) {
+  if (!b || !p || !out) return BOWSHOCK_INVALID;
+  bk3::Batch3& B = b->b;
+  const int nb = B.B.nb;
+  int rc = B.reset();
+  if (rc) return b3from(b, rc);
+  std::vector<bk3::StopRule3> rules(nb);
+  for (auto& r : rules) r.window = p->window, r.nwin = std::max<size_t>(p->window / 50, 1), r.rel_tol = p->rel_tol;
+  std::vector<int> act(nb, 1);
+  std::vector<uint64_t> its(nb, 0);
+  if ((rc = B.set_active(act))) return b3from(b, rc);
+  std::vector<double> res(50 * (size_t)nb), f;
+  uint64_t done_it = 0;
+  while (true) {
+    int left = 0;
+    for (int k = 0; k < nb; ++k) left += act[k];
+    if (!left || done_it >= p->max_iter) break;
+    int chunk = (int)std::min<uint64_t>(50, p->max_iter - done_it);
+    if ((rc = B.run(chunk, res.data()))) return b3from(b, rc);
+    if ((rc = B.forces(p->x_max, f))) return b3from(b, rc);
+    bool changed = false;
+    for (int k = 0; k < nb; ++k) {
+      if (!act[k]) continue;
+      for (int t = 0; t < chunk && act[k]; ++t) {
+        size_t it = (size_t)(done_it + t);
+        bool sampled = (it + 1) % 50 == 0;
+        its[k] = it + 1;
+        if (rules[k].check(it, res[(size_t)t * nb + k], sampled, f[3 * k])) act[k] = 0, changed = true;
+      }
+    }
+    done_it += chunk;
+    if (changed && (rc = B.set_active(act))) return b3from(b, rc);
+  }
+  if ((rc = B.forces(p->x_max, f))) return b3from(b, rc);
+  for (int k = 0; k < nb; ++k) {
+    bowshock3_result& o = out[k];
+    o.cn = f[3 * k], o.ca = f[3 * k + 1], o.x_cp = f[3 * k + 2];
+    o.iterations = its[k];
+    o.stop_reason = rules[k].reason;
+    o.drop_orders = rules[k].rmax > 0.0 && rules[k].r > 0.0 ? std::log10(rules[k].rmax / rules[k].r) : 0.0;
+  }
+  std::vector<int> all(nb, 1);
+  return b3from(b, B.set_active(all));
+}
+int bowshock3_last_ms_per_iter(const bowshock3_batch* b, double* ms) {
+  if (!b || !ms) return BOWSHOCK_INVALID;
+  *ms = b->b.last_ms_per_iter;
+  return BOWSHOCK_OK;
+}
+}  // extern "C"

@@ -1,0 +1,751 @@
+// 3D Euler path (crates/bowshock-cfd/src/{gas3,bc3,flux3,grid3,solver3,implicit3}.rs; forces and stop rules of
+// crates/bowshock-core/src/engine/run3.rs) on the B200: a batch of cases (Mach number, incidence) that share one revolved
+// grid, so the geometry is stored once and read through L2 by every case. Per case the state is SoA FP32 planes
+// [case][var][cell]; the face fluxes and the cell residual are evaluated in FP64 from the FP32 primitives; the three-factor
+// line-implicit operator (5x5 blocks, Roe |A| with the entropy fix, shock-sensor blend) is assembled in registers and
+// solved one thread per line (block Thomas), i then j then k, with defect-correction passes.
+//   k3_prims      conserved -> primitive (padded, 2 ghost layers)                    (solver3.rs:222-236)
+//   k3_ghosts     characteristic far field (FP64), axis (the cell across the axis), slip wall, symmetry planes (solver3.rs:171-219)
+//   k3_flux       MUSCL in the face's cylindrical frame + HLLC / Rusanov blend + low-Mach correction, FP64 (flux3.rs, solver3.rs:365-418)
+//   k3_residual   R = -(1/V) sum S F (FP64 accumulation), local time step, FP64 density norm (solver3.rs:251-300)
+//   k3_lines      (I - dt J_dir) x = b along every line of direction dir (implicit3.rs:274-382)
+//   k3_defect     dt R - (A_i du + A_j du + A_k du - 2 du)                            (implicit3.rs:384-455)
+//   k3_stage      SSP-RK3 stage                                                       (solver3.rs:303-327)
+//   k3_forces     FP64 wall-pressure force integration: CN, CA, centre of pressure     (run3.rs:150-190)
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "device_math.cuh"
+
+namespace bk3 {
+using bk::LIM_FIRST;
+using bk::LIM_MINMOD;
+using bk::limited_slope;
+using bk::shock_weight;
+
+constexpr double GD = 1.4;
+
+template <typename T>
+struct V5 {
+  T v[5];
+  __host__ __device__ __forceinline__ T& operator[](int k) { return v[k]; }
+  __host__ __device__ __forceinline__ const T& operator[](int k) const { return v[k]; }
+};
+template <typename T>
+struct M5 {
+  T a[25];
+  __host__ __device__ __forceinline__ T& operator[](int k) { return a[k]; }
+  __host__ __device__ __forceinline__ const T& operator[](int k) const { return a[k]; }
+};
+template <typename T>
+__device__ __forceinline__ V5<T> cons_to_prim3(const V5<T>& q) {  // gas3.rs:20-25
+  T rho = q[0];
+  T u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+  T p = (T)(GD - 1.0) * (q[4] - (T)0.5 * rho * (u * u + v * v + w * w));
+  return V5<T>{{rho, u, v, w, p}};
+}
+template <typename T>
+__device__ __forceinline__ V5<T> prim_to_cons3(const V5<T>& w) {  // gas3.rs:14-17
+  return V5<T>{{w[0], w[0] * w[1], w[0] * w[2], w[0] * w[3], w[4] / (T)(GD - 1.0) + (T)0.5 * w[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3])}};
+}
+template <typename T>
+__device__ __forceinline__ V5<T> physical_flux3(const V5<T>& w, T nx, T ny, T nz) {  // gas3.rs:34-39
+  T un = w[1] * nx + w[2] * ny + w[3] * nz;
+  T e = w[4] / (T)(GD - 1.0) + (T)0.5 * w[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+  return V5<T>{{w[0] * un, w[0] * w[1] * un + w[4] * nx, w[0] * w[2] * un + w[4] * ny, w[0] * w[3] * un + w[4] * nz, (e + w[4]) * un}};
+}
+template <typename T>
+__device__ __forceinline__ V5<T> reflect3(const V5<T>& w, T nx, T ny, T nz) {  // gas3.rs:48-51
+  T un = w[1] * nx + w[2] * ny + w[3] * nz;
+  return V5<T>{{w[0], w[1] - (T)2 * un * nx, w[2] - (T)2 * un * ny, w[3] - (T)2 * un * nz, w[4]}};
+}
+__device__ __forceinline__ V5<double> char_ghost3(const V5<double>& fs, const V5<double>& in, double nx, double ny, double nz) {  // bc3.rs:30-56
+  double ci = sqrt(GD * in[4] / in[0]);
+  double uni = in[1] * nx + in[2] * ny + in[3] * nz;
+  double m = uni / ci;
+  if (m <= -1.0) return fs;
+  if (m >= 1.0) return in;
+  const double g1 = GD - 1.0;
+  double ce = sqrt(GD * fs[4] / fs[0]);
+  double une = fs[1] * nx + fs[2] * ny + fs[3] * nz;
+  double r_out = uni + 2.0 * ci / g1, r_in = une - 2.0 * ce / g1;
+  double un_b = 0.5 * (r_out + r_in);
+  double c_b = fmax(0.25 * g1 * (r_out - r_in), 1e-8);
+  const V5<double>& rf = un_b >= 0.0 ? in : fs;
+  double un_ref = un_b >= 0.0 ? uni : une;
+  double s = rf[4] / pow(rf[0], GD);
+  double rho = pow(c_b * c_b / (GD * s), 1.0 / g1);
+  double p = rho * c_b * c_b / GD;
+  double dn = un_b - un_ref;
+  return V5<double>{{rho, rf[1] + dn * nx, rf[2] + dn * ny, rf[3] + dn * nz, p}};
+}
+// flux3.rs:27-54: MUSCL with the lateral velocity limited in the face's cylindrical frame (s, co)
+__device__ __forceinline__ void reconstruct3(const V5<double>& m2, const V5<double>& m1, const V5<double>& p0, const V5<double>& p1, int lim,
+                                             double s, double co, V5<double>& lo, V5<double>& ro) {
+  auto fwd = [&](const V5<double>& w) { return V5<double>{{w[0], w[1], w[2] * s + w[3] * co, w[2] * co - w[3] * s, w[4]}}; };
+  V5<double> a = fwd(m2), b = fwd(m1), c = fwd(p0), d = fwd(p1);
+  V5<double> l = b, r = c;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    l[k] = b[k] + 0.5 * limited_slope<double>(b[k] - a[k], c[k] - b[k], lim);
+    r[k] = c[k] - 0.5 * limited_slope<double>(c[k] - b[k], d[k] - c[k], lim);
+  }
+  if (l[0] <= 0.0 || l[4] <= 0.0) l = b;
+  if (r[0] <= 0.0 || r[4] <= 0.0) r = c;
+  bool lb = true, rc = true;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) lb = lb && l[k] == b[k], rc = rc && r[k] == c[k];
+  lo = lb ? m1 : V5<double>{{l[0], l[1], l[2] * s + l[3] * co, l[2] * co - l[3] * s, l[4]}};
+  ro = rc ? p0 : V5<double>{{r[0], r[1], r[2] * s + r[3] * co, r[2] * co - r[3] * s, r[4]}};
+}
+__device__ __forceinline__ V5<double> hllc3(const V5<double>& wl, const V5<double>& wr, double nx, double ny, double nz) {  // flux3.rs:59-117
+  double rl = wl[0], ul = wl[1], vl = wl[2], zl = wl[3], pl = wl[4];
+  double rr = wr[0], ur = wr[1], vr = wr[2], zr = wr[3], pr = wr[4];
+  double unl = ul * nx + vl * ny + zl * nz, unr = ur * nx + vr * ny + zr * nz;
+  double cl = sqrt(GD * pl / rl), cr = sqrt(GD * pr / rr);
+  double el = pl / (GD - 1.0) + 0.5 * rl * (ul * ul + vl * vl + zl * zl);
+  double er = pr / (GD - 1.0) + 0.5 * rr * (ur * ur + vr * vr + zr * zr);
+  double sql = sqrt(rl), sqr = sqrt(rr), inv = 1.0 / (sql + sqr);
+  double uh = (sql * ul + sqr * ur) * inv, vh = (sql * vl + sqr * vr) * inv, wh = (sql * zl + sqr * zr) * inv;
+  double hh = (sql * ((el + pl) / rl) + sqr * ((er + pr) / rr)) * inv;
+  double ch = sqrt(fmax((GD - 1.0) * (hh - 0.5 * (uh * uh + vh * vh + wh * wh)), 1e-300));
+  double unh = uh * nx + vh * ny + wh * nz;
+  double sl = fmin(unl - cl, unh - ch), sr = fmax(unr + cr, unh + ch);
+  if (sl >= 0.0) return physical_flux3<double>(wl, nx, ny, nz);
+  if (sr <= 0.0) return physical_flux3<double>(wr, nx, ny, nz);
+  double sm = (pr - pl + rl * unl * (sl - unl) - rr * unr * (sr - unr)) / (rl * (sl - unl) - rr * (sr - unr));
+  V5<double> out;
+  if (sm >= 0.0) {
+    V5<double> f = physical_flux3<double>(wl, nx, ny, nz);
+    double fac = rl * (sl - unl) / (sl - sm), d = sm - unl;
+    double st[5] = {fac, fac * (ul + d * nx), fac * (vl + d * ny), fac * (zl + d * nz), fac * (el / rl + d * (sm + pl / (rl * (sl - unl))))};
+    double q[5] = {rl, rl * ul, rl * vl, rl * zl, el};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = f[k] + sl * (st[k] - q[k]);
+  } else {
+    V5<double> f = physical_flux3<double>(wr, nx, ny, nz);
+    double fac = rr * (sr - unr) / (sr - sm), d = sm - unr;
+    double st[5] = {fac, fac * (ur + d * nx), fac * (vr + d * ny), fac * (zr + d * nz), fac * (er / rr + d * (sm + pr / (rr * (sr - unr))))};
+    double q[5] = {rr, rr * ur, rr * vr, rr * zr, er};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = f[k] + sr * (st[k] - q[k]);
+  }
+  return out;
+}
+__device__ __forceinline__ V5<double> rusanov3(const V5<double>& wl, const V5<double>& wr, double nx, double ny, double nz) {  // flux3.rs:121-135
+  double unl = wl[1] * nx + wl[2] * ny + wl[3] * nz, unr = wr[1] * nx + wr[2] * ny + wr[3] * nz;
+  double smax = fmax(fabs(unl) + sqrt(GD * wl[4] / wl[0]), fabs(unr) + sqrt(GD * wr[4] / wr[0]));
+  V5<double> fl = physical_flux3<double>(wl, nx, ny, nz), fr = physical_flux3<double>(wr, nx, ny, nz);
+  V5<double> ql = prim_to_cons3<double>(wl), qr = prim_to_cons3<double>(wr);
+  V5<double> out;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) out[k] = 0.5 * (fl[k] + fr[k]) - 0.5 * smax * (qr[k] - ql[k]);
+  return out;
+}
+__device__ __forceinline__ V5<double> face_flux_lm3(const V5<double>& m2, const V5<double>& m1, const V5<double>& p0, const V5<double>& p1,
+                                                    int lim, double nx, double ny, double nz, double s, double co, bool low_mach) {
+  V5<double> l, r;
+  reconstruct3(m2, m1, p0, p1, lim, s, co, l, r);
+  if (low_mach) {  // flux3.rs:163-176
+    double unl = l[1] * nx + l[2] * ny + l[3] * nz, unr = r[1] * nx + r[2] * ny + r[3] * nz;
+    double ml = sqrt(l[1] * l[1] + l[2] * l[2] + l[3] * l[3]) / sqrt(GD * l[4] / l[0]);
+    double mr = sqrt(r[1] * r[1] + r[2] * r[2] + r[3] * r[3]) / sqrt(GD * r[4] / r[0]);
+    double z = fmin(fmax(fmax(ml, mr), 0.05), 1.0);
+    if (z < 1.0) {
+      double avg = 0.5 * (unl + unr);
+      double dl = avg + z * (unl - avg) - unl, dr = avg + z * (unr - avg) - unr;
+      l[1] += dl * nx, l[2] += dl * ny, l[3] += dl * nz;
+      r[1] += dr * nx, r[2] += dr * ny, r[3] += dr * nz;
+    }
+  }
+  V5<double> c = hllc3(l, r, nx, ny, nz);  // flux3.rs:146-158
+  double t = shock_weight<double>(m1[4], p0[4]);
+  if (t == 0.0) return c;
+  V5<double> f = rusanov3(l, r, nx, ny, nz);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) c[k] = (1.0 - t) * c[k] + t * f[k];
+  return c;
+}
+
+// ---------------------------------------------------------------- 5x5 blocks (implicit3.rs)
+__device__ __forceinline__ M5<float> zero5() {
+  M5<float> m;
+#pragma unroll
+  for (int k = 0; k < 25; ++k) m[k] = 0.f;
+  return m;
+}
+__device__ __forceinline__ M5<float> eye5() {
+  M5<float> m = zero5();
+#pragma unroll
+  for (int q = 0; q < 5; ++q) m[6 * q] = 1.f;
+  return m;
+}
+__device__ __forceinline__ M5<float> flux_jacobian3(const V5<float>& w, float nx, float ny, float nz) {  // implicit3.rs:44-60
+  const float G = 1.4f, g1 = 0.4f;
+  float rho = w[0], u = w[1], v = w[2], ww = w[3], p = w[4];
+  float q2 = u * u + v * v + ww * ww, th = u * nx + v * ny + ww * nz, phi = 0.5f * g1 * q2, h = G * p / (g1 * rho) + 0.5f * q2;
+  return M5<float>{{0.f, nx, ny, nz, 0.f,                                                                                   //
+                    phi * nx - u * th, th + (2.f - G) * u * nx, u * ny - g1 * v * nx, u * nz - g1 * ww * nx, g1 * nx,        //
+                    phi * ny - v * th, v * nx - g1 * u * ny, th + (2.f - G) * v * ny, v * nz - g1 * ww * ny, g1 * ny,        //
+                    phi * nz - ww * th, ww * nx - g1 * u * nz, ww * ny - g1 * v * nz, th + (2.f - G) * ww * nz, g1 * nz,     //
+                    th * (phi - h), h * nx - g1 * u * th, h * ny - g1 * v * th, h * nz - g1 * ww * th, G * th}};
+}
+__device__ __forceinline__ M5<float> mm5(const M5<float>& a, const M5<float>& b) {
+  M5<float> c;
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      float s = 0.f;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) s += a[5 * i + k] * b[5 * k + j];
+      c[5 * i + j] = s;
+    }
+  return c;
+}
+__device__ __forceinline__ V5<float> mv5(const M5<float>& a, const V5<float>& x) {
+  V5<float> y;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) y[i] = a[5 * i] * x[0] + a[5 * i + 1] * x[1] + a[5 * i + 2] * x[2] + a[5 * i + 3] * x[3] + a[5 * i + 4] * x[4];
+  return y;
+}
+__device__ __forceinline__ void axpy5(M5<float>& a, float s, const M5<float>& b) {
+#pragma unroll
+  for (int k = 0; k < 25; ++k) a[k] += s * b[k];
+}
+// Gauss-Jordan with partial pivoting (implicit3.rs:94-125), register-resident: row swaps by selects
+__device__ __forceinline__ M5<float> inv5(const M5<float>& m) {
+  float a[5][5], v[5][5];
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) a[r][c] = m[5 * r + c], v[r][c] = r == c ? 1.f : 0.f;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    int piv = c;
+    float best = fabsf(a[c][c]);
+#pragma unroll
+    for (int r = c + 1; r < 5; ++r) {
+      float x = fabsf(a[r][c]);
+      if (x > best) best = x, piv = r;
+    }
+#pragma unroll
+    for (int r = c + 1; r < 5; ++r) {
+      bool sw = piv == r;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        float t0 = a[c][k], t1 = a[r][k], u0 = v[c][k], u1 = v[r][k];
+        a[c][k] = sw ? t1 : t0, a[r][k] = sw ? t0 : t1;
+        v[c][k] = sw ? u1 : u0, v[r][k] = sw ? u0 : u1;
+      }
+    }
+    float d = 1.f / a[c][c];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) a[c][k] *= d, v[c][k] *= d;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      if (r == c) continue;
+      float f = a[r][c];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) a[r][k] -= f * a[c][k], v[r][k] -= f * v[c][k];
+    }
+  }
+  M5<float> out;
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) out[5 * r + c] = v[r][c];
+  return out;
+}
+__device__ __forceinline__ M5<float> abs_jacobian3(const V5<float>& wl, const V5<float>& wr, float nx, float ny, float nz, float eps_fix) {
+  const float G = 1.4f, g1 = 0.4f;  // implicit3.rs:160-193
+  float sl = sqrtf(wl[0]), sr = sqrtf(wr[0]), inv = 1.f / (sl + sr);
+  float u = (sl * wl[1] + sr * wr[1]) * inv, v = (sl * wl[2] + sr * wr[2]) * inv, ww = (sl * wl[3] + sr * wr[3]) * inv;
+  float hl = G * wl[4] / (g1 * wl[0]) + 0.5f * (wl[1] * wl[1] + wl[2] * wl[2] + wl[3] * wl[3]);
+  float hr = G * wr[4] / (g1 * wr[0]) + 0.5f * (wr[1] * wr[1] + wr[2] * wr[2] + wr[3] * wr[3]);
+  float h = (sl * hl + sr * hr) * inv, q2h = 0.5f * (u * u + v * v + ww * ww);
+  float c = sqrtf(fmaxf(g1 * (h - q2h), 1e-30f));
+  float a = u * nx + v * ny + ww * nz, eps = eps_fix * c;
+  auto fix = [&](float l) { return fabsf(l) >= eps ? fabsf(l) : 0.5f * (l * l / eps + eps); };
+  float e1 = fix(a), e2 = fix(a + c), e3 = fix(a - c);
+  float d1 = (e2 - e1) / c, d2 = (e2 + e3 - 2.f * e1) / (2.f * c * c);
+  V5<float> wa{{1.f, u, v, ww, g1 / G * (h - q2h)}};
+  M5<float> b1 = flux_jacobian3(wa, nx, ny, nz), b2 = b1;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) b1[6 * q] -= a, b2[6 * q] -= a + c;
+  M5<float> prod = mm5(b1, b2);
+#pragma unroll
+  for (int k = 0; k < 25; ++k) prod[k] = d1 * b1[k] + d2 * prod[k];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) prod[6 * q] += e1;
+  return prod;
+}
+__device__ __forceinline__ float spectral3(const V5<float>& w, float nx, float ny, float nz) {
+  return fabsf(w[1] * nx + w[2] * ny + w[3] * nz) + sqrtf(1.4f * w[4] / w[0]);
+}
+__device__ __forceinline__ M5<float> reflection3(float nx, float ny, float nz) {  // implicit3.rs:202-210
+  M5<float> m = eye5();
+  float n[3] = {nx, ny, nz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) m[5 * (1 + a) + 1 + b] -= 2.f * n[a] * n[b];
+  return m;
+}
+
+// ---------------------------------------------------------------- batch layout
+struct Case3Dev {
+  double fs[5];
+  float cfl, cfl0, cfl_max, growth, eps_fix;
+  int limiter, low_mach, first_order_iters, implicit, dt_mode, sub_iters, roe, implicit_bc, lines;
+};
+
+struct B3 {
+  int ni, nj, nk, nb, axis_cells;
+  long long nc, npad, nfi, nfj, nfk;
+  const float4 *fi, *fj, *fk;  // (nx, ny, nz, area)
+  const float2 *ri, *rj, *rk;  // face_rot (s, co)
+  const float* vol;
+  const int* axis_k;  // [i * nk + k], i < axis_cells
+  const Case3Dev* cs;
+  int *iter, *ramp, *active;
+  float *U, *U0, *W, *R, *X, *DU, *RR, *dt, *scr;  // [case][var][cell]; W [case][var][padded]; scr [case][30][cell]
+  double *FI, *FJ, *FK;                             // face flux x area, [case][var][face]
+  double* rsum;                                     // [slot][case]
+};
+
+__device__ __forceinline__ long long pidx3(const B3& B, int i, int j, int k) {
+  return ((long long)(k + 2) * (B.nj + 4) + (j + 2)) * (B.ni + 4) + (i + 2);
+}
+__device__ __forceinline__ long long cell3(const B3& B, int i, int j, int k) { return ((long long)k * B.nj + j) * B.ni + i; }
+__device__ __forceinline__ V5<float> ldU(const B3& B, const float* a, int b, long long c) {
+  const float* p = a + (long long)b * 5 * B.nc + c;
+  return V5<float>{{p[0], p[B.nc], p[2 * B.nc], p[3 * B.nc], p[4 * B.nc]}};
+}
+__device__ __forceinline__ void stU(const B3& B, float* a, int b, long long c, const V5<float>& v) {
+  float* p = a + (long long)b * 5 * B.nc + c;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) p[q * B.nc] = v[q];
+}
+__device__ __forceinline__ V5<float> ldW(const B3& B, int b, long long pi) {
+  const float* p = B.W + (long long)b * 5 * B.npad + pi;
+  return V5<float>{{p[0], p[B.npad], p[2 * B.npad], p[3 * B.npad], p[4 * B.npad]}};
+}
+__device__ __forceinline__ void stW(const B3& B, int b, long long pi, const V5<double>& v) {
+  float* p = B.W + (long long)b * 5 * B.npad + pi;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) p[q * B.npad] = (float)v[q];
+}
+__device__ __forceinline__ V5<double> f2d5(const V5<float>& v) { return V5<double>{{v[0], v[1], v[2], v[3], v[4]}}; }
+__device__ __forceinline__ V5<double> fs3(const Case3Dev& c) { return V5<double>{{c.fs[0], c.fs[1], c.fs[2], c.fs[3], c.fs[4]}}; }
+
+// ---------------------------------------------------------------- kernels
+__global__ void k3_prims(B3 B) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (t >= B.nc || !B.active[b]) return;
+  int i = (int)(t % B.ni), j = (int)((t / B.ni) % B.nj), k = (int)(t / ((long long)B.ni * B.nj));
+  V5<float> w = cons_to_prim3<float>(ldU(B, B.U, b, t));
+  stW(B, b, pidx3(B, i, j, k), f2d5(w));
+}
+
+// ghosts of every boundary face column: i ends, j = 0 (axis or slip wall), j = nj, k ends (symmetry planes)
+__global__ void k3_ghosts(B3 B) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (!B.active[b]) return;
+  const Case3Dev& c = B.cs[b];
+  const long long njk = (long long)B.nj * B.nk, nik = (long long)B.ni * B.nk, nij = (long long)B.ni * B.nj;
+  if (t < 2 * njk) {  // i ends: characteristic far field (FP64)
+    bool hi = t >= njk;
+    long long q = hi ? t - njk : t;
+    int j = (int)(q % B.nj), k = (int)(q / B.nj);
+    long long f = ((long long)k * B.nj + j) * (B.ni + 1) + (hi ? B.ni : 0);
+    float4 n = B.fi[f];
+    double o = hi ? 1.0 : -1.0;
+    V5<double> g = char_ghost3(fs3(c), f2d5(ldW(B, b, pidx3(B, hi ? B.ni - 1 : 0, j, k))), o * n.x, o * n.y, o * n.z);
+    for (int m = 1; m <= 2; ++m) stW(B, b, pidx3(B, hi ? B.ni + m - 1 : -m, j, k), g);
+    return;
+  }
+  t -= 2 * njk;
+  if (t < nik) {  // j = 0: the axis (the cell across it, lateral velocity mirrored) or the slip wall
+    int i = (int)(t % B.ni), k = (int)(t / B.ni);
+    if (i < B.axis_cells) {
+      int kp = B.axis_k[i * B.nk + k];
+      for (int m = 1; m <= 2; ++m) {
+        V5<float> s = ldW(B, b, pidx3(B, i, m - 1, kp));
+        s[2] = -s[2];
+        stW(B, b, pidx3(B, i, -m, k), f2d5(s));
+      }
+    } else {
+      float4 n = B.fj[((long long)k * (B.nj + 1)) * B.ni + i];
+      for (int m = 1; m <= 2; ++m)
+        stW(B, b, pidx3(B, i, -m, k), reflect3<double>(f2d5(ldW(B, b, pidx3(B, i, m - 1, k))), n.x, n.y, n.z));
+    }
+    return;
+  }
+  t -= nik;
+  if (t < nik) {  // j = nj: characteristic far field
+    int i = (int)(t % B.ni), k = (int)(t / B.ni);
+    float4 n = B.fj[((long long)k * (B.nj + 1) + B.nj) * B.ni + i];
+    V5<double> g = char_ghost3(fs3(c), f2d5(ldW(B, b, pidx3(B, i, B.nj - 1, k))), n.x, n.y, n.z);
+    for (int m = 1; m <= 2; ++m) stW(B, b, pidx3(B, i, B.nj + m - 1, k), g);
+    return;
+  }
+  t -= nik;
+  if (t < 2 * nij) {  // k ends: symmetry planes
+    bool hi = t >= nij;
+    long long q = hi ? t - nij : t;
+    int i = (int)(q % B.ni), j = (int)(q / B.ni);
+    float4 n = B.fk[(hi ? (long long)B.nk * nij : 0) + (long long)j * B.ni + i];
+    for (int m = 1; m <= 2; ++m) {
+      int src = hi ? B.nk - m : m - 1, dst = hi ? B.nk + m - 1 : -m;
+      stW(B, b, pidx3(B, i, j, dst), reflect3<double>(f2d5(ldW(B, b, pidx3(B, i, j, src))), n.x, n.y, n.z));
+    }
+  }
+}
+
+// face fluxes of direction dir (0 i, 1 j, 2 k), FP64, times the face area
+__global__ void k3_flux(B3 B, int dir) {
+  long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  const long long nf = dir == 0 ? B.nfi : dir == 1 ? B.nfj : B.nfk;
+  if (f >= nf || !B.active[b]) return;
+  const Case3Dev& c = B.cs[b];
+  const int nfi = B.ni + (dir == 0), nfj = B.nj + (dir == 1);
+  int i = (int)(f % nfi), j = (int)((f / nfi) % nfj), k = (int)(f / ((long long)nfi * nfj));
+  float4 n = dir == 0 ? B.fi[f] : dir == 1 ? B.fj[f] : B.fk[f];
+  double* out = (dir == 0 ? B.FI : dir == 1 ? B.FJ : B.FK) + (long long)b * 5 * nf + f;
+  if (n.w == 0.f) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) out[q * nf] = 0.0;
+    return;
+  }
+  float2 rot = dir == 0 ? B.ri[f] : dir == 1 ? B.rj[f] : B.rk[f];
+  int ei = dir == 0, ej = dir == 1, ek = dir == 2;
+  auto at = [&](int s) { return f2d5(ldW(B, b, pidx3(B, i + s * ei, j + s * ej, k + s * ek))); };
+  int lim = B.iter[b] < c.first_order_iters ? LIM_FIRST : c.limiter;
+  V5<double> fl = face_flux_lm3(at(-2), at(-1), at(0), at(1), lim, n.x, n.y, n.z, rot.x, rot.y, c.low_mach != 0);
+  double area = n.w;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) out[q * nf] = fl[q] * area;
+}
+
+// cell residual (FP64 sums, stored FP32), the local time step (dt_kind 1 explicit CFL, 2 implicit ramp), the density norm
+__global__ void k3_residual(B3 B, int dt_kind, int slot) {
+  __shared__ double sred[8];
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (!B.active[b]) return;
+  const Case3Dev& cs = B.cs[b];
+  double rr = 0.0;
+  if (c < B.nc) {
+    int i = (int)(c % B.ni), j = (int)((c / B.ni) % B.nj), k = (int)(c / ((long long)B.ni * B.nj));
+    long long il = ((long long)k * B.nj + j) * (B.ni + 1) + i, jl = ((long long)k * (B.nj + 1) + j) * B.ni + i, kl = c;
+    long long ir = il + 1, jr = jl + B.ni, kr = c + (long long)B.ni * B.nj;
+    const double *FI = B.FI + (long long)b * 5 * B.nfi, *FJ = B.FJ + (long long)b * 5 * B.nfj, *FK = B.FK + (long long)b * 5 * B.nfk;
+    double inv_v = 1.0 / (double)B.vol[c];
+    V5<float> r;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double s = -((FI[q * B.nfi + ir] - FI[q * B.nfi + il]) + (FJ[q * B.nfj + jr] - FJ[q * B.nfj + jl]) + (FK[q * B.nfk + kr] - FK[q * B.nfk + kl])) * inv_v;
+      r[q] = (float)s;
+      if (q == 0) rr = s * s;
+    }
+    stU(B, B.R, b, c, r);
+    if (dt_kind) {
+      V5<float> w = ldW(B, b, pidx3(B, i, j, k));
+      float csnd = sqrtf(1.4f * w[4] / w[0]);
+      auto lam = [&](float4 f) { return (fabsf(w[1] * f.x + w[2] * f.y + w[3] * f.z) + csnd) * f.w; };
+      float li = 0.5f * (lam(B.fi[il]) + lam(B.fi[ir])), lj = 0.5f * (lam(B.fj[jl]) + lam(B.fj[jr])), lk = 0.5f * (lam(B.fk[kl]) + lam(B.fk[kr]));
+      float cfl = cs.cfl;
+      int mode = 0;
+      if (dt_kind == 2) {
+        int rk = B.ramp[b];
+        cfl = (float)fmin((double)cs.cfl0 * pow((double)cs.growth, (double)(rk < 10000 ? rk : 10000)), (double)cs.cfl_max);
+        mode = cs.dt_mode;
+      }
+      float v = B.vol[c];
+      B.dt[(long long)b * B.nc + c] = mode == 0 ? cfl * v / (li + lj + lk) : cfl * v / (3.f * fminf(fminf(li, lj), lk));
+    }
+  }
+  if (slot >= 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rr += __shfl_down_sync(0xffffffffu, rr, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = rr;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sred[q];
+      atomicAdd(&B.rsum[(long long)slot * B.nb + b], s);
+    }
+  }
+}
+
+__global__ void k3_stage(B3 B, float a, float bb, int copy, int last) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (c >= B.nc || !B.active[b]) return;
+  if (last && c == 0) B.iter[b] += 1;
+  V5<float> u = ldU(B, B.U, b, c);
+  if (copy) stU(B, B.U0, b, c, u);
+  V5<float> u0 = copy ? u : ldU(B, B.U0, b, c);
+  V5<float> r = ldU(B, B.R, b, c);
+  float d = B.dt[(long long)b * B.nc + c];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) u[q] = a * (u[q] + d * r[q]) + bb * u0[q];
+  stU(B, B.U, b, c, u);
+}
+
+// blocks (lo, d, up) of I - dt J_dir of cell (i, j, k) with the line-end ghost Jacobians folded in (implicit3.rs:214-355)
+__device__ void blocks3(const B3& B, int b, int dir, int i, int j, int k, M5<float>& lo, M5<float>& d, M5<float>& up) {
+  const Case3Dev& cs = B.cs[b];
+  const int ei = dir == 0, ej = dir == 1, ek = dir == 2;
+  const int m = dir == 0 ? i : dir == 1 ? j : k, nl = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
+  const long long c = cell3(B, i, j, k);
+  float4 fl, fr;
+  if (dir == 0) {
+    long long il = ((long long)k * B.nj + j) * (B.ni + 1) + i;
+    fl = B.fi[il], fr = B.fi[il + 1];
+  } else if (dir == 1) {
+    long long jl = ((long long)k * (B.nj + 1) + j) * B.ni + i;
+    fl = B.fj[jl], fr = B.fj[jl + B.ni];
+  } else {
+    fl = B.fk[c], fr = B.fk[c + (long long)B.ni * B.nj];
+  }
+  V5<float> wk = ldW(B, b, pidx3(B, i, j, k)), wm = ldW(B, b, pidx3(B, i - ei, j - ej, k - ek)), wp = ldW(B, b, pidx3(B, i + ei, j + ej, k + ek));
+  const float s = 0.5f * B.dt[(long long)b * B.nc + c] / B.vol[c], al = fl.w, ar = fr.w;
+  M5<float> dl, dr;
+  if (cs.roe) {
+    dl = abs_jacobian3(wm, wk, fl.x, fl.y, fl.z, cs.eps_fix);
+    dr = abs_jacobian3(wk, wp, fr.x, fr.y, fr.z, cs.eps_fix);
+    float tl = shock_weight<float>(wm[4], wk[4]), tr = shock_weight<float>(wk[4], wp[4]);
+    if (tl > 0.f || tr > 0.f) {
+      float lam_l = fmaxf(spectral3(wk, fl.x, fl.y, fl.z), spectral3(wm, fl.x, fl.y, fl.z));
+      float lam_r = fmaxf(spectral3(wk, fr.x, fr.y, fr.z), spectral3(wp, fr.x, fr.y, fr.z));
+#pragma unroll
+      for (int q = 0; q < 25; ++q) dl[q] *= 1.f - tl, dr[q] *= 1.f - tr;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) dl[6 * q] += tl * lam_l, dr[6 * q] += tr * lam_r;
+    }
+  } else {
+    float lam_l = fmaxf(spectral3(wk, fl.x, fl.y, fl.z), spectral3(wm, fl.x, fl.y, fl.z));
+    float lam_r = fmaxf(spectral3(wk, fr.x, fr.y, fr.z), spectral3(wp, fr.x, fr.y, fr.z));
+    dl = zero5(), dr = zero5();
+#pragma unroll
+    for (int q = 0; q < 5; ++q) dl[6 * q] = lam_l, dr[6 * q] = lam_r;
+  }
+  d = eye5();
+  axpy5(d, s * ar, flux_jacobian3(wk, fr.x, fr.y, fr.z));
+  axpy5(d, -s * al, flux_jacobian3(wk, fl.x, fl.y, fl.z));
+  axpy5(d, s * ar, dr);
+  axpy5(d, s * al, dl);
+  if (!cs.lines) {
+    lo = zero5(), up = zero5();
+    return;
+  }
+  lo = flux_jacobian3(wm, fl.x, fl.y, fl.z);
+  axpy5(lo, 1.f, dl);
+#pragma unroll
+  for (int q = 0; q < 25; ++q) lo[q] *= -s * al;
+  up = flux_jacobian3(wp, fr.x, fr.y, fr.z);
+  axpy5(up, -1.f, dr);
+#pragma unroll
+  for (int q = 0; q < 25; ++q) up[q] *= s * ar;
+  // ghost Jacobians: far field (i ends, j = nj) frozen, T = 0; the axis frozen; slip wall and symmetry planes reflect
+  if (m == 0) {
+    bool refl = cs.implicit_bc && ((dir == 1 && i >= B.axis_cells) || dir == 2);
+    if (refl) axpy5(d, 1.f, mm5(lo, reflection3(fl.x, fl.y, fl.z)));
+    lo = zero5();
+  }
+  if (m == nl - 1) {
+    if (cs.implicit_bc && dir == 2) axpy5(d, 1.f, mm5(up, reflection3(fr.x, fr.y, fr.z)));
+    up = zero5();
+  }
+}
+
+__device__ __forceinline__ void damped_update3(const B3& B, int b, long long c, const V5<float>& dq) {  // implicit3.rs:456-469
+  V5<float> u = ldU(B, B.U, b, c);
+  float alpha = 1.f;
+  for (int t = 0; t < 8; ++t) {
+    V5<float> q;
+#pragma unroll
+    for (int m = 0; m < 5; ++m) q[m] = u[m] + alpha * dq[m];
+    V5<float> w = cons_to_prim3<float>(q);
+    bool fin = true;
+#pragma unroll
+    for (int m = 0; m < 5; ++m) fin = fin && isfinite(q[m]);
+    if (w[0] > 0.f && w[4] > 0.f && fin) {
+      stU(B, B.U, b, c, q);
+      return;
+    }
+    alpha *= 0.5f;
+  }
+}
+
+// One thread per line of direction dir: block Thomas with the blocks assembled on the way (implicit3.rs:133-156).
+// in: the right-hand side (from_res: dt R); epilogue 0: x -> out; 1: du = x; 2: du += x; `update` applies the damped update.
+__global__ void __launch_bounds__(128) k3_lines(B3 B, int dir, const float* in, int from_res, float* out, int epilogue, int pass) {
+  long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  const long long nlines = dir == 0 ? (long long)B.nj * B.nk : dir == 1 ? (long long)B.ni * B.nk : (long long)B.ni * B.nj;
+  if (L >= nlines || !B.active[b]) return;
+  const Case3Dev& cs = B.cs[b];
+  if (pass >= (cs.sub_iters > 1 ? cs.sub_iters : 1)) return;
+  const bool update = epilogue != 0 && pass == (cs.sub_iters > 1 ? cs.sub_iters : 1) - 1;
+  int i0, j0, k0;
+  if (dir == 0) i0 = 0, j0 = (int)(L % B.nj), k0 = (int)(L / B.nj);
+  else if (dir == 1) i0 = (int)(L % B.ni), j0 = 0, k0 = (int)(L / B.ni);
+  else i0 = (int)(L % B.ni), j0 = (int)(L / B.ni), k0 = 0;
+  const int n = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
+  const long long stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
+  const long long c0 = cell3(B, i0, j0, k0);
+  float* Ys = B.scr + (long long)b * 30 * B.nc;  // [30][cell]: Y (25), g (5)
+  M5<float> Y = zero5();
+  V5<float> g{{0, 0, 0, 0, 0}};
+  for (int m = 0; m < n; ++m) {
+    long long c = c0 + m * stride;
+    M5<float> lo, d, up;
+    blocks3(B, b, dir, i0 + (dir == 0) * m, j0 + (dir == 1) * m, k0 + (dir == 2) * m, lo, d, up);
+    V5<float> r = ldU(B, in, b, c);
+    if (from_res) {
+      float dtc = B.dt[(long long)b * B.nc + c];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) r[q] *= dtc;
+    }
+    if (m > 0) {
+      axpy5(d, -1.f, mm5(lo, Y));
+      V5<float> t = mv5(lo, g);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) r[q] -= t[q];
+    }
+    M5<float> Minv = inv5(d);
+    g = mv5(Minv, r);
+    Y = mm5(Minv, up);
+#pragma unroll
+    for (int q = 0; q < 25; ++q) Ys[q * B.nc + c] = Y[q];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) Ys[(25 + q) * B.nc + c] = g[q];
+  }
+  V5<float> xn = g;
+  auto emit = [&](long long c, const V5<float>& x) {
+    if (epilogue == 0) {
+      stU(B, out, b, c, x);
+      return;
+    }
+    V5<float> du = x;
+    if (epilogue == 2) {
+      V5<float> o = ldU(B, B.DU, b, c);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) du[q] += o[q];
+    }
+    stU(B, B.DU, b, c, du);
+    if (update) damped_update3(B, b, c, du);
+  };
+  emit(c0 + (long long)(n - 1) * stride, xn);
+  for (int m = n - 2; m >= 0; --m) {
+    long long c = c0 + m * stride;
+    M5<float> Ym;
+    V5<float> gm;
+#pragma unroll
+    for (int q = 0; q < 25; ++q) Ym[q] = Ys[q * B.nc + c];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gm[q] = Ys[(25 + q) * B.nc + c];
+    V5<float> t = mv5(Ym, xn);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gm[q] -= t[q];
+    emit(c, gm);
+    xn = gm;
+  }
+  if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
+}
+
+// defect of the unfactored operator (implicit3.rs:440-446): rr = dt R - (A_i du + A_j du + A_k du - 2 du)
+__global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (c >= B.nc || !B.active[b]) return;
+  const Case3Dev& cs = B.cs[b];
+  if (pass >= cs.sub_iters) return;
+  int i = (int)(c % B.ni), j = (int)((c / B.ni) % B.nj), k = (int)(c / ((long long)B.ni * B.nj));
+  V5<float> du = ldU(B, B.DU, b, c);
+  V5<float> acc{{0, 0, 0, 0, 0}};
+  for (int dir = 0; dir < 3; ++dir) {
+    M5<float> lo, d, up;
+    blocks3(B, b, dir, i, j, k, lo, d, up);
+    const int m = dir == 0 ? i : dir == 1 ? j : k, nl = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
+    const long long stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
+    V5<float> v = mv5(d, du);
+    if (m > 0) {
+      V5<float> t = mv5(lo, ldU(B, B.DU, b, c - stride));
+#pragma unroll
+      for (int q = 0; q < 5; ++q) v[q] += t[q];
+    }
+    if (m + 1 < nl) {
+      V5<float> t = mv5(up, ldU(B, B.DU, b, c + stride));
+#pragma unroll
+      for (int q = 0; q < 5; ++q) v[q] += t[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc[q] += v[q];
+  }
+  V5<float> r = ldU(B, B.R, b, c);
+  float d = B.dt[(long long)b * B.nc + c];
+  V5<float> o;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) o[q] = r[q] * d - (acc[q] - 2.f * du[q]);
+  stU(B, B.RR, b, c, o);
+}
+
+// FP64 wall forces of every case (run3.rs:150-190, body wall without fins): one block per case.
+// wall: per j = 0 face (i >= axis_cells) n[3], area, c[3], the centroids of cells (i, 0, k) and (i, 1, k); x <= x_max.
+__global__ void k3_forces(B3 B, const double* wall, int nwall, double x_max, double* out) {
+  __shared__ double acc[3][256];
+  int b = blockIdx.x;
+  double p_inf = B.cs[b].fs[4];
+  double fx = 0, fz = 0, mz = 0;
+  const int nw = B.ni - B.axis_cells;
+  for (int q = threadIdx.x; q < nwall; q += blockDim.x) {
+    const double* w = wall + 13 * (long long)q;
+    if (w[4] > x_max) continue;
+    int i = B.axis_cells + q % nw, k = q / nw;
+    long long ca = cell3(B, i, 0, k);
+    auto pres = [&](long long cc) {
+      const float* p = B.U + (long long)b * 5 * B.nc + cc;
+      double rho = p[0], u = p[B.nc] / rho, v = p[2 * B.nc] / rho, ww = p[3 * B.nc] / rho;
+      return (GD - 1.0) * ((double)p[4 * B.nc] - 0.5 * rho * (u * u + v * v + ww * ww));
+    };
+    double p0 = pres(ca), pw = p0;
+    if (B.nj > 1) {
+      double d0 = sqrt((w[7] - w[4]) * (w[7] - w[4]) + (w[8] - w[5]) * (w[8] - w[5]) + (w[9] - w[6]) * (w[9] - w[6]));
+      double d1 = sqrt((w[10] - w[4]) * (w[10] - w[4]) + (w[11] - w[5]) * (w[11] - w[5]) + (w[12] - w[6]) * (w[12] - w[6]));
+      pw = p0 + (p0 - pres(cell3(B, i, 1, k))) * d0 / (d1 - d0);
+    }
+    double dd = (pw - p_inf) * w[3] * -1.0;
+    fx += dd * w[0];
+    fz += dd * w[2];
+    mz += dd * w[2] * w[4];
+  }
+  acc[0][threadIdx.x] = fx, acc[1][threadIdx.x] = fz, acc[2][threadIdx.x] = mz;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int q = 0; q < 3; ++q) acc[q][threadIdx.x] += acc[q][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double mach = sqrt(B.cs[b].fs[1] * B.cs[b].fs[1] + B.cs[b].fs[3] * B.cs[b].fs[3]);
+    double norm = 2.0 / (0.5 * mach * mach * (M_PI / 4.0));
+    out[3 * b] = norm * acc[1][0];
+    out[3 * b + 1] = norm * acc[0][0];
+    out[3 * b + 2] = fabs(acc[1][0]) < 1e-12 ? NAN : acc[2][0] / acc[1][0];
+  }
+}
+
+}  // namespace bk3

@@ -1,0 +1,441 @@
+// Host side of the 3D batch (euler3.cuh): FP64 grid metrics from the node coordinates (grid3.rs:66-174: faces from their four
+// corners, volumes by the divergence theorem over the face centroids, one global handedness sign), the cell across the
+// axis (solver3.rs:98-117), device buffers, the iteration launch sequence, and the reference's 3D stop rules
+// (run3.rs:220-330) with per-case masks.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "euler3.cuh"
+
+namespace bk3 {
+
+struct Grid3H {
+  size_t ni = 0, nj = 0, nk = 0;
+  std::vector<double> fi, fj, fk;  // 7 per face: n[3], area, c[3]
+  std::vector<double> vol, xc;     // xc 3 per cell
+};
+
+static inline void face_of(const double* p0, const double* p1, const double* p2, const double* p3, double* out, double* s) {
+  double a[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]}, b[3] = {p3[0] - p1[0], p3[1] - p1[1], p3[2] - p1[2]};
+  s[0] = 0.5 * (a[1] * b[2] - a[2] * b[1]);
+  s[1] = 0.5 * (a[2] * b[0] - a[0] * b[2]);
+  s[2] = 0.5 * (a[0] * b[1] - a[1] * b[0]);
+  double area = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+  if (area < 1e-300) {
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+  } else {
+    out[0] = s[0] / area, out[1] = s[1] / area, out[2] = s[2] / area, out[3] = area;
+  }
+  for (int m = 0; m < 3; ++m) out[4 + m] = 0.25 * (p0[m] + p1[m] + p2[m] + p3[m]);
+}
+
+// false (with a message) on a negative cell volume
+inline bool grid3_metrics(size_t ni, size_t nj, size_t nk, const double* x, const double* y, const double* z, Grid3H& g, std::string& err) {
+  g = Grid3H{};
+  g.ni = ni, g.nj = nj, g.nk = nk;
+  auto pt = [&](size_t i, size_t j, size_t k, double* p) {
+    size_t n = (k * (nj + 1) + j) * (ni + 1) + i;
+    p[0] = x[n], p[1] = y[n], p[2] = z[n];
+  };
+  size_t nfi = (ni + 1) * nj * nk, nfj = ni * (nj + 1) * nk, nfk = ni * nj * (nk + 1);
+  g.fi.assign(7 * nfi, 0.0), g.fj.assign(7 * nfj, 0.0), g.fk.assign(7 * nfk, 0.0);
+  std::vector<double> si(3 * nfi), sj(3 * nfj), sk(3 * nfk);
+  double p[4][3];
+  for (size_t k = 0; k < nk; ++k)
+    for (size_t j = 0; j < nj; ++j)
+      for (size_t i = 0; i <= ni; ++i) {
+        size_t q = (k * nj + j) * (ni + 1) + i;
+        pt(i, j, k, p[0]), pt(i, j + 1, k, p[1]), pt(i, j + 1, k + 1, p[2]), pt(i, j, k + 1, p[3]);
+        face_of(p[0], p[1], p[2], p[3], &g.fi[7 * q], &si[3 * q]);
+      }
+  for (size_t k = 0; k < nk; ++k)
+    for (size_t j = 0; j <= nj; ++j)
+      for (size_t i = 0; i < ni; ++i) {
+        size_t q = (k * (nj + 1) + j) * ni + i;
+        pt(i, j, k, p[0]), pt(i, j, k + 1, p[1]), pt(i + 1, j, k + 1, p[2]), pt(i + 1, j, k, p[3]);
+        face_of(p[0], p[1], p[2], p[3], &g.fj[7 * q], &sj[3 * q]);
+      }
+  for (size_t k = 0; k <= nk; ++k)
+    for (size_t j = 0; j < nj; ++j)
+      for (size_t i = 0; i < ni; ++i) {
+        size_t q = (k * nj + j) * ni + i;
+        pt(i, j, k, p[0]), pt(i + 1, j, k, p[1]), pt(i + 1, j + 1, k, p[2]), pt(i, j + 1, k, p[3]);
+        face_of(p[0], p[1], p[2], p[3], &g.fk[7 * q], &sk[3 * q]);
+      }
+  size_t nc = ni * nj * nk;
+  g.vol.assign(nc, 0.0), g.xc.assign(3 * nc, 0.0);
+  auto dotc = [](const double* f, const double* s) { return f[4] * s[0] + f[5] * s[1] + f[6] * s[2]; };
+  double tot = 0.0;
+  for (size_t k = 0; k < nk; ++k)
+    for (size_t j = 0; j < nj; ++j)
+      for (size_t i = 0; i < ni; ++i) {
+        size_t il = (k * nj + j) * (ni + 1) + i, jl = (k * (nj + 1) + j) * ni + i, kl = (k * nj + j) * ni + i;
+        size_t jr = jl + ni, kr = kl + ni * nj;
+        double v = 0.0;
+        v += dotc(&g.fi[7 * (il + 1)], &si[3 * (il + 1)]);
+        v -= dotc(&g.fi[7 * il], &si[3 * il]);
+        v += dotc(&g.fj[7 * jr], &sj[3 * jr]);
+        v -= dotc(&g.fj[7 * jl], &sj[3 * jl]);
+        v += dotc(&g.fk[7 * kr], &sk[3 * kr]);
+        v -= dotc(&g.fk[7 * kl], &sk[3 * kl]);
+        size_t c = kl;
+        g.vol[c] = v / 3.0;
+        tot += g.vol[c];
+        double m[3] = {0, 0, 0};
+        for (int bb = 0; bb < 8; ++bb) {
+          double q[3];
+          pt(i + (bb & 1), j + (bb >> 1 & 1), k + (bb >> 2 & 1), q);
+          for (int a = 0; a < 3; ++a) m[a] += 0.125 * q[a];
+        }
+        for (int a = 0; a < 3; ++a) g.xc[3 * c + a] = m[a];
+      }
+  if (tot < 0.0) {
+    for (auto* fam : {&g.fi, &g.fj, &g.fk})
+      for (size_t q = 0; q < fam->size(); q += 7) (*fam)[q] = -(*fam)[q], (*fam)[q + 1] = -(*fam)[q + 1], (*fam)[q + 2] = -(*fam)[q + 2];
+    for (auto& v : g.vol) v = -v;
+  }
+  double vmax = 0.0;
+  for (double v : g.vol) vmax = std::fmax(vmax, std::fabs(v));
+  for (size_t c = 0; c < nc; ++c)
+    if (g.vol[c] < -1e-12 * vmax || std::isnan(g.vol[c])) {
+      err = "negative cell volume at cell " + std::to_string(c);
+      return false;
+    }
+  return true;
+}
+
+struct Case3Host {
+  double mach = 0.5, alpha = 0.0, cfl = 0.5;
+  int limiter = 1, low_mach = 0, implicit = 1;
+  long long first_order_iters = 0;
+  double cfl0 = 1.0, cfl_max = 30.0, growth = 1.02, eps_fix = 0.1;
+  int dt_mode = 0, sub_iters = 2, roe = 1, implicit_bc = 1, lines = 1;
+};
+
+#define BK3_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+      return 3;                                                                 \
+    }                                                                           \
+  } while (0)
+
+struct Batch3 {
+  B3 B{};
+  Grid3H g;
+  std::vector<Case3Host> cases;
+  std::vector<int> axis_k;
+  std::vector<double> wall;  // 13 per j = 0 wall face: n[3], area, c[3], centroid of (i,0,k), centroid of (i,1,k)
+  int nwall = 0, device = 0, slots = 64;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms_per_iter = 0.0;
+  std::string err;
+  std::vector<void*> owned;
+  double *d_wall = nullptr, *d_forces = nullptr;
+  std::vector<int> h_active;
+
+  ~Batch3() { release(); }
+  void release() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* p : owned)
+      if (p) cudaFree(p);
+    owned.clear();
+    if (ev0) cudaEventDestroy(ev0), ev0 = nullptr;
+    if (ev1) cudaEventDestroy(ev1), ev1 = nullptr;
+    if (stream) cudaStreamDestroy(stream), stream = nullptr;
+  }
+  template <class T>
+  int alloc(T** p, size_t n) {
+    *p = nullptr;
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+      err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return 3;
+    }
+    owned.push_back((void*)*p);
+    return 0;
+  }
+
+  static void to_dev(const Case3Host& h, Case3Dev& d) {
+    double a = h.alpha;
+    d.fs[0] = 1.0, d.fs[1] = h.mach * std::cos(a), d.fs[2] = 0.0, d.fs[3] = h.mach * std::sin(a), d.fs[4] = 1.0 / 1.4;  // gas3.rs:42-44
+    d.cfl = (float)h.cfl, d.cfl0 = (float)h.cfl0, d.cfl_max = (float)h.cfl_max, d.growth = (float)h.growth, d.eps_fix = (float)h.eps_fix;
+    d.limiter = h.limiter, d.low_mach = h.low_mach, d.first_order_iters = (int)h.first_order_iters, d.implicit = h.implicit;
+    d.dt_mode = h.dt_mode, d.sub_iters = h.sub_iters, d.roe = h.roe, d.implicit_bc = h.implicit_bc, d.lines = h.lines;
+  }
+
+  int create(size_t ni, size_t nj, size_t nk, const double* x, const double* y, const double* z, size_t axis_cells,
+             const std::vector<Case3Host>& cs, int dev) {
+    if (ni < 2 || nj < 2 || nk < 2 || cs.empty() || axis_cells > ni) {
+      err = "invalid 3D grid or case list";
+      return 2;
+    }
+    if (!grid3_metrics(ni, nj, nk, x, y, z, g, err)) return 2;
+    cases = cs;
+    device = dev;
+    BK3_CUDA(cudaSetDevice(dev));
+    BK3_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    BK3_CUDA(cudaEventCreate(&ev0));
+    BK3_CUDA(cudaEventCreate(&ev1));
+    const int nb = (int)cs.size();
+    B.ni = (int)ni, B.nj = (int)nj, B.nk = (int)nk, B.nb = nb, B.axis_cells = (int)axis_cells;
+    B.nc = (long long)ni * nj * nk;
+    B.npad = (long long)(ni + 4) * (nj + 4) * (nk + 4);
+    B.nfi = (long long)(ni + 1) * nj * nk, B.nfj = (long long)ni * (nj + 1) * nk, B.nfk = (long long)ni * nj * (nk + 1);
+    // the cell across the axis: the one whose centroid azimuth is closest to pi - theta (solver3.rs:98-117)
+    axis_k.assign(std::max<size_t>(axis_cells * nk, 1), 0);
+    auto theta = [&](size_t i, size_t k) {
+      const double* c = &g.xc[3 * ((k * nj) * ni + i)];
+      return std::atan2(c[1], c[2]);
+    };
+    for (size_t i = 0; i < axis_cells; ++i)
+      for (size_t k = 0; k < nk; ++k) {
+        double target = M_PI - theta(i, k), best = INFINITY;
+        size_t bk = 0;
+        for (size_t kk = 0; kk < nk; ++kk) {
+          double d = std::fabs(theta(i, kk) - target);
+          if (d < best) best = d, bk = kk;
+        }
+        axis_k[i * nk + k] = (int)bk;
+      }
+    // wall faces for the forces
+    wall.clear();
+    for (size_t k = 0; k < nk; ++k)
+      for (size_t i = axis_cells; i < ni; ++i) {
+        const double* f = &g.fj[7 * (k * (nj + 1) * ni + i)];
+        for (int q = 0; q < 7; ++q) wall.push_back(f[q]);
+        const double* c0 = &g.xc[3 * ((k * nj) * ni + i)];
+        const double* c1 = &g.xc[3 * ((k * nj + 1) * ni + i)];
+        for (int q = 0; q < 3; ++q) wall.push_back(c0[q]);
+        for (int q = 0; q < 3; ++q) wall.push_back(c1[q]);
+      }
+    nwall = (int)(wall.size() / 13);
+    int rc;
+    float4 *fi, *fj, *fk;
+    float2 *ri, *rj, *rk;
+    float* vol;
+    int* ak;
+    Case3Dev* dcs;
+    if ((rc = alloc(&fi, B.nfi)) || (rc = alloc(&fj, B.nfj)) || (rc = alloc(&fk, B.nfk)) || (rc = alloc(&ri, B.nfi)) || (rc = alloc(&rj, B.nfj)) ||
+        (rc = alloc(&rk, B.nfk)) || (rc = alloc(&vol, B.nc)) || (rc = alloc(&ak, axis_k.size())) || (rc = alloc(&dcs, nb)) ||
+        (rc = alloc(&B.iter, nb)) || (rc = alloc(&B.ramp, nb)) || (rc = alloc(&B.active, nb)))
+      return rc;
+    size_t ns = (size_t)nb * 5 * B.nc;
+    if ((rc = alloc(&B.U, ns)) || (rc = alloc(&B.U0, ns)) || (rc = alloc(&B.W, (size_t)nb * 5 * B.npad)) || (rc = alloc(&B.R, ns)) ||
+        (rc = alloc(&B.X, ns)) || (rc = alloc(&B.DU, ns)) || (rc = alloc(&B.RR, ns)) || (rc = alloc(&B.dt, (size_t)nb * B.nc)) ||
+        (rc = alloc(&B.scr, (size_t)nb * 30 * B.nc)) || (rc = alloc(&B.FI, (size_t)nb * 5 * B.nfi)) || (rc = alloc(&B.FJ, (size_t)nb * 5 * B.nfj)) ||
+        (rc = alloc(&B.FK, (size_t)nb * 5 * B.nfk)) || (rc = alloc(&B.rsum, (size_t)slots * nb)) || (rc = alloc(&d_wall, wall.size())) ||
+        (rc = alloc(&d_forces, 3 * (size_t)nb)))
+      return rc;
+    auto up_faces = [&](const std::vector<double>& f, long long n, float4* d4, float2* d2) -> int {
+      std::vector<float4> h4(n);
+      std::vector<float2> h2(n);
+      for (long long q = 0; q < n; ++q) {
+        const double* p = &f[7 * q];
+        h4[q] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+        double r = std::hypot(p[5], p[6]);  // face_rot (flux3.rs:11-19)
+        h2[q] = r < 1e-300 ? make_float2(0.f, 1.f) : make_float2((float)(p[5] / r), (float)(p[6] / r));
+      }
+      BK3_CUDA(cudaMemcpy(d4, h4.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+      BK3_CUDA(cudaMemcpy(d2, h2.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+      return 0;
+    };
+    if ((rc = up_faces(g.fi, B.nfi, fi, ri)) || (rc = up_faces(g.fj, B.nfj, fj, rj)) || (rc = up_faces(g.fk, B.nfk, fk, rk))) return rc;
+    std::vector<float> hv(B.nc);
+    for (long long c = 0; c < B.nc; ++c) hv[c] = (float)g.vol[c];
+    BK3_CUDA(cudaMemcpy(vol, hv.data(), B.nc * sizeof(float), cudaMemcpyHostToDevice));
+    BK3_CUDA(cudaMemcpy(ak, axis_k.data(), axis_k.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(cudaMemcpy(d_wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice));
+    B.fi = fi, B.fj = fj, B.fk = fk, B.ri = ri, B.rj = rj, B.rk = rk, B.vol = vol, B.axis_k = ak, B.cs = dcs;
+    if ((rc = upload_cases())) return rc;
+    h_active.assign(nb, 1);
+    BK3_CUDA(cudaMemcpy(B.active, h_active.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    return reset();
+  }
+  int upload_cases() {
+    std::vector<Case3Dev> h(cases.size());
+    for (size_t k = 0; k < cases.size(); ++k) to_dev(cases[k], h[k]);
+    BK3_CUDA(cudaMemcpy(const_cast<Case3Dev*>(B.cs), h.data(), h.size() * sizeof(Case3Dev), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  // every case to its free stream, iteration and ramp counters to zero
+  int reset() {
+    for (int b = 0; b < B.nb; ++b) {
+      Case3Dev d;
+      to_dev(cases[b], d);
+      double q[5] = {d.fs[0], d.fs[0] * d.fs[1], d.fs[0] * d.fs[2], d.fs[0] * d.fs[3],
+                     d.fs[4] / 0.4 + 0.5 * d.fs[0] * (d.fs[1] * d.fs[1] + d.fs[2] * d.fs[2] + d.fs[3] * d.fs[3])};
+      std::vector<float> h(B.nc);
+      for (int v = 0; v < 5; ++v) {
+        std::fill(h.begin(), h.end(), (float)q[v]);
+        BK3_CUDA(cudaMemcpy(B.U + ((size_t)b * 5 + v) * B.nc, h.data(), B.nc * sizeof(float), cudaMemcpyHostToDevice));
+      }
+    }
+    std::vector<int> z(B.nb, 0);
+    BK3_CUDA(cudaMemcpy(B.iter, z.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(cudaMemcpy(B.ramp, z.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int set_state(int b, const double* u) {  // u: ncell x 5 (Cons3 layout)
+    std::vector<float> h(5 * B.nc);
+    for (long long c = 0; c < B.nc; ++c)
+      for (int v = 0; v < 5; ++v) h[v * B.nc + c] = (float)u[5 * c + v];
+    BK3_CUDA(cudaMemcpy(B.U + (size_t)b * 5 * B.nc, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int get_state(int b, double* u) {
+    std::vector<float> h(5 * B.nc);
+    BK3_CUDA(cudaStreamSynchronize(stream));
+    BK3_CUDA(cudaMemcpy(h.data(), B.U + (size_t)b * 5 * B.nc, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (long long c = 0; c < B.nc; ++c)
+      for (int v = 0; v < 5; ++v) u[5 * c + v] = h[v * B.nc + c];
+    return 0;
+  }
+  int set_counters(int it, int ramp) {
+    std::vector<int> a(B.nb, it), r(B.nb, ramp);
+    BK3_CUDA(cudaMemcpy(B.iter, a.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(cudaMemcpy(B.ramp, r.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int set_active(const std::vector<int>& act) {
+    h_active = act;
+    BK3_CUDA(cudaMemcpyAsync(B.active, h_active.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice, stream));
+    BK3_CUDA(cudaStreamSynchronize(stream));
+    return 0;
+  }
+
+  dim3 grid_of(long long n, int threads) const { return dim3((unsigned)((n + threads - 1) / threads), (unsigned)B.nb); }
+  void launch_prep() {
+    k3_prims<<<grid_of(B.nc, 256), 256, 0, stream>>>(B);
+    long long ng = 2LL * B.nj * B.nk + 2LL * B.ni * B.nk + 2LL * B.ni * B.nj;
+    k3_ghosts<<<grid_of(ng, 128), 128, 0, stream>>>(B);
+    k3_flux<<<grid_of(B.nfi, 128), 128, 0, stream>>>(B, 0);
+    k3_flux<<<grid_of(B.nfj, 128), 128, 0, stream>>>(B, 1);
+    k3_flux<<<grid_of(B.nfk, 128), 128, 0, stream>>>(B, 2);
+  }
+  bool implicit() const { return cases[0].implicit != 0; }
+  int max_sub() const {
+    int s = 1;
+    for (auto& c : cases) s = std::max(s, c.sub_iters);
+    return s;
+  }
+  void launch_iteration(int slot) {
+    if (implicit()) {
+      launch_prep();
+      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2, slot);
+      const long long li = (long long)B.nj * B.nk, lj = (long long)B.ni * B.nk, lk = (long long)B.ni * B.nj;
+      for (int p = 0; p < max_sub(); ++p) {
+        if (p > 0) k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
+        k3_lines<<<grid_of(li, 64), 64, 0, stream>>>(B, 0, p == 0 ? B.R : B.RR, p == 0, B.X, 0, p);
+        k3_lines<<<grid_of(lj, 64), 64, 0, stream>>>(B, 1, B.X, 0, B.X, 0, p);
+        k3_lines<<<grid_of(lk, 64), 64, 0, stream>>>(B, 2, B.X, 0, nullptr, p == 0 ? 1 : 2, p);
+      }
+    } else {  // SSP-RK3 (solver3.rs:303-314)
+      launch_prep();
+      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 1, slot);
+      k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 1.f, 0.f, 1, 0);
+      launch_prep();
+      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0, -1);
+      k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0.25f, 0.75f, 0, 0);
+      launch_prep();
+      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0, -1);
+      k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2.f / 3.f, 1.f / 3.f, 0, 1);
+    }
+  }
+  // n iterations; residual: n x nb (iteration-major), may be null
+  int run(long long n, double* residual) {
+    const int nb = B.nb;
+    std::vector<double> h;
+    long long done = 0;
+    double ms_total = 0.0;
+    std::vector<long long> n_active(nb, B.nc);
+    while (done < n) {
+      int chunk = (int)std::min<long long>(n - done, slots);
+      BK3_CUDA(cudaMemsetAsync(B.rsum, 0, (size_t)chunk * nb * sizeof(double), stream));
+      BK3_CUDA(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      BK3_CUDA(cudaGetLastError());
+      BK3_CUDA(cudaEventRecord(ev1, stream));
+      h.resize((size_t)chunk * nb);
+      BK3_CUDA(cudaMemcpyAsync(h.data(), B.rsum, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      BK3_CUDA(cudaStreamSynchronize(stream));
+      float ms = 0.f;
+      BK3_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      ms_total += ms;
+      if (residual)
+        for (int k = 0; k < chunk; ++k)
+          for (int b = 0; b < nb; ++b) residual[(done + k) * nb + b] = std::sqrt(h[(size_t)k * nb + b] / (double)B.nc);
+      done += chunk;
+    }
+    last_ms_per_iter = n > 0 ? ms_total / (double)n : 0.0;
+    return 0;
+  }
+  // residual (and implicit time step with the current ramp) of the current state of every active case
+  int eval_residual(std::vector<double>& dens) {
+    BK3_CUDA(cudaMemsetAsync(B.rsum, 0, B.nb * sizeof(double), stream));
+    launch_prep();
+    k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, implicit() ? 2 : 1, 0);
+    BK3_CUDA(cudaGetLastError());
+    dens.resize(B.nb);
+    BK3_CUDA(cudaMemcpyAsync(dens.data(), B.rsum, B.nb * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    BK3_CUDA(cudaStreamSynchronize(stream));
+    for (auto& d : dens) d = std::sqrt(d / (double)B.nc);
+    return 0;
+  }
+  int read_residual(int b, double* res, double* dt) {
+    std::vector<float> h(5 * B.nc), hd(B.nc);
+    BK3_CUDA(cudaMemcpy(h.data(), B.R + (size_t)b * 5 * B.nc, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    BK3_CUDA(cudaMemcpy(hd.data(), B.dt + (size_t)b * B.nc, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (long long c = 0; c < B.nc; ++c) {
+      if (res)
+        for (int v = 0; v < 5; ++v) res[5 * c + v] = h[v * B.nc + c];
+      if (dt) dt[c] = hd[c];
+    }
+    return 0;
+  }
+  int forces(double x_max, std::vector<double>& out) {
+    k3_forces<<<B.nb, 256, 0, stream>>>(B, d_wall, nwall, x_max, d_forces);
+    BK3_CUDA(cudaGetLastError());
+    out.resize(3 * (size_t)B.nb);
+    BK3_CUDA(cudaMemcpyAsync(out.data(), d_forces, out.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    BK3_CUDA(cudaStreamSynchronize(stream));
+    return 0;
+  }
+};
+
+// run3.rs:253-330 StopRule3
+struct StopRule3 {
+  size_t skip = 20, nwin = 10, window = 500;
+  double rel_tol = 0.002, rmax = 0.0, r = NAN;
+  std::vector<double> hist;
+  int reason = 0;  // 0 max iterations, 1 residual drop, 2 CN stationary, 5 non-finite
+  bool check(size_t it, double res, bool sampled, double cn) {
+    r = res;
+    if (!std::isfinite(res)) return reason = 5, true;
+    if (it >= skip) rmax = std::fmax(rmax, res);
+    double drop = rmax > 0.0 ? std::log10(rmax / std::fmax(res, 1e-300)) : 0.0;
+    if (drop >= 6.0) return reason = 1, true;
+    if (sampled) {
+      if (!std::isfinite(cn) || std::fabs(cn) > 1e3) return reason = 5, true;
+      hist.push_back(cn);
+      if (it + 1 >= std::max<size_t>(window, 1000) && hist.size() >= nwin) {
+        const double* w = hist.data() + hist.size() - nwin;
+        bool frozen = true;
+        for (size_t q = 0; q < nwin; ++q) frozen = frozen && std::memcmp(&w[q], &w[0], sizeof(double)) == 0;
+        if (drop < 1.0 && frozen) return reason = 5, true;
+        double lo = INFINITY, hi = -INFINITY, sum = 0.0;
+        for (size_t q = 0; q < nwin; ++q) lo = std::fmin(lo, w[q]), hi = std::fmax(hi, w[q]), sum += w[q];
+        if (hi - lo < rel_tol * std::fabs(sum / (double)nwin)) return reason = 2, true;
+      }
+    }
+    return false;
+  }
+};
+
+}  // namespace bk3

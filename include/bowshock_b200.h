@@ -295,6 +295,52 @@ int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
 #define BOWSHOCK_PROFILE_GROUPS 11
 int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
 
+/* ---------------------------------------------------------------------------------------------- 3D Euler
+ * The stability path (crates/bowshock-cfd/src/solver3.rs + implicit3.rs behind `GpuSolver3`, gpu/mod.rs:442-560, driven
+ * by engine/run3.rs): a batch of cases (Mach number, incidence) on one shared 3D grid. Nodes (ni+1)(nj+1)(nk+1), index
+ * (k*(nj+1)+j)*(ni+1)+i; j = 0 is the axis for i < axis_cells and the body wall beyond, j = nj and the i ends the far
+ * field, k = 0 and k = nk symmetry planes (a half body revolved over [0, pi]). No fins. */
+typedef struct {
+  double mach, alpha;       /* incidence [rad]: the air moves towards +z (gas3.rs:42-44) */
+  double cfl;               /* CFL of the explicit scheme */
+  int32_t limiter, low_mach;
+  uint64_t first_order_iters;
+  bowshock_scheme scheme;   /* BOWSHOCK_SCHEME_EXPLICIT or BOWSHOCK_SCHEME_IMPLICIT (three-factor, 5x5 blocks) */
+} bowshock3_config;
+typedef struct {            /* run3.rs:220-330 stop rules */
+  uint64_t max_iter;
+  double rel_tol;           /* CN stationary: range over the window below rel_tol |mean| */
+  uint64_t window;          /* iterations, a multiple of 50 */
+  double x_max;             /* wall faces with centroid x <= x_max carry the forces (the base station) */
+} bowshock3_run_params;
+typedef struct {            /* run3.rs `PointResult3` (scalars) */
+  double cn, ca, x_cp;
+  uint64_t iterations;
+  int32_t stop_reason;      /* 0 max iterations, 1 residual drop, 2 CN stationary, 5 non-finite */
+  double drop_orders;
+} bowshock3_result;
+typedef struct bowshock3_batch bowshock3_batch;
+int bowshock3_create(uint64_t ni, uint64_t nj, uint64_t nk, const double* x, const double* y, const double* z, uint64_t axis_cells,
+                     uint64_t ncases, const bowshock3_config* cfg, int device, bowshock3_batch** out);
+void bowshock3_destroy(bowshock3_batch* b);
+const char* bowshock3_last_error(const bowshock3_batch* b);
+/* every case back to its free stream at iteration 0 (GpuSolver3::reset) */
+int bowshock3_reset(bowshock3_batch* b);
+/* iteration counter (first-order start-up) and CFL-ramp counter of every case */
+int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp);
+/* conserved state of case k, ni*nj*nk x 5 (Solver3::u layout) */
+int bowshock3_set_state(bowshock3_batch* b, uint64_t k, const double* u);
+int bowshock3_state(bowshock3_batch* b, uint64_t k, double* u);
+/* n iterations of every active case; residual (n x ncases, iteration-major) may be NULL (GpuSolver3::run) */
+int bowshock3_run(bowshock3_batch* b, uint64_t n, double* residual);
+/* residual (ncell x 5) and time step of case k for the current state (no update); density residual of case k */
+int bowshock3_eval_residual(bowshock3_batch* b, uint64_t k, double* res, double* dt, double* density_residual);
+/* FP64 pressure forces of every case: (cn, ca, x_cp) x ncases (run3.rs `forces_on`, no fins) */
+int bowshock3_forces(bowshock3_batch* b, double x_max, double* out);
+/* cold start of every case, iterated to the stop rules with per-case masks (run3.rs:220-330) */
+int bowshock3_solve(bowshock3_batch* b, const bowshock3_run_params* p, bowshock3_result* out);
+int bowshock3_last_ms_per_iter(const bowshock3_batch* b, double* ms);
+
 /* bowshock_solver_run without any device allocation. No counterpart in the reference. For hosts that create their solvers
  * up front and then step them from code that may not allocate device memory: the GPU's free memory belongs to the host's
  * own pool (another framework's caching allocator on the same device), or the stepping loop cannot take the device-wide

@@ -1,0 +1,113 @@
+"""3D Euler on the B200 (bowshock3_* through the C ABI) against the 3D oracle (oracle/solver3.cpp), with the reference's
+GPU-vs-CPU protocol: the same start state, the per-cell residual of one evaluation, N iterations of the explicit (1e-5) and
+implicit (1e-3) schemes, the batch against single cases, and a converged small case's normal force; at the full sweep grid
+(192 x 64 x 64) the per-cell residual of one evaluation."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_ffi as o
+
+pytestmark = pytest.mark.gpu
+
+
+def _grid(ni, nj, nk, mach=1.2, alpha_deg=4.0):
+    from bowshock_b200.euler3 import lift_sweep_cases
+    c = lift_sweep_cases((alpha_deg,), (mach,), ni=ni, nj=nj, nk=nk)[0]
+    ni2, nj2, x2, r2, _ = c.case2.grid()
+    return c, ni2, nj2, np.asarray(x2), np.asarray(r2)
+
+
+def _pair(ni, nj, nk, mach, alpha_deg, implicit=True, first_order=0, limiter=o.MINMOD):
+    import bowshock_b200.euler3 as e3
+    c, ni2, nj2, x2, r2 = _grid(ni, nj, nk, mach, alpha_deg)
+    theta = np.pi * np.arange(nk + 1) / nk
+    axis = c.case2.grid_sting.n_up
+    alpha = math.radians(alpha_deg)
+    p = o.implicit3_params(cfl_max=10.0)
+    cpu = o.Solver3(ni2, nj2, x2, r2, nk, theta, axis, mach, alpha, limiter=limiter, first_order_iters=first_order, implicit=implicit,
+                    params=p)
+    cfg = e3.Config3(mach, alpha, 0.5, limiter, first_order, False, e3.ImplicitParams(cfl_max=10.0) if implicit else e3.EXPLICIT)
+    x, y, z = e3.revolve(x2, r2, nk)
+    gpu = e3.Batch3(ni2, nj2, nk, x, y, z, axis, [cfg])
+    return cpu, gpu, c
+
+
+def _perturb(cpu, seed, amp=0.02):
+    rng = np.random.default_rng(seed)
+    w = o.cons_to_prim3(cpu.u)
+    w[:, 0] *= 1 + amp * rng.standard_normal(len(w))
+    w[:, 1:4] += amp * rng.standard_normal((len(w), 3))
+    w[:, 4] *= 1 + amp * rng.standard_normal(len(w))
+    return o.prim_to_cons3(w)
+
+
+def _residual_check(ni, nj, nk, tol):
+    cpu, gpu, _ = _pair(ni, nj, nk, 1.2, 4.0)
+    u0 = _perturb(cpu, 3)
+    cpu.u = u0
+    gpu.set_state(0, u0)
+    dc = cpu.eval_residual(1.0)  # implicit dt at the first ramp step: cfl0 = 1
+    rg, dtg, dg = gpu.eval_residual(0)
+    rc = cpu.res
+    for k in range(5):
+        scale = np.max(np.abs(rc[:, k])) + 1e-30
+        err = np.max(np.abs(rg[:, k] - rc[:, k])) / scale
+        assert err < tol, f"component {k}: max rel err {err:.3e}"
+    assert abs(dg - dc) / dc < 1e-5
+    assert np.max(np.abs(dtg - cpu.dt) / cpu.dt) < 1e-5
+
+
+def test_residual_per_cell_small():
+    _residual_check(48, 16, 8, 1e-5)
+
+
+def test_residual_per_cell_at_the_sweep_grid():  # 192 x 64 x 64 = 786,432 cells
+    _residual_check(192, 64, 64, 1e-5)
+
+
+def test_explicit_state_matches_oracle():  # explicit.rs protocol, f32 tolerance
+    cpu, gpu, _ = _pair(48, 16, 8, 2.5, 6.0, implicit=False, limiter=o.MINMOD)
+    u0 = _perturb(cpu, 5, 0.01)
+    cpu.u = u0
+    gpu.set_state(0, u0)
+    rc = cpu.steps(20)
+    rg = gpu.run(20)[:, 0]
+    d = np.max(np.abs(gpu.state(0) - cpu.u) / (1 + np.abs(cpu.u)))
+    assert d < 1e-5, d
+    assert np.max(np.abs(rg - rc) / rc) < 1e-4
+
+
+@pytest.mark.parametrize("mach,alpha", [(0.8, 4.0), (2.5, 8.0)])
+def test_implicit_state_matches_oracle(mach, alpha):  # implicit.rs protocol (f32 left-hand side): 1e-3
+    cpu, gpu, _ = _pair(48, 16, 8, mach, alpha, implicit=True, first_order=5)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)[:, 0]
+    d = np.max(np.abs(gpu.state(0) - cpu.u) / (1 + np.abs(cpu.u)))
+    assert d < 1e-3, d
+    assert np.all(np.isfinite(rg))
+    assert np.max(np.abs(rg[:5] - rc[:5]) / rc[:5]) < 1e-3
+
+
+def test_batch_matches_single_cases():
+    import bowshock_b200.euler3 as e3
+    cases = e3.lift_sweep_cases((0.0, 4.0), (0.8, 2.5), ni=48, nj=16, nk=8)
+    batch, _ = e3.batch_of(cases)
+    rb = batch.run(25)
+    for k, c in enumerate(cases):
+        single, _ = e3.batch_of([c])
+        rs = single.run(25)[:, 0]
+        assert np.array_equal(rs, rb[:, k])
+        assert np.array_equal(single.state(0), batch.state(k))
+
+
+def test_converged_normal_force_matches_oracle():  # run3.rs stop rules on both, CN and centre of pressure
+    cpu, gpu, c = _pair(48, 16, 8, 2.5, 4.0, implicit=True, first_order=100)
+    x_base = c.body.x_base()
+    rc = cpu.run(x_base, max_iter=4000)
+    rg = gpu.solve(x_base, max_iter=4000)[0]
+    assert rc["stop_reason"] in ("residual drop", "CN stationary"), rc
+    assert rg["stop_reason"] in ("residual drop", "CN stationary"), rg
+    assert abs(rg["cn"] - rc["cn"]) <= 2e-3 * abs(rc["cn"]) + 1e-4, (rg, rc)
+    assert abs(rg["x_cp"] - rc["x_cp"]) <= 2e-2, (rg, rc)
