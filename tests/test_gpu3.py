@@ -98,8 +98,9 @@ def test_batch_matches_single_cases():
     for k, c in enumerate(cases):
         single, _ = e3.batch_of([c])
         rs = single.run(25)[:, 0]
-        assert np.array_equal(rs, rb[:, k])
         assert np.array_equal(single.state(0), batch.state(k))
+        # the norm's FP64 block sums are added atomically in no fixed order: equal to round-off
+        assert np.max(np.abs(rs - rb[:, k]) / rb[:, k]) < 1e-12
 
 
 def test_converged_normal_force_matches_oracle():  # run3.rs stop rules on both, CN and centre of pressure
