@@ -286,27 +286,25 @@ def run_ours(args, rank, world, dist):
     ms_step, total_value, e2e_value = combine_ranks(dist, ms_local, value_rank, e2e_rank)
     if rank != 0:
         return None
-    # roofline of the dominant kernel group
+    # roofline of the dominant kernel group: the block line sweeps (k_lines, the factorising first pass of each direction,
+    # and k_lines_subst, the defect-correction passes), half of an iteration in the launch list
     groups = {g: v for g, v in prof.items() if v[1] > 0}
-    top = max(groups, key=lambda g: groups[g][0])
-    ms_top, launches_top = groups[top]
+    sweep_groups = [g for g in ("lines_i", "lines_j", "subst_i", "subst_j") if g in groups]
+    top = "line sweeps (k_lines + k_lines_subst)"
+    ms_sweeps = sum(groups[g][0] for g in sweep_groups) / 5.0  # per iteration (profile over 5 iterations)
+    launches_iter = sum(groups[g][1] for g in sweep_groups) / 5.0
     viscous = np.array([c.viscous is not None for c in cases])
-    if top in ("lines_i", "lines_j", "subst_i", "subst_j"):
-        words = np.where(viscous, SWEEP_WORDS[True], SWEEP_WORDS[False])
-        sub = np.array([c.numerics.scheme.sub_iters for c in cases])
-        if top.startswith("lines"):  # the factorising first pass sweeps every case once
-            bytes_iter = float(np.sum(cells * words * 4))
-        else:  # a substitution launch sweeps the cases with a pass at that position: the mean over the launches
-            bytes_iter = float(np.sum(cells * words * 4 * (sub - 1))) / max(sub.max() - 1, 1)
-    else:
-        bytes_iter = float(np.sum(cells * (42 + np.where(viscous, 21, 0)) * 4))  # residual pass: 2 nv + g + v + 1 words
-    ms_launch = ms_top / launches_top
+    words = np.where(viscous, SWEEP_WORDS[True], SWEEP_WORDS[False])
+    sub = np.array([c.numerics.scheme.sub_iters for c in cases])
+    bytes_sweeps = float(np.sum(cells * words * 4 * 2 * sub))  # 3 nv + g + v + 1 words per cell, 2 directions x sub_iters passes
+    bytes_iter = bytes_sweeps / launches_iter
+    ms_launch = ms_sweeps / launches_iter
     achieved = bytes_iter / (ms_launch / 1000.0) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(top)
+            traffic = json.load(open(tpath)).get("line_sweep_per_launch")
         except Exception:
             traffic = None
     # CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
@@ -359,8 +357,15 @@ def run_ours(args, rank, world, dist):
 
 
 def run_kernels(args):
-    """The timed region alone (arena, warm-up, K iterations): the command the ncu captures of the kernels run."""
+    """The timed region alone (arena, warm-up, K iterations): the command the ncu captures of the kernels run. With
+    --workload lift3: the 15-case 3D Euler batch (192 x 64 x 64 cells per case) instead."""
     import bowshock_b200  # noqa: F401
+    if args.workload == "lift3":
+        import bowshock_b200.euler3 as e3
+        b, _ = e3.batch_of(e3.lift_sweep_cases())
+        b.run(max(args.warmup, 1))
+        b.run(args.steps)
+        return {"kernels_only": True, "workload": "lift3", "cells": b.nc * b.nb, "steps": args.steps, "ms_per_step": b.ms_per_iter()}
     from bowshock_b200.arena import Arena
     cases = build_cases(0)
     arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
@@ -378,6 +383,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kernels-only", action="store_true", help="only the timed arena iterations (for ncu captures)")
+    ap.add_argument("--workload", default="sweep32", choices=["sweep32", "lift3"], help="workload of --kernels-only")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
