@@ -2,14 +2,17 @@
 // crates/bowshock-core/src/engine/run3.rs) on the B200: a batch of cases (Mach number, incidence) that share one revolved
 // grid, so the geometry is stored once and read through L2 by every case. Per case the state is SoA FP32 planes
 // [case][var][cell]; the face fluxes and the cell residual are evaluated in FP64 from the FP32 primitives; the three-factor
-// line-implicit operator (5x5 blocks, Roe |A| with the entropy fix, shock-sensor blend) is assembled in registers and
-// solved one thread per line (block Thomas), i then j then k, with defect-correction passes.
+// line-implicit operator (5x5 blocks, Roe |A| with the entropy fix, shock-sensor blend) is assembled once per iteration,
+// thread per cell, into line records, factorised and solved one thread per line (block Thomas), i then j then k, and the
+// defect-correction passes reuse the kept blocks and factors.
 //   k3_prims      conserved -> primitive (padded, 2 ghost layers)                    (solver3.rs:222-236)
 //   k3_ghosts     characteristic far field (FP64), axis (the cell across the axis), slip wall, symmetry planes (solver3.rs:171-219)
 //   k3_flux       MUSCL in the face's cylindrical frame + HLLC / Rusanov blend + low-Mach correction, FP64 (flux3.rs, solver3.rs:365-418)
 //   k3_residual   R = -(1/V) sum S F (FP64 accumulation), local time step, FP64 density norm (solver3.rs:251-300)
-//   k3_lines      (I - dt J_dir) x = b along every line of direction dir (implicit3.rs:274-382)
-//   k3_defect     dt R - (A_i du + A_j du + A_k du - 2 du)                            (implicit3.rs:384-455)
+//   k3_assemble   blocks of I - dt J_i, J_j, J_k per cell into the line records           (implicit3.rs:214-355)
+//   k3_lines      first pass: block Thomas along every line of direction dir on the kept blocks, factors kept
+//   k3_lines_subst the defect-correction passes with the kept factors                  (implicit3.rs:274-382)
+//   k3_defect     dt R - (A_i du + A_j du + A_k du - 2 du) with the kept blocks         (implicit3.rs:384-455)
 //   k3_stage      SSP-RK3 stage                                                       (solver3.rs:303-327)
 //   k3_forces     FP64 wall-pressure force integration: CN, CA, centre of pressure     (run3.rs:150-190)
 #pragma once
@@ -315,7 +318,7 @@ struct B3 {
   const int* axis_k;  // [i * nk + k], i < axis_cells
   const Case3Dev* cs;
   int *iter, *ramp, *active;
-  float *U, *U0, *W, *R, *X, *DU, *RR, *dt, *scr;  // [case][var][cell]; W [case][var][padded]; scr [case][30][cell]
+  float *U, *U0, *W, *R, *X, *DU, *RR, *dt, *scr;  // [case][var][cell]; W [case][var][padded]; scr: line records (rec3)
   double *FI, *FJ, *FK;                             // face flux x area, [case][var][face]
   double* rsum;                                     // [slot][case]
 };
@@ -589,37 +592,108 @@ __device__ __forceinline__ void damped_update3(const B3& B, int b, long long c, 
   }
 }
 
-// One thread per line of direction dir: block Thomas with the blocks assembled on the way (implicit3.rs:133-156).
-// in: the right-hand side (from_res: dt R); epilogue 0: x -> out; 1: du = x; 2: du += x; `update` applies the damped update.
-__global__ void __launch_bounds__(128) k3_lines(B3 B, int dir, const float* in, int from_res, float* out, int epilogue, int pass) {
-  long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Line records of case b, direction dir: 130 planes of ncell floats: lo (25), d (25), up (25) assembled by k3_assemble;
+// M^-1 (25), Y = M^-1 up (25) by the factorising pass; g (5), the forward sweep of the current right-hand side.
+constexpr int REC3 = 130, R_LO = 0, R_D = 25, R_UP = 50, R_MINV = 75, R_Y = 100, R_G = 125;
+__device__ __forceinline__ float* rec3(const B3& B, int b, int dir) { return B.scr + ((long long)b * 3 + dir) * REC3 * B.nc; }
+// Index of cell (i, j, k) in the records of direction dir: the i-direction records are transposed (j fastest) so that the
+// threads of neighbouring i lines, which walk the lines side by side, read neighbouring addresses.
+__device__ __forceinline__ long long rcell(const B3& B, int dir, int i, int j, int k) {
+  return dir == 0 ? ((long long)k * B.ni + i) * B.nj + j : cell3(B, i, j, k);
+}
+__device__ __forceinline__ M5<float> ld5(const float* p, long long stride) {
+  M5<float> m;
+#pragma unroll
+  for (int q = 0; q < 25; ++q) m[q] = p[q * stride];
+  return m;
+}
+__device__ __forceinline__ void st5(float* p, long long stride, const M5<float>& m) {
+#pragma unroll
+  for (int q = 0; q < 25; ++q) p[q * stride] = m[q];
+}
+
+// Blocks of every cell into the line records (thread per cell). part 0: the i direction, threads ordered j fastest so that
+// the transposed i records are written side by side; part 1: the j and k directions, threads ordered i fastest.
+__global__ void __launch_bounds__(128) k3_assemble(B3 B, int part) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b = blockIdx.y;
-  const long long nlines = dir == 0 ? (long long)B.nj * B.nk : dir == 1 ? (long long)B.ni * B.nk : (long long)B.ni * B.nj;
-  if (L >= nlines || !B.active[b]) return;
-  const Case3Dev& cs = B.cs[b];
-  if (pass >= (cs.sub_iters > 1 ? cs.sub_iters : 1)) return;
-  const bool update = epilogue != 0 && pass == (cs.sub_iters > 1 ? cs.sub_iters : 1) - 1;
+  if (t >= B.nc || !B.active[b]) return;
+  int i, j, k;
+  if (part == 0) {
+    j = (int)(t % B.nj), i = (int)((t / B.nj) % B.ni), k = (int)(t / ((long long)B.ni * B.nj));
+  } else {
+    i = (int)(t % B.ni), j = (int)((t / B.ni) % B.nj), k = (int)(t / ((long long)B.ni * B.nj));
+  }
+#pragma unroll 1
+  for (int dir = part == 0 ? 0 : 1; dir < (part == 0 ? 1 : 3); ++dir) {
+    M5<float> lo, d, up;
+    blocks3(B, b, dir, i, j, k, lo, d, up);
+    float* r = rec3(B, b, dir) + rcell(B, dir, i, j, k);
+    st5(r + R_LO * B.nc, B.nc, lo);
+    st5(r + R_D * B.nc, B.nc, d);
+    st5(r + R_UP * B.nc, B.nc, up);
+  }
+}
+
+// line of direction dir through line index L: first cell, cell stride, length
+__device__ __forceinline__ void line3(const B3& B, int dir, long long L, long long& c0, long long& stride, int& n, long long& r0,
+                                      long long& rstride) {
   int i0, j0, k0;
   if (dir == 0) i0 = 0, j0 = (int)(L % B.nj), k0 = (int)(L / B.nj);
   else if (dir == 1) i0 = (int)(L % B.ni), j0 = 0, k0 = (int)(L / B.ni);
   else i0 = (int)(L % B.ni), j0 = (int)(L / B.ni), k0 = 0;
-  const int n = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
-  const long long stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
-  const long long c0 = cell3(B, i0, j0, k0);
-  float* Ys = B.scr + (long long)b * 30 * B.nc;  // [30][cell]: Y (25), g (5)
+  n = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
+  stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
+  c0 = cell3(B, i0, j0, k0);
+  r0 = rcell(B, dir, i0, j0, k0);
+  rstride = dir == 0 ? B.nj : stride;
+}
+__device__ __forceinline__ long long nlines3(const B3& B, int dir) {
+  return dir == 0 ? (long long)B.nj * B.nk : dir == 1 ? (long long)B.ni * B.nk : (long long)B.ni * B.nj;
+}
+
+// x of cell c: epilogue 0: x -> out; 1: du = x; 2: du += x; `update` applies the damped update
+__device__ __forceinline__ void emit3(const B3& B, int b, int epilogue, bool update, float* out, long long c, const V5<float>& x) {
+  if (epilogue == 0) {
+    stU(B, out, b, c, x);
+    return;
+  }
+  V5<float> du = x;
+  if (epilogue == 2) {
+    V5<float> o = ldU(B, B.DU, b, c);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) du[q] += o[q];
+  }
+  stU(B, B.DU, b, c, du);
+  if (update) damped_update3(B, b, c, du);
+}
+
+// First pass of an iteration, one thread per line: block Thomas on the kept blocks (implicit3.rs:133-156), keeping M^-1,
+// Y and g for the defect-correction passes. in: the right-hand side (from_res: dt R).
+__global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, int from_res, float* out, int epilogue) {
+  long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (L >= nlines3(B, dir) || !B.active[b]) return;
+  const Case3Dev& cs = B.cs[b];
+  const bool update = epilogue != 0 && (cs.sub_iters > 1 ? cs.sub_iters : 1) == 1;
+  long long c0, stride, r0, rs;
+  int n;
+  line3(B, dir, L, c0, stride, n, r0, rs);
+  float* R = rec3(B, b, dir) + r0;
+  const long long nc = B.nc;
   M5<float> Y = zero5();
   V5<float> g{{0, 0, 0, 0, 0}};
   for (int m = 0; m < n; ++m) {
-    long long c = c0 + m * stride;
-    M5<float> lo, d, up;
-    blocks3(B, b, dir, i0 + (dir == 0) * m, j0 + (dir == 1) * m, k0 + (dir == 2) * m, lo, d, up);
+    long long c = c0 + m * stride, rr = m * rs;
+    M5<float> d = ld5(R + R_D * nc + rr, nc);
     V5<float> r = ldU(B, in, b, c);
     if (from_res) {
-      float dtc = B.dt[(long long)b * B.nc + c];
+      float dtc = B.dt[(long long)b * nc + c];
 #pragma unroll
       for (int q = 0; q < 5; ++q) r[q] *= dtc;
     }
     if (m > 0) {
+      M5<float> lo = ld5(R + R_LO * nc + rr, nc);
       axpy5(d, -1.f, mm5(lo, Y));
       V5<float> t = mv5(lo, g);
 #pragma unroll
@@ -627,46 +701,104 @@ __global__ void __launch_bounds__(128) k3_lines(B3 B, int dir, const float* in, 
     }
     M5<float> Minv = inv5(d);
     g = mv5(Minv, r);
-    Y = mm5(Minv, up);
+    Y = mm5(Minv, ld5(R + R_UP * nc + rr, nc));
+    st5(R + R_MINV * nc + rr, nc, Minv);
+    st5(R + R_Y * nc + rr, nc, Y);
 #pragma unroll
-    for (int q = 0; q < 25; ++q) Ys[q * B.nc + c] = Y[q];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) Ys[(25 + q) * B.nc + c] = g[q];
+    for (int q = 0; q < 5; ++q) R[(R_G + q) * nc + rr] = g[q];
   }
   V5<float> xn = g;
-  auto emit = [&](long long c, const V5<float>& x) {
-    if (epilogue == 0) {
-      stU(B, out, b, c, x);
-      return;
-    }
-    V5<float> du = x;
-    if (epilogue == 2) {
-      V5<float> o = ldU(B, B.DU, b, c);
-#pragma unroll
-      for (int q = 0; q < 5; ++q) du[q] += o[q];
-    }
-    stU(B, B.DU, b, c, du);
-    if (update) damped_update3(B, b, c, du);
-  };
-  emit(c0 + (long long)(n - 1) * stride, xn);
+  emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
   for (int m = n - 2; m >= 0; --m) {
-    long long c = c0 + m * stride;
-    M5<float> Ym;
+    long long c = c0 + m * stride, rr = m * rs;
+    M5<float> Ym = ld5(R + R_Y * nc + rr, nc);
     V5<float> gm;
 #pragma unroll
-    for (int q = 0; q < 25; ++q) Ym[q] = Ys[q * B.nc + c];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) gm[q] = Ys[(25 + q) * B.nc + c];
+    for (int q = 0; q < 5; ++q) gm[q] = R[(R_G + q) * nc + rr];
     V5<float> t = mv5(Ym, xn);
 #pragma unroll
     for (int q = 0; q < 5; ++q) gm[q] -= t[q];
-    emit(c, gm);
+    emit3(B, b, epilogue, update, out, c, gm);
     xn = gm;
   }
   if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
 }
 
-// defect of the unfactored operator (implicit3.rs:440-446): rr = dt R - (A_i du + A_j du + A_k du - 2 du)
+// Defect-correction pass `pass` >= 1: the same line solve with the kept factors (forward g = M^-1 (r - lo g_prev),
+// backward x = g - Y x_next).
+__global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float* in, float* out, int epilogue, int pass) {
+  long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (L >= nlines3(B, dir) || !B.active[b]) return;
+  const Case3Dev& cs = B.cs[b];
+  const int s = cs.sub_iters > 1 ? cs.sub_iters : 1;
+  if (pass >= s) return;
+  const bool update = epilogue != 0 && pass == s - 1;
+  long long c0, stride, r0, rs;
+  int n;
+  line3(B, dir, L, c0, stride, n, r0, rs);
+  float* R = rec3(B, b, dir) + r0;
+  const long long nc = B.nc;
+  V5<float> g{{0, 0, 0, 0, 0}};
+  for (int m = 0; m < n; ++m) {
+    long long c = c0 + m * stride, rr = m * rs;
+    V5<float> r = ldU(B, in, b, c);
+    if (m > 0) {
+      V5<float> t = mv5(ld5(R + R_LO * nc + rr, nc), g);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) r[q] -= t[q];
+    }
+    g = mv5(ld5(R + R_MINV * nc + rr, nc), r);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) R[(R_G + q) * nc + rr] = g[q];
+  }
+  V5<float> xn = g;
+  emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
+  for (int m = n - 2; m >= 0; --m) {
+    long long c = c0 + m * stride, rr = m * rs;
+    V5<float> gm;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gm[q] = R[(R_G + q) * nc + rr];
+    V5<float> t = mv5(ld5(R + R_Y * nc + rr, nc), xn);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gm[q] -= t[q];
+    emit3(B, b, epilogue, update, out, c, gm);
+    xn = gm;
+  }
+  if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
+}
+
+// A_dir du of cell (i, j, k) with the kept blocks of direction dir (implicit3.rs:384-410)
+__device__ __forceinline__ V5<float> apply3(const B3& B, int b, int dir, int i, int j, int k, long long c, const V5<float>& du) {
+  const long long nc = B.nc;
+  const float* R = rec3(B, b, dir) + rcell(B, dir, i, j, k);
+  const int m = dir == 0 ? i : dir == 1 ? j : k, nl = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
+  const long long stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
+  V5<float> v = mv5(ld5(R + R_D * nc, nc), du);
+  if (m > 0) {
+    V5<float> t = mv5(ld5(R + R_LO * nc, nc), ldU(B, B.DU, b, c - stride));
+#pragma unroll
+    for (int q = 0; q < 5; ++q) v[q] += t[q];
+  }
+  if (m + 1 < nl) {
+    V5<float> t = mv5(ld5(R + R_UP * nc, nc), ldU(B, B.DU, b, c + stride));
+#pragma unroll
+    for (int q = 0; q < 5; ++q) v[q] += t[q];
+  }
+  return v;
+}
+
+// the i-direction product A_i du into X (free between passes), threads ordered j fastest like the transposed i records
+__global__ void __launch_bounds__(128) k3_defect_i(B3 B, int pass) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (t >= B.nc || !B.active[b] || pass >= B.cs[b].sub_iters) return;
+  int j = (int)(t % B.nj), i = (int)((t / B.nj) % B.ni), k = (int)(t / ((long long)B.ni * B.nj));
+  long long c = cell3(B, i, j, k);
+  stU(B, B.X, b, c, apply3(B, b, 0, i, j, k, c, ldU(B, B.DU, b, c)));
+}
+
+// defect of the unfactored operator (implicit3.rs:440-446): rr = dt R - (A_i du + A_j du + A_k du - 2 du), A_i du from X
 __global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b = blockIdx.y;
@@ -675,23 +807,10 @@ __global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
   if (pass >= cs.sub_iters) return;
   int i = (int)(c % B.ni), j = (int)((c / B.ni) % B.nj), k = (int)(c / ((long long)B.ni * B.nj));
   V5<float> du = ldU(B, B.DU, b, c);
-  V5<float> acc{{0, 0, 0, 0, 0}};
-  for (int dir = 0; dir < 3; ++dir) {
-    M5<float> lo, d, up;
-    blocks3(B, b, dir, i, j, k, lo, d, up);
-    const int m = dir == 0 ? i : dir == 1 ? j : k, nl = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
-    const long long stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
-    V5<float> v = mv5(d, du);
-    if (m > 0) {
-      V5<float> t = mv5(lo, ldU(B, B.DU, b, c - stride));
-#pragma unroll
-      for (int q = 0; q < 5; ++q) v[q] += t[q];
-    }
-    if (m + 1 < nl) {
-      V5<float> t = mv5(up, ldU(B, B.DU, b, c + stride));
-#pragma unroll
-      for (int q = 0; q < 5; ++q) v[q] += t[q];
-    }
+  V5<float> acc = ldU(B, B.X, b, c);
+#pragma unroll 1
+  for (int dir = 1; dir < 3; ++dir) {
+    V5<float> v = apply3(B, b, dir, i, j, k, c, du);
 #pragma unroll
     for (int q = 0; q < 5; ++q) acc[q] += v[q];
   }

@@ -229,7 +229,7 @@ struct Batch3 {
     size_t ns = (size_t)nb * 5 * B.nc;
     if ((rc = alloc(&B.U, ns)) || (rc = alloc(&B.U0, ns)) || (rc = alloc(&B.W, (size_t)nb * 5 * B.npad)) || (rc = alloc(&B.R, ns)) ||
         (rc = alloc(&B.X, ns)) || (rc = alloc(&B.DU, ns)) || (rc = alloc(&B.RR, ns)) || (rc = alloc(&B.dt, (size_t)nb * B.nc)) ||
-        (rc = alloc(&B.scr, (size_t)nb * 30 * B.nc)) || (rc = alloc(&B.FI, (size_t)nb * 5 * B.nfi)) || (rc = alloc(&B.FJ, (size_t)nb * 5 * B.nfj)) ||
+        (rc = alloc(&B.scr, (size_t)nb * 3 * REC3 * B.nc)) || (rc = alloc(&B.FI, (size_t)nb * 5 * B.nfi)) || (rc = alloc(&B.FJ, (size_t)nb * 5 * B.nfj)) ||
         (rc = alloc(&B.FK, (size_t)nb * 5 * B.nfk)) || (rc = alloc(&B.rsum, (size_t)slots * nb)) || (rc = alloc(&d_wall, wall.size())) ||
         (rc = alloc(&d_forces, 3 * (size_t)nb)))
       return rc;
@@ -330,11 +330,17 @@ struct Batch3 {
       launch_prep();
       k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2, slot);
       const long long li = (long long)B.nj * B.nk, lj = (long long)B.ni * B.nk, lk = (long long)B.ni * B.nj;
-      for (int p = 0; p < max_sub(); ++p) {
-        if (p > 0) k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
-        k3_lines<<<grid_of(li, 64), 64, 0, stream>>>(B, 0, p == 0 ? B.R : B.RR, p == 0, B.X, 0, p);
-        k3_lines<<<grid_of(lj, 64), 64, 0, stream>>>(B, 1, B.X, 0, B.X, 0, p);
-        k3_lines<<<grid_of(lk, 64), 64, 0, stream>>>(B, 2, B.X, 0, nullptr, p == 0 ? 1 : 2, p);
+      k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 0);
+      k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 1);
+      k3_lines<<<grid_of(li, 64), 64, 0, stream>>>(B, 0, B.R, 1, B.X, 0);
+      k3_lines<<<grid_of(lj, 64), 64, 0, stream>>>(B, 1, B.X, 0, B.X, 0);
+      k3_lines<<<grid_of(lk, 64), 64, 0, stream>>>(B, 2, B.X, 0, nullptr, 1);
+      for (int p = 1; p < max_sub(); ++p) {
+        k3_defect_i<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
+        k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
+        k3_lines_subst<<<grid_of(li, 128), 128, 0, stream>>>(B, 0, B.RR, B.X, 0, p);
+        k3_lines_subst<<<grid_of(lj, 128), 128, 0, stream>>>(B, 1, B.X, B.X, 0, p);
+        k3_lines_subst<<<grid_of(lk, 128), 128, 0, stream>>>(B, 2, B.X, nullptr, 2, p);
       }
     } else {  // SSP-RK3 (solver3.rs:303-314)
       launch_prep();
