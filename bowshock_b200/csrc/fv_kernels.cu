@@ -120,7 +120,7 @@ __device__ __forceinline__ double4 to_d4(const V4<double>& v) { return make_doub
 __device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(v.x, v.y, v.z, v.w); }
 
 // dt_kind: 0 = keep dt, 1 = explicit local time step (solver.rs:614-643), 2 = implicit pseudo-time step (implicit.rs:666-695)
-__global__ void __launch_bounds__(TI* TJ) k_residual(Arena A, int dt_kind, int slot) {
+__global__ void __launch_bounds__(TI* TJ, 3) k_residual(Arena A, int dt_kind, int slot) {
   __shared__ float4 sW[TJ + 4][TI + 4], sWl[TJ + 4][TI + 4];
   __shared__ double4 sFI[TJ][TI + 1];
   __shared__ double4 sFJ[TJ + 1][TI];
@@ -429,7 +429,7 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
 
 // Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
 // one thread per cell: the assembly is the arithmetic-heavy part of the operator and has no dependence along the lines.
-__global__ void __launch_bounds__(TI* TJ, 2) k_assemble(Arena A) {
+__global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
   int t = blockIdx.x;
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
