@@ -759,30 +759,52 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines_subst(Arena A, int di
   const int L = G.L, N = G.N, a = G.a, e = G.e, ke = G.ke;
   const int s = lane;
   auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
+  // the loops load the next cell's record before the dependent arithmetic of the current one (software pipelining)
   V4<float> g = mk4<float>(0, 0, 0, 0);
   if (G.act) {
+    long long cc = cell(a);
+    float4* rec = line_rec(A, dir_i != 0, cc);
+    M4<float> Lo = ld_m4(rec), Mi = ld_m4(rec + 12);
+    float4 rin = in[cc];
     for (int k = a; k <= ke; ++k) {
-      long long cc = cell(k);
-      float4* rec = line_rec(A, dir_i != 0, cc);
-      V4<float> r = from_f4(in[cc]);
+      M4<float> Lo_n = Lo, Mi_n = Mi;
+      float4 rin_n = rin;
+      float4* rec_n = rec;
+      if (k < ke) {
+        long long cn = cell(k + 1);
+        rec_n = line_rec(A, dir_i != 0, cn);
+        Lo_n = ld_m4(rec_n), Mi_n = ld_m4(rec_n + 12);
+        rin_n = in[cn];
+      }
+      V4<float> r = from_f4(rin);
       if (k > a) {
-        V4<float> t = mv(ld_m4(rec), g);
+        V4<float> t = mv(Lo, g);
 #pragma unroll
         for (int q = 0; q < 4; ++q) r[q] -= t[q];
       }
-      g = mv(ld_m4(rec + 12), r);
+      g = mv(Mi, r);
       rec[24] = to_f4(g);
+      rec = rec_n, Lo = Lo_n, Mi = Mi_n, rin = rin_n;
     }
   }
   const V4<float> v_l = g;
   V4<float> v_f = v_l;
-  if (G.act) {
+  if (G.act && ke - 1 >= a) {
+    const float4* rec = line_rec(A, dir_i != 0, cell(ke - 1));
+    M4<float> Yk = ld_m4(rec + 16);
+    float4 gk4 = rec[24];
     for (int k = ke - 1; k >= a; --k) {
-      const float4* rec = line_rec(A, dir_i != 0, cell(k));
-      V4<float> t = mv(ld_m4(rec + 16), v_f);
-      V4<float> gk = from_f4(rec[24]);
+      M4<float> Y_n = Yk;
+      float4 g_n = gk4;
+      if (k > a) {
+        const float4* rn = line_rec(A, dir_i != 0, cell(k - 1));
+        Y_n = ld_m4(rn + 16), g_n = rn[24];
+      }
+      V4<float> t = mv(Yk, v_f);
+      V4<float> gk = from_f4(gk4);
 #pragma unroll
       for (int q = 0; q < 4; ++q) v_f[q] = gk[q] - t[q];
+      Yk = Y_n, gk4 = g_n;
     }
   }
   const V4<float> vn = shfl_down4(v_f, 1);
@@ -821,16 +843,29 @@ __global__ void __launch_bounds__(32 * LINE_WARPS) k_lines_subst(Arena A, int di
   if (!G.act) return;
   V4<float> xn = G.has_sep ? lsep : mk4<float>(0, 0, 0, 0);
   if (G.has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
-  for (int k = ke; k >= a; --k) {
-    long long cc = cell(k);
+  {
+    long long cc = cell(ke);
     const float4* rec = line_rec(A, dir_i != 0, cc);
-    V4<float> t1 = mv(ld_m4(rec + 20), lprev), t2 = mv(ld_m4(rec + 16), xn);
-    V4<float> gk = from_f4(rec[24]);
-    V4<float> x;
+    M4<float> GEk = ld_m4(rec + 20), Yk = ld_m4(rec + 16);
+    float4 gk4 = rec[24];
+    for (int k = ke; k >= a; --k) {
+      M4<float> GE_n = GEk, Y_n = Yk;
+      float4 g_n = gk4;
+      long long cn = cc;
+      if (k > a) {
+        cn = cell(k - 1);
+        const float4* rn = line_rec(A, dir_i != 0, cn);
+        GE_n = ld_m4(rn + 20), Y_n = ld_m4(rn + 16), g_n = rn[24];
+      }
+      V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
+      V4<float> gk = from_f4(gk4);
+      V4<float> x;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
-    line_emit(A, epilogue, update, out, cc, x);
-    xn = x;
+      for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
+      line_emit(A, epilogue, update, out, cc, x);
+      xn = x;
+      cc = cn, GEk = GE_n, Yk = Y_n, gk4 = g_n;
+    }
   }
   if (update && L == 0 && lane == 0) {
     A.iter[ci] += 1;
