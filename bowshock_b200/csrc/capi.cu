@@ -585,10 +585,6 @@ struct bowshock_arena {
   double last_solve_ms = 0.0;
 };
 
-static int afail(bowshock_arena* a, int code, const std::string& m) {
-  if (a) a->last_error = m;
-  return code;
-}
 static int afrom(bowshock_arena* a, int rc) {
   if (rc) a->last_error = a->ar.err;
   return rc;

@@ -45,7 +45,7 @@ __global__ void k_forces(Arena A, const BodyDev* bodies, const double* nx, const
   for (int k = threadIdx.x; k <= F_NF; k += blockDim.x) acc[k] = 0.0;
   if (threadIdx.x == 0) yplus_bits = 0ull;
   __syncthreads();
-  const int ni = c.ni, nj = c.nj;
+  const int ni = c.ni;
   const long long no = node_off[ci];
   auto X = [&](int i, int j) { return nx[no + (long long)j * (ni + 1) + i]; };
   auto R = [&](int i, int j) { return nr[no + (long long)j * (ni + 1) + i]; };

@@ -293,7 +293,7 @@ __global__ void k_stage(Arena A, float a, float b, int copy, int last) {
 
 // Blocks (lo, d, up) of I - dt J_dir for fluid cell (i, j) of a line (implicit.rs:379-467).
 __device__ void assemble(const Arena& A, const CaseDev& c, bool dir_i, int i, int j, M4<float>& lo, M4<float>& d, M4<float>& up) {
-  const int k = dir_i ? i : j, n = dir_i ? c.ni : c.nj;
+  const int k = dir_i ? i : j;
   const int k0 = dir_i ? row_start(c, j) : col_start(c, i);
   const long long cc = cidx(c, i, j);
   V4<float> wk = Wat(A, c, i, j);
