@@ -269,6 +269,7 @@ def run_ours(args, rank, world, dist):
     steady = 3600.0 * len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * n_k)))
     # per-kernel profile (CUDA events around every launch) for the roofline of the dominant kernel group
     prof = arena.profile(5)
+    tuning = arena.tuning()
     del arena
     hbm, peak_kind = peaks()
     # plain single-case backend: each case alone, to its stop rule, wall clock
@@ -339,6 +340,7 @@ def run_ours(args, rank, world, dist):
             "batched_vs_plain_e2e": e2e_value / world / plain_cases_per_hr if plain_cases_per_hr else None,
             "learned_warm_start": "not built: cold (free-stream) starts",
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
+            "autotuned_lines_per_block": tuning,
             "parallelism": f"cases-per-GPU replicas x{world}",
         },
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -373,7 +375,8 @@ def run_kernels(args):
     arena.run(args.steps)
     ms = arena.ms_per_iter()
     prof = {g: round(v[0] / v[1], 4) for g, v in arena.profile(3).items() if v[1]} if args.steps >= 10 else None
-    return {"kernels_only": True, "cells": arena.cells, "steps": args.steps, "ms_per_step": ms, "ms_per_launch": prof}
+    return {"kernels_only": True, "cells": arena.cells, "steps": args.steps, "ms_per_step": ms, "ms_per_launch": prof,
+            "autotuned_lines_per_block": arena.tuning()}
 
 
 def main():

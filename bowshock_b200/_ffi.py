@@ -140,6 +140,7 @@ SIGNATURES = {
     "bowshock_arena_last_ms_per_iter": (_I, [_P, _dp]),
     "bowshock_arena_last_solve_ms": (_I, [_P, _dp]),
     "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
+    "bowshock_arena_tuning": (_I, [_P, C.POINTER(C.c_int32)]),
     "bowshock_solver_run_noalloc": (_I, [_P, _U, _dp]),
 }
 

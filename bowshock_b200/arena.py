@@ -64,7 +64,7 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_last_solve_ms(self._h, C.byref(d)))
         return d.value
 
-    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage", "subst_i", "subst_j", "assemble")
+    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage", "subst_i", "subst_j", "assemble", "turb_lines")
 
     def profile(self, n: int):
         """Per-kernel-group device time over n iterations launched one kernel at a time: {group: (ms, launches)}."""
@@ -72,6 +72,12 @@ class Arena:
         cnt = (C.c_uint64 * len(self.PROFILE_GROUPS))()
         self._check(_ffi.load().bowshock_arena_profile(self._h, int(n), _ffi.dptr(ms), cnt))
         return {g: (float(ms[k]), int(cnt[k])) for k, g in enumerate(self.PROFILE_GROUPS)}
+
+    def tuning(self):
+        """Lines per block the autotuner picked: {"lines": .., "subst": .., "turb_lines": ..}."""
+        out = (C.c_int32 * 3)()
+        self._check(_ffi.load().bowshock_arena_tuning(self._h, out))
+        return dict(lines=out[0], subst=out[1], turb_lines=out[2])
 
     def solve(self, progress=None):
         """Cold-start every case and iterate each to its stop rule (converged cases are masked out)."""

@@ -655,11 +655,19 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
   for (uint64_t k = 0; !rc && k < ncases; ++k) rc = a->fp.set_body(a->ar, (int)k, &cases[k].body);
   for (uint64_t k = 0; !rc && k < ncases; ++k)
     if (a->ar.cases[k].viscous && a->ar.cases[k].turbulence == 1) rc = a->ar.turb_init((int)k);
+  // lines per block of the line kernels, tuned on the arena's own cases when it is large enough to matter
+  if (!rc && a->ar.ncell >= 100000) rc = a->ar.autotune();
   if (rc) {
     delete a;
     return BOWSHOCK_CUDA_ERROR;
   }
   *out = a;
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_tuning(const bowshock_arena* a, int32_t* lines_per_block) {
+  if (!a || !lines_per_block) return BOWSHOCK_INVALID;
+  lines_per_block[0] = a->ar.lw_lines, lines_per_block[1] = a->ar.lw_subst, lines_per_block[2] = a->ar.lw_turb;
   return BOWSHOCK_OK;
 }
 

@@ -377,7 +377,7 @@ __device__ __forceinline__ void damped_update(const Arena& A, long long cc, cons
   }
 }
 
-constexpr int LINE_WARPS = 4;
+constexpr int LINE_WARPS = 4;  // default lines per block of the line kernels
 struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
   float a[16], b[16], c[16], d[4];
 };
@@ -523,11 +523,12 @@ __global__ void k_line_ends(Arena A) {
 // reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
 // back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line
 // records for the later passes and the defect.
-__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out) {
-  __shared__ PcrSlot sp[LINE_WARPS][32];
-  __shared__ float4 sl[LINE_WARPS][32];
+template <int W>  // lines (warps) per block, chosen by the arena's autotuner
+__global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out) {
+  __shared__ PcrSlot sp[W][32];
+  __shared__ float4 sl[W][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * LINE_WARPS + warp;
+  const int gw = blockIdx.x * W + warp;
   LineSeg G;
   if (!line_seg(A, dir_i, gw, lane, G)) return;
   const int ci = G.ci;
@@ -746,9 +747,10 @@ __device__ __forceinline__ V4<float> shfl_down4(const V4<float>& v, int h) {
 // Defect-correction pass `pass` >= 1 (implicit.rs:622-639) of every case with more than `pass` passes: the same solve
 // with the factors of the first pass. Per cell: g = M^-1 (r - lo g_prev) forward, the separators' right-hand sides, the
 // reduction of the right-hand side alone with the kept multipliers (warp shuffles), x = g + GE l_left - Y x_next backward.
-__global__ void __launch_bounds__(32 * LINE_WARPS) k_lines_subst(Arena A, int dir_i, const float4* in, float4* out, int pass) {
+template <int W>  // lines (warps) per block, chosen by the arena's autotuner
+__global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, const float4* in, float4* out, int pass) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * LINE_WARPS + warp;
+  const int gw = blockIdx.x * W + warp;
   LineSeg G;
   if (!line_seg(A, dir_i, gw, lane, G)) return;
   const int ci = G.ci;

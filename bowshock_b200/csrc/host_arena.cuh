@@ -680,7 +680,7 @@ struct ArenaHost {
 
   // ---------------------------------------------------------------- one iteration (stream-ordered launches)
   // Kernel groups of the per-kernel profile (CUDA events around every launch when `profiling` is set).
-  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_SUBST_I, G_SUBST_J, G_ASSEMBLE, G_N };
+  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_SUBST_I, G_SUBST_J, G_ASSEMBLE, G_TURB_LINES, G_N };
   bool profiling = false;
   double prof_ms[G_N] = {0};
   long long prof_launches[G_N] = {0};
@@ -701,6 +701,80 @@ struct ArenaHost {
     prof_ms[g] += ms;
     prof_launches[g] += 1;
   }
+  // lines per block of the line kernels (1, 2, 4 or 8), picked by autotune()
+  int lw_lines = LINE_WARPS, lw_subst = LINE_WARPS, lw_turb = TL_WARPS;
+  void launch_lines(int dir_i, const float4* in, int from_res, float4* out) {
+    const int nl = dir_i ? nil : njl, w = lw_lines > 4 ? 4 : lw_lines;  // 8 lines would exceed the static shared memory
+    const int nb = (nl + w - 1) / w;
+    switch (w) {
+      case 1: k_lines<1><<<nb, 32, 0, stream>>>(A, dir_i, in, from_res, out); break;
+      case 2: k_lines<2><<<nb, 64, 0, stream>>>(A, dir_i, in, from_res, out); break;
+      default: k_lines<4><<<nb, 128, 0, stream>>>(A, dir_i, in, from_res, out); break;
+    }
+  }
+  void launch_subst(int dir_i, const float4* in, float4* out, int pass) {
+    const int nl = dir_i ? nil : njl, w = lw_subst;
+    const int nb = (nl + w - 1) / w;
+    switch (w) {
+      case 1: k_lines_subst<1><<<nb, 32, 0, stream>>>(A, dir_i, in, out, pass); break;
+      case 2: k_lines_subst<2><<<nb, 64, 0, stream>>>(A, dir_i, in, out, pass); break;
+      case 8: k_lines_subst<8><<<nb, 256, 0, stream>>>(A, dir_i, in, out, pass); break;
+      default: k_lines_subst<4><<<nb, 128, 0, stream>>>(A, dir_i, in, out, pass); break;
+    }
+  }
+  void launch_turb_lines(int dir_i) {
+    const int nl = dir_i ? nil : njl, w = lw_turb;
+    const int nb = (nl + w - 1) / w;
+    switch (w) {
+      case 1: k_turb_lines_w<1><<<nb, 32, 0, stream>>>(A, dir_i); break;
+      case 2: k_turb_lines_w<2><<<nb, 64, 0, stream>>>(A, dir_i); break;
+      case 8: k_turb_lines_w<8><<<nb, 256, 0, stream>>>(A, dir_i); break;
+      default: k_turb_lines_w<4><<<nb, 128, 0, stream>>>(A, dir_i); break;
+    }
+  }
+  // Autotuner: lines per block of the block line kernels (first pass and substitution passes) and of the SST line
+  // kernel, each the fastest of {1, 2, 4, 8} over two timed iterations of this arena's own cases. The state, turbulence
+  // and counters are restored afterwards; the choice does not change any result (every warp solves one line alone).
+  int autotune() {
+    if (scheme_of_arena() != SCHEME_IMPLICIT) return 0;
+    const size_t nc = cases.size();
+    std::vector<float4> hu(ncell), hl(ncell);
+    std::vector<float2> ht(any_sst ? ncell : 0);
+    std::vector<float> hm(any_sst ? ncell : 0);
+    std::vector<int> hit(nc), hr(nc);
+    BK_CUDA(cudaStreamSynchronize(stream));
+    BK_CUDA(cudaMemcpy(hu.data(), A.U, ncell * sizeof(float4), cudaMemcpyDeviceToHost));
+    BK_CUDA(cudaMemcpy(hl.data(), A.Ulo, ncell * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (any_sst) {
+      BK_CUDA(cudaMemcpy(ht.data(), A.turb, ncell * sizeof(float2), cudaMemcpyDeviceToHost));
+      BK_CUDA(cudaMemcpy(hm.data(), A.mu_t, ncell * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    BK_CUDA(cudaMemcpy(hit.data(), d_iter, nc * sizeof(int), cudaMemcpyDeviceToHost));
+    BK_CUDA(cudaMemcpy(hr.data(), d_ramp, nc * sizeof(int), cudaMemcpyDeviceToHost));
+    const int cand[4] = {1, 2, 4, 8};
+    double best[3] = {1e30, 1e30, 1e30};
+    int pick[3] = {LINE_WARPS, LINE_WARPS, TL_WARPS};
+    int rc = 0;
+    for (int w : cand) {
+      lw_lines = lw_subst = lw_turb = w;
+      if ((rc = profile(1))) return rc;  // warm-up of this variant
+      if ((rc = profile(2))) return rc;
+      double t[3] = {prof_ms[G_LINES_I] + prof_ms[G_LINES_J], prof_ms[G_SUBST_I] + prof_ms[G_SUBST_J], prof_ms[G_TURB_LINES]};
+      for (int q = 0; q < 3; ++q)
+        if (t[q] < best[q]) best[q] = t[q], pick[q] = w;
+    }
+    lw_lines = pick[0] > 4 ? 4 : pick[0], lw_subst = pick[1], lw_turb = pick[2];
+    BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
+    if (any_sst) {
+      BK_CUDA(cudaMemcpy(A.turb, ht.data(), ncell * sizeof(float2), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(A.mu_t, hm.data(), ncell * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    BK_CUDA(cudaMemcpy(d_iter, hit.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(cudaMemcpy(d_ramp, hr.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    return 0;
+  }
   void launch_mean_flow_prep() {
     L(G_PRIMS, [&] { k_prims<<<npblk, 256, 0, stream>>>(A); });
     if (any_viscous) {
@@ -715,7 +789,6 @@ struct ArenaHost {
     return s;
   }
   void launch_iteration(int slot) {
-    const int lb_i = (nil + LINE_WARPS - 1) / LINE_WARPS, lb_j = (njl + LINE_WARPS - 1) / LINE_WARPS;
     if (scheme_of_arena() == SCHEME_MULTIGRID) {
       mg_level(0, slot);
       set_level(0);
@@ -725,12 +798,12 @@ struct ArenaHost {
       const int s = sub_iters_of_arena();
       L(G_ASSEMBLE, [&] { k_assemble<<<ntiles, TI * TJ, 0, stream>>>(A); });
       L(G_ASSEMBLE, [&] { k_line_ends<<<(nil + njl + 127) / 128, 128, 0, stream>>>(A); });
-      L(G_LINES_I, [&] { k_lines<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.R, 1, A.X); });
-      L(G_LINES_J, [&] { k_lines<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, 0, nullptr); });
+      L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
+      L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
         L(G_DEFECT, [&] { k_defect<<<ntiles, TI * TJ, 0, stream>>>(A, p); });
-        L(G_SUBST_I, [&] { k_lines_subst<<<lb_i, 32 * LINE_WARPS, 0, stream>>>(A, 1, A.RR, A.X, p); });
-        L(G_SUBST_J, [&] { k_lines_subst<<<lb_j, 32 * LINE_WARPS, 0, stream>>>(A, 0, A.X, nullptr, p); });
+        L(G_SUBST_I, [&] { launch_subst(1, A.RR, A.X, p); });
+        L(G_SUBST_J, [&] { launch_subst(0, A.X, nullptr, p); });
       }
       if (any_sst) {
         // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step
@@ -738,8 +811,8 @@ struct ArenaHost {
         L(G_TURB, [&] { k_turb_blend<<<ntiles, TI * TJ, 0, stream>>>(A); });
         L(G_TURB, [&] { k_turb_cell<<<ntiles, TI * TJ, 0, stream>>>(A, slot); });
         if (max_line <= 32 * TL_MAXM) {
-          L(G_TURB, [&] { k_turb_lines_w<<<(nil + TL_WARPS - 1) / TL_WARPS, 32 * TL_WARPS, 0, stream>>>(A, 1); });
-          L(G_TURB, [&] { k_turb_lines_w<<<(njl + TL_WARPS - 1) / TL_WARPS, 32 * TL_WARPS, 0, stream>>>(A, 0); });
+          L(G_TURB_LINES, [&] { launch_turb_lines(1); });
+          L(G_TURB_LINES, [&] { launch_turb_lines(0); });
         } else {
           L(G_TURB, [&] { k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1); });
           L(G_TURB, [&] { k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0); });

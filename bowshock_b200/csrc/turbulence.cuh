@@ -330,9 +330,10 @@ __device__ __forceinline__ float2 shfl_down2(float2 v, int h) {
   return make_float2(__shfl_down_sync(0xffffffffu, v.x, h), __shfl_down_sync(0xffffffffu, v.y, h));
 }
 
-__global__ void __launch_bounds__(32 * TL_WARPS) k_turb_lines_w(Arena A, int dir_i) {
+template <int W>  // lines (warps) per block, chosen by the arena's autotuner
+__global__ void __launch_bounds__(32 * W) k_turb_lines_w(Arena A, int dir_i) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int line = blockIdx.x * TL_WARPS + warp;
+  const int line = blockIdx.x * W + warp;
   const int nl = dir_i ? A.nilines : A.njlines;
   if (line >= nl) return;  // uniform per warp
   const int ci = dir_i ? A.iline_case[line] : A.jline_case[line];

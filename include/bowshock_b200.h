@@ -290,10 +290,16 @@ int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
 
 /* Per-kernel profile (the reference's Profile of gpu/mod.rs:533-542): n iterations launched one kernel at a time with CUDA
  * events around each launch; per kernel group (prims, viscous, residual, i-lines, j-lines (the factorising first pass),
- * defect, turbulence, stage, i- and j-substitution passes, block assembly) the
+ * defect, turbulence, stage, i- and j-substitution passes, block assembly, SST line systems) the
  * total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
-#define BOWSHOCK_PROFILE_GROUPS 11
+#define BOWSHOCK_PROFILE_GROUPS 12
 int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
+/* Lines per block (1, 2 or 4 for the first pass; 1, 2, 4 or 8 otherwise) of the block line kernels' first pass, of their
+ * substitution passes and of the SST line
+ * kernel, as the arena's autotuner picked them at creation (arenas of 100,000 cells or more; 4 otherwise): the fastest
+ * of two timed iterations of the arena's own cases per candidate, the state restored afterwards. No counterpart in the
+ * reference (its line solves run in Luma, gpu/implicit.rs:731-732). */
+int bowshock_arena_tuning(const bowshock_arena* a, int32_t* lines_per_block);
 
 /* ---------------------------------------------------------------------------------------------- 3D Euler
  * The stability path (crates/bowshock-cfd/src/solver3.rs + implicit3.rs behind `GpuSolver3`, gpu/mod.rs:442-560, driven
