@@ -89,6 +89,10 @@ struct Arena {
   // FAS multigrid: the restricted state at the start of a coarse cycle, and the user's mask the level masks derive from
   float4 *MG0, *MG0lo;
   int* enabled;
+  // Compaction: when some cases are masked out, the launches run over the active cases' tiles, padded-array blocks and
+  // lines only; the kernels map their block / line index through these lists (null: every entry).
+  const int *tile_list, *pblk_list, *iline_list, *jline_list;
+  int n_tl, n_pb, n_il, n_jl;
 };
 
 constexpr int TI = 32, TJ = 8;  // residual tile
@@ -125,6 +129,18 @@ __device__ __forceinline__ void pair_st(float4* hi, float4* lo, long long k, con
   lo[k] = make_float4((float)(q[0] - (double)h.x), (float)(q[1] - (double)h.y), (float)(q[2] - (double)h.z), (float)(q[3] - (double)h.w));
 }
 __device__ __forceinline__ V4<double> state_of(const Arena& A, long long k) { return pair_ld(A.U[k], A.Ulo[k]); }
+
+__device__ __forceinline__ int tile_at(const Arena& A) { return A.tile_list ? A.tile_list[blockIdx.x] : (int)blockIdx.x; }
+__device__ __forceinline__ int pblk_at(const Arena& A) { return A.pblk_list ? A.pblk_list[blockIdx.x] : (int)blockIdx.x; }
+__device__ __forceinline__ int lines_of(const Arena& A, bool dir_i) {
+  return dir_i ? (A.iline_list ? A.n_il : A.nilines) : (A.jline_list ? A.n_jl : A.njlines);
+}
+// the idx-th line of direction dir of this launch, -1 past the end
+__device__ __forceinline__ int line_at(const Arena& A, bool dir_i, int idx) {
+  if (idx >= lines_of(A, dir_i)) return -1;
+  const int* l = dir_i ? A.iline_list : A.jline_list;
+  return l ? l[idx] : idx;
+}
 
 __device__ __forceinline__ long long cidx(const CaseDev& c, int i, int j) { return c.cell_off + (long long)j * c.ni + i; }
 __device__ __forceinline__ long long pidx(const CaseDev& c, int i, int j) { return c.pad_off + (long long)(j + 2) * (c.ni + 4) + (i + 2); }

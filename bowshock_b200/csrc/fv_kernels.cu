@@ -24,7 +24,7 @@ __device__ __forceinline__ V4<double> fs_of(const CaseDev& c) { return mk4<doubl
 // ==================================================================================== primitives + ghosts
 // FP64 from the state pair, stored as the pair (W, Wlo); the ghosts in FP64 as well.
 __global__ void k_prims(Arena A) {
-  int b = blockIdx.x;
+  int b = pblk_at(A);
   int ci = A.pblk_case[b];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_residual(Arena A, int dt_kind, in
   __shared__ double4 sFJ[TJ + 1][TI];
   __shared__ double sred[TI * TJ / 32];
   __shared__ float s_cfl;
-  const int t = blockIdx.x;
+  const int t = tile_at(A);
   const int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_residual(Arena A, int dt_kind, in
 // ==================================================================================== explicit stage
 // u = a (u + dt R) + b u0 on the fluid cells; `copy` first saves u0 = u; `last` advances the iteration counter.
 __global__ void k_stage(Arena A, float a, float b, int copy, int last) {
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
@@ -385,12 +385,14 @@ struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
 // Line geometry shared by the factorisation and substitution kernels: warp `gw` solves line L of case c; lane s owns the
 // segment [a, e) of m = max(2, ceil(len/32)) cells, the last cell of every segment but the last is a separator.
 struct LineSeg {
-  int ci, L, n, k0, len, m, P, N, a, e, ke;
+  int gw, ci, L, n, k0, len, m, P, N, a, e, ke;
   bool act, has_sep;
 };
-__device__ __forceinline__ bool line_seg(const Arena& A, int dir_i, int gw, int lane, LineSeg& g) {
-  const int nl = dir_i ? A.nilines : A.njlines;
-  if (gw >= nl) return false;
+// idx: the line's position in this launch (mapped through the compaction list)
+__device__ __forceinline__ bool line_seg(const Arena& A, int dir_i, int idx, int lane, LineSeg& g) {
+  const int gw = line_at(A, dir_i != 0, idx);
+  if (gw < 0) return false;
+  g.gw = gw;
   g.ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
   const CaseDev& c = A.cases[g.ci];
   g.L = gw - (dir_i ? c.iline_off : c.jline_off);
@@ -430,7 +432,7 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
 // Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
 // one thread per cell: the assembly is the arithmetic-heavy part of the operator and has no dependence along the lines.
 __global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
@@ -509,9 +511,10 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
 // every i line, then every j line, of the active cases
 __global__ void k_line_ends(Arena A) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool dir_i = t < A.nilines;
-  int gw = dir_i ? t : t - A.nilines;
-  if (!dir_i && gw >= A.njlines) return;
+  const int nli = lines_of(A, true);
+  bool dir_i = t < nli;
+  int gw = line_at(A, dir_i, dir_i ? t : t - nli);
+  if (gw < 0) return;
   int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
@@ -635,7 +638,7 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   }
   __syncwarp();
   // ---- parallel cyclic reduction of the N separator rows across the warp; multipliers kept per level
-  float4* prec = pcr_rec(A, dir_i != 0, gw, s);
+  float4* prec = pcr_rec(A, dir_i != 0, G.gw, s);
   int lvl = 0;
   for (int h = 1; h < N; h <<= 1, ++lvl) {
     M4<float> binv = inv4(rb);
@@ -819,7 +822,7 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
 #pragma unroll
     for (int q = 0; q < 4; ++q) rd[q] = r[q] - t1[q] - t2[q];
   }
-  const float4* prec = pcr_rec(A, dir_i != 0, gw, s);
+  const float4* prec = pcr_rec(A, dir_i != 0, G.gw, s);
   int lvl = 0;
   for (int h = 1; h < N; h <<= 1, ++lvl) {
     V4<float> dm = shfl_up4(rd, h), dp = shfl_down4(rd, h);
@@ -878,7 +881,7 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
 // Defect of the unfactored operator (implicit.rs:622-630): rr = dt R - (A_i du + A_j du - du), per fluid cell, with the
 // blocks the first pass kept in the line records.
 __global__ void k_defect(Arena A, int pass) {
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || pass >= c.sub_iters) return;

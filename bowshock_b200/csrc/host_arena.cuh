@@ -244,6 +244,11 @@ struct ArenaHost {
   long long ncell = 0, npad = 0, nif = 0, njf = 0;
   int ntiles = 0, nil = 0, njl = 0, npblk = 0;
   int max_line = 0;  // longest i or j line of any case
+  int *d_tlist = nullptr, *d_pblist = nullptr, *d_illist = nullptr, *d_jllist = nullptr;  // compaction lists
+  // launch sizes: the active entries when compacted, every entry otherwise
+  int LT() const { return A.tile_list ? A.n_tl : ntiles; }
+  int LP() const { return A.pblk_list ? A.n_pb : npblk; }
+  int LI(int dir_i) const { return dir_i ? (A.iline_list ? A.n_il : nil) : (A.jline_list ? A.n_jl : njl); }
   // floats of the line-solve records: 25 float4 per cell and direction, 44 float4 per lane of every line
   size_t scratch_floats() const { return 4 * ((size_t)2 * ncell * 25 + (size_t)(nil + njl) * 32 * 44); }
   bool any_viscous = false, any_sst = false;
@@ -268,8 +273,9 @@ struct ArenaHost {
     void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0, A.Ulo, A.Wlo, A.U0lo, A.MG0lo,
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
                     A.grad4, A.gradT, A.mu, A.mu_t, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
-                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled};
+                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled, d_tlist, d_pblist, d_illist, d_jllist};
     d_enabled = nullptr;
+    d_tlist = d_pblist = d_illist = d_jllist = nullptr;
     for (void* p : ptrs)
       if (p) cudaFree(p);
     d_cases = nullptr;
@@ -374,6 +380,10 @@ struct ArenaHost {
     ALLOC(d_iline, nil);
     ALLOC(d_jline, njl);
     ALLOC(d_pblk, npblk);
+    ALLOC(d_tlist, ntiles);
+    ALLOC(d_pblist, npblk);
+    ALLOC(d_illist, nil);
+    ALLOC(d_jllist, njl);
     ALLOC(A.U, ncell);
     ALLOC(A.W, npad);
     ALLOC(A.R, ncell);
@@ -636,6 +646,38 @@ struct ArenaHost {
     else
       BK_CUDA(cudaMemcpyAsync(d_active, h_active.data(), cases.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
     BK_CUDA(cudaStreamSynchronize(stream));
+    return compact_lists();
+  }
+  // Launch only over the active cases' tiles, padded blocks and lines once some cases are masked out (not with a
+  // multigrid hierarchy, whose level masks change inside an iteration). A changed list invalidates the captured graph.
+  int compact_lists() {
+    const int nc = (int)cases.size();
+    int n_act = 0;
+    for (int k = 0; k < nc; ++k) n_act += h_active[k];
+    const bool want = mg_levels <= 1 && n_act > 0 && n_act < nc;
+    std::vector<int> tl, pb, il, jl;
+    if (want) {
+      for (int k = 0; k < nc; ++k) {
+        if (!h_active[k]) continue;
+        const CaseDev& c = desc[k];
+        const HostCase& h = cases[k];
+        int nt = c.ntx * c.nty, nb = (int)(((long long)(h.ni + 4) * (h.nj + 4) + 255) / 256);
+        for (int q = 0; q < nt; ++q) tl.push_back(c.tile_off + q);
+        for (int q = 0; q < nb; ++q) pb.push_back(c.pblk_off + q);
+        for (int q = 0; q < h.nj; ++q) il.push_back(c.iline_off + q);
+        for (int q = 0; q < h.ni; ++q) jl.push_back(c.jline_off + q);
+      }
+      BK_CUDA(cudaMemcpy(d_tlist, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(d_pblist, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(d_illist, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(d_jllist, jl.data(), jl.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    A.tile_list = want ? d_tlist : nullptr;
+    A.pblk_list = want ? d_pblist : nullptr;
+    A.iline_list = want ? d_illist : nullptr;
+    A.jline_list = want ? d_jllist : nullptr;
+    A.n_tl = (int)tl.size(), A.n_pb = (int)pb.size(), A.n_il = (int)il.size(), A.n_jl = (int)jl.size();
+    if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
     return 0;
   }
 
@@ -704,7 +746,7 @@ struct ArenaHost {
   // lines per block of the line kernels (1, 2, 4 or 8), picked by autotune()
   int lw_lines = LINE_WARPS, lw_subst = LINE_WARPS, lw_turb = TL_WARPS;
   void launch_lines(int dir_i, const float4* in, int from_res, float4* out) {
-    const int nl = dir_i ? nil : njl, w = lw_lines > 4 ? 4 : lw_lines;  // 8 lines would exceed the static shared memory
+    const int nl = LI(dir_i), w = lw_lines > 4 ? 4 : lw_lines;  // 8 lines would exceed the static shared memory
     const int nb = (nl + w - 1) / w;
     switch (w) {
       case 1: k_lines<1><<<nb, 32, 0, stream>>>(A, dir_i, in, from_res, out); break;
@@ -713,7 +755,7 @@ struct ArenaHost {
     }
   }
   void launch_subst(int dir_i, const float4* in, float4* out, int pass) {
-    const int nl = dir_i ? nil : njl, w = lw_subst;
+    const int nl = LI(dir_i), w = lw_subst;
     const int nb = (nl + w - 1) / w;
     switch (w) {
       case 1: k_lines_subst<1><<<nb, 32, 0, stream>>>(A, dir_i, in, out, pass); break;
@@ -723,7 +765,7 @@ struct ArenaHost {
     }
   }
   void launch_turb_lines(int dir_i) {
-    const int nl = dir_i ? nil : njl, w = lw_turb;
+    const int nl = LI(dir_i), w = lw_turb;
     const int nb = (nl + w - 1) / w;
     switch (w) {
       case 1: k_turb_lines_w<1><<<nb, 32, 0, stream>>>(A, dir_i); break;
@@ -776,10 +818,10 @@ struct ArenaHost {
     return 0;
   }
   void launch_mean_flow_prep() {
-    L(G_PRIMS, [&] { k_prims<<<npblk, 256, 0, stream>>>(A); });
+    L(G_PRIMS, [&] { k_prims<<<LP(), 256, 0, stream>>>(A); });
     if (any_viscous) {
-      L(G_VISC, [&] { k_visc_cell<<<ntiles, TI * TJ, 0, stream>>>(A); });
-      L(G_VISC, [&] { k_visc_face<<<ntiles, TI * TJ, 0, stream>>>(A); });
+      L(G_VISC, [&] { k_visc_cell<<<LT(), TI * TJ, 0, stream>>>(A); });
+      L(G_VISC, [&] { k_visc_face<<<LT(), TI * TJ, 0, stream>>>(A); });
     }
   }
   int scheme_of_arena() const { return desc.empty() ? 0 : desc[0].scheme; }
@@ -794,41 +836,41 @@ struct ArenaHost {
       set_level(0);
     } else if (scheme_of_arena() == SCHEME_IMPLICIT) {
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 2, slot); });
+      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 2, slot); });
       const int s = sub_iters_of_arena();
-      L(G_ASSEMBLE, [&] { k_assemble<<<ntiles, TI * TJ, 0, stream>>>(A); });
-      L(G_ASSEMBLE, [&] { k_line_ends<<<(nil + njl + 127) / 128, 128, 0, stream>>>(A); });
+      L(G_ASSEMBLE, [&] { k_assemble<<<LT(), TI * TJ, 0, stream>>>(A); });
+      L(G_ASSEMBLE, [&] { k_line_ends<<<(LI(1) + LI(0) + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
-        L(G_DEFECT, [&] { k_defect<<<ntiles, TI * TJ, 0, stream>>>(A, p); });
+        L(G_DEFECT, [&] { k_defect<<<LT(), TI * TJ, 0, stream>>>(A, p); });
         L(G_SUBST_I, [&] { launch_subst(1, A.RR, A.X, p); });
         L(G_SUBST_J, [&] { launch_subst(0, A.X, nullptr, p); });
       }
       if (any_sst) {
         // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step
-        L(G_TURB, [&] { k_turb_grad<<<ntiles, TI * TJ, 0, stream>>>(A); });
-        L(G_TURB, [&] { k_turb_blend<<<ntiles, TI * TJ, 0, stream>>>(A); });
-        L(G_TURB, [&] { k_turb_cell<<<ntiles, TI * TJ, 0, stream>>>(A, slot); });
+        L(G_TURB, [&] { k_turb_grad<<<LT(), TI * TJ, 0, stream>>>(A); });
+        L(G_TURB, [&] { k_turb_blend<<<LT(), TI * TJ, 0, stream>>>(A); });
+        L(G_TURB, [&] { k_turb_cell<<<LT(), TI * TJ, 0, stream>>>(A, slot); });
         if (max_line <= 32 * TL_MAXM) {
           L(G_TURB_LINES, [&] { launch_turb_lines(1); });
           L(G_TURB_LINES, [&] { launch_turb_lines(0); });
         } else {
-          L(G_TURB, [&] { k_turb_lines<<<(2 * nil + 127) / 128, 128, 0, stream>>>(A, 1); });
-          L(G_TURB, [&] { k_turb_lines<<<(2 * njl + 127) / 128, 128, 0, stream>>>(A, 0); });
+          L(G_TURB, [&] { k_turb_lines<<<(2 * LI(1) + 127) / 128, 128, 0, stream>>>(A, 1); });
+          L(G_TURB, [&] { k_turb_lines<<<(2 * LI(0) + 127) / 128, 128, 0, stream>>>(A, 0); });
         }
-        L(G_TURB, [&] { k_turb_update<<<ntiles, TI * TJ, 0, stream>>>(A); });
+        L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
       }
     } else {
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot); });
-      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
+      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 1, slot); });
+      L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
-      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
+      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
-      L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1); });
+      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1); });
     }
   }
   // n iterations with CUDA events around every launch (no graph); per-group totals in prof_ms / prof_launches
@@ -930,7 +972,7 @@ struct ArenaHost {
     const int nc = (int)cases.size();
     BK_CUDA(cudaMemsetAsync(A.rsum, 0, nc * sizeof(double), stream));
     launch_mean_flow_prep();
-    k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, dt_kind, 0);
+    k_residual<<<LT(), TI * TJ, 0, stream>>>(A, dt_kind, 0);
     BK_CUDA(cudaGetLastError());
     std::vector<double> h(nc);
     BK_CUDA(cudaMemcpyAsync(h.data(), A.rsum, nc * sizeof(double), cudaMemcpyDeviceToHost, stream));

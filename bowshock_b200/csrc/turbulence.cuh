@@ -55,7 +55,7 @@ __device__ __forceinline__ float2 kw_side(const Arena& A, const CaseDev& c, cons
 }
 
 __global__ void k_turb_grad(Arena A) {  // turbulence.rs:337-372
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;
@@ -91,7 +91,7 @@ __global__ void k_turb_grad(Arena A) {  // turbulence.rs:337-372
 }
 
 __global__ void k_turb_blend(Arena A) {  // turbulence.rs:375-397
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;
@@ -168,7 +168,7 @@ __device__ __forceinline__ float strain2(float4 g, float v, float r) {  // turbu
 //   [3c+2] = (up_j k / d0k, up_j w / d0w, d_j k, d_j w); trhs[c] = V R (the i-line right-hand side).
 __global__ void k_turb_cell(Arena A, int slot) {
   __shared__ double sred[TI * TJ / 32];
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;
@@ -256,9 +256,8 @@ __global__ void k_turb_cell(Arena A, int slot) {
 // in trhs (turbulence.rs:580-581 with the block solver's diagonal blocks, implicit.rs:179-204).
 __global__ void k_turb_lines(Arena A, int dir_i) {
   int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  int nl = dir_i ? A.nilines : A.njlines;
-  if (gt >= 2 * nl) return;
-  int line = gt >> 1, e = gt & 1;
+  int line = line_at(A, dir_i != 0, gt >> 1), e = gt & 1;
+  if (line < 0) return;
   int ci = dir_i ? A.iline_case[line] : A.jline_case[line];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;
@@ -333,9 +332,8 @@ __device__ __forceinline__ float2 shfl_down2(float2 v, int h) {
 template <int W>  // lines (warps) per block, chosen by the arena's autotuner
 __global__ void __launch_bounds__(32 * W) k_turb_lines_w(Arena A, int dir_i) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int line = blockIdx.x * W + warp;
-  const int nl = dir_i ? A.nilines : A.njlines;
-  if (line >= nl) return;  // uniform per warp
+  const int line = line_at(A, dir_i != 0, blockIdx.x * W + warp);
+  if (line < 0) return;  // uniform per warp
   const int ci = dir_i ? A.iline_case[line] : A.jline_case[line];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;
@@ -448,7 +446,7 @@ __global__ void __launch_bounds__(32 * W) k_turb_lines_w(Arena A, int dir_i) {
 }
 
 __global__ void k_turb_update(Arena A) {  // turbulence.rs:584-603
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;

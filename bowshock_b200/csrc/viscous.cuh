@@ -113,7 +113,7 @@ __device__ __forceinline__ V4<float> phi3(const V4<float>& w) { return mk4<float
 
 // Cell pass (viscous.rs:280-316): Sutherland viscosity and Green-Gauss gradient (u_x, u_r, v_x, v_r, T_x, T_r).
 __global__ void k_visc_cell(Arena A) {
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.viscous) return;
@@ -196,7 +196,7 @@ __device__ V4<float> viscous_flux_d(const Arena& A, const SidesD& s, float4 f, f
 
 // Face pass (viscous.rs:347-381): one thread per face of a residual tile's rows / columns.
 __global__ void k_visc_face(Arena A) {
-  int t = blockIdx.x;
+  int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.viscous) return;
