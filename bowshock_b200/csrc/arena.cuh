@@ -72,6 +72,7 @@ struct Arena {
   float2* gradT;   // (T_x, T_r)
   float* mu;
   float* mu_t;
+  float4* rough;   // rough-wall runs: (k_w, omega_w, mu_t,w, 0) of the cells next to a no-slip face (null: no rough case)
   float4* fvi;     // viscous i-face fluxes
   float4* fvj;     // viscous j-face fluxes
   float2* turb;    // (k, omega)
@@ -116,6 +117,19 @@ __device__ __forceinline__ bool noslip_jface(const CaseDev& c, int i, int j) {
 }
 __device__ __forceinline__ bool noslip_iface(const CaseDev& c, int i, int j) {
   return c.viscous && c.has_block && i == c.i_end && j >= c.j_sting && j < c.j_end && !(c.has_nozzle && j < c.nz_j_end);
+}
+// SST with a sand-grain roughness (viscous.rs:52-56)
+__device__ __forceinline__ bool is_rough(const CaseDev& c) { return c.sst && c.roughness > 0.0; }
+// viscous.rs:111-121: the body surface is the rough wall; the base wall and the sting keep the smooth state
+__device__ __forceinline__ bool rough_jface(const CaseDev& c, int i, int j) {
+  if (!is_rough(c)) return false;
+  if (!c.has_block) return j == 0 && c.bc[2] == 2 && i >= c.wall_i_start;
+  return j == c.j_end && i >= c.wall_i_start && i < c.i_end;
+}
+// turbulence.rs:280-290: the roughness is phased in over the first 8 wall cells
+__device__ __forceinline__ double rough_ramp(const CaseDev& c, int i) {
+  int a = i + 1 - c.wall_i_start;
+  return fmin((double)(a > 0 ? a : 0) / 8.0, 1.0);
 }
 __device__ __forceinline__ bool jet_iface(const CaseDev& c, int i, int j) { return c.has_block && i == c.i_end && c.has_nozzle && j < c.nz_j_end; }
 

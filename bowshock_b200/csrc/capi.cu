@@ -247,7 +247,7 @@ int bowshock_solver_set_viscous(bowshock_solver* s, const bowshock_viscous* v) {
   if (!s) return BOWSHOCK_INVALID;
   HostCase& h = s->ar.cases[0];
   if (v) {
-    if (v->roughness != 0.0) return fail(s, BOWSHOCK_UNSUPPORTED, "rough walls are not implemented on this backend");
+    if (!(v->roughness >= 0.0 && std::isfinite(v->roughness))) return fail(s, BOWSHOCK_INVALID, "roughness must be finite and >= 0");
     if (!(v->re_c > 0 && v->sutherland > 0)) return fail(s, BOWSHOCK_INVALID, "re_c and sutherland must be positive");
     if (v->turbulence == BOWSHOCK_TURB_SST && h.scheme != BOWSHOCK_SCHEME_IMPLICIT)
       return fail(s, BOWSHOCK_UNSUPPORTED, "the SST model runs with the implicit scheme on this backend");
@@ -256,7 +256,7 @@ int bowshock_solver_set_viscous(bowshock_solver* s, const bowshock_viscous* v) {
     h.wall_i_start = (long long)v->wall_i_start;
     h.re_c = v->re_c;
     h.sutherland = v->sutherland;
-    h.roughness = 0;
+    h.roughness = v->roughness;
   } else {
     h.viscous = false;
     h.turbulence = 0;
@@ -602,7 +602,7 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
     const bowshock_case_desc& d = cases[k];
     if (d.ni < 4 || d.nj < 2 || !d.x || !d.r || !valid_config(&d.cfg, m) || !valid_body(&d.body, m) ||
         d.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT || d.scheme.sub_iters < 1 || d.scheme.sub_iters > 16 ||
-        (d.has_viscous && d.viscous.roughness != 0.0)) {
+        (d.has_viscous && !(d.viscous.roughness >= 0.0 && std::isfinite(d.viscous.roughness)))) {
       delete a;
       return BOWSHOCK_INVALID;
     }
@@ -640,6 +640,7 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
       h.wall_i_start = (long long)d.viscous.wall_i_start;
       h.re_c = d.viscous.re_c;
       h.sutherland = d.viscous.sutherland;
+      h.roughness = d.viscous.roughness;
     }
     if (!compute_metrics(h, m)) {
       delete a;

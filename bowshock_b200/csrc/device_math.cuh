@@ -532,4 +532,27 @@ BK_HD void cell_blocks(const V4<T>& wk, const V4<T>& wm, const V4<T>& wp, T fl_n
   for (int k = 0; k < 16; ++k) up[k] *= sr_;
 }
 
+// Aupoix (2015) "Colebrook" rough-wall state of a no-slip wall cell (turbulence.rs:292-320): kinematic viscosity nu, speed
+// |u|, wall distance d, equivalent sand-grain roughness ks > 0 -> (k_w, omega_w, nu_t,w), omega_w bounded by the smooth
+// wall value 60 nu / (beta_1 d^2) and nu_t,w by 1e5 nu; u_tau^2 = (nu + nu_t,w) |u| / d by 16 fixed-point steps from
+// the laminar u_tau^2 = nu |u| / d. FP64: it runs once per wall cell and iteration.
+__device__ inline void aupoix_state(double nu, double speed, double d, double ks, double u2, double out[3]) {
+  const double u_tau = sqrt(u2);
+  const double ks_plus = fmax(u_tau * ks / nu, 1e-30);
+  const double t = tanh(ks_plus / 125.0);
+  const double k_plus = fmax(tanh((log10(ks_plus / 30.0) + 1.0 - t) * t), 0.0) / sqrt(0.09);
+  const double om_rough = 300.0 * nu / (ks * ks) / tanh(15.0 / (4.0 * ks_plus)) + 191.0 * u_tau / ks * (1.0 - exp(-ks_plus / 250.0));
+  out[0] = k_plus * u2;
+  out[1] = fmin(om_rough, 60.0 * nu / (0.075 * d * d));
+  out[2] = fmin(out[0] / out[1], 1e5 * nu);
+}
+__device__ inline void aupoix_wall(double nu, double speed, double d, double ks, double out[3]) {
+  double u2 = nu * speed / d;
+  for (int k = 0; k < 16; ++k) {
+    aupoix_state(nu, speed, d, ks, u2, out);
+    u2 = (nu + out[2]) * speed / d;
+  }
+  aupoix_state(nu, speed, d, ks, u2, out);
+}
+
 }  // namespace bk

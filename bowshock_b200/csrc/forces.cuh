@@ -92,7 +92,7 @@ __global__ void k_forces(Arena A, const BodyDev* bodies, const double* nx, const
       atomicAdd(&acc[F_NF], ds);
     }
   }
-  // skin friction and y+ (run.rs:207-248), smooth walls
+  // skin friction and y+ (run.rs:207-248); a rough wall adds its mu_t,w (Aupoix state at the full roughness)
   if (c.viscous) {
     int rows[2] = {c.has_block ? c.j_end : 0, c.has_block ? c.j_sting : -1};
     for (int rr = 0; rr < 2; ++rr) {
@@ -114,7 +114,13 @@ __global__ void k_forces(Arena A, const BodyDev* bodies, const double* nx, const
         double d_n = fabs((dxc[cc] - xm) * fnx + (drc[cc] - frm) * fnr);
         double T = 1.4 * p / rho;
         double mu = pow(T, 1.5) * (1.0 + c.sutherland) / (T + c.sutherland) / c.re_c;
-        double tau = mu * u_t / d_n;
+        double mu_tw = 0.0;
+        if (is_rough(c)) {
+          double a[3];
+          aupoix_wall(mu / rho, hypot(u, v), d_n, c.roughness, a);
+          mu_tw = rho * a[2];
+        }
+        double tau = (mu + mu_tw) * u_t / d_n;
         atomicAdd(&acc[F_CD_FRICTION], 2.0 * tau * tx * frm * len / (q_inf * rb2));
         double yp = d_n * sqrt(rho * fabs(tau)) / mu;
         atomicMax(&yplus_bits, (unsigned long long)__double_as_longlong(yp));  // yp >= 0: the bit patterns order like the values

@@ -251,7 +251,7 @@ struct ArenaHost {
   int LI(int dir_i) const { return dir_i ? (A.iline_list ? A.n_il : nil) : (A.jline_list ? A.n_jl : njl); }
   // floats of the line-solve records: 25 float4 per cell and direction, 44 float4 per lane of every line
   size_t scratch_floats() const { return 4 * ((size_t)2 * ncell * 25 + (size_t)(nil + njl) * 32 * 44); }
-  bool any_viscous = false, any_sst = false;
+  bool any_viscous = false, any_sst = false, any_rough = false;
   // device buffers
   Arena A{};
   CaseDev* d_cases = nullptr;
@@ -272,7 +272,7 @@ struct ArenaHost {
     if (pe1) cudaEventDestroy(pe1), pe1 = nullptr;
     void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0, A.Ulo, A.Wlo, A.U0lo, A.MG0lo,
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
-                    A.grad4, A.gradT, A.mu, A.mu_t, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
+                    A.grad4, A.gradT, A.mu, A.mu_t, A.rough, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
                     A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled, d_tlist, d_pblist, d_illist, d_jllist};
     d_enabled = nullptr;
     d_tlist = d_pblist = d_illist = d_jllist = nullptr;
@@ -488,7 +488,7 @@ struct ArenaHost {
 
   // Re-derive the descriptors from the host configuration (config, scheme, block, viscous changes).
   int upload_desc() {
-    any_viscous = any_sst = false;
+    any_viscous = any_sst = any_rough = false;
     for (size_t k = 0; k < cases.size(); ++k) {
       CaseDev c = make_desc(cases[k]);
       CaseDev& d = desc[k];
@@ -505,6 +505,7 @@ struct ArenaHost {
       d = c;
       any_viscous |= c.viscous != 0;
       any_sst |= c.sst != 0;
+      any_rough |= c.sst != 0 && c.roughness > 0.0;
     }
     int rc = 0;
     if (any_viscous && !A.mu) {
@@ -517,6 +518,10 @@ struct ArenaHost {
       BK_CUDA(cudaMemset(A.mu_t, 0, ncell * sizeof(float)));
       BK_CUDA(cudaMemset(A.fvi, 0, nif * sizeof(float4)));
       BK_CUDA(cudaMemset(A.fvj, 0, njf * sizeof(float4)));
+    }
+    if (any_rough && !A.rough) {
+      ALLOC(A.rough, ncell);
+      BK_CUDA(cudaMemset(A.rough, 0, ncell * sizeof(float4)));
     }
     if (any_sst && !A.turb) {
       ALLOC(A.turb, ncell);

@@ -40,13 +40,18 @@ __device__ __forceinline__ int jkind(const CaseDev& c, int j, const SidesD& s) {
   if (s.r.ghost) return bc_kind(c.bc[3]);
   return KIND_CELL;
 }
-// Ctx::kw (turbulence.rs:224-245), smooth walls
+// Ctx::kw (turbulence.rs:224-245): a wall ghost mirrors (0, omega_w) of a smooth wall, or the rough-wall state of the
+// wall cell stored by the last viscous pass
 __device__ __forceinline__ float2 kw_side(const Arena& A, const CaseDev& c, const SideD& s, int kind) {
   float2 t = A.turb[s.cell];
   if (!s.ghost || kind == KIND_CELL) return t;
   if (kind == KIND_INF) return make_float2(K_INF, omega_inf(c));
   if (kind == KIND_FIXED) return make_float2(c.nz_turb[0], c.nz_turb[1]);
   long long cc = s.cell;
+  if (is_rough(c)) {
+    float4 r = A.rough[cc];
+    return make_float2(2.f * r.x - t.x, 2.f * r.y - t.y);
+  }
   int i = (int)((cc - c.cell_off) % c.ni), j = (int)((cc - c.cell_off) / c.ni);
   float rho = A.W[pidx(c, i, j)].x;
   float nu = A.mu[cc] / rho;
@@ -133,7 +138,7 @@ __device__ TFaceD tface_d(const Arena& A, const CaseDev& c, const SidesD& s, int
   float dd = st.x, ex = st.y, er = st.z;
   float4 gl = A.grad_kw[s.l.cell], gr = A.grad_kw[s.r.cell];
   float mu_f, mut_f;
-  face_mu_d(A, s, mu_f, mut_f);
+  face_mu_d(A, c, s, mu_f, mut_f);
   float f1l = A.blend[s.l.cell].x, f1r = A.blend[s.r.cell].x;
   {
     float sigma = 0.5f * (f1l * SIGMA_K1 + (1.f - f1l) * SIGMA_K2 + f1r * SIGMA_K1 + (1.f - f1r) * SIGMA_K2);

@@ -97,12 +97,13 @@ __device__ bool jface_sides_d(const Arena& A, const CaseDev& c, int i, int j, Si
   return true;
 }
 
-// viscous.rs:256-270 (smooth walls: the ghost across a no-slip face carries -mu_t, so the face value is 0)
-__device__ __forceinline__ void face_mu_d(const Arena& A, const SidesD& s, float& mu_f, float& mut_f) {
+// viscous.rs:256-270: the ghost across a no-slip face carries -mu_t (smooth walls: the face value is 0), or
+// 2 mu_t,w - mu_t with the rough-wall state of the wall cell (the face value is the wall's mu_t,w)
+__device__ __forceinline__ void face_mu_d(const Arena& A, const CaseDev& c, const SidesD& s, float& mu_f, float& mut_f) {
   auto mus = [&](const SideD& d) { return d.fixed ? d.fmu : A.mu[d.cell]; };
   auto muts = [&](const SideD& d) {
     if (d.fixed) return d.fmut;
-    if (d.ghost && s.noslip) return -A.mu_t[d.cell];
+    if (d.ghost && s.noslip) return is_rough(c) ? 2.f * A.rough[d.cell].z - A.mu_t[d.cell] : -A.mu_t[d.cell];
     return A.mu_t[d.cell];
   };
   mu_f = 0.5f * (mus(s.l) + mus(s.r));
@@ -128,7 +129,23 @@ __global__ void k_visc_cell(Arena A) {
     return;
   }
   V4<float> wc = from_f4(A.W[pidx(c, i, j)]);
-  A.mu[cc] = mu_of(c, temperature(wc));
+  const float mu_c = mu_of(c, temperature(wc));
+  A.mu[cc] = mu_c;
+  if (is_rough(c)) {  // viscous.rs:387-409: the wall state of the cells next to a no-slip face, from this pass's mu
+    float4 rw = make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool rough = rough_jface(c, i, j);
+    if (rough || noslip_jface(c, i, j) || noslip_iface(c, i, j)) {
+      const double rho = wc[0], nu = (double)mu_c / rho, d = A.dwall[cc];
+      if (rough) {
+        double a[3];
+        aupoix_wall(nu, hypot((double)wc[1], (double)wc[2]), d, c.roughness * rough_ramp(c, i), a);
+        rw = make_float4((float)a[0], (float)a[1], (float)(rho * a[2]), 0.f);
+      } else {
+        rw = make_float4(0.f, (float)(60.0 * nu / (0.075 * d * d)), 0.f, 0.f);
+      }
+    }
+    A.rough[cc] = rw;
+  }
   V4<float> pc = phi3(wc);
   SidesD s;
   iface_sides_d(A, c, i, j, s);
@@ -165,7 +182,7 @@ __device__ __forceinline__ void grad6(const Arena& A, long long cc, float* g) {
 }
 
 // Viscous flux of one face (viscous.rs:319-343).
-__device__ V4<float> viscous_flux_d(const Arena& A, const SidesD& s, float4 f, float4 st) {
+__device__ V4<float> viscous_flux_d(const Arena& A, const CaseDev& c, const SidesD& s, float4 f, float4 st) {
   if (f.w == 0.f) return mk4<float>(0, 0, 0, 0);  // r_mid = 0 (axis): weight len * r_mid is 0 exactly
   float dd = st.x, ex = st.y, er = st.z;
   float gl[6], gr[6];
@@ -181,7 +198,7 @@ __device__ V4<float> viscous_flux_d(const Arena& A, const SidesD& s, float4 f, f
     gf[2 * m + 1] = gbr + corr * er;
   }
   float mu_f, mut_f;
-  face_mu_d(A, s, mu_f, mut_f);
+  face_mu_d(A, c, s, mu_f, mut_f);
   float uf = 0.5f * (s.l.w[1] + s.r.w[1]), vf = 0.5f * (s.l.w[2] + s.r.w[2]);
   float rm = f.w / f.z;
   float div = gf[0] + gf[3] + vf / rm;
@@ -210,7 +227,7 @@ __global__ void k_visc_face(Arena A) {
       if (q == TI && i != c.ni) continue;  // owned by the next tile
       SidesD s;
       V4<float> fv = mk4<float>(0, 0, 0, 0);
-      if (iface_sides_d(A, c, i, j, s)) fv = viscous_flux_d(A, s, A.iface[ifidx(c, i, j)], A.ifs[ifidx(c, i, j)]);
+      if (iface_sides_d(A, c, i, j, s)) fv = viscous_flux_d(A, c, s, A.iface[ifidx(c, i, j)], A.ifs[ifidx(c, i, j)]);
       A.fvi[ifidx(c, i, j)] = to_f4(fv);
     } else {
       int k = idx - TJ * (TI + 1);
@@ -220,7 +237,7 @@ __global__ void k_visc_face(Arena A) {
       if (r == TJ && j != c.nj) continue;
       SidesD s;
       V4<float> fv = mk4<float>(0, 0, 0, 0);
-      if (jface_sides_d(A, c, i, j, s)) fv = viscous_flux_d(A, s, A.jface[jfidx(c, i, j)], A.jfs[jfidx(c, i, j)]);
+      if (jface_sides_d(A, c, i, j, s)) fv = viscous_flux_d(A, c, s, A.jface[jfidx(c, i, j)], A.jfs[jfidx(c, i, j)]);
       A.fvj[jfidx(c, i, j)] = to_f4(fv);
     }
   }
@@ -238,7 +255,7 @@ __device__ float face_lambda_dev(const Arena& A, const CaseDev& c, bool dir_i, i
     dd = A.jfs[jfidx(c, fi, fj)].x;
   }
   float mu_f, mut_f;
-  face_mu_d(A, s, mu_f, mut_f);
+  face_mu_d(A, c, s, mu_f, mut_f);
   float rho_f = 0.5f * (s.l.w[0] + s.r.w[0]);
   return 1.4f * (mu_f / PR + mut_f / PR_T) / (rho_f * dd);
 }

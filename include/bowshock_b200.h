@@ -81,7 +81,8 @@ typedef struct {
   uint64_t i_end, j_end, j_sting;
 } bowshock_block;
 
-/* solver.rs:164-176 `Viscous` (smooth walls: roughness must be 0 on this backend) */
+/* solver.rs:164-176 `Viscous`: roughness = equivalent sand grain of the body surface in nose diameters (0: smooth walls;
+ * > 0 with SST: the Aupoix rough-wall state, turbulence.rs:292-320) */
 typedef struct {
   double re_c, sutherland;
   int32_t turbulence;
@@ -119,7 +120,7 @@ int bowshock_solver_set_nozzle(bowshock_solver* s, const bowshock_nozzle* nozzle
 /* GpuSolver::set_scheme (gpu/mod.rs:331-337): explicit or implicit; the CFL ramp restarts */
 int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* scheme);
 /* GpuSolver::set_viscous (gpu/mod.rs:351-357): NULL = Euler; the turbulence state restarts at the free stream, the wall
- * distance is computed on the device; roughness > 0 is UNSUPPORTED */
+ * distance is computed on the device; roughness must be finite and >= 0 (INVALID otherwise) */
 int bowshock_solver_set_viscous(bowshock_solver* s, const bowshock_viscous* v);
 /* GpuSolver::set_state (gpu/mod.rs:378-381): overwrite the conserved state, restart the iteration counter and the ramp */
 int bowshock_solver_set_state(bowshock_solver* s, const double* u);

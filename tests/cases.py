@@ -28,6 +28,7 @@ class Spec:
     scheme: dict | None = None  # None = explicit; else implicit params
     viscous: dict | None = None
     u0: np.ndarray | None = None
+    nozzle: tuple | None = None  # (j_end, state[4], turb[2]) of the base-face jet
     label: str = ""
 
 
@@ -95,6 +96,8 @@ def oracle_solver(spec: Spec) -> o.Solver:
         s.set_block(spec.block)
     if spec.scheme is not None:
         s.set_scheme(o.implicit_params(**spec.scheme))
+    if spec.nozzle is not None:  # the jet rows before the viscous walls (solver.rs:333-347)
+        s.set_nozzle(*spec.nozzle)
     if spec.viscous is not None:
         s.set_viscous(spec.viscous)
     if spec.u0 is not None:
@@ -113,6 +116,8 @@ def gpu_solver(spec: Spec):
         s.set_scheme(bk.ImplicitParams(**spec.scheme))
     else:
         s.set_scheme(bk.EXPLICIT)
+    if spec.nozzle is not None:
+        s.set_nozzle(spec.nozzle)
     if spec.viscous is not None:
         s.set_viscous(bk.Viscous(**spec.viscous))
     if spec.u0 is not None:

@@ -21,8 +21,11 @@ def g3_cases():
     return pc, g3_case()
 
 
-def test_device_forces_match_the_oracle_post_processing():  # engine/run.rs:188-313 on the same state
+@pytest.mark.parametrize("roughness", [0.0, 2e-5])
+def test_device_forces_match_the_oracle_post_processing(roughness):  # engine/run.rs:188-313 on the same state
     pc, oc = g3_cases()
+    pc.viscous.roughness = roughness  # rough: the friction adds the Aupoix mu_t,w (run.rs:241)
+    oc.roughness = roughness
     s = pc.build_solver()
     s.run(300)
     f = s.forces(pc.body)
