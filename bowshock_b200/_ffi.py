@@ -80,6 +80,10 @@ class StingGridC(C.Structure):  # bowshock_sting_grid
                 ("n_seg", C.c_uint64 * 8), ("n_ext", C.c_uint64), ("nj", C.c_uint64), ("dx_tip", C.c_double), ("dr_wall", C.c_double)]
 
 
+class LineTuning(C.Structure):  # bowshock_line_tuning
+    _fields_ = [(n, C.c_int32) for n in ("lines_i", "lines_j", "prefetch_i", "prefetch_j", "subst_i", "subst_j", "turb_lines")]
+
+
 class CaseDesc(C.Structure):  # bowshock_case_desc
     _fields_ = [("ni", C.c_uint64), ("nj", C.c_uint64), ("x", C.POINTER(C.c_double)), ("r", C.POINTER(C.c_double)), ("cfg", Config),
                 ("low_mach", C.c_int32), ("has_block", C.c_int32), ("block", Block), ("scheme", Scheme), ("has_viscous", C.c_int32),
@@ -140,7 +144,7 @@ SIGNATURES = {
     "bowshock_arena_last_ms_per_iter": (_I, [_P, _dp]),
     "bowshock_arena_last_solve_ms": (_I, [_P, _dp]),
     "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
-    "bowshock_arena_tuning": (_I, [_P, C.POINTER(C.c_int32)]),
+    "bowshock_arena_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_solver_run_noalloc": (_I, [_P, _U, _dp]),
 }
 

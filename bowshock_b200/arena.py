@@ -74,10 +74,11 @@ class Arena:
         return {g: (float(ms[k]), int(cnt[k])) for k, g in enumerate(self.PROFILE_GROUPS)}
 
     def tuning(self):
-        """Lines per block the autotuner picked: {"lines": .., "subst": .., "turb_lines": ..}."""
-        out = (C.c_int32 * 3)()
-        self._check(_ffi.load().bowshock_arena_tuning(self._h, out))
-        return dict(lines=out[0], subst=out[1], turb_lines=out[2])
+        """Launch shapes of the line kernels the autotuner picked: lines per block and prefetching of the first pass per
+        direction, lines per block of the substitution passes per direction and of the SST line kernel."""
+        t = _ffi.LineTuning()
+        self._check(_ffi.load().bowshock_arena_tuning(self._h, C.byref(t)))
+        return {n: int(getattr(t, n)) for n, _ in _ffi.LineTuning._fields_}
 
     def solve(self, progress=None):
         """Cold-start every case and iterate each to its stop rule (converged cases are masked out)."""

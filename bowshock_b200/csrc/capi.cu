@@ -666,9 +666,12 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
   return BOWSHOCK_OK;
 }
 
-int bowshock_arena_tuning(const bowshock_arena* a, int32_t* lines_per_block) {
-  if (!a || !lines_per_block) return BOWSHOCK_INVALID;
-  lines_per_block[0] = a->ar.lw_lines, lines_per_block[1] = a->ar.lw_subst, lines_per_block[2] = a->ar.lw_turb;
+int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out) {
+  if (!a || !out) return BOWSHOCK_INVALID;
+  const auto& r = a->ar;
+  out->lines_i = r.lw_lines[1] > 4 ? 4 : r.lw_lines[1], out->lines_j = r.lw_lines[0] > 4 ? 4 : r.lw_lines[0];
+  out->prefetch_i = r.pf_lines[1], out->prefetch_j = r.pf_lines[0];
+  out->subst_i = r.lw_subst[1], out->subst_j = r.lw_subst[0], out->turb_lines = r.lw_turb;
   return BOWSHOCK_OK;
 }
 

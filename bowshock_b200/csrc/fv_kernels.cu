@@ -4,13 +4,14 @@
 //               HLLC blended to Rusanov, low-Mach correction), the cell residual with the axisymmetric source, the local
 //               time step, and the FP64 density-residual norm (block reduce + one atomic per block)   (solver.rs:474-654)
 //   k_stage     SSP-RK3 stage update                                                   (solver.rs:694-720)
+//   k_assemble  blocks (lo, d, up) of I - dt J_i and I - dt J_j of every cell into its two line records
+//               (implicit.rs:284-438); k_line_ends folds the line-end ghost Jacobians in (implicit.rs:440-467)
 //   k_lines     line-implicit solve of (I - dt J_dir) x = b along every i or j line: one warp per line, a partitioned
-//               block-tridiagonal (4x4) solver — each lane eliminates its own segment in registers, the separator
-//               unknowns form a reduced block-tridiagonal system solved by parallel cyclic reduction across the warp
-//               through shared memory, then each lane back-substitutes its segment       (implicit.rs:528-563)
-//   k_defect    defect r = dt R - (A_i du + A_j du - du) of the unfactored operator     (implicit.rs:622-630)
-// The Jacobian blocks are assembled in registers from W, the face metrics and dt wherever they are needed
-// (implicit.rs:284-467); they are never stored.
+//               block-tridiagonal (4x4) solver — each lane eliminates its own segment, the separator unknowns form a
+//               reduced block-tridiagonal system solved by parallel cyclic reduction across the warp through shared
+//               memory, then each lane back-substitutes its segment; factors kept in the records (implicit.rs:528-563)
+//   k_lines_subst  the defect-correction passes with the kept factors                  (implicit.rs:622-639)
+//   k_defect    defect r = dt R - (A_i du + A_j du - du) with the kept blocks           (implicit.rs:622-630)
 #include "arena.cuh"
 #include "device_math.cuh"
 #include "viscous.cuh"
@@ -333,18 +334,31 @@ __device__ __forceinline__ V4<float> rhs_of(const Arena& A, const float4* in, bo
   return r;
 }
 
-// Line-solve records in A.scratch (float4 units): for every cell and direction (i first, then j) 25 float4 =
-//   [0..3] lo, [4..7] d, [8..11] up  (the assembled blocks of I - dt J_dir, line ends folded in)
-//   [12..15] M^-1, [16..19] Y = M^-1 up, [20..23] GE (the left spike), [24] g (the right-hand side's forward sweep);
+// Line-solve records in A.scratch: per direction (i lines first, then j lines) a plane per field over the arena's cells,
+//   F_LO, F_D, F_UP  the assembled blocks lo, d, up of I - dt J_dir (line ends folded in),
+//   F_MINV, F_Y, F_GE, F_T  the factors M^-1, Y = M^-1 up, the left spike GE and the weight T of the cell's forward value
+//                    in its segment's first interior cell   (a 4x4 block = 4 float4 per cell each),
+//   F_G              g, the right-hand side's forward sweep (1 float4 per cell);
 // then for every line and lane of the reduced separator system 44 float4 = 5 PCR levels x (alpha, gamma) + b^-1.
-// The first pass of an iteration assembles and factorises (k_lines); later passes (k_lines_subst) and the defect (k_defect)
-// only read them.
-constexpr int REC = 25, PREC = 44, PCR_LEVELS = 5;
-__device__ __forceinline__ float4* line_rec(const Arena& A, bool dir_i, long long cc) {
-  return reinterpret_cast<float4*>(A.scratch) + ((dir_i ? 0 : A.ncell) + cc) * REC;
+// A plane keeps one field of consecutive cells contiguous: the per-cell kernels (assembly, defect) store and load whole
+// sectors across a warp, and a lane walking its segment of an i line reads consecutive 64-byte blocks.
+// The first pass of an iteration assembles and factorises (k_assemble, k_line_ends, k_lines); later passes
+// (k_lines_subst) and the defect (k_defect) only read them.
+enum { F_LO = 0, F_D, F_UP, F_MINV, F_Y, F_GE, F_T, F_G };
+constexpr int REC = 29, PREC = 44, PCR_LEVELS = 5;  // REC: float4 per cell and direction
+// float4 per direction, rounded up to whole 64-byte blocks so that the j planes start on sector boundaries
+__host__ __device__ __forceinline__ long long rec_dir_stride(long long ncell) { return (ncell * REC + 3) & ~3LL; }
+struct Rec {  // the record of one cell in one direction
+  float4* base;
+  long long n, cc;
+  __device__ __forceinline__ float4* blk(int f) const { return base + (n * f + cc) * 4; }
+  __device__ __forceinline__ float4* g() const { return base + n * 28 + cc; }
+};
+__device__ __forceinline__ Rec line_rec(const Arena& A, bool dir_i, long long cc) {
+  return Rec{reinterpret_cast<float4*>(A.scratch) + (dir_i ? 0 : rec_dir_stride(A.ncell)), A.ncell, cc};
 }
 __device__ __forceinline__ float4* pcr_rec(const Arena& A, bool dir_i, int gw, int lane) {
-  float4* base = reinterpret_cast<float4*>(A.scratch) + 2 * A.ncell * REC;
+  float4* base = reinterpret_cast<float4*>(A.scratch) + 2 * rec_dir_stride(A.ncell);
   if (!dir_i) base += (long long)A.nilines * 32 * PREC;
   return base + ((long long)gw * 32 + lane) * PREC;
 }
@@ -444,10 +458,10 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
   for (int dir = 0; dir < 2; ++dir) {
     M4<float> lo, d, up;
     assemble(A, c, dir == 0, i, j, lo, d, up);
-    float4* rec = line_rec(A, dir == 0, cc);
-    st_m4(rec, lo);
-    st_m4(rec + 4, d);
-    st_m4(rec + 8, up);
+    Rec rec = line_rec(A, dir == 0, cc);
+    st_m4(rec.blk(F_LO), lo);
+    st_m4(rec.blk(F_D), d);
+    st_m4(rec.blk(F_UP), up);
   }
 }
 
@@ -482,11 +496,11 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
         for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
       }
     }
-    float4* rec = line_rec(A, dir_i, cc);
-    M4<float> d = ld_m4(rec + 4);
-    axpy(d, 1.f, mm(ld_m4(rec), T));
-    st_m4(rec, zero4<float>());
-    st_m4(rec + 4, d);
+    Rec rec = line_rec(A, dir_i, cc);
+    M4<float> d = ld_m4(rec.blk(F_D));
+    axpy(d, 1.f, mm(ld_m4(rec.blk(F_LO)), T));
+    st_m4(rec.blk(F_LO), zero4<float>());
+    st_m4(rec.blk(F_D), d);
   }
   {
     const int i = dir_i ? n - 1 : L, j = dir_i ? L : n - 1;
@@ -500,11 +514,11 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
 #pragma unroll
       for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
     }
-    float4* rec = line_rec(A, dir_i, cc);
-    M4<float> d = ld_m4(rec + 4);
-    axpy(d, 1.f, mm(ld_m4(rec + 8), T));
-    st_m4(rec + 8, zero4<float>());
-    st_m4(rec + 4, d);
+    Rec rec = line_rec(A, dir_i, cc);
+    M4<float> d = ld_m4(rec.blk(F_D));
+    axpy(d, 1.f, mm(ld_m4(rec.blk(F_UP)), T));
+    st_m4(rec.blk(F_UP), zero4<float>());
+    st_m4(rec.blk(F_D), d);
   }
 }
 
@@ -526,7 +540,10 @@ __global__ void k_line_ends(Arena A) {
 // reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
 // back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line
 // records for the later passes and the defect.
-template <int W>  // lines (warps) per block, chosen by the arena's autotuner
+// W: lines (warps) per block; PF: the walks load the next cell's record before the arithmetic of the current one
+// (software pipelining: more memory parallelism per lane, ~80 more registers, so fewer warps per SM). The arena's
+// autotuner picks both per direction; the results do not depend on them.
+template <int W, bool PF>
 __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out) {
   __shared__ PcrSlot sp[W][32];
   __shared__ float4 sl[W][32];
@@ -545,15 +562,35 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
   (void)n;
   (void)P;
-  // ---- forward elimination of the segment interior
-  M4<float> Y = zero4<float>(), GE = zero4<float>();
-  V4<float> g = mk4<float>(0, 0, 0, 0);
+  // ---- forward elimination of the segment interior. The segment's first interior cell in terms of the separators,
+  // x_a = v_f + E_f l_left + F_f l_right, follows from the back substitution x_k = g_k + GE_k l_left - Y_k x_k+1 unrolled:
+  // v_f = sum_k T_k g_k, E_f = sum_k T_k GE_k, F_f = T_ke+1 with T_a = I, T_k+1 = -T_k Y_k; the sums are accumulated
+  // on the way down (no backward walk), and T_k is kept for the substitution passes' v_f.
+  M4<float> Y = zero4<float>(), GE = zero4<float>(), T = eye4<float>(), E_f = zero4<float>();
+  V4<float> g = mk4<float>(0, 0, 0, 0), v_f = mk4<float>(0, 0, 0, 0);
   if (act) {
+    Rec rec = line_rec(A, dir_i != 0, cell(a));
+    M4<float> An, Bn, Cn;
+    V4<float> rn;
+    if (PF) {
+      An = ld_m4(rec.blk(F_LO)), Bn = ld_m4(rec.blk(F_D)), Cn = ld_m4(rec.blk(F_UP));
+      rn = rhs_of(A, in, from_res != 0, cell(a));
+    }
     for (int k = a; k <= ke; ++k) {
-      long long cc = cell(k);
-      float4* rec = line_rec(A, dir_i != 0, cc);
-      M4<float> Ak = ld_m4(rec), Bk = ld_m4(rec + 4), Ck = ld_m4(rec + 8);
-      V4<float> r = rhs_of(A, in, from_res != 0, cc);
+      if (!PF) {
+        rec = line_rec(A, dir_i != 0, cell(k));
+        An = ld_m4(rec.blk(F_LO)), Bn = ld_m4(rec.blk(F_D)), Cn = ld_m4(rec.blk(F_UP));
+        rn = rhs_of(A, in, from_res != 0, cell(k));
+      }
+      const M4<float> Ak = An, Bk = Bn, Ck = Cn;
+      V4<float> r = rn;
+      const Rec rec_k = rec;
+      if (PF && k < ke) {
+        const long long cn = cell(k + 1);
+        rec = line_rec(A, dir_i != 0, cn);
+        An = ld_m4(rec.blk(F_LO)), Bn = ld_m4(rec.blk(F_D)), Cn = ld_m4(rec.blk(F_UP));
+        rn = rhs_of(A, in, from_res != 0, cn);
+      }
       M4<float> M = Bk;
       M4<float> GEr;
       if (k > a) {
@@ -571,35 +608,27 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
       g = mv(Minv, r);
       GE = mm(Minv, GEr);
       Y = mm(Minv, Ck);
-      st_m4(rec + 12, Minv);
-      st_m4(rec + 16, Y);
-      st_m4(rec + 20, GE);
-      rec[24] = to_f4(g);
+      st_m4(rec_k.blk(F_MINV), Minv);
+      st_m4(rec_k.blk(F_Y), Y);
+      st_m4(rec_k.blk(F_GE), GE);
+      st_m4(rec_k.blk(F_T), T);
+      *rec_k.g() = to_f4(g);
+      const V4<float> tg = mv(T, g);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v_f[q] += tg[q];
+      axpy(E_f, 1.f, mm(T, GE));
+      T = mm(T, Y);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) T[q] = -T[q];
     }
   }
-  // ---- (v, E, F) at the last interior cell and, by a backward pass, at the first
-  V4<float> v_l = g;
-  M4<float> E_l = GE, F_l;
+  // ---- (v, E, F) at the last interior cell (the forward sweep's last values) and at the first (the sums)
+  const V4<float> v_l = g;
+  const M4<float> E_l = GE;
+  M4<float> F_l;
 #pragma unroll
   for (int q = 0; q < 16; ++q) F_l[q] = -Y[q];
-  V4<float> v_f = v_l;
-  M4<float> E_f = E_l, F_f = F_l;
-  if (act) {
-    for (int k = ke - 1; k >= a; --k) {
-      const float4* rec = line_rec(A, dir_i != 0, cell(k));
-      M4<float> Yk = ld_m4(rec + 16), GEk = ld_m4(rec + 20);
-      V4<float> gk = from_f4(rec[24]);
-      V4<float> t = mv(Yk, v_f);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) v_f[q] = gk[q] - t[q];
-      M4<float> tE = mm(Yk, E_f), tF = mm(Yk, F_f);
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        E_f[q] = GEk[q] - tE[q];
-        F_f[q] = -tF[q];
-      }
-    }
-  }
+  const M4<float> F_f = T;
   // publish (v, E, F) of the first interior cell for the lane on the left
   PcrSlot* my = &sp[warp][s];
 #pragma unroll
@@ -614,8 +643,8 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   M4<float> ra = zero4<float>(), rb = eye4<float>(), rc = zero4<float>();
   V4<float> rd = mk4<float>(0, 0, 0, 0);
   if (has_sep) {
-    const float4* rec = line_rec(A, dir_i != 0, cell(e - 1));
-    M4<float> As = ld_m4(rec), Bs = ld_m4(rec + 4), Cs = ld_m4(rec + 8);
+    Rec rec = line_rec(A, dir_i != 0, cell(e - 1));
+    M4<float> As = ld_m4(rec.blk(F_LO)), Bs = ld_m4(rec.blk(F_D)), Cs = ld_m4(rec.blk(F_UP));
     V4<float> r = rhs_of(A, in, from_res != 0, cell(e - 1));
     const PcrSlot* nx = &sp[warp][s + 1];
     M4<float> En, Fn;
@@ -715,11 +744,26 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   V4<float> lprev = s > 0 ? from_f4(sl[warp][s - 1]) : mk4<float>(0, 0, 0, 0);
   V4<float> xn = has_sep ? lsep : mk4<float>(0, 0, 0, 0);
   if (has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
+  long long cn = cell(ke);
+  Rec recb = line_rec(A, dir_i != 0, cn);
+  M4<float> Yn, GEn;
+  float4 gn;
+  if (PF) Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE)), gn = *recb.g();
   for (int k = ke; k >= a; --k) {
-    long long cc = cell(k);
-    const float4* rec = line_rec(A, dir_i != 0, cc);
-    M4<float> Yk = ld_m4(rec + 16), GEk = ld_m4(rec + 20);
-    V4<float> gk = from_f4(rec[24]);
+    if (!PF) {
+      cn = cell(k);
+      recb = line_rec(A, dir_i != 0, cn);
+      Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE)), gn = *recb.g();
+    }
+    const long long cc = cn;
+    const M4<float> Yk = Yn, GEk = GEn;
+    const V4<float> gk = from_f4(gn);
+    if (PF && k > a) {
+      cn = cell(k - 1);
+      recb = line_rec(A, dir_i != 0, cn);
+      Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE));
+      gn = *recb.g();
+    }
     V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
     V4<float> x;
 #pragma unroll
@@ -764,21 +808,22 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
   const int L = G.L, N = G.N, a = G.a, e = G.e, ke = G.ke;
   const int s = lane;
   auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
-  // the loops load the next cell's record before the dependent arithmetic of the current one (software pipelining)
-  V4<float> g = mk4<float>(0, 0, 0, 0);
+  // the loops load the next cell's record before the dependent arithmetic of the current one (software pipelining);
+  // the forward sweep also sums the first interior cell's value v_f = sum_k T_k g_k with the kept weights
+  V4<float> g = mk4<float>(0, 0, 0, 0), v_f = mk4<float>(0, 0, 0, 0);
   if (G.act) {
     long long cc = cell(a);
-    float4* rec = line_rec(A, dir_i != 0, cc);
-    M4<float> Lo = ld_m4(rec), Mi = ld_m4(rec + 12);
+    Rec rec = line_rec(A, dir_i != 0, cc);
+    M4<float> Lo = ld_m4(rec.blk(F_LO)), Mi = ld_m4(rec.blk(F_MINV)), Tk = ld_m4(rec.blk(F_T));
     float4 rin = in[cc];
     for (int k = a; k <= ke; ++k) {
-      M4<float> Lo_n = Lo, Mi_n = Mi;
+      M4<float> Lo_n = Lo, Mi_n = Mi, T_n = Tk;
       float4 rin_n = rin;
-      float4* rec_n = rec;
+      Rec rec_n = rec;
       if (k < ke) {
         long long cn = cell(k + 1);
         rec_n = line_rec(A, dir_i != 0, cn);
-        Lo_n = ld_m4(rec_n), Mi_n = ld_m4(rec_n + 12);
+        Lo_n = ld_m4(rec_n.blk(F_LO)), Mi_n = ld_m4(rec_n.blk(F_MINV)), T_n = ld_m4(rec_n.blk(F_T));
         rin_n = in[cn];
       }
       V4<float> r = from_f4(rin);
@@ -788,37 +833,21 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
         for (int q = 0; q < 4; ++q) r[q] -= t[q];
       }
       g = mv(Mi, r);
-      rec[24] = to_f4(g);
-      rec = rec_n, Lo = Lo_n, Mi = Mi_n, rin = rin_n;
+      *rec.g() = to_f4(g);
+      const V4<float> tg = mv(Tk, g);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v_f[q] += tg[q];
+      rec = rec_n, Lo = Lo_n, Mi = Mi_n, Tk = T_n, rin = rin_n;
     }
   }
   const V4<float> v_l = g;
-  V4<float> v_f = v_l;
-  if (G.act && ke - 1 >= a) {
-    const float4* rec = line_rec(A, dir_i != 0, cell(ke - 1));
-    M4<float> Yk = ld_m4(rec + 16);
-    float4 gk4 = rec[24];
-    for (int k = ke - 1; k >= a; --k) {
-      M4<float> Y_n = Yk;
-      float4 g_n = gk4;
-      if (k > a) {
-        const float4* rn = line_rec(A, dir_i != 0, cell(k - 1));
-        Y_n = ld_m4(rn + 16), g_n = rn[24];
-      }
-      V4<float> t = mv(Yk, v_f);
-      V4<float> gk = from_f4(gk4);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) v_f[q] = gk[q] - t[q];
-      Yk = Y_n, gk4 = g_n;
-    }
-  }
   const V4<float> vn = shfl_down4(v_f, 1);
   V4<float> rd = mk4<float>(0, 0, 0, 0);
   if (G.has_sep) {
     long long cs = cell(e - 1);
-    const float4* rec = line_rec(A, dir_i != 0, cs);
+    Rec rec = line_rec(A, dir_i != 0, cs);
     V4<float> r = from_f4(in[cs]);
-    V4<float> t1 = mv(ld_m4(rec), v_l), t2 = mv(ld_m4(rec + 8), vn);
+    V4<float> t1 = mv(ld_m4(rec.blk(F_LO)), v_l), t2 = mv(ld_m4(rec.blk(F_UP)), vn);
 #pragma unroll
     for (int q = 0; q < 4; ++q) rd[q] = r[q] - t1[q] - t2[q];
   }
@@ -850,17 +879,17 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
   if (G.has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
   {
     long long cc = cell(ke);
-    const float4* rec = line_rec(A, dir_i != 0, cc);
-    M4<float> GEk = ld_m4(rec + 20), Yk = ld_m4(rec + 16);
-    float4 gk4 = rec[24];
+    Rec rec = line_rec(A, dir_i != 0, cc);
+    M4<float> GEk = ld_m4(rec.blk(F_GE)), Yk = ld_m4(rec.blk(F_Y));
+    float4 gk4 = *rec.g();
     for (int k = ke; k >= a; --k) {
       M4<float> GE_n = GEk, Y_n = Yk;
       float4 g_n = gk4;
       long long cn = cc;
       if (k > a) {
         cn = cell(k - 1);
-        const float4* rn = line_rec(A, dir_i != 0, cn);
-        GE_n = ld_m4(rn + 20), Y_n = ld_m4(rn + 16), g_n = rn[24];
+        Rec rn = line_rec(A, dir_i != 0, cn);
+        GE_n = ld_m4(rn.blk(F_GE)), Y_n = ld_m4(rn.blk(F_Y)), g_n = *rn.g();
       }
       V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
       V4<float> gk = from_f4(gk4);
@@ -897,17 +926,17 @@ __global__ void k_defect(Arena A, int pass) {
   V4<float> acc = mk4<float>(0, 0, 0, 0);
   for (int dir = 0; dir < 2; ++dir) {
     bool di = dir == 0;
-    const float4* rec = line_rec(A, di, cc);
-    V4<float> v = mv(ld_m4(rec + 4), du);
+    Rec rec = line_rec(A, di, cc);
+    V4<float> v = mv(ld_m4(rec.blk(F_D)), du);
     int k = di ? i : j, kn = di ? c.ni : c.nj;
     int k0 = di ? row_start(c, j) : col_start(c, i);
     if (k > k0) {
-      V4<float> t2 = mv(ld_m4(rec), from_f4(A.DU[di ? cidx(c, i - 1, j) : cidx(c, i, j - 1)]));
+      V4<float> t2 = mv(ld_m4(rec.blk(F_LO)), from_f4(A.DU[di ? cidx(c, i - 1, j) : cidx(c, i, j - 1)]));
 #pragma unroll
       for (int q = 0; q < 4; ++q) v[q] += t2[q];
     }
     if (k + 1 < kn) {
-      V4<float> t2 = mv(ld_m4(rec + 8), from_f4(A.DU[di ? cidx(c, i + 1, j) : cidx(c, i, j + 1)]));
+      V4<float> t2 = mv(ld_m4(rec.blk(F_UP)), from_f4(A.DU[di ? cidx(c, i + 1, j) : cidx(c, i, j + 1)]));
 #pragma unroll
       for (int q = 0; q < 4; ++q) v[q] += t2[q];
     }

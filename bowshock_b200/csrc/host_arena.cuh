@@ -249,8 +249,9 @@ struct ArenaHost {
   int LT() const { return A.tile_list ? A.n_tl : ntiles; }
   int LP() const { return A.pblk_list ? A.n_pb : npblk; }
   int LI(int dir_i) const { return dir_i ? (A.iline_list ? A.n_il : nil) : (A.jline_list ? A.n_jl : njl); }
-  // floats of the line-solve records: 25 float4 per cell and direction, 44 float4 per lane of every line
-  size_t scratch_floats() const { return 4 * ((size_t)2 * ncell * 25 + (size_t)(nil + njl) * 32 * 44); }
+  // floats of the line-solve records: 29 float4 per cell and direction (rounded up to 64-byte blocks per direction),
+  // 44 float4 per lane of every line
+  size_t scratch_floats() const { return 4 * ((size_t)2 * rec_dir_stride(ncell) + (size_t)(nil + njl) * 32 * PREC); }
   bool any_viscous = false, any_sst = false, any_rough = false;
   // device buffers
   Arena A{};
@@ -748,19 +749,29 @@ struct ArenaHost {
     prof_ms[g] += ms;
     prof_launches[g] += 1;
   }
-  // lines per block of the line kernels (1, 2, 4 or 8), picked by autotune()
-  int lw_lines = LINE_WARPS, lw_subst = LINE_WARPS, lw_turb = TL_WARPS;
-  void launch_lines(int dir_i, const float4* in, int from_res, float4* out) {
-    const int nl = LI(dir_i), w = lw_lines > 4 ? 4 : lw_lines;  // 8 lines would exceed the static shared memory
+  // Launch shapes of the line kernels, picked by autotune() per direction ([0] = j lines, [1] = i lines): lines per
+  // block (1, 2, 4, or 8 except for the first pass, whose shared memory holds 4 lines at most) and, for the first pass,
+  // whether the walks prefetch the next cell's record.
+  int lw_lines[2] = {LINE_WARPS, LINE_WARPS}, pf_lines[2] = {0, 0}, lw_subst[2] = {LINE_WARPS, LINE_WARPS}, lw_turb = TL_WARPS;
+  template <bool PF>
+  void launch_lines_pf(int dir_i, int w, const float4* in, int from_res, float4* out) {
+    const int nl = LI(dir_i);
     const int nb = (nl + w - 1) / w;
     switch (w) {
-      case 1: k_lines<1><<<nb, 32, 0, stream>>>(A, dir_i, in, from_res, out); break;
-      case 2: k_lines<2><<<nb, 64, 0, stream>>>(A, dir_i, in, from_res, out); break;
-      default: k_lines<4><<<nb, 128, 0, stream>>>(A, dir_i, in, from_res, out); break;
+      case 1: k_lines<1, PF><<<nb, 32, 0, stream>>>(A, dir_i, in, from_res, out); break;
+      case 2: k_lines<2, PF><<<nb, 64, 0, stream>>>(A, dir_i, in, from_res, out); break;
+      default: k_lines<4, PF><<<nb, 128, 0, stream>>>(A, dir_i, in, from_res, out); break;
     }
   }
+  void launch_lines(int dir_i, const float4* in, int from_res, float4* out) {
+    const int d = dir_i ? 1 : 0, w = lw_lines[d] > 4 ? 4 : lw_lines[d];
+    if (pf_lines[d])
+      launch_lines_pf<true>(dir_i, w, in, from_res, out);
+    else
+      launch_lines_pf<false>(dir_i, w, in, from_res, out);
+  }
   void launch_subst(int dir_i, const float4* in, float4* out, int pass) {
-    const int nl = LI(dir_i), w = lw_subst;
+    const int nl = LI(dir_i), w = lw_subst[dir_i ? 1 : 0];
     const int nb = (nl + w - 1) / w;
     switch (w) {
       case 1: k_lines_subst<1><<<nb, 32, 0, stream>>>(A, dir_i, in, out, pass); break;
@@ -779,9 +790,10 @@ struct ArenaHost {
       default: k_turb_lines_w<4><<<nb, 128, 0, stream>>>(A, dir_i); break;
     }
   }
-  // Autotuner: lines per block of the block line kernels (first pass and substitution passes) and of the SST line
-  // kernel, each the fastest of {1, 2, 4, 8} over two timed iterations of this arena's own cases. The state, turbulence
-  // and counters are restored afterwards; the choice does not change any result (every warp solves one line alone).
+  // Autotuner: per direction, lines per block and prefetching of the first pass and lines per block of the substitution
+  // passes, and lines per block of the SST line kernel: each the fastest candidate over two timed iterations of this
+  // arena's own cases. The state, turbulence and counters are restored afterwards; the choice does not change any
+  // result (every warp solves one line alone, with the same arithmetic).
   int autotune() {
     if (scheme_of_arena() != SCHEME_IMPLICIT) return 0;
     const size_t nc = cases.size();
@@ -799,18 +811,30 @@ struct ArenaHost {
     BK_CUDA(cudaMemcpy(hit.data(), d_iter, nc * sizeof(int), cudaMemcpyDeviceToHost));
     BK_CUDA(cudaMemcpy(hr.data(), d_ramp, nc * sizeof(int), cudaMemcpyDeviceToHost));
     const int cand[4] = {1, 2, 4, 8};
-    double best[3] = {1e30, 1e30, 1e30};
-    int pick[3] = {LINE_WARPS, LINE_WARPS, TL_WARPS};
+    // timed groups: first pass j / i, substitution j / i, SST lines
+    const int grp[5] = {G_LINES_J, G_LINES_I, G_SUBST_J, G_SUBST_I, G_TURB_LINES};
+    double best[5] = {1e30, 1e30, 1e30, 1e30, 1e30};
+    int pick_w[5] = {LINE_WARPS, LINE_WARPS, LINE_WARPS, LINE_WARPS, TL_WARPS}, pick_pf[2] = {0, 0};
     int rc = 0;
-    for (int w : cand) {
-      lw_lines = lw_subst = lw_turb = w;
-      if ((rc = profile(1))) return rc;  // warm-up of this variant
-      if ((rc = profile(2))) return rc;
-      double t[3] = {prof_ms[G_LINES_I] + prof_ms[G_LINES_J], prof_ms[G_SUBST_I] + prof_ms[G_SUBST_J], prof_ms[G_TURB_LINES]};
-      for (int q = 0; q < 3; ++q)
-        if (t[q] < best[q]) best[q] = t[q], pick[q] = w;
-    }
-    lw_lines = pick[0] > 4 ? 4 : pick[0], lw_subst = pick[1], lw_turb = pick[2];
+    for (int pf = 0; pf < 2; ++pf)
+      for (int w : cand) {
+        if (pf && w > 4) continue;
+        lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
+        pf_lines[0] = pf_lines[1] = pf;
+        if ((rc = profile(1))) return rc;  // warm-up of this variant
+        if ((rc = profile(2))) return rc;
+        for (int q = 0; q < 5; ++q) {
+          if (q >= 2 && pf) continue;  // only the first pass has the prefetching variant
+          if (q < 2 && w > 4) continue;
+          const double t = prof_ms[grp[q]];
+          if (t < best[q]) {
+            best[q] = t, pick_w[q] = w;
+            if (q < 2) pick_pf[q] = pf;
+          }
+        }
+      }
+    lw_lines[0] = pick_w[0], lw_lines[1] = pick_w[1], pf_lines[0] = pick_pf[0], pf_lines[1] = pick_pf[1];
+    lw_subst[0] = pick_w[2], lw_subst[1] = pick_w[3], lw_turb = pick_w[4];
     BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     if (any_sst) {

@@ -295,12 +295,16 @@ int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
  * total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
 #define BOWSHOCK_PROFILE_GROUPS 12
 int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
-/* Lines per block (1, 2 or 4 for the first pass; 1, 2, 4 or 8 otherwise) of the block line kernels' first pass, of their
- * substitution passes and of the SST line
- * kernel, as the arena's autotuner picked them at creation (arenas of 100,000 cells or more; 4 otherwise): the fastest
- * of two timed iterations of the arena's own cases per candidate, the state restored afterwards. No counterpart in the
- * reference (its line solves run in Luma, gpu/implicit.rs:731-732). */
-int bowshock_arena_tuning(const bowshock_arena* a, int32_t* lines_per_block);
+/* Launch shapes of the line kernels as the arena's autotuner picked them at creation (arenas of 100,000 cells or more;
+ * otherwise 4 lines per block, no prefetching): per direction, lines per block (1, 2 or 4) of the block line solves'
+ * first pass and whether its walks prefetch the next cell's record (0 / 1), lines per block (1, 2, 4 or 8) of their
+ * substitution passes, and lines per block of the SST line kernel; each the fastest of two timed iterations of the
+ * arena's own cases per candidate, the state restored afterwards. No counterpart in the reference (its line solves run
+ * in Luma, gpu/implicit.rs:731-732). */
+typedef struct {
+  int32_t lines_i, lines_j, prefetch_i, prefetch_j, subst_i, subst_j, turb_lines;
+} bowshock_line_tuning;
+int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out);
 
 /* ---------------------------------------------------------------------------------------------- 3D Euler
  * The stability path (crates/bowshock-cfd/src/solver3.rs + implicit3.rs behind `GpuSolver3`, gpu/mod.rs:442-560, driven
@@ -354,14 +358,14 @@ int bowshock3_last_ms_per_iter(const bowshock3_batch* b, double* ms);
  * synchronisation an allocation may cause. bowshock_solver_run allocates on its first call (CUDA graph instantiation,
  * timing events); this variant launches the same kernels directly on the solver's stream and takes the line solves'
  * records (blocks, factors, reduction multipliers) from a static 64 MiB device array of the library. A solver needs
- * BOWSHOCK_NOALLOC_BYTES(cells, lines) of it, cells and i + j lines of all multigrid levels counted (about 80,000 cells
- * for a grid of aspect 2); a larger one gets BOWSHOCK_INVALID with a message and nothing is launched. Same residual
+ * BOWSHOCK_NOALLOC_BYTES(cells, lines) of it, cells and i + j lines of all multigrid levels counted (about 60,000 cells
+ * for a single-level grid of aspect 2); a larger one gets BOWSHOCK_INVALID with a message and nothing is launched. Same residual
  * semantics and results as bowshock_solver_run.
  * The first call on a device looks the array's device address up (cudaGetSymbolAddress with that device current); make
  * that first call before any stream capture. Every call on a device shares the array (nothing in it needs to start at
  * zero); calls that overlap on one GPU, from solvers on other streams or threads, race on it and must be serialised. */
 #define BOWSHOCK_NOALLOC_SCRATCH_BYTES (64u << 20)
-#define BOWSHOCK_NOALLOC_BYTES(cells, lines) (400ull * 2ull * (unsigned long long)(cells) + 22528ull * (unsigned long long)(lines))
+#define BOWSHOCK_NOALLOC_BYTES(cells, lines) (928ull * (unsigned long long)(cells) + 128ull + 22528ull * (unsigned long long)(lines))
 int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, double* residual);
 
 #ifdef __cplusplus

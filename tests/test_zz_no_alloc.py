@@ -57,8 +57,8 @@ def test_noalloc_rejects_a_solver_beyond_the_static_scratch():
     from bowshock_b200._ffi import BowshockError
     from tests.test_oracle_solver import curved_grid
     import oracle_ffi as o
-    ni, nj = 512, 256  # 131,072 cells, 768 lines: 122 MB of line records
-    assert 800 * ni * nj + 22528 * (ni + nj) > 64 << 20
+    ni, nj = 512, 256  # 131,072 cells, 768 lines: 139 MB of line records
+    assert 928 * ni * nj + 22528 * (ni + nj) > 64 << 20
     x, r = curved_grid(ni, nj)
     spec = cases.Spec(ni, nj, x, r, 0.5, o.MINMOD, tuple(o.freestream(0.5)),
                       (o.BC_CHARACTERISTIC, o.BC_CHARACTERISTIC, o.BC_SLIPWALL, o.BC_CHARACTERISTIC), 0, label="large")
