@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
   int lt = t - c.tile_off;
   int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
   if (i >= c.ni || j >= c.nj || is_solid(c, i, j)) return;
-  long long cc = cidx(c, i, j);
+  const long long cc = cidx(c, i, j);
 #pragma unroll 1
   for (int dir = 0; dir < 2; ++dir) {
     M4<float> lo, d, up;
@@ -467,12 +467,13 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
 
 // Ghost Jacobians of the two ends of line `L` folded into the diagonal blocks (implicit.rs:440-467): at the first cell
 // d += lo T and lo = 0, with T the wall reflection / no-slip, the jet's zero, or the far-field ghost Jacobian (FP64 finite
-// differences); at the last cell d += up T and up = 0. One thread per line, after k_assemble.
-__device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int L) {
+// differences); at the last cell d += up T and up = 0. One thread per line end (`ends` bit 0: first, bit 1: last; a line
+// of one cell has both ends in one thread), after k_assemble.
+__device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int L, int ends) {
   const int n = dir_i ? c.ni : c.nj;
   const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
   if (k0 >= n) return;
-  {
+  if (ends & 1) {
     const int i = dir_i ? k0 : L, j = dir_i ? L : k0;
     const long long cc = cidx(c, i, j);
     float4 fl = dir_i ? A.iface[ifidx(c, i, j)] : A.jface[jfidx(c, i, j)];
@@ -502,7 +503,7 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
     st_m4(rec.blk(F_LO), zero4<float>());
     st_m4(rec.blk(F_D), d);
   }
-  {
+  if (ends & 2) {
     const int i = dir_i ? n - 1 : L, j = dir_i ? L : n - 1;
     const long long cc = cidx(c, i, j);
     float4 fr = dir_i ? A.iface[ifidx(c, i + 1, j)] : A.jface[jfidx(c, i, j + 1)];
@@ -522,17 +523,25 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
   }
 }
 
-// every i line, then every j line, of the active cases
+// two threads per line (first end, last end): every i line, then every j line, of the active cases
 __global__ void k_line_ends(Arena A) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = t & 1, l = t >> 1;
   const int nli = lines_of(A, true);
-  bool dir_i = t < nli;
-  int gw = line_at(A, dir_i, dir_i ? t : t - nli);
+  const bool dir_i = l < nli;
+  const int gw = line_at(A, dir_i, dir_i ? l : l - nli);
   if (gw < 0) return;
-  int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
-  fold_line_ends(A, c, dir_i, gw - (dir_i ? c.iline_off : c.jline_off));
+  const int L = gw - (dir_i ? c.iline_off : c.jline_off);
+  const int n = dir_i ? c.ni : c.nj;
+  const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
+  if (n - k0 == 1) {  // one cell: both ends in the first thread (the two folds update the same diagonal block)
+    if (e == 0) fold_line_ends(A, c, dir_i, L, 3);
+    return;
+  }
+  fold_line_ends(A, c, dir_i, L, e ? 2 : 1);
 }
 
 // First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble and k_line_ends left in the line records, factorise

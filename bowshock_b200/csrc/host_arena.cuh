@@ -780,14 +780,27 @@ struct ArenaHost {
       default: k_lines_subst<4><<<nb, 128, 0, stream>>>(A, dir_i, in, out, pass); break;
     }
   }
-  void launch_turb_lines(int dir_i) {
+  void launch_turb_lines(int dir_i, cudaStream_t st) {
     const int nl = LI(dir_i), w = lw_turb;
     const int nb = (nl + w - 1) / w;
     switch (w) {
-      case 1: k_turb_lines_w<1><<<nb, 32, 0, stream>>>(A, dir_i); break;
-      case 2: k_turb_lines_w<2><<<nb, 64, 0, stream>>>(A, dir_i); break;
-      case 8: k_turb_lines_w<8><<<nb, 256, 0, stream>>>(A, dir_i); break;
-      default: k_turb_lines_w<4><<<nb, 128, 0, stream>>>(A, dir_i); break;
+      case 1: k_turb_lines_w<1><<<nb, 32, 0, st>>>(A, dir_i); break;
+      case 2: k_turb_lines_w<2><<<nb, 64, 0, st>>>(A, dir_i); break;
+      case 8: k_turb_lines_w<8><<<nb, 256, 0, st>>>(A, dir_i); break;
+      default: k_turb_lines_w<4><<<nb, 128, 0, st>>>(A, dir_i); break;
+    }
+  }
+  // turbulence.rs:542-581, from this iteration's primitives, mass fluxes, gradients and time step: the SST update up to
+  // its final step
+  void launch_turb_chain(cudaStream_t st, int slot) {
+    L(G_TURB, [&] { k_turb_grad<<<LT(), TI * TJ, 0, st>>>(A); });
+    L(G_TURB, [&] { k_turb_cell<<<LT(), TI * TJ, 0, st>>>(A, slot); });
+    if (max_line <= 32 * TL_MAXM) {
+      L(G_TURB_LINES, [&] { launch_turb_lines(1, st); });
+      L(G_TURB_LINES, [&] { launch_turb_lines(0, st); });
+    } else {  // thread-per-line kernel: its Thomas coefficients borrow the line records, so it runs after the mean flow
+      L(G_TURB, [&] { k_turb_lines<<<(2 * LI(1) + 127) / 128, 128, 0, st>>>(A, 1); });
+      L(G_TURB, [&] { k_turb_lines<<<(2 * LI(0) + 127) / 128, 128, 0, st>>>(A, 0); });
     }
   }
   // Autotuner: per direction, lines per block and prefetching of the first pass and lines per block of the substitution
@@ -868,7 +881,7 @@ struct ArenaHost {
       L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 2, slot); });
       const int s = sub_iters_of_arena();
       L(G_ASSEMBLE, [&] { k_assemble<<<LT(), TI * TJ, 0, stream>>>(A); });
-      L(G_ASSEMBLE, [&] { k_line_ends<<<(LI(1) + LI(0) + 127) / 128, 128, 0, stream>>>(A); });
+      L(G_ASSEMBLE, [&] { k_line_ends<<<(2 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
@@ -877,17 +890,7 @@ struct ArenaHost {
         L(G_SUBST_J, [&] { launch_subst(0, A.X, nullptr, p); });
       }
       if (any_sst) {
-        // turbulence.rs:542-611, from this iteration's primitives, mass fluxes, gradients and time step
-        L(G_TURB, [&] { k_turb_grad<<<LT(), TI * TJ, 0, stream>>>(A); });
-        L(G_TURB, [&] { k_turb_blend<<<LT(), TI * TJ, 0, stream>>>(A); });
-        L(G_TURB, [&] { k_turb_cell<<<LT(), TI * TJ, 0, stream>>>(A, slot); });
-        if (max_line <= 32 * TL_MAXM) {
-          L(G_TURB_LINES, [&] { launch_turb_lines(1); });
-          L(G_TURB_LINES, [&] { launch_turb_lines(0); });
-        } else {
-          L(G_TURB, [&] { k_turb_lines<<<(2 * LI(1) + 127) / 128, 128, 0, stream>>>(A, 1); });
-          L(G_TURB, [&] { k_turb_lines<<<(2 * LI(0) + 127) / 128, 128, 0, stream>>>(A, 0); });
-        }
+        launch_turb_chain(stream, slot);
         L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
       }
     } else {

@@ -1,7 +1,7 @@
 // Menter SST k-omega update (crates/bowshock-cfd/src/turbulence.rs:542-611) on the arena, loosely coupled after each
 // mean-flow iteration as in the reference:
-//   k_turb_grad   Green-Gauss gradients of k and omega with the boundary states of the two scalars (turbulence.rs:337-372)
-//   k_turb_blend  F1 and the cross-diffusion X (turbulence.rs:375-397)
+//   k_turb_grad   Green-Gauss gradients of k and omega with the boundary states of the two scalars (turbulence.rs:337-372),
+//                 then F1 and the cross-diffusion X of the cell (turbulence.rs:375-397)
 //   k_turb_cell   face convection / diffusion data of the four faces (turbulence.rs:413-435) and the cell terms: residual,
 //                 diag0 and the coefficients of the i- and j-line systems (turbulence.rs:477-519, 559-579)
 //   k_turb_lines  the two scalar tridiagonal line systems, i then j, one thread per (line, scalar) (turbulence.rs:580-581);
@@ -59,7 +59,23 @@ __device__ __forceinline__ float2 kw_side(const Arena& A, const CaseDev& c, cons
   return make_float2(-t.x, 2.f * (60.f * nu / (BETA1 * d * d)) - t.y);
 }
 
-__global__ void k_turb_grad(Arena A) {  // turbulence.rs:337-372
+// F1 and the cross-diffusion X of a fluid cell from its own gradient (turbulence.rs:375-397)
+__device__ __forceinline__ float2 blend_of(const Arena& A, const CaseDev& c, int i, int j, long long cc, float4 g) {
+  float rho = A.W[pidx(c, i, j)].x;
+  float nu = A.mu[cc] / rho;
+  float2 kw = A.turb[cc];
+  float d = A.dwall[cc];
+  float x = 2.f * rho * SIGMA_W2 * (g.x * g.z + g.y * g.w) / kw.y;
+  float cd = fmaxf(x, 1e-20f);
+  float t1 = sqrtf(kw.x) / (BETA_STAR * kw.y * d), t2 = 500.f * nu / (d * d * kw.y);
+  float t3 = 4.f * rho * SIGMA_W2 * kw.x / (cd * d * d);
+  float a = fminf(fmaxf(t1, t2), t3);
+  float a2 = a * a;
+  return make_float2(tanhf(a2 * a2), x);
+}
+
+// Green-Gauss gradients of k and omega (turbulence.rs:337-372) and, from the cell's own gradient, its blend (F1, X)
+__global__ void k_turb_grad(Arena A) {
   int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
@@ -70,6 +86,7 @@ __global__ void k_turb_grad(Arena A) {  // turbulence.rs:337-372
   long long cc = cidx(c, i, j);
   if (is_solid(c, i, j)) {
     A.grad_kw[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+    A.blend[cc] = make_float2(0.f, 0.f);
     return;
   }
   float2 pc = A.turb[cc];
@@ -92,34 +109,9 @@ __global__ void k_turb_grad(Arena A) {  // turbulence.rs:337-372
     g[3] += sg[f] * pw * fs4[f].y * fs4[f].z;
   }
   float inv_a = 1.f / A.cellg[cc].y;
-  A.grad_kw[cc] = make_float4(g[0] * inv_a, g[1] * inv_a, g[2] * inv_a, g[3] * inv_a);
-}
-
-__global__ void k_turb_blend(Arena A) {  // turbulence.rs:375-397
-  int t = tile_at(A);
-  int ci = A.tile_case[t];
-  const CaseDev& c = A.cases[ci];
-  if (!A.active[ci] || !c.sst) return;
-  int lt = t - c.tile_off;
-  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
-  if (i >= c.ni || j >= c.nj) return;
-  long long cc = cidx(c, i, j);
-  if (is_solid(c, i, j)) {
-    A.blend[cc] = make_float2(0.f, 0.f);
-    return;
-  }
-  float rho = A.W[pidx(c, i, j)].x;
-  float nu = A.mu[cc] / rho;
-  float2 kw = A.turb[cc];
-  float d = A.dwall[cc];
-  float4 g = A.grad_kw[cc];
-  float x = 2.f * rho * SIGMA_W2 * (g.x * g.z + g.y * g.w) / kw.y;
-  float cd = fmaxf(x, 1e-20f);
-  float t1 = sqrtf(kw.x) / (BETA_STAR * kw.y * d), t2 = 500.f * nu / (d * d * kw.y);
-  float t3 = 4.f * rho * SIGMA_W2 * kw.x / (cd * d * d);
-  float a = fminf(fmaxf(t1, t2), t3);
-  float a2 = a * a;
-  A.blend[cc] = make_float2(tanhf(a2 * a2), x);
+  const float4 gk = make_float4(g[0] * inv_a, g[1] * inv_a, g[2] * inv_a, g[3] * inv_a);
+  A.grad_kw[cc] = gk;
+  A.blend[cc] = blend_of(A, c, i, j, cc, gk);
 }
 
 struct TFaceD {

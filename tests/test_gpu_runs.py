@@ -62,3 +62,15 @@ def test_arena_cases_match_single_case_solvers():
         rs = s.run(40)
         assert np.array_equal(a.state(k), s.state_f64()), f"case {k} differs from its single-case solver"
         assert np.allclose(ra[:, k], rs, rtol=1e-12)
+
+
+def test_captured_chunks_match_kernel_by_kernel_launches():
+    """run() replays 50-iteration chunks captured as CUDA graphs; profile() launches the same kernels one at a time
+    (SST case). The states agree bit for bit."""
+    from bowshock_b200.arena import Arena
+    pc, _ = g3_cases()
+    pc.numerics.first_order_iters = 5
+    a, b = Arena([pc]), Arena([pc])
+    a.run(30)
+    b.profile(30)
+    assert np.array_equal(a.state(0), b.state(0))
