@@ -360,19 +360,26 @@ def run_ours(args, rank, world, dist):
 
 def run_kernels(args):
     """The timed region alone (arena, warm-up, K iterations): the command the ncu captures of the kernels run. With
-    --workload lift3: the 15-case 3D Euler batch (192 x 64 x 64 cells per case) instead."""
+    --workload lift3: the 15-case 3D Euler batch (192 x 64 x 64 cells per case) instead. The K timed iterations are
+    bracketed by cudaProfilerStart / Stop, so that `ncu --profile-from-start off` captures exactly their launches."""
+    import torch
+
     import bowshock_b200  # noqa: F401
     if args.workload == "lift3":
         import bowshock_b200.euler3 as e3
         b, _ = e3.batch_of(e3.lift_sweep_cases())
         b.run(max(args.warmup, 1))
+        torch.cuda.profiler.start()
         b.run(args.steps)
+        torch.cuda.profiler.stop()
         return {"kernels_only": True, "workload": "lift3", "cells": b.nc * b.nb, "steps": args.steps, "ms_per_step": b.ms_per_iter()}
     from bowshock_b200.arena import Arena
     cases = build_cases(0)
     arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
     arena.run(max(args.warmup, 3))
+    torch.cuda.profiler.start()
     arena.run(args.steps)
+    torch.cuda.profiler.stop()
     ms = arena.ms_per_iter()
     prof = {g: round(v[0] / v[1], 4) for g, v in arena.profile(3).items() if v[1]} if args.steps >= 10 else None
     return {"kernels_only": True, "cells": arena.cells, "steps": args.steps, "ms_per_step": ms, "ms_per_launch": prof,
