@@ -81,7 +81,8 @@ class StingGridC(C.Structure):  # bowshock_sting_grid
 
 
 class LineTuning(C.Structure):  # bowshock_line_tuning
-    _fields_ = [(n, C.c_int32) for n in ("lines_i", "lines_j", "prefetch_i", "prefetch_j", "subst_i", "subst_j", "turb_lines")]
+    _fields_ = [(n, C.c_int32) for n in ("lines_i", "lines_j", "prefetch_i", "prefetch_j", "subst_i", "subst_j", "turb_lines",
+                                              "segment_i", "segment_j")]
 
 
 class CaseDesc(C.Structure):  # bowshock_case_desc
@@ -145,6 +146,7 @@ SIGNATURES = {
     "bowshock_arena_last_solve_ms": (_I, [_P, _dp]),
     "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
     "bowshock_arena_tuning": (_I, [_P, C.POINTER(LineTuning)]),
+    "bowshock_arena_set_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_solver_run_noalloc": (_I, [_P, _U, _dp]),
 }
 

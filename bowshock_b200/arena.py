@@ -80,6 +80,13 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_tuning(self._h, C.byref(t)))
         return {n: int(getattr(t, n)) for n, _ in _ffi.LineTuning._fields_}
 
+    def set_tuning(self, **shape):
+        """Pin launch shapes (the keys of tuning(); unspecified ones keep their current values)."""
+        cur = self.tuning()
+        cur.update(shape)
+        t = _ffi.LineTuning(*[int(cur[n]) for n, _ in _ffi.LineTuning._fields_])
+        self._check(_ffi.load().bowshock_arena_set_tuning(self._h, C.byref(t)))
+
     def solve(self, progress=None):
         """Cold-start every case and iterate each to its stop rule (converged cases are masked out)."""
         res = (_ffi.PointResult * self.ncases)()

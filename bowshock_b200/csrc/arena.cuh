@@ -94,6 +94,9 @@ struct Arena {
   // lines only; the kernels map their block / line index through these lists (null: every entry).
   const int *tile_list, *pblk_list, *iline_list, *jline_list;
   int n_tl, n_pb, n_il, n_jl;
+  // Smallest segment (cells per lane) of the block line solves, i and j lines (>= 2; the same for a first pass and the
+  // substitution passes that reuse its factors)
+  int mmin_i = 2, mmin_j = 2;
 };
 
 constexpr int TI = 32, TJ = 8;  // residual tile

@@ -397,7 +397,10 @@ struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
 };
 
 // Line geometry shared by the factorisation and substitution kernels: warp `gw` solves line L of case c; lane s owns the
-// segment [a, e) of m = max(2, ceil(len/32)) cells, the last cell of every segment but the last is a separator.
+// segment [a, e) of m = max(m_min, ceil(len/32)) cells, the last cell of every segment but the last is a separator.
+// m_min >= 2 (Arena::mmin_i / mmin_j, picked per direction by the autotuner): short lines with a larger m_min have fewer
+// separators, so fewer reduction multipliers to store and read (22.5 KB per line at 31 separators), and longer segments
+// per lane.
 struct LineSeg {
   int gw, ci, L, n, k0, len, m, P, N, a, e, ke;
   bool act, has_sep;
@@ -415,7 +418,8 @@ __device__ __forceinline__ bool line_seg(const Arena& A, int dir_i, int idx, int
   g.len = g.n - g.k0;
   if (g.len <= 0) return false;
   g.m = (g.len + 31) / 32;
-  if (g.m < 2) g.m = 2;
+  const int mmin = dir_i ? A.mmin_i : A.mmin_j;
+  if (g.m < mmin) g.m = mmin;
   g.P = (g.len + g.m - 1) / g.m;
   g.N = g.P - 1;
   g.act = lane < g.P;

@@ -74,3 +74,22 @@ def test_captured_chunks_match_kernel_by_kernel_launches():
     a.run(30)
     b.profile(30)
     assert np.array_equal(a.state(0), b.state(0))
+
+
+@pytest.mark.parametrize("segment", [4, 8])
+def test_longer_line_segments_match_the_oracle(segment):
+    """Line solves with at least `segment` cells per lane (fewer separators on short lines, a shape the autotuner may
+    pick): the viscous.rs body protocol against the oracle, 30 implicit iterations, state within 1e-3."""
+    from bowshock_b200.arena import Arena
+    from tests import cases
+    pc, oc = g3_cases()
+    pc.numerics.first_order_iters = 5
+    a = Arena([pc])
+    a.set_tuning(segment_i=segment, segment_j=segment)
+    assert a.tuning()["segment_i"] == segment
+    a.run(30)
+    spec = cases.from_case(oc, "G3")
+    spec.first_order_iters = 5
+    cpu = cases.oracle_solver(spec)
+    cpu.steps(30)
+    assert cases.state_diff(a.state(0), cpu.u) < 1e-3
