@@ -121,11 +121,15 @@ __device__ __forceinline__ double4 to_d4(const V4<double>& v) { return make_doub
 __device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(v.x, v.y, v.z, v.w); }
 
 // dt_kind: 0 = keep dt, 1 = explicit local time step (solver.rs:614-643), 2 = implicit pseudo-time step (implicit.rs:666-695)
-__global__ void __launch_bounds__(TI* TJ, 3) k_residual(Arena A, int dt_kind, int slot) {
+// NT threads per block (>= TI * TJ; the first TI * TJ also own a cell each): the tile's TJ (TI + 1) + (TJ + 1) TI = 552 face
+// fluxes are spread over all NT, so with NT = 288 no thread computes more than two of them (three with 256); MINB blocks
+// per SM bound the registers. The arena's autotuner picks the variant of the implicit iteration; the results are the same.
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int slot) {
   __shared__ float4 sW[TJ + 4][TI + 4], sWl[TJ + 4][TI + 4];
   __shared__ double4 sFI[TJ][TI + 1];
   __shared__ double4 sFJ[TJ + 1][TI];
-  __shared__ double sred[TI * TJ / 32];
+  __shared__ double sred[NT / 32];
   __shared__ float s_cfl;
   const int t = tile_at(A);
   const int ci = A.tile_case[t];
@@ -196,7 +200,7 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_residual(Arena A, int dt_kind, in
   const int q = tid % TI, r = tid / TI;
   const int i = i0 + q, j = j0 + r;
   double rr = 0.0;
-  if (i < ni && j < nj) {
+  if (tid < TI * TJ && i < ni && j < nj) {
     long long cc = cidx(c, i, j);
     if (is_solid(c, i, j)) {
       A.R[cc] = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -694,13 +694,13 @@ struct ArenaHost {
   // one SSP-RK3 step of the active level (solver.rs:694-710); `slot` records the first stage's density residual
   void rk3(int slot, int last) {
     launch_mean_flow_prep();
-    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot); });
+    L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot); });
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
     launch_mean_flow_prep();
-    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
     launch_mean_flow_prep();
-    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, last); });
   }
   void mg_level(int l, int slot) {  // multigrid.rs:87-112
@@ -710,11 +710,11 @@ struct ArenaHost {
     for (int k = 0; k < n_pre; ++k) rk3(l == 0 && k == 0 ? slot : -1, 0);
     if (coarsest) return;
     launch_mean_flow_prep();
-    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, (l == 0 && n_pre == 0) ? slot : -1); });
+    L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, (l == 0 && n_pre == 0) ? slot : -1); });
     L(G_STAGE, [&] { k_restrict_state<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
     set_level(l + 1);
     launch_mean_flow_prep();
-    L(G_RESIDUAL, [&] { k_residual<<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
     L(G_STAGE, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
     for (int g = 0; g < std::max(mg_gamma, 1); ++g) mg_level(l + 1, -1);
     L(G_STAGE, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l); });
@@ -748,6 +748,15 @@ struct ArenaHost {
     cudaEventElapsedTime(&ms, pe0, pe1);
     prof_ms[g] += ms;
     prof_launches[g] += 1;
+  }
+  // residual kernel of the implicit iteration: 0 = 256 threads and 3 blocks per SM, 1 = 288 and 2, 2 = 288 and 3
+  int res_variant = 0;
+  void launch_residual(int dt_kind, int slot) {
+    switch (res_variant) {
+      case 1: k_residual<288, 2><<<LT(), 288, 0, stream>>>(A, dt_kind, slot); break;
+      case 2: k_residual<288, 3><<<LT(), 288, 0, stream>>>(A, dt_kind, slot); break;
+      default: k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, dt_kind, slot); break;
+    }
   }
   // Launch shapes of the line kernels, picked by autotune() per direction ([0] = j lines, [1] = i lines): lines per
   // block (1, 2, 4, or 8 except for the first pass, whose shared memory holds 4 lines at most) and, for the first pass,
@@ -804,7 +813,7 @@ struct ArenaHost {
     }
   }
   // Autotuner: per direction, the smallest segment per lane, lines per block and prefetching of the first pass and lines
-  // per block of the substitution passes, and lines per block of the SST line kernel: each the fastest candidate over
+  // per block of the substitution passes, lines per block of the SST line kernel, and the residual kernel's variant: each the fastest candidate over
   // two timed iterations of this arena's own cases. The state, turbulence and counters are restored afterwards; the choice does not change any
   // result (every warp solves one line alone, with the same arithmetic).
   int autotune() {
@@ -862,6 +871,15 @@ struct ArenaHost {
     lw_lines[0] = pick_w[mj][0], pf_lines[0] = pick_pf[mj][0], lw_subst[0] = pick_w[mj][2];
     lw_lines[1] = pick_w[mi_][1], pf_lines[1] = pick_pf[mi_][1], lw_subst[1] = pick_w[mi_][3];
     lw_turb = pick_w[mt][4];
+    double best_r = 1e30;
+    int pick_r = 0;
+    for (int v = 0; v < 3; ++v) {
+      res_variant = v;
+      if ((rc = profile(1))) return rc;
+      if ((rc = profile(2))) return rc;
+      if (prof_ms[G_RESIDUAL] < best_r) best_r = prof_ms[G_RESIDUAL], pick_r = v;
+    }
+    res_variant = pick_r;
     BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     if (any_sst) {
@@ -892,7 +910,7 @@ struct ArenaHost {
       set_level(0);
     } else if (scheme_of_arena() == SCHEME_IMPLICIT) {
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 2, slot); });
+      L(G_RESIDUAL, [&] { launch_residual(2, slot); });
       const int s = sub_iters_of_arena();
       L(G_ASSEMBLE, [&] { k_assemble<<<LT(), TI * TJ, 0, stream>>>(A); });
       L(G_ASSEMBLE, [&] { k_line_ends<<<(2 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
@@ -909,13 +927,13 @@ struct ArenaHost {
       }
     } else {
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 1, slot); });
+      L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 1, slot); });
       L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
       L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
       launch_mean_flow_prep();
-      L(G_RESIDUAL, [&] { k_residual<<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
       L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1); });
     }
   }
@@ -1018,7 +1036,7 @@ struct ArenaHost {
     const int nc = (int)cases.size();
     BK_CUDA(cudaMemsetAsync(A.rsum, 0, nc * sizeof(double), stream));
     launch_mean_flow_prep();
-    k_residual<<<LT(), TI * TJ, 0, stream>>>(A, dt_kind, 0);
+    k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, dt_kind, 0);
     BK_CUDA(cudaGetLastError());
     std::vector<double> h(nc);
     BK_CUDA(cudaMemcpyAsync(h.data(), A.rsum, nc * sizeof(double), cudaMemcpyDeviceToHost, stream));

@@ -298,12 +298,13 @@ int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* 
 /* Launch shapes of the line kernels as the arena's autotuner picked them at creation (arenas of 100,000 cells or more;
  * otherwise 4 lines per block, no prefetching, segments of at least 2 cells): per direction, lines per block (1, 2 or 4)
  * of the block line solves' first pass and whether its walks prefetch the next cell's record (0 / 1), lines per block
- * (1, 2, 4 or 8) of their substitution passes, lines per block of the SST line kernel, and per direction the smallest
- * segment a lane eliminates (2, 4 or 8 cells: fewer separators on short lines); each the fastest of two timed iterations
+ * (1, 2, 4 or 8) of their substitution passes, lines per block of the SST line kernel, per direction the smallest
+ * segment a lane eliminates (2, 4 or 8 cells: fewer separators on short lines), and the residual kernel's variant (0: 256
+ * threads per 32 x 8 tile, 3 blocks per SM; 1: 288 threads, 2 blocks; 2: 288 threads, 3 blocks); each the fastest of two timed iterations
  * of the arena's own cases per candidate, the state restored afterwards. No counterpart in the reference (its line
  * solves run in Luma, gpu/implicit.rs:731-732). */
 typedef struct {
-  int32_t lines_i, lines_j, prefetch_i, prefetch_j, subst_i, subst_j, turb_lines, segment_i, segment_j;
+  int32_t lines_i, lines_j, prefetch_i, prefetch_j, subst_i, subst_j, turb_lines, segment_i, segment_j, residual;
 } bowshock_line_tuning;
 int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out);
 /* Pin the launch shapes instead of the autotuner's (for reproducible runs: the segment lengths change the order of
