@@ -2,8 +2,9 @@
 // mean-flow iteration as in the reference:
 //   k_turb_grad   Green-Gauss gradients of k and omega with the boundary states of the two scalars (turbulence.rs:337-372),
 //                 then F1 and the cross-diffusion X of the cell (turbulence.rs:375-397)
-//   k_turb_cell   face convection / diffusion data of the four faces (turbulence.rs:413-435) and the cell terms: residual,
-//                 diag0 and the coefficients of the i- and j-line systems (turbulence.rs:477-519, 559-579)
+//   k_turb_cell   face convection / diffusion data of the tile's faces, each once in shared memory (turbulence.rs:413-435),
+//                 and the cell terms: residual, diag0 and the coefficients of the i- and j-line systems
+//                 (turbulence.rs:477-519, 559-579)
 //   k_turb_lines  the two scalar tridiagonal line systems, i then j, one thread per (line, scalar) (turbulence.rs:580-581);
 //                 k_turb_lines_w the same with one warp per line (partitioned Thomas), used for lines up to 512 cells
 //   k_turb_update clipped update and the new eddy viscosity (turbulence.rs:584-603)
@@ -165,12 +166,35 @@ __device__ __forceinline__ float strain2(float4 g, float v, float r) {  // turbu
 //   [3c+2] = (up_j k / d0k, up_j w / d0w, d_j k, d_j w); trhs[c] = V R (the i-line right-hand side).
 __global__ void k_turb_cell(Arena A, int slot) {
   __shared__ double sred[TI * TJ / 32];
+  __shared__ TFaceD sFI[TJ][TI + 1];  // the tile's face data, each face once (turbulence.rs:413-435)
+  __shared__ TFaceD sFJ[TJ + 1][TI];
   int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci] || !c.sst) return;
   int lt = t - c.tile_off;
-  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  const int i0 = (lt % c.ntx) * TI, j0 = (lt / c.ntx) * TJ;
+  for (int idx = threadIdx.x; idx < TJ * (TI + 1) + (TJ + 1) * TI; idx += blockDim.x) {
+    SidesD s;
+    if (idx < TJ * (TI + 1)) {
+      const int r = idx / (TI + 1), q = idx % (TI + 1), fi = i0 + q, fj = j0 + r;
+      if (fi > c.ni || fj >= c.nj) continue;
+      if (!((fi < c.ni && !is_solid(c, fi, fj)) || (fi > 0 && !is_solid(c, fi - 1, fj)))) continue;  // no fluid side
+      iface_sides_d(A, c, fi, fj, s);
+      sFI[r][q] = tface_d(A, c, s, ikind(c, fi, s), A.iface[ifidx(c, fi, fj)], A.ifs[ifidx(c, fi, fj)],
+                          A.mflux_i[ifidx(c, fi, fj)] * A.iface[ifidx(c, fi, fj)].w);
+    } else {
+      const int k = idx - TJ * (TI + 1), r = k / TI, q = k % TI, fi = i0 + q, fj = j0 + r;
+      if (fi >= c.ni || fj > c.nj) continue;
+      if (!((fj < c.nj && !is_solid(c, fi, fj)) || (fj > 0 && !is_solid(c, fi, fj - 1)))) continue;
+      jface_sides_d(A, c, fi, fj, s);
+      sFJ[r][q] = tface_d(A, c, s, jkind(c, fj, s), A.jface[jfidx(c, fi, fj)], A.jfs[jfidx(c, fi, fj)],
+                          A.mflux_j[jfidx(c, fi, fj)] * A.jface[jfidx(c, fi, fj)].w);
+    }
+  }
+  __syncthreads();
+  const int q = threadIdx.x % TI, r = threadIdx.x / TI;
+  int i = i0 + q, j = j0 + r;
   double rr = 0.0;
   if (i < c.ni && j < c.nj) {
     long long cc = cidx(c, i, j);
@@ -196,20 +220,7 @@ __global__ void k_turb_cell(Arena A, int slot) {
       float src1 = gamma * rho * prod / fmaxf(mut_c, 1e-30f) - beta * rho * kw.y * kw.y + (1.f - f1) * bl.y;
       float dest0 = BETA_STAR * kw.y, dest1 = 2.f * beta * kw.y;
       // the four faces
-      TFaceD fa[4];
-      {
-        SidesD s;
-        iface_sides_d(A, c, i, j, s);
-        fa[0] = tface_d(A, c, s, ikind(c, i, s), A.iface[ifidx(c, i, j)], A.ifs[ifidx(c, i, j)], A.mflux_i[ifidx(c, i, j)] * A.iface[ifidx(c, i, j)].w);
-        iface_sides_d(A, c, i + 1, j, s);
-        fa[1] = tface_d(A, c, s, ikind(c, i + 1, s), A.iface[ifidx(c, i + 1, j)], A.ifs[ifidx(c, i + 1, j)],
-                        A.mflux_i[ifidx(c, i + 1, j)] * A.iface[ifidx(c, i + 1, j)].w);
-        jface_sides_d(A, c, i, j, s);
-        fa[2] = tface_d(A, c, s, jkind(c, j, s), A.jface[jfidx(c, i, j)], A.jfs[jfidx(c, i, j)], A.mflux_j[jfidx(c, i, j)] * A.jface[jfidx(c, i, j)].w);
-        jface_sides_d(A, c, i, j + 1, s);
-        fa[3] = tface_d(A, c, s, jkind(c, j + 1, s), A.jface[jfidx(c, i, j + 1)], A.jfs[jfidx(c, i, j + 1)],
-                        A.mflux_j[jfidx(c, i, j + 1)] * A.jface[jfidx(c, i, j + 1)].w);
-      }
+      const TFaceD fa[4] = {sFI[r][q], sFI[r][q + 1], sFJ[r][q], sFJ[r + 1][q]};
       bool ends_lo[2] = {i == row_start(c, j), j == col_start(c, i)};
       bool ends_up[2] = {i == c.ni - 1, j == c.nj - 1};
       float rate0 = 0.f, rate1 = 0.f;

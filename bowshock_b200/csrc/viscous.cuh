@@ -219,7 +219,20 @@ __global__ void k_visc_face(Arena A) {
   if (!A.active[ci] || !c.viscous) return;
   int lt = t - c.tile_off;
   int i0 = (lt % c.ntx) * TI, j0 = (lt / c.ntx) * TJ;
-  for (int idx = threadIdx.x; idx < TJ * (TI + 1) + (TJ + 1) * TI; idx += blockDim.x) {
+  // The tile owns its TJ x TI left i faces and TJ x TI lower j faces (two per thread); a tile at the case's right or top
+  // edge also owns the case's last i faces (q = TI) or last j faces (r = TJ), taken last.
+  const int n_own = 2 * TI * TJ;
+  for (int e = threadIdx.x; e < n_own + TJ + TI; e += blockDim.x) {
+    int idx;
+    if (e < TI * TJ) {
+      idx = (e / TI) * (TI + 1) + e % TI;  // i face (r, q < TI)
+    } else if (e < n_own) {
+      idx = TJ * (TI + 1) + (e - TI * TJ);  // j face (r < TJ, q)
+    } else if (e < n_own + TJ) {
+      idx = (e - n_own) * (TI + 1) + TI;  // i face (r, q = TI)
+    } else {
+      idx = TJ * (TI + 1) + TJ * TI + (e - n_own - TJ);  // j face (r = TJ, q)
+    }
     if (idx < TJ * (TI + 1)) {
       int r = idx / (TI + 1), q = idx % (TI + 1);
       int i = i0 + q, j = j0 + r;
