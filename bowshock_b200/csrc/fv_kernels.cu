@@ -402,9 +402,9 @@ struct PcrSlot {  // one reduced row: a, b^-1 (or b), c, d
 
 // Line geometry shared by the factorisation and substitution kernels: warp `gw` solves line L of case c; lane s owns the
 // segment [a, e) of m = max(m_min, ceil(len/32)) cells, the last cell of every segment but the last is a separator.
-// m_min >= 2 (Arena::mmin_i / mmin_j, picked per direction by the autotuner): short lines with a larger m_min have fewer
-// separators, so fewer reduction multipliers to store and read (22.5 KB per line at 31 separators), and longer segments
-// per lane.
+// m_min >= 2 (Arena::mmin_i / mmin_j: 2 unless pinned by bowshock_arena_set_tuning): short lines with a larger m_min
+// have fewer separators, so fewer reduction multipliers to store and read (22.5 KB per line at 31 separators), and longer
+// segments per lane; the rounding of the solve changes with it.
 struct LineSeg {
   int gw, ci, L, n, k0, len, m, P, N, a, e, ke;
   bool act, has_sep;
@@ -453,7 +453,10 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
 
 // Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
 // one thread per cell: the assembly is the arithmetic-heavy part of the operator and has no dependence along the lines.
-__global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
+// MINB blocks per SM bound the registers (3: more warps, some spilled registers; 2: none spilled); the arena's autotuner
+// picks the variant, the results are the same.
+template <int MINB>
+__global__ void __launch_bounds__(TI* TJ, MINB) k_assemble(Arena A) {
   int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];

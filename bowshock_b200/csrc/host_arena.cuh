@@ -751,6 +751,8 @@ struct ArenaHost {
   }
   // residual kernel of the implicit iteration: 0 = 256 threads and 3 blocks per SM, 1 = 288 and 2, 2 = 288 and 3
   int res_variant = 0;
+  // block assembly: 0 = 3 blocks per SM, 1 = 2 blocks per SM
+  int asm_variant = 0;
   void launch_residual(int dt_kind, int slot) {
     switch (res_variant) {
       case 1: k_residual<288, 2><<<LT(), 288, 0, stream>>>(A, dt_kind, slot); break;
@@ -812,8 +814,9 @@ struct ArenaHost {
       L(G_TURB, [&] { k_turb_lines<<<(2 * LI(0) + 127) / 128, 128, 0, st>>>(A, 0); });
     }
   }
-  // Autotuner: per direction, the smallest segment per lane, lines per block and prefetching of the first pass and lines
-  // per block of the substitution passes, lines per block of the SST line kernel, and the residual kernel's variant: each the fastest candidate over
+  // Autotuner: per direction, lines per block and prefetching of the first pass and lines per block of the substitution
+  // passes, lines per block of the SST line kernel, and the residual and assembly kernels'
+  // variants: each the fastest candidate over
   // two timed iterations of this arena's own cases. The state, turbulence and counters are restored afterwards; the choice does not change any
   // result (every warp solves one line alone, with the same arithmetic).
   int autotune() {
@@ -832,45 +835,33 @@ struct ArenaHost {
     }
     BK_CUDA(cudaMemcpy(hit.data(), d_iter, nc * sizeof(int), cudaMemcpyDeviceToHost));
     BK_CUDA(cudaMemcpy(hr.data(), d_ramp, nc * sizeof(int), cudaMemcpyDeviceToHost));
-    const int cand[4] = {1, 2, 4, 8}, cand_m[3] = {2, 4, 8};
-    // timed groups: first pass j / i, substitution j / i, SST lines; per smallest segment m_min (the first pass and the
-    // substitution passes of a direction share it, so it is picked on their sum)
+    // The smallest segment per lane (Arena::mmin_i / mmin_j) keeps its setting (2 unless pinned): a longer one changes the
+    // rounding of the line solves, and on a limit-cycle case of the sweep it moved the window-mean CD by 2e-4.
+    const int cand[4] = {1, 2, 4, 8};
+    // timed groups: first pass j / i, substitution j / i, SST lines
     const int grp[5] = {G_LINES_J, G_LINES_I, G_SUBST_J, G_SUBST_I, G_TURB_LINES};
-    double best[3][5];
-    int pick_w[3][5], pick_pf[3][2];
+    double best[5] = {1e30, 1e30, 1e30, 1e30, 1e30};
+    int pick_w[5] = {LINE_WARPS, LINE_WARPS, LINE_WARPS, LINE_WARPS, TL_WARPS}, pick_pf[2] = {0, 0};
     int rc = 0;
-    for (int mi = 0; mi < 3; ++mi) {
-      A.mmin_i = A.mmin_j = cand_m[mi];
-      for (int q = 0; q < 5; ++q) best[mi][q] = 1e30, pick_w[mi][q] = q < 4 ? LINE_WARPS : TL_WARPS;
-      pick_pf[mi][0] = pick_pf[mi][1] = 0;
-      for (int pf = 0; pf < 2; ++pf)
-        for (int w : cand) {
-          if (pf && w > 4) continue;
-          lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
-          pf_lines[0] = pf_lines[1] = pf;
-          if ((rc = profile(1))) return rc;  // warm-up of this variant
-          if ((rc = profile(2))) return rc;
-          for (int q = 0; q < 5; ++q) {
-            if (q >= 2 && pf) continue;  // only the first pass has the prefetching variant
-            if (q < 2 && w > 4) continue;
-            const double t = prof_ms[grp[q]];
-            if (t < best[mi][q]) {
-              best[mi][q] = t, pick_w[mi][q] = w;
-              if (q < 2) pick_pf[mi][q] = pf;
-            }
+    for (int pf = 0; pf < 2; ++pf)
+      for (int w : cand) {
+        if (pf && w > 4) continue;
+        lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
+        pf_lines[0] = pf_lines[1] = pf;
+        if ((rc = profile(1))) return rc;  // warm-up of this variant
+        if ((rc = profile(2))) return rc;
+        for (int q = 0; q < 5; ++q) {
+          if (q >= 2 && pf) continue;  // only the first pass has the prefetching variant
+          if (q < 2 && w > 4) continue;
+          const double t = prof_ms[grp[q]];
+          if (t < best[q]) {
+            best[q] = t, pick_w[q] = w;
+            if (q < 2) pick_pf[q] = pf;
           }
         }
-    }
-    int mj = 0, mi_ = 0, mt = 0;
-    for (int k = 1; k < 3; ++k) {
-      if (best[k][0] + best[k][2] < best[mj][0] + best[mj][2]) mj = k;
-      if (best[k][1] + best[k][3] < best[mi_][1] + best[mi_][3]) mi_ = k;
-      if (best[k][4] < best[mt][4]) mt = k;
-    }
-    A.mmin_j = cand_m[mj], A.mmin_i = cand_m[mi_];
-    lw_lines[0] = pick_w[mj][0], pf_lines[0] = pick_pf[mj][0], lw_subst[0] = pick_w[mj][2];
-    lw_lines[1] = pick_w[mi_][1], pf_lines[1] = pick_pf[mi_][1], lw_subst[1] = pick_w[mi_][3];
-    lw_turb = pick_w[mt][4];
+      }
+    lw_lines[0] = pick_w[0], lw_lines[1] = pick_w[1], pf_lines[0] = pick_pf[0], pf_lines[1] = pick_pf[1];
+    lw_subst[0] = pick_w[2], lw_subst[1] = pick_w[3], lw_turb = pick_w[4];
     double best_r = 1e30;
     int pick_r = 0;
     for (int v = 0; v < 3; ++v) {
@@ -880,6 +871,15 @@ struct ArenaHost {
       if (prof_ms[G_RESIDUAL] < best_r) best_r = prof_ms[G_RESIDUAL], pick_r = v;
     }
     res_variant = pick_r;
+    double best_a = 1e30;
+    int pick_a = 0;
+    for (int v = 0; v < 2; ++v) {
+      asm_variant = v;
+      if ((rc = profile(1))) return rc;
+      if ((rc = profile(2))) return rc;
+      if (prof_ms[G_ASSEMBLE] < best_a) best_a = prof_ms[G_ASSEMBLE], pick_a = v;
+    }
+    asm_variant = pick_a;
     BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     if (any_sst) {
@@ -912,7 +912,12 @@ struct ArenaHost {
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { launch_residual(2, slot); });
       const int s = sub_iters_of_arena();
-      L(G_ASSEMBLE, [&] { k_assemble<<<LT(), TI * TJ, 0, stream>>>(A); });
+      L(G_ASSEMBLE, [&] {
+        if (asm_variant == 1)
+          k_assemble<2><<<LT(), TI * TJ, 0, stream>>>(A);
+        else
+          k_assemble<3><<<LT(), TI * TJ, 0, stream>>>(A);
+      });
       L(G_ASSEMBLE, [&] { k_line_ends<<<(2 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
