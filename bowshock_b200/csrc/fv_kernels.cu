@@ -452,7 +452,10 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
 }
 
 // Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
-// one thread per cell: the assembly is the arithmetic-heavy part of the operator and has no dependence along the lines.
+// one thread per cell and direction (two blocks per tile): the assembly is the arithmetic-heavy part of the operator and
+// has no dependence along the lines. The direction loop is kept: in this form the compiled arithmetic, and so every
+// result, is bit for bit that of one thread doing both directions (a straight-line form was measured to round
+// differently).
 // MINB blocks per SM bound the registers (3: more warps, some spilled registers; 2: none spilled); the arena's autotuner
 // picks the variant, the results are the same.
 template <int MINB>
@@ -467,6 +470,7 @@ __global__ void __launch_bounds__(TI* TJ, MINB) k_assemble(Arena A) {
   const long long cc = cidx(c, i, j);
 #pragma unroll 1
   for (int dir = 0; dir < 2; ++dir) {
+    if (dir != (int)blockIdx.y) continue;  // blockIdx.y: the direction of this block (0 = i lines, 1 = j lines)
     M4<float> lo, d, up;
     assemble(A, c, dir == 0, i, j, lo, d, up);
     Rec rec = line_rec(A, dir == 0, cc);

@@ -914,9 +914,9 @@ struct ArenaHost {
       const int s = sub_iters_of_arena();
       L(G_ASSEMBLE, [&] {
         if (asm_variant == 1)
-          k_assemble<2><<<LT(), TI * TJ, 0, stream>>>(A);
+          k_assemble<2><<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
         else
-          k_assemble<3><<<LT(), TI * TJ, 0, stream>>>(A);
+          k_assemble<3><<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
       });
       L(G_ASSEMBLE, [&] { k_line_ends<<<(8 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
