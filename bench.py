@@ -181,7 +181,7 @@ class OracleSample:
 
 def cd_error(ours, oracle):
     """CD error of a case against the oracle: the final total CD; for a run that both stopped on a limit cycle (mean
-    stationary), the mean CD over the two windows the rule compared, since the instantaneous CD depends on the phase."""
+    stationary), the mean CD over the last window the rule compared, since the instantaneous CD depends on the phase."""
     if ours["stop_reason"] == "mean stationary" and oracle["stop"] == "mean stationary" and "cd_window" in oracle:
         return ours["cd_window"] - oracle["cd_window"]
     return ours["cd_total"] - oracle["cd_total"]

@@ -210,8 +210,10 @@ inline void fill_point(const CaseRun& cr, const Forces& f, bowshock_point_result
   o->forces.cd_total = f.cd_total(cr.nseg);
   o->last_monitor = cr.last_monitor;
   o->cd_window = o->forces.cd_total;
-  if (cr.reason == 4 && cr.p.mean_window >= SYNC) {  // mean stationary: the two windows mean_stationary compared
-    size_t k = 2 * (size_t)(cr.p.mean_window / SYNC);
+  // mean stationary: the mean of the last window the rule compared (run.rs:157-172); its 120 samples lie on the
+  // limit cycle, so the value does not depend on the 50-iteration chunk at which the rule first holds
+  if (cr.reason == 4 && cr.p.mean_window >= SYNC) {
+    size_t k = (size_t)(cr.p.mean_window / SYNC);
     if (cr.hist.size() >= k) {
       double m = 0.0;
       for (size_t t = cr.hist.size() - k; t < cr.hist.size(); ++t) m += cr.hist[t].second;

@@ -215,8 +215,9 @@ typedef struct {
   int32_t stop_reason;
   bowshock_forces forces;
   double last_monitor;
-  /* a run stopped on a limit cycle (mean stationary): the mean of the monitored CD over the two windows the rule compared;
-   * otherwise the final total CD. Not in the reference: the instantaneous CD of a limit cycle depends on the phase. */
+  /* a run stopped on a limit cycle (mean stationary): the mean of the monitored CD over the last window the rule compared
+   * (6,000 iterations on the cycle); otherwise the final total CD. Not in the reference: the instantaneous CD of a limit
+   * cycle depends on the phase, and a mean that reaches back to the start-up transient on the chunk the rule holds. */
   double cd_window;
 } bowshock_point_result;
 

@@ -87,7 +87,7 @@ typedef struct {
   int stop_reason;
   double cd_nose, cd_nose_cell, cd_aft[8], cd_base, cd_friction, cd_total, cp_base, cp_base_cell, y_plus_max, farfield_dp, min_rho, min_p,
       m_max, m_wall_max;
-  double cd_window;  // mean stationary: mean monitored CD over the two compared windows; otherwise cd_total
+  double cd_window;  // mean stationary: mean monitored CD over the last compared window; otherwise cd_total
 } OrcPointResult;
 
 }  // extern "C"
@@ -705,7 +705,7 @@ int orc_run_on(const OrcCase* c, void* h, int warm, double r_ref, OrcPointResult
   PointResult p = run_on(cc, *s, warm != 0, r_ref >= 0 ? &r_ref : nullptr);
   fill_result(p, out);
   out->cd_window = p.cd_total;
-  size_t k = 2 * (cc.numerics.mean_window / MONITOR_EVERY);
+  size_t k = cc.numerics.mean_window / MONITOR_EVERY;
   if (p.stop_reason == STOP_MEAN_STATIONARY && k > 0 && p.monitor_history.size() >= k) {
     double m = 0.0;
     for (size_t t = p.monitor_history.size() - k; t < p.monitor_history.size(); ++t) m += p.monitor_history[t].second;
