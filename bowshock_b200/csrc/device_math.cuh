@@ -463,37 +463,6 @@ BK_HD M4<double> ghost_jacobian(int bc, const V4<double>& fs, const V4<double>& 
   return t;
 }
 
-// Column q of ghost_jacobian (the same arithmetic: every column is its own finite difference).
-BK_HD V4<double> ghost_jacobian_col(int bc, const V4<double>& fs, const V4<double>& edge, double nx, double nr, double outward,
-                                    int q) {
-  V4<double> col = mk4<double>(0, 0, 0, 0);
-  if (bc == BC_FREESTREAM) return col;
-  if (bc == BC_EXTRAPOLATE || bc == BC_SLIPWALL) {
-    const M4<double> t = bc == BC_EXTRAPOLATE ? eye4<double>() : reflection<double>(nx, nr);
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (k == q) col[r] = t[4 * r + k];
-    return col;
-  }
-  V4<double> u0 = prim_to_cons(edge);
-  V4<double> g0 = prim_to_cons(ghost_state<double>(bc, fs, edge, edge, nx, nr, outward));
-  double h = 0.0;
-  V4<double> up = u0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (k == q) {
-      h = 1e-7 * (1.0 + fabs(u0[k]));
-      up[k] += h;
-    }
-  V4<double> e = cons_to_prim(up);
-  V4<double> g = prim_to_cons(ghost_state<double>(bc, fs, e, e, nx, nr, outward));
-#pragma unroll
-  for (int r = 0; r < 4; ++r) col[r] = (g[r] - g0[r]) / h;
-  return col;
-}
-
 // Blocks (lo, d, up) of I - dt J for one cell (implicit.rs:284-367).
 template <typename T>
 BK_HD void cell_blocks(const V4<T>& wk, const V4<T>& wm, const V4<T>& wp, T fl_nx, T fl_nr, T fl_w, T fr_nx, T fr_nr, T fr_w, T vol, T dt,

@@ -482,71 +482,66 @@ __global__ void __launch_bounds__(TI* TJ, MINB) k_assemble(Arena A) {
 
 // Ghost Jacobians of the two ends of line `L` folded into the diagonal blocks (implicit.rs:440-467): at the first cell
 // d += lo T and lo = 0, with T the wall reflection / no-slip, the jet's zero, or the far-field ghost Jacobian (FP64 finite
-// differences); at the last cell d += up T and up = 0. Column q of T gives column q of the product, so one thread per
-// (line end, column): the four finite differences of a far-field end run in parallel. `first` / `last` select the ends
-// (a line of one cell folds both, first then last, in one thread per column).
-__device__ void fold_line_end_col(const Arena& A, const CaseDev& c, bool dir_i, int L, bool first, bool last, int q) {
+// differences); at the last cell d += up T and up = 0. One thread per line end (`ends` bit 0: first, bit 1: last; a line
+// of one cell has both ends in one thread), after k_assemble.
+__device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int L, int ends) {
   const int n = dir_i ? c.ni : c.nj;
   const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
   if (k0 >= n) return;
-  auto fold = [&](int i, int j, int blk, const V4<float>& t) {  // d[., q] += (B T)[., q], B[., q] = 0
-    Rec rec = line_rec(A, dir_i, cidx(c, i, j));
-    const M4<float> B = ld_m4(rec.blk(blk));
-    float* dp = reinterpret_cast<float*>(rec.blk(F_D));
-    float* bp = reinterpret_cast<float*>(rec.blk(blk));
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      dp[4 * r + q] += 1.f * (B[4 * r] * t[0] + B[4 * r + 1] * t[1] + B[4 * r + 2] * t[2] + B[4 * r + 3] * t[3]);
-      bp[4 * r + q] = 0.f;
-    }
-  };
-  auto col_of = [&](const M4<float>& m) {
-    V4<float> t = mk4<float>(0, 0, 0, 0);
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (k == q) t[r] = m[4 * r + k];
-    return t;
-  };
-  auto col_fd = [&](int bc, int i, int j, float nx, float nr, double outward) {
-    V4<double> td = ghost_jacobian_col(bc, fs_of(c), cvt4<double>(Wat(A, c, i, j)), nx, nr, outward, q);
-    return mk4<float>((float)td[0], (float)td[1], (float)td[2], (float)td[3]);
-  };
-  if (first) {
+  if (ends & 1) {
     const int i = dir_i ? k0 : L, j = dir_i ? L : k0;
+    const long long cc = cidx(c, i, j);
     float4 fl = dir_i ? A.iface[ifidx(c, i, j)] : A.jface[jfidx(c, i, j)];
     bool wall_lower = k0 > 0;
     bool jet = wall_lower && dir_i && jet_iface(c, k0, j);
-    V4<float> t;
+    M4<float> T;
     if (jet) {
-      t = mk4<float>(0, 0, 0, 0);
+      T = zero4<float>();
     } else if (wall_lower) {
       bool ns = dir_i ? noslip_iface(c, k0, j) : noslip_jface(c, i, k0);
-      t = col_of(ns ? noslip4<float>() : reflection<float>(fl.x, fl.y));
+      T = ns ? noslip4<float>() : reflection<float>(fl.x, fl.y);
     } else if (!c.implicit_bc) {
-      t = mk4<float>(0, 0, 0, 0);
+      T = zero4<float>();
     } else {
       int bc = dir_i ? c.bc[0] : c.bc[2];
-      if (!dir_i && noslip_jface(c, i, 0) && bc == BC_SLIPWALL)
-        t = col_of(noslip4<float>());
-      else
-        t = col_fd(bc, i, j, fl.x, fl.y, -1.0);
+      if (!dir_i && noslip_jface(c, i, 0) && bc == BC_SLIPWALL) {
+        T = noslip4<float>();
+      } else {
+        M4<double> Td = ghost_jacobian(bc, fs_of(c), cvt4<double>(Wat(A, c, i, j)), fl.x, fl.y, -1.0);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
+      }
     }
-    fold(i, j, F_LO, t);
+    Rec rec = line_rec(A, dir_i, cc);
+    M4<float> d = ld_m4(rec.blk(F_D));
+    axpy(d, 1.f, mm(ld_m4(rec.blk(F_LO)), T));
+    st_m4(rec.blk(F_LO), zero4<float>());
+    st_m4(rec.blk(F_D), d);
   }
-  if (last) {
+  if (ends & 2) {
     const int i = dir_i ? n - 1 : L, j = dir_i ? L : n - 1;
+    const long long cc = cidx(c, i, j);
     float4 fr = dir_i ? A.iface[ifidx(c, i + 1, j)] : A.jface[jfidx(c, i, j + 1)];
-    const V4<float> t = c.implicit_bc ? col_fd(dir_i ? c.bc[1] : c.bc[3], i, j, fr.x, fr.y, 1.0) : mk4<float>(0, 0, 0, 0);
-    fold(i, j, F_UP, t);
+    M4<float> T;
+    if (!c.implicit_bc) {
+      T = zero4<float>();
+    } else {
+      M4<double> Td = ghost_jacobian(dir_i ? c.bc[1] : c.bc[3], fs_of(c), cvt4<double>(Wat(A, c, i, j)), fr.x, fr.y, 1.0);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
+    }
+    Rec rec = line_rec(A, dir_i, cc);
+    M4<float> d = ld_m4(rec.blk(F_D));
+    axpy(d, 1.f, mm(ld_m4(rec.blk(F_UP)), T));
+    st_m4(rec.blk(F_UP), zero4<float>());
+    st_m4(rec.blk(F_D), d);
   }
 }
 
-// eight threads per line (first end, last end) x (column): every i line, then every j line, of the active cases
+// two threads per line (first end, last end): every i line, then every j line, of the active cases
 __global__ void k_line_ends(Arena A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int q = t & 3, e = (t >> 2) & 1, l = t >> 3;
+  const int e = t & 1, l = t >> 1;
   const int nli = lines_of(A, true);
   const bool dir_i = l < nli;
   const int gw = line_at(A, dir_i, dir_i ? l : l - nli);
@@ -557,11 +552,11 @@ __global__ void k_line_ends(Arena A) {
   const int L = gw - (dir_i ? c.iline_off : c.jline_off);
   const int n = dir_i ? c.ni : c.nj;
   const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
-  if (n - k0 == 1) {  // one cell: both folds of a column in one thread (they update the same diagonal block)
-    if (e == 0) fold_line_end_col(A, c, dir_i, L, true, true, q);
+  if (n - k0 == 1) {  // one cell: both ends in the first thread (the two folds update the same diagonal block)
+    if (e == 0) fold_line_ends(A, c, dir_i, L, 3);
     return;
   }
-  fold_line_end_col(A, c, dir_i, L, e == 0, e == 1, q);
+  fold_line_ends(A, c, dir_i, L, e ? 2 : 1);
 }
 
 // First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble and k_line_ends left in the line records, factorise

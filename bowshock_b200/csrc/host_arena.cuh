@@ -918,7 +918,7 @@ struct ArenaHost {
         else
           k_assemble<3><<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
       });
-      L(G_ASSEMBLE, [&] { k_line_ends<<<(8 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
+      L(G_ASSEMBLE, [&] { k_line_ends<<<(2 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
