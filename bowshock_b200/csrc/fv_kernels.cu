@@ -746,8 +746,9 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
 #pragma unroll
         for (int q = 0; q < 4; ++q) nd[q] += t[q];
       }
-      st_m4(prec + 8 * lvl, al);
-      st_m4(prec + 8 * lvl + 4, ga);
+      // only the multipliers the substitution passes read (they skip the same out-of-range neighbours)
+      if (s - h >= 0) st_m4(prec + 8 * lvl, al);
+      if (s + h < N) st_m4(prec + 8 * lvl + 4, ga);
       ra = na;
       rb = nb;
       rc = nc;
