@@ -123,7 +123,8 @@ __device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(
 // dt_kind: 0 = keep dt, 1 = explicit local time step (solver.rs:614-643), 2 = implicit pseudo-time step (implicit.rs:666-695)
 // NT threads per block (>= TI * TJ; the first TI * TJ also own a cell each): the tile's TJ (TI + 1) + (TJ + 1) TI = 552 face
 // fluxes are spread over all NT, so with NT = 288 no thread computes more than two of them (three with 256); MINB blocks
-// per SM bound the registers. The arena's autotuner picks the variant of the implicit iteration; the results are the same.
+// per SM bound the registers. The arena's autotuner picks NT for the implicit iteration, with MINB = 3: the two compile to
+// the same arithmetic (checked bit for bit), whereas MINB = 2 rounds differently.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int slot) {
   __shared__ float4 sW[TJ + 4][TI + 4], sWl[TJ + 4][TI + 4];
@@ -453,13 +454,11 @@ __device__ __forceinline__ void line_emit(const Arena& A, int epilogue, bool upd
 
 // Blocks (lo, d, up) of I - dt J_i and I - dt J_j of every fluid cell into its two line records (implicit.rs:379-467),
 // one thread per cell and direction (two blocks per tile): the assembly is the arithmetic-heavy part of the operator and
-// has no dependence along the lines. The direction loop is kept: in this form the compiled arithmetic, and so every
-// result, is bit for bit that of one thread doing both directions (a straight-line form was measured to round
-// differently).
-// MINB blocks per SM bound the registers (3: more warps, some spilled registers; 2: none spilled); the arena's autotuner
-// picks the variant, the results are the same.
-template <int MINB>
-__global__ void __launch_bounds__(TI* TJ, MINB) k_assemble(Arena A) {
+// has no dependence along the lines. The direction loop and the register budget (3 blocks per SM) are kept: in this
+// form the compiled arithmetic, and so every result, is bit for bit that of one thread doing both directions; a
+// straight-line form and a budget of 2 blocks per SM were measured to round differently (ptxas contracts multiply-adds
+// by register budget).
+__global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
   int t = tile_at(A);
   int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];

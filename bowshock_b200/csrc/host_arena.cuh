@@ -749,16 +749,14 @@ struct ArenaHost {
     prof_ms[g] += ms;
     prof_launches[g] += 1;
   }
-  // residual kernel of the implicit iteration: 0 = 256 threads and 3 blocks per SM, 1 = 288 and 2, 2 = 288 and 3
+  // residual kernel of the implicit iteration: 0 = 256 threads, 1 = 288 threads (3 blocks per SM both: the variants
+  // compile to the same arithmetic, checked bit for bit; a register budget of 2 blocks per SM did not, see autotune)
   int res_variant = 0;
-  // block assembly: 0 = 3 blocks per SM, 1 = 2 blocks per SM
-  int asm_variant = 0;
   void launch_residual(int dt_kind, int slot) {
-    switch (res_variant) {
-      case 1: k_residual<288, 2><<<LT(), 288, 0, stream>>>(A, dt_kind, slot); break;
-      case 2: k_residual<288, 3><<<LT(), 288, 0, stream>>>(A, dt_kind, slot); break;
-      default: k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, dt_kind, slot); break;
-    }
+    if (res_variant == 1)
+      k_residual<288, 3><<<LT(), 288, 0, stream>>>(A, dt_kind, slot);
+    else
+      k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, dt_kind, slot);
   }
   // Launch shapes of the line kernels, picked by autotune() per direction ([0] = j lines, [1] = i lines): lines per
   // block (1, 2, 4, or 8 except for the first pass, whose shared memory holds 4 lines at most) and, for the first pass,
@@ -815,8 +813,9 @@ struct ArenaHost {
     }
   }
   // Autotuner: per direction, lines per block and prefetching of the first pass and lines per block of the substitution
-  // passes, lines per block of the SST line kernel, and the residual and assembly kernels'
-  // variants: each the fastest candidate over
+  // passes, lines per block of the SST line kernel, and the residual kernel's variant; only variants that compile to the
+  // same arithmetic are candidates (ptxas contracts multiply-adds differently under different register budgets, so a
+  // launch-bounds variant can round differently; every candidate here was checked bit for bit): each the fastest candidate over
   // two timed iterations of this arena's own cases. The state, turbulence and counters are restored afterwards; the choice does not change any
   // result (every warp solves one line alone, with the same arithmetic).
   int autotune() {
@@ -864,22 +863,14 @@ struct ArenaHost {
     lw_subst[0] = pick_w[2], lw_subst[1] = pick_w[3], lw_turb = pick_w[4];
     double best_r = 1e30;
     int pick_r = 0;
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < 2; ++v) {
       res_variant = v;
       if ((rc = profile(1))) return rc;
       if ((rc = profile(2))) return rc;
       if (prof_ms[G_RESIDUAL] < best_r) best_r = prof_ms[G_RESIDUAL], pick_r = v;
     }
     res_variant = pick_r;
-    double best_a = 1e30;
-    int pick_a = 0;
-    for (int v = 0; v < 2; ++v) {
-      asm_variant = v;
-      if ((rc = profile(1))) return rc;
-      if ((rc = profile(2))) return rc;
-      if (prof_ms[G_ASSEMBLE] < best_a) best_a = prof_ms[G_ASSEMBLE], pick_a = v;
-    }
-    asm_variant = pick_a;
+
     BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     if (any_sst) {
@@ -913,10 +904,7 @@ struct ArenaHost {
       L(G_RESIDUAL, [&] { launch_residual(2, slot); });
       const int s = sub_iters_of_arena();
       L(G_ASSEMBLE, [&] {
-        if (asm_variant == 1)
-          k_assemble<2><<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
-        else
-          k_assemble<3><<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
+        k_assemble<<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
       });
       L(G_ASSEMBLE, [&] { k_line_ends<<<(2 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
