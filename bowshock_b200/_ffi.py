@@ -147,6 +147,7 @@ SIGNATURES = {
     "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
     "bowshock_arena_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_arena_set_tuning": (_I, [_P, C.POINTER(LineTuning)]),
+    "bowshock_arena_prepare": (_I, [_P, _U]),
     "bowshock_solver_run_noalloc": (_I, [_P, _U, _dp]),
 }
 

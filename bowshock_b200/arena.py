@@ -53,6 +53,10 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_run(self._h, int(n), _ffi.dptr(out)))
         return out.reshape(n, self.ncases)
 
+    def prepare(self, n: int):
+        """Build the CUDA graph run(n) launches first, without running it."""
+        self._check(_ffi.load().bowshock_arena_prepare(self._h, int(n)))
+
     def ms_per_iter(self) -> float:
         d = C.c_double()
         self._check(_ffi.load().bowshock_arena_last_ms_per_iter(self._h, C.byref(d)))

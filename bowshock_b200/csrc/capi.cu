@@ -709,6 +709,11 @@ int bowshock_arena_run(bowshock_arena* a, uint64_t n, double* residual) {
   return afrom(a, a->ar.run((long long)n, residual));
 }
 
+int bowshock_arena_prepare(bowshock_arena* a, uint64_t n) {
+  if (!a) return BOWSHOCK_INVALID;
+  return afrom(a, a->ar.prepare((long long)n));
+}
+
 int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bowshock_progress_fn progress, void* user) {
   if (!a || !results) return BOWSHOCK_INVALID;
   const int nc = (int)a->ar.cases.size();

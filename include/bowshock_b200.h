@@ -276,6 +276,11 @@ const char* bowshock_arena_last_error(const bowshock_arena* a);
 int bowshock_arena_cells(const bowshock_arena* a, uint64_t* ncells);
 /* n iterations of every active case; residual (n x ncases, iteration-major) may be NULL */
 int bowshock_arena_run(bowshock_arena* a, uint64_t n, double* residual);
+/* Capture and instantiate the CUDA graph that bowshock_arena_run(a, n, ...) launches first (a chunk of min(n, 256)
+ * iterations), without running anything: a following run of n iterations then spends no host time on graph
+ * construction (the graph is rebuilt after a change of the active cases or the launch shapes). No counterpart in the
+ * reference. */
+int bowshock_arena_prepare(bowshock_arena* a, uint64_t n);
 /* cold-start every case and iterate each to its stop rule, masking converged cases out; results per case */
 int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bowshock_progress_fn progress, void* user);
 /* FP64 forces of every case's current state (ncases entries) */
