@@ -261,6 +261,7 @@ struct ArenaHost {
   std::vector<double> h_rsum;
   cudaGraphExec_t graph = nullptr;
   int graph_len = 0;
+  bool graph_dirty = false;  // `graph` is stale but has the topology of the next capture
   std::vector<int> h_active;
 
   ~ArenaHost() { release(); }
@@ -683,7 +684,7 @@ struct ArenaHost {
     A.iline_list = want ? d_illist : nullptr;
     A.jline_list = want ? d_jllist : nullptr;
     A.n_tl = (int)tl.size(), A.n_pb = (int)pb.size(), A.n_il = (int)il.size(), A.n_jl = (int)jl.size();
-    if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    graph_dirty = true;  // same kernels, new grids and lists: the next capture updates the instantiated graph
     return 0;
   }
 
@@ -963,8 +964,7 @@ struct ArenaHost {
   // The CUDA graph of a chunk of `chunk` iterations, captured and instantiated unless it is the one already held.
   int capture_chunk(int chunk) {
     const int nc = (int)cases.size();
-    if (!graph || graph_len != chunk) {
-      if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    if (!graph || graph_len != chunk || graph_dirty) {
       cudaGraph_t g;
       BK_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream);
@@ -977,6 +977,17 @@ struct ArenaHost {
         err = std::string("launch during capture: ") + cudaGetErrorString(le);
         return 3;
       }
+      if (graph && graph_len == chunk) {  // a change of the active cases: update the instantiated graph in place
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(graph, g, &info) == cudaSuccess) {
+          cudaGraphDestroy(g);
+          graph_dirty = false;
+          return 0;
+        }
+        cudaGetLastError();  // the update was refused: instantiate anew
+      }
+      if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+      graph_dirty = false;
       cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
       cudaGraphDestroy(g);
       if (ie != cudaSuccess) {
