@@ -739,31 +739,51 @@ __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float
   line3(B, dir, L, c0, stride, n, r0, rs);
   float* R = rec3(B, b, dir) + r0;
   const long long nc = B.nc;
+  // both walks load the next cell's factors before the arithmetic of the current one (software pipelining)
   V5<float> g{{0, 0, 0, 0, 0}};
+  M5<float> lo_n = ld5(R + R_LO * nc, nc), mi_n = ld5(R + R_MINV * nc, nc);
+  V5<float> r_n = ldU(B, in, b, c0);
   for (int m = 0; m < n; ++m) {
-    long long c = c0 + m * stride, rr = m * rs;
-    V5<float> r = ldU(B, in, b, c);
+    const long long rr = m * rs;
+    const M5<float> lo = lo_n, mi = mi_n;
+    V5<float> r = r_n;
+    if (m + 1 < n) {
+      const long long rn = (m + 1) * rs;
+      lo_n = ld5(R + R_LO * nc + rn, nc), mi_n = ld5(R + R_MINV * nc + rn, nc);
+      r_n = ldU(B, in, b, c0 + (m + 1) * stride);
+    }
     if (m > 0) {
-      V5<float> t = mv5(ld5(R + R_LO * nc + rr, nc), g);
+      V5<float> t = mv5(lo, g);
 #pragma unroll
       for (int q = 0; q < 5; ++q) r[q] -= t[q];
     }
-    g = mv5(ld5(R + R_MINV * nc + rr, nc), r);
+    g = mv5(mi, r);
 #pragma unroll
     for (int q = 0; q < 5; ++q) R[(R_G + q) * nc + rr] = g[q];
   }
   V5<float> xn = g;
   emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
-  for (int m = n - 2; m >= 0; --m) {
-    long long c = c0 + m * stride, rr = m * rs;
-    V5<float> gm;
+  if (n >= 2) {
+    M5<float> y_n = ld5(R + R_Y * nc + (n - 2) * rs, nc);
+    V5<float> g_n;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) gm[q] = R[(R_G + q) * nc + rr];
-    V5<float> t = mv5(ld5(R + R_Y * nc + rr, nc), xn);
+    for (int q = 0; q < 5; ++q) g_n[q] = R[(R_G + q) * nc + (n - 2) * rs];
+    for (int m = n - 2; m >= 0; --m) {
+      const long long c = c0 + m * stride;
+      const M5<float> ym = y_n;
+      V5<float> gm = g_n;
+      if (m > 0) {
+        const long long rn = (m - 1) * rs;
+        y_n = ld5(R + R_Y * nc + rn, nc);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) gm[q] -= t[q];
-    emit3(B, b, epilogue, update, out, c, gm);
-    xn = gm;
+        for (int q = 0; q < 5; ++q) g_n[q] = R[(R_G + q) * nc + rn];
+      }
+      V5<float> t = mv5(ym, xn);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) gm[q] -= t[q];
+      emit3(B, b, epilogue, update, out, c, gm);
+      xn = gm;
+    }
   }
   if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
 }
