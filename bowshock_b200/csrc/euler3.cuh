@@ -614,7 +614,7 @@ __device__ __forceinline__ void st5(float* p, long long stride, const M5<float>&
 
 // Blocks of every cell into the line records (thread per cell). part 0: the i direction, threads ordered j fastest so that
 // the transposed i records are written side by side; part 1: the j and k directions, threads ordered i fastest.
-__global__ void __launch_bounds__(128) k3_assemble(B3 B, int part) {
+__global__ void __launch_bounds__(128, 4) k3_assemble(B3 B, int part) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b = blockIdx.y;
   if (t >= B.nc || !B.active[b]) return;
