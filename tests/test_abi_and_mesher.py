@@ -68,3 +68,25 @@ def test_rans_params_match_the_oracle_atmosphere():
         a, b = isa(h), o.isa(h)
         for k in a:
             assert abs(a[k] - b[k]) <= 1e-12 * abs(b[k])
+
+
+def test_line_tuning_struct_matches_the_header():
+    """The ctypes mirror of bowshock_line_tuning has the header's fields, in the header's order."""
+    from bowshock_b200 import _ffi
+    hdr = open(os.path.join(ROOT, "include", "bowshock_b200.h")).read()
+    m = re.search(r"typedef struct \{\s*int32_t ([^;]*);\s*\} bowshock_line_tuning;", hdr)
+    assert m, "bowshock_line_tuning not found in the header"
+    names = [n.strip() for n in m.group(1).replace("\n", " ").split(",")]
+    assert names == [n for n, _ in _ffi.LineTuning._fields_]
+
+
+def test_limit_cycle_cd_comparison():
+    """bench.py compares a case that both sides stopped on a limit cycle by the mean of the last compared window, any
+    other case by its final total CD."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    ours = dict(stop_reason="mean stationary", cd_window=0.3200, cd_total=0.3210)
+    assert abs(bench.cd_error(ours, dict(stop="mean stationary", cd_window=0.3199, cd_total=0.3190)) - 1e-4) < 1e-12
+    assert abs(bench.cd_error(ours, dict(stop="CD stationary", cd_window=0.3199, cd_total=0.3190)) - 2e-3) < 1e-12
