@@ -818,7 +818,10 @@ __device__ __forceinline__ V4<float> shfl_down4(const V4<float>& v, int h) {
 // Defect-correction pass `pass` >= 1 (implicit.rs:622-639) of every case with more than `pass` passes: the same solve
 // with the factors of the first pass. Per cell: g = M^-1 (r - lo g_prev) forward, the separators' right-hand sides, the
 // reduction of the right-hand side alone with the kept multipliers (warp shuffles), x = g + GE l_left - Y x_next backward.
-template <int W>  // lines (warps) per block, chosen by the arena's autotuner
+// W: lines (warps) per block; PF: the walks load the next cell's record before the arithmetic of the current one (more
+// loads in flight per warp, ~60 more registers, so fewer warps per SM). The arena's autotuner picks both per direction;
+// the arithmetic is the same.
+template <int W, bool PF>
 __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, const float4* in, float4* out, int pass) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * W + warp;
@@ -832,19 +835,24 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
   const int L = G.L, N = G.N, a = G.a, e = G.e, ke = G.ke;
   const int s = lane;
   auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
-  // the loops load the next cell's record before the dependent arithmetic of the current one (software pipelining);
   // the forward sweep also sums the first interior cell's value v_f = sum_k T_k g_k with the kept weights
   V4<float> g = mk4<float>(0, 0, 0, 0), v_f = mk4<float>(0, 0, 0, 0);
   if (G.act) {
     long long cc = cell(a);
     Rec rec = line_rec(A, dir_i != 0, cc);
-    M4<float> Lo = ld_m4(rec.blk(F_LO)), Mi = ld_m4(rec.blk(F_MINV)), Tk = ld_m4(rec.blk(F_T));
-    float4 rin = in[cc];
+    M4<float> Lo, Mi, Tk;
+    float4 rin;
+    if (PF) Lo = ld_m4(rec.blk(F_LO)), Mi = ld_m4(rec.blk(F_MINV)), Tk = ld_m4(rec.blk(F_T)), rin = in[cc];
     for (int k = a; k <= ke; ++k) {
+      if (!PF) {
+        cc = cell(k);
+        rec = line_rec(A, dir_i != 0, cc);
+        Lo = ld_m4(rec.blk(F_LO)), Mi = ld_m4(rec.blk(F_MINV)), Tk = ld_m4(rec.blk(F_T)), rin = in[cc];
+      }
       M4<float> Lo_n = Lo, Mi_n = Mi, T_n = Tk;
       float4 rin_n = rin;
       Rec rec_n = rec;
-      if (k < ke) {
+      if (PF && k < ke) {
         long long cn = cell(k + 1);
         rec_n = line_rec(A, dir_i != 0, cn);
         Lo_n = ld_m4(rec_n.blk(F_LO)), Mi_n = ld_m4(rec_n.blk(F_MINV)), T_n = ld_m4(rec_n.blk(F_T));
@@ -904,13 +912,19 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
   {
     long long cc = cell(ke);
     Rec rec = line_rec(A, dir_i != 0, cc);
-    M4<float> GEk = ld_m4(rec.blk(F_GE)), Yk = ld_m4(rec.blk(F_Y));
-    float4 gk4 = *rec.g();
+    M4<float> GEk, Yk;
+    float4 gk4;
+    if (PF) GEk = ld_m4(rec.blk(F_GE)), Yk = ld_m4(rec.blk(F_Y)), gk4 = *rec.g();
     for (int k = ke; k >= a; --k) {
+      if (!PF) {
+        cc = cell(k);
+        rec = line_rec(A, dir_i != 0, cc);
+        GEk = ld_m4(rec.blk(F_GE)), Yk = ld_m4(rec.blk(F_Y)), gk4 = *rec.g();
+      }
       M4<float> GE_n = GEk, Y_n = Yk;
       float4 g_n = gk4;
       long long cn = cc;
-      if (k > a) {
+      if (PF && k > a) {
         cn = cell(k - 1);
         Rec rn = line_rec(A, dir_i != 0, cn);
         GE_n = ld_m4(rn.blk(F_GE)), Y_n = ld_m4(rn.blk(F_Y)), g_n = *rn.g();

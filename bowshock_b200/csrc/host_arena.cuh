@@ -763,6 +763,7 @@ struct ArenaHost {
   // block (1, 2, 4, or 8 except for the first pass, whose shared memory holds 4 lines at most) and, for the first pass,
   // whether the walks prefetch the next cell's record.
   int lw_lines[2] = {LINE_WARPS, LINE_WARPS}, pf_lines[2] = {0, 0}, lw_subst[2] = {LINE_WARPS, LINE_WARPS}, lw_turb = TL_WARPS;
+  int pf_subst[2] = {0, 0};  // whether the substitution walks prefetch the next cell's record
   template <bool PF>
   void launch_lines_pf(int dir_i, int w, const float4* in, int from_res, float4* out) {
     const int nl = LI(dir_i);
@@ -780,15 +781,23 @@ struct ArenaHost {
     else
       launch_lines_pf<false>(dir_i, w, in, from_res, out);
   }
-  void launch_subst(int dir_i, const float4* in, float4* out, int pass) {
-    const int nl = LI(dir_i), w = lw_subst[dir_i ? 1 : 0];
+  template <bool PF>
+  void launch_subst_pf(int dir_i, int w, const float4* in, float4* out, int pass) {
+    const int nl = LI(dir_i);
     const int nb = (nl + w - 1) / w;
     switch (w) {
-      case 1: k_lines_subst<1><<<nb, 32, 0, stream>>>(A, dir_i, in, out, pass); break;
-      case 2: k_lines_subst<2><<<nb, 64, 0, stream>>>(A, dir_i, in, out, pass); break;
-      case 8: k_lines_subst<8><<<nb, 256, 0, stream>>>(A, dir_i, in, out, pass); break;
-      default: k_lines_subst<4><<<nb, 128, 0, stream>>>(A, dir_i, in, out, pass); break;
+      case 1: k_lines_subst<1, PF><<<nb, 32, 0, stream>>>(A, dir_i, in, out, pass); break;
+      case 2: k_lines_subst<2, PF><<<nb, 64, 0, stream>>>(A, dir_i, in, out, pass); break;
+      case 8: k_lines_subst<8, PF><<<nb, 256, 0, stream>>>(A, dir_i, in, out, pass); break;
+      default: k_lines_subst<4, PF><<<nb, 128, 0, stream>>>(A, dir_i, in, out, pass); break;
     }
+  }
+  void launch_subst(int dir_i, const float4* in, float4* out, int pass) {
+    const int d = dir_i ? 1 : 0;
+    if (pf_subst[d])
+      launch_subst_pf<true>(dir_i, lw_subst[d], in, out, pass);
+    else
+      launch_subst_pf<false>(dir_i, lw_subst[d], in, out, pass);
   }
   void launch_turb_lines(int dir_i, cudaStream_t st) {
     const int nl = LI(dir_i), w = lw_turb;
@@ -813,8 +822,7 @@ struct ArenaHost {
       L(G_TURB, [&] { k_turb_lines<<<(2 * LI(0) + 127) / 128, 128, 0, st>>>(A, 0); });
     }
   }
-  // Autotuner: per direction, lines per block and prefetching of the first pass and lines per block of the substitution
-  // passes, lines per block of the SST line kernel, and the residual kernel's variant; only variants that compile to the
+  // Autotuner: per direction, lines per block and prefetching of the first pass and of the substitution passes, lines per block of the SST line kernel, and the residual kernel's variant; only variants that compile to the
   // same arithmetic are candidates (ptxas contracts multiply-adds differently under different register budgets, so a
   // launch-bounds variant can round differently; every candidate here was checked bit for bit): each the fastest candidate over
   // two timed iterations of this arena's own cases. The state, turbulence and counters are restored afterwards; the choice does not change any
@@ -841,27 +849,29 @@ struct ArenaHost {
     // timed groups: first pass j / i, substitution j / i, SST lines
     const int grp[5] = {G_LINES_J, G_LINES_I, G_SUBST_J, G_SUBST_I, G_TURB_LINES};
     double best[5] = {1e30, 1e30, 1e30, 1e30, 1e30};
-    int pick_w[5] = {LINE_WARPS, LINE_WARPS, LINE_WARPS, LINE_WARPS, TL_WARPS}, pick_pf[2] = {0, 0};
+    // pick_pf: prefetching of the first pass (q = 0, 1) and of the substitution passes (q = 2, 3)
+    int pick_w[5] = {LINE_WARPS, LINE_WARPS, LINE_WARPS, LINE_WARPS, TL_WARPS}, pick_pf[4] = {0, 0, 0, 0};
     int rc = 0;
     for (int pf = 0; pf < 2; ++pf)
       for (int w : cand) {
         if (pf && w > 4) continue;
         lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
-        pf_lines[0] = pf_lines[1] = pf;
+        pf_lines[0] = pf_lines[1] = pf_subst[0] = pf_subst[1] = pf;
         if ((rc = profile(1))) return rc;  // warm-up of this variant
         if ((rc = profile(2))) return rc;
         for (int q = 0; q < 5; ++q) {
-          if (q >= 2 && pf) continue;  // only the first pass has the prefetching variant
+          if (q == 4 && pf) continue;  // the SST line kernel has no prefetching variant
           if (q < 2 && w > 4) continue;
           const double t = prof_ms[grp[q]];
           if (t < best[q]) {
             best[q] = t, pick_w[q] = w;
-            if (q < 2) pick_pf[q] = pf;
+            if (q < 4) pick_pf[q] = pf;
           }
         }
       }
     lw_lines[0] = pick_w[0], lw_lines[1] = pick_w[1], pf_lines[0] = pick_pf[0], pf_lines[1] = pick_pf[1];
     lw_subst[0] = pick_w[2], lw_subst[1] = pick_w[3], lw_turb = pick_w[4];
+    pf_subst[0] = pick_pf[2], pf_subst[1] = pick_pf[3];
     double best_r = 1e30;
     int pick_r = 0;
     for (int v = 0; v < 2; ++v) {

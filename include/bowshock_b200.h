@@ -305,13 +305,14 @@ int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* 
  * prefetching, variant 0) the autotuner picks, each the fastest of two timed iterations of the arena's own cases per
  * candidate (the state restored afterwards): per direction, lines per block (1, 2 or 4) of the block line solves' first
  * pass and whether its walks prefetch the next cell's record (0 / 1), lines per block (1, 2, 4 or 8) of their
- * substitution passes, lines per block of the SST line kernel, and the residual kernel's variant (0: 256 threads per
+ * substitution passes and whether those walks prefetch (0 / 1), lines per block of the SST line kernel, and the residual kernel's variant (0: 256 threads per
  * 32 x 8 tile, 1: 288). Every candidate compiles to the same arithmetic (checked bit for bit), so none of these changes
  * a result. The smallest segment a lane eliminates per direction (segment_i / segment_j: 2, 4 or 8 cells; fewer
  * separators on short lines) is 2 unless pinned: it changes the rounding of the line solves. No counterpart in the
  * reference (its line solves run in Luma, gpu/implicit.rs:731-732). */
 typedef struct {
-  int32_t lines_i, lines_j, prefetch_i, prefetch_j, subst_i, subst_j, turb_lines, segment_i, segment_j, residual;
+  int32_t lines_i, lines_j, prefetch_i, prefetch_j, subst_i, subst_j, turb_lines, segment_i, segment_j, residual, subst_prefetch_i,
+      subst_prefetch_j;
 } bowshock_line_tuning;
 int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out);
 /* Pin the launch shapes instead of the autotuner's (for reproducible runs: the segment lengths change the order of
