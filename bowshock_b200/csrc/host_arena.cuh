@@ -49,6 +49,7 @@ struct HostCase {
   }
   bool solid(int i, int j) const { return has_block && (i < i_end ? j < j_end : j < j_sting); }
   int col_start(int i) const { return has_block ? (int)(i < i_end ? j_end : j_sting) : 0; }
+  int row_start(int j) const { return !has_block ? 0 : j < j_sting ? ni : j < j_end ? (int)i_end : 0; }
   // viscous.rs:97-109 (host side: wall distance)
   bool noslip_jface(int i, int j) const {
     if (!viscous) return false;
@@ -485,7 +486,7 @@ struct ArenaHost {
     if ((rc = upload_desc())) return rc;
     for (int k = 0; k < nc; ++k)
       if ((rc = reset_case(k))) return rc;
-    return 0;
+    return compact_lists();
   }
 
   // Re-derive the descriptors from the host configuration (config, scheme, block, viscous changes).
@@ -656,33 +657,42 @@ struct ArenaHost {
     return compact_lists();
   }
   // Launch only over the active cases' tiles, padded blocks and lines once some cases are masked out (not with a
-  // multigrid hierarchy, whose level masks change inside an iteration). A changed list invalidates the captured graph.
+  // multigrid hierarchy, whose level masks change inside an iteration). The line lists also order the lines longest
+  // first, so the blocks with the longest per-lane chains start in the first wave of a line launch instead of trailing
+  // it (a line's arithmetic does not depend on its position in the launch). A changed list invalidates the captured graph.
   int compact_lists() {
     const int nc = (int)cases.size();
     int n_act = 0;
     for (int k = 0; k < nc; ++k) n_act += h_active[k];
-    const bool want = mg_levels <= 1 && n_act > 0 && n_act < nc;
+    const bool lists = mg_levels <= 1 && n_act > 0, want = lists && n_act < nc;
     std::vector<int> tl, pb, il, jl;
-    if (want) {
+    if (lists) {
+      std::vector<std::pair<int, int>> li, lj;  // (-fluid cells of the line, global line)
       for (int k = 0; k < nc; ++k) {
         if (!h_active[k]) continue;
         const CaseDev& c = desc[k];
         const HostCase& h = cases[k];
         int nt = c.ntx * c.nty, nb = (int)(((long long)(h.ni + 4) * (h.nj + 4) + 255) / 256);
-        for (int q = 0; q < nt; ++q) tl.push_back(c.tile_off + q);
-        for (int q = 0; q < nb; ++q) pb.push_back(c.pblk_off + q);
-        for (int q = 0; q < h.nj; ++q) il.push_back(c.iline_off + q);
-        for (int q = 0; q < h.ni; ++q) jl.push_back(c.jline_off + q);
+        for (int q = 0; want && q < nt; ++q) tl.push_back(c.tile_off + q);
+        for (int q = 0; want && q < nb; ++q) pb.push_back(c.pblk_off + q);
+        for (int q = 0; q < h.nj; ++q) li.push_back({-(h.ni - h.row_start(q)), c.iline_off + q});
+        for (int q = 0; q < h.ni; ++q) lj.push_back({-(h.nj - h.col_start(q)), c.jline_off + q});
       }
-      BK_CUDA(cudaMemcpy(d_tlist, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy(d_pblist, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
+      std::stable_sort(li.begin(), li.end());
+      std::stable_sort(lj.begin(), lj.end());
+      for (auto& p : li) il.push_back(p.second);
+      for (auto& p : lj) jl.push_back(p.second);
+      if (want) {
+        BK_CUDA(cudaMemcpy(d_tlist, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice));
+        BK_CUDA(cudaMemcpy(d_pblist, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
+      }
       BK_CUDA(cudaMemcpy(d_illist, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
       BK_CUDA(cudaMemcpy(d_jllist, jl.data(), jl.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
     A.tile_list = want ? d_tlist : nullptr;
     A.pblk_list = want ? d_pblist : nullptr;
-    A.iline_list = want ? d_illist : nullptr;
-    A.jline_list = want ? d_jllist : nullptr;
+    A.iline_list = lists ? d_illist : nullptr;
+    A.jline_list = lists ? d_jllist : nullptr;
     A.n_tl = (int)tl.size(), A.n_pb = (int)pb.size(), A.n_il = (int)il.size(), A.n_jl = (int)jl.size();
     graph_dirty = true;  // same kernels, new grids and lists: the next capture updates the instantiated graph
     return 0;
