@@ -83,7 +83,7 @@ class StingGridC(C.Structure):  # bowshock_sting_grid
 class LineTuning(C.Structure):  # bowshock_line_tuning
     _fields_ = [(n, C.c_int32) for n in ("lines_i", "lines_j", "prefetch_i", "prefetch_j", "subst_i", "subst_j", "turb_lines",
                                               "segment_i", "segment_j", "residual", "subst_prefetch_i",
-                                              "subst_prefetch_j")]
+                                              "subst_prefetch_j", "staged_lines")]
 
 
 class CaseDesc(C.Structure):  # bowshock_case_desc

@@ -674,6 +674,7 @@ int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out) {
   out->subst_i = r.lw_subst[1], out->subst_j = r.lw_subst[0], out->turb_lines = r.lw_turb;
   out->segment_i = r.A.mmin_i, out->segment_j = r.A.mmin_j, out->residual = r.res_variant;
   out->subst_prefetch_i = r.pf_subst[1], out->subst_prefetch_j = r.pf_subst[0];
+  out->staged_lines = r.staged_lines;
   return BOWSHOCK_OK;
 }
 
@@ -683,9 +684,10 @@ int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) 
   auto w8 = [](int32_t w) { return w == 1 || w == 2 || w == 4 || w == 8; };
   auto m8 = [](int32_t m) { return m == 2 || m == 4 || m == 8; };
   auto b01 = [](int32_t b) { return b == 0 || b == 1; };
+  auto b012 = [](int32_t b) { return b >= 0 && b <= 2; };
   if (!(w4(t->lines_i) && w4(t->lines_j) && b01(t->prefetch_i) && b01(t->prefetch_j) && w8(t->subst_i) && w8(t->subst_j) &&
         w8(t->turb_lines) && m8(t->segment_i) && m8(t->segment_j) && (t->residual == 0 || t->residual == 1) &&
-        b01(t->subst_prefetch_i) && b01(t->subst_prefetch_j))) {
+        b012(t->subst_prefetch_i) && b012(t->subst_prefetch_j) && t->staged_lines >= 0)) {
     a->last_error = "line tuning out of range";
     return BOWSHOCK_INVALID;
   }
@@ -694,6 +696,7 @@ int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) 
   r.lw_subst[1] = t->subst_i, r.lw_subst[0] = t->subst_j, r.lw_turb = t->turb_lines;
   r.A.mmin_i = t->segment_i, r.A.mmin_j = t->segment_j, r.res_variant = t->residual;
   r.pf_subst[1] = t->subst_prefetch_i, r.pf_subst[0] = t->subst_prefetch_j;
+  r.staged_lines = t->staged_lines;
   if (r.graph) cudaGraphExecDestroy(r.graph), r.graph = nullptr;  // the chunk graph holds the old shapes
   return BOWSHOCK_OK;
 }

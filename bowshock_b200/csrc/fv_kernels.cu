@@ -382,8 +382,8 @@ __device__ __forceinline__ M4<float> ld_m4(const float4* p) {
 }
 
 // Positivity-damped update u += alpha du, alpha halved up to 8 times (implicit.rs:641-660), on the state pair in FP64.
-__device__ __forceinline__ void damped_update(const Arena& A, long long cc, const V4<float>& dq) {
-  V4<double> u = state_of(A, cc);
+// u: the cell's state before the update (state_of(A, cc), or the same pair fetched ahead of time)
+__device__ __forceinline__ void damped_update_from(const Arena& A, long long cc, const V4<float>& dq, const V4<double>& u) {
   double alpha = 1.0;
   for (int t = 0; t < 8; ++t) {
     V4<double> q = mk4<double>(u[0] + alpha * dq[0], u[1] + alpha * dq[1], u[2] + alpha * dq[2], u[3] + alpha * dq[3]);
@@ -394,6 +394,9 @@ __device__ __forceinline__ void damped_update(const Arena& A, long long cc, cons
     }
     alpha *= 0.5;
   }
+}
+__device__ __forceinline__ void damped_update(const Arena& A, long long cc, const V4<float>& dq) {
+  damped_update_from(A, cc, dq, state_of(A, cc));
 }
 
 constexpr int LINE_WARPS = 4;  // default lines per block of the line kernels
@@ -939,6 +942,203 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
       cc = cn, GEk = GE_n, Yk = Y_n, gk4 = g_n;
     }
   }
+  if (update && L == 0 && lane == 0) {
+    A.iter[ci] += 1;
+    A.ramp_k[ci] += 1;
+  }
+}
+
+// ---- substitution passes with the walks' records staged through shared memory
+// Each lane copies the records of the next SUB_SD cells of its segment into shared memory ahead of the arithmetic
+// (cp.async, one commit group per cell), and the separator row and the reduction multipliers it will read are fetched at
+// the start: a walk waits for one memory round trip per SUB_SD cells instead of one per cell, which is what bounds the
+// passes when few lines are left (a lane's segment of a handful of cells is a chain of dependent loads otherwise). One
+// line per block, 47 KB of shared memory. Every lane copies and reads only its own slots, so the copies need no barrier
+// across the warp; the __syncwarp before each refill orders a slot's reads before the copy that overwrites it.
+constexpr int SUB_SD = 3;
+struct SubstStage {
+  float4 w[SUB_SD][13][32];  // forward: lo 0-3, M^-1 4-7, T 8-11, r 12; backward: GE 0-3, Y 4-7, g 8, du 9, U 10, Ulo 11
+  float4 p[PREC][32];        // the lane's reduction multipliers
+  float4 sp[9][32];          // the separator row: lo 0-3, up 4-7, r 8
+};
+static_assert(sizeof(SubstStage) <= 48 * 1024, "static shared memory");
+__device__ __forceinline__ void cp16(float4* smem, const float4* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// a 4x4 block whose rows lie 32 float4 apart (one lane's slots of a staging array)
+__device__ __forceinline__ M4<float> ld_m4s(const float4* p) {
+  M4<float> m;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 v = p[32 * q];
+    m[4 * q] = v.x, m[4 * q + 1] = v.y, m[4 * q + 2] = v.z, m[4 * q + 3] = v.w;
+  }
+  return m;
+}
+__device__ __forceinline__ void cp_m4(float4* smem, const float4* gmem) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) cp16(smem + 32 * q, gmem + q);
+}
+
+// The defect-correction pass of k_lines_subst (same arithmetic, same results) with the staged records.
+__global__ void __launch_bounds__(32) k_lines_subst_st(Arena A, int dir_i, const float4* in, float4* out, int pass) {
+  __shared__ SubstStage S;
+  const int lane = threadIdx.x;
+  LineSeg G;
+  if (!line_seg(A, dir_i, blockIdx.x, lane, G)) return;
+  const int ci = G.ci;
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || pass >= c.sub_iters) return;
+  const bool di = dir_i != 0;
+  const int epilogue = dir_i ? 0 : 2;
+  const bool update = !dir_i && pass == c.sub_iters - 1;
+  const int L = G.L, N = G.N, a = G.a, e = G.e, ke = G.ke;
+  const int s = lane;
+  auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
+  // the separator row and the multipliers this lane reads (the predicates of the reduction below)
+  if (G.has_sep) {
+    const long long cs = cell(e - 1);
+    const Rec r = line_rec(A, di, cs);
+    cp_m4(&S.sp[0][lane], r.blk(F_LO));
+    cp_m4(&S.sp[4][lane], r.blk(F_UP));
+    cp16(&S.sp[8][lane], in + cs);
+  }
+  const float4* prec = pcr_rec(A, di, G.gw, s);
+  if (s < N) {
+    int lvl = 0;
+    for (int h = 1; h < N; h <<= 1, ++lvl) {
+      if (s - h >= 0) cp_m4(&S.p[8 * lvl][lane], prec + 8 * lvl);
+      if (s + h < N) cp_m4(&S.p[8 * lvl + 4][lane], prec + 8 * lvl + 4);
+    }
+    cp_m4(&S.p[8 * PCR_LEVELS][lane], prec + 8 * PCR_LEVELS);
+  }
+  cp_commit();
+  const int nk = G.act ? ke - a + 1 : 0, mk = G.m;  // cells of this lane's walks; mk >= nk for every lane
+  // forward: g = M^-1 (r - lo g_prev), v_f = sum_k T_k g_k
+  auto issue_f = [&](int k, int slot) {
+    const long long cc = cell(a + k);
+    const Rec r = line_rec(A, di, cc);
+    cp_m4(&S.w[slot][0][lane], r.blk(F_LO));
+    cp_m4(&S.w[slot][4][lane], r.blk(F_MINV));
+    cp_m4(&S.w[slot][8][lane], r.blk(F_T));
+    cp16(&S.w[slot][12][lane], in + cc);
+  };
+#pragma unroll
+  for (int q = 0; q < SUB_SD; ++q) {
+    if (q < nk) issue_f(q, q);
+    cp_commit();
+  }
+  V4<float> g = mk4<float>(0, 0, 0, 0), v_f = mk4<float>(0, 0, 0, 0);
+  for (int k = 0; k < mk; ++k) {
+    cp_wait<SUB_SD - 1>();
+    const int slot = k % SUB_SD;
+    if (k < nk) {
+      const long long cc = cell(a + k);
+      const M4<float> Lo = ld_m4s(&S.w[slot][0][lane]), Mi = ld_m4s(&S.w[slot][4][lane]), Tk = ld_m4s(&S.w[slot][8][lane]);
+      V4<float> r = from_f4(S.w[slot][12][lane]);
+      if (k > 0) {
+        V4<float> t = mv(Lo, g);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r[q] -= t[q];
+      }
+      g = mv(Mi, r);
+      *line_rec(A, di, cc).g() = to_f4(g);
+      const V4<float> tg = mv(Tk, g);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v_f[q] += tg[q];
+    }
+    __syncwarp();
+    if (k + SUB_SD < nk) issue_f(k + SUB_SD, slot);
+    cp_commit();
+  }
+  const V4<float> v_l = g;
+  const V4<float> vn = shfl_down4(v_f, 1);
+  V4<float> rd = mk4<float>(0, 0, 0, 0);
+  if (G.has_sep) {
+    V4<float> r = from_f4(S.sp[8][lane]);
+    V4<float> t1 = mv(ld_m4s(&S.sp[0][lane]), v_l), t2 = mv(ld_m4s(&S.sp[4][lane]), vn);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rd[q] = r[q] - t1[q] - t2[q];
+  }
+  int lvl = 0;
+  for (int h = 1; h < N; h <<= 1, ++lvl) {
+    V4<float> dm = shfl_up4(rd, h), dp = shfl_down4(rd, h);
+    if (s < N) {
+      V4<float> nd = rd;
+      if (s - h >= 0) {
+        V4<float> t = mv(ld_m4s(&S.p[8 * lvl][lane]), dm);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nd[q] += t[q];
+      }
+      if (s + h < N) {
+        V4<float> t = mv(ld_m4s(&S.p[8 * lvl + 4][lane]), dp);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nd[q] += t[q];
+      }
+      rd = nd;
+    }
+  }
+  V4<float> lsep = mk4<float>(0, 0, 0, 0);
+  if (s < N) lsep = mv(ld_m4s(&S.p[8 * PCR_LEVELS][lane]), rd);
+  V4<float> lprev = shfl_up4(lsep, 1);
+  if (s == 0) lprev = mk4<float>(0, 0, 0, 0);
+  V4<float> xn = G.has_sep ? lsep : mk4<float>(0, 0, 0, 0);
+  if (G.has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
+  // backward: x = g + GE l_left - Y x_next, from the last interior cell down; the j passes also fetch du (and the
+  // state, for the last pass's update) ahead of time
+  auto issue_b = [&](int k, int slot) {
+    const long long cc = cell(ke - k);
+    const Rec r = line_rec(A, di, cc);
+    cp_m4(&S.w[slot][0][lane], r.blk(F_GE));
+    cp_m4(&S.w[slot][4][lane], r.blk(F_Y));
+    cp16(&S.w[slot][8][lane], r.g());
+    if (epilogue == 2) cp16(&S.w[slot][9][lane], A.DU + cc);
+    if (update) {
+      cp16(&S.w[slot][10][lane], A.U + cc);
+      cp16(&S.w[slot][11][lane], A.Ulo + cc);
+    }
+  };
+  __threadfence_block();  // the forward walk's g stores before the copies that read them back
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < SUB_SD; ++q) {
+    if (q < nk) issue_b(q, q);
+    cp_commit();
+  }
+  for (int k = 0; k < mk; ++k) {
+    cp_wait<SUB_SD - 1>();
+    const int slot = k % SUB_SD;
+    if (k < nk) {
+      const long long cc = cell(ke - k);
+      const M4<float> GEk = ld_m4s(&S.w[slot][0][lane]), Yk = ld_m4s(&S.w[slot][4][lane]);
+      V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
+      V4<float> gk = from_f4(S.w[slot][8][lane]);
+      V4<float> x;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
+      if (epilogue == 0) {
+        out[cc] = to_f4(x);
+      } else {
+        V4<float> du = x;
+        V4<float> o = from_f4(S.w[slot][9][lane]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) du[q] += o[q];
+        A.DU[cc] = to_f4(du);
+        if (update) damped_update_from(A, cc, du, pair_ld(S.w[slot][10][lane], S.w[slot][11][lane]));
+      }
+      xn = x;
+    }
+    __syncwarp();
+    if (k + SUB_SD < nk) issue_b(k + SUB_SD, slot);
+    cp_commit();
+  }
+  cp_wait<0>();
   if (update && L == 0 && lane == 0) {
     A.iter[ci] += 1;
     A.ramp_k[ci] += 1;

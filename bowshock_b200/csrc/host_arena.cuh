@@ -486,6 +486,10 @@ struct ArenaHost {
     if ((rc = upload_desc())) return rc;
     for (int k = 0; k < nc; ++k)
       if ((rc = reset_case(k))) return rc;
+    int nb = 0, sms = 0;
+    BK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_lines_subst_st, 32, 0));
+    BK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    staged_lines = 2 * nb * sms;
     return compact_lists();
   }
 
@@ -773,7 +777,13 @@ struct ArenaHost {
   // block (1, 2, 4, or 8 except for the first pass, whose shared memory holds 4 lines at most) and, for the first pass,
   // whether the walks prefetch the next cell's record.
   int lw_lines[2] = {LINE_WARPS, LINE_WARPS}, pf_lines[2] = {0, 0}, lw_subst[2] = {LINE_WARPS, LINE_WARPS}, lw_turb = TL_WARPS;
-  int pf_subst[2] = {0, 0};  // whether the substitution walks prefetch the next cell's record
+  // how the substitution walks fetch their records: 0 one cell at a time, 1 the next cell's ahead (registers), 2 staged
+  // through shared memory SUB_SD cells ahead (one line per block, lw_subst not used)
+  int pf_subst[2] = {0, 0};
+  // A direction with at most this many lines in the launch runs its substitution passes staged (pf_subst 2) whatever
+  // pf_subst says: with few lines the passes wait on memory latency, not bandwidth, and the staged walks wait once per
+  // SUB_SD cells. Set at setup to two waves of the staged kernel (its blocks per SM x SMs x 2); 0 never.
+  int staged_lines = 0;
   template <bool PF>
   void launch_lines_pf(int dir_i, int w, const float4* in, int from_res, float4* out) {
     const int nl = LI(dir_i);
@@ -804,7 +814,9 @@ struct ArenaHost {
   }
   void launch_subst(int dir_i, const float4* in, float4* out, int pass) {
     const int d = dir_i ? 1 : 0;
-    if (pf_subst[d])
+    if (pf_subst[d] == 2 || LI(dir_i) <= staged_lines)
+      k_lines_subst_st<<<LI(dir_i), 32, 0, stream>>>(A, dir_i, in, out, pass);
+    else if (pf_subst[d])
       launch_subst_pf<true>(dir_i, lw_subst[d], in, out, pass);
     else
       launch_subst_pf<false>(dir_i, lw_subst[d], in, out, pass);
@@ -862,16 +874,19 @@ struct ArenaHost {
     // pick_pf: prefetching of the first pass (q = 0, 1) and of the substitution passes (q = 2, 3)
     int pick_w[5] = {LINE_WARPS, LINE_WARPS, LINE_WARPS, LINE_WARPS, TL_WARPS}, pick_pf[4] = {0, 0, 0, 0};
     int rc = 0;
-    for (int pf = 0; pf < 2; ++pf)
+    const int staged_keep = staged_lines;
+    staged_lines = 0;  // time the variants as requested
+    for (int pf = 0; pf < 3; ++pf)
       for (int w : cand) {
-        if (pf && w > 4) continue;
+        if ((pf == 1 && w > 4) || (pf == 2 && w > 1)) continue;
         lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
-        pf_lines[0] = pf_lines[1] = pf_subst[0] = pf_subst[1] = pf;
+        pf_lines[0] = pf_lines[1] = pf == 1;
+        pf_subst[0] = pf_subst[1] = pf;
         if ((rc = profile(1))) return rc;  // warm-up of this variant
         if ((rc = profile(2))) return rc;
         for (int q = 0; q < 5; ++q) {
           if (q == 4 && pf) continue;  // the SST line kernel has no prefetching variant
-          if (q < 2 && w > 4) continue;
+          if (q < 2 && (w > 4 || pf == 2)) continue;  // the first pass has no staged variant
           const double t = prof_ms[grp[q]];
           if (t < best[q]) {
             best[q] = t, pick_w[q] = w;
@@ -891,6 +906,7 @@ struct ArenaHost {
       if (prof_ms[G_RESIDUAL] < best_r) best_r = prof_ms[G_RESIDUAL], pick_r = v;
     }
     res_variant = pick_r;
+    staged_lines = staged_keep;
 
     BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
     BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
