@@ -134,6 +134,7 @@ int bowshock_solver_set_block(bowshock_solver* s, const bowshock_block* b) {
     h.has_block = false;
     h.has_nozzle = false;
   }
+  h.dwall.clear();
   return from_arena(s, s->ar.upload_desc());
 }
 
@@ -155,6 +156,7 @@ int bowshock_solver_set_nozzle(bowshock_solver* s, const bowshock_nozzle* n) {
   } else {
     h.has_nozzle = false;
   }
+  h.dwall.clear();
   return from_arena(s, s->ar.upload_desc());
 }
 
@@ -261,6 +263,7 @@ int bowshock_solver_set_viscous(bowshock_solver* s, const bowshock_viscous* v) {
     h.viscous = false;
     h.turbulence = 0;
   }
+  h.dwall.clear();  // the no-slip faces may have changed
   int rc = s->ar.upload_desc();
   if (rc) return from_arena(s, rc);
   if (h.viscous && h.turbulence == BOWSHOCK_TURB_SST) return from_arena(s, s->ar.turb_init(0));
@@ -642,18 +645,20 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
       h.sutherland = d.viscous.sutherland;
       h.roughness = d.viscous.roughness;
     }
-    if (!compute_metrics(h, m)) {
-      delete a;
-      return BOWSHOCK_INVALID;
-    }
     a->ar.cases.push_back(std::move(h));
     a->descs.push_back(d);
     a->nseg.push_back(d.body.nseg);
+  }
+  // the FP64 metrics of each case, the cases spread over the host threads
+  if (!parallel_cases(a->ar.cases.size(), [&](size_t k, std::string& e) { return compute_metrics(a->ar.cases[k], e); }, m)) {
+    delete a;
+    return BOWSHOCK_INVALID;
   }
   a->ar.device = device;
   int rc = a->ar.setup();
   if (!rc) rc = a->fp.setup(a->ar);
   for (uint64_t k = 0; !rc && k < ncases; ++k) rc = a->fp.set_body(a->ar, (int)k, &cases[k].body);
+  if (!rc) a->ar.wall_distances();
   for (uint64_t k = 0; !rc && k < ncases; ++k)
     if (a->ar.cases[k].viscous && a->ar.cases[k].turbulence == 1) rc = a->ar.turb_init((int)k);
   // lines per block of the line kernels, tuned on the arena's own cases when it is large enough to matter

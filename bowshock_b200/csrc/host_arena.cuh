@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -22,6 +23,7 @@ struct HostCase {
   std::vector<double> if_nx, if_nr, if_len, if_rm;  // (ni+1)*nj
   std::vector<double> jf_nx, jf_nr, jf_len, jf_rm;  // ni*(nj+1)
   std::vector<double> area, vol, xc, rc;
+  std::vector<double> dwall;  // wall distance of the cells (turbulence.rs:91-125), computed once; empty until then
   // configuration (doubles as given by the caller)
   double cfl = 0.5;
   int limiter = 1;
@@ -118,43 +120,117 @@ inline void face_stencils(const HostCase& h, std::vector<float4>& fis, std::vect
     }
 }
 
-// Distance of every cell centroid to the nearest no-slip wall face segment (turbulence.rs:91-125), FP64, brute force.
-inline std::vector<double> wall_distance(const HostCase& h) {
-  const int ni = h.ni, nj = h.nj;
-  std::vector<double> segs;
-  auto node = [&](int i, int j) { return std::make_pair(h.x[(size_t)j * (ni + 1) + i], h.r[(size_t)j * (ni + 1) + i]); };
-  for (int j = 0; j <= nj; ++j)
-    for (int i = 0; i < ni; ++i)
-      if (h.noslip_jface(i, j)) {
-        auto a = node(i, j), b = node(i + 1, j);
-        segs.insert(segs.end(), {a.first, a.second, b.first, b.second});
-      }
-  for (int j = 0; j < nj; ++j)
-    for (int i = 0; i <= ni; ++i)
-      if (h.noslip_iface(i, j)) {
-        auto a = node(i, j), b = node(i, j + 1);
-        segs.insert(segs.end(), {a.first, a.second, b.first, b.second});
-      }
-  std::vector<double> d((size_t)ni * nj, std::numeric_limits<double>::infinity());
-  auto rows = [&](int j0, int j1) {
-    for (int j = j0; j < j1; ++j)
-      for (int i = 0; i < ni; ++i) {
-        if (h.solid(i, j)) continue;
-        size_t c = (size_t)j * ni + i;
-        double px = h.xc[c], pr = h.rc[c], best = d[c];
-        for (size_t s = 0; s + 3 < segs.size(); s += 4) {
-          double ex = segs[s + 2] - segs[s], er = segs[s + 3] - segs[s + 1];
-          double t = ((px - segs[s]) * ex + (pr - segs[s + 1]) * er) / (ex * ex + er * er);
-          t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
-          best = std::fmin(best, std::hypot(px - (segs[s] + t * ex), pr - (segs[s + 1] + t * er)));
-        }
-        d[c] = best;
-      }
+// Run f(k, err) for k in [0, n) over the host threads; false (with err of a failing k) if any call fails.
+template <typename F>
+inline bool parallel_cases(size_t n, F f, std::string& err) {
+  const size_t nt = std::min<size_t>(n, std::max(1u, std::min(32u, std::thread::hardware_concurrency())));
+  std::vector<std::string> errs(n);
+  std::vector<char> ok(n, 1);
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t k = next++; k < n; k = next++) ok[k] = f(k, errs[k]) ? 1 : 0;
   };
-  // rows are independent: split them over the host threads
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto& x : th) x.join();
+  for (size_t k = 0; k < n; ++k)
+    if (!ok[k]) {
+      err = errs[k];
+      return false;
+    }
+  return true;
+}
+
+// No-slip wall face segments of a case (turbulence.rs:91-125): endpoints and bounding box.
+struct WallSegs {
+  std::vector<double> s;  // x0, r0, x1, r1, xmin, xmax, rmin, rmax per segment
+  explicit WallSegs(const HostCase& h) {
+    const int ni = h.ni, nj = h.nj;
+    auto node = [&](int i, int j) { return std::make_pair(h.x[(size_t)j * (ni + 1) + i], h.r[(size_t)j * (ni + 1) + i]); };
+    auto add = [&](std::pair<double, double> a, std::pair<double, double> b) {
+      s.insert(s.end(), {a.first, a.second, b.first, b.second, std::fmin(a.first, b.first), std::fmax(a.first, b.first),
+                         std::fmin(a.second, b.second), std::fmax(a.second, b.second)});
+    };
+    for (int j = 0; j <= nj; ++j)
+      for (int i = 0; i < ni; ++i)
+        if (h.noslip_jface(i, j)) add(node(i, j), node(i + 1, j));
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i <= ni; ++i)
+        if (h.noslip_iface(i, j)) add(node(i, j), node(i, j + 1));
+    group();
+  }
+  static constexpr size_t GROUP = 8;  // consecutive segments (neighbours along the wall) under one bounding box
+  std::vector<double> gb;              // xmin, xmax, rmin, rmax per group
+  void group() {
+    for (size_t q0 = 0; q0 < n(); q0 += GROUP) {
+      double b[4] = {INFINITY, -INFINITY, INFINITY, -INFINITY};
+      for (size_t q = q0; q < std::min(n(), q0 + GROUP); ++q) {
+        const double* g = &s[8 * q];
+        b[0] = std::fmin(b[0], g[4]), b[1] = std::fmax(b[1], g[5]), b[2] = std::fmin(b[2], g[6]), b[3] = std::fmax(b[3], g[7]);
+      }
+      gb.insert(gb.end(), b, b + 4);
+    }
+  }
+  size_t n() const { return s.size() / 8; }
+  static double box(const double* b, double px, double pr) {
+    double dx = std::fmax(std::fmax(b[0] - px, px - b[1]), 0.0), dr = std::fmax(std::fmax(b[2] - pr, pr - b[3]), 0.0);
+    return std::sqrt(dx * dx + dr * dr);
+  }
+  // distance of (px, pr) to segment q: the clamped projection, FP64
+  double dist(size_t q, double px, double pr) const {
+    const double* g = &s[8 * q];
+    double ex = g[2] - g[0], er = g[3] - g[1];
+    double t = ((px - g[0]) * ex + (pr - g[1]) * er) / (ex * ex + er * er);
+    t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    return std::hypot(px - (g[0] + t * ex), pr - (g[1] + t * er));
+  }
+  // lower bounds of that distance: the distance to the segment's bounding box, and to its group's
+  double bound(size_t q, double px, double pr) const { return box(&s[8 * q + 4], px, pr); }
+  double group_bound(size_t g, double px, double pr) const { return box(&gb[4 * g], px, pr); }
+};
+
+// Distance of the centroids of rows [j0, j1) to the nearest wall segment, the minimum over every segment as the
+// reference takes it. The minimum is the same: a segment is skipped only when its bounding box lies farther than the
+// current minimum by a margin (1e-9 relative plus 1e-9 absolute, in nose diameters) far above the rounding of either
+// distance (the bounds are tested per group of neighbouring segments, then per segment), and the segment nearest to the
+// previous cell of the row is evaluated first.
+inline void wall_distance_rows(const HostCase& h, const WallSegs& w, std::vector<double>& d, int j0, int j1) {
+  const int ni = h.ni;
+  const size_t ns = w.n();
+  for (int j = j0; j < j1; ++j) {
+    size_t hint = 0;
+    for (int i = 0; i < ni; ++i) {
+      if (h.solid(i, j)) continue;
+      size_t c = (size_t)j * ni + i;
+      double px = h.xc[c], pr = h.rc[c], best = d[c];
+      if (ns == 0) continue;
+      best = std::fmin(best, w.dist(hint, px, pr));
+      size_t arg = hint;
+      for (size_t g0 = 0; g0 < ns; g0 += WallSegs::GROUP) {
+        if (w.group_bound(g0 / WallSegs::GROUP, px, pr) > best * (1.0 + 1e-9) + 1e-9) continue;
+        for (size_t q = g0; q < std::min(ns, g0 + WallSegs::GROUP); ++q) {
+          if (q == hint || w.bound(q, px, pr) > best * (1.0 + 1e-9) + 1e-9) continue;
+          double dq = w.dist(q, px, pr);
+          if (dq < best) arg = q;
+          best = std::fmin(best, dq);
+        }
+      }
+      d[c] = best;
+      hint = arg;
+    }
+  }
+}
+
+// The wall distance of every cell of one case (infinity where no wall exists), rows split over the host threads.
+inline std::vector<double> wall_distance(const HostCase& h) {
+  const WallSegs w(h);
+  std::vector<double> d((size_t)h.ni * h.nj, std::numeric_limits<double>::infinity());
+  const int nj = h.nj;
   int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   std::vector<std::thread> th;
-  for (int t = 0; t < nt; ++t) th.emplace_back(rows, (int)((long long)nj * t / nt), (int)((long long)nj * (t + 1) / nt));
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&, t] { wall_distance_rows(h, w, d, (int)((long long)nj * t / nt), (int)((long long)nj * (t + 1) / nt)); });
   for (auto& x : th) x.join();
   return d;
 }
@@ -559,6 +635,21 @@ struct ArenaHost {
     return 0;
   }
 
+  // The wall distances of every SST case not computed yet, the cases spread over the host threads (each case's rows
+  // serially) and kept for the turbulence (re)initialisations of later runs.
+  void wall_distances() {
+    std::vector<size_t> todo;
+    for (size_t k = 0; k < cases.size(); ++k)
+      if (cases[k].viscous && cases[k].turbulence == 1 && cases[k].dwall.empty()) todo.push_back(k);
+    std::string unused;
+    parallel_cases(todo.size(), [&](size_t q, std::string&) {
+      HostCase& h = cases[todo[q]];
+      std::vector<double> d((size_t)h.ni * h.nj, std::numeric_limits<double>::infinity());
+      wall_distance_rows(h, WallSegs(h), d, 0, h.nj);
+      h.dwall = std::move(d);
+      return true;
+    }, unused);
+  }
   // turbulence.rs:128-138: free-stream (k, omega) everywhere, the wall distance, mu_t = rho k / omega on fluid cells
   std::vector<double> last_turb_residual;
   int turb_init(int k) {
@@ -566,7 +657,8 @@ struct ArenaHost {
     const CaseDev& c = desc[k];
     size_t n = (size_t)h.ni * h.nj;
     double winf = 1e-6 * h.re_c, kinf = 9e-9;
-    std::vector<double> d = wall_distance(h);
+    if (cases[k].dwall.empty()) cases[k].dwall = wall_distance(h);
+    const std::vector<double>& d = cases[k].dwall;
     std::vector<float> df(n), mt(n);
     std::vector<float2> t(n, make_float2((float)kinf, (float)winf));
     std::vector<double> u(4 * n);
@@ -847,24 +939,43 @@ struct ArenaHost {
   // Autotuner: per direction, lines per block and prefetching of the first pass and of the substitution passes, lines per block of the SST line kernel, and the residual kernel's variant; only variants that compile to the
   // same arithmetic are candidates (ptxas contracts multiply-adds differently under different register budgets, so a
   // launch-bounds variant can round differently; every candidate here was checked bit for bit): each the fastest candidate over
-  // two timed iterations of this arena's own cases. The state, turbulence and counters are restored afterwards; the choice does not change any
+  // one timed iteration of this arena's own cases (after one warm-up iteration, every candidate kernel loaded first). The
+  // state, turbulence and counters are kept in a device copy and restored afterwards; the choice does not change any
   // result (every warp solves one line alone, with the same arithmetic).
   int autotune() {
     if (scheme_of_arena() != SCHEME_IMPLICIT) return 0;
     const size_t nc = cases.size();
-    std::vector<float4> hu(ncell), hl(ncell);
-    std::vector<float2> ht(any_sst ? ncell : 0);
-    std::vector<float> hm(any_sst ? ncell : 0);
-    std::vector<int> hit(nc), hr(nc);
-    BK_CUDA(cudaStreamSynchronize(stream));
-    BK_CUDA(cudaMemcpy(hu.data(), A.U, ncell * sizeof(float4), cudaMemcpyDeviceToHost));
-    BK_CUDA(cudaMemcpy(hl.data(), A.Ulo, ncell * sizeof(float4), cudaMemcpyDeviceToHost));
-    if (any_sst) {
-      BK_CUDA(cudaMemcpy(ht.data(), A.turb, ncell * sizeof(float2), cudaMemcpyDeviceToHost));
-      BK_CUDA(cudaMemcpy(hm.data(), A.mu_t, ncell * sizeof(float), cudaMemcpyDeviceToHost));
+    // the state the timed iterations advance, kept in a device copy and put back afterwards
+    struct Keep {
+      void* dst;
+      const void* src;
+      size_t bytes;
+    };
+    std::vector<Keep> keep = {{nullptr, A.U, ncell * sizeof(float4)}, {nullptr, A.Ulo, ncell * sizeof(float4)},
+                              {nullptr, d_iter, nc * sizeof(int)}, {nullptr, d_ramp, nc * sizeof(int)}};
+    if (any_sst) keep.push_back({nullptr, A.turb, ncell * sizeof(float2)}), keep.push_back({nullptr, A.mu_t, ncell * sizeof(float)});
+    size_t kb = 0;
+    for (auto& q : keep) kb += (q.bytes + 255) & ~(size_t)255;
+    char* kbuf = nullptr;
+    BK_CUDA(cudaMalloc(&kbuf, kb));
+    kb = 0;
+    for (auto& q : keep) {
+      q.dst = kbuf + kb, kb += (q.bytes + 255) & ~(size_t)255;
+      BK_CUDA(cudaMemcpyAsync(q.dst, q.src, q.bytes, cudaMemcpyDeviceToDevice, stream));
     }
-    BK_CUDA(cudaMemcpy(hit.data(), d_iter, nc * sizeof(int), cudaMemcpyDeviceToHost));
-    BK_CUDA(cudaMemcpy(hr.data(), d_ramp, nc * sizeof(int), cudaMemcpyDeviceToHost));
+    // load every candidate kernel now (lazy module loading would otherwise charge a variant's first launch)
+    {
+      cudaFuncAttributes fa;
+      const void* fns[] = {(const void*)&k_lines<1, false>, (const void*)&k_lines<2, false>, (const void*)&k_lines<4, false>,
+                           (const void*)&k_lines<1, true>, (const void*)&k_lines<2, true>, (const void*)&k_lines<4, true>,
+                           (const void*)&k_lines_subst<1, false>, (const void*)&k_lines_subst<2, false>,
+                           (const void*)&k_lines_subst<4, false>, (const void*)&k_lines_subst<8, false>,
+                           (const void*)&k_lines_subst<1, true>, (const void*)&k_lines_subst<2, true>,
+                           (const void*)&k_lines_subst<4, true>, (const void*)&k_lines_subst<8, true>,
+                           (const void*)&k_turb_lines_w<1>, (const void*)&k_turb_lines_w<2>, (const void*)&k_turb_lines_w<4>,
+                           (const void*)&k_turb_lines_w<8>, (const void*)&k_residual<288, 3>, (const void*)&k_residual<TI * TJ, 3>};
+      for (const void* f : fns) BK_CUDA(cudaFuncGetAttributes(&fa, f));
+    }
     // The smallest segment per lane (Arena::mmin_i / mmin_j) keeps its setting (2 unless pinned): a longer one changes the
     // rounding of the line solves, and on a limit-cycle case of the sweep it moved the window-mean CD by 2e-4.
     const int cand[4] = {1, 2, 4, 8};
@@ -874,19 +985,20 @@ struct ArenaHost {
     // pick_pf: prefetching of the first pass (q = 0, 1) and of the substitution passes (q = 2, 3)
     int pick_w[5] = {LINE_WARPS, LINE_WARPS, LINE_WARPS, LINE_WARPS, TL_WARPS}, pick_pf[4] = {0, 0, 0, 0};
     int rc = 0;
+    // the staged substitution walks are not candidates: they are chosen by the number of lines (staged_lines), and
+    // the variants here are timed as requested
     const int staged_keep = staged_lines;
-    staged_lines = 0;  // time the variants as requested
-    for (int pf = 0; pf < 3; ++pf)
+    staged_lines = 0;
+    if ((rc = profile(1))) return rc;  // warm-up
+    for (int pf = 0; pf < 2; ++pf)
       for (int w : cand) {
-        if ((pf == 1 && w > 4) || (pf == 2 && w > 1)) continue;
+        if (pf && w > 4) continue;
         lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
-        pf_lines[0] = pf_lines[1] = pf == 1;
-        pf_subst[0] = pf_subst[1] = pf;
-        if ((rc = profile(1))) return rc;  // warm-up of this variant
-        if ((rc = profile(2))) return rc;
+        pf_lines[0] = pf_lines[1] = pf_subst[0] = pf_subst[1] = pf;
+        if ((rc = profile(1))) return rc;
         for (int q = 0; q < 5; ++q) {
           if (q == 4 && pf) continue;  // the SST line kernel has no prefetching variant
-          if (q < 2 && (w > 4 || pf == 2)) continue;  // the first pass has no staged variant
+          if (q < 2 && w > 4) continue;
           const double t = prof_ms[grp[q]];
           if (t < best[q]) {
             best[q] = t, pick_w[q] = w;
@@ -902,20 +1014,13 @@ struct ArenaHost {
     for (int v = 0; v < 2; ++v) {
       res_variant = v;
       if ((rc = profile(1))) return rc;
-      if ((rc = profile(2))) return rc;
       if (prof_ms[G_RESIDUAL] < best_r) best_r = prof_ms[G_RESIDUAL], pick_r = v;
     }
     res_variant = pick_r;
     staged_lines = staged_keep;
-
-    BK_CUDA(cudaMemcpy(A.U, hu.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(A.Ulo, hl.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
-    if (any_sst) {
-      BK_CUDA(cudaMemcpy(A.turb, ht.data(), ncell * sizeof(float2), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy(A.mu_t, hm.data(), ncell * sizeof(float), cudaMemcpyHostToDevice));
-    }
-    BK_CUDA(cudaMemcpy(d_iter, hit.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_ramp, hr.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    for (auto& q : keep) BK_CUDA(cudaMemcpyAsync(const_cast<void*>(q.src), q.dst, q.bytes, cudaMemcpyDeviceToDevice, stream));
+    BK_CUDA(cudaStreamSynchronize(stream));
+    BK_CUDA(cudaFree(kbuf));
     if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
     return 0;
   }
