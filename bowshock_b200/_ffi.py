@@ -135,6 +135,7 @@ SIGNATURES = {
     "bowshock_large_domain_grid": (_I, [C.POINTER(BowshockBody), C.POINTER(StingGridC), C.POINTER(_U), C.POINTER(_U), _dp, _dp]),
     "bowshock_arena_create": (_I, [_U, C.POINTER(CaseDesc), _I, C.POINTER(_P)]),
     "bowshock_arena_destroy": (None, [_P]),
+    "bowshock_case_wall_distance": (_I, [C.POINTER(CaseDesc), _dp]),
     "bowshock_arena_last_error": (C.c_char_p, [_P]),
     "bowshock_arena_cells": (_I, [_P, C.POINTER(_U)]),
     "bowshock_arena_run": (_I, [_P, _U, _dp]),

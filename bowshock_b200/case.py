@@ -264,6 +264,16 @@ class Case:
         d.run = self.numerics.run_params(self.wake)
         return d
 
+    def wall_distance(self, grid=None):
+        """Distance of every cell centroid to the nearest no-slip wall face (turbulence.rs:91-125), computed on the host:
+        an (nj, ni) array, +inf on solid cells and where the case has no wall."""
+        d = self.case_desc(grid)
+        out = np.zeros(d.ni * d.nj)
+        rc = _ffi.load().bowshock_case_wall_distance(C.byref(d), _ffi.dptr(out))
+        if rc:
+            raise BowshockError(rc, "invalid case")
+        return out.reshape(d.nj, d.ni)
+
 
 def isa(altitude_m):
     """atmosphere.rs:84-112: (T, p, rho, c, mu)."""

@@ -588,6 +588,50 @@ struct bowshock_arena {
   double last_solve_ms = 0.0;
 };
 
+// The host description of one arena case (validated; the metrics are computed separately): false if invalid.
+static bool host_case_of(const bowshock_case_desc& d, HostCase& h, std::string& m) {
+  if (d.ni < 4 || d.nj < 2 || !d.x || !d.r || !valid_config(&d.cfg, m) || !valid_body(&d.body, m) ||
+      d.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT || d.scheme.sub_iters < 1 || d.scheme.sub_iters > 16 ||
+      (d.has_viscous && !(d.viscous.roughness >= 0.0 && std::isfinite(d.viscous.roughness)))) {
+    return false;
+  }
+  h.ni = (int)d.ni;
+  h.nj = (int)d.nj;
+  h.x.assign(d.x, d.x + (d.ni + 1) * (d.nj + 1));
+  h.r.assign(d.r, d.r + (d.ni + 1) * (d.nj + 1));
+  apply_config(h, &d.cfg);
+  h.low_mach = d.low_mach ? 1 : 0;
+  h.scheme = BOWSHOCK_SCHEME_IMPLICIT;
+  h.cfl0 = d.scheme.cfl0;
+  h.cfl_max = d.scheme.cfl_max;
+  h.growth = d.scheme.growth;
+  h.dt_mode = d.scheme.dt_mode;
+  h.lines = d.scheme.lines;
+  h.implicit_bc = d.scheme.implicit_bc;
+  h.sub_iters = (int)d.scheme.sub_iters;
+  h.roe = d.scheme.roe;
+  h.eps_fix = d.scheme.eps_fix;
+  if (d.has_block) {
+    const bowshock_block& b = d.block;
+    if (!(b.i_end >= 1 && b.i_end + 2 <= d.ni && b.j_end >= 2 && b.j_end + 2 <= d.nj && b.j_end > b.j_sting && (b.j_sting == 0 || b.j_sting >= 2))) {
+      return false;
+    }
+    h.has_block = true;
+    h.i_end = (long long)b.i_end;
+    h.j_end = (long long)b.j_end;
+    h.j_sting = (long long)b.j_sting;
+  }
+  if (d.has_viscous) {
+    h.viscous = true;
+    h.turbulence = d.viscous.turbulence;
+    h.wall_i_start = (long long)d.viscous.wall_i_start;
+    h.re_c = d.viscous.re_c;
+    h.sutherland = d.viscous.sutherland;
+    h.roughness = d.viscous.roughness;
+  }
+  return true;
+}
+
 static int afrom(bowshock_arena* a, int rc) {
   if (rc) a->last_error = a->ar.err;
   return rc;
@@ -603,47 +647,10 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
   std::string m;
   for (uint64_t k = 0; k < ncases; ++k) {
     const bowshock_case_desc& d = cases[k];
-    if (d.ni < 4 || d.nj < 2 || !d.x || !d.r || !valid_config(&d.cfg, m) || !valid_body(&d.body, m) ||
-        d.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT || d.scheme.sub_iters < 1 || d.scheme.sub_iters > 16 ||
-        (d.has_viscous && !(d.viscous.roughness >= 0.0 && std::isfinite(d.viscous.roughness)))) {
+    HostCase h;
+    if (!host_case_of(d, h, m)) {
       delete a;
       return BOWSHOCK_INVALID;
-    }
-    HostCase h;
-    h.ni = (int)d.ni;
-    h.nj = (int)d.nj;
-    h.x.assign(d.x, d.x + (d.ni + 1) * (d.nj + 1));
-    h.r.assign(d.r, d.r + (d.ni + 1) * (d.nj + 1));
-    apply_config(h, &d.cfg);
-    h.low_mach = d.low_mach ? 1 : 0;
-    h.scheme = BOWSHOCK_SCHEME_IMPLICIT;
-    h.cfl0 = d.scheme.cfl0;
-    h.cfl_max = d.scheme.cfl_max;
-    h.growth = d.scheme.growth;
-    h.dt_mode = d.scheme.dt_mode;
-    h.lines = d.scheme.lines;
-    h.implicit_bc = d.scheme.implicit_bc;
-    h.sub_iters = (int)d.scheme.sub_iters;
-    h.roe = d.scheme.roe;
-    h.eps_fix = d.scheme.eps_fix;
-    if (d.has_block) {
-      const bowshock_block& b = d.block;
-      if (!(b.i_end >= 1 && b.i_end + 2 <= d.ni && b.j_end >= 2 && b.j_end + 2 <= d.nj && b.j_end > b.j_sting && (b.j_sting == 0 || b.j_sting >= 2))) {
-        delete a;
-        return BOWSHOCK_INVALID;
-      }
-      h.has_block = true;
-      h.i_end = (long long)b.i_end;
-      h.j_end = (long long)b.j_end;
-      h.j_sting = (long long)b.j_sting;
-    }
-    if (d.has_viscous) {
-      h.viscous = true;
-      h.turbulence = d.viscous.turbulence;
-      h.wall_i_start = (long long)d.viscous.wall_i_start;
-      h.re_c = d.viscous.re_c;
-      h.sutherland = d.viscous.sutherland;
-      h.roughness = d.viscous.roughness;
     }
     a->ar.cases.push_back(std::move(h));
     a->descs.push_back(d);
@@ -703,6 +710,16 @@ int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) 
   r.pf_subst[1] = t->subst_prefetch_i, r.pf_subst[0] = t->subst_prefetch_j;
   r.staged_lines = t->staged_lines;
   if (r.graph) cudaGraphExecDestroy(r.graph), r.graph = nullptr;  // the chunk graph holds the old shapes
+  return BOWSHOCK_OK;
+}
+
+int bowshock_case_wall_distance(const bowshock_case_desc* d, double* out) {
+  if (!d || !out) return BOWSHOCK_INVALID;
+  HostCase h;
+  std::string m;
+  if (!host_case_of(*d, h, m) || !compute_metrics(h, m)) return BOWSHOCK_INVALID;
+  const std::vector<double> w = wall_distance(h);
+  std::copy(w.begin(), w.end(), out);
   return BOWSHOCK_OK;
 }
 

@@ -267,6 +267,13 @@ typedef struct {
   bowshock_body body;
   bowshock_run_params run;
 } bowshock_case_desc;
+/* Distance of every cell centroid of one arena case to the nearest no-slip wall face, FP64 (turbulence.rs:91-125,
+ * `wall_distance`), computed on the host with no device: the minimum over every wall segment of the clamped projection
+ * distance, segments skipped only where their bounding box lies beyond the current minimum by a margin far above
+ * rounding (the result is bit for bit that of the full search). The SST cases of an arena use it (computed once per
+ * case). out: ni * nj values (row j, column i at j * ni + i); +inf for solid cells and where the case has no wall.
+ * INVALID for a descriptor the arena would refuse. */
+int bowshock_case_wall_distance(const bowshock_case_desc* d, double* out);
 
 typedef struct bowshock_arena bowshock_arena;
 int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int device, bowshock_arena** out);

@@ -1,6 +1,6 @@
 """CPU checks of the product library without a GPU: the C ABI loads and exports every entry point that
-include/bowshock_b200.h declares, and the library's FP64 mesher reproduces the oracle's restatement of the reference
-mesher (body_grid.rs) bit for bit."""
+include/bowshock_b200.h declares, the library's FP64 mesher reproduces the oracle's restatement of the reference
+mesher (body_grid.rs) bit for bit, and its host-side wall distance matches the oracle's."""
 import os
 import re
 import subprocess
@@ -60,6 +60,23 @@ def test_mesher_matches_the_oracle_bit_for_bit(wake, viscous):
         assert np.array_equal(x, ox) and np.array_equal(r, orr)
         assert blk == s.block
         assert pc.config().first_order_iters == s.config.first_order_iters
+
+
+@pytest.mark.parametrize("wake", [0, 1])
+def test_wall_distance_matches_the_oracle(wake):
+    """The arena's SST wall distance (bowshock_case_wall_distance, host only: the search over every no-slip segment with
+    bounding-box skips) against the oracle's full search (turbulence.rs:91-125) on the viscous cases of the mesher
+    test, sting and base wakes: equal bit for bit."""
+    from bowshock_b200.case import Case, rans_params
+    re_c, suth = rans_params(0.0, 0.1)
+    for pb, ob in _bodies():
+        pc = Case.viscous_case(0.9, pb, 0, wake, re_c, suth, 0.9)
+        oc = o.case_viscous(0.9, ob, 0, wake, re_c, suth, 0.9)
+        d = pc.wall_distance().ravel()
+        ref = np.asarray(o.Solver.from_case(oc).dwall, dtype=float).ravel()
+        fin = np.isfinite(ref)
+        assert fin.any() and np.array_equal(np.isfinite(d), fin)
+        assert np.array_equal(d[fin], ref[fin])  # bit for bit: the skips drop no minimum
 
 
 def test_rans_params_match_the_oracle_atmosphere():
