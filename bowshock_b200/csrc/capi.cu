@@ -697,7 +697,7 @@ int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) 
   auto m8 = [](int32_t m) { return m == 2 || m == 4 || m == 8; };
   auto b01 = [](int32_t b) { return b == 0 || b == 1; };
   auto b012 = [](int32_t b) { return b >= 0 && b <= 2; };
-  if (!(w4(t->lines_i) && w4(t->lines_j) && b01(t->prefetch_i) && b01(t->prefetch_j) && w8(t->subst_i) && w8(t->subst_j) &&
+  if (!(w4(t->lines_i) && w4(t->lines_j) && b012(t->prefetch_i) && b012(t->prefetch_j) && w8(t->subst_i) && w8(t->subst_j) &&
         w8(t->turb_lines) && m8(t->segment_i) && m8(t->segment_j) && (t->residual == 0 || t->residual == 1) &&
         b012(t->subst_prefetch_i) && b012(t->subst_prefetch_j) && t->staged_lines >= 0)) {
     a->last_error = "line tuning out of range";

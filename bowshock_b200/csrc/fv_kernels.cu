@@ -561,18 +561,59 @@ __global__ void k_line_ends(Arena A) {
   fold_line_ends(A, c, dir_i, L, e ? 2 : 1);
 }
 
+// cp.async copies of 16 (or 4) bytes from global into shared memory, one commit group per call of cp_commit; cp_wait<N>
+// waits until at most N of this thread's groups are in flight (the staged walks below keep one group per cell, SUB_SD
+// cells ahead of the arithmetic).
+constexpr int SUB_SD = 3;
+__device__ __forceinline__ void cp16(float4* smem, const float4* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp4(float* smem, const float* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// a 4x4 block whose rows lie 32 float4 apart (one lane's slots of a staging array)
+__device__ __forceinline__ M4<float> ld_m4s(const float4* p) {
+  M4<float> m;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 v = p[32 * q];
+    m[4 * q] = v.x, m[4 * q + 1] = v.y, m[4 * q + 2] = v.z, m[4 * q + 3] = v.w;
+  }
+  return m;
+}
+__device__ __forceinline__ void cp_m4(float4* smem, const float4* gmem) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) cp16(smem + 32 * q, gmem + q);
+}
+
 // First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble and k_line_ends left in the line records, factorise
 // with the partitioned solver (each lane eliminates its segment, the separator unknowns form a
 // reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
 // back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line
 // records for the later passes and the defect.
-// W: lines (warps) per block; PF: the walks load the next cell's record before the arithmetic of the current one
-// (software pipelining: more memory parallelism per lane, ~80 more registers, so fewer warps per SM). The arena's
-// autotuner picks both per direction; the results do not depend on them.
-template <int W, bool PF>
+// W: lines (warps) per block; PF 1: the walks load the next cell's record before the arithmetic of the current one
+// (software pipelining: more memory parallelism per lane, ~80 more registers, so fewer warps per SM); PF 2: each lane's
+// records staged through shared memory SUB_SD cells ahead (cp.async, one line per block), for directions with few lines
+// left, whose walks otherwise wait for one memory round trip per cell. The arena's autotuner picks W and PF 0 / 1 per
+// direction; the results do not depend on them.
+template <int W, int PF>
 __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const float4* in, int from_res, float4* out) {
+  static_assert(PF != 2 || W == 1, "the staged walks run one line per block");
   __shared__ PcrSlot sp[W][32];
   __shared__ float4 sl[W][32];
+  // PF == 2: per lane SUB_SD cells of records in flight (forward: lo 0-3, d 4-7, up 8-11, r 12; backward: Y 0-3, GE 4-7,
+  // g 8), their time steps, and the separator row (lo, d, up, r and its time step)
+  __shared__ float4 stg[PF == 2 ? SUB_SD : 1][PF == 2 ? 13 : 1][32];
+  __shared__ float stg_dt[PF == 2 ? SUB_SD : 1][32];
+  __shared__ float4 ssep[PF == 2 ? 13 : 1][32];
+  __shared__ float ssep_dt[32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * W + warp;
   LineSeg G;
@@ -594,16 +635,91 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   // on the way down (no backward walk), and T_k is kept for the substitution passes' v_f.
   M4<float> Y = zero4<float>(), GE = zero4<float>(), T = eye4<float>(), E_f = zero4<float>();
   V4<float> g = mk4<float>(0, 0, 0, 0), v_f = mk4<float>(0, 0, 0, 0);
-  if (act) {
+  if constexpr (PF == 2) {
+    // the walk of k_lines<W, 0> with each lane's records staged SUB_SD cells ahead (the same arithmetic)
+    const bool di = dir_i != 0;
+    if (has_sep) {
+      const long long cs = cell(e - 1);
+      const Rec r = line_rec(A, di, cs);
+      cp_m4(&ssep[0][lane], r.blk(F_LO));
+      cp_m4(&ssep[4][lane], r.blk(F_D));
+      cp_m4(&ssep[8][lane], r.blk(F_UP));
+      cp16(&ssep[12][lane], in + cs);
+      if (from_res) cp4(&ssep_dt[lane], A.dt + cs);
+    }
+    cp_commit();
+    const int nk = act ? ke - a + 1 : 0, mk = G.m;
+    auto issue_f = [&](int k, int slot) {
+      const long long cc = cell(a + k);
+      const Rec r = line_rec(A, di, cc);
+      cp_m4(&stg[slot][0][lane], r.blk(F_LO));
+      cp_m4(&stg[slot][4][lane], r.blk(F_D));
+      cp_m4(&stg[slot][8][lane], r.blk(F_UP));
+      cp16(&stg[slot][12][lane], in + cc);
+      if (from_res) cp4(&stg_dt[slot][lane], A.dt + cc);
+    };
+#pragma unroll
+    for (int q = 0; q < SUB_SD; ++q) {
+      if (q < nk) issue_f(q, q);
+      cp_commit();
+    }
+    for (int kk = 0; kk < mk; ++kk) {
+      cp_wait<SUB_SD - 1>();
+      const int slot = kk % SUB_SD;
+      if (kk < nk) {
+        const int k = a + kk;
+        const Rec rec_k = line_rec(A, di, cell(k));
+        const M4<float> Ak = ld_m4s(&stg[slot][0][lane]), Bk = ld_m4s(&stg[slot][4][lane]), Ck = ld_m4s(&stg[slot][8][lane]);
+        V4<float> r = from_f4(stg[slot][12][lane]);
+        if (from_res) {
+          float d = stg_dt[slot][lane];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) r[q] *= d;
+        }
+        M4<float> M = Bk;
+        M4<float> GEr;
+        if (k > a) {
+          axpy(M, -1.f, mm(Ak, Y));
+          V4<float> t = mv(Ak, g);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) r[q] -= t[q];
+          GEr = mm(Ak, GE);
+        } else {
+          GEr = Ak;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) GEr[q] = -GEr[q];
+        M4<float> Minv = inv4(M);
+        g = mv(Minv, r);
+        GE = mm(Minv, GEr);
+        Y = mm(Minv, Ck);
+        st_m4(rec_k.blk(F_MINV), Minv);
+        st_m4(rec_k.blk(F_Y), Y);
+        st_m4(rec_k.blk(F_GE), GE);
+        st_m4(rec_k.blk(F_T), T);
+        *rec_k.g() = to_f4(g);
+        const V4<float> tg = mv(T, g);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v_f[q] += tg[q];
+        axpy(E_f, 1.f, mm(T, GE));
+        T = mm(T, Y);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) T[q] = -T[q];
+      }
+      __syncwarp();
+      if (kk + SUB_SD < nk) issue_f(kk + SUB_SD, slot);
+      cp_commit();
+    }
+  } else if (act) {
     Rec rec = line_rec(A, dir_i != 0, cell(a));
     M4<float> An, Bn, Cn;
     V4<float> rn;
-    if (PF) {
+    if (PF == 1) {
       An = ld_m4(rec.blk(F_LO)), Bn = ld_m4(rec.blk(F_D)), Cn = ld_m4(rec.blk(F_UP));
       rn = rhs_of(A, in, from_res != 0, cell(a));
     }
     for (int k = a; k <= ke; ++k) {
-      if (!PF) {
+      if (PF == 0) {
         rec = line_rec(A, dir_i != 0, cell(k));
         An = ld_m4(rec.blk(F_LO)), Bn = ld_m4(rec.blk(F_D)), Cn = ld_m4(rec.blk(F_UP));
         rn = rhs_of(A, in, from_res != 0, cell(k));
@@ -611,7 +727,7 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
       const M4<float> Ak = An, Bk = Bn, Ck = Cn;
       V4<float> r = rn;
       const Rec rec_k = rec;
-      if (PF && k < ke) {
+      if (PF == 1 && k < ke) {
         const long long cn = cell(k + 1);
         rec = line_rec(A, dir_i != 0, cn);
         An = ld_m4(rec.blk(F_LO)), Bn = ld_m4(rec.blk(F_D)), Cn = ld_m4(rec.blk(F_UP));
@@ -669,9 +785,21 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   M4<float> ra = zero4<float>(), rb = eye4<float>(), rc = zero4<float>();
   V4<float> rd = mk4<float>(0, 0, 0, 0);
   if (has_sep) {
-    Rec rec = line_rec(A, dir_i != 0, cell(e - 1));
-    M4<float> As = ld_m4(rec.blk(F_LO)), Bs = ld_m4(rec.blk(F_D)), Cs = ld_m4(rec.blk(F_UP));
-    V4<float> r = rhs_of(A, in, from_res != 0, cell(e - 1));
+    M4<float> As, Bs, Cs;
+    V4<float> r;
+    if constexpr (PF == 2) {
+      As = ld_m4s(&ssep[0][lane]), Bs = ld_m4s(&ssep[4][lane]), Cs = ld_m4s(&ssep[8][lane]);
+      r = from_f4(ssep[12][lane]);
+      if (from_res) {
+        float d = ssep_dt[lane];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) r[k] *= d;
+      }
+    } else {
+      Rec rec = line_rec(A, dir_i != 0, cell(e - 1));
+      As = ld_m4(rec.blk(F_LO)), Bs = ld_m4(rec.blk(F_D)), Cs = ld_m4(rec.blk(F_UP));
+      r = rhs_of(A, in, from_res != 0, cell(e - 1));
+    }
     const PcrSlot* nx = &sp[warp][s + 1];
     M4<float> En, Fn;
     V4<float> vn;
@@ -766,6 +894,51 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   }
   sl[warp][s] = to_f4(lsep);
   __syncwarp();
+  if constexpr (PF == 2) {
+    // the back substitution with Y, GE and g (this lane's own forward results) staged SUB_SD cells ahead
+    const bool di = dir_i != 0;
+    V4<float> lprev = s > 0 ? from_f4(sl[warp][s - 1]) : mk4<float>(0, 0, 0, 0);
+    V4<float> xn = has_sep ? lsep : mk4<float>(0, 0, 0, 0);
+    if (has_sep) line_emit(A, epilogue, update, out, cell(e - 1), lsep);
+    const int nk = act ? ke - a + 1 : 0, mk = G.m;
+    auto issue_b = [&](int k, int slot) {
+      const Rec r = line_rec(A, di, cell(ke - k));
+      cp_m4(&stg[slot][0][lane], r.blk(F_Y));
+      cp_m4(&stg[slot][4][lane], r.blk(F_GE));
+      cp16(&stg[slot][8][lane], r.g());
+    };
+    __threadfence_block();  // the forward walk's stores before the copies that read them back
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < SUB_SD; ++q) {
+      if (q < nk) issue_b(q, q);
+      cp_commit();
+    }
+    for (int kk = 0; kk < mk; ++kk) {
+      cp_wait<SUB_SD - 1>();
+      const int slot = kk % SUB_SD;
+      if (kk < nk) {
+        const long long cc = cell(ke - kk);
+        const M4<float> Yk = ld_m4s(&stg[slot][0][lane]), GEk = ld_m4s(&stg[slot][4][lane]);
+        const V4<float> gk = from_f4(stg[slot][8][lane]);
+        V4<float> t1 = mv(GEk, lprev), t2 = mv(Yk, xn);
+        V4<float> x;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = gk[q] + t1[q] - t2[q];
+        line_emit(A, epilogue, update, out, cc, x);
+        xn = x;
+      }
+      __syncwarp();
+      if (kk + SUB_SD < nk) issue_b(kk + SUB_SD, slot);
+      cp_commit();
+    }
+    cp_wait<0>();
+    if (update && L == 0 && lane == 0) {
+      A.iter[ci] += 1;
+      A.ramp_k[ci] += 1;
+    }
+    return;
+  }
   if (!act) return;
   // ---- back substitution of the segment
   V4<float> lprev = s > 0 ? from_f4(sl[warp][s - 1]) : mk4<float>(0, 0, 0, 0);
@@ -775,9 +948,9 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
   Rec recb = line_rec(A, dir_i != 0, cn);
   M4<float> Yn, GEn;
   float4 gn;
-  if (PF) Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE)), gn = *recb.g();
+  if (PF == 1) Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE)), gn = *recb.g();
   for (int k = ke; k >= a; --k) {
-    if (!PF) {
+    if (PF == 0) {
       cn = cell(k);
       recb = line_rec(A, dir_i != 0, cn);
       Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE)), gn = *recb.g();
@@ -785,7 +958,7 @@ __global__ void __launch_bounds__(32 * W) k_lines(Arena A, int dir_i, const floa
     const long long cc = cn;
     const M4<float> Yk = Yn, GEk = GEn;
     const V4<float> gk = from_f4(gn);
-    if (PF && k > a) {
+    if (PF == 1 && k > a) {
       cn = cell(k - 1);
       recb = line_rec(A, dir_i != 0, cn);
       Yn = ld_m4(recb.blk(F_Y)), GEn = ld_m4(recb.blk(F_GE));
@@ -955,37 +1128,12 @@ __global__ void __launch_bounds__(32 * W) k_lines_subst(Arena A, int dir_i, cons
 // passes when few lines are left (a lane's segment of a handful of cells is a chain of dependent loads otherwise). One
 // line per block, 47 KB of shared memory. Every lane copies and reads only its own slots, so the copies need no barrier
 // across the warp; the __syncwarp before each refill orders a slot's reads before the copy that overwrites it.
-constexpr int SUB_SD = 3;
 struct SubstStage {
   float4 w[SUB_SD][13][32];  // forward: lo 0-3, M^-1 4-7, T 8-11, r 12; backward: GE 0-3, Y 4-7, g 8, du 9, U 10, Ulo 11
   float4 p[PREC][32];        // the lane's reduction multipliers
   float4 sp[9][32];          // the separator row: lo 0-3, up 4-7, r 8
 };
 static_assert(sizeof(SubstStage) <= 48 * 1024, "static shared memory");
-__device__ __forceinline__ void cp16(float4* smem, const float4* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-// a 4x4 block whose rows lie 32 float4 apart (one lane's slots of a staging array)
-__device__ __forceinline__ M4<float> ld_m4s(const float4* p) {
-  M4<float> m;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    float4 v = p[32 * q];
-    m[4 * q] = v.x, m[4 * q + 1] = v.y, m[4 * q + 2] = v.z, m[4 * q + 3] = v.w;
-  }
-  return m;
-}
-__device__ __forceinline__ void cp_m4(float4* smem, const float4* gmem) {
-#pragma unroll
-  for (int q = 0; q < 4; ++q) cp16(smem + 32 * q, gmem + q);
-}
-
 // The defect-correction pass of k_lines_subst (same arithmetic, same results) with the staged records.
 __global__ void __launch_bounds__(32) k_lines_subst_st(Arena A, int dir_i, const float4* in, float4* out, int pass) {
   __shared__ SubstStage S;

@@ -872,11 +872,12 @@ struct ArenaHost {
   // how the substitution walks fetch their records: 0 one cell at a time, 1 the next cell's ahead (registers), 2 staged
   // through shared memory SUB_SD cells ahead (one line per block, lw_subst not used)
   int pf_subst[2] = {0, 0};
-  // A direction with at most this many lines in the launch runs its substitution passes staged (pf_subst 2) whatever
-  // pf_subst says: with few lines the passes wait on memory latency, not bandwidth, and the staged walks wait once per
-  // SUB_SD cells. Set at setup to two waves of the staged kernel (its blocks per SM x SMs x 2); 0 never.
+  // A direction with at most this many lines in the launch runs its line solves staged (pf_lines / pf_subst 2) whatever
+  // pf_lines / pf_subst say: with few lines the walks wait on memory latency, not bandwidth, and the staged walks wait
+  // once per SUB_SD cells. Set at setup to two waves of the staged substitution kernel (its blocks per SM x SMs x 2); 0
+  // never.
   int staged_lines = 0;
-  template <bool PF>
+  template <int PF>
   void launch_lines_pf(int dir_i, int w, const float4* in, int from_res, float4* out) {
     const int nl = LI(dir_i);
     const int nb = (nl + w - 1) / w;
@@ -888,10 +889,12 @@ struct ArenaHost {
   }
   void launch_lines(int dir_i, const float4* in, int from_res, float4* out) {
     const int d = dir_i ? 1 : 0, w = lw_lines[d] > 4 ? 4 : lw_lines[d];
-    if (pf_lines[d])
-      launch_lines_pf<true>(dir_i, w, in, from_res, out);
+    if (pf_lines[d] == 2 || LI(dir_i) <= staged_lines)
+      k_lines<1, 2><<<LI(dir_i), 32, 0, stream>>>(A, dir_i, in, from_res, out);
+    else if (pf_lines[d])
+      launch_lines_pf<1>(dir_i, w, in, from_res, out);
     else
-      launch_lines_pf<false>(dir_i, w, in, from_res, out);
+      launch_lines_pf<0>(dir_i, w, in, from_res, out);
   }
   template <bool PF>
   void launch_subst_pf(int dir_i, int w, const float4* in, float4* out, int pass) {
@@ -966,8 +969,8 @@ struct ArenaHost {
     // load every candidate kernel now (lazy module loading would otherwise charge a variant's first launch)
     {
       cudaFuncAttributes fa;
-      const void* fns[] = {(const void*)&k_lines<1, false>, (const void*)&k_lines<2, false>, (const void*)&k_lines<4, false>,
-                           (const void*)&k_lines<1, true>, (const void*)&k_lines<2, true>, (const void*)&k_lines<4, true>,
+      const void* fns[] = {(const void*)&k_lines<1, 0>, (const void*)&k_lines<2, 0>, (const void*)&k_lines<4, 0>,
+                           (const void*)&k_lines<1, 1>, (const void*)&k_lines<2, 1>, (const void*)&k_lines<4, 1>,
                            (const void*)&k_lines_subst<1, false>, (const void*)&k_lines_subst<2, false>,
                            (const void*)&k_lines_subst<4, false>, (const void*)&k_lines_subst<8, false>,
                            (const void*)&k_lines_subst<1, true>, (const void*)&k_lines_subst<2, true>,
@@ -994,7 +997,7 @@ struct ArenaHost {
       for (int w : cand) {
         if (pf && w > 4) continue;
         lw_lines[0] = lw_lines[1] = lw_subst[0] = lw_subst[1] = lw_turb = w;
-        pf_lines[0] = pf_lines[1] = pf_subst[0] = pf_subst[1] = pf;
+        pf_lines[0] = pf_lines[1] = pf_subst[0] = pf_subst[1] = pf;  // the staged variants (2) are chosen by staged_lines
         if ((rc = profile(1))) return rc;
         for (int q = 0; q < 5; ++q) {
           if (q == 4 && pf) continue;  // the SST line kernel has no prefetching variant

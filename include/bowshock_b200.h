@@ -311,13 +311,13 @@ int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* 
 /* Launch shapes of the arena's kernels. At creation (arenas of 100,000 cells or more; otherwise 4 lines per block, no
  * prefetching, variant 0) the autotuner picks, each the fastest in one timed iteration of the arena's own cases per
  * candidate (the state restored afterwards): per direction, lines per block (1, 2 or 4) of the block line solves' first
- * pass and whether its walks prefetch the next cell's record (0 / 1), lines per block (1, 2, 4 or 8) of their
- * substitution passes and how those walks fetch their records (0: one cell at a time, 1: the next cell's ahead; 2,
- * staged through shared memory three cells ahead with one line per block, only when pinned), lines per block of the
- * SST line kernel, and the residual kernel's variant (0: 256 threads per 32 x 8 tile, 1: 288). A direction with at
- * most staged_lines lines left in the launch (set at creation to two waves of the staged kernel: 1,184 lines on a
- * 148-SM B200; >= 0, 0 never) runs its substitution passes staged whatever subst_prefetch says: with few lines they
- * wait on memory latency. Every candidate compiles to the same arithmetic (checked bit for bit), so none of these
+ * pass and how its walks fetch the cells' records (0: one cell at a time, 1: the next cell's ahead; 2, staged through
+ * shared memory three cells ahead with one line per block, only when pinned), lines per block (1, 2, 4 or 8) of their
+ * substitution passes and how those walks fetch their records (0 / 1 / 2 likewise), lines per block of the SST line
+ * kernel, and the residual kernel's variant (0: 256 threads per 32 x 8 tile, 1: 288). A direction with at most
+ * staged_lines lines left in the launch (set at creation to two waves of the staged substitution kernel: 1,184 lines on
+ * a 148-SM B200; >= 0, 0 never) runs both passes staged whatever prefetch / subst_prefetch say: with few lines the
+ * walks wait on memory latency. Every candidate compiles to the same arithmetic (checked bit for bit), so none of these
  * changes a result. The smallest segment a lane eliminates per direction (segment_i / segment_j: 2, 4 or 8 cells;
  * fewer separators on short lines) is 2 unless pinned: it changes the rounding of the line solves. No counterpart in
  * the reference (its line solves run in Luma, gpu/implicit.rs:731-732). */

@@ -97,7 +97,7 @@ def test_longer_line_segments_match_the_oracle(segment):
 
 def test_autotuner_candidates_give_bit_identical_states():
     """Every launch shape the autotuner may pick (lines per block and prefetching of the first pass and of the
-    substitution passes, the substitution walks staged through shared memory, lines per block of the SST line kernel,
+    substitution passes, the walks of both passes staged through shared memory, lines per block of the SST line kernel,
     the residual kernel's threads per tile) compiles to the same
     arithmetic, so the state after a run does not depend on the tuning: checked bit for bit on a mixed Euler / SST arena."""
     from bowshock_b200.arena import Arena
@@ -107,7 +107,8 @@ def test_autotuner_candidates_give_bit_identical_states():
                 residual=0, subst_prefetch_i=0, subst_prefetch_j=0, staged_lines=0)
     variants = [dict(residual=1), dict(lines_i=1, lines_j=2, prefetch_i=1, prefetch_j=1), dict(subst_i=1, subst_j=8),
                 dict(subst_prefetch_i=1, subst_prefetch_j=1), dict(subst_i=1, subst_j=8, subst_prefetch_i=1, subst_prefetch_j=1),
-                dict(subst_prefetch_i=2, subst_prefetch_j=2), dict(subst_prefetch_i=2), dict(staged_lines=1 << 20),
+                dict(subst_prefetch_i=2, subst_prefetch_j=2), dict(subst_prefetch_i=2), dict(prefetch_i=2, prefetch_j=2),
+                dict(staged_lines=1 << 20),
                 dict(turb_lines=1), dict(turb_lines=8)]
     ref = None
     for v in [dict()] + variants:
