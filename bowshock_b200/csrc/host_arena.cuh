@@ -313,6 +313,12 @@ struct ArenaHost {
   std::vector<HostCase> cases;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // With few lines left, the captured iteration runs the SST chain up to its final step on a second branch of the graph,
+  // beside the mean-flow line solves (both read this iteration's primitives, fluxes and time step; neither writes what
+  // the other reads until k_turb_update, which joins them).
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool capturing = false;
   std::string err;
   bool ready = false;
   int slots = 256;  // residual history slots per chunk
@@ -361,6 +367,9 @@ struct ArenaHost {
     d_iter = d_ramp = d_active = d_tile_case = d_iline = d_jline = d_pblk = nullptr;
     A = Arena{};
     if (stream) cudaStreamDestroy(stream), stream = nullptr;
+    if (side) cudaStreamDestroy(side), side = nullptr;
+    if (ev_fork) cudaEventDestroy(ev_fork), ev_fork = nullptr;
+    if (ev_join) cudaEventDestroy(ev_join), ev_join = nullptr;
     ready = false;
   }
 
@@ -413,6 +422,9 @@ struct ArenaHost {
     release();
     BK_CUDA(cudaSetDevice(device));
     BK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    BK_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    BK_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    BK_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     const int nc = (int)cases.size();
     desc.resize(nc);
     ncell = npad = nif = njf = 0;
@@ -1048,6 +1060,16 @@ struct ArenaHost {
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { launch_residual(2, slot); });
       const int s = sub_iters_of_arena();
+      // the SST chain on the graph's second branch (only the warp-per-line SST kernel: the thread-per-line one borrows
+      // the line records)
+      const bool fork = any_sst && capturing && !profiling && max_line <= 32 * TL_MAXM && LI(1) <= staged_lines &&
+                        LI(0) <= staged_lines;
+      if (fork) {
+        cudaEventRecord(ev_fork, stream);
+        cudaStreamWaitEvent(side, ev_fork, 0);
+        launch_turb_chain(side, slot);
+        cudaEventRecord(ev_join, side);
+      }
       L(G_ASSEMBLE, [&] {
         k_assemble<<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
       });
@@ -1060,7 +1082,10 @@ struct ArenaHost {
         L(G_SUBST_J, [&] { launch_subst(0, A.X, nullptr, p); });
       }
       if (any_sst) {
-        launch_turb_chain(stream, slot);
+        if (fork)
+          cudaStreamWaitEvent(stream, ev_join, 0);
+        else
+          launch_turb_chain(stream, slot);
         L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
       }
     } else {
@@ -1113,7 +1138,9 @@ struct ArenaHost {
       BK_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream);
       if (any_sst) cudaMemsetAsync(A.tsum, 0, (size_t)chunk * nc * sizeof(double), stream);
+      capturing = true;
       for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      capturing = false;
       cudaError_t le = cudaGetLastError();
       BK_CUDA(cudaStreamEndCapture(stream, &g));
       if (le != cudaSuccess) {
