@@ -57,6 +57,7 @@ struct Arena {
   const float4 *iface, *jface, *cellg;
   const float2 *ifc, *jfc;  // face centres (mean of the end nodes)
   float* scratch;  // line-solve records (fv_kernels.cu: line_rec, pcr_rec)
+  float4* lend;    // ghost Jacobian T of every line end, 4 float4 each (fv_kernels.cu: lend_slot)
   long long ncell;
   double* rsum;    // sum of R_rho^2, [slot * ncases + case]
   const int* tile_case;

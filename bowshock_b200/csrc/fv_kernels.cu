@@ -5,7 +5,7 @@
 //               time step, and the FP64 density-residual norm (block reduce + one atomic per block)   (solver.rs:474-654)
 //   k_stage     SSP-RK3 stage update                                                   (solver.rs:694-720)
 //   k_assemble  blocks (lo, d, up) of I - dt J_i and I - dt J_j of every cell into its two line records
-//               (implicit.rs:284-438); k_line_ends folds the line-end ghost Jacobians in (implicit.rs:440-467)
+//               (implicit.rs:284-438); k_line_ends_T / _fold fold the line-end ghost Jacobians in (implicit.rs:440-467)
 //   k_lines     line-implicit solve of (I - dt J_dir) x = b along every i or j line: one warp per line, a partitioned
 //               block-tridiagonal (4x4) solver — each lane eliminates its own segment, the separator unknowns form a
 //               reduced block-tridiagonal system solved by parallel cyclic reduction across the warp through shared
@@ -347,7 +347,7 @@ __device__ __forceinline__ V4<float> rhs_of(const Arena& A, const float4* in, bo
 // then for every line and lane of the reduced separator system 44 float4 = 5 PCR levels x (alpha, gamma) + b^-1.
 // A plane keeps one field of consecutive cells contiguous: the per-cell kernels (assembly, defect) store and load whole
 // sectors across a warp, and a lane walking its segment of an i line reads consecutive 64-byte blocks.
-// The first pass of an iteration assembles and factorises (k_assemble, k_line_ends, k_lines); later passes
+// The first pass of an iteration assembles and factorises (k_assemble, k_line_ends_fold, k_lines); later passes
 // (k_lines_subst) and the defect (k_defect) only read them.
 enum { F_LO = 0, F_D, F_UP, F_MINV, F_Y, F_GE, F_T, F_G };
 constexpr int REC = 29, PREC = 44, PCR_LEVELS = 5;  // REC: float4 per cell and direction
@@ -484,19 +484,20 @@ __global__ void __launch_bounds__(TI* TJ, 3) k_assemble(Arena A) {
 
 // Ghost Jacobians of the two ends of line `L` folded into the diagonal blocks (implicit.rs:440-467): at the first cell
 // d += lo T and lo = 0, with T the wall reflection / no-slip, the jet's zero, or the far-field ghost Jacobian (FP64 finite
-// differences); at the last cell d += up T and up = 0. One thread per line end (`ends` bit 0: first, bit 1: last; a line
-// of one cell has both ends in one thread), after k_assemble.
-__device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int L, int ends) {
+// differences); at the last cell d += up T and up = 0. In two launches: k_line_ends_T computes every end's T from the
+// primitives alone (so it can run beside the residual and the assembly), k_line_ends_fold folds them in after k_assemble.
+
+// T of end `end` (0 first, 1 last) of line L; zero where the line has no fluid cell
+__device__ __forceinline__ M4<float> line_end_T(const Arena& A, const CaseDev& c, bool dir_i, int L, int end) {
   const int n = dir_i ? c.ni : c.nj;
   const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
-  if (k0 >= n) return;
-  if (ends & 1) {
+  M4<float> T = zero4<float>();
+  if (k0 >= n) return T;
+  if (end == 0) {
     const int i = dir_i ? k0 : L, j = dir_i ? L : k0;
-    const long long cc = cidx(c, i, j);
     float4 fl = dir_i ? A.iface[ifidx(c, i, j)] : A.jface[jfidx(c, i, j)];
     bool wall_lower = k0 > 0;
     bool jet = wall_lower && dir_i && jet_iface(c, k0, j);
-    M4<float> T;
     if (jet) {
       T = zero4<float>();
     } else if (wall_lower) {
@@ -514,17 +515,9 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
         for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
       }
     }
-    Rec rec = line_rec(A, dir_i, cc);
-    M4<float> d = ld_m4(rec.blk(F_D));
-    axpy(d, 1.f, mm(ld_m4(rec.blk(F_LO)), T));
-    st_m4(rec.blk(F_LO), zero4<float>());
-    st_m4(rec.blk(F_D), d);
-  }
-  if (ends & 2) {
+  } else {
     const int i = dir_i ? n - 1 : L, j = dir_i ? L : n - 1;
-    const long long cc = cidx(c, i, j);
     float4 fr = dir_i ? A.iface[ifidx(c, i + 1, j)] : A.jface[jfidx(c, i, j + 1)];
-    M4<float> T;
     if (!c.implicit_bc) {
       T = zero4<float>();
     } else {
@@ -532,22 +525,49 @@ __device__ void fold_line_ends(const Arena& A, const CaseDev& c, bool dir_i, int
 #pragma unroll
       for (int q = 0; q < 16; ++q) T[q] = (float)Td[q];
     }
-    Rec rec = line_rec(A, dir_i, cc);
-    M4<float> d = ld_m4(rec.blk(F_D));
-    axpy(d, 1.f, mm(ld_m4(rec.blk(F_UP)), T));
-    st_m4(rec.blk(F_UP), zero4<float>());
-    st_m4(rec.blk(F_D), d);
   }
+  return T;
 }
-
-// two threads per line (first end, last end): every i line, then every j line, of the active cases
-__global__ void k_line_ends(Arena A) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = t & 1, l = t >> 1;
-  const int nli = lines_of(A, true);
-  const bool dir_i = l < nli;
-  const int gw = line_at(A, dir_i, dir_i ? l : l - nli);
-  if (gw < 0) return;
+// d += lo T, lo = 0 (first end) or d += up T, up = 0 (last end) in the end cell's line record
+__device__ __forceinline__ void fold_line_end(const Arena& A, const CaseDev& c, bool dir_i, int L, int end, const M4<float>& T) {
+  const int n = dir_i ? c.ni : c.nj;
+  const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
+  if (k0 >= n) return;
+  const int k = end == 0 ? k0 : n - 1;
+  const long long cc = dir_i ? cidx(c, k, L) : cidx(c, L, k);
+  const int f = end == 0 ? F_LO : F_UP;
+  Rec rec = line_rec(A, dir_i, cc);
+  M4<float> d = ld_m4(rec.blk(F_D));
+  axpy(d, 1.f, mm(ld_m4(rec.blk(f)), T));
+  st_m4(rec.blk(f), zero4<float>());
+  st_m4(rec.blk(F_D), d);
+}
+// the slot of end `end` of global line gw in A.lend (4 float4 per end; i lines first)
+__device__ __forceinline__ float4* lend_slot(const Arena& A, bool dir_i, int gw, int end) {
+  return A.lend + ((long long)(dir_i ? gw : A.nilines + gw) * 2 + end) * 4;
+}
+// thread t: line t / 2 of the launch (every i line, then every j line, of the active cases), end t % 2
+__device__ __forceinline__ bool line_end_of(const Arena& A, int t, bool& dir_i, int& gw, int& e) {
+  e = t & 1;
+  const int l = t >> 1, nli = lines_of(A, true);
+  dir_i = l < nli;
+  gw = line_at(A, dir_i, dir_i ? l : l - nli);
+  return gw >= 0;
+}
+__global__ void k_line_ends_T(Arena A) {
+  bool dir_i;
+  int gw, e;
+  if (!line_end_of(A, blockIdx.x * blockDim.x + threadIdx.x, dir_i, gw, e)) return;
+  const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  const int L = gw - (dir_i ? c.iline_off : c.jline_off);
+  st_m4(lend_slot(A, dir_i, gw, e), line_end_T(A, c, dir_i, L, e));
+}
+__global__ void k_line_ends_fold(Arena A) {
+  bool dir_i;
+  int gw, e;
+  if (!line_end_of(A, blockIdx.x * blockDim.x + threadIdx.x, dir_i, gw, e)) return;
   const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
   const CaseDev& c = A.cases[ci];
   if (!A.active[ci]) return;
@@ -555,10 +575,13 @@ __global__ void k_line_ends(Arena A) {
   const int n = dir_i ? c.ni : c.nj;
   const int k0 = dir_i ? row_start(c, L) : col_start(c, L);
   if (n - k0 == 1) {  // one cell: both ends in the first thread (the two folds update the same diagonal block)
-    if (e == 0) fold_line_ends(A, c, dir_i, L, 3);
+    if (e == 0) {
+      fold_line_end(A, c, dir_i, L, 0, ld_m4(lend_slot(A, dir_i, gw, 0)));
+      fold_line_end(A, c, dir_i, L, 1, ld_m4(lend_slot(A, dir_i, gw, 1)));
+    }
     return;
   }
-  fold_line_ends(A, c, dir_i, L, e ? 2 : 1);
+  fold_line_end(A, c, dir_i, L, e, ld_m4(lend_slot(A, dir_i, gw, e)));
 }
 
 // cp.async copies of 16 (or 4) bytes from global into shared memory, one commit group per call of cp_commit; cp_wait<N>
@@ -593,7 +616,7 @@ __device__ __forceinline__ void cp_m4(float4* smem, const float4* gmem) {
   for (int q = 0; q < 4; ++q) cp16(smem + 32 * q, gmem + q);
 }
 
-// First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble and k_line_ends left in the line records, factorise
+// First pass of an iteration (implicit.rs:619-621): with the blocks k_assemble and k_line_ends_fold left in the line records, factorise
 // with the partitioned solver (each lane eliminates its segment, the separator unknowns form a
 // reduced 4x4-block tridiagonal system solved by parallel cyclic reduction through shared memory, each lane
 // back-substitutes), solve for the first right-hand side, and keep blocks, factors and reduction multipliers in the line

@@ -317,7 +317,7 @@ struct ArenaHost {
   // beside the mean-flow line solves (both read this iteration's primitives, fluxes and time step; neither writes what
   // the other reads until k_turb_update, which joins them).
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ends = nullptr;
   bool capturing = false;
   std::string err;
   bool ready = false;
@@ -358,7 +358,8 @@ struct ArenaHost {
     void* ptrs[] = {d_cases, d_iter, d_ramp, d_active, d_tile_case, d_iline, d_jline, d_pblk, A.U, A.W, A.R, A.X, A.DU, A.RR, A.U0, A.Ulo, A.Wlo, A.U0lo, A.MG0lo,
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
                     A.grad4, A.gradT, A.mu, A.mu_t, A.rough, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
-                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled, d_tlist, d_pblist, d_illist, d_jllist};
+                    A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled, d_tlist, d_pblist, d_illist, d_jllist,
+                    A.lend};
     d_enabled = nullptr;
     d_tlist = d_pblist = d_illist = d_jllist = nullptr;
     for (void* p : ptrs)
@@ -370,6 +371,7 @@ struct ArenaHost {
     if (side) cudaStreamDestroy(side), side = nullptr;
     if (ev_fork) cudaEventDestroy(ev_fork), ev_fork = nullptr;
     if (ev_join) cudaEventDestroy(ev_join), ev_join = nullptr;
+    if (ev_ends) cudaEventDestroy(ev_ends), ev_ends = nullptr;
     ready = false;
   }
 
@@ -425,6 +427,7 @@ struct ArenaHost {
     BK_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
     BK_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     BK_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    BK_CUDA(cudaEventCreateWithFlags(&ev_ends, cudaEventDisableTiming));
     const int nc = (int)cases.size();
     desc.resize(nc);
     ncell = npad = nif = njf = 0;
@@ -500,6 +503,7 @@ struct ArenaHost {
     A.ifc = ic;
     A.jfc = jc;
     ALLOC(A.scratch, scratch_floats());
+    ALLOC(A.lend, (size_t)8 * (nil + njl));
     ALLOC(A.rsum, (size_t)slots * nc);
     ALLOC(A.tsum, (size_t)slots * nc);
     ALLOC(d_enabled, nc);
@@ -1057,7 +1061,23 @@ struct ArenaHost {
       mg_level(0, slot);
       set_level(0);
     } else if (scheme_of_arena() == SCHEME_IMPLICIT) {
-      launch_mean_flow_prep();
+      // the line ends' ghost Jacobians need only the primitives: in a captured iteration they run on the graph's second
+      // branch beside the viscous terms, the residual and the assembly
+      const int nle = 2 * (LI(1) + LI(0));
+      const bool fork_ends = capturing && !profiling;
+      L(G_PRIMS, [&] { k_prims<<<LP(), 256, 0, stream>>>(A); });
+      if (fork_ends) {
+        cudaEventRecord(ev_fork, stream);
+        cudaStreamWaitEvent(side, ev_fork, 0);
+        k_line_ends_T<<<(nle + 127) / 128, 128, 0, side>>>(A);
+        cudaEventRecord(ev_ends, side);
+      } else {
+        L(G_ASSEMBLE, [&] { k_line_ends_T<<<(nle + 127) / 128, 128, 0, stream>>>(A); });
+      }
+      if (any_viscous) {
+        L(G_VISC, [&] { k_visc_cell<<<LT(), TI * TJ, 0, stream>>>(A); });
+        L(G_VISC, [&] { k_visc_face<<<LT(), TI * TJ, 0, stream>>>(A); });
+      }
       L(G_RESIDUAL, [&] { launch_residual(2, slot); });
       const int s = sub_iters_of_arena();
       // the SST chain on the graph's second branch (only the warp-per-line SST kernel: the thread-per-line one borrows
@@ -1073,7 +1093,8 @@ struct ArenaHost {
       L(G_ASSEMBLE, [&] {
         k_assemble<<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
       });
-      L(G_ASSEMBLE, [&] { k_line_ends<<<(2 * (LI(1) + LI(0)) + 127) / 128, 128, 0, stream>>>(A); });
+      if (fork_ends) cudaStreamWaitEvent(stream, ev_ends, 0);
+      L(G_ASSEMBLE, [&] { k_line_ends_fold<<<(nle + 127) / 128, 128, 0, stream>>>(A); });
       L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
       L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
       for (int p = 1; p < s; ++p) {
