@@ -695,7 +695,6 @@ int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) 
   auto w4 = [](int32_t w) { return w == 1 || w == 2 || w == 4; };
   auto w8 = [](int32_t w) { return w == 1 || w == 2 || w == 4 || w == 8; };
   auto m8 = [](int32_t m) { return m == 2 || m == 4 || m == 8; };
-  auto b01 = [](int32_t b) { return b == 0 || b == 1; };
   auto b012 = [](int32_t b) { return b >= 0 && b <= 2; };
   if (!(w4(t->lines_i) && w4(t->lines_j) && b012(t->prefetch_i) && b012(t->prefetch_j) && w8(t->subst_i) && w8(t->subst_j) &&
         w8(t->turb_lines) && m8(t->segment_i) && m8(t->segment_j) && (t->residual == 0 || t->residual == 1) &&

@@ -313,9 +313,9 @@ struct ArenaHost {
   std::vector<HostCase> cases;
   int device = 0;
   cudaStream_t stream = nullptr;
-  // With few lines left, the captured iteration runs the SST chain up to its final step on a second branch of the graph,
-  // beside the mean-flow line solves (both read this iteration's primitives, fluxes and time step; neither writes what
-  // the other reads until k_turb_update, which joins them).
+  // The captured iteration runs the SST chain up to its final step on a second branch of the graph, beside the
+  // mean-flow line solves (both read this iteration's primitives, fluxes and time step; neither writes what the other
+  // reads until k_turb_update, which joins them), and the line ends' ghost Jacobians beside the residual.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ends = nullptr;
   bool capturing = false;
@@ -1082,8 +1082,7 @@ struct ArenaHost {
       const int s = sub_iters_of_arena();
       // the SST chain on the graph's second branch (only the warp-per-line SST kernel: the thread-per-line one borrows
       // the line records)
-      const bool fork = any_sst && capturing && !profiling && max_line <= 32 * TL_MAXM && LI(1) <= staged_lines &&
-                        LI(0) <= staged_lines;
+      const bool fork = any_sst && capturing && !profiling && max_line <= 32 * TL_MAXM;
       if (fork) {
         cudaEventRecord(ev_fork, stream);
         cudaStreamWaitEvent(side, ev_fork, 0);
