@@ -14,7 +14,11 @@ Metric: converged cases per hour on one B200 at |dCD| <= 1e-4 against the FP64 o
   plain         the plain single-case backend: each case alone through GpuSolver.run_to_stop (same kernels, one case per
                 launch), wall clock, reported as config.plain_single_case_cases_per_hr.
   cpu_baseline  the oracle (f64 C++ restatement of the reference CPU path, all host threads) timed on a bounded sample of
-                iterations of every case, times the oracle's own iteration counts to its stop rules.
+                iterations of every case, times the oracle's own iteration counts to its stop rules (one GPU only).
+  --gpus N      one process per GPU (started here through torch.distributed.run unless launched by it): the 32 cases are
+                partitioned over the ranks (longest processing time on cells x expected iterations, bowshock_b200.shard),
+                each rank runs its share in its own arena, the point results are gathered (gloo, host objects); times
+                are the max over ranks, `scaling` "strong" (the sweep is fixed).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -97,11 +101,27 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_cases(rank=0):
-    """The 32-case sweep; every rank solves the same seeded sweep (replicas: the cases shard across GPUs with no exchange,
-    and the oracle's census of this seed checks every rank's CDs)."""
+def build_cases():
+    """The 32-case sweep (the same seeded draw on every rank; each rank solves its own share of it)."""
     from bowshock_b200.sweep import SEED, sweep_cases
     return sweep_cases(32, SEED)
+
+
+def shard(cases, grids, rank, world):
+    """This rank's case indices: the longest-processing-time partition of the sweep over the ranks by cells x expected
+    iterations (bowshock_b200.shard); every rank computes the same partition."""
+    from bowshock_b200.shard import case_cost, lpt_partition
+    return lpt_partition([case_cost(c, g) for c, g in zip(cases, grids)], world)[rank]
+
+
+def reduce_scalars(dist, values, op):
+    """(max or sum over ranks of each value); identity with one process."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t]
 
 
 def h2d_bytes(cases, grids):
@@ -123,19 +143,6 @@ def d2h_bytes(ncases, iters):
     """Bytes read back per 50-iteration chunk (density residuals, turbulence residual, FP64 forces), over the census."""
     chunks = (max(iters) + 49) // 50
     return int(chunks * (50 * ncases * 8 + ncases * 8 + ncases * 15 * 8))
-
-
-def combine_ranks(dist, ms_step, value, e2e):
-    """Cases-per-GPU replicas: the step time is the max over ranks, the throughputs add up (scalars only, no data-path
-    collective)."""
-    if dist is None:
-        return ms_step, value, e2e
-    import torch
-    t = torch.tensor([ms_step], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    s = torch.tensor([value, e2e], dtype=torch.float64)
-    dist.all_reduce(s, op=dist.ReduceOp.SUM)
-    return float(t.item()), float(s[0]), float(s[1])
 
 
 def census_fixture():
@@ -206,7 +213,7 @@ def run_reference(args, rank, world):
     and the oracle's own iteration counts to its stop rules."""
     if rank != 0:
         return None
-    cases = build_cases(0)
+    cases = build_cases()
     fx = census_fixture()
     iters, filled = oracle_iters(fx, cases)
     smp = OracleSample(cases)
@@ -234,9 +241,13 @@ def run_reference(args, rank, world):
 def run_ours(args, rank, world, dist):
     import bowshock_b200  # noqa: F401
     from bowshock_b200.arena import Arena
+    from bowshock_b200.shard import gather_results
     device = int(os.environ.get("LOCAL_RANK", "0"))
-    cases = build_cases(rank)
-    grids = [c.grid() for c in cases]
+    all_cases = build_cases()
+    all_grids = [c.grid() for c in all_cases]
+    mine = shard(all_cases, all_grids, rank, world)  # this rank's share of the sweep (all of it on one GPU)
+    cases = [all_cases[k] for k in mine]
+    grids = [all_grids[k] for k in mine]
     cells = np.array([g[0] * g[1] for g in grids], dtype=float)
     arena = Arena(cases, device=device, grids=grids)
     ncell = arena.cells
@@ -249,45 +260,45 @@ def run_ours(args, rank, world, dist):
     clocks.start()
     arena.run(args.steps)
     ms_local = arena.ms_per_iter()
-    # census: every case to its stop rule, through the public API (wall clock = e2e; device time = value)
-    cen_cases = build_cases(rank)
+    # census: this rank's cases to their stop rules, through the public API (wall clock = e2e; device time = value)
+    cen_cases = [build_cases()[k] for k in mine]
     t1 = time.perf_counter()
     cen_grids = [c.grid() for c in cen_cases]
     cen = Arena(cen_cases, device=device, grids=cen_grids)
-    results = cen.solve()
+    results_local = cen.solve()
     wall_census = time.perf_counter() - t1
     clk = clocks.stop()
     census_dev_s = cen.last_solve_ms() / 1000.0
     del cen
-    iters = [r["iters"] for r in results]
-    n_k = np.array(iters, dtype=float)
+    results = gather_results(dist, mine, [{k: v for k, v in r.items() if k != "residual"} for r in results_local], len(all_cases))
+    iters_local = np.array([r["iters"] for r in results_local], dtype=float)
     fx = census_fixture()
-    dcd = {k: cd_error(results[k], fx[k]) for k in range(len(cases)) if k in fx}
+    dcd = {k: cd_error(results[k], fx[k]) for k in range(len(all_cases)) if k in fx}
     ok = [k for k, d in dcd.items() if abs(d) <= 1e-4]
     n_ok = len(ok)
-    value_rank = 3600.0 * n_ok / census_dev_s
-    e2e_rank = 3600.0 * n_ok / wall_census
-    steady = 3600.0 * len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * n_k)))
+    steady_local = 3600.0 * len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * iters_local)))
     # per-kernel profile (CUDA events around every launch) for the roofline of the dominant kernel group
     prof = arena.profile(5)
     tuning = arena.tuning()
     del arena
     hbm, peak_kind = peaks()
-    # plain single-case backend: each case alone, to its stop rule, wall clock
+    # plain single-case backend: each of this rank's cases alone, to its stop rule, wall clock
     t_plain = 0.0
     plain_ok = 0
-    for k, c in enumerate(cases):
-        s1 = c.build_solver(device, grid=grids[k])
+    for q, c in enumerate(cases):
+        k = mine[q]
+        s1 = c.build_solver(device, grid=grids[q])
         t0 = time.perf_counter()
         r1 = s1.run_to_stop(c.body, c.numerics, c.wake)
         t_plain += time.perf_counter() - t0
         if k in fx and abs(cd_error(r1, fx[k])) <= 1e-4:
             plain_ok += 1
         del s1
-    plain_cases_per_hr = 3600.0 * plain_ok / t_plain
-    ms_step, total_value, e2e_value = combine_ranks(dist, ms_local, value_rank, e2e_rank)
-    if rank != 0:
-        return None
+    ms_step, census_dev_max, wall_max, plain_max = reduce_scalars(dist, [ms_local, census_dev_s, wall_census, t_plain], "max")
+    ncell_all, plain_ok_all, steady_all = reduce_scalars(dist, [float(ncell), float(plain_ok), steady_local], "sum")
+    total_value = 3600.0 * n_ok / census_dev_max
+    e2e_value = 3600.0 * n_ok / wall_max
+    plain_cases_per_hr = 3600.0 * plain_ok_all / plain_max
     # roofline of the dominant kernel group: the block line sweeps (k_lines, the factorising first pass of each direction,
     # and k_lines_subst, the defect-correction passes), half of an iteration in the launch list
     groups = {g: v for g, v in prof.items() if v[1] > 0}
@@ -302,61 +313,76 @@ def run_ours(args, rank, world, dist):
     bytes_iter = bytes_sweeps / launches_iter
     ms_launch = ms_sweeps / launches_iter
     achieved = bytes_iter / (ms_launch / 1000.0) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("line_sweep_per_launch")
-        except Exception:
-            traffic = None
-    # CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
-    smp = OracleSample(cases)
-    for k in range(len(cases)):
-        smp.solvers[k].step()
-    for _ in range(3):
-        for k in range(len(cases)):
-            smp.step(k)
-    o_iters, filled = oracle_iters(fx, cases)
-    cpu_val = smp.cases_per_hr(o_iters)
+    launches_per_iter = sum(v[1] for v in prof.values()) / 5.0
+    (launches_all,) = reduce_scalars(dist, [launches_per_iter * args.steps], "sum")
+    if rank != 0:
+        return None
+    traffic = line_sweep_traffic()
+    cpu_base = None
+    if world == 1:  # the CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
+        smp = OracleSample(all_cases)
+        for k in range(len(all_cases)):
+            smp.solvers[k].step()
+        for _ in range(3):
+            for k in range(len(all_cases)):
+                smp.step(k)
+        o_iters, filled = oracle_iters(fx, all_cases)
+        cpu_base = {"value": smp.cases_per_hr(o_iters), "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())),
+                    "kind": "port",
+                    "sample": "3 oracle iterations of each of the 32 cases (all host threads) x the oracle's iterations to its stop rules"
+                              + (f" (cases {filled} not in the census fixture: mean of their kind)" if filled else "")}
     stops = {}
     for r in results:
         stops[r["stop_reason"]] = stops.get(r["stop_reason"], 0) + 1
-    launches_per_iter = sum(v[1] for v in prof.values()) / 5.0
-    h2d = h2d_bytes(cen_cases, cen_grids)
-    d2h = d2h_bytes(len(cases), iters)
+    iters = [r["iters"] for r in results]
+    h2d = h2d_bytes(all_cases, all_grids)
+    d2h = d2h_bytes(len(all_cases), iters)
     line = {
         "metric": METRIC, "value": total_value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
-        "data": "synthetic (seeded 32-case sweep, SplitMix64 seed 0x0B05C0C2, the same sweep on every GPU)",
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+        "dtype": "fp32+fp64",
+        "data": "synthetic (seeded 32-case sweep, SplitMix64 seed 0x0B05C0C2, partitioned over the GPUs)",
         "config": {
             "workload": "32-case mixed Euler/RANS-SST sweep, grids 96x48..320x160, line-implicit, batched arena (one launch per kernel "
                         "for all cases), CUDA graph per 50-iteration chunk; state FP32 pair, lines FP32, residual/forces/norms FP64",
-            "cases": len(cases), "cells": int(ncell), "cell_updates_per_s": float(ncell / (ms_step / 1000.0)),
+            "cases": len(all_cases), "cells": int(ncell_all), "cell_updates_per_s": float(ncell_all / (ms_step / 1000.0)),
             "l2": "no flush: the step's working set (~%.0f MB) is larger than the 126 MB L2" % (ncell * 600 / 1e6),
             "converged_within_1e-4": n_ok, "checked_against_oracle": len(dcd),
             "dcd": {str(k): float(f"{d:.3e}") for k, d in dcd.items()},
-            "census_device_s": census_dev_s, "census_wall_s": wall_census, "census_iters": iters, "census_stop_reasons": stops,
-            "steady_state_cases_per_hr": steady,
-            "plain_single_case_cases_per_hr": plain_cases_per_hr, "plain_wall_s": t_plain, "plain_converged_within_1e-4": plain_ok,
-            "batched_vs_plain_e2e": e2e_value / world / plain_cases_per_hr if plain_cases_per_hr else None,
+            "census_device_s": census_dev_max, "census_wall_s": wall_max, "census_iters": iters, "census_stop_reasons": stops,
+            "steady_state_cases_per_hr": steady_all,
+            "plain_single_case_cases_per_hr": plain_cases_per_hr, "plain_wall_s": plain_max, "plain_converged_within_1e-4": int(plain_ok_all),
+            "batched_vs_plain_e2e": e2e_value / plain_cases_per_hr if plain_cases_per_hr else None,
             "learned_warm_start": "not built: cold (free-stream) starts",
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "autotuned_lines_per_block": tuning,
-            "parallelism": f"cases-per-GPU replicas x{world}",
+            "parallelism": (f"cases partitioned over {world} GPUs (longest-processing-time on cells x expected iterations), results "
+                            "gathered" if world > 1 else "one GPU, one batched arena"),
         },
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_iter, "ms_per_launch": ms_launch,
                      "traffic": traffic},
-        "cpu_baseline": {"value": cpu_val, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "kind": "port",
-                         "sample": "3 oracle iterations of each of the 32 cases (all host threads) x the oracle's iterations to its stop rules"
-                                   + (f" (cases {filled} not in the census fixture: mean of their kind)" if filled else "")},
+        "cpu_baseline": cpu_base,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "what": "census by the wall clock through the public API: meshing, arena creation (host->device), solve with chunked "
                         "read-backs (device->host), forces"},
         "clocks": clk,
-        "gpu_launches": int(round(launches_per_iter * args.steps)),
+        "gpu_launches": int(round(launches_all)),
     }
     return line
+
+
+def line_sweep_traffic():
+    """DRAM bytes per line-sweep launch from the committed ncu summary of the line kernels (profiles/line_sweeps_sweep32.md:
+    the `traffic_per_launch_bytes` line, written from dram__bytes_read.sum + dram__bytes_write.sum of that capture)."""
+    p = os.path.join(ROOT, "profiles", "line_sweeps_sweep32.md")
+    try:
+        for l in open(p):
+            if l.startswith("traffic_per_launch_bytes:"):
+                return float(l.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
 
 
 # The sweep's cases that stop on the mean-stationary rule after 14,000-14,050 iterations (limit-cycle SST cases): the
@@ -381,7 +407,7 @@ def run_kernels(args):
         torch.cuda.profiler.stop()
         return {"kernels_only": True, "workload": "lift3", "cells": b.nc * b.nb, "steps": args.steps, "ms_per_step": b.ms_per_iter()}
     from bowshock_b200.arena import Arena
-    cases = build_cases(0)
+    cases = build_cases()
     arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
     arena.run(max(args.warmup, 3))
     if args.workload == "tail6":  # the census's last ~8,650 iterations: only the 6 mean-stationary SST cases left
@@ -406,6 +432,16 @@ def main():
     ap.add_argument("--kernels-only", action="store_true", help="only the timed arena iterations (for ncu captures)")
     ap.add_argument("--workload", default="sweep32", choices=["sweep32", "tail6", "lift3"], help="workload of --kernels-only")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the ranks here when the command was not launched by torchrun
+        import socket
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+        sk.close()
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1",
+               f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

@@ -99,9 +99,14 @@ def dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
 # every symbol the header declares, with its ctypes signature
 _P, _D, _U, _I = C.c_void_p, C.c_double, C.c_uint64, C.c_int
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 SIGNATURES = {
     "bowshock_solver_create": (_I, [_U, _U, _dp, _dp, C.POINTER(Config), _I, C.POINTER(_P)]),
     "bowshock_solver_destroy": (None, [_P]),
@@ -151,6 +156,26 @@ SIGNATURES = {
     "bowshock_arena_set_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_arena_prepare": (_I, [_P, _U]),
     "bowshock_solver_run_noalloc": (_I, [_P, _U, _dp]),
+    "bowshock_arena_set_run": (_I, [_P, _U, C.POINTER(RunParams)]),
+    "bowshock_arena_turb_state": (_I, [_P, _U, _dp, _dp]),
+    "bowshock_arena_set_turb": (_I, [_P, _U, _dp, _dp]),
+    "bowshock_arena_first_residuals": (_I, [_P, C.POINTER(C.c_int32), _dp]),
+    "bowshock_arena_residual_history": (_I, [_P, _U, _dp, _U, C.POINTER(_U)]),
+    "bowshock_net_create": (_I, [_I, _U, C.POINTER(_P)]),
+    "bowshock_net_destroy": (None, [_P]),
+    "bowshock_net_last_error": (C.c_char_p, [_P]),
+    "bowshock_net_num_params": (_I, [_P, C.POINTER(_U)]),
+    "bowshock_net_layout": (_I, [_P, C.POINTER(C.c_int64), _U, C.POINTER(_U)]),
+    "bowshock_net_set_params": (_I, [_P, _fp]),
+    "bowshock_net_get_params": (_I, [_P, _fp]),
+    "bowshock_net_set_mask": (_I, [_P, C.POINTER(C.c_uint8)]),
+    "bowshock_net_forward": (_I, [_P, _U, _fp, _fp]),
+    "bowshock_net_gradients": (_I, [_P, _U, _fp, _fp, _fp, _dp]),
+    "bowshock_net_set_dataset": (_I, [_P, _U, _fp, _fp]),
+    "bowshock_net_reset_optimizer": (_I, [_P]),
+    "bowshock_net_train": (_I, [_P, _U, _U, _D, _U, _dp]),
+    "bowshock_net_last_train_ms": (_I, [_P, _dp]),
+    "bowshock_gemm_bf16": (_I, [_P, C.c_int64, _P, C.c_int64, _P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P, _P]),
 }
 
 _lib = None

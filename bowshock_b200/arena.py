@@ -116,3 +116,36 @@ class Arena:
     def set_active(self, mask):
         m = (C.c_int32 * self.ncases)(*[int(bool(v)) for v in mask])
         self._check(_ffi.load().bowshock_arena_set_active(self._h, m))
+
+    def set_run(self, k: int, numerics, warm=False, r_ref=None):
+        """Run parameters of case k for the next solve(): its numerics' stop rules, a warm start (keep the state and
+        turbulence set through set_state / set_turb, no first-order start-up) and the drop reference r_ref."""
+        p = numerics.run_params(self.cases[k].wake, warm, r_ref)
+        self._check(_ffi.load().bowshock_arena_set_run(self._h, int(k), C.byref(p)))
+
+    def turb_state(self, k: int):
+        """(k, omega) [n, 2] and mu_t [n] of SST case k."""
+        n = self._descs[k].ni * self._descs[k].nj
+        t, m = np.zeros(2 * n), np.zeros(n)
+        self._check(_ffi.load().bowshock_arena_turb_state(self._h, int(k), _ffi.dptr(t), _ffi.dptr(m)))
+        return t.reshape(-1, 2), m
+
+    def set_turb(self, k: int, turb, mu_t):
+        t = np.ascontiguousarray(turb, dtype=np.float64).reshape(-1)
+        m = np.ascontiguousarray(mu_t, dtype=np.float64).reshape(-1)
+        self._check(_ffi.load().bowshock_arena_set_turb(self._h, int(k), _ffi.dptr(t), _ffi.dptr(m)))
+
+    def first_residuals(self, warm) -> np.ndarray:
+        """The density residual each case's run would see first from its current state (warm: per-case flags)."""
+        w = (C.c_int32 * self.ncases)(*[int(bool(v)) for v in warm])
+        out = np.zeros(self.ncases)
+        self._check(_ffi.load().bowshock_arena_first_residuals(self._h, w, _ffi.dptr(out)))
+        return out
+
+    def residual_history(self, k: int) -> np.ndarray:
+        """The density residual of every iteration of case k in the last solve()."""
+        n = C.c_uint64()
+        self._check(_ffi.load().bowshock_arena_residual_history(self._h, int(k), None, 0, C.byref(n)))
+        out = np.zeros(n.value)
+        self._check(_ffi.load().bowshock_arena_residual_history(self._h, int(k), _ffi.dptr(out), n.value, C.byref(n)))
+        return out

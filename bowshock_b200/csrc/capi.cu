@@ -586,6 +586,7 @@ struct bowshock_arena {
   std::vector<int> nseg;
   std::string last_error;
   double last_solve_ms = 0.0;
+  std::vector<std::vector<double>> hist;  // density residual per iteration of each case's last solve
 };
 
 // The host description of one arena case (validated; the metrics are computed separately): false if invalid.
@@ -759,6 +760,8 @@ int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bows
   std::vector<Forces> f;
   if ((rc = a->fp.run(a->ar, f))) return afrom(a, rc);
   for (int k = 0; k < nc; ++k) fill_point(runs[k], f[k], &results[k]);
+  a->hist.resize(nc);
+  for (int k = 0; k < nc; ++k) a->hist[k].swap(runs[k].residual);
   std::vector<int> all(nc, 1);
   return afrom(a, a->ar.set_active(all.data()));
 }
@@ -781,6 +784,66 @@ int bowshock_arena_state(const bowshock_arena* a, uint64_t k, double* u) {
 int bowshock_arena_set_state(bowshock_arena* a, uint64_t k, const double* u) {
   if (!a || !u || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
   return afrom(a, a->ar.set_state((int)k, u));
+}
+
+int bowshock_arena_set_run(bowshock_arena* a, uint64_t k, const bowshock_run_params* p) {
+  if (!a || !p || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
+  if (p->max_iter == 0 || !(p->drop_orders > 0.0) || (p->has_mean_window && p->mean_window < 50) || p->monitor_window == 0) {
+    a->last_error = "run parameters out of range";
+    return BOWSHOCK_INVALID;
+  }
+  a->descs[k].run = *p;
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_turb_state(const bowshock_arena* a, uint64_t k, double* turb, double* mu_t) {
+  if (!a || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
+  bowshock_arena* m = const_cast<bowshock_arena*>(a);
+  if (!(a->ar.cases[k].viscous && a->ar.cases[k].turbulence == 1)) {
+    m->last_error = "turb_state needs an SST case";
+    return BOWSHOCK_UNSUPPORTED;
+  }
+  std::vector<double> t, mt;
+  int rc = m->ar.download_cells((int)k, m->ar.A.turb, t, 2);
+  if (!rc) rc = m->ar.download_cells((int)k, m->ar.A.mu_t, mt, 1);
+  if (rc) return afrom(m, rc);
+  if (turb) std::memcpy(turb, t.data(), t.size() * sizeof(double));
+  if (mu_t) std::memcpy(mu_t, mt.data(), mt.size() * sizeof(double));
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_set_turb(bowshock_arena* a, uint64_t k, const double* turb, const double* mu_t) {
+  if (!a || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
+  if (!(a->ar.cases[k].viscous && a->ar.cases[k].turbulence == 1)) {
+    a->last_error = "set_turb needs an SST case";
+    return BOWSHOCK_UNSUPPORTED;
+  }
+  return afrom(a, a->ar.turb_upload((int)k, turb, mu_t));
+}
+
+int bowshock_arena_first_residuals(bowshock_arena* a, const int32_t* warm, double* out) {
+  if (!a || !out) return BOWSHOCK_INVALID;
+  ArenaHost& ar = a->ar;
+  const int nc = (int)ar.cases.size();
+  int rc = 0;
+  for (int k = 0; k < nc; ++k) {
+    const int it = (warm && warm[k]) ? (int)ar.cases[k].first_order_iters : 0;
+    if ((rc = ar.set_counter(ar.d_iter, k, it))) return afrom(a, rc);
+  }
+  std::vector<double> dens;
+  if ((rc = ar.eval_residual(2, &dens))) return afrom(a, rc);
+  for (int k = 0; k < nc; ++k) out[k] = dens[k];
+  return BOWSHOCK_OK;
+}
+
+int bowshock_arena_residual_history(const bowshock_arena* a, uint64_t k, double* out, uint64_t cap, uint64_t* n) {
+  if (!a || !n || k >= a->ar.cases.size()) return BOWSHOCK_INVALID;
+  const std::vector<double> empty;
+  const std::vector<double>& h = k < a->hist.size() ? a->hist[k] : empty;
+  *n = h.size();
+  if (out)
+    for (size_t q = 0; q < h.size() && q < cap; ++q) out[q] = h[q];
+  return BOWSHOCK_OK;
 }
 
 int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active) {
@@ -838,43 +901,68 @@ extern "C" int bowshock_solver_set_ramp(bowshock_solver* s, uint64_t ramp_k) {
 namespace {
 constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) float g_noalloc_scratch[BOWSHOCK_NOALLOC_SCRATCH_BYTES / sizeof(float)];
+// per device: the looked-up address (null until a lookup succeeded; a failed lookup is not kept, the next call retries)
 float* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
-cudaError_t g_noalloc_err[NOALLOC_MAX_DEVICES];
-std::once_flag g_noalloc_once[NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mu;
 
-void noalloc_setup(int device) {
+// The static array's device address on `device`, looked up with that device current (cudaGetSymbolAddress); the previous
+// current device is restored. Returns the CUDA status of the lookup.
+cudaError_t noalloc_address(int device, float** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_ptr[device]) {
+    *out = g_noalloc_ptr[device];
+    return cudaSuccess;
+  }
   int prev = -1;
   cudaError_t e = cudaGetDevice(&prev);
   if (e == cudaSuccess && prev != device) e = cudaSetDevice(device);
   void* p = nullptr;
   if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (prev >= 0 && prev != device) cudaSetDevice(prev);
-  g_noalloc_err[device] = e;
-  g_noalloc_ptr[device] = e == cudaSuccess ? static_cast<float*>(p) : nullptr;
+  if (e == cudaSuccess && !p) e = cudaErrorInvalidSymbol;
+  if (e == cudaSuccess) g_noalloc_ptr[device] = static_cast<float*>(p);
+  *out = g_noalloc_ptr[device];
+  return e;
 }
 
-// n iterations of the solver's arena with `scratch` as the line solves' spike storage; errors in ar.err
+// The solver's own line-record pointer swapped for the static array for the duration of one call, and put back on every
+// return path (the kernels take the arena by value at launch, so only launches inside the call see the swap).
+struct ScratchSwap {
+  ArenaHost& ar;
+  float* own;
+  ScratchSwap(ArenaHost& a, float* scratch) : ar(a), own(a.A.scratch) { ar.A.scratch = scratch; }
+  ~ScratchSwap() { ar.A.scratch = own; }
+};
+
+// n iterations of the solver's arena with `scratch` as the line solves' spike storage; errors in ar.err. Like
+// ArenaHost::run, the turbulence residual of the last iteration is kept (bowshock_solver_turb_residual); the per-iteration
+// device time (bowshock_arena_last_ms_per_iter) is not measured here: that would need timing events.
 int noalloc_iterate(ArenaHost& ar, float* scratch, uint64_t n, double* residual) {
   std::string& err = ar.err;
   BK_CUDA(cudaSetDevice(ar.device));
   const int nc = (int)ar.cases.size();  // > 1 with a multigrid hierarchy: the fine level is case 0
   const double n_active = (double)ar.desc[0].n_active;
+  ScratchSwap swap(ar, scratch);
+  double tsum_last = 0.0;
   uint64_t done = 0;
   while (done < n) {
     const int chunk = (int)std::min<uint64_t>(n - done, (uint64_t)ar.slots);
     BK_CUDA(cudaMemsetAsync(ar.A.rsum, 0, (size_t)chunk * nc * sizeof(double), ar.stream));
     if (ar.any_sst) BK_CUDA(cudaMemsetAsync(ar.A.tsum, 0, (size_t)chunk * nc * sizeof(double), ar.stream));
-    float* own = ar.A.scratch;
-    ar.A.scratch = scratch;  // the kernels take the arena by value at launch
     for (int k = 0; k < chunk; ++k) ar.launch_iteration(k);
-    ar.A.scratch = own;
     BK_CUDA(cudaGetLastError());
     if (residual)  // case 0's column of the [slot][case] sums of R_rho^2
       BK_CUDA(cudaMemcpy2DAsync(residual + done, sizeof(double), ar.A.rsum, (size_t)nc * sizeof(double), sizeof(double), chunk,
                                 cudaMemcpyDeviceToHost, ar.stream));
+    if (ar.any_sst)  // case 0's sum of the turbulence residual in the chunk's last iteration (pageable copy, no allocation)
+      BK_CUDA(cudaMemcpyAsync(&tsum_last, ar.A.tsum + (size_t)(chunk - 1) * nc, sizeof(double), cudaMemcpyDeviceToHost, ar.stream));
     BK_CUDA(cudaStreamSynchronize(ar.stream));
     if (residual)
       for (int k = 0; k < chunk; ++k) residual[done + k] = std::sqrt(residual[done + k] / n_active);
+    if (ar.any_sst) {
+      ar.last_turb_residual.resize(nc);  // host memory only
+      ar.last_turb_residual[0] = std::sqrt(tsum_last / n_active);
+    }
     done += chunk;
   }
   return 0;
@@ -892,10 +980,11 @@ extern "C" int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, doubl
                 "the solver's " + std::to_string((long long)ar.ncell) + " cells and " + std::to_string(ar.nil + ar.njl) + " lines need " +
                     std::to_string(need) + " bytes of line-solve records, more than the static maximum of " +
                     std::to_string(BOWSHOCK_NOALLOC_SCRATCH_BYTES) + " bytes");
-  std::call_once(g_noalloc_once[dev], noalloc_setup, dev);
-  if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev])
-    return fail(s, BOWSHOCK_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(g_noalloc_err[dev]));
-  int rc = noalloc_iterate(ar, g_noalloc_ptr[dev], n, residual);
+  float* scratch = nullptr;
+  const cudaError_t e = noalloc_address(dev, &scratch);
+  if (e != cudaSuccess || !scratch)
+    return fail(s, BOWSHOCK_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(e));
+  int rc = noalloc_iterate(ar, scratch, n, residual);
   if (rc) return from_arena(s, rc);
   if (residual)
     for (uint64_t k = 0; k < n; ++k)

@@ -294,6 +294,20 @@ int bowshock_arena_solve(bowshock_arena* a, bowshock_point_result* results, bows
 int bowshock_arena_forces(bowshock_arena* a, bowshock_forces* out);
 int bowshock_arena_state(const bowshock_arena* a, uint64_t k, double* u);
 int bowshock_arena_set_state(bowshock_arena* a, uint64_t k, const double* u);
+/* Per-case run parameters for the next bowshock_arena_solve (replacing the descriptor's): a warm start (warm = 1 keeps
+ * the state and turbulence set through bowshock_arena_set_state / bowshock_arena_set_turb, no first-order start-up, drop
+ * measured from r_ref; run.rs:54-63). No counterpart in the reference (its runs are one solver each). */
+int bowshock_arena_set_run(bowshock_arena* a, uint64_t k, const bowshock_run_params* p);
+/* (k, omega) and mu_t of SST case k (ni*nj*2 and ni*nj doubles; either may be NULL); UNSUPPORTED for other cases */
+int bowshock_arena_turb_state(const bowshock_arena* a, uint64_t k, double* turb, double* mu_t);
+int bowshock_arena_set_turb(bowshock_arena* a, uint64_t k, const double* turb, const double* mu_t);
+/* The density residual every case's run would see first from its current state (FP64): with warm[k] != 0 as a warm run
+ * (second-order reconstruction from the first iteration), else as a cold run's first iteration (first order); warm may
+ * be NULL (all cold). The iteration counters are left as a run would start them. */
+int bowshock_arena_first_residuals(bowshock_arena* a, const int32_t* warm, double* out);
+/* The density residual of every iteration of case k in the last bowshock_arena_solve (n entries; at most cap copied into
+ * out, which may be NULL to query n): the history GpuRunner::run_on keeps per run (engine/gpu.rs:143-158). */
+int bowshock_arena_residual_history(const bowshock_arena* a, uint64_t k, double* out, uint64_t cap, uint64_t* n);
 /* per-case activity mask (1 = iterate), ncases entries */
 int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active);
 /* mean device time of one arena iteration over the last bowshock_arena_run, in milliseconds (CUDA events) */
@@ -377,6 +391,53 @@ int bowshock3_forces(bowshock3_batch* b, double x_max, double* out);
 int bowshock3_solve(bowshock3_batch* b, const bowshock3_run_params* p, bowshock3_result* out);
 int bowshock3_last_ms_per_iter(const bowshock3_batch* b, double* ms);
 
+/* ---------------------------------------------------------------------------------------------- learned warm start
+ * No counterpart in the reference (its only warm start is the previous Mach point's field, crates/bowshock-core/src/engine/
+ * run.rs:54-63, analysis.rs:744-748). A conv decoder (about 1.84 M parameters) maps BOWSHOCK_NET_IN inputs (12 geometry
+ * parameters, the Mach number and log10 of the Reynolds number, zero-padded to 16) to BOWSHOCK_NET_OUT channels on the
+ * 64 x 32 coarse level of the normalized 128 x 64 body-fitted grid (BOWSHOCK_NET_CELLS cells, row j = 0..31 of 64 columns
+ * i, channel fastest). Layers: fully connected 16 -> 256 -> 4 x 8 x 128, then 3x3 convolutions with leaky ReLU (slope
+ * 0.1) at 4 x 8 (128 -> 128, twice), 8 x 16 (nearest 2x upsampling, 128 -> 128, twice), 16 x 32 (up, 128 -> 64, 64 -> 64),
+ * 32 x 64 (up, 64 -> 64, twice) and a linear 3x3 output convolution 64 -> 16 of which the first 6 channels are the
+ * prediction. Every contraction, forward and backward, is a BF16 tcgen05 GEMM with FP32 accumulation in TMEM; weights are
+ * FP32 masters trained by Adam (lr given, betas 0.9 / 0.999, eps 1e-8) on the masked mean squared error. The parameter
+ * vector is, per layer in order, W [cout][kin] (kin = cin for a fully connected layer, 9 cin for a convolution with
+ * column (ky*3 + kx)*cin + c) then b [cout], each layer's block padded to a multiple of 8 floats (bowshock_net_layout). */
+#define BOWSHOCK_NET_IN 16
+#define BOWSHOCK_NET_OUT 6
+#define BOWSHOCK_NET_OUT_PAD 16
+#define BOWSHOCK_NET_CELLS 2048
+#define BOWSHOCK_NET_SLOPE 0.1f
+typedef struct bowshock_net bowshock_net;
+/* max_batch: a multiple of 8 (at most 4096); the buffers of every layer are sized for it */
+int bowshock_net_create(int device, uint64_t max_batch, bowshock_net** out);
+void bowshock_net_destroy(bowshock_net* n);
+const char* bowshock_net_last_error(const bowshock_net* n);
+int bowshock_net_num_params(const bowshock_net* n, uint64_t* nparams);
+/* 9 integers per layer (fully connected, cin, cout, H, W, upsampled, activated, W offset, b offset) into out (cap entries) */
+int bowshock_net_layout(const bowshock_net* n, int64_t* out, uint64_t cap, uint64_t* nlayers);
+int bowshock_net_set_params(bowshock_net* n, const float* params);
+int bowshock_net_get_params(bowshock_net* n, float* params);
+/* fluid mask of the coarse cells (BOWSHOCK_NET_CELLS bytes, nonzero = fluid): the loss counts only these */
+int bowshock_net_set_mask(bowshock_net* n, const uint8_t* mask);
+/* y [batch][BOWSHOCK_NET_CELLS][BOWSHOCK_NET_OUT] from x [batch][BOWSHOCK_NET_IN] (host arrays) */
+int bowshock_net_forward(bowshock_net* n, uint64_t batch, const float* x, float* y);
+/* loss and its gradient with respect to every parameter (grad: num_params floats, may be NULL) for one batch (a multiple
+ * of 8, at most max_batch) of inputs x and targets [batch][BOWSHOCK_NET_CELLS][BOWSHOCK_NET_OUT]; no update */
+int bowshock_net_gradients(bowshock_net* n, uint64_t batch, const float* x, const float* target, float* grad, double* loss);
+/* the training set, kept on the device: x [n][BOWSHOCK_NET_IN], target [n][BOWSHOCK_NET_CELLS][BOWSHOCK_NET_OUT] */
+int bowshock_net_set_dataset(bowshock_net* n, uint64_t n_samples, const float* x, const float* target);
+int bowshock_net_reset_optimizer(bowshock_net* n);
+/* `steps` Adam steps on batches from epochs of a seeded shuffle of the dataset; loss (steps entries, may be NULL) */
+int bowshock_net_train(bowshock_net* n, uint64_t steps, uint64_t batch, double lr, uint64_t seed, double* loss);
+/* device time of the last bowshock_net_train (CUDA events), milliseconds */
+int bowshock_net_last_train_ms(const bowshock_net* n, double* ms);
+/* The network's tensor-core GEMM on caller-owned device memory: d[m][n] = sum_k a[m][k] b[n][k], a and b BF16 row-major
+ * (lda, ldb multiples of 8 elements, 16-byte aligned), d FP32 (ldd >= n); splits > 1 adds K slices atomically into d
+ * (zeroed by the caller). stream: a cudaStream_t or NULL; err_flag: a device int set to 1 if a bounded wait gave up. */
+int bowshock_gemm_bf16(const void* a, int64_t lda, const void* b, int64_t ldb, float* d, int64_t ldd, int64_t m, int64_t n, int64_t k,
+                       int64_t splits, void* stream, int* err_flag);
+
 /* bowshock_solver_run without any device allocation. No counterpart in the reference. For hosts that create their solvers
  * up front and then step them from code that may not allocate device memory: the GPU's free memory belongs to the host's
  * own pool (another framework's caching allocator on the same device), or the stepping loop cannot take the device-wide
@@ -385,10 +446,13 @@ int bowshock3_last_ms_per_iter(const bowshock3_batch* b, double* ms);
  * records (blocks, factors, reduction multipliers) from a static 64 MiB device array of the library. A solver needs
  * BOWSHOCK_NOALLOC_BYTES(cells, lines) of it, cells and i + j lines of all multigrid levels counted (about 60,000 cells
  * for a single-level grid of aspect 2); a larger one gets BOWSHOCK_INVALID with a message and nothing is launched. Same residual
- * semantics and results as bowshock_solver_run.
- * The first call on a device looks the array's device address up (cudaGetSymbolAddress with that device current); make
- * that first call before any stream capture. Every call on a device shares the array (nothing in it needs to start at
- * zero); calls that overlap on one GPU, from solvers on other streams or threads, race on it and must be serialised. */
+ * semantics and results as bowshock_solver_run (bit for bit), and bowshock_solver_turb_residual afterwards returns the
+ * turbulence residual of its last iteration; the device time per iteration is not measured (no timing events).
+ * The first call on a device looks the array's device address up (cudaGetSymbolAddress with that device current; a failed
+ * lookup is retried by the next call); make that first call before any stream capture. Every call on a device shares the
+ * array (nothing in it needs to start at zero); calls that overlap on one GPU, from solvers on other streams or threads,
+ * race on it and must be serialised. As for every entry point, one solver must not be used from two host threads at once:
+ * during this call the solver's launches point at the static array. */
 #define BOWSHOCK_NOALLOC_SCRATCH_BYTES (64u << 20)
 #define BOWSHOCK_NOALLOC_BYTES(cells, lines) (928ull * (unsigned long long)(cells) + 128ull + 22528ull * (unsigned long long)(lines))
 int bowshock_solver_run_noalloc(bowshock_solver* s, uint64_t n, double* residual);

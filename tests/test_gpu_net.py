@@ -1,0 +1,109 @@
+"""The learned warm start's tensor-core path on the B200: the tcgen05 GEMM (TMA-fed BF16 operands, FP32 accumulation in
+TMEM) against a plain PyTorch FP32 matmul of the same BF16 inputs, on aligned, ragged and split-K shapes; the network's
+forward pass and its gradients against the float64 CPU oracle (oracle/net_oracle.py, itself pinned by finite
+differences) on the same BF16-rounded weights and inputs; and a short training run that lowers the loss.
+
+Tolerances: the GEMM accumulates exactly-representable BF16 products in FP32, so it agrees with the FP32 matmul to
+round-off of the summation order (1e-4 relative to the row scale). The network rounds every activation to BF16 between
+layers (8 significant bits), so its outputs and gradients agree with the float64 oracle to a few per cent in the
+relative L2 norm (3e-2 outputs, 8e-2 per-layer gradients)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import net_oracle as no
+
+pytestmark = pytest.mark.gpu
+
+
+def _gemm(a, b, splits=1):
+    import torch
+    from bowshock_b200 import _ffi
+    m, k = a.shape
+    n = b.shape[0]
+    d = torch.zeros((m, n), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = _ffi.load().bowshock_gemm_bf16(C.c_void_p(a.data_ptr()), a.stride(0), C.c_void_p(b.data_ptr()), b.stride(0),
+                                       C.c_void_p(d.data_ptr()), d.stride(0), m, n, k, splits,
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream), C.c_void_p(err.data_ptr()))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0, "a bounded wait of the GEMM gave up"
+    return d
+
+
+@pytest.mark.parametrize("m,n,k,splits", [(128, 64, 64, 1), (256, 128, 512, 1), (300, 200, 136, 1), (64, 16, 16, 1),
+                                          (1000, 256, 1024, 1), (512, 576, 4096, 8), (16, 576, 2048, 5), (131072, 64, 576, 1)])
+def test_gemm_matches_torch_fp32(m, n, k, splits):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(m * 7 + n * 3 + k)
+    a = torch.randn((m, k), generator=g, device="cuda").to(torch.bfloat16)
+    b = torch.randn((n, k), generator=g, device="cuda").to(torch.bfloat16)
+    d = _gemm(a, b, splits)
+    ref = a.float() @ b.float().T
+    scale = ref.abs().amax(dim=1, keepdim=True) + 1e-6
+    err = ((d - ref).abs() / scale).max().item()
+    assert err < 1e-4, f"{m}x{n}x{k} splits {splits}: max rel err {err:.2e}"
+
+
+def _net_and_oracle(batch=8, seed=5):
+    from bowshock_b200.net import Net
+    L, n = no.layers()
+    net = Net(max_batch=64)
+    assert net.nparams == n
+    lay = net.layout()
+    assert [(l["fc"], l["cin"], l["cout"], l["H"], l["W"], l["up"], l["act"], l["woff"], l["boff"]) for l in L] == lay
+    rng = np.random.default_rng(seed)
+    p = no.init_params(seed, L, n)
+    for l in L:
+        p[l["boff"]:l["boff"] + l["cout"]] = (0.05 * rng.standard_normal(l["cout"])).astype(np.float32)
+    x = no.bf16_round(rng.standard_normal((batch, no.NET_IN)).astype(np.float32))
+    net.set_params(p)
+    # the GPU multiplies BF16 copies of the weights (biases stay FP32): the oracle gets the same rounded weights
+    pr = p.copy()
+    for l in L:
+        w = slice(l["woff"], l["woff"] + l["cout"] * l["kin"])
+        pr[w] = no.bf16_round(p[w])
+    return net, L, n, pr, x, rng
+
+
+def test_net_forward_matches_oracle():
+    net, L, n, pr, x, _ = _net_and_oracle()
+    y = net.forward(x)
+    ref, _ = no.forward(pr, x, L)
+    ref = ref[..., :no.NET_OUT]
+    rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    assert rel < 3e-2, f"forward rel L2 err {rel:.3e}"
+
+
+def test_net_gradients_match_oracle():
+    net, L, n, pr, x, rng = _net_and_oracle()
+    t = rng.standard_normal((x.shape[0], no.NET_CELLS, no.NET_OUT)).astype(np.float32) * 0.5
+    mask = (rng.random(no.NET_CELLS) > 0.15).astype(np.uint8)
+    net.set_mask(mask)
+    loss, g = net.gradients(x, t)
+    lref, gref = no.loss_and_grad(pr, x, t, mask, L)
+    assert abs(loss - lref) / lref < 1e-2, f"loss {loss} vs {lref}"
+    for k, l in enumerate(L):
+        for name, sl in (("W", slice(l["woff"], l["woff"] + l["cout"] * l["kin"])), ("b", slice(l["boff"], l["boff"] + l["cout"]))):
+            rel = np.linalg.norm(g[sl] - gref[sl]) / (np.linalg.norm(gref[sl]) + 1e-30)
+            assert rel < 8e-2, f"layer {k} {name}: gradient rel L2 err {rel:.3e}"
+
+
+def test_net_training_lowers_the_loss():
+    from bowshock_b200.net import Net
+    L, n = no.layers()
+    net = Net(max_batch=64)
+    net.set_params(no.init_params(1, L, n))
+    rng = np.random.default_rng(2)
+    N = 256
+    x = rng.uniform(-1, 1, (N, no.NET_IN)).astype(np.float32)
+    jj, ii = np.meshgrid(np.linspace(0, 1, 32), np.linspace(0, 1, 64), indexing="ij")
+    base = np.stack([np.sin(np.pi * ii), np.cos(2 * np.pi * jj), ii * jj, ii - jj, np.sin(3 * jj), np.cos(ii)], -1).reshape(-1, 6)
+    t = (x[:, :6, None].transpose(0, 2, 1) * base[None]).astype(np.float32)  # smooth fields scaled by the inputs
+    net.set_dataset(x, t)
+    loss = net.train(300, 64, 1e-3, seed=0)
+    assert np.all(np.isfinite(loss))
+    assert loss[-20:].mean() < 0.2 * loss[:5].mean(), f"loss {loss[:5].mean():.3e} -> {loss[-20:].mean():.3e}"
+    assert net.last_train_ms() > 0

@@ -159,3 +159,37 @@ def test_multigrid_reaches_the_explicit_fixed_point():  # multigrid.rs:260-291, 
     # an FP32 state stalls about 4-5 orders down (the reference's f32 runs: crates/bowshock-cfd/src/gpu/mod.rs:61-62)
     assert r[-1] < 1e-4 * r[0]
     assert np.max(np.abs(gpu.state_f64() - cpu.u)) < 1e-5
+
+
+# Per-cell residual on the two single-case workloads' own grids (config 0: Euler, 128 x 64, M 1.5 with its bow shock;
+# config 1: RANS SST, 256 x 128, y+ ~ 1 wall cells, M 0.9), from a developed state: 40 oracle iterations of the case's
+# own numerics from the free stream, handed to both sides (mean flow and, for SST, k, omega and mu_t), then one residual
+# evaluation with the second-order reconstruction. Tolerance relative to each component's largest magnitude: 2e-5 for
+# the inviscid residual, 1e-4 with the viscous and SST terms (gradients and eddy viscosity read the FP32 state).
+@pytest.mark.parametrize("name,tol", [("config0", 2e-5), ("config1", 1e-4)])
+def test_residual_per_cell_on_config_grids(name, tol):
+    from tests.golden.configs import CONFIGS
+    from tests.golden.sweep_oracle import oracle_case
+    c = CONFIGS[name]()
+    spec = cases.from_case(oracle_case(c), name)
+    dev = cases.oracle_solver(spec)
+    dev.steps(40)
+    spec.u0 = dev.u.copy()
+    spec.first_order_iters = 0
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    if spec.viscous is not None:
+        cpu.turb, cpu.mu_t = dev.turb.copy(), dev.mu_t.copy()
+        gpu.set_turb(dev.turb, dev.mu_t)
+    cpu.eval_residual(True)
+    rc, dc = cpu.res, cpu.dt
+    rg, dg, dens = gpu.eval_residual(True)
+    errs = []
+    for k in range(4):
+        scale = np.max(np.abs(rc[:, k])) + 1e-30
+        errs.append(np.max(np.abs(rg[:, k] - rc[:, k])) / scale)
+    print(name, "per-component max rel residual error", [f"{e:.2e}" for e in errs])
+    assert max(errs) < tol, f"{name}: residual max rel err {max(errs):.3e}"
+    fluid = dc > 0
+    assert np.max(np.abs(dg[fluid] - dc[fluid]) / dc[fluid]) < 1e-5
+    assert abs(dens - cpu.density_residual()) / cpu.density_residual() < 1e-4
