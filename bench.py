@@ -318,6 +318,7 @@ def run_ours(args, rank, world, dist):
     if rank != 0:
         return None
     traffic = line_sweep_traffic()
+    lift3 = measure_lift3(args, device) if world == 1 else None
     cpu_base = None
     if world == 1:  # the CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
         smp = OracleSample(all_cases)
@@ -356,6 +357,7 @@ def run_ours(args, rank, world, dist):
             "learned_warm_start": "not built: cold (free-stream) starts",
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "autotuned_lines_per_block": tuning,
+            "lift3": lift3,
             "parallelism": (f"cases partitioned over {world} GPUs (longest-processing-time on cells x expected iterations), results "
                             "gathered" if world > 1 else "one GPU, one batched arena"),
         },
@@ -370,6 +372,33 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": int(round(launches_all)),
     }
     return line
+
+
+# algorithmic bytes per cell-update of the 3D Euler line-implicit iteration (nv = 5, 16 geometry words, 3 directions,
+# 2 sweeps each: 271 words; the per-kernel model of the 2D path applied to 3D)
+WORDS_3D = 271
+
+
+def measure_lift3(args, device):
+    """Secondary figure: the 3D Euler lift sweep (15 cases, Mach x incidence, on one 192 x 64 x 64 revolved grid) as one
+    batch, CUDA events over K line-implicit iterations after warm-up: ms per iteration, cell-updates/s, and the model's
+    bytes per cell-update over the time against the measured HBM copy bandwidth."""
+    import bowshock_b200.euler3 as e3
+    t0 = time.perf_counter()
+    b, _ = e3.batch_of(e3.lift_sweep_cases(), device=device)
+    setup_s = time.perf_counter() - t0
+    b.run(max(args.warmup, 3))
+    n = max(5, min(args.steps, 20))
+    b.run(n)
+    ms = b.ms_per_iter()
+    cells = b.nc * b.nb
+    hbm, kind = peaks()
+    gbs = cells * WORDS_3D * 4 / (ms / 1000.0) / 1e9
+    del b
+    return {"workload": "15-case 3D Euler lift sweep (alpha 0-8 deg x Mach 0.8/1.2/2.5), 192 x 64 x 64 cells each, one batch",
+            "cells": int(cells), "iterations_timed": n, "ms_per_iter": ms, "cell_updates_per_s": cells / (ms / 1000.0),
+            "model_bytes_per_cell_update": WORDS_3D * 4, "achieved_gbs": gbs, "hbm_frac": gbs / hbm, "peak_kind": kind,
+            "setup_s": setup_s}
 
 
 def line_sweep_traffic():

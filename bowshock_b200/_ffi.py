@@ -30,7 +30,8 @@ class Scheme(C.Structure):  # bowshock_scheme
     _fields_ = [("kind", C.c_int32), ("cfl0", C.c_double), ("cfl_max", C.c_double), ("growth", C.c_double),
                 ("dt_mode", C.c_int32), ("lines", C.c_int32), ("implicit_bc", C.c_int32), ("sub_iters", C.c_uint64),
                 ("roe", C.c_int32), ("eps_fix", C.c_double), ("mg_levels", C.c_uint64), ("mg_pre", C.c_uint64),
-                ("mg_post", C.c_uint64), ("mg_gamma", C.c_uint64), ("mg_coarsest", C.c_uint64)]
+                ("mg_post", C.c_uint64), ("mg_gamma", C.c_uint64), ("mg_coarsest", C.c_uint64), ("cfl_star", C.c_double),
+                ("mg_cfl_star", C.c_double)]
 
 
 class Block(C.Structure):  # bowshock_block

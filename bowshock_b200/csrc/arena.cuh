@@ -16,7 +16,7 @@
 
 namespace bk {
 
-enum { SCHEME_EXPLICIT = 0, SCHEME_MULTIGRID = 2, SCHEME_IMPLICIT = 3 };
+enum { SCHEME_EXPLICIT = 0, SCHEME_SMOOTHED = 1, SCHEME_MULTIGRID = 2, SCHEME_IMPLICIT = 3 };
 enum { DT_SUM = 0, DT_MIN_DIRECTION = 1 };
 
 struct CaseDev {
@@ -35,6 +35,7 @@ struct CaseDev {
   int scheme;
   float cfl0, cfl_max, growth, eps_fix;
   int dt_mode, lines, implicit_bc, sub_iters, roe;
+  float cfl_star;  // implicit residual smoothing of the SSP-RK3 stages (solver.rs:104-120): > 0 on, per-direction CFL limit
   int viscous, sst, wall_i_start;
   double re_c, sutherland, roughness;
   int n_active;
@@ -54,6 +55,8 @@ struct Arena {
   // preconditions (Jacobians, line solves, turbulence, viscous gradients) reads the high words alone.
   float4 *Ulo, *Wlo, *U0lo;
   float* dt;
+  float2* irs_eps;  // implicit residual smoothing: (eps_i, eps_j) of every cell, set with the explicit time step
+  float* irs_c;     // its Thomas multipliers
   const float4 *iface, *jface, *cellg;
   const float2 *ifc, *jfc;  // face centres (mean of the end nodes)
   float* scratch;  // line-solve records (fv_kernels.cu: line_rec, pcr_rec)

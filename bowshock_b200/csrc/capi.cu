@@ -206,8 +206,10 @@ static int rebuild_levels(bowshock_solver* s, int nlev) {
 
 int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
   if (!s || !sc) return BOWSHOCK_INVALID;
-  if (sc->kind != BOWSHOCK_SCHEME_EXPLICIT && sc->kind != BOWSHOCK_SCHEME_IMPLICIT && sc->kind != BOWSHOCK_SCHEME_MULTIGRID)
+  if (sc->kind != BOWSHOCK_SCHEME_EXPLICIT && sc->kind != BOWSHOCK_SCHEME_SMOOTHED && sc->kind != BOWSHOCK_SCHEME_IMPLICIT &&
+      sc->kind != BOWSHOCK_SCHEME_MULTIGRID)
     return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
+  if (!std::isfinite(sc->cfl_star) || !std::isfinite(sc->mg_cfl_star)) return fail(s, BOWSHOCK_INVALID, "cfl_star must be finite");
   if (sc->kind == BOWSHOCK_SCHEME_IMPLICIT && (sc->sub_iters < 1 || sc->sub_iters > 16 || !(sc->cfl0 > 0) || !(sc->cfl_max > 0)))
     return fail(s, BOWSHOCK_INVALID, "implicit parameters out of range");
   if (sc->kind == BOWSHOCK_SCHEME_MULTIGRID) {
@@ -228,7 +230,11 @@ int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
   ar.mg_post = (int)sc->mg_post;
   ar.mg_gamma = (int)sc->mg_gamma;
   ar.mg_coarsest = (int)sc->mg_coarsest;
-  for (auto& hc : ar.cases) hc.scheme = sc->kind;
+  for (auto& hc : ar.cases) {
+    hc.scheme = sc->kind;
+    // Scheme::Smoothed(Irs) smooths the SSP-RK3 stages; the multigrid smoother on every level with MgParams::irs
+    hc.cfl_star = sc->kind == BOWSHOCK_SCHEME_SMOOTHED ? sc->cfl_star : sc->kind == BOWSHOCK_SCHEME_MULTIGRID ? sc->mg_cfl_star : 0.0;
+  }
   HostCase& h = s->ar.cases[0];
   h.scheme = sc->kind;
   h.cfl0 = sc->cfl0;
@@ -517,7 +523,8 @@ int bowshock_solver_run_to_stop(bowshock_solver* s, const bowshock_body* body, c
   if (!s || !p || !out) return BOWSHOCK_INVALID;
   std::string m;
   if (!valid_body(body, m)) return fail(s, BOWSHOCK_INVALID, m);
-  if (s->ar.cases[0].scheme != BOWSHOCK_SCHEME_IMPLICIT && s->ar.cases[0].scheme != BOWSHOCK_SCHEME_EXPLICIT)
+  if (s->ar.cases[0].scheme != BOWSHOCK_SCHEME_IMPLICIT && s->ar.cases[0].scheme != BOWSHOCK_SCHEME_EXPLICIT &&
+      s->ar.cases[0].scheme != BOWSHOCK_SCHEME_SMOOTHED)
     return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
   int rc = 0;
   ForcePass* fp = solver_forces(s, rc);

@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int
     if (is_solid(c, i, j)) {
       A.R[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
       if (dt_kind) A.dt[cc] = 0.f;
+      if (dt_kind == 1 && c.cfl_star > 0.f) A.irs_eps[cc] = make_float2(0.f, 0.f);
     } else {
       float4 fl = A.iface[ifidx(c, i, j)], fr = A.iface[ifidx(c, i + 1, j)];
       float4 fb = A.jface[jfidx(c, i, j)], ft = A.jface[jfidx(c, i, j + 1)];
@@ -248,7 +249,18 @@ __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int
           xj = diffusion_rate(mu_c, mut_c, wc[0], 0.5f * (fb.z + ft.z), g.y);
         }
         float cfl = s_cfl, d;
-        if (dt_kind == 1) {
+        if (dt_kind == 1 && c.cfl_star > 0.f) {
+          // with implicit residual smoothing: dt = CFL A / (L_i + L_j), and each direction whose CFL number
+          // c_d = dt L_d / A exceeds cfl_star smoothed with eps_d = ((c_d / cfl_star)^2 - 1) / 4 (solver.rs:631-641)
+          float li = 0.5f * (lam(fl) + lam(fr)), lj = 0.5f * (lam(fb) + lam(ft));
+          if (c.viscous) li += xi, lj += xj;
+          d = cfl * g.y / (li + lj);
+          auto coef = [&](float l) {
+            const float rr = d * l / g.y / c.cfl_star;
+            return fmaxf(0.25f * (rr * rr - 1.f), 0.f);
+          };
+          A.irs_eps[cc] = make_float2(coef(li), coef(lj));
+        } else if (dt_kind == 1) {
           float sum = lam(fl) + lam(fr) + lam(fb) + lam(ft);
           d = c.viscous ? cfl * g.y / (0.5f * sum + xi + xj) : cfl * g.y / (0.5f * sum);
         } else {
@@ -293,6 +305,51 @@ __global__ void k_stage(Arena A, float a, float b, int copy, int last) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) u[k] = (double)a * (u[k] + d * rd[k]) + (double)b * u0[k];
   pair_st(A.U, A.Ulo, cc, u);
+}
+
+// ==================================================================================== implicit residual smoothing
+// One factor of (1 - eps_i d_ii)(1 - eps_j d_jj) R_bar = R along every i line (dir_i) or j line: the conservative scalar
+// tridiagonal system -e_- x_{k-1} + (1 + e_- + e_+) x_k - e_+ x_{k+1} = r_k with face coefficients e = (eps_k +
+// eps_{k+1}) / 2, zero next to solid cells, solved by the Thomas algorithm, one thread per line, the four conserved
+// components together (solver.rs:722-803). in -> out (the i factor R -> X, then the j factor X -> R).
+__global__ void k_irs(Arena A, int dir_i, const float4* __restrict__ in, float4* __restrict__ out) {
+  const int gw = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gw >= (dir_i ? A.nilines : A.njlines)) return;
+  const int ci = dir_i ? A.iline_case[gw] : A.jline_case[gw];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !(c.cfl_star > 0.f)) return;
+  const int L = gw - (dir_i ? c.iline_off : c.jline_off);
+  const int n = dir_i ? c.ni : c.nj;
+  auto cell = [&](int k) { return dir_i ? cidx(c, k, L) : cidx(c, L, k); };
+  auto solid = [&](int k) { return dir_i ? is_solid(c, k, L) : is_solid(c, L, k); };
+  auto eps = [&](int k) {
+    const float2 v = A.irs_eps[cell(k)];
+    return dir_i ? v.x : v.y;
+  };
+  auto face = [&](int k) { return (solid(k) || solid(k + 1)) ? 0.f : 0.5f * (eps(k) + eps(k + 1)); };  // between k and k + 1
+  float4 prev = make_float4(0.f, 0.f, 0.f, 0.f);
+  float cprev = 0.f, fprev = 0.f;
+  for (int k = 0; k < n; ++k) {
+    const float a = k > 0 ? fprev : 0.f;
+    const float up = k + 1 < n ? face(k) : 0.f;
+    const float m = (1.f + a + up) + a * (k > 0 ? cprev : 0.f);
+    const float cp = -up / m;
+    const long long cc = cell(k);
+    const float4 r = in[cc];
+    const float4 x = make_float4((r.x + a * prev.x) / m, (r.y + a * prev.y) / m, (r.z + a * prev.z) / m, (r.w + a * prev.w) / m);
+    out[cc] = x;
+    A.irs_c[cc] = cp;
+    prev = x, cprev = cp, fprev = up;
+  }
+  float4 nx = prev;
+  for (int k = n - 2; k >= 0; --k) {
+    const long long cc = cell(k);
+    const float cp = A.irs_c[cc];
+    float4 x = out[cc];
+    x.x -= cp * nx.x, x.y -= cp * nx.y, x.z -= cp * nx.z, x.w -= cp * nx.w;
+    out[cc] = x;
+    nx = x;
+  }
 }
 
 // ==================================================================================== implicit operator

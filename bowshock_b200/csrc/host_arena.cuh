@@ -34,6 +34,7 @@ struct HostCase {
   int scheme = SCHEME_EXPLICIT;
   double cfl0 = 1, cfl_max = 30, growth = 1.02, eps_fix = 0.1;
   int dt_mode = 0, lines = 1, implicit_bc = 1, sub_iters = 2, roe = 1;
+  double cfl_star = 0.0;  // implicit residual smoothing of the SSP-RK3 stages (Scheme::Smoothed, or the multigrid smoother)
   bool has_block = false;
   long long i_end = 0, j_end = 0, j_sting = 0;
   bool has_nozzle = false;
@@ -406,6 +407,7 @@ struct ArenaHost {
     c.implicit_bc = h.implicit_bc;
     c.sub_iters = h.sub_iters;
     c.roe = h.roe;
+    c.cfl_star = (h.scheme == SCHEME_SMOOTHED || h.scheme == SCHEME_MULTIGRID) && h.cfl_star > 0.0 ? (float)h.cfl_star : 0.f;
     c.viscous = h.viscous;
     c.sst = h.viscous && h.turbulence == 1;
     c.wall_i_start = (int)h.wall_i_start;
@@ -490,6 +492,8 @@ struct ArenaHost {
     ALLOC(A.U0lo, ncell);
     BK_CUDA(cudaMemset(A.Ulo, 0, ncell * sizeof(float4)));
     ALLOC(A.dt, ncell);
+    ALLOC(A.irs_eps, ncell);
+    ALLOC(A.irs_c, ncell);
     float4 *fi, *fj, *cg;
     float2 *ic, *jc;
     ALLOC(fi, nif);
@@ -818,12 +822,15 @@ struct ArenaHost {
   void rk3(int slot, int last) {
     launch_mean_flow_prep();
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 1, slot); });
+    launch_irs();
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
     launch_mean_flow_prep();
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    launch_irs();
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
     launch_mean_flow_prep();
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    launch_irs();
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, last); });
   }
   void mg_level(int l, int slot) {  // multigrid.rs:87-112
@@ -1108,17 +1115,32 @@ struct ArenaHost {
           launch_turb_chain(stream, slot);
         L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
       }
-    } else {
+    } else {  // SSP-RK3, with implicit residual smoothing of every stage's residual for Scheme::Smoothed
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 1, slot); });
+      launch_irs();
       L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 1.f, 0.f, 1, 0); });
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
+      launch_irs();
       L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 0.25f, 0.75f, 0, 0); });
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 0, -1); });
+      launch_irs();
       L(G_STAGE, [&] { k_stage<<<LT(), TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, 1); });
     }
+  }
+  // implicit residual smoothing of A.R (solver.rs:722-803): the i factor into X, the j factor back into R; the kernels
+  // return at once for cases without smoothing
+  bool any_irs() const {
+    for (const HostCase& h : cases)
+      if ((h.scheme == SCHEME_SMOOTHED || h.scheme == SCHEME_MULTIGRID) && h.cfl_star > 0.0) return true;
+    return false;
+  }
+  void launch_irs() {
+    if (!any_irs()) return;
+    L(G_STAGE, [&] { k_irs<<<(nil + 127) / 128, 128, 0, stream>>>(A, 1, A.R, A.X); });
+    L(G_STAGE, [&] { k_irs<<<(njl + 127) / 128, 128, 0, stream>>>(A, 0, A.X, A.R); });
   }
   // n iterations with CUDA events around every launch (no graph); per-group totals in prof_ms / prof_launches
   int profile(long long n) {

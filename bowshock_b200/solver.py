@@ -19,7 +19,7 @@ from ._ffi import BowshockError
 GAMMA = 1.4
 LIM_FIRST_ORDER, LIM_MINMOD, LIM_VAN_ALBADA, LIM_VENKATAKRISHNAN = 0, 1, 2, 3
 BC_FREESTREAM, BC_EXTRAPOLATE, BC_SLIPWALL, BC_CHARACTERISTIC, BC_PRESSURE_OUTFLOW = 0, 1, 2, 3, 4
-SCHEME_EXPLICIT, SCHEME_IMPLICIT = 0, 3
+SCHEME_EXPLICIT, SCHEME_SMOOTHED, SCHEME_MULTIGRID, SCHEME_IMPLICIT = 0, 1, 2, 3
 DT_SUM, DT_MIN_DIRECTION = 0, 1
 TURB_LAMINAR, TURB_SST = 0, 1
 
@@ -73,6 +73,12 @@ class MgParams:  # solver.rs:123-140 (DEFAULT): FAS multigrid with the SSP-RK3 s
     post: int = 1
     gamma: int = 1
     coarsest: int = 4
+    cfl_star: float = 0.0  # implicit residual smoothing of the smoother (MgParams::irs)
+
+
+@dataclass
+class Smoothed:  # solver.rs:104-120 `Scheme::Smoothed(Irs)`: SSP-RK3 with implicit residual smoothing
+    cfl_star: float = 2.0
 
 
 @dataclass
@@ -148,12 +154,14 @@ class GpuSolver:
             self._check(_ffi.load().bowshock_solver_set_nozzle(self._h, C.byref(n)))
 
     def set_scheme(self, scheme):
-        """`scheme`: EXPLICIT or an ImplicitParams."""
-        if scheme == EXPLICIT:
+        """`scheme`: EXPLICIT, Smoothed, MgParams or ImplicitParams."""
+        if isinstance(scheme, str) and scheme == EXPLICIT:
             s = _ffi.Scheme(kind=SCHEME_EXPLICIT)
+        elif isinstance(scheme, Smoothed):
+            s = _ffi.Scheme(kind=SCHEME_SMOOTHED, cfl_star=scheme.cfl_star)
         elif isinstance(scheme, MgParams):
-            s = _ffi.Scheme(kind=2, mg_levels=scheme.levels, mg_pre=scheme.pre, mg_post=scheme.post, mg_gamma=scheme.gamma,
-                            mg_coarsest=scheme.coarsest)
+            s = _ffi.Scheme(kind=SCHEME_MULTIGRID, mg_levels=scheme.levels, mg_pre=scheme.pre, mg_post=scheme.post, mg_gamma=scheme.gamma,
+                            mg_coarsest=scheme.coarsest, mg_cfl_star=scheme.cfl_star)
         else:
             p = scheme
             s = _ffi.Scheme(SCHEME_IMPLICIT, p.cfl0, p.cfl_max, p.growth, p.dt_mode, int(p.lines), int(p.implicit_bc),

@@ -46,8 +46,9 @@ extern "C" {
 #define BOWSHOCK_BC_SLIPWALL 2
 #define BOWSHOCK_BC_CHARACTERISTIC 3
 #define BOWSHOCK_BC_PRESSURE_OUTFLOW 4
-/* scheme kinds (solver.rs:143-153): the GPU implements Explicit and Implicit, like the reference's GPU solver */
+/* scheme kinds (solver.rs:143-153) */
 #define BOWSHOCK_SCHEME_EXPLICIT 0
+#define BOWSHOCK_SCHEME_SMOOTHED 1
 #define BOWSHOCK_SCHEME_MULTIGRID 2
 #define BOWSHOCK_SCHEME_IMPLICIT 3
 #define BOWSHOCK_DT_SUM 0
@@ -64,8 +65,11 @@ typedef struct {
   uint64_t first_order_iters;
 } bowshock_config;
 
-/* implicit.rs:59-84 `ImplicitParams` (kind = BOWSHOCK_SCHEME_IMPLICIT), the explicit SSP-RK3 scheme, or FAS multigrid
- * with the SSP-RK3 smoother, solver.rs:123-140 `MgParams` (kind = BOWSHOCK_SCHEME_MULTIGRID; Euler only, as the reference) */
+/* implicit.rs:59-84 `ImplicitParams` (kind = BOWSHOCK_SCHEME_IMPLICIT), the explicit SSP-RK3 scheme, SSP-RK3 with implicit
+ * residual smoothing (kind = BOWSHOCK_SCHEME_SMOOTHED, solver.rs:104-120 `Irs`: cfl_star > 0 is the per-direction CFL
+ * limit above which a direction is smoothed, <= 0 none), or FAS multigrid with the SSP-RK3 smoother, solver.rs:123-140
+ * `MgParams` (kind = BOWSHOCK_SCHEME_MULTIGRID, the smoother's residual smoothing in mg_cfl_star; Euler only, as the
+ * reference) */
 typedef struct {
   int32_t kind;
   double cfl0, cfl_max, growth;
@@ -74,6 +78,7 @@ typedef struct {
   int32_t roe;
   double eps_fix;
   uint64_t mg_levels, mg_pre, mg_post, mg_gamma, mg_coarsest;
+  double cfl_star, mg_cfl_star;
 } bowshock_scheme;
 
 /* solver.rs:59-102 `Block` */
