@@ -318,7 +318,9 @@ def run_ours(args, rank, world, dist):
     if rank != 0:
         return None
     traffic = line_sweep_traffic()
+    learned = learned_census(all_cases, all_grids, fx, plain_cases_per_hr, device) if world == 1 else None
     lift3 = measure_lift3(args, device) if world == 1 else None
+    mg0 = measure_config0_multigrid(device) if world == 1 else None
     cpu_base = None
     if world == 1:  # the CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
         smp = OracleSample(all_cases)
@@ -354,10 +356,12 @@ def run_ours(args, rank, world, dist):
             "steady_state_cases_per_hr": steady_all,
             "plain_single_case_cases_per_hr": plain_cases_per_hr, "plain_wall_s": plain_max, "plain_converged_within_1e-4": int(plain_ok_all),
             "batched_vs_plain_e2e": e2e_value / plain_cases_per_hr if plain_cases_per_hr else None,
-            "learned_warm_start": "not built: cold (free-stream) starts",
+            "learned_warm_start": learned,
+            "learned_plus_batched_vs_plain": (learned or {}).get("learned_plus_batched_vs_plain"),
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "autotuned_lines_per_block": tuning,
             "lift3": lift3,
+            "config0_multigrid": mg0,
             "parallelism": (f"cases partitioned over {world} GPUs (longest-processing-time on cells x expected iterations), results "
                             "gathered" if world > 1 else "one GPU, one batched arena"),
         },
@@ -377,6 +381,48 @@ def run_ours(args, rank, world, dist):
 # algorithmic bytes per cell-update of the 3D Euler line-implicit iteration (nv = 5, 16 geometry words, 3 directions,
 # 2 sweeps each: 271 words; the per-kernel model of the 2D path applied to 3D)
 WORDS_3D = 271
+
+
+def learned_census(cases, grids, fx, plain_cases_per_hr, device):
+    """The census again with the learned warm start (bowshock_b200.learned, the committed trained network): a 50-iteration
+    cold probe of every case (its first residual is the fallback rule's base, its peak after iteration 20 the warm runs'
+    drop reference), then every SST case restarted from the network's predicted field (unless its first residual exceeds
+    10x the cold one), the Euler cases cold (the network models the SST base-wake flows), all to the reference's stop
+    rules; device time of the probe and the solve; CDs against the oracle."""
+    from bowshock_b200 import learned as lw
+    from bowshock_b200.arena import Arena
+    if not os.path.exists(lw.WEIGHTS):
+        return {"status": "no trained network committed"}
+    model = lw.WarmStart.load(lw.WEIGHTS, device=device)
+    t0 = time.perf_counter()
+    a = Arena(cases, device=device, grids=grids)
+    probe = a.run(50)
+    probe_ms = a.ms_per_iter() * 50
+    sst = [k for k, c in enumerate(cases) if c.viscous is not None]
+    fields = model.start_fields([cases[k] for k in sst])
+    for q, k in enumerate(sst):
+        u, t, mt = fields[q]
+        a.set_state(k, u)
+        a.set_turb(k, t, mt)
+    first = a.first_residuals([1 if k in sst else 0 for k in range(len(cases))])
+    fallback = []
+    for k, c in enumerate(cases):
+        warm = k in sst and np.isfinite(first[k]) and first[k] <= lw.FALLBACK_RATIO * probe[0, k]
+        if k in sst and not warm:
+            fallback.append(k)
+        a.set_run(k, c.numerics, warm=bool(warm), r_ref=float(probe[20:, k].max()) if warm else None)
+    res = a.solve()
+    dev_s = (probe_ms + a.last_solve_ms()) / 1000.0
+    wall = time.perf_counter() - t0
+    del a
+    dcd = {k: cd_error(res[k], fx[k]) for k in range(len(cases)) if k in fx}
+    n_ok = sum(abs(d) <= 1e-4 for d in dcd.values())
+    value = 3600.0 * n_ok / dev_s
+    e2e = 3600.0 * n_ok / wall
+    return {"census_device_s": dev_s, "census_wall_s": wall, "converged_within_1e-4": n_ok, "checked_against_oracle": len(dcd),
+            "cases_per_hr": value, "e2e_cases_per_hr": e2e, "warm_cases": [k for k in sst if k not in fallback], "fallbacks": fallback,
+            "iters": [r["iters"] for r in res], "dcd": {str(k): float(f"{d:.3e}") for k, d in dcd.items()},
+            "learned_plus_batched_vs_plain": e2e / plain_cases_per_hr if plain_cases_per_hr else None}
 
 
 def measure_lift3(args, device):
@@ -399,6 +445,45 @@ def measure_lift3(args, device):
             "cells": int(cells), "iterations_timed": n, "ms_per_iter": ms, "cell_updates_per_s": cells / (ms / 1000.0),
             "model_bytes_per_cell_update": WORDS_3D * 4, "achieved_gbs": gbs, "hbm_frac": gbs / hbm, "peak_kind": kind,
             "setup_s": setup_s}
+
+
+# algorithmic words of the FAS transfers per coarse cell (nv = 4): the restriction reads 4 fine cells x (state, defect,
+# volume) and writes the coarse state and forcing, the prolongation reads the coarse state and its start value and
+# reads and writes the 4 fine states
+TRANSFER_WORDS = 4 * 9 + 8 + 8 + 4 * 8
+
+
+def measure_config0_multigrid(device):
+    """Config 0 (Euler, 128 x 64, M 1.5) to the reference's stop rules, single-grid line-implicit and 3-level FAS with the
+    line-implicit smoother, wall clock of each GpuSolver.run_to_stop, CD against the FP64 oracle's converged run; and the
+    transfer kernels' model bytes over their CUDA-event time (a grid this small stays in the L2 cache)."""
+    import bowshock_b200 as bk
+    from bowshock_b200.configs import config0_case
+    with open(os.path.join(ROOT, "tests", "golden", "configs_oracle.json")) as f:
+        ref = json.load(f)["config0"]
+    out = {"workload": "config 0: Euler, tangent ogive + cylinder, base wake, M 1.5, 128 x 64 (FAS levels 64 x 32, 32 x 16)"}
+    for name, levels in (("single_grid", 1), ("multigrid3", 3)):
+        c = config0_case()
+        s = c.build_solver(device)
+        if levels > 1:
+            s.set_scheme(bk.solver.MgParams(levels=levels, pre=1, post=1, implicit=c.numerics.scheme))
+        t0 = time.perf_counter()
+        r = s.run_to_stop(c.body, c.numerics, c.wake)
+        wall = time.perf_counter() - t0
+        out[name] = {"iters": r["iters"], "stop": r["stop_reason"], "wall_s": wall, "dcd_total": r["cd_total"] - ref["cd_total"],
+                     "dcd_base": r["cd_base"] - ref["cd_base"]}
+        if levels > 1:
+            prof = s.profile(10)
+            ms, n = prof["transfer"]
+            coarse = (64 * 32 + 32 * 16)  # coarse cells of one cycle's transfers (pre = post = 1, gamma = 1)
+            if ms > 0:
+                gbs = coarse * TRANSFER_WORDS * 4 * 10 / (ms / 1000.0) / 1e9
+                out[name]["transfer_ms_per_cycle"] = ms / 10
+                out[name]["transfer_launches_per_cycle"] = n / 10
+                out[name]["transfer_model_gbs"] = gbs
+                out[name]["transfer_hbm_frac"] = gbs / peaks()[0]
+        del s
+    return out
 
 
 def line_sweep_traffic():

@@ -31,7 +31,7 @@ class Scheme(C.Structure):  # bowshock_scheme
                 ("dt_mode", C.c_int32), ("lines", C.c_int32), ("implicit_bc", C.c_int32), ("sub_iters", C.c_uint64),
                 ("roe", C.c_int32), ("eps_fix", C.c_double), ("mg_levels", C.c_uint64), ("mg_pre", C.c_uint64),
                 ("mg_post", C.c_uint64), ("mg_gamma", C.c_uint64), ("mg_coarsest", C.c_uint64), ("cfl_star", C.c_double),
-                ("mg_cfl_star", C.c_double)]
+                ("mg_cfl_star", C.c_double), ("mg_implicit", C.c_int32)]
 
 
 class Block(C.Structure):  # bowshock_block
@@ -153,6 +153,7 @@ SIGNATURES = {
     "bowshock_arena_last_ms_per_iter": (_I, [_P, _dp]),
     "bowshock_arena_last_solve_ms": (_I, [_P, _dp]),
     "bowshock_arena_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
+    "bowshock_solver_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
     "bowshock_arena_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_arena_set_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_arena_prepare": (_I, [_P, _U]),

@@ -68,7 +68,8 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_last_solve_ms(self._h, C.byref(d)))
         return d.value
 
-    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage", "subst_i", "subst_j", "assemble", "turb_lines")
+    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage", "subst_i", "subst_j", "assemble",
+                      "turb_lines", "transfer")
 
     def profile(self, n: int):
         """Per-kernel-group device time over n iterations launched one kernel at a time: {group: (ms, launches)}."""

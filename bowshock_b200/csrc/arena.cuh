@@ -9,6 +9,7 @@
 // Case descriptors, iteration counters and convergence masks live in device memory so that an iteration launched
 // from a CUDA graph reads everything it needs on the device.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -54,6 +55,9 @@ struct Arena {
   // so that the FP64 residual, not FP32 rounding of the state, decides the converged state. Everything that only
   // preconditions (Jacobians, line solves, turbulence, viscous gradients) reads the high words alone.
   float4 *Ulo, *Wlo, *U0lo;
+  // per case two tensor maps (W, then Wlo) over its padded primitives, 16-byte elements as 4 floats, boxes of the
+  // residual tile and its 2-cell halo: the residual kernel stages its tile with TMA
+  const CUtensorMap* wmaps;
   float* dt;
   float2* irs_eps;  // implicit residual smoothing: (eps_i, eps_j) of every cell, set with the explicit time step
   float* irs_c;     // its Thomas multipliers

@@ -210,7 +210,8 @@ int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
       sc->kind != BOWSHOCK_SCHEME_MULTIGRID)
     return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
   if (!std::isfinite(sc->cfl_star) || !std::isfinite(sc->mg_cfl_star)) return fail(s, BOWSHOCK_INVALID, "cfl_star must be finite");
-  if (sc->kind == BOWSHOCK_SCHEME_IMPLICIT && (sc->sub_iters < 1 || sc->sub_iters > 16 || !(sc->cfl0 > 0) || !(sc->cfl_max > 0)))
+  const bool implicit_params = sc->kind == BOWSHOCK_SCHEME_IMPLICIT || (sc->kind == BOWSHOCK_SCHEME_MULTIGRID && sc->mg_implicit);
+  if (implicit_params && (sc->sub_iters < 1 || sc->sub_iters > 16 || !(sc->cfl0 > 0) || !(sc->cfl_max > 0)))
     return fail(s, BOWSHOCK_INVALID, "implicit parameters out of range");
   if (sc->kind == BOWSHOCK_SCHEME_MULTIGRID) {
     // multigrid.rs:29-31: refused with viscous terms and with a nozzle
@@ -230,7 +231,12 @@ int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
   ar.mg_post = (int)sc->mg_post;
   ar.mg_gamma = (int)sc->mg_gamma;
   ar.mg_coarsest = (int)sc->mg_coarsest;
+  ar.mg_implicit = sc->kind == BOWSHOCK_SCHEME_MULTIGRID && sc->mg_implicit != 0;
   for (auto& hc : ar.cases) {
+    if (implicit_params) {  // every level smooths with the same implicit parameters (each with its own CFL ramp)
+      hc.cfl0 = sc->cfl0, hc.cfl_max = sc->cfl_max, hc.growth = sc->growth, hc.dt_mode = sc->dt_mode, hc.lines = sc->lines;
+      hc.implicit_bc = sc->implicit_bc, hc.sub_iters = (int)sc->sub_iters, hc.roe = sc->roe, hc.eps_fix = sc->eps_fix;
+    }
     hc.scheme = sc->kind;
     // Scheme::Smoothed(Irs) smooths the SSP-RK3 stages; the multigrid smoother on every level with MgParams::irs
     hc.cfl_star = sc->kind == BOWSHOCK_SCHEME_SMOOTHED ? sc->cfl_star : sc->kind == BOWSHOCK_SCHEME_MULTIGRID ? sc->mg_cfl_star : 0.0;
@@ -248,7 +254,9 @@ int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
   h.eps_fix = sc->eps_fix;
   int rc = s->ar.upload_desc();
   if (rc) return from_arena(s, rc);
-  return from_arena(s, s->ar.set_counter(s->ar.d_ramp, 0, 0));
+  for (int k = 0; k < (int)s->ar.cases.size(); ++k)
+    if ((rc = s->ar.set_counter(s->ar.d_ramp, k, 0))) return from_arena(s, rc);
+  return BOWSHOCK_OK;
 }
 
 int bowshock_solver_set_viscous(bowshock_solver* s, const bowshock_viscous* v) {
@@ -524,7 +532,7 @@ int bowshock_solver_run_to_stop(bowshock_solver* s, const bowshock_body* body, c
   std::string m;
   if (!valid_body(body, m)) return fail(s, BOWSHOCK_INVALID, m);
   if (s->ar.cases[0].scheme != BOWSHOCK_SCHEME_IMPLICIT && s->ar.cases[0].scheme != BOWSHOCK_SCHEME_EXPLICIT &&
-      s->ar.cases[0].scheme != BOWSHOCK_SCHEME_SMOOTHED)
+      s->ar.cases[0].scheme != BOWSHOCK_SCHEME_SMOOTHED && s->ar.cases[0].scheme != BOWSHOCK_SCHEME_MULTIGRID)
     return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
   int rc = 0;
   ForcePass* fp = solver_forces(s, rc);
@@ -535,6 +543,8 @@ int bowshock_solver_run_to_stop(bowshock_solver* s, const bowshock_body* body, c
   runs[0].nseg = body->nseg;
   runs[0].skip = runs[0].p.warm ? 0 : 20;
   if ((rc = start_case(s->ar, 0, runs[0].p, s->ar.cases[0].first_order_iters))) return from_arena(s, rc);
+  for (int k = 1; k < (int)s->ar.cases.size(); ++k)  // multigrid levels: their counters and CFL ramps restart with the run
+    if ((rc = s->ar.set_counter(s->ar.d_iter, k, 0)) || (rc = s->ar.set_counter(s->ar.d_ramp, k, 0))) return from_arena(s, rc);
   std::function<bool(int, long long, double, double)> cb;
   if (progress) cb = [&](int k, long long it, double r, double mon) { return progress(user, (uint64_t)k, (uint64_t)it, r, mon) == 0; };
   if ((rc = solve_arena(s->ar, *fp, runs, cb))) return from_arena(s, rc);
@@ -543,8 +553,8 @@ int bowshock_solver_run_to_stop(bowshock_solver* s, const bowshock_body* body, c
   fill_point(runs[0], f[0], out);
   if (residual)
     for (size_t k = 0; k < runs[0].residual.size() && k < cap; ++k) residual[k] = runs[0].residual[k];
-  int one = 1;
-  s->ar.set_active(&one);
+  std::vector<int> all(s->ar.cases.size(), 1);
+  s->ar.set_active(all.data());
   return runs[0].reason == 5 ? fail(s, BOWSHOCK_NONFINITE, "non-finite residual or monitor") : BOWSHOCK_OK;
 }
 
@@ -880,6 +890,17 @@ extern "C" int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms,
   for (int g = 0; g < ArenaHost::G_N; ++g) {
     ms[g] = a->ar.prof_ms[g];
     launches[g] = (uint64_t)a->ar.prof_launches[g];
+  }
+  return BOWSHOCK_OK;
+}
+
+extern "C" int bowshock_solver_profile(bowshock_solver* s, uint64_t n, double* ms, uint64_t* launches) {
+  if (!s || !ms || !launches) return BOWSHOCK_INVALID;
+  int rc = s->ar.profile((long long)n);
+  if (rc) return from_arena(s, rc);
+  for (int g = 0; g < ArenaHost::G_N; ++g) {
+    ms[g] = s->ar.prof_ms[g];
+    launches[g] = (uint64_t)s->ar.prof_launches[g];
   }
   return BOWSHOCK_OK;
 }

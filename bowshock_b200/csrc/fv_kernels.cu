@@ -12,6 +12,7 @@
 //               memory, then each lane back-substitutes its segment; factors kept in the records (implicit.rs:528-563)
 //   k_lines_subst  the defect-correction passes with the kept factors                  (implicit.rs:622-639)
 //   k_defect    defect r = dt R - (A_i du + A_j du - du) with the kept blocks           (implicit.rs:622-630)
+#include "tma.cuh"
 #include "arena.cuh"
 #include "device_math.cuh"
 #include "viscous.cuh"
@@ -127,11 +128,14 @@ __device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(
 // the same arithmetic (checked bit for bit), whereas MINB = 2 rounds differently.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int slot) {
-  __shared__ float4 sW[TJ + 4][TI + 4], sWl[TJ + 4][TI + 4];
+  __shared__ __align__(128) float4 sW[TJ + 4][TI + 4];
+  __shared__ __align__(128) float4 sWl[TJ + 4][TI + 4];
   __shared__ double4 sFI[TJ][TI + 1];
   __shared__ double4 sFJ[TJ + 1][TI];
   __shared__ double sred[NT / 32];
   __shared__ float s_cfl;
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int s_ok;
   const int t = tile_at(A);
   const int ci = A.tile_case[t];
   const CaseDev& c = A.cases[ci];
@@ -150,16 +154,32 @@ __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int
     } else {
       s_cfl = c.cfl;
     }
-  }
-  // stage the padded primitives of the tile and its 2-cell halo
-  for (int idx = tid; idx < (TJ + 4) * (TI + 4); idx += blockDim.x) {
-    int r = idx / (TI + 4), q = idx % (TI + 4);
-    int gi = i0 - 2 + q, gj = j0 - 2 + r;
-    bool in = gi < ni + 2 && gj < nj + 2;
-    sW[r][q] = in ? A.W[pidx(c, gi, gj)] : make_float4(1.f, 0.f, 0.f, 1.f);
-    sWl[r][q] = in ? A.Wlo[pidx(c, gi, gj)] : make_float4(0.f, 0.f, 0.f, 0.f);
+    bktma::mbar_init(&s_bar, 1);
+    bktma::mbar_init_fence();
   }
   __syncthreads();
+  // stage the padded primitives of the tile and its 2-cell halo, (TJ + 4) x (TI + 4) cells of both words of the pair,
+  // with two TMA box loads: the tile's padded origin (i0, j0) is cell (i0 - 2, j0 - 2), its x offset 4 i0 floats is
+  // 16-byte aligned; cells beyond the padded array read zeros and are never used (faces past i = ni, j = nj are skipped)
+  if (tid == 0) {
+    const CUtensorMap* m = A.wmaps + 2 * ci;
+    bktma::tensormap_acquire(m);
+    bktma::tensormap_acquire(m + 1);
+    bktma::mbar_expect_tx(&s_bar, (uint32_t)(2 * sizeof(sW)));
+    bktma::tma_load_2d(&sW[0][0], m, &s_bar, 4 * i0, j0);
+    bktma::tma_load_2d(&sWl[0][0], m + 1, &s_bar, 4 * i0, j0);
+  }
+  const bool staged = bktma::mbar_wait(&s_bar, 0);
+  if (tid == 0) s_ok = 1;
+  __syncthreads();
+  if (!staged) s_ok = 0;
+  __syncthreads();
+  if (!s_ok) {  // the staging never completed (bounded wait): the tile's residual becomes NaN, which the host reports
+    const int q = tid % TI, r = tid / TI;
+    if (tid < TI * TJ && i0 + q < ni && j0 + r < nj) A.R[cidx(c, i0 + q, j0 + r)] = make_float4(NAN, NAN, NAN, NAN);
+    if (tid == 0 && slot >= 0) atomicAdd(&A.rsum[(long long)slot * A.ncases + ci], (double)NAN);
+    return;
+  }
   auto wd = [&](int r, int q) { return pair_ld(sW[r][q], sWl[r][q]); };
   // i faces (TI+1 per row) and j faces (TJ+1 per column), FP64
   for (int idx = tid; idx < TJ * (TI + 1) + (TJ + 1) * TI; idx += blockDim.x) {

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "arena.cuh"
+#include "tma.cuh"
 
 namespace bk {
 
@@ -360,7 +361,7 @@ struct ArenaHost {
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
                     A.grad4, A.gradT, A.mu, A.mu_t, A.rough, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
                     A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled, d_tlist, d_pblist, d_illist, d_jllist,
-                    A.lend};
+                    A.lend, A.irs_eps, A.irs_c, (void*)A.wmaps};
     d_enabled = nullptr;
     d_tlist = d_pblist = d_illist = d_jllist = nullptr;
     for (void* p : ptrs)
@@ -419,6 +420,35 @@ struct ArenaHost {
     c.fine_case = h.fine_case;
     c.coarse_case = h.coarse_case;
     return c;
+  }
+
+  // The residual kernel's tensor maps: per case W then Wlo of its padded primitives as a 2D array of floats,
+  // 4 (ni + 4) wide (each cell's float4 = 4 floats) and nj + 4 high, boxes of 4 (TI + 4) x (TJ + 4) floats.
+  int build_wmaps() {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = bktma::encoder(err);
+    if (!enc) return 3;
+    const int nc = (int)cases.size();
+    std::vector<CUtensorMap> maps(2 * (size_t)nc);
+    for (int k = 0; k < nc; ++k)
+      for (int w = 0; w < 2; ++w) {
+        const CaseDev& c = desc[k];
+        float4* base = (w ? A.Wlo : A.W) + c.pad_off;
+        cuuint64_t dims[2] = {(cuuint64_t)4 * (c.ni + 4), (cuuint64_t)(c.nj + 4)};
+        cuuint64_t strides[1] = {(cuuint64_t)(c.ni + 4) * sizeof(float4)};
+        cuuint32_t box[2] = {(cuuint32_t)4 * (TI + 4), (cuuint32_t)(TJ + 4)};
+        cuuint32_t es[2] = {1, 1};
+        CUresult r = enc(&maps[2 * k + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+          err = "cuTensorMapEncodeTiled of the primitives of case " + std::to_string(k) + " failed (" + std::to_string((int)r) + ")";
+          return 3;
+        }
+      }
+    CUtensorMap* d = nullptr;
+    BK_CUDA(cudaMalloc(&d, maps.size() * sizeof(CUtensorMap)));
+    A.wmaps = d;
+    BK_CUDA(cudaMemcpy(d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    return 0;
   }
 
   // Lay out the arena, allocate and upload geometry (once; the case dimensions are fixed afterwards).
@@ -491,6 +521,7 @@ struct ArenaHost {
     ALLOC(A.Wlo, npad);
     ALLOC(A.U0lo, ncell);
     BK_CUDA(cudaMemset(A.Ulo, 0, ncell * sizeof(float4)));
+    if ((rc = build_wmaps())) return rc;
     ALLOC(A.dt, ncell);
     ALLOC(A.irs_eps, ncell);
     ALLOC(A.irs_c, ncell);
@@ -833,24 +864,35 @@ struct ArenaHost {
     launch_irs();
     L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 2.f / 3.f, 1.f / 3.f, 0, last); });
   }
+  // The smoother of a level: SSP-RK3 (the reference's, multigrid.rs:87-112), or with mg_implicit one line-implicit
+  // iteration (the implicit scheme's residual, assembly, line solves, defect corrections and damped update) of the active
+  // level, its time step from that level's own CFL ramp; the implicit iteration advances the level's iteration and ramp
+  // counters itself (so the fine level's counters advance once per smoothing step).
+  bool mg_implicit = false;
+  void smooth(int slot, int last) {
+    if (mg_implicit)
+      implicit_step(slot);
+    else
+      rk3(slot, last);
+  }
   void mg_level(int l, int slot) {  // multigrid.rs:87-112
     const bool coarsest = l == mg_levels - 1;
     const int n_pre = coarsest ? mg_coarsest : mg_pre;
     set_level(l);
-    for (int k = 0; k < n_pre; ++k) rk3(l == 0 && k == 0 ? slot : -1, 0);
+    for (int k = 0; k < n_pre; ++k) smooth(l == 0 && k == 0 ? slot : -1, 0);
     if (coarsest) return;
     launch_mean_flow_prep();
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, (l == 0 && n_pre == 0) ? slot : -1); });
-    L(G_STAGE, [&] { k_restrict_state<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+    L(G_TRANSFER, [&] { k_restrict_state<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
     set_level(l + 1);
     launch_mean_flow_prep();
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
-    L(G_STAGE, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+    L(G_TRANSFER, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
     for (int g = 0; g < std::max(mg_gamma, 1); ++g) mg_level(l + 1, -1);
-    L(G_STAGE, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l); });
+    L(G_TRANSFER, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l); });
     set_level(l);
-    for (int k = 0; k < mg_post; ++k) rk3(-1, l == 0 && k == mg_post - 1 ? 1 : 0);
-    if (l == 0 && mg_post == 0) {  // the cycle still counts one iteration
+    for (int k = 0; k < mg_post; ++k) smooth(-1, l == 0 && k == mg_post - 1 ? 1 : 0);
+    if (l == 0 && mg_post == 0 && !mg_implicit) {  // the cycle still counts one iteration
       launch_mean_flow_prep();
       L(G_STAGE, [&] { k_stage<<<ntiles, TI * TJ, 0, stream>>>(A, 1.f, 0.f, 0, 1); });
     }
@@ -858,7 +900,8 @@ struct ArenaHost {
 
   // ---------------------------------------------------------------- one iteration (stream-ordered launches)
   // Kernel groups of the per-kernel profile (CUDA events around every launch when `profiling` is set).
-  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_SUBST_I, G_SUBST_J, G_ASSEMBLE, G_TURB_LINES, G_N };
+  enum { G_PRIMS = 0, G_VISC, G_RESIDUAL, G_LINES_I, G_LINES_J, G_DEFECT, G_TURB, G_STAGE, G_SUBST_I, G_SUBST_J, G_ASSEMBLE, G_TURB_LINES, G_TRANSFER,
+         G_N };
   bool profiling = false;
   double prof_ms[G_N] = {0};
   long long prof_launches[G_N] = {0};
@@ -1063,58 +1106,64 @@ struct ArenaHost {
     for (auto& d : desc) s = std::max(s, d.sub_iters);
     return s;
   }
+  // One line-implicit iteration of every active case (implicit.rs:601-663): primitives, residual and time step, the
+  // blocks of both directions, the factorising line solves and sub_iters - 1 defect corrections, the damped update, and
+  // the SST update for SST cases.
+  void implicit_step(int slot) {
+    // the line ends' ghost Jacobians need only the primitives: in a captured iteration they run on the graph's second
+    // branch beside the viscous terms, the residual and the assembly
+    const int nle = 2 * (LI(1) + LI(0));
+    const bool fork_ends = capturing && !profiling;
+    L(G_PRIMS, [&] { k_prims<<<LP(), 256, 0, stream>>>(A); });
+    if (fork_ends) {
+      cudaEventRecord(ev_fork, stream);
+      cudaStreamWaitEvent(side, ev_fork, 0);
+      k_line_ends_T<<<(nle + 127) / 128, 128, 0, side>>>(A);
+      cudaEventRecord(ev_ends, side);
+    } else {
+      L(G_ASSEMBLE, [&] { k_line_ends_T<<<(nle + 127) / 128, 128, 0, stream>>>(A); });
+    }
+    if (any_viscous) {
+      L(G_VISC, [&] { k_visc_cell<<<LT(), TI * TJ, 0, stream>>>(A); });
+      L(G_VISC, [&] { k_visc_face<<<LT(), TI * TJ, 0, stream>>>(A); });
+    }
+    L(G_RESIDUAL, [&] { launch_residual(2, slot); });
+    const int s = sub_iters_of_arena();
+    // the SST chain on the graph's second branch (only the warp-per-line SST kernel: the thread-per-line one borrows
+    // the line records)
+    const bool fork = any_sst && capturing && !profiling && max_line <= 32 * TL_MAXM;
+    if (fork) {
+      cudaEventRecord(ev_fork, stream);
+      cudaStreamWaitEvent(side, ev_fork, 0);
+      launch_turb_chain(side, slot);
+      cudaEventRecord(ev_join, side);
+    }
+    L(G_ASSEMBLE, [&] {
+      k_assemble<<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
+    });
+    if (fork_ends) cudaStreamWaitEvent(stream, ev_ends, 0);
+    L(G_ASSEMBLE, [&] { k_line_ends_fold<<<(nle + 127) / 128, 128, 0, stream>>>(A); });
+    L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
+    L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
+    for (int p = 1; p < s; ++p) {
+      L(G_DEFECT, [&] { k_defect<<<LT(), TI * TJ, 0, stream>>>(A, p); });
+      L(G_SUBST_I, [&] { launch_subst(1, A.RR, A.X, p); });
+      L(G_SUBST_J, [&] { launch_subst(0, A.X, nullptr, p); });
+    }
+    if (any_sst) {
+      if (fork)
+        cudaStreamWaitEvent(stream, ev_join, 0);
+      else
+        launch_turb_chain(stream, slot);
+      L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
+    }
+  }
   void launch_iteration(int slot) {
     if (scheme_of_arena() == SCHEME_MULTIGRID) {
       mg_level(0, slot);
       set_level(0);
     } else if (scheme_of_arena() == SCHEME_IMPLICIT) {
-      // the line ends' ghost Jacobians need only the primitives: in a captured iteration they run on the graph's second
-      // branch beside the viscous terms, the residual and the assembly
-      const int nle = 2 * (LI(1) + LI(0));
-      const bool fork_ends = capturing && !profiling;
-      L(G_PRIMS, [&] { k_prims<<<LP(), 256, 0, stream>>>(A); });
-      if (fork_ends) {
-        cudaEventRecord(ev_fork, stream);
-        cudaStreamWaitEvent(side, ev_fork, 0);
-        k_line_ends_T<<<(nle + 127) / 128, 128, 0, side>>>(A);
-        cudaEventRecord(ev_ends, side);
-      } else {
-        L(G_ASSEMBLE, [&] { k_line_ends_T<<<(nle + 127) / 128, 128, 0, stream>>>(A); });
-      }
-      if (any_viscous) {
-        L(G_VISC, [&] { k_visc_cell<<<LT(), TI * TJ, 0, stream>>>(A); });
-        L(G_VISC, [&] { k_visc_face<<<LT(), TI * TJ, 0, stream>>>(A); });
-      }
-      L(G_RESIDUAL, [&] { launch_residual(2, slot); });
-      const int s = sub_iters_of_arena();
-      // the SST chain on the graph's second branch (only the warp-per-line SST kernel: the thread-per-line one borrows
-      // the line records)
-      const bool fork = any_sst && capturing && !profiling && max_line <= 32 * TL_MAXM;
-      if (fork) {
-        cudaEventRecord(ev_fork, stream);
-        cudaStreamWaitEvent(side, ev_fork, 0);
-        launch_turb_chain(side, slot);
-        cudaEventRecord(ev_join, side);
-      }
-      L(G_ASSEMBLE, [&] {
-        k_assemble<<<dim3(LT(), 2), TI * TJ, 0, stream>>>(A);
-      });
-      if (fork_ends) cudaStreamWaitEvent(stream, ev_ends, 0);
-      L(G_ASSEMBLE, [&] { k_line_ends_fold<<<(nle + 127) / 128, 128, 0, stream>>>(A); });
-      L(G_LINES_I, [&] { launch_lines(1, A.R, 1, A.X); });
-      L(G_LINES_J, [&] { launch_lines(0, A.X, 0, nullptr); });
-      for (int p = 1; p < s; ++p) {
-        L(G_DEFECT, [&] { k_defect<<<LT(), TI * TJ, 0, stream>>>(A, p); });
-        L(G_SUBST_I, [&] { launch_subst(1, A.RR, A.X, p); });
-        L(G_SUBST_J, [&] { launch_subst(0, A.X, nullptr, p); });
-      }
-      if (any_sst) {
-        if (fork)
-          cudaStreamWaitEvent(stream, ev_join, 0);
-        else
-          launch_turb_chain(stream, slot);
-        L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
-      }
+      implicit_step(slot);
     } else {  // SSP-RK3, with implicit residual smoothing of every stage's residual for Scheme::Smoothed
       launch_mean_flow_prep();
       L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<LT(), TI * TJ, 0, stream>>>(A, 1, slot); });

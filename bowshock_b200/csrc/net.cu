@@ -23,45 +23,18 @@
 #include <vector>
 
 #include "../../include/bowshock_b200.h"
+#include "tma.cuh"
 
 namespace bknet {
 
 typedef __nv_bfloat16 bf16;
 
 // ------------------------------------------------------------------------------------------------ device primitives
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t n) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred P1;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, P1;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Every wait of the GEMM is bounded: about a second of SM clock, then the caller records the failure and winds down.
-constexpr long long WAIT_CYCLES = 2000000000ll;
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-  if (mbar_try_wait(b, parity)) return true;
-  const long long t0 = clock64();
-  while (!mbar_try_wait(b, parity))
-    if (clock64() - t0 > WAIT_CYCLES) return false;
-  return true;
-}
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-      : "memory");
-}
+using bktma::mbar_expect_tx;
+using bktma::mbar_init;
+using bktma::mbar_wait;
+using bktma::smem_u32;
+using bktma::tma_load_2d;
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
@@ -157,8 +130,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtenso
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(full + s, 1), mbar_init(empty + s, 1);
     mbar_init(done, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    bktma::mbar_init_fence();
     s_abort = 0;
   }
   if (warp == 0) {
@@ -389,20 +361,9 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
 
 // ------------------------------------------------------------------------------------------------ host side
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-static std::mutex g_encode_mu;
-
 static bool get_encode(std::string& err) {
-  std::lock_guard<std::mutex> lk(g_encode_mu);
-  if (g_encode) return true;
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
-    err = "cuTensorMapEncodeTiled not available from the driver";
-    return false;
-  }
-  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  return true;
+  if (!g_encode) g_encode = bktma::encoder(err);
+  return g_encode != nullptr;
 }
 
 // Tensor map of a row-major BF16 matrix [rows, cols] with leading dimension ld (elements, a multiple of 8), boxes of

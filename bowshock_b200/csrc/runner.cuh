@@ -238,23 +238,29 @@ inline int start_case(ArenaHost& ar, int k, const RunParams& p, long long first_
 inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
                        const std::function<bool(int, long long, double, double)>& progress, double* device_ms = nullptr) {
   double dev_ms = 0.0;
-  const int nc = (int)ar.cases.size();
+  // runs: one per arena case, or, for a single case with a multigrid hierarchy, one for the fine level (the coarse
+  // levels, cases 1.., follow its activity)
+  const int nc = (int)ar.cases.size(), nr = (int)runs.size();
   std::vector<int> act(nc);
-  for (int k = 0; k < nc; ++k) act[k] = runs[k].done ? 0 : 1;
+  auto sync_levels = [&] {
+    for (int k = nr; k < nc; ++k) act[k] = act[0];
+  };
+  for (int k = 0; k < nr; ++k) act[k] = runs[k].done ? 0 : 1;
+  sync_levels();
   int rc = ar.set_active(act.data());
   if (rc) return rc;
   std::vector<double> res((size_t)SYNC * nc);
   std::vector<Forces> f;
   while (true) {
     int left = 0;
-    for (int k = 0; k < nc; ++k) left += !runs[k].done;
+    for (int k = 0; k < nr; ++k) left += !runs[k].done;
     if (!left) break;
     if ((rc = ar.run(SYNC, res.data()))) return rc;
     if ((rc = fp.run(ar, f))) return rc;
     dev_ms += ar.last_ms_per_iter * SYNC + fp.last_ms;
     if (device_ms) *device_ms = dev_ms;
     bool mask_changed = false;
-    for (int k = 0; k < nc; ++k) {
+    for (int k = 0; k < nr; ++k) {
       CaseRun& cr = runs[k];
       if (cr.done) continue;
       double mon = monitor_of(ar.cases[k], cr.p, f[k], cr.nseg);
@@ -281,6 +287,7 @@ inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
       }
       if (cr.done) act[k] = 0, mask_changed = true;
     }
+    sync_levels();
     if (mask_changed && (rc = ar.set_active(act.data()))) return rc;
   }
   return 0;

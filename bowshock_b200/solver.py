@@ -74,6 +74,7 @@ class MgParams:  # solver.rs:123-140 (DEFAULT): FAS multigrid with the SSP-RK3 s
     gamma: int = 1
     coarsest: int = 4
     cfl_star: float = 0.0  # implicit residual smoothing of the smoother (MgParams::irs)
+    implicit: "ImplicitParams | None" = None  # the line-implicit smoother (no counterpart in the reference) with these parameters
 
 
 @dataclass
@@ -162,6 +163,11 @@ class GpuSolver:
         elif isinstance(scheme, MgParams):
             s = _ffi.Scheme(kind=SCHEME_MULTIGRID, mg_levels=scheme.levels, mg_pre=scheme.pre, mg_post=scheme.post, mg_gamma=scheme.gamma,
                             mg_coarsest=scheme.coarsest, mg_cfl_star=scheme.cfl_star)
+            if scheme.implicit is not None:
+                p = scheme.implicit
+                s.mg_implicit = 1
+                s.cfl0, s.cfl_max, s.growth, s.dt_mode, s.lines = p.cfl0, p.cfl_max, p.growth, p.dt_mode, int(p.lines)
+                s.implicit_bc, s.sub_iters, s.roe, s.eps_fix = int(p.implicit_bc), int(p.sub_iters), int(p.roe), p.eps_fix
         else:
             p = scheme
             s = _ffi.Scheme(SCHEME_IMPLICIT, p.cfl0, p.cfl_max, p.growth, p.dt_mode, int(p.lines), int(p.implicit_bc),
@@ -239,6 +245,16 @@ class GpuSolver:
         d = C.c_double()
         self._check(_ffi.load().bowshock_solver_eval_residual(self._h, int(compute_dt), _dp(res), _dp(dt), C.byref(d)))
         return res.reshape(-1, 4), dt, d.value
+
+    PROFILE_GROUPS = ("prims", "viscous", "residual", "lines_i", "lines_j", "defect", "turbulence", "stage", "subst_i", "subst_j", "assemble",
+                      "turb_lines", "transfer")
+
+    def profile(self, n: int):
+        """Per-kernel-group device time over n iterations launched one kernel at a time: {group: (ms, launches)}."""
+        ms = np.zeros(len(self.PROFILE_GROUPS))
+        cnt = (C.c_uint64 * len(self.PROFILE_GROUPS))()
+        self._check(_ffi.load().bowshock_solver_profile(self._h, int(n), _dp(ms), cnt))
+        return {g: (float(ms[k]), int(cnt[k])) for k, g in enumerate(self.PROFILE_GROUPS)}
 
     def turb_residual(self) -> float:
         d = C.c_double()

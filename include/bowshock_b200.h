@@ -79,6 +79,10 @@ typedef struct {
   double eps_fix;
   uint64_t mg_levels, mg_pre, mg_post, mg_gamma, mg_coarsest;
   double cfl_star, mg_cfl_star;
+  /* multigrid with the line-implicit smoother (no counterpart in the reference, whose FAS smoother is SSP-RK3,
+   * multigrid.rs:87-112): each smoothing step one implicit iteration with the parameters above (cfl0 .. eps_fix) of the
+   * active level, from that level's own CFL ramp; the same FAS transfers */
+  int32_t mg_implicit;
 } bowshock_scheme;
 
 /* solver.rs:59-102 `Block` */
@@ -323,10 +327,12 @@ int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
 
 /* Per-kernel profile (the reference's Profile of gpu/mod.rs:533-542): n iterations launched one kernel at a time with CUDA
  * events around each launch; per kernel group (prims, viscous, residual, i-lines, j-lines (the factorising first pass),
- * defect, turbulence, stage, i- and j-substitution passes, block assembly, SST line systems) the
- * total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
-#define BOWSHOCK_PROFILE_GROUPS 12
+ * defect, turbulence, stage (and residual smoothing), i- and j-substitution passes, block assembly, SST line systems,
+ * multigrid transfers) the total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
+#define BOWSHOCK_PROFILE_GROUPS 13
 int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
+/* the same profile of a single-case solver (any scheme, multigrid levels included) */
+int bowshock_solver_profile(bowshock_solver* s, uint64_t n, double* ms, uint64_t* launches);
 /* Launch shapes of the arena's kernels. At creation (arenas of 100,000 cells or more; otherwise 4 lines per block, no
  * prefetching, variant 0) the autotuner picks, each the fastest in one timed iteration of the arena's own cases per
  * candidate (the state restored afterwards): per direction, lines per block (1, 2 or 4) of the block line solves' first
