@@ -150,3 +150,7 @@ class Arena:
         out = np.zeros(n.value)
         self._check(_ffi.load().bowshock_arena_residual_history(self._h, int(k), _ffi.dptr(out), n.value, C.byref(n)))
         return out
+
+    def set_run_control(self, on_device: bool):
+        """Stop rules of solve() on the device after every chunk (True, the default) or on the host (False)."""
+        self._check(_ffi.load().bowshock_arena_set_run_control(self._h, int(bool(on_device))))

@@ -863,6 +863,12 @@ int bowshock_arena_residual_history(const bowshock_arena* a, uint64_t k, double*
   return BOWSHOCK_OK;
 }
 
+int bowshock_arena_set_run_control(bowshock_arena* a, int on_device) {
+  if (!a) return BOWSHOCK_INVALID;
+  a->ar.device_run_control = on_device != 0;
+  return BOWSHOCK_OK;
+}
+
 int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active) {
   if (!a || !active) return BOWSHOCK_INVALID;
   std::vector<int> v(active, active + a->ar.cases.size());
@@ -902,6 +908,12 @@ extern "C" int bowshock_solver_profile(bowshock_solver* s, uint64_t n, double* m
     ms[g] = s->ar.prof_ms[g];
     launches[g] = (uint64_t)s->ar.prof_launches[g];
   }
+  return BOWSHOCK_OK;
+}
+
+extern "C" int bowshock_solver_set_run_control(bowshock_solver* s, int on_device) {
+  if (!s) return BOWSHOCK_INVALID;
+  s->ar.device_run_control = on_device != 0;
   return BOWSHOCK_OK;
 }
 

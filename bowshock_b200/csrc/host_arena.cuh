@@ -1204,6 +1204,8 @@ struct ArenaHost {
   }
 
   bool use_graphs = true;
+  // the stop rules of a solve evaluated on the device after every chunk (runner.cuh: k_run_control); false: on the host
+  bool device_run_control = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms_per_iter = 0.0;
   // one chunk of `chunk` iterations: captured once into a CUDA graph, replayed afterwards

@@ -3,6 +3,7 @@
 // device->host exchange, the stop iteration found CPU-equivalently inside a chunk) and, for the batched arena, the
 // per-case convergence masks. Each chunk of iterations is captured once into a CUDA graph and replayed.
 #pragma once
+#include <cstddef>
 #include <functional>
 
 #include "forces.cuh"
@@ -108,6 +109,7 @@ struct CaseRun {
   bool done = false;
   int reason = 0;
   double last_monitor = NAN;
+  double cd_window = NAN;  // set by the device run control when it stops a case on the mean-stationary rule
 };
 
 struct ForcePass {
@@ -212,7 +214,9 @@ inline void fill_point(const CaseRun& cr, const Forces& f, bowshock_point_result
   o->cd_window = o->forces.cd_total;
   // mean stationary: the mean of the last window the rule compared (run.rs:157-172); its 120 samples lie on the
   // limit cycle, so the value does not depend on the 50-iteration chunk at which the rule first holds
-  if (cr.reason == 4 && cr.p.mean_window >= SYNC) {
+  if (cr.reason == 4 && !std::isnan(cr.cd_window)) {
+    o->cd_window = cr.cd_window;
+  } else if (cr.reason == 4 && cr.p.mean_window >= SYNC) {
     size_t k = (size_t)(cr.p.mean_window / SYNC);
     if (cr.hist.size() >= k) {
       double m = 0.0;
@@ -220,6 +224,140 @@ inline void fill_point(const CaseRun& cr, const Forces& f, bowshock_point_result
       o->cd_window = m / (double)k;
     }
   }
+}
+
+// ==================================================================================== GPU-resident run control
+// The stop rules above evaluated on the device after every chunk (no counterpart in the reference, whose rules run on
+// the host, engine/gpu.rs:123-164): one thread per case walks the chunk's iterations with the density residuals of the
+// arena's residual sums and the monitor of the FP64 force pass, in the same order and arithmetic as stop_reason (the
+// drop threshold 10^drop_orders is computed on the host, so no device pow enters a decision), and keeps the monitor
+// samples in a ring of RUN_RING entries. The host reads back only each case's status.
+constexpr int RUN_RING = 256;  // monitor samples kept: twice a mean window of 6,400 iterations
+struct RunDev {
+  long long max_iter, min_iter, monitor_window, mean_window;
+  double drop_thresh, monitor_tol, drag_rel_tol, r_ref, n_active;
+  int has_monitor_tol, has_mean_window, has_drag_rel_tol, wake, viscous, nseg, cd_of_wake_base;
+  // state
+  long long it, skip;
+  double rmax, last_r, last_monitor, cd_window;
+  int done, reason, nh, n_after;  // samples so far, samples past iteration 2000
+  long long hit[RUN_RING];
+  double hv[RUN_RING];
+};
+
+__device__ __forceinline__ double ring(const RunDev& d, int q) { return d.hv[q % RUN_RING]; }
+
+// run.rs:157-170 on the last 2k samples of the ring
+__device__ bool mean_stationary_dev(const RunDev& d, int k) {
+  if (k == 0 || d.n_after < 2 * k) return false;
+  const int b = d.nh - 2 * k;
+  double m0 = 0, m1 = 0;
+  for (int t = 0; t < k; ++t) m0 += ring(d, b + t);
+  for (int t = k; t < 2 * k; ++t) m1 += ring(d, b + t);
+  m0 /= (double)k;
+  m1 /= (double)k;
+  double m = 0.5 * (m0 + m1), lo = INFINITY, hi = -INFINITY;
+  for (int t = 0; t < 2 * k; ++t) lo = fmin(lo, ring(d, b + t)), hi = fmax(hi, ring(d, b + t));
+  double a = ring(d, b + 2 * k - 2) - m, c = ring(d, b + 2 * k - 1) - m;
+  return fabs(m1 - m0) <= 2e-3 * fabs(m) && hi - lo <= 0.05 * fabs(m) && a * c < 0.0;
+}
+
+// run.rs:105-150, the device restatement of stop_reason
+__device__ bool stop_reason_dev(const RunDev& d, long long it, double r, double reference, int& why) {
+  const bool sampled_now = d.nh > 0 && d.hit[(d.nh - 1) % RUN_RING] == it + 1;
+  if (!isfinite(r) || (sampled_now && (!isfinite(ring(d, d.nh - 1)) || fabs(ring(d, d.nh - 1)) > 1e3))) {
+    why = 5;
+    return true;
+  }
+  if (it + 1 < d.min_iter) return false;
+  if (it > d.skip && reference / r >= d.drop_thresh) {
+    why = 1;
+    return true;
+  }
+  if (d.has_drag_rel_tol) {
+    const int k = (int)(DRAG_REL_WINDOW / SYNC);
+    if (d.viscous && sampled_now && it + 1 >= (long long)DRAG_REL_WINDOW && reference / r >= 100.0 && d.nh >= k) {
+      double lo = INFINITY, hi = -INFINITY, mean = 0;
+      for (int t = d.nh - k; t < d.nh; ++t) lo = fmin(lo, ring(d, t)), hi = fmax(hi, ring(d, t)), mean += ring(d, t);
+      mean /= (double)k;
+      if (hi - lo < d.drag_rel_tol * fabs(mean)) {
+        why = 2;
+        return true;
+      }
+    }
+  }
+  if (d.has_monitor_tol && it % 500 == 499 && it + 1 >= 2 * d.monitor_window && reference / r >= 100.0) {
+    const int k = (int)(d.monitor_window / SYNC);
+    if (d.nh >= k) {
+      double lo = INFINITY, hi = -INFINITY;
+      for (int t = d.nh - k; t < d.nh; ++t) lo = fmin(lo, ring(d, t)), hi = fmax(hi, ring(d, t));
+      if (hi - lo < d.monitor_tol) {
+        why = (!d.viscous && d.wake == 1) ? 3 : 2;
+        return true;
+      }
+    }
+  }
+  if (d.viscous && d.has_mean_window && sampled_now && mean_stationary_dev(d, (int)(d.mean_window / SYNC))) {
+    why = 4;
+    return true;
+  }
+  return false;
+}
+
+// One chunk of `n` iterations for every case still running: residuals from rsum [slot][case], the monitor from the force
+// pass output (run.rs:174-185: the total CD of a viscous case, else the nose CD of a sting or the base Cp of a base wake).
+__global__ void k_run_control(RunDev* runs, int nruns, const double* __restrict__ rsum, int ncases, const double* __restrict__ forces, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nruns) return;
+  RunDev& d = runs[k];
+  if (d.done) return;
+  const double* f = forces + (size_t)k * F_NF;
+  double mon;
+  if (d.viscous) {
+    double fore = f[F_CD_NOSE];
+    for (int s = 0; s < d.nseg; ++s) fore = fore + f[F_CD_AFT0 + s];
+    mon = fore + f[F_CD_FRICTION] + f[F_CD_BASE];
+  } else {
+    mon = d.wake == 0 ? f[F_CD_NOSE] : f[F_CP_BASE];
+  }
+  const bool sample = d.wake == 1 || d.has_monitor_tol || d.has_drag_rel_tol;
+  for (int t = 0; t < n && !d.done; ++t) {
+    const long long it = d.it;
+    const double r = sqrt(rsum[(size_t)t * ncases + k] / d.n_active);
+    d.last_r = r;
+    if (it >= d.skip) d.rmax = fmax(d.rmax, r);
+    if (sample && it % SYNC == SYNC - 1) {
+      d.hit[d.nh % RUN_RING] = it + 1;
+      d.hv[d.nh % RUN_RING] = mon;
+      d.nh += 1;
+      if (it + 1 > 2000) d.n_after += 1;
+      d.last_monitor = mon;
+    }
+    int why = 0;
+    if (stop_reason_dev(d, it, r, d.r_ref >= 0 ? d.r_ref : d.rmax, why)) {
+      d.done = 1;
+      d.reason = why;
+      if (why == 4 && d.mean_window >= SYNC) {  // the mean of the last window the rule compared
+        const int kk = (int)(d.mean_window / SYNC);
+        double m = 0.0;
+        for (int q = d.nh - kk; q < d.nh; ++q) m += ring(d, q);
+        d.cd_window = m / (double)kk;
+      }
+    } else if (it + 1 >= d.max_iter) {
+      d.done = 1;
+      d.reason = 0;
+    }
+    d.it += 1;
+  }
+}
+
+// Whether the stop rules of these runs fit the device ring (their windows at most RUN_RING / 2 mean samples)
+inline bool device_control_fits(const std::vector<CaseRun>& runs) {
+  for (const CaseRun& cr : runs) {
+    if (cr.p.has_mean_window && 2 * (cr.p.mean_window / SYNC) > RUN_RING) return false;
+    if (cr.p.has_monitor_tol && cr.p.monitor_window / SYNC > RUN_RING) return false;
+  }
+  return true;
 }
 
 // Cold (or warm) start of case k for a run: free stream, turbulence re-initialised, counters reset (run.rs:44-63).
@@ -251,6 +389,33 @@ inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
   if (rc) return rc;
   std::vector<double> res((size_t)SYNC * nc);
   std::vector<Forces> f;
+  // the stop rules on the device (the host then reads each case's status) unless switched off or beyond the ring
+  const bool dev = ar.device_run_control && device_control_fits(runs);
+  std::vector<RunDev> hr(dev ? nr : 0);
+  RunDev* d_runs = nullptr;
+  struct Free {
+    RunDev*& p;
+    ~Free() {
+      if (p) cudaFree(p);
+    }
+  } free_runs{d_runs};
+  const size_t head = offsetof(RunDev, hit);  // the parameters and the status, without the monitor ring
+  if (dev) {
+    for (int k = 0; k < nr; ++k) {
+      const CaseRun& cr = runs[k];
+      RunDev& d = hr[k];
+      std::memset(&d, 0, sizeof(RunDev));
+      d.max_iter = cr.p.max_iter, d.min_iter = cr.p.min_iter, d.monitor_window = cr.p.monitor_window, d.mean_window = cr.p.mean_window;
+      d.drop_thresh = std::pow(10.0, cr.p.drop_orders), d.monitor_tol = cr.p.monitor_tol, d.drag_rel_tol = cr.p.drag_rel_tol;
+      d.r_ref = cr.p.r_ref, d.n_active = (double)ar.desc[k].n_active;
+      d.has_monitor_tol = cr.p.has_monitor_tol, d.has_mean_window = cr.p.has_mean_window, d.has_drag_rel_tol = cr.p.has_drag_rel_tol;
+      d.wake = cr.p.wake, d.viscous = ar.cases[k].viscous ? 1 : 0, d.nseg = cr.nseg;
+      d.it = cr.it, d.skip = cr.skip, d.rmax = cr.rmax, d.done = cr.done ? 1 : 0, d.last_monitor = NAN, d.cd_window = NAN;
+    }
+    std::string& err = ar.err;
+    BK_CUDA(cudaMalloc(&d_runs, (size_t)nr * sizeof(RunDev)));
+    BK_CUDA(cudaMemcpy(d_runs, hr.data(), (size_t)nr * sizeof(RunDev), cudaMemcpyHostToDevice));
+  }
   while (true) {
     int left = 0;
     for (int k = 0; k < nr; ++k) left += !runs[k].done;
@@ -259,31 +424,50 @@ inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
     if ((rc = fp.run(ar, f))) return rc;
     dev_ms += ar.last_ms_per_iter * SYNC + fp.last_ms;
     if (device_ms) *device_ms = dev_ms;
+    if (dev) {
+      std::string& err = ar.err;
+      k_run_control<<<(nr + 127) / 128, 128, 0, ar.stream>>>(d_runs, nr, ar.A.rsum, nc, fp.out, SYNC);
+      BK_CUDA(cudaGetLastError());
+      BK_CUDA(cudaMemcpy2DAsync(hr.data(), sizeof(RunDev), d_runs, sizeof(RunDev), head, nr, cudaMemcpyDeviceToHost, ar.stream));
+      BK_CUDA(cudaStreamSynchronize(ar.stream));
+    }
     bool mask_changed = false;
     for (int k = 0; k < nr; ++k) {
       CaseRun& cr = runs[k];
       if (cr.done) continue;
       double mon = monitor_of(ar.cases[k], cr.p, f[k], cr.nseg);
-      bool sample = cr.p.wake == 1 || cr.p.has_monitor_tol || cr.p.has_drag_rel_tol;
-      for (int t = 0; t < SYNC && !cr.done; ++t) {
-        long long it = cr.it;
-        double r = res[(size_t)t * nc + k];
-        cr.residual.push_back(r);
-        if (it >= cr.skip) cr.rmax = std::fmax(cr.rmax, r);
-        if (sample && it % SYNC == SYNC - 1) cr.hist.emplace_back(it + 1, mon), cr.last_monitor = mon;
-        int why = 0;
-        if (stop_reason(cr.p, ar.cases[k].viscous, it, r, cr.p.r_ref >= 0 ? cr.p.r_ref : cr.rmax, cr.skip, cr.hist, why)) {
-          cr.done = true;
-          cr.reason = why;
-        } else if (it + 1 >= cr.p.max_iter) {
-          cr.done = true;
-          cr.reason = 0;
+      if (dev) {  // the device's decision; the host keeps the residual history
+        const RunDev& d = hr[k];
+        for (long long t = 0; cr.it + t < d.it; ++t) cr.residual.push_back(res[(size_t)t * nc + k]);
+        cr.it = d.it, cr.rmax = d.rmax, cr.last_monitor = d.last_monitor;
+        if (d.done) cr.done = true, cr.reason = d.reason, cr.cd_window = d.cd_window;
+      } else {
+        bool sample = cr.p.wake == 1 || cr.p.has_monitor_tol || cr.p.has_drag_rel_tol;
+        for (int t = 0; t < SYNC && !cr.done; ++t) {
+          long long it = cr.it;
+          double r = res[(size_t)t * nc + k];
+          cr.residual.push_back(r);
+          if (it >= cr.skip) cr.rmax = std::fmax(cr.rmax, r);
+          if (sample && it % SYNC == SYNC - 1) cr.hist.emplace_back(it + 1, mon), cr.last_monitor = mon;
+          int why = 0;
+          if (stop_reason(cr.p, ar.cases[k].viscous, it, r, cr.p.r_ref >= 0 ? cr.p.r_ref : cr.rmax, cr.skip, cr.hist, why)) {
+            cr.done = true;
+            cr.reason = why;
+          } else if (it + 1 >= cr.p.max_iter) {
+            cr.done = true;
+            cr.reason = 0;
+          }
+          cr.it += 1;
         }
-        cr.it += 1;
       }
       if (!cr.done && progress && !progress(k, cr.it, cr.residual.back(), mon)) {
         cr.done = true;
         cr.reason = 6;
+        if (dev) {  // the device stops iterating this run too
+          std::string& err = ar.err;
+          const int one = 1;
+          BK_CUDA(cudaMemcpy(reinterpret_cast<char*>(d_runs + k) + offsetof(RunDev, done), &one, sizeof(int), cudaMemcpyHostToDevice));
+        }
       }
       if (cr.done) act[k] = 0, mask_changed = true;
     }

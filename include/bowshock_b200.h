@@ -317,6 +317,11 @@ int bowshock_arena_first_residuals(bowshock_arena* a, const int32_t* warm, doubl
 /* The density residual of every iteration of case k in the last bowshock_arena_solve (n entries; at most cap copied into
  * out, which may be NULL to query n): the history GpuRunner::run_on keeps per run (engine/gpu.rs:143-158). */
 int bowshock_arena_residual_history(const bowshock_arena* a, uint64_t k, double* out, uint64_t cap, uint64_t* n);
+/* Where bowshock_arena_solve evaluates the stop rules (engine/run.rs:105-170): on the device after every 50-iteration
+ * chunk (1, the default: one thread per case restates the rules, the host reads back each case's status), or on the
+ * host from the read-back residuals and monitor (0, as engine/gpu.rs:123-164 does). The decisions are the same; a
+ * mean window beyond 6,400 iterations always runs on the host. No counterpart in the reference. */
+int bowshock_arena_set_run_control(bowshock_arena* a, int on_device);
 /* per-case activity mask (1 = iterate), ncases entries */
 int bowshock_arena_set_active(bowshock_arena* a, const int32_t* active);
 /* mean device time of one arena iteration over the last bowshock_arena_run, in milliseconds (CUDA events) */
@@ -331,6 +336,8 @@ int bowshock_arena_last_solve_ms(const bowshock_arena* a, double* ms);
  * multigrid transfers) the total milliseconds and launch counts (BOWSHOCK_PROFILE_GROUPS entries each). */
 #define BOWSHOCK_PROFILE_GROUPS 13
 int bowshock_arena_profile(bowshock_arena* a, uint64_t n, double* ms, uint64_t* launches);
+/* bowshock_arena_set_run_control for bowshock_solver_run_to_stop */
+int bowshock_solver_set_run_control(bowshock_solver* s, int on_device);
 /* the same profile of a single-case solver (any scheme, multigrid levels included) */
 int bowshock_solver_profile(bowshock_solver* s, uint64_t n, double* ms, uint64_t* launches);
 /* Launch shapes of the arena's kernels. At creation (arenas of 100,000 cells or more; otherwise 4 lines per block, no
