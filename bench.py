@@ -512,6 +512,20 @@ def run_kernels(args):
     import torch
 
     import bowshock_b200  # noqa: F401
+    if args.workload == "net":  # training steps of the warm-start network (batch 64): its tensor-core GEMMs
+        from bowshock_b200 import learned as lw
+        from bowshock_b200.net import Net, flops_per_sample
+        net = Net(max_batch=64)
+        net.set_params(lw.init_params(0, net.layout(), net.nparams))
+        rng = np.random.default_rng(0)
+        net.set_dataset(rng.standard_normal((256, 16)).astype(np.float32), rng.standard_normal((256, 2048 * 6)).astype(np.float32))
+        net.train(max(args.warmup, 3), 64, 1e-4)
+        torch.cuda.profiler.start()
+        net.train(args.steps, 64, 1e-4)
+        torch.cuda.profiler.stop()
+        ms = net.last_train_ms() / args.steps
+        fl = 3.0 * flops_per_sample(net.layout()) * 64
+        return {"kernels_only": True, "workload": "net", "steps": args.steps, "ms_per_step": ms, "tflops": fl / (ms / 1000.0) / 1e12}
     if args.workload == "lift3":
         import bowshock_b200.euler3 as e3
         b, _ = e3.batch_of(e3.lift_sweep_cases())
@@ -544,7 +558,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kernels-only", action="store_true", help="only the timed arena iterations (for ncu captures)")
-    ap.add_argument("--workload", default="sweep32", choices=["sweep32", "tail6", "lift3"], help="workload of --kernels-only")
+    ap.add_argument("--workload", default="sweep32", choices=["sweep32", "tail6", "lift3", "net"], help="workload of --kernels-only")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # one process per GPU: start the ranks here when the command was not launched by torchrun

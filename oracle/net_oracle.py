@@ -80,8 +80,9 @@ def _conv_forward(x, w, b):
     return y
 
 
-def forward(params, x, L=None):
-    """x [B, 16] -> (out [B, 32, 64, 16] linear output, cache of every layer's input and output)."""
+def forward(params, x, L=None, bf16=False):
+    """x [B, 16] -> (out [B, 32, 64, 16] linear output, cache of every layer's input and output). bf16: round every
+    activated layer's output to BF16, as the tensor-core path stores its activations."""
     if L is None:
         L, _ = layers()
     p = np.asarray(params, dtype=np.float64)
@@ -98,19 +99,22 @@ def forward(params, x, L=None):
             xin = h.reshape(B, l["H"] >> l["up"], l["W"] >> l["up"], l["cin"])
             z = _conv_forward(_up(xin, l["up"]), W.reshape(l["cout"], 3, 3, l["cin"]), b)
         y = _lrelu(z) if l["act"] else z
+        if bf16 and l["act"]:
+            y = bf16_round(y.astype(np.float32)).astype(np.float64)
         cache.append((xin, y))
         h = y
     return h.reshape(B, H_OUT, W_OUT, NET_OUT_PAD), cache
 
 
-def loss_and_grad(params, x, target, mask, L=None):
-    """Masked mean squared error over [B, 2048, 6] (mean over every entry, masked ones counting 0) and its gradient."""
+def loss_and_grad(params, x, target, mask, L=None, bf16=False):
+    """Masked mean squared error over [B, 2048, 6] (mean over every entry, masked ones counting 0) and its gradient.
+    bf16: the tensor-core path's roundings (BF16 activations, BF16 output gradients of every layer), the rest float64."""
     if L is None:
         L, n = layers()
     else:
         n = len(params)
     p = np.asarray(params, dtype=np.float64)
-    out, cache = forward(p, x, L)
+    out, cache = forward(p, x, L, bf16=bf16)
     B = out.shape[0]
     o = out.reshape(B, NET_CELLS, NET_OUT_PAD)[:, :, :NET_OUT]
     t = np.asarray(target, dtype=np.float64).reshape(B, NET_CELLS, NET_OUT)
@@ -126,6 +130,8 @@ def loss_and_grad(params, x, target, mask, L=None):
         l = L[k]
         xin, y = cache[k]
         gz = gy * np.where(y > 0.0, 1.0, SLOPE) if l["act"] else gy
+        if bf16:
+            gz = bf16_round(gz.astype(np.float32)).astype(np.float64)
         W = p[l["woff"]:l["woff"] + l["cout"] * l["kin"]].reshape(l["cout"], l["kin"])
         if l["fc"]:
             gz2 = gz.reshape(B, l["cout"])

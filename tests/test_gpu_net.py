@@ -4,9 +4,10 @@ forward pass and its gradients against the float64 CPU oracle (oracle/net_oracle
 differences) on the same BF16-rounded weights and inputs; and a short training run that lowers the loss.
 
 Tolerances: the GEMM accumulates exactly-representable BF16 products in FP32, so it agrees with the FP32 matmul to
-round-off of the summation order (1e-4 relative to the row scale). The network rounds every activation to BF16 between
-layers (8 significant bits), so its outputs and gradients agree with the float64 oracle to a few per cent in the
-relative L2 norm (3e-2 outputs, 8e-2 per-layer gradients)."""
+round-off of the summation order (1e-4 relative to the row scale). The network rounds every activation and every
+layer's output gradient to BF16 (8 significant bits), so its outputs agree with the float64 oracle to 3e-2 in the
+relative L2 norm, and its gradients to 3e-2 against the oracle with the same roundings emulated (1.5e-1 against the
+exact oracle, where the rounding compounds through ten layers)."""
 import ctypes as C
 
 import numpy as np
@@ -78,17 +79,28 @@ def test_net_forward_matches_oracle():
 
 
 def test_net_gradients_match_oracle():
+    """Against the oracle with the tensor-core path's BF16 roundings emulated (activations and each layer's output
+    gradient stored as BF16): every layer's weight and bias gradients to 3e-2 in the relative L2 norm (the remaining
+    difference is FP32 against float64 accumulation, which moves a few BF16 roundings); against the exact float64
+    oracle, the rounding compounds through the ten layers below the output, to 1.5e-1 at the first layer."""
     net, L, n, pr, x, rng = _net_and_oracle()
     t = rng.standard_normal((x.shape[0], no.NET_CELLS, no.NET_OUT)).astype(np.float32) * 0.5
     mask = (rng.random(no.NET_CELLS) > 0.15).astype(np.uint8)
     net.set_mask(mask)
     loss, g = net.gradients(x, t)
+    lemu, gemu = no.loss_and_grad(pr, x, t, mask, L, bf16=True)
     lref, gref = no.loss_and_grad(pr, x, t, mask, L)
-    assert abs(loss - lref) / lref < 1e-2, f"loss {loss} vs {lref}"
+    assert abs(loss - lemu) / lemu < 1e-2 and abs(loss - lref) / lref < 1e-2, f"loss {loss} vs {lemu} / {lref}"
+    worst = []
     for k, l in enumerate(L):
         for name, sl in (("W", slice(l["woff"], l["woff"] + l["cout"] * l["kin"])), ("b", slice(l["boff"], l["boff"] + l["cout"]))):
-            rel = np.linalg.norm(g[sl] - gref[sl]) / (np.linalg.norm(gref[sl]) + 1e-30)
-            assert rel < 8e-2, f"layer {k} {name}: gradient rel L2 err {rel:.3e}"
+            rel_e = np.linalg.norm(g[sl] - gemu[sl]) / (np.linalg.norm(gemu[sl]) + 1e-30)
+            rel_x = np.linalg.norm(g[sl] - gref[sl]) / (np.linalg.norm(gref[sl]) + 1e-30)
+            worst.append((k, name, rel_e, rel_x))
+    print("per-layer gradient rel L2 err (emulated BF16, exact):", [(k, nm, f"{a:.2e}", f"{b:.2e}") for k, nm, a, b in worst])
+    for k, name, rel_e, rel_x in worst:
+        assert rel_e < 3e-2, f"layer {k} {name}: gradient rel L2 err {rel_e:.3e} against the BF16-emulating oracle"
+        assert rel_x < 1.5e-1, f"layer {k} {name}: gradient rel L2 err {rel_x:.3e} against the exact oracle"
 
 
 def test_net_training_lowers_the_loss():
