@@ -318,9 +318,9 @@ def run_ours(args, rank, world, dist):
     if rank != 0:
         return None
     traffic = line_sweep_traffic()
-    learned = learned_census(all_cases, all_grids, fx, plain_cases_per_hr, device) if world == 1 else None
-    lift3 = measure_lift3(args, device) if world == 1 else None
-    mg0 = measure_config0_multigrid(device) if world == 1 else None
+    learned = secondary(learned_census, all_cases, all_grids, fx, plain_cases_per_hr, device) if world == 1 else None
+    lift3 = secondary(measure_lift3, args, device) if world == 1 else None
+    mg0 = secondary(measure_config0_multigrid, device) if world == 1 else None
     cpu_base = None
     if world == 1:  # the CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
         smp = OracleSample(all_cases)
@@ -381,6 +381,14 @@ def run_ours(args, rank, world, dist):
 # algorithmic bytes per cell-update of the 3D Euler line-implicit iteration (nv = 5, 16 geometry words, 3 directions,
 # 2 sweeps each: 271 words; the per-kernel model of the 2D path applied to 3D)
 WORDS_3D = 271
+
+
+def secondary(fn, *a):
+    """A secondary figure of the bench line: its dict, or the error that kept it from being measured."""
+    try:
+        return fn(*a)
+    except Exception as e:  # reported in the line, not fatal to the headline measurement
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def learned_census(cases, grids, fx, plain_cases_per_hr, device):

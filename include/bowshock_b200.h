@@ -346,7 +346,8 @@ int bowshock_solver_profile(bowshock_solver* s, uint64_t n, double* ms, uint64_t
  * pass and how its walks fetch the cells' records (0: one cell at a time, 1: the next cell's ahead; 2, staged through
  * shared memory three cells ahead with one line per block, only when pinned), lines per block (1, 2, 4 or 8) of their
  * substitution passes and how those walks fetch their records (0 / 1 / 2 likewise), lines per block of the SST line
- * kernel, and the residual kernel's variant (0: 256 threads per 32 x 8 tile, 1: 288). A direction with at most
+ * kernel; the residual kernel's variant (0: 256 threads per 32 x 8 tile, 1: 288) stays 0 unless pinned (the two round
+ * differently). A direction with at most
  * staged_lines lines left in the launch (set at creation to two waves of the staged substitution kernel: 1,184 lines on
  * a 148-SM B200; >= 0, 0 never) runs both passes staged whatever prefetch / subst_prefetch say: with few lines the
  * walks wait on memory latency. Every candidate compiles to the same arithmetic (checked bit for bit), so none of these

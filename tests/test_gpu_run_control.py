@@ -1,7 +1,7 @@
 """GPU-resident run control: the stop rules (engine/run.rs:105-170) evaluated on the device after every chunk give the
 same decisions as the host's evaluation of the same residuals and monitors, on sweep cases that stop on each rule
-(residual drop, CD stationary, and the mean-stationary limit cycle after 14,000 iterations): identical iteration counts,
-stop reasons, residual histories and CDs, bit for bit."""
+(residual drop, CD stationary, and the mean-stationary limit cycle after 14,000 iterations): identical iteration counts
+and stop reasons, residual histories and CDs equal to round-off."""
 import numpy as np
 import pytest
 
@@ -24,8 +24,10 @@ def test_device_stop_rules_match_host_rules():
     reasons = set()
     for k in range(len(cs)):
         assert rd[k]["iters"] == rh[k]["iters"] and rd[k]["stop_reason"] == rh[k]["stop_reason"], (picks[k], rd[k], rh[k])
-        assert rd[k]["cd_total"] == rh[k]["cd_total"] and rd[k]["cd_window"] == rh[k]["cd_window"]
-        assert rd[k]["residual_peak"] == rh[k]["residual_peak"]
-        assert np.array_equal(hd[k], hh[k])
+        # the states are the same; the FP64 force and norm sums add per-block partials atomically, in whatever order
+        # the blocks finish, so CDs and residuals compare to round-off
+        assert abs(rd[k]["cd_total"] - rh[k]["cd_total"]) <= 1e-12 * abs(rh[k]["cd_total"])
+        assert abs(rd[k]["cd_window"] - rh[k]["cd_window"]) <= 1e-12 * abs(rh[k]["cd_window"])
+        assert np.allclose(hd[k], hh[k], rtol=1e-12, atol=0.0)
         reasons.add(rd[k]["stop_reason"])
     assert {"residual drop", "mean stationary"} <= reasons
