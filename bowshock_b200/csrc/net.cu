@@ -271,14 +271,51 @@ __global__ void k_flip_weights(const bf16* __restrict__ w, int Cin, int Cout, bf
   }
 }
 
-// db[c] += sum over rows of g[r][c] (rows split over blocks)
+// db[c] += sum over rows of g[r][c]: blocks of 32 columns x 8 row groups over a slice of the rows, reduced through
+// shared memory, one atomic per column and block
 __global__ void k_bias_grad(const bf16* __restrict__ g, long long rows, int C, float* __restrict__ db) {
-  const long long per = (rows + gridDim.x - 1) / gridDim.x;
-  const long long r0 = blockIdx.x * per, r1 = min(rows, r0 + per);
-  for (int c = threadIdx.x; c < C; c += blockDim.x) {
-    float s = 0.f;
-    for (long long r = r0; r < r1; ++r) s += __bfloat162float(g[r * C + c]);
-    atomicAdd(db + c, s);
+  __shared__ float part[8][33];
+  const int c = blockIdx.x * 32 + threadIdx.x;
+  const long long per = (rows + gridDim.y - 1) / gridDim.y;
+  const long long r0 = blockIdx.y * per, r1 = min(rows, r0 + per);
+  float acc = 0.f;
+  if (c < C)
+    for (long long r = r0 + threadIdx.y; r < r1; r += 8) acc += __bfloat162float(g[r * C + c]);
+  part[threadIdx.y][threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < C) {
+    float t = 0.f;
+    for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x];
+    atomicAdd(db + c, t);
+  }
+}
+
+// The transposed im2col of a 3x3 'same' convolution's input (the dW operand): colT[(tap * C + c)][p], p over the
+// B * H * W output pixels, written directly in 32 x 32 tiles through shared memory (reads along the channels, writes
+// along the pixels); up = 1 reads the input through the nearest 2x upsampling.
+__global__ void k_im2col_t(const bf16* __restrict__ x, int B, int Hin, int Win, int C, int up, bf16* __restrict__ colT, long long P) {
+  __shared__ bf16 t[32][33];
+  const int H = Hin << up, W = Win << up;
+  const long long p0 = (long long)blockIdx.x * 32;
+  const int cblocks = (C + 31) / 32;
+  const int tap = blockIdx.y / cblocks, c0 = (blockIdx.y % cblocks) * 32;
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const long long p = p0 + k;
+    const int c = c0 + threadIdx.x;
+    bf16 v = __float2bfloat16_rn(0.f);
+    if (p < P && c < C) {
+      const int xo = (int)(p % W), yo = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+      const int yy = yo + dy, xx = xo + dx;
+      if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = x[(((long long)b * Hin + (yy >> up)) * Win + (xx >> up)) * C + c];
+    }
+    t[k][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int c = c0 + k;
+    const long long p = p0 + threadIdx.x;
+    if (c < C && p < P) colT[((long long)tap * C + c) * P + p] = t[threadIdx.x][k];
   }
 }
 
@@ -638,9 +675,8 @@ struct Net {
         XT = colT;
       } else {
         const int Hin = l.H >> l.up, Win = l.W >> l.up;
-        k_im2col<<<grid_for(r * 9 * (l.cin / 8)), 256, 0, stream>>>(xin, B, Hin, Win, l.cin, l.up, col);
-        dim3 tx((unsigned)((l.kin + 31) / 32), (unsigned)((r + 31) / 32));
-        k_transpose<<<tx, dim3(32, 8), 0, stream>>>(col, l.kin, (int)r, (int)l.kin, colT, r);
+        dim3 tx((unsigned)((r + 31) / 32), (unsigned)(9 * ((l.cin + 31) / 32)));
+        k_im2col_t<<<tx, dim3(32, 8), 0, stream>>>(xin, B, Hin, Win, l.cin, l.up, colT, r);
         XT = colT;
       }
       GemmArgs gd{};
@@ -648,7 +684,8 @@ struct Net {
       const int tiles = ((l.cout + BM - 1) / BM) * (int)((l.kin + pick_bn((int)l.kin) - 1) / pick_bn((int)l.kin));
       const int splits = std::max(1, 2 * 148 / tiles);
       if ((rc = gemm(gT, r, XT, r, l.cout, (int)l.kin, (int)r, gd, splits, stream, err))) return rc;
-      k_bias_grad<<<std::min<long long>(148, (r + 63) / 64), 128, 0, stream>>>(g, r, l.cout, gw + l.boff);
+      k_bias_grad<<<dim3((unsigned)((l.cout + 31) / 32), (unsigned)std::min<long long>(1024, (r + 255) / 256)), dim3(32, 8), 0, stream>>>(
+          g, r, l.cout, gw + l.boff);
       if (k == 0) break;
       // dX = g W (through the flipped convolution); then the previous layer's leaky ReLU derivative
       GemmArgs gx{};
