@@ -396,7 +396,8 @@ def learned_census(cases, grids, fx, plain_cases_per_hr, device):
     cold probe of every case (its first residual is the fallback rule's base, its peak after iteration 20 the warm runs'
     drop reference), then every SST case restarted from the network's predicted field (unless its first residual exceeds
     10x the cold one), the Euler cases cold (the network models the SST base-wake flows), all to the reference's stop
-    rules; device time of the probe and the solve; CDs against the oracle."""
+    rules, a warm run that ends neither converged nor stationary solved again cold; device time of the probe and the
+    solves; CDs against the oracle."""
     from bowshock_b200 import learned as lw
     from bowshock_b200.arena import Arena
     if not os.path.exists(lw.WEIGHTS):
@@ -421,6 +422,16 @@ def learned_census(cases, grids, fx, plain_cases_per_hr, device):
         a.set_run(k, c.numerics, warm=bool(warm), r_ref=float(probe[20:, k].max()) if warm else None)
     res = a.solve()
     dev_s = (probe_ms + a.last_solve_ms()) / 1000.0
+    # the reference keeps a warm result only when it converged or became stationary (analysis.rs:744-771): the rest
+    # are solved again from the free stream
+    redo = [k for k in sst if k not in fallback and res[k]["stop_reason"] not in lw.ACCEPTED]
+    if redo:
+        b = Arena([cases[k] for k in redo], device=device, grids=[grids[k] for k in redo])
+        rr = b.solve()
+        dev_s += b.last_solve_ms() / 1000.0
+        for q, k in enumerate(redo):
+            res[k] = rr[q]
+        del b
     wall = time.perf_counter() - t0
     del a
     dcd = {k: cd_error(res[k], fx[k]) for k in range(len(cases)) if k in fx}
@@ -429,6 +440,7 @@ def learned_census(cases, grids, fx, plain_cases_per_hr, device):
     e2e = 3600.0 * n_ok / wall
     return {"census_device_s": dev_s, "census_wall_s": wall, "converged_within_1e-4": n_ok, "checked_against_oracle": len(dcd),
             "cases_per_hr": value, "e2e_cases_per_hr": e2e, "warm_cases": [k for k in sst if k not in fallback], "fallbacks": fallback,
+            "warm_resolved_cold": redo,
             "iters": [r["iters"] for r in res], "dcd": {str(k): float(f"{d:.3e}") for k, d in dcd.items()},
             "learned_plus_batched_vs_plain": e2e / plain_cases_per_hr if plain_cases_per_hr else None}
 

@@ -31,7 +31,7 @@ class Scheme(C.Structure):  # bowshock_scheme
                 ("dt_mode", C.c_int32), ("lines", C.c_int32), ("implicit_bc", C.c_int32), ("sub_iters", C.c_uint64),
                 ("roe", C.c_int32), ("eps_fix", C.c_double), ("mg_levels", C.c_uint64), ("mg_pre", C.c_uint64),
                 ("mg_post", C.c_uint64), ("mg_gamma", C.c_uint64), ("mg_coarsest", C.c_uint64), ("cfl_star", C.c_double),
-                ("mg_cfl_star", C.c_double), ("mg_implicit", C.c_int32)]
+                ("mg_cfl_star", C.c_double), ("mg_implicit", C.c_int32), ("mg_relax", C.c_double), ("mg_cfl_scale", C.c_double)]
 
 
 class Block(C.Structure):  # bowshock_block

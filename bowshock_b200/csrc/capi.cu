@@ -210,6 +210,8 @@ int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
       sc->kind != BOWSHOCK_SCHEME_MULTIGRID)
     return fail(s, BOWSHOCK_UNSUPPORTED, "unknown scheme");
   if (!std::isfinite(sc->cfl_star) || !std::isfinite(sc->mg_cfl_star)) return fail(s, BOWSHOCK_INVALID, "cfl_star must be finite");
+  if (sc->kind == BOWSHOCK_SCHEME_MULTIGRID && (!(sc->mg_relax >= 0.0 && sc->mg_relax <= 1.0) || !(sc->mg_cfl_scale >= 0.0 && sc->mg_cfl_scale <= 1.0)))
+    return fail(s, BOWSHOCK_INVALID, "mg_relax and mg_cfl_scale must lie in [0, 1] (0: the default 1)");
   const bool implicit_params = sc->kind == BOWSHOCK_SCHEME_IMPLICIT || (sc->kind == BOWSHOCK_SCHEME_MULTIGRID && sc->mg_implicit);
   if (implicit_params && (sc->sub_iters < 1 || sc->sub_iters > 16 || !(sc->cfl0 > 0) || !(sc->cfl_max > 0)))
     return fail(s, BOWSHOCK_INVALID, "implicit parameters out of range");
@@ -232,9 +234,13 @@ int bowshock_solver_set_scheme(bowshock_solver* s, const bowshock_scheme* sc) {
   ar.mg_gamma = (int)sc->mg_gamma;
   ar.mg_coarsest = (int)sc->mg_coarsest;
   ar.mg_implicit = sc->kind == BOWSHOCK_SCHEME_MULTIGRID && sc->mg_implicit != 0;
+  ar.mg_relax = sc->kind == BOWSHOCK_SCHEME_MULTIGRID && sc->mg_relax > 0.0 ? sc->mg_relax : 1.0;
+  const double cfl_scale = sc->kind == BOWSHOCK_SCHEME_MULTIGRID && sc->mg_cfl_scale > 0.0 ? sc->mg_cfl_scale : 1.0;
   for (auto& hc : ar.cases) {
-    if (implicit_params) {  // every level smooths with the same implicit parameters (each with its own CFL ramp)
-      hc.cfl0 = sc->cfl0, hc.cfl_max = sc->cfl_max, hc.growth = sc->growth, hc.dt_mode = sc->dt_mode, hc.lines = sc->lines;
+    if (implicit_params) {  // every level smooths with the same implicit parameters (each with its own CFL ramp), the
+                            // CFL numbers of level l scaled by mg_cfl_scale^l
+      const double f = std::pow(cfl_scale, (double)hc.level);
+      hc.cfl0 = sc->cfl0 * f, hc.cfl_max = sc->cfl_max * f, hc.growth = sc->growth, hc.dt_mode = sc->dt_mode, hc.lines = sc->lines;
       hc.implicit_bc = sc->implicit_bc, hc.sub_iters = (int)sc->sub_iters, hc.roe = sc->roe, hc.eps_fix = sc->eps_fix;
     }
     hc.scheme = sc->kind;

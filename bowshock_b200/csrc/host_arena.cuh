@@ -869,6 +869,7 @@ struct ArenaHost {
   // level, its time step from that level's own CFL ramp; the implicit iteration advances the level's iteration and ramp
   // counters itself (so the fine level's counters advance once per smoothing step).
   bool mg_implicit = false;
+  double mg_relax = 1.0;  // fraction of the prolongated correction applied (1: the reference's FAS)
   void smooth(int slot, int last) {
     if (mg_implicit)
       implicit_step(slot);
@@ -889,7 +890,7 @@ struct ArenaHost {
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
     L(G_TRANSFER, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
     for (int g = 0; g < std::max(mg_gamma, 1); ++g) mg_level(l + 1, -1);
-    L(G_TRANSFER, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l); });
+    L(G_TRANSFER, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l, mg_relax); });
     set_level(l);
     for (int k = 0; k < mg_post; ++k) smooth(-1, l == 0 && k == mg_post - 1 ? 1 : 0);
     if (l == 0 && mg_post == 0 && !mg_implicit) {  // the cycle still counts one iteration

@@ -72,7 +72,8 @@ __global__ void k_restrict_forcing(Arena A, int level) {
 }
 
 // over the tiles of the fine cases of `level` (their coarse level is level + 1)
-__global__ void k_prolong(Arena A, int level) {
+// relax: the fraction of the interpolated correction applied (1: the reference's full correction)
+__global__ void k_prolong(Arena A, int level, double relax) {
   int t = blockIdx.x;
   int fi_case = A.tile_case[t];
   const CaseDev& f = A.cases[fi_case];
@@ -94,7 +95,7 @@ __global__ void k_prolong(Arena A, int level) {
     for (int k = 0; k < 4; ++k) d[k] += wt[q] * (u[k] - u0[k]);
     wsum += wt[q];
   }
-  for (int q = 0; q < 4; ++q) d[q] /= wsum;
+  for (int q = 0; q < 4; ++q) d[q] = relax * (d[q] / wsum);
   long long fc = cidx(f, i, j);
   V4<double> u = state_of(A, fc);
   double alpha = 1.0;

@@ -5,18 +5,21 @@ reference, whose only warm start is the previous Mach point's field (crates/bows
 analysis.rs:744-748: keep the state, skip the first-order start-up, measure the drop from the cold run's residual peak).
 
   data      SST cases drawn from the sweep's distribution (bowshock_b200.sweep.draw: nose shape, fineness, cylinder L/D,
-            boattail, Mach U[0.3, 3.0], ISA altitude U[0, 10] km) from SplitMix64 seed TRAIN_SEED, each meshed on the
-            normalized 128 x 64 base-wake grid (fixed section counts: 16 upstream, 28 nose, 44 body, 40 wake cells along
-            the body; 12 base-gap and 52 outer cells across) and solved by the batched arena to the reference's stop rules
-            (iterations capped); the converged state and (k, omega) as 6 channels (log rho, u / M, v / M, log(p gamma),
-            log(k / k_inf), log(omega / omega_inf)), averaged 2 x 2 to the 64 x 32 coarse level and standardized.
+            boattail, Mach U[0.3, 3.0], ISA altitude U[0, 10] km) from SplitMix64 seed TRAIN_SEED, each meshed on its own
+            grid as the sweep's cases are (96 x 48 to 320 x 160) and solved by the batched arena to the reference's stop
+            rules (iterations capped); the converged state and (k, omega) as 6 channels (log rho, u / M, v / M,
+            log(p gamma), log(k / k_inf), log(omega / omega_inf)), resampled onto the normalized 128 x 64 base-wake grid
+            (fixed section counts: 16 upstream, 28 nose, 44 body, 40 wake cells along the body; 12 base-gap and 52 outer
+            cells across), averaged 2 x 2 to the 64 x 32 coarse level and standardized. Solves that end non-finite are
+            left out.
   network   16 inputs (12 geometry parameters, Mach, log10 Re, 2 zeros) -> 6 channels at 64 x 32 (bowshock_b200.net).
   start     the prediction mapped section by section onto the case's grid (bilinear in each section's normalized index
             coordinate, so the nose, body, wake, gap and outer blocks of any cell counts line up), decoded to the
             conserved state and (k, omega, mu_t); the run then starts warm: no first-order phase, the drop measured from
             the cold run's residual peak r_ref.
   fallback  the free-stream (cold) start whenever the predicted field's first residual exceeds 10 x the cold start's
-            first residual.
+            first residual; and, as the reference keeps a warm result only when it converged or became stationary, a
+            warm run that ends otherwise is solved again cold.
 """
 from __future__ import annotations
 
@@ -52,6 +55,16 @@ def draw_sst(n, seed):
     for p in ps:
         p["viscous"] = True
     return ps
+
+
+def sweep_case(p, max_iter=None) -> Case:
+    """The SST case of parameters p on its own grid, sized as the sweep's cases are (bowshock_b200.sweep.make_case:
+    96 x 48 to 320 x 160 with the body length, the wall cell from the reference's y+ ~ 1 rule)."""
+    from .sweep import make_case
+    c = make_case(dict(p, viscous=True))
+    if max_iter is not None:
+        c.numerics = replace(c.numerics, max_iter=int(max_iter))
+    return c
 
 
 def normalized_case(p, max_iter=None) -> Case:
@@ -225,10 +238,17 @@ class WarmStart:
         return out
 
 
-def warm_solve(arena, model: WarmStart, r_ref, cold_first):
+ACCEPTED = ("residual drop", "CD stationary", "mean stationary", "base pressure stationary")
+
+
+def warm_solve(arena, model: WarmStart, r_ref, cold_first, device=0):
     """Warm-start every case of `arena` (all SST) from the model and solve to the stop rules. r_ref[k]: the drop reference
-    (a cold run's residual peak); cold_first[k]: the cold start's first residual (the fallback threshold's base). Returns
-    (results, fallback flags, first residuals of the predicted fields)."""
+    (a cold run's residual peak); cold_first[k]: the cold start's first residual (the fallback threshold's base). As the
+    reference's sweep keeps a warm result only when it converged or became stationary and solves the point cold
+    otherwise (analysis.rs:744-771), a warm run that ends non-finite or at the iteration cap is solved again from the
+    free stream (in a second arena of those cases). Returns (results, fallback flags, first residuals of the predicted
+    fields, indices re-solved cold, device seconds of the re-solve)."""
+    from .arena import Arena
     fields = model.start_fields(arena.cases)
     for k, (u, t, mt) in enumerate(fields):
         arena.set_state(k, u)
@@ -240,7 +260,17 @@ def warm_solve(arena, model: WarmStart, r_ref, cold_first):
             arena.set_run(k, c.numerics, warm=False)
         else:
             arena.set_run(k, c.numerics, warm=True, r_ref=float(r_ref[k]))
-    return arena.solve(), fallback, first
+    res = arena.solve()
+    redo = [k for k in range(arena.ncases) if not fallback[k] and res[k]["stop_reason"] not in ACCEPTED]
+    redo_s = 0.0
+    if redo:
+        b = Arena([arena.cases[k] for k in redo], device=device)
+        rr = b.solve()
+        redo_s = b.last_solve_ms() / 1000.0
+        for q, k in enumerate(redo):
+            res[k] = rr[q]
+        del b
+    return res, fallback, first, redo, redo_s
 
 
 def iters_to_drop(hist, r_ref, orders):
@@ -254,14 +284,15 @@ def _cd(r):
 
 
 # ---------------------------------------------------------------------------------------------------- pipeline
-def generate(n, seed, max_iter, batch=500, device=0, log=print):
-    """Solve n SST cases on the normalized grid with the batched arena: (features [n, 16], coarse targets [n, 32, 64, 6],
-    per-case results)."""
+def generate(n, seed, max_iter, batch=250, device=0, log=print):
+    """Solve n SST cases of the sweep's distribution on their own grids with the batched arena and resample each
+    converged field onto the normalized grid's coarse level: (features [n', 16], coarse targets [n', 32, 64, 6], per-case
+    results); the cases whose solve ended non-finite are left out (n' <= n)."""
     from .arena import Arena
     ps = draw_sst(n, seed)
     X, T, R = [], [], []
     for b0 in range(0, n, batch):
-        cs = [normalized_case(p, max_iter) for p in ps[b0:b0 + batch]]
+        cs = [sweep_case(p, max_iter) for p in ps[b0:b0 + batch]]
         t0 = time.perf_counter()
         a = Arena(cs, device=device)
         res = a.solve()
@@ -318,58 +349,61 @@ def init_params(seed, net_layout, n):
 
 
 def evaluate(model: WarmStart, n, seed, max_iter, device=0, log=print):
-    """Held-out evaluation: each case solved cold and then warm (from the model, with the fallback rule) in one arena,
-    both to the reference's stop rules (iterations capped at max_iter); the warm run's drop measured from the cold run's
-    residual peak. Returns a report dict and the held-out coarse targets' loss."""
+    """Held-out evaluation on n SST cases of the sweep's distribution (their own grids): each solved cold and then warm
+    (from the model, with the fallback rule and the cold re-run of a warm run that does not converge) in one arena, both
+    to the reference's stop rules (iterations capped at max_iter); the warm run's drop measured from the cold run's
+    residual peak, as the reference's warm runs measure theirs (analysis.rs:744-748). Cases whose cold run ends
+    non-finite have no reference to compare with and are counted apart."""
     from .arena import Arena
     ps = draw_sst(n, seed)
-    cs = [normalized_case(p, max_iter) for p in ps]
+    cs = [sweep_case(p, max_iter) for p in ps]
     a = Arena(cs, device=device)
     t0 = time.perf_counter()
     cold = a.solve()
     cold_s = a.last_solve_ms() / 1000.0
     hist_c = [a.residual_history(k) for k in range(n)]
-    X = np.stack([features(c) for c in cs])
-    T = []
-    for k, c in enumerate(cs):
+    ok = [k for k in range(n) if cold[k]["stop_reason"] != "non-finite residual"]
+    T = {}
+    for k in ok:
         t, _ = a.turb_state(k)
-        T.append(target_of(c, a.state(k), t))
-    T = np.stack(T)
+        T[k] = target_of(cs[k], a.state(k), t)
     r_ref = [r["residual_peak"] for r in cold]
-    warm, fallback, first = warm_solve(a, model, r_ref, [h[0] for h in hist_c])
-    warm_s = a.last_solve_ms() / 1000.0
+    warm, fallback, first, redo, redo_s = warm_solve(a, model, r_ref, [h[0] for h in hist_c], device=device)
+    warm_s = a.last_solve_ms() / 1000.0 + redo_s
     hist_w = [a.residual_history(k) for k in range(n)]
-    log(f"held-out: cold {cold_s:.1f} s, warm {warm_s:.1f} s of device time ({time.perf_counter() - t0:.1f} s wall)")
+    warm_iters = [warm[k]["iters"] + (len(hist_w[k]) if k in redo else 0) for k in range(n)]  # a re-run pays for both runs
+    log(f"held-out: cold {cold_s:.1f} s, warm {warm_s:.1f} s of device time ({time.perf_counter() - t0:.1f} s wall), "
+        f"{len(ok)} of {n} cold runs finite, {len(redo)} warm runs re-solved cold")
     mask = coarse_mask().astype(bool)
-    pred = model.predict(cs)
-    held_loss = float(np.mean((((pred - T) / model.std) ** 2)[:, mask]))
-    rep = {"cases": n, "seed": hex(seed), "max_iter": max_iter, "fallbacks": int(sum(fallback)),
-           "cold_device_s": cold_s, "warm_device_s": warm_s, "held_out_loss_standardized": held_loss,
-           "first_residual_ratio_median": float(np.median([first[k] / hist_c[k][0] for k in range(n)])),
+    pred = model.predict([cs[k] for k in ok])
+    held_loss = float(np.mean((((pred - np.stack([T[k] for k in ok])) / model.std) ** 2)[:, mask])) if ok else None
+    rep = {"cases": n, "seed": hex(seed), "max_iter": max_iter, "cold_finite": len(ok), "fallbacks": int(sum(fallback)),
+           "warm_resolved_cold": len(redo), "cold_device_s": cold_s, "warm_device_s": warm_s, "held_out_loss_standardized": held_loss,
+           "first_residual_ratio_median": float(np.median([first[k] / hist_c[k][0] for k in ok])) if ok else None,
            "stop_cold": {}, "stop_warm": {}, "drop": {}}
-    for r in cold:
-        rep["stop_cold"][r["stop_reason"]] = rep["stop_cold"].get(r["stop_reason"], 0) + 1
-    for r in warm:
-        rep["stop_warm"][r["stop_reason"]] = rep["stop_warm"].get(r["stop_reason"], 0) + 1
+    for k in ok:
+        rep["stop_cold"][cold[k]["stop_reason"]] = rep["stop_cold"].get(cold[k]["stop_reason"], 0) + 1
+        rep["stop_warm"][warm[k]["stop_reason"]] = rep["stop_warm"].get(warm[k]["stop_reason"], 0) + 1
+    direct = [k for k in ok if k not in redo and not fallback[k]]
     for orders in (1, 2, 3, 4, 5):
-        ic = [iters_to_drop(hist_c[k], r_ref[k], orders) for k in range(n)]
-        iw = [iters_to_drop(hist_w[k], r_ref[k], orders) if not fallback[k] else ic[k] for k in range(n)]
-        both = [k for k in range(n) if ic[k] is not None and iw[k] is not None]
-        rep["drop"][str(orders)] = {"reached_cold": sum(v is not None for v in ic), "reached_warm": sum(v is not None for v in iw),
+        ic = {k: iters_to_drop(hist_c[k], r_ref[k], orders) for k in direct}
+        iw = {k: iters_to_drop(hist_w[k], r_ref[k], orders) for k in direct}
+        both = [k for k in direct if ic[k] is not None and iw[k] is not None]
+        rep["drop"][str(orders)] = {"reached_cold": sum(v is not None for v in ic.values()), "reached_warm": sum(v is not None for v in iw.values()),
                                     "median_iters_cold": float(np.median([ic[k] for k in both])) if both else None,
                                     "median_iters_warm": float(np.median([iw[k] for k in both])) if both else None,
                                     "mean_ratio_warm_over_cold": float(np.mean([iw[k] / ic[k] for k in both])) if both else None}
-    conv = [k for k in range(n) if cold[k]["stop_reason"] in ("residual drop", "CD stationary", "mean stationary")
-            and warm[k]["stop_reason"] in ("residual drop", "CD stationary", "mean stationary")]
+    conv = [k for k in ok if cold[k]["stop_reason"] in ACCEPTED and warm[k]["stop_reason"] in ACCEPTED]
     dcd = [abs(_cd(warm[k]) - _cd(cold[k])) for k in conv]
     rep["converged_both"] = len(conv)
     rep["dcd_max"] = float(max(dcd)) if dcd else None
     rep["dcd_median"] = float(np.median(dcd)) if dcd else None
     rep["within_1e-4"] = int(sum(d <= 1e-4 for d in dcd))
-    rep["iters_cold_total"] = int(sum(r["iters"] for r in cold))
-    rep["iters_warm_total"] = int(sum(r["iters"] for r in warm))
+    rep["iters_cold_total"] = int(sum(cold[k]["iters"] for k in ok))
+    rep["iters_warm_total"] = int(sum(warm_iters[k] for k in ok))
     rep["per_case"] = [{"mach": ps[k]["mach"], "cold": [cold[k]["iters"], cold[k]["stop_reason"], _cd(cold[k])],
-                        "warm": [warm[k]["iters"], warm[k]["stop_reason"], _cd(warm[k])], "fallback": fallback[k]} for k in range(n)]
+                        "warm": [warm_iters[k], warm[k]["stop_reason"], _cd(warm[k])], "fallback": fallback[k],
+                        "resolved_cold": k in redo} for k in range(n)]
     return rep
 
 
@@ -378,7 +412,7 @@ def main():
     ap = argparse.ArgumentParser(description="train the warm-start network on solver-generated SST solutions and evaluate it")
     ap.add_argument("--train-cases", type=int, default=2000)
     ap.add_argument("--eval-cases", type=int, default=200)
-    ap.add_argument("--max-iter", type=int, default=6000, help="iteration cap of the training solves")
+    ap.add_argument("--max-iter", type=int, default=4000, help="iteration cap of the training solves")
     ap.add_argument("--eval-max-iter", type=int, default=8000)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=64)

@@ -75,6 +75,8 @@ class MgParams:  # solver.rs:123-140 (DEFAULT): FAS multigrid with the SSP-RK3 s
     coarsest: int = 4
     cfl_star: float = 0.0  # implicit residual smoothing of the smoother (MgParams::irs)
     implicit: "ImplicitParams | None" = None  # the line-implicit smoother (no counterpart in the reference) with these parameters
+    relax: float = 1.0  # fraction of the prolongated correction applied
+    cfl_scale: float = 1.0  # the implicit smoother's CFL numbers on level l times cfl_scale^l
 
 
 @dataclass
@@ -162,7 +164,7 @@ class GpuSolver:
             s = _ffi.Scheme(kind=SCHEME_SMOOTHED, cfl_star=scheme.cfl_star)
         elif isinstance(scheme, MgParams):
             s = _ffi.Scheme(kind=SCHEME_MULTIGRID, mg_levels=scheme.levels, mg_pre=scheme.pre, mg_post=scheme.post, mg_gamma=scheme.gamma,
-                            mg_coarsest=scheme.coarsest, mg_cfl_star=scheme.cfl_star)
+                            mg_coarsest=scheme.coarsest, mg_cfl_star=scheme.cfl_star, mg_relax=scheme.relax, mg_cfl_scale=scheme.cfl_scale)
             if scheme.implicit is not None:
                 p = scheme.implicit
                 s.mg_implicit = 1

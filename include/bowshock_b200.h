@@ -83,6 +83,9 @@ typedef struct {
    * multigrid.rs:87-112): each smoothing step one implicit iteration with the parameters above (cfl0 .. eps_fix) of the
    * active level, from that level's own CFL ramp; the same FAS transfers */
   int32_t mg_implicit;
+  /* multigrid options (0 = the default 1): the fraction of the prolongated correction applied, and the factor of the
+   * implicit smoother's CFL numbers per level (level l runs cfl0 and cfl_max times mg_cfl_scale^l) */
+  double mg_relax, mg_cfl_scale;
 } bowshock_scheme;
 
 /* solver.rs:59-102 `Block` */
