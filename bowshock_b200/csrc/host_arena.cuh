@@ -923,9 +923,10 @@ struct ArenaHost {
     prof_ms[g] += ms;
     prof_launches[g] += 1;
   }
-  // residual kernel of the implicit iteration: 0 = 256 threads, 1 = 288 threads (3 blocks per SM both; they round
-  // differently, so the autotuner keeps 0 and 1 is only used when pinned)
-  int res_variant = 0;
+  // residual kernel of the implicit iteration: 0 = 256 threads, 1 = 288 threads (3 blocks per SM both; at most two
+  // face fluxes per thread with 288). The two round differently, so the variant is fixed (288) and only a pinned
+  // tuning changes it.
+  int res_variant = 1;
   void launch_residual(int dt_kind, int slot) {
     if (res_variant == 1)
       k_residual<288, 3><<<LT(), 288, 0, stream>>>(A, dt_kind, slot);
@@ -1080,7 +1081,7 @@ struct ArenaHost {
     lw_subst[0] = pick_w[2], lw_subst[1] = pick_w[3], lw_turb = pick_w[4];
     pf_subst[0] = pick_pf[2], pf_subst[1] = pick_pf[3];
     // the residual kernel's variant is not a candidate: with its tile staged by TMA, the 288-thread build rounds
-    // differently from the 256-thread one (ptxas fuses multiply-adds by register budget), so it stays at 0 unless pinned
+    // differently from the 256-thread one (ptxas fuses multiply-adds by register budget), so it stays at 1 unless pinned
     staged_lines = staged_keep;
     for (auto& q : keep) BK_CUDA(cudaMemcpyAsync(const_cast<void*>(q.src), q.dst, q.bytes, cudaMemcpyDeviceToDevice, stream));
     BK_CUDA(cudaStreamSynchronize(stream));

@@ -344,12 +344,12 @@ int bowshock_solver_set_run_control(bowshock_solver* s, int on_device);
 /* the same profile of a single-case solver (any scheme, multigrid levels included) */
 int bowshock_solver_profile(bowshock_solver* s, uint64_t n, double* ms, uint64_t* launches);
 /* Launch shapes of the arena's kernels. At creation (arenas of 100,000 cells or more; otherwise 4 lines per block, no
- * prefetching, variant 0) the autotuner picks, each the fastest in one timed iteration of the arena's own cases per
+ * prefetching) the autotuner picks, each the fastest in one timed iteration of the arena's own cases per
  * candidate (the state restored afterwards): per direction, lines per block (1, 2 or 4) of the block line solves' first
  * pass and how its walks fetch the cells' records (0: one cell at a time, 1: the next cell's ahead; 2, staged through
  * shared memory three cells ahead with one line per block, only when pinned), lines per block (1, 2, 4 or 8) of their
  * substitution passes and how those walks fetch their records (0 / 1 / 2 likewise), lines per block of the SST line
- * kernel; the residual kernel's variant (0: 256 threads per 32 x 8 tile, 1: 288) stays 0 unless pinned (the two round
+ * kernel; the residual kernel's variant (0: 256 threads per 32 x 8 tile, 1: 288) stays 1 unless pinned (the two round
  * differently). A direction with at most
  * staged_lines lines left in the launch (set at creation to two waves of the staged substitution kernel: 1,184 lines on
  * a 148-SM B200; >= 0, 0 never) runs both passes staged whatever prefetch / subst_prefetch say: with few lines the

@@ -104,7 +104,7 @@ def test_autotuner_candidates_give_bit_identical_states():
     from bowshock_b200.sweep import sweep_cases
     sel = [sweep_cases()[k] for k in (0, 9)]  # an Euler sting case and an SST limit-cycle case
     base = dict(lines_i=4, lines_j=4, prefetch_i=0, prefetch_j=0, subst_i=4, subst_j=4, turb_lines=4, segment_i=2, segment_j=2,
-                residual=0, subst_prefetch_i=0, subst_prefetch_j=0, staged_lines=0)
+                residual=1, subst_prefetch_i=0, subst_prefetch_j=0, staged_lines=0)
     variants = [dict(lines_i=1, lines_j=2, prefetch_i=1, prefetch_j=1), dict(subst_i=1, subst_j=8),
                 dict(subst_prefetch_i=1, subst_prefetch_j=1), dict(subst_i=1, subst_j=8, subst_prefetch_i=1, subst_prefetch_j=1),
                 dict(subst_prefetch_i=2, subst_prefetch_j=2), dict(subst_prefetch_i=2), dict(prefetch_i=2, prefetch_j=2),
