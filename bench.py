@@ -145,6 +145,16 @@ def d2h_bytes(ncases, iters):
     return int(chunks * (50 * ncases * 8 + ncases * 8 + ncases * 15 * 8))
 
 
+def census_fixture_implicit():
+    """The oracle's census of the sweep's Euler cases at M >= 0.85 with the B200 path's line-implicit scheme and stop rules
+    (tests/golden/sweep_census_implicit.json): {case index: {...}}."""
+    p = os.path.join(ROOT, "tests", "golden", "sweep_census_implicit.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return {int(k): v for k, v in json.load(f)["cases"].items()}
+    return {}
+
+
 def census_fixture():
     """The oracle's census of the sweep: {case index: {iters, cd_total, ...}} (cases it has not finished are absent)."""
     p = os.path.join(ROOT, "tests", "golden", "sweep_census.json")
@@ -274,6 +284,8 @@ def run_ours(args, rank, world, dist):
     iters_local = np.array([r["iters"] for r in results_local], dtype=float)
     fx = census_fixture()
     dcd = {k: cd_error(results[k], fx[k]) for k in range(len(all_cases)) if k in fx}
+    fxi = census_fixture_implicit()
+    dcd_same = {k: results[k]["cd_total"] - fxi[k]["cd_total"] for k in range(len(all_cases)) if k in fxi}
     ok = [k for k, d in dcd.items() if abs(d) <= 1e-4]
     n_ok = len(ok)
     steady_local = 3600.0 * len(cases) * cells.sum() / ((ms_local / 1000.0) * float(np.sum(cells * iters_local)))
@@ -320,7 +332,7 @@ def run_ours(args, rank, world, dist):
     traffic = line_sweep_traffic()
     learned = secondary(learned_census, all_cases, all_grids, fx, plain_cases_per_hr, device) if world == 1 else None
     lift3 = secondary(measure_lift3, args, device) if world == 1 else None
-    mg0 = secondary(measure_config0_multigrid, device) if world == 1 else None
+    mg0 = secondary(measure_multigrid, device) if world == 1 else None
     cpu_base = None
     if world == 1:  # the CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
         smp = OracleSample(all_cases)
@@ -352,6 +364,7 @@ def run_ours(args, rank, world, dist):
             "l2": "no flush: the step's working set (~%.0f MB) is larger than the 126 MB L2" % (ncell * 600 / 1e6),
             "converged_within_1e-4": n_ok, "checked_against_oracle": len(dcd),
             "dcd": {str(k): float(f"{d:.3e}") for k, d in dcd.items()},
+            "dcd_euler_transonic_same_scheme": {str(k): float(f"{d:.3e}") for k, d in dcd_same.items()},
             "census_device_s": census_dev_max, "census_wall_s": wall_max, "census_iters": iters, "census_stop_reasons": stops,
             "steady_state_cases_per_hr": steady_all,
             "plain_single_case_cases_per_hr": plain_cases_per_hr, "plain_wall_s": plain_max, "plain_converged_within_1e-4": int(plain_ok_all),
@@ -361,7 +374,7 @@ def run_ours(args, rank, world, dist):
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "autotuned_lines_per_block": tuning,
             "lift3": lift3,
-            "config0_multigrid": mg0,
+            "multigrid": mg0,
             "parallelism": (f"cases partitioned over {world} GPUs (longest-processing-time on cells x expected iterations), results "
                             "gathered" if world > 1 else "one GPU, one batched arena"),
         },
@@ -473,36 +486,46 @@ def measure_lift3(args, device):
 TRANSFER_WORDS = 4 * 9 + 8 + 8 + 4 * 8
 
 
-def measure_config0_multigrid(device):
-    """Config 0 (Euler, 128 x 64, M 1.5) to the reference's stop rules, single-grid line-implicit and 3-level FAS with the
-    line-implicit smoother, wall clock of each GpuSolver.run_to_stop, CD against the FP64 oracle's converged run; and the
-    transfer kernels' model bytes over their CUDA-event time (a grid this small stays in the L2 cache)."""
+def measure_multigrid(device):
+    """Single-grid line-implicit against 3-level FAS with the line-implicit smoother, each to the reference's stop rules
+    (wall clock of GpuSolver.run_to_stop): a sting-mounted ogive + cylinder at M 2.0 (attached flow, the coarse-grid
+    correction under-relaxed by 0.5, coarse CFL halved per level) and config 0 (Euler, 128 x 64, M 1.5, separated base
+    flow, correction under-relaxed by 0.5; CD against the FP64 oracle's converged run); and the transfer kernels' model
+    bytes over their CUDA-event time (grids this small stay in the L2 cache)."""
     import bowshock_b200 as bk
+    from bowshock_b200.case import Body, Case, NOSE_TANGENT_OGIVE, WAKE_STING
     from bowshock_b200.configs import config0_case
     with open(os.path.join(ROOT, "tests", "golden", "configs_oracle.json")) as f:
         ref = json.load(f)["config0"]
-    out = {"workload": "config 0: Euler, tangent ogive + cylinder, base wake, M 1.5, 128 x 64 (FAS levels 64 x 32, 32 x 16)"}
-    for name, levels in (("single_grid", 1), ("multigrid3", 3)):
-        c = config0_case()
-        s = c.build_solver(device)
-        if levels > 1:
-            s.set_scheme(bk.solver.MgParams(levels=levels, pre=1, post=1, implicit=c.numerics.scheme))
-        t0 = time.perf_counter()
-        r = s.run_to_stop(c.body, c.numerics, c.wake)
-        wall = time.perf_counter() - t0
-        out[name] = {"iters": r["iters"], "stop": r["stop_reason"], "wall_s": wall, "dcd_total": r["cd_total"] - ref["cd_total"],
-                     "dcd_base": r["cd_base"] - ref["cd_base"]}
-        if levels > 1:
-            prof = s.profile(10)
-            ms, n = prof["transfer"]
-            coarse = (64 * 32 + 32 * 16)  # coarse cells of one cycle's transfers (pre = post = 1, gamma = 1)
-            if ms > 0:
-                gbs = coarse * TRANSFER_WORDS * 4 * 10 / (ms / 1000.0) / 1e9
-                out[name]["transfer_ms_per_cycle"] = ms / 10
-                out[name]["transfer_launches_per_cycle"] = n / 10
-                out[name]["transfer_model_gbs"] = gbs
-                out[name]["transfer_hbm_frac"] = gbs / peaks()[0]
-        del s
+    body = Body(NOSE_TANGENT_OGIVE, fineness=3.0, segments=((6.0, 0.0),))
+    work = {"sting_m2": ("sting-mounted tangent ogive + cylinder, Euler, M 2.0, level 0", lambda: Case.new(2.0, body, 0, WAKE_STING), 0.5, 0.5),
+            "config0": ("config 0: Euler, tangent ogive + cylinder, base wake, M 1.5, 128 x 64", config0_case, 0.5, 1.0)}
+    out = {}
+    for key, (label, make, relax, scale) in work.items():
+        o = out[key] = {"workload": label, "relax": relax, "cfl_scale": scale}
+        for name, levels in (("single_grid", 1), ("multigrid3", 3)):
+            c = make()
+            s = c.build_solver(device)
+            if levels > 1:
+                s.set_scheme(bk.solver.MgParams(levels=levels, pre=1, post=1, implicit=c.numerics.scheme, relax=relax, cfl_scale=scale))
+            t0 = time.perf_counter()
+            r = s.run_to_stop(c.body, c.numerics, c.wake)
+            wall = time.perf_counter() - t0
+            o[name] = {"iters": r["iters"], "stop": r["stop_reason"], "wall_s": wall, "cd_total": r["cd_total"]}
+            if key == "config0":
+                o[name]["dcd_total_vs_oracle"] = r["cd_total"] - ref["cd_total"]
+            if levels > 1 and key == "config0":
+                prof = s.profile(10)
+                ms, n = prof["transfer"]
+                coarse = (64 * 32 + 32 * 16)  # coarse cells of one cycle's transfers (pre = post = 1, gamma = 1)
+                if ms > 0:
+                    gbs = coarse * TRANSFER_WORDS * 4 * 10 / (ms / 1000.0) / 1e9
+                    o[name]["transfer_ms_per_cycle"] = ms / 10
+                    o[name]["transfer_launches_per_cycle"] = n / 10
+                    o[name]["transfer_model_gbs"] = gbs
+                    o[name]["transfer_hbm_frac"] = gbs / peaks()[0]
+            del s
+        o["dcd_multigrid_vs_single"] = o["multigrid3"]["cd_total"] - o["single_grid"]["cd_total"]
     return out
 
 

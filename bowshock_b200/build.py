@@ -10,7 +10,7 @@ ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libbowshock_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "capi.cu"), os.path.join(HERE, "csrc", "net.cu")]
-HEADERS = ["arena.cuh", "tma.cuh", "device_math.cuh", "viscous.cuh", "turbulence.cuh", "host_arena.cuh", "fv_kernels.cu", "forces.cuh", "mesher.cuh", "runner.cuh", "euler3.cuh", "host3.cuh"]
+HEADERS = ["arena.cuh", "tma.cuh", "stream_copy.cuh", "device_math.cuh", "viscous.cuh", "turbulence.cuh", "host_arena.cuh", "fv_kernels.cu", "forces.cuh", "mesher.cuh", "runner.cuh", "euler3.cuh", "host3.cuh"]
 
 
 def nvcc():

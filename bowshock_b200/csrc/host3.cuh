@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "euler3.cuh"
+#include "stream_copy.cuh"
 
 namespace bk3 {
 
@@ -242,26 +243,26 @@ struct Batch3 {
         double r = std::hypot(p[5], p[6]);  // face_rot (flux3.rs:11-19)
         h2[q] = r < 1e-300 ? make_float2(0.f, 1.f) : make_float2((float)(p[5] / r), (float)(p[6] / r));
       }
-      BK3_CUDA(cudaMemcpy(d4, h4.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-      BK3_CUDA(cudaMemcpy(d2, h2.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+      BK3_CUDA(copy_sync(stream, d4, h4.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+      BK3_CUDA(copy_sync(stream, d2, h2.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
       return 0;
     };
     if ((rc = up_faces(g.fi, B.nfi, fi, ri)) || (rc = up_faces(g.fj, B.nfj, fj, rj)) || (rc = up_faces(g.fk, B.nfk, fk, rk))) return rc;
     std::vector<float> hv(B.nc);
     for (long long c = 0; c < B.nc; ++c) hv[c] = (float)g.vol[c];
-    BK3_CUDA(cudaMemcpy(vol, hv.data(), B.nc * sizeof(float), cudaMemcpyHostToDevice));
-    BK3_CUDA(cudaMemcpy(ak, axis_k.data(), axis_k.size() * sizeof(int), cudaMemcpyHostToDevice));
-    BK3_CUDA(cudaMemcpy(d_wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, vol, hv.data(), B.nc * sizeof(float), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, ak, axis_k.data(), axis_k.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, d_wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice));
     B.fi = fi, B.fj = fj, B.fk = fk, B.ri = ri, B.rj = rj, B.rk = rk, B.vol = vol, B.axis_k = ak, B.cs = dcs;
     if ((rc = upload_cases())) return rc;
     h_active.assign(nb, 1);
-    BK3_CUDA(cudaMemcpy(B.active, h_active.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, B.active, h_active.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
     return reset();
   }
   int upload_cases() {
     std::vector<Case3Dev> h(cases.size());
     for (size_t k = 0; k < cases.size(); ++k) to_dev(cases[k], h[k]);
-    BK3_CUDA(cudaMemcpy(const_cast<Case3Dev*>(B.cs), h.data(), h.size() * sizeof(Case3Dev), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, const_cast<Case3Dev*>(B.cs), h.data(), h.size() * sizeof(Case3Dev), cudaMemcpyHostToDevice));
     return 0;
   }
   // every case to its free stream, iteration and ramp counters to zero
@@ -274,33 +275,33 @@ struct Batch3 {
       std::vector<float> h(B.nc);
       for (int v = 0; v < 5; ++v) {
         std::fill(h.begin(), h.end(), (float)q[v]);
-        BK3_CUDA(cudaMemcpy(B.U + ((size_t)b * 5 + v) * B.nc, h.data(), B.nc * sizeof(float), cudaMemcpyHostToDevice));
+        BK3_CUDA(copy_sync(stream, B.U + ((size_t)b * 5 + v) * B.nc, h.data(), B.nc * sizeof(float), cudaMemcpyHostToDevice));
       }
     }
     std::vector<int> z(B.nb, 0);
-    BK3_CUDA(cudaMemcpy(B.iter, z.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
-    BK3_CUDA(cudaMemcpy(B.ramp, z.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, B.iter, z.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, B.ramp, z.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
     return 0;
   }
   int set_state(int b, const double* u) {  // u: ncell x 5 (Cons3 layout)
     std::vector<float> h(5 * B.nc);
     for (long long c = 0; c < B.nc; ++c)
       for (int v = 0; v < 5; ++v) h[v * B.nc + c] = (float)u[5 * c + v];
-    BK3_CUDA(cudaMemcpy(B.U + (size_t)b * 5 * B.nc, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, B.U + (size_t)b * 5 * B.nc, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
     return 0;
   }
   int get_state(int b, double* u) {
     std::vector<float> h(5 * B.nc);
     BK3_CUDA(cudaStreamSynchronize(stream));
-    BK3_CUDA(cudaMemcpy(h.data(), B.U + (size_t)b * 5 * B.nc, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    BK3_CUDA(copy_sync(stream, h.data(), B.U + (size_t)b * 5 * B.nc, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
     for (long long c = 0; c < B.nc; ++c)
       for (int v = 0; v < 5; ++v) u[5 * c + v] = h[v * B.nc + c];
     return 0;
   }
   int set_counters(int it, int ramp) {
     std::vector<int> a(B.nb, it), r(B.nb, ramp);
-    BK3_CUDA(cudaMemcpy(B.iter, a.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
-    BK3_CUDA(cudaMemcpy(B.ramp, r.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, B.iter, a.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
+    BK3_CUDA(copy_sync(stream, B.ramp, r.data(), B.nb * sizeof(int), cudaMemcpyHostToDevice));
     return 0;
   }
   int set_active(const std::vector<int>& act) {
@@ -396,8 +397,8 @@ struct Batch3 {
   }
   int read_residual(int b, double* res, double* dt) {
     std::vector<float> h(5 * B.nc), hd(B.nc);
-    BK3_CUDA(cudaMemcpy(h.data(), B.R + (size_t)b * 5 * B.nc, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
-    BK3_CUDA(cudaMemcpy(hd.data(), B.dt + (size_t)b * B.nc, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    BK3_CUDA(copy_sync(stream, h.data(), B.R + (size_t)b * 5 * B.nc, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    BK3_CUDA(copy_sync(stream, hd.data(), B.dt + (size_t)b * B.nc, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
     for (long long c = 0; c < B.nc; ++c) {
       if (res)
         for (int v = 0; v < 5; ++v) res[5 * c + v] = h[v * B.nc + c];

@@ -15,6 +15,7 @@
 
 #include "arena.cuh"
 #include "tma.cuh"
+#include "stream_copy.cuh"
 
 namespace bk {
 
@@ -447,7 +448,7 @@ struct ArenaHost {
     CUtensorMap* d = nullptr;
     BK_CUDA(cudaMalloc(&d, maps.size() * sizeof(CUtensorMap)));
     A.wmaps = d;
-    BK_CUDA(cudaMemcpy(d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
     return 0;
   }
 
@@ -520,7 +521,7 @@ struct ArenaHost {
     ALLOC(A.Ulo, ncell);
     ALLOC(A.Wlo, npad);
     ALLOC(A.U0lo, ncell);
-    BK_CUDA(cudaMemset(A.Ulo, 0, ncell * sizeof(float4)));
+    BK_CUDA(cudaMemsetAsync(A.Ulo, 0, ncell * sizeof(float4), stream));
     if ((rc = build_wmaps())) return rc;
     ALLOC(A.dt, ncell);
     ALLOC(A.irs_eps, ncell);
@@ -547,17 +548,17 @@ struct ArenaHost {
       ALLOC(A.MG0, ncell);
       ALLOC(A.MG0lo, ncell);
       ALLOC(A.FORCE, ncell);
-      BK_CUDA(cudaMemset(A.FORCE, 0, ncell * sizeof(float4)));
+      BK_CUDA(cudaMemsetAsync(A.FORCE, 0, ncell * sizeof(float4), stream));
     }
     float4 *fis, *fjs;
     ALLOC(fis, nif);
     ALLOC(fjs, njf);
     A.ifs = fis;
     A.jfs = fjs;
-    BK_CUDA(cudaMemcpy(d_tile_case, tile_case.data(), tile_case.size() * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_iline, iline.data(), iline.size() * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_jline, jline.data(), jline.size() * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_pblk, pblk.data(), pblk.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_tile_case, tile_case.data(), tile_case.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_iline, iline.data(), iline.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_jline, jline.data(), jline.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_pblk, pblk.data(), pblk.size() * sizeof(int), cudaMemcpyHostToDevice));
     // geometry
     std::vector<float4> hfi(nif), hfj(njf), hcg(ncell);
     std::vector<float2> hic(nif), hjc(njf);
@@ -584,11 +585,11 @@ struct ArenaHost {
           hcg[c.cell_off + cc] = make_float4((float)h.vol[cc], (float)h.area[cc], (float)h.xc[cc], (float)h.rc[cc]);
         }
     }
-    BK_CUDA(cudaMemcpy(fi, hfi.data(), nif * sizeof(float4), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(fj, hfj.data(), njf * sizeof(float4), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(cg, hcg.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(ic, hic.data(), nif * sizeof(float2), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(jc, hjc.data(), njf * sizeof(float2), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, fi, hfi.data(), nif * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, fj, hfj.data(), njf * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, cg, hcg.data(), ncell * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, ic, hic.data(), nif * sizeof(float2), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, jc, hjc.data(), njf * sizeof(float2), cudaMemcpyHostToDevice));
     A.ncases = nc;
     A.cases = d_cases;
     A.iter = d_iter;
@@ -605,10 +606,10 @@ struct ArenaHost {
     A.npblk = npblk;
     std::vector<int> zero(nc, 0);
     h_active.assign(nc, 1);
-    BK_CUDA(cudaMemcpy(d_iter, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_ramp, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_active, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_enabled, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_iter, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_ramp, zero.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_active, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_enabled, h_active.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
     ready = true;
     if ((rc = upload_desc())) return rc;
     for (int k = 0; k < nc; ++k)
@@ -649,13 +650,13 @@ struct ArenaHost {
       ALLOC(A.mu_t, ncell);
       ALLOC(A.fvi, nif);
       ALLOC(A.fvj, njf);
-      BK_CUDA(cudaMemset(A.mu_t, 0, ncell * sizeof(float)));
-      BK_CUDA(cudaMemset(A.fvi, 0, nif * sizeof(float4)));
-      BK_CUDA(cudaMemset(A.fvj, 0, njf * sizeof(float4)));
+      BK_CUDA(cudaMemsetAsync(A.mu_t, 0, ncell * sizeof(float), stream));
+      BK_CUDA(cudaMemsetAsync(A.fvi, 0, nif * sizeof(float4), stream));
+      BK_CUDA(cudaMemsetAsync(A.fvj, 0, njf * sizeof(float4), stream));
     }
     if (any_rough && !A.rough) {
       ALLOC(A.rough, ncell);
-      BK_CUDA(cudaMemset(A.rough, 0, ncell * sizeof(float4)));
+      BK_CUDA(cudaMemsetAsync(A.rough, 0, ncell * sizeof(float4), stream));
     }
     if (any_sst && !A.turb) {
       ALLOC(A.turb, ncell);
@@ -666,11 +667,11 @@ struct ArenaHost {
       ALLOC(A.trhs, ncell);
       ALLOC(A.grad_kw, ncell);
       ALLOC(A.blend, ncell);
-      BK_CUDA(cudaMemset(A.mflux_i, 0, nif * sizeof(float)));
-      BK_CUDA(cudaMemset(A.mflux_j, 0, njf * sizeof(float)));
+      BK_CUDA(cudaMemsetAsync(A.mflux_i, 0, nif * sizeof(float), stream));
+      BK_CUDA(cudaMemsetAsync(A.mflux_j, 0, njf * sizeof(float), stream));
     }
     if ((rc = upload_stencils())) return rc;
-    BK_CUDA(cudaMemcpy(d_cases, desc.data(), desc.size() * sizeof(CaseDev), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_cases, desc.data(), desc.size() * sizeof(CaseDev), cudaMemcpyHostToDevice));
     if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
     return 0;
   }
@@ -680,8 +681,8 @@ struct ArenaHost {
     std::vector<float4> fis, fjs;
     for (size_t k = 0; k < cases.size(); ++k) {
       face_stencils(cases[k], fis, fjs);
-      BK_CUDA(cudaMemcpy((void*)(A.ifs + desc[k].if_off), fis.data(), fis.size() * sizeof(float4), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy((void*)(A.jfs + desc[k].jf_off), fjs.data(), fjs.size() * sizeof(float4), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, (void*)(A.ifs + desc[k].if_off), fis.data(), fis.size() * sizeof(float4), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, (void*)(A.jfs + desc[k].jf_off), fjs.data(), fjs.size() * sizeof(float4), cudaMemcpyHostToDevice));
     }
     return 0;
   }
@@ -719,9 +720,9 @@ struct ArenaHost {
       df[cc] = std::isfinite(d[cc]) ? (float)d[cc] : 3.0e38f;
       mt[cc] = h.solid((int)(cc % h.ni), (int)(cc / h.ni)) ? 0.f : (float)(u[4 * cc] * kinf / winf);
     }
-    BK_CUDA(cudaMemcpy(A.dwall + c.cell_off, df.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(A.turb + c.cell_off, t.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(A.mu_t + c.cell_off, mt.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, A.dwall + c.cell_off, df.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, A.turb + c.cell_off, t.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, A.mu_t + c.cell_off, mt.data(), n * sizeof(float), cudaMemcpyHostToDevice));
     return 0;
   }
   int turb_upload(int k, const double* turb, const double* mu_t) {
@@ -730,12 +731,12 @@ struct ArenaHost {
     if (turb) {
       std::vector<float2> t(n);
       for (size_t i = 0; i < n; ++i) t[i] = make_float2((float)turb[2 * i], (float)turb[2 * i + 1]);
-      BK_CUDA(cudaMemcpy(A.turb + c.cell_off, t.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, A.turb + c.cell_off, t.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
     }
     if (mu_t) {
       std::vector<float> m(n);
       for (size_t i = 0; i < n; ++i) m[i] = (float)mu_t[i];
-      BK_CUDA(cudaMemcpy(A.mu_t + c.cell_off, m.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, A.mu_t + c.cell_off, m.data(), n * sizeof(float), cudaMemcpyHostToDevice));
     }
     return 0;
   }
@@ -760,11 +761,11 @@ struct ArenaHost {
       l[i] = make_float4((float)(q[0] - (double)h[i].x), (float)(q[1] - (double)h[i].y), (float)(q[2] - (double)h[i].z),
                          (float)(q[3] - (double)h[i].w));
     }
-    BK_CUDA(cudaMemcpy(A.U + c.cell_off, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(A.Ulo + c.cell_off, l.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, A.U + c.cell_off, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, A.Ulo + c.cell_off, l.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
     int z = 0;
-    BK_CUDA(cudaMemcpy(d_iter + k, &z, sizeof(int), cudaMemcpyHostToDevice));
-    BK_CUDA(cudaMemcpy(d_ramp + k, &z, sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_iter + k, &z, sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d_ramp + k, &z, sizeof(int), cudaMemcpyHostToDevice));
     return 0;
   }
 
@@ -773,8 +774,8 @@ struct ArenaHost {
     size_t n = (size_t)c.ni * c.nj;
     std::vector<float4> h(n), l(n);
     BK_CUDA(cudaStreamSynchronize(stream));
-    BK_CUDA(cudaMemcpy(h.data(), A.U + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    BK_CUDA(cudaMemcpy(l.data(), A.Ulo + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    BK_CUDA(copy_sync(stream, h.data(), A.U + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    BK_CUDA(copy_sync(stream, l.data(), A.Ulo + c.cell_off, n * sizeof(float4), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) {
       u[4 * i] = (double)h[i].x + (double)l[i].x;
       u[4 * i + 1] = (double)h[i].y + (double)l[i].y;
@@ -785,12 +786,12 @@ struct ArenaHost {
   }
 
   int set_counter(int* d, int k, int v) {
-    BK_CUDA(cudaMemcpy(d + k, &v, sizeof(int), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(stream, d + k, &v, sizeof(int), cudaMemcpyHostToDevice));
     return 0;
   }
   int get_counter(const int* d, int k, int& v) {
     BK_CUDA(cudaStreamSynchronize(stream));
-    BK_CUDA(cudaMemcpy(&v, d + k, sizeof(int), cudaMemcpyDeviceToHost));
+    BK_CUDA(copy_sync(stream, &v, d + k, sizeof(int), cudaMemcpyDeviceToHost));
     return 0;
   }
   int set_active(const int* act) {
@@ -830,11 +831,11 @@ struct ArenaHost {
       for (auto& p : li) il.push_back(p.second);
       for (auto& p : lj) jl.push_back(p.second);
       if (want) {
-        BK_CUDA(cudaMemcpy(d_tlist, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice));
-        BK_CUDA(cudaMemcpy(d_pblist, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
+        BK_CUDA(copy_sync(stream, d_tlist, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice));
+        BK_CUDA(copy_sync(stream, d_pblist, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
       }
-      BK_CUDA(cudaMemcpy(d_illist, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy(d_jllist, jl.data(), jl.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, d_illist, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, d_jllist, jl.data(), jl.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
     A.tile_list = want ? d_tlist : nullptr;
     A.pblk_list = want ? d_pblist : nullptr;
@@ -1332,7 +1333,7 @@ struct ArenaHost {
     size_t n = (size_t)c.ni * c.nj;
     std::vector<T> h(n);
     BK_CUDA(cudaStreamSynchronize(stream));
-    BK_CUDA(cudaMemcpy(h.data(), dptr + c.cell_off, n * sizeof(T), cudaMemcpyDeviceToHost));
+    BK_CUDA(copy_sync(stream, h.data(), dptr + c.cell_off, n * sizeof(T), cudaMemcpyDeviceToHost));
     out.resize(n * comps);
     const float* f = reinterpret_cast<const float*>(h.data());
     for (size_t i = 0; i < n * comps; ++i) out[i] = f[i];

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/bowshock_b200.h"
+#include "stream_copy.cuh"
 #include "tma.cuh"
 
 namespace bknet {
@@ -96,6 +97,10 @@ struct GemmArgs {
   const float* bias;
   float slope;  // leaky ReLU slope of EPI_BIAS_ACT_BF16 (1 = identity)
   int* err;     // set to 1 when a wait gave up
+  // implicit-GEMM convolution (k_gemm_conv): A is the im2col of the NHWC input cx [cB, cHin, cWin, cC] of a 3x3 'same'
+  // convolution at (cHin << cup) x (cWin << cup), never stored; cC a multiple of 64
+  const bf16* cx;
+  int cB, cHin, cWin, cC, cup;
 };
 
 template <int BN>
@@ -175,6 +180,183 @@ __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtenso
   bool ok = nkb > 0 && mbar_wait(done, 0);
   if (!ok && nkb > 0) s_abort = 1;
   ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
+  tc_fence_after();
+  const int row = m0 + warp * 32 + lane;
+  if (ok) {
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 16) {
+      uint32_t r[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+      tmem_ld_wait();
+      if (row >= g.M) continue;
+      const int nb = n0 + c;
+      if (g.mode == EPI_BIAS_ACT_BF16) {
+        bf16* yp = g.y + (long long)row * g.ldy + nb;
+#pragma unroll
+        for (int q = 0; q < 16; q += 2) {
+          if (nb + q >= g.N) break;
+          float v0 = __uint_as_float(r[q]) + g.bias[nb + q];
+          v0 = v0 > 0.f ? v0 : g.slope * v0;
+          if (nb + q + 1 < g.N) {
+            float v1 = __uint_as_float(r[q + 1]) + g.bias[nb + q + 1];
+            v1 = v1 > 0.f ? v1 : g.slope * v1;
+            *reinterpret_cast<__nv_bfloat162*>(yp + q) = __floats2bfloat162_rn(v0, v1);
+          } else {
+            yp[q] = __float2bfloat16_rn(v0);
+          }
+        }
+      } else {
+        float* dp = g.d + (long long)row * g.ldd + nb;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          if (nb + q >= g.N) break;
+          float v = __uint_as_float(r[q]);
+          if (g.mode == EPI_F32_ATOMIC)
+            atomicAdd(dp + q, v);
+          else if (g.mode == EPI_BIAS_F32)
+            dp[q] = v + g.bias[nb + q];
+          else
+            dp[q] = v;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TCOLS);
+  }
+}
+
+// The same GEMM with its A operand gathered on the fly (implicit-GEMM convolution): row m of A is output pixel m, and its
+// K block kb holds the 64 input channels c0 .. c0 + 63 of tap (kb * 64) / C at the pixel shifted by the tap (zeros
+// outside the image), 128 contiguous bytes of the NHWC input. The 64 threads of warps 2 and 3 copy each 128-row A tile
+// with cp.async (16-byte chunks, zero fill outside), placed in the 128-byte-swizzle layout a TMA load would give (chunk
+// q of row r at r * 128 + (q ^ (r & 7)) * 16); warp 0 lane 0 brings B (the weights) by TMA. A stage's barrier completes
+// after that lane's expect-tx arrival (with the B bytes) and one arrival per copying thread, each made once the thread's
+// copies of the stage have landed and been fenced for the tensor cores (the copies run LAG = 2 stages ahead of the
+// arrivals). Warp 1 lane 0 issues the MMAs, all four warps run the epilogue.
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+template <int BN>
+__global__ void __launch_bounds__(128, 1) k_gemm_conv(const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, TCOLS = tmem_cols<BN>(), LAG = 2;
+  uint8_t* sa = smem;
+  uint8_t* sb = smem + STAGES * A_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sb + STAGES * B_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  __shared__ int s_abort;
+  __shared__ int rb[BM], ry[BM], rx[BM];  // image, row and column of each output pixel of the tile (rb < 0: past M)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nkb_total = (g.K + BK - 1) / BK;
+  const int kb0 = blockIdx.z * g.kb_per_split;
+  const int nkb = min(g.kb_per_split, nkb_total - kb0);
+  const int H = g.cHin << g.cup, W = g.cWin << g.cup;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(full + s, 65), mbar_init(empty + s, 1);
+    mbar_init(done, 1);
+    bktma::mbar_init_fence();
+    s_abort = 0;
+  }
+  {
+    const int m = threadIdx.x, p = m0 + m;  // 128 threads, one row each
+    if (p < g.M) {
+      rx[m] = p % W;
+      ry[m] = (p / W) % H;
+      rb[m] = p / (W * H);
+    } else {
+      rb[m] = -1, ry[m] = 0, rx[m] = 0;
+    }
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, TCOLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  constexpr uint32_t IDESC = idesc_bf16(BM, BN);
+  if (nkb > 0 && warp == 0 && lane == 0) {  // B (the weights) by TMA
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % STAGES;
+      const uint32_t ph = (uint32_t)((i / STAGES) & 1);
+      if (i >= STAGES && !mbar_wait(empty + s, ph ^ 1u)) {
+        s_abort = 1;
+        break;
+      }
+      mbar_expect_tx(full + s, (uint32_t)B_BYTES);
+      tma_load_2d(sb + s * B_BYTES, &tb, full + s, (kb0 + i) * BK, n0);
+    }
+  } else if (nkb > 0 && warp >= 2) {  // warps 2 and 3: A gathered by cp.async
+    const int q = threadIdx.x - 64, part = q & 7, r0 = q >> 3;
+    int issued = 0;
+    bool aborted = false;
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % STAGES;
+      const uint32_t ph = (uint32_t)((i / STAGES) & 1);
+      int ok = 1;
+      if (i >= STAGES && lane == 0) ok = mbar_wait(empty + s, ph ^ 1u) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) s_abort = 1;
+        aborted = true;
+        break;
+      }
+      const int k0 = (kb0 + i) * BK, tap = k0 / g.cC, c0 = k0 % g.cC;
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+      const uint32_t base = smem_u32(sa + s * A_BYTES);
+#pragma unroll 4
+      for (int t = 0; t < BM / 8; ++t) {
+        const int r = r0 + 8 * t;
+        const int b = rb[r], yy = ry[r] + dy, xx = rx[r] + dx;
+        const bool in = b >= 0 && yy >= 0 && yy < H && xx >= 0 && xx < W;
+        const bf16* src = in ? g.cx + ((((long long)b * g.cHin + (yy >> g.cup)) * g.cWin + (xx >> g.cup)) * g.cC + c0 + part * 8) : g.cx;
+        cp_async16_zfill(base + (uint32_t)(r * 128 + ((part ^ (r & 7)) << 4)), src, in ? 16u : 0u);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      ++issued;
+      if (i >= LAG) {
+        asm volatile("cp.async.wait_group 2;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(full + (i - LAG) % STAGES);
+      }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (!aborted)
+      for (int i = max(0, issued - LAG); i < issued; ++i) mbar_arrive(full + i % STAGES);
+  } else if (nkb > 0 && warp == 1 && lane == 0) {  // MMA issuer (as k_gemm)
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % STAGES;
+      const uint32_t ph = (uint32_t)((i / STAGES) & 1);
+      if (!mbar_wait(full + s, ph)) {
+        s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint64_t ad = sw128_desc(sa + s * A_BYTES), bd = sw128_desc(sb + s * B_BYTES);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) mma_bf16(tmem, ad + 2ull * kk, bd + 2ull * kk, IDESC, (i | kk) != 0);
+      mma_commit(empty + s);
+    }
+    mma_commit(done);
+  }
+  __syncwarp();
+  bool ok = nkb > 0 && mbar_wait(done, 0);
+  if (!ok && nkb > 0) s_abort = 1;
+  ok = __all_sync(0xffffffffu, ok);
   tc_fence_after();
   const int row = m0 + warp * 32 + lane;
   if (ok) {
@@ -467,6 +649,50 @@ static int gemm(const bf16* A, long long lda, const bf16* B, long long ldb, int 
   return 0;
 }
 
+template <int BN>
+static cudaError_t launch_conv_bn(const CUtensorMap& tb, const GemmArgs& g, dim3 grid, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_conv<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>());
+  if (e != cudaSuccess) return e;
+  k_gemm_conv<BN><<<grid, 128, gemm_smem_bytes<BN>(), st>>>(tb, g);
+  return cudaGetLastError();
+}
+
+// D[p, n] = sum over taps and channels of x[pixel p shifted by the tap][c] w[n][tap * C + c]: the 3x3 'same'
+// convolution of the NHWC input x [B, Hin, Win, C] (C a multiple of 64, read through a 2x upsampling when up = 1) by the
+// weights w [N, 9 C] (BF16, ldw elements per row) as an implicit GEMM (no im2col matrix); the epilogue as in g.
+static int conv_gemm(const bf16* x, int B, int Hin, int Win, int C, int up, const bf16* w, long long ldw, int N, GemmArgs g, cudaStream_t st,
+                     std::string& err) {
+  if (C % 64) {
+    err = "the implicit-GEMM convolution needs a multiple of 64 input channels";
+    return BOWSHOCK_INVALID;
+  }
+  if (!get_encode(err)) return BOWSHOCK_CUDA_ERROR;
+  const int bn = pick_bn(N);
+  const long long M = (long long)B * (Hin << up) * (Win << up);
+  CUtensorMap tb;
+  if (!make_map(&tb, w, N, 9LL * C, ldw, bn, err)) return BOWSHOCK_INVALID;
+  if (((uintptr_t)x & 15)) {
+    err = "convolution input not 16-byte aligned";
+    return BOWSHOCK_INVALID;
+  }
+  g.M = (int)M, g.N = N, g.K = 9 * C, g.kb_per_split = (9 * C) / BK;
+  g.cx = x, g.cB = B, g.cHin = Hin, g.cWin = Win, g.cC = C, g.cup = up;
+  dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)((N + bn - 1) / bn), 1);
+  cudaError_t e;
+  switch (bn) {
+    case 16: e = launch_conv_bn<16>(tb, g, grid, st); break;
+    case 32: e = launch_conv_bn<32>(tb, g, grid, st); break;
+    case 64: e = launch_conv_bn<64>(tb, g, grid, st); break;
+    case 128: e = launch_conv_bn<128>(tb, g, grid, st); break;
+    default: e = launch_conv_bn<256>(tb, g, grid, st); break;
+  }
+  if (e != cudaSuccess) {
+    err = std::string("convolution GEMM launch: ") + cudaGetErrorString(e);
+    return BOWSHOCK_CUDA_ERROR;
+  }
+  return 0;
+}
+
 static int grid_for(long long n, int threads = 256) { return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148 * 16)); }
 
 // ---------------------------------------------------------------------------------------------------- the network
@@ -506,6 +732,7 @@ struct Net {
   int* idx = nullptr;
   long long idx_cap = 0;
   double last_ms = 0.0;
+  bool implicit_conv = true;  // 3x3 convolutions of 64k channels as implicit GEMMs (else im2col + GEMM)
 
   ~Net() {
     for (void* p : {(void*)w, (void*)gw, (void*)m1, (void*)m2, (void*)wb, (void*)x, (void*)out, (void*)col, (void*)colT, (void*)gT, (void*)wt,
@@ -560,8 +787,8 @@ struct Net {
     NCK(cudaMalloc(&m1, nparam * 4));
     NCK(cudaMalloc(&m2, nparam * 4));
     NCK(cudaMalloc(&wb, nparam * 2));
-    NCK(cudaMemset(w, 0, nparam * 4));
-    NCK(cudaMemset(wb, 0, nparam * 2));
+    NCK(cudaMemsetAsync(w, 0, nparam * 4, stream));
+    NCK(cudaMemsetAsync(wb, 0, nparam * 2, stream));
     NCK(cudaMalloc(&x, (size_t)maxB * BOWSHOCK_NET_IN * 2));
     act.assign(L.size(), nullptr);
     long long max_col = 0, max_rows_c = 0;
@@ -585,13 +812,13 @@ struct Net {
     for (auto& l : L) maxw = std::max(maxw, (long long)l.cout * l.kin);
     NCK(cudaMalloc(&wt, maxw * 2));
     NCK(cudaMalloc(&d_err, sizeof(int)));
-    NCK(cudaMemset(d_err, 0, sizeof(int)));
+    NCK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     NCK(cudaMalloc(&d_step, sizeof(int)));
     NCK(cudaMalloc(&coef, sizeof(float)));
     NCK(cudaMalloc(&loss1, sizeof(float)));
     NCK(cudaMalloc(&tb, (size_t)maxB * BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT * 4));
     NCK(cudaMalloc(&mask, BOWSHOCK_NET_CELLS));
-    NCK(cudaMemset(mask, 1, BOWSHOCK_NET_CELLS));
+    NCK(cudaMemsetAsync(mask, 1, BOWSHOCK_NET_CELLS, stream));
     return reset_optimizer();
   }
 
@@ -604,7 +831,7 @@ struct Net {
   }
 
   int set_params(const float* h) {
-    NCK(cudaMemcpy(w, h, nparam * 4, cudaMemcpyHostToDevice));
+    NCK(copy_sync(stream, w, h, nparam * 4, cudaMemcpyHostToDevice));
     k_to_bf16<<<grid_for(nparam), 256, 0, stream>>>(w, nparam, wb);
     NCK(cudaGetLastError());
     NCK(cudaStreamSynchronize(stream));
@@ -613,9 +840,10 @@ struct Net {
 
   int check_err() {
     int h = 0;
-    NCK(cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    NCK(copy_sync(stream, &h, d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) {
-      cudaMemset(d_err, 0, sizeof(int));
+      cudaMemsetAsync(d_err, 0, sizeof(int), stream);
+      cudaStreamSynchronize(stream);
       return fail(BOWSHOCK_TIMEOUT, "a tensor-core GEMM gave up waiting on its pipeline (bounded wait)");
     }
     return 0;
@@ -633,17 +861,22 @@ struct Net {
       g.bias = w + l.boff;
       const bf16* A;
       long long lda;
+      if (l.act) {
+        g.mode = EPI_BIAS_ACT_BF16, g.y = act[k], g.ldy = l.cout, g.slope = BOWSHOCK_NET_SLOPE;
+      } else {
+        g.mode = EPI_BIAS_F32, g.d = out, g.ldd = l.cout;
+      }
+      if (!l.fc && implicit_conv && l.cin % 64 == 0) {  // the convolution as an implicit GEMM: no im2col matrix
+        if ((rc = conv_gemm(in, B, l.H >> l.up, l.W >> l.up, l.cin, l.up, wb + l.woff, l.kin, l.cout, g, stream, err))) return rc;
+        in = act[k];
+        continue;
+      }
       if (l.fc) {
         A = in, lda = l.cin;
       } else {
         const int Hin = l.H >> l.up, Win = l.W >> l.up;
         k_im2col<<<grid_for(r * 9 * (l.cin / 8)), 256, 0, stream>>>(in, B, Hin, Win, l.cin, l.up, col);
         A = col, lda = l.kin;
-      }
-      if (l.act) {
-        g.mode = EPI_BIAS_ACT_BF16, g.y = act[k], g.ldy = l.cout, g.slope = BOWSHOCK_NET_SLOPE;
-      } else {
-        g.mode = EPI_BIAS_F32, g.d = out, g.ldd = l.cout;
       }
       if ((rc = gemm(A, lda, wb + l.woff, l.kin, (int)r, l.cout, (int)l.kin, g, 1, stream, err))) return rc;
       in = act[k];
@@ -696,9 +929,13 @@ struct Net {
         if ((rc = gemm(g, l.cout, wt, l.cout, (int)r, l.cin, l.cout, gx, 1, stream, err))) return rc;
         k_grad_prev<<<grid_for(r * l.cin), 256, 0, stream>>>(dx, B, 1, 1, l.cin, 0, xin, BOWSHOCK_NET_SLOPE, gnext);
       } else {
-        k_im2col<<<grid_for(r * 9 * (l.cout / 8)), 256, 0, stream>>>(g, B, l.H, l.W, l.cout, 0, col);
         k_flip_weights<<<grid_for((long long)l.cin * 9 * l.cout), 256, 0, stream>>>(wb + l.woff, l.cin, l.cout, wt);
-        if ((rc = gemm(col, 9LL * l.cout, wt, 9LL * l.cout, (int)r, l.cin, 9 * l.cout, gx, 1, stream, err))) return rc;
+        if (implicit_conv && l.cout % 64 == 0) {
+          if ((rc = conv_gemm(g, B, l.H, l.W, l.cout, 0, wt, 9LL * l.cout, l.cin, gx, stream, err))) return rc;
+        } else {
+          k_im2col<<<grid_for(r * 9 * (l.cout / 8)), 256, 0, stream>>>(g, B, l.H, l.W, l.cout, 0, col);
+          if ((rc = gemm(col, 9LL * l.cout, wt, 9LL * l.cout, (int)r, l.cin, 9 * l.cout, gx, 1, stream, err))) return rc;
+        }
         // the previous layer's output resolution (a fully connected layer's 4096 features are the 4 x 8 x 128 map)
         const int Hin = l.H >> l.up, Win = l.W >> l.up;
         k_grad_prev<<<grid_for((long long)B * Hin * Win * l.cin), 256, 0, stream>>>(dx, B, Hin, Win, l.cin, l.up, xin, BOWSHOCK_NET_SLOPE, gnext);
@@ -798,14 +1035,14 @@ int bowshock_net_get_params(bowshock_net* h, float* p) {
   if (!h || !p) return BOWSHOCK_INVALID;
   NET_CK(h, cudaSetDevice(h->n.device));
   NET_CK(h, cudaStreamSynchronize(h->n.stream));
-  NET_CK(h, cudaMemcpy(p, h->n.w, h->n.nparam * 4, cudaMemcpyDeviceToHost));
+  NET_CK(h, copy_sync(h->n.stream, p, h->n.w, h->n.nparam * 4, cudaMemcpyDeviceToHost));
   return BOWSHOCK_OK;
 }
 
 int bowshock_net_set_mask(bowshock_net* h, const uint8_t* mask) {
   if (!h || !mask) return BOWSHOCK_INVALID;
   NET_CK(h, cudaSetDevice(h->n.device));
-  NET_CK(h, cudaMemcpy(h->n.mask, mask, BOWSHOCK_NET_CELLS, cudaMemcpyHostToDevice));
+  NET_CK(h, copy_sync(h->n.stream, h->n.mask, mask, BOWSHOCK_NET_CELLS, cudaMemcpyHostToDevice));
   return BOWSHOCK_OK;
 }
 
@@ -863,8 +1100,8 @@ int bowshock_net_set_dataset(bowshock_net* h, uint64_t n_samples, const float* x
   const size_t nt = (size_t)BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT;
   NET_CK(h, cudaMalloc(&n.dsx, n_samples * BOWSHOCK_NET_IN * 4));
   NET_CK(h, cudaMalloc(&n.dst, n_samples * nt * 4));
-  NET_CK(h, cudaMemcpy(n.dsx, x, n_samples * BOWSHOCK_NET_IN * 4, cudaMemcpyHostToDevice));
-  NET_CK(h, cudaMemcpy(n.dst, target, n_samples * nt * 4, cudaMemcpyHostToDevice));
+  NET_CK(h, copy_sync(n.stream, n.dsx, x, n_samples * BOWSHOCK_NET_IN * 4, cudaMemcpyHostToDevice));
+  NET_CK(h, copy_sync(n.stream, n.dst, target, n_samples * nt * 4, cudaMemcpyHostToDevice));
   n.nds = (long long)n_samples;
   return BOWSHOCK_OK;
 }
@@ -922,7 +1159,7 @@ int bowshock_net_train(bowshock_net* h, uint64_t steps, uint64_t batch, double l
   if (rc) return rc;
   if (loss) {
     std::vector<float> hl(steps);
-    NET_CK(h, cudaMemcpy(hl.data(), n.loss, steps * sizeof(float), cudaMemcpyDeviceToHost));
+    NET_CK(h, copy_sync(n.stream, hl.data(), n.loss, steps * sizeof(float), cudaMemcpyDeviceToHost));
     for (uint64_t s = 0; s < steps; ++s) loss[s] = hl[s];
   }
   return n.check_err();
@@ -932,6 +1169,22 @@ int bowshock_net_last_train_ms(const bowshock_net* h, double* ms) {
   if (!h || !ms) return BOWSHOCK_INVALID;
   *ms = h->n.last_ms;
   return BOWSHOCK_OK;
+}
+
+int bowshock_net_set_implicit_conv(bowshock_net* h, int on) {
+  if (!h) return BOWSHOCK_INVALID;
+  h->n.implicit_conv = on != 0;
+  return BOWSHOCK_OK;
+}
+
+int bowshock_conv3x3_bf16(const void* x, int64_t batch, int64_t h_in, int64_t w_in, int64_t c, int64_t up, const void* w, int64_t n, float* d,
+                          void* stream, int* err_flag) {
+  if (!x || !w || !d || !err_flag || batch <= 0 || h_in <= 0 || w_in <= 0 || c <= 0 || n <= 0 || (up != 0 && up != 1)) return BOWSHOCK_INVALID;
+  std::string err;
+  bknet::GemmArgs g{};
+  g.mode = bknet::EPI_F32, g.d = d, g.ldd = n, g.err = err_flag;
+  return bknet::conv_gemm(reinterpret_cast<const bknet::bf16*>(x), (int)batch, (int)h_in, (int)w_in, (int)c, (int)up,
+                          reinterpret_cast<const bknet::bf16*>(w), 9 * c, (int)n, g, reinterpret_cast<cudaStream_t>(stream), err);
 }
 
 int bowshock_gemm_bf16(const void* a, int64_t lda, const void* b, int64_t ldb, float* d, int64_t ldd, int64_t m, int64_t n, int64_t k, int64_t splits,

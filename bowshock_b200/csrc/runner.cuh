@@ -8,6 +8,7 @@
 
 #include "forces.cuh"
 #include "host_arena.cuh"
+#include "stream_copy.cuh"
 
 namespace bk {
 
@@ -138,12 +139,12 @@ struct ForcePass {
       return rc_;
     for (int k = 0; k < nc; ++k) {
       const HostCase& h = ar.cases[k];
-      BK_CUDA(cudaMemcpy(nx + off[k], h.x.data(), h.x.size() * sizeof(double), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy(nr + off[k], h.r.data(), h.r.size() * sizeof(double), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy(xc + ar.desc[k].cell_off, h.xc.data(), h.xc.size() * sizeof(double), cudaMemcpyHostToDevice));
-      BK_CUDA(cudaMemcpy(rc + ar.desc[k].cell_off, h.rc.data(), h.rc.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(ar.stream, nx + off[k], h.x.data(), h.x.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(ar.stream, nr + off[k], h.r.data(), h.r.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(ar.stream, xc + ar.desc[k].cell_off, h.xc.data(), h.xc.size() * sizeof(double), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(ar.stream, rc + ar.desc[k].cell_off, h.rc.data(), h.rc.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
-    BK_CUDA(cudaMemcpy(node_off, off.data(), nc * sizeof(long long), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(ar.stream, node_off, off.data(), nc * sizeof(long long), cudaMemcpyHostToDevice));
     hb.assign(nc, BodyDev{});
     return 0;
   }
@@ -163,7 +164,7 @@ struct ForcePass {
     for (int s = 0; s <= d.nseg; ++s) d.stations[s] = mb.station(s).first;
     d.has_body = 1;
     hb[k] = d;
-    BK_CUDA(cudaMemcpy(bodies + k, &d, sizeof(BodyDev), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(ar.stream, bodies + k, &d, sizeof(BodyDev), cudaMemcpyHostToDevice));
     return 0;
   }
   int run(ArenaHost& ar, std::vector<Forces>& res) {
@@ -414,7 +415,7 @@ inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
     }
     std::string& err = ar.err;
     BK_CUDA(cudaMalloc(&d_runs, (size_t)nr * sizeof(RunDev)));
-    BK_CUDA(cudaMemcpy(d_runs, hr.data(), (size_t)nr * sizeof(RunDev), cudaMemcpyHostToDevice));
+    BK_CUDA(copy_sync(ar.stream, d_runs, hr.data(), (size_t)nr * sizeof(RunDev), cudaMemcpyHostToDevice));
   }
   while (true) {
     int left = 0;
@@ -466,7 +467,7 @@ inline int solve_arena(ArenaHost& ar, ForcePass& fp, std::vector<CaseRun>& runs,
         if (dev) {  // the device stops iterating this run too
           std::string& err = ar.err;
           const int one = 1;
-          BK_CUDA(cudaMemcpy(reinterpret_cast<char*>(d_runs + k) + offsetof(RunDev, done), &one, sizeof(int), cudaMemcpyHostToDevice));
+          BK_CUDA(copy_sync(ar.stream, reinterpret_cast<char*>(d_runs + k) + offsetof(RunDev, done), &one, sizeof(int), cudaMemcpyHostToDevice));
         }
       }
       if (cr.done) act[k] = 0, mask_changed = true;

@@ -92,6 +92,10 @@ class Net:
         self._check(_ffi.load().bowshock_net_train(self._h, int(steps), int(batch), float(lr), int(seed), _ffi.dptr(loss)))
         return loss
 
+    def set_implicit_conv(self, on: bool):
+        """3x3 convolutions as implicit GEMMs (True, the default) or through an im2col matrix (False)."""
+        self._check(_ffi.load().bowshock_net_set_implicit_conv(self._h, int(bool(on))))
+
     def last_train_ms(self) -> float:
         ms = C.c_double()
         self._check(_ffi.load().bowshock_net_last_train_ms(self._h, C.byref(ms)))

@@ -127,3 +127,59 @@ def test_net_training_lowers_the_loss():
     assert np.all(np.isfinite(loss))
     assert loss[-20:].mean() < 0.2 * loss[:5].mean(), f"loss {loss[:5].mean():.3e} -> {loss[-20:].mean():.3e}"
     assert net.last_train_ms() > 0
+
+
+@pytest.mark.parametrize("batch,h,w,c,up,n", [(2, 4, 8, 128, 0, 128), (3, 8, 16, 128, 1, 64), (2, 16, 32, 64, 1, 64),
+                                              (1, 32, 64, 64, 0, 16), (5, 7, 9, 64, 0, 200), (4, 32, 64, 64, 0, 64)])
+def test_implicit_conv_matches_torch_fp32(batch, h, w, c, up, n):
+    """The implicit-GEMM convolution (A gathered by cp.async into the swizzled tile, no im2col matrix) against torch's
+    FP32 convolution of the same BF16 input (nearest 2x upsampled when up = 1) and weights, zero padding 1."""
+    import torch
+    from bowshock_b200 import _ffi
+    g = torch.Generator(device="cuda").manual_seed(batch * 31 + h * 7 + c + n + up)
+    x = torch.randn((batch, h, w, c), generator=g, device="cuda").to(torch.bfloat16)
+    wt = torch.randn((n, 3, 3, c), generator=g, device="cuda").to(torch.bfloat16)
+    H, W = h << up, w << up
+    d = torch.zeros((batch * H * W, n), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = _ffi.load().bowshock_conv3x3_bf16(C.c_void_p(x.data_ptr()), batch, h, w, c, up, C.c_void_p(wt.data_ptr()), n,
+                                          C.c_void_p(d.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                          C.c_void_p(err.data_ptr()))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0, "a bounded wait of the convolution gave up"
+    xi = x.float().permute(0, 3, 1, 2)
+    if up:
+        xi = torch.nn.functional.interpolate(xi, scale_factor=2, mode="nearest")
+    ref = torch.nn.functional.conv2d(xi, wt.float().permute(0, 3, 1, 2), padding=1).permute(0, 2, 3, 1).reshape(-1, n)
+    scale = ref.abs().amax(dim=1, keepdim=True) + 1e-6
+    e = ((d - ref).abs() / scale).max().item()
+    assert e < 1e-4, f"conv {batch}x{h}x{w}x{c} up {up} -> {n}: max rel err {e:.2e}"
+
+
+def test_implicit_conv_network_equals_im2col():
+    """The network's forward outputs and gradients are the same, bit for bit, with its convolutions as implicit GEMMs
+    and through im2col matrices: both feed the tensor cores the same K blocks in the same order."""
+    net, L, n, pr, x, rng = _net_and_oracle()
+    t = rng.standard_normal((x.shape[0], no.NET_CELLS, no.NET_OUT)).astype(np.float32) * 0.5
+    outs = []
+    for on in (True, False):
+        net.set_implicit_conv(on)
+        y = net.forward(x)
+        loss, g = net.gradients(x, t)
+        outs.append((y, loss, g))
+    (y1, l1, g1), (y0, l0, g0) = outs
+    assert np.array_equal(y1, y0)
+    assert l1 == l0
+    assert np.array_equal(g1, g0)
+
+
+def test_net_forward_repeatable():
+    """Two forward passes of the same inputs give the same outputs, bit for bit, and a pass of a smaller batch the same
+    rows (the epilogue and the GEMM tiles do not depend on the batch's other rows)."""
+    net, L, n, pr, x, _ = _net_and_oracle()
+    y1 = net.forward(x)
+    y2 = net.forward(x)
+    assert np.array_equal(y1, y2)
+    y3 = net.forward(x[:3])
+    assert np.array_equal(y3, y1[:3])
