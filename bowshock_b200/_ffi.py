@@ -81,6 +81,10 @@ class StingGridC(C.Structure):  # bowshock_sting_grid
                 ("n_seg", C.c_uint64 * 8), ("n_ext", C.c_uint64), ("nj", C.c_uint64), ("dx_tip", C.c_double), ("dr_wall", C.c_double)]
 
 
+class MeshRequest(C.Structure):  # bowshock_mesh_request
+    _fields_ = [("wake", C.c_int32), ("body", BowshockBody), ("base", BaseGridC), ("sting", StingGridC)]
+
+
 class LineTuning(C.Structure):  # bowshock_line_tuning
     _fields_ = [(n, C.c_int32) for n in ("lines_i", "lines_j", "prefetch_i", "prefetch_j", "subst_i", "subst_j", "turb_lines",
                                               "segment_i", "segment_j", "residual", "subst_prefetch_i",
@@ -140,6 +144,9 @@ SIGNATURES = {
                                        C.POINTER(Block)]),
     "bowshock_large_domain_grid": (_I, [C.POINTER(BowshockBody), C.POINTER(StingGridC), C.POINTER(_U), C.POINTER(_U), _dp, _dp]),
     "bowshock_arena_create": (_I, [_U, C.POINTER(CaseDesc), _I, C.POINTER(_P)]),
+    "bowshock_arena_create_meshed": (_I, [_U, C.POINTER(CaseDesc), C.POINTER(MeshRequest), _I, C.POINTER(_P)]),
+    "bowshock_mesh_dims": (_I, [C.POINTER(MeshRequest), C.POINTER(_U), C.POINTER(_U), C.POINTER(Block)]),
+    "bowshock_mesh_batch": (_I, [_U, C.POINTER(MeshRequest), _I, _dp, _dp, _dp, _dp]),
     "bowshock_arena_destroy": (None, [_P]),
     "bowshock_case_wall_distance": (_I, [C.POINTER(CaseDesc), _dp]),
     "bowshock_arena_last_error": (C.c_char_p, [_P]),

@@ -13,17 +13,34 @@ from .solver import point_dict, forces_dict
 
 
 class Arena:
-    def __init__(self, cases, device=0, grids=None):
-        """`cases`: list of case.Case; `grids`: optional precomputed (ni, nj, x, r, block) per case."""
+    def __init__(self, cases, device=0, grids=None, device_mesh=False):
+        """`cases`: list of case.Case; `grids`: optional precomputed (ni, nj, x, r, block) per case; `device_mesh`: build
+        every grid and its metrics on the device (bowshock_arena_create_meshed) instead of on the host."""
         lib = _ffi.load()
         self.cases = list(cases)
         self._descs = (_ffi.CaseDesc * len(self.cases))()
         self._keep = []
+        h = C.c_void_p()
+        if device_mesh:
+            qs = (_ffi.MeshRequest * len(self.cases))()
+            for k, c in enumerate(self.cases):
+                ni, nj, blk = c.mesh_dims()
+                n = (ni + 1) * (nj + 1)
+                # the descriptor wants node arrays of the right size; the arena ignores their values
+                d = c.case_desc((ni, nj, np.zeros(n), np.zeros(n), blk))
+                self._keep.append((d._x, d._r))
+                self._descs[k] = d
+                qs[k] = c.mesh_request()
+            rc = lib.bowshock_arena_create_meshed(len(self.cases), self._descs, qs, device, C.byref(h))
+            if rc:
+                raise BowshockError(rc, "bowshock_arena_create_meshed failed (invalid case, or no usable CUDA device)")
+            self._h = h
+            self.ncases = len(self.cases)
+            return
         for k, c in enumerate(self.cases):
             d = c.case_desc(grids[k] if grids is not None else None)
             self._keep.append((d._x, d._r))
             self._descs[k] = d
-        h = C.c_void_p()
         rc = lib.bowshock_arena_create(len(self.cases), self._descs, device, C.byref(h))
         if rc:
             raise BowshockError(rc, "bowshock_arena_create failed (invalid case, or no usable CUDA device)")

@@ -226,6 +226,30 @@ class Case:
         lib.bowshock_large_domain_grid(C.byref(b), C.byref(p), C.byref(ni), C.byref(nj), _ffi.dptr(x), _ffi.dptr(r))
         return ni.value, nj.value, x, r, None
 
+    def mesh_request(self):
+        """bowshock_mesh_request of this case's grid (the device mesher's input: body and grid parameters)."""
+        q = _ffi.MeshRequest()
+        q.wake = self.wake
+        q.body = self.body.c()
+        if self.wake == WAKE_BASE:
+            g = self.grid_base
+            q.base = _ffi.BaseGridC(g.x_up, g.x_down, g.r_far, g.n_up, g.n_nose, (C.c_uint64 * 8)(*g.n_seg), g.n_wake, g.n_sting, g.n_gap,
+                                    g.nj_out, g.dx_tip, g.dr_wall, int(g.gap_one_sided))
+        else:
+            g = self.grid_sting
+            q.sting = _ffi.StingGridC(g.x_up, g.x_down, g.r_far, g.n_up, g.n_nose, (C.c_uint64 * 8)(*g.n_seg), g.n_ext, g.nj, g.dx_tip,
+                                      g.dr_wall)
+        return q
+
+    def mesh_dims(self):
+        """(ni, nj, block or None) of this case's grid, from the cell counts (no meshing)."""
+        q = self.mesh_request()
+        ni, nj, blk = C.c_uint64(), C.c_uint64(), _ffi.Block()
+        rc = _ffi.load().bowshock_mesh_dims(C.byref(q), C.byref(ni), C.byref(nj), C.byref(blk))
+        if rc:
+            raise BowshockError(rc, "invalid grid parameters")
+        return ni.value, nj.value, ((blk.i_end, blk.j_end, blk.j_sting) if self.wake == WAKE_BASE else None)
+
     def config(self) -> Config:  # case.rs:148-155
         n = self.numerics
         return Config(n.cfl, n.limiter, freestream(self.mach), (BC_CHARACTERISTIC, n.outflow, BC_SLIPWALL, BC_CHARACTERISTIC),
@@ -294,3 +318,39 @@ def rans_params(altitude_m, d_nose):
     """analysis.rs:447-469: re_c = rho c d / mu and the Sutherland constant of the free stream."""
     a = isa(altitude_m)
     return a["density"] * a["sound_speed"] * d_nose / a["viscosity"], SUTHERLAND_S / a["temperature_k"]
+
+
+METRIC_NAMES = ("if_nx", "if_nr", "if_len", "if_rm", "jf_nx", "jf_nr", "jf_len", "jf_rm", "area", "vol", "xc", "rc")
+
+
+def mesh_batch(cases, device=0, metrics=True):
+    """The grids of `cases` built on the device (bowshock_mesh_batch): a list of (ni, nj, x, r, block) like Case.grid(),
+    the metrics of each case (a dict of METRIC_NAMES arrays, i faces (nj, ni+1), j faces (nj+1, ni), cells (nj, ni)) when
+    `metrics`, and the device time in ms."""
+    lib = _ffi.load()
+    qs = (_ffi.MeshRequest * len(cases))()
+    dims = []
+    for k, c in enumerate(cases):
+        qs[k] = c.mesh_request()
+        dims.append(c.mesh_dims())
+    nodes = sum((ni + 1) * (nj + 1) for ni, nj, _ in dims)
+    words = sum(4 * ((ni + 1) * nj + ni * (nj + 1) + ni * nj) for ni, nj, _ in dims)
+    x, r = np.zeros(nodes), np.zeros(nodes)
+    m = np.zeros(words) if metrics else None
+    ms = C.c_double()
+    rc = lib.bowshock_mesh_batch(len(cases), qs, int(device), _ffi.dptr(x), _ffi.dptr(r), _ffi.dptr(m) if metrics else None, C.byref(ms))
+    if rc:
+        raise BowshockError(rc, "bowshock_mesh_batch failed (invalid request, non-positive cell area, or no CUDA device)")
+    grids, mets, o, mo = [], [], 0, 0
+    for ni, nj, blk in dims:
+        n = (ni + 1) * (nj + 1)
+        grids.append((ni, nj, x[o:o + n].copy(), r[o:o + n].copy(), blk))
+        o += n
+        if metrics:
+            d = {}
+            for name, shape in zip(METRIC_NAMES, [(nj, ni + 1)] * 4 + [(nj + 1, ni)] * 4 + [(nj, ni)] * 4):
+                sz = shape[0] * shape[1]
+                d[name] = m[mo:mo + sz].reshape(shape).copy()
+                mo += sz
+            mets.append(d)
+    return grids, (mets if metrics else None), ms.value

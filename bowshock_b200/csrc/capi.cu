@@ -11,6 +11,7 @@
 #include "host_arena.cuh"
 #include "mesher.cuh"
 #include "host3.cuh"
+#include "mesher_dev.h"
 
 using namespace bk;
 
@@ -663,9 +664,9 @@ static int afrom(bowshock_arena* a, int rc) {
 
 extern "C" {
 
-int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int device, bowshock_arena** out) {
-  if (!out || !cases || ncases == 0) return BOWSHOCK_INVALID;
-  *out = nullptr;
+// The arena of ncases descriptors; met[k] (when met is not null): case k's metrics from the device mesher
+// (BOWSHOCK_MESH_METRIC_WORDS, in its order), else the FP64 metrics are computed here on the host.
+static int arena_build(uint64_t ncases, const bowshock_case_desc* cases, const std::vector<const double*>* met, int device, bowshock_arena** out) {
   bowshock_arena* a = new (std::nothrow) bowshock_arena();
   if (!a) return BOWSHOCK_INVALID;
   std::string m;
@@ -680,8 +681,21 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
     a->descs.push_back(d);
     a->nseg.push_back(d.body.nseg);
   }
-  // the FP64 metrics of each case, the cases spread over the host threads
-  if (!parallel_cases(a->ar.cases.size(), [&](size_t k, std::string& e) { return compute_metrics(a->ar.cases[k], e); }, m)) {
+  if (met) {
+    for (uint64_t k = 0; k < ncases; ++k) {
+      HostCase& h = a->ar.cases[k];
+      const size_t nif = (size_t)(h.ni + 1) * h.nj, njf = (size_t)h.ni * (h.nj + 1), nc = (size_t)h.ni * h.nj;
+      const double* p = (*met)[k];
+      auto take = [&](std::vector<double>& v, size_t n) {
+        v.assign(p, p + n);
+        p += n;
+      };
+      take(h.if_nx, nif), take(h.if_nr, nif), take(h.if_len, nif), take(h.if_rm, nif);
+      take(h.jf_nx, njf), take(h.jf_nr, njf), take(h.jf_len, njf), take(h.jf_rm, njf);
+      take(h.area, nc), take(h.vol, nc), take(h.xc, nc), take(h.rc, nc);
+    }
+  } else if (!parallel_cases(a->ar.cases.size(), [&](size_t k, std::string& e) { return compute_metrics(a->ar.cases[k], e); }, m)) {
+    // the FP64 metrics of each case, the cases spread over the host threads
     delete a;
     return BOWSHOCK_INVALID;
   }
@@ -700,6 +714,47 @@ int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int 
   }
   *out = a;
   return BOWSHOCK_OK;
+}
+
+int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int device, bowshock_arena** out) {
+  if (!out || !cases || ncases == 0) return BOWSHOCK_INVALID;
+  *out = nullptr;
+  return arena_build(ncases, cases, nullptr, device, out);
+}
+
+int bowshock_arena_create_meshed(uint64_t ncases, const bowshock_case_desc* cases, const bowshock_mesh_request* meshes, int device,
+                                 bowshock_arena** out) {
+  if (!out || !cases || !meshes || ncases == 0) return BOWSHOCK_INVALID;
+  *out = nullptr;
+  std::string m;
+  std::vector<size_t> noff(ncases), moff(ncases);
+  size_t nodes = 0, mets = 0;
+  for (uint64_t k = 0; k < ncases; ++k) {
+    bkmesh::Dims d;
+    const bowshock_case_desc& c = cases[k];
+    if (!bkmesh::dims(meshes[k], d, m) || (long long)c.ni != d.ni || (long long)c.nj != d.nj) return BOWSHOCK_INVALID;
+    const bool base = meshes[k].wake == BOWSHOCK_WAKE_BASE;
+    if (base != (c.has_block != 0)) return BOWSHOCK_INVALID;
+    if (base && ((long long)c.block.i_end != d.i_end || (long long)c.block.j_end != d.j_end || (long long)c.block.j_sting != d.j_sting))
+      return BOWSHOCK_INVALID;
+    noff[k] = nodes, moff[k] = mets;
+    nodes += (size_t)(d.ni + 1) * (d.nj + 1);
+    mets += (size_t)BOWSHOCK_MESH_METRIC_WORDS(d.ni, d.nj);
+  }
+  std::vector<double> X(nodes), R(nodes), M(mets);
+  int rc = bkmesh::mesh_batch(ncases, meshes, device, X.data(), R.data(), M.data(), nullptr, m);
+  if (rc) return rc;
+  std::vector<bowshock_case_desc> ds(cases, cases + ncases);
+  std::vector<const double*> met(ncases);
+  for (uint64_t k = 0; k < ncases; ++k) {
+    ds[k].x = X.data() + noff[k], ds[k].r = R.data() + noff[k];
+    met[k] = M.data() + moff[k];
+  }
+  rc = arena_build(ncases, ds.data(), &met, device, out);
+  if (rc == BOWSHOCK_OK) {  // the descriptors keep pointing at the caller's (possibly null) node arrays, as passed
+    for (uint64_t k = 0; k < ncases; ++k) (*out)->descs[k].x = cases[k].x, (*out)->descs[k].r = cases[k].r;
+  }
+  return rc;
 }
 
 int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out) {

@@ -132,9 +132,8 @@ struct StingGrid {  // body_grid.rs:112-131
   double dx_tip, dr_wall;
 };
 
-// body_grid.rs:360-452
-inline bool base_domain_grid(const Body& bb, const BaseGrid& p, size_t& ni, size_t& nj, std::vector<double>& x, std::vector<double>& r,
-                             size_t blk[3], std::string& err) {
+// The argument checks of base_domain_grid (body_grid.rs:360-375), shared with the device mesher
+inline bool base_grid_check(const Body& bb, const BaseGrid& p, std::string& err) {
   double ln = bb.nose_length();
   if (!(p.n_up >= 1 && p.n_nose >= 2 && p.n_wake >= 2 && p.n_gap >= 2 && p.nj_out >= 1)) return err = "cell counts", false;
   if (bb.seg_len.empty() || p.n_seg.size() != bb.seg_len.size()) return err = "n_seg needs one entry per body segment", false;
@@ -144,6 +143,14 @@ inline bool base_domain_grid(const Body& bb, const BaseGrid& p, size_t& ni, size
   if (bb.sting_radius >= bb.base_radius()) return err = "sting thicker than the base", false;
   if (!(ln > 0.0 && p.x_up > 0.0 && p.x_down > 0.0 && p.dx_tip > 0.0 && p.dr_wall > 0.0 && p.r_far > bb.base_radius()))
     return err = "x_up, x_down, dx_tip, dr_wall must be positive, r_far must exceed the base radius", false;
+  return true;
+}
+
+// body_grid.rs:360-452
+inline bool base_domain_grid(const Body& bb, const BaseGrid& p, size_t& ni, size_t& nj, std::vector<double>& x, std::vector<double>& r,
+                             size_t blk[3], std::string& err) {
+  double ln = bb.nose_length();
+  if (!base_grid_check(bb, p, err)) return false;
   std::vector<double> nose = two_sided_nodes(ln, p.n_nose, p.dx_tip);
   std::vector<double> xs, up = geometric_offsets(nose[1] - nose[0], p.x_up, p.n_up);
   for (size_t k = p.n_up; k >= 1; --k) xs.push_back(-up[k]);
@@ -197,9 +204,8 @@ inline bool base_domain_grid(const Body& bb, const BaseGrid& p, size_t& ni, size
   return true;
 }
 
-// body_grid.rs:160-231
-inline bool large_domain_grid(const Body& bb, const StingGrid& p, size_t& ni, size_t& nj, std::vector<double>& x, std::vector<double>& r,
-                              std::string& err) {
+// The argument checks of large_domain_grid (body_grid.rs:160-175), shared with the device mesher
+inline bool large_grid_check(const Body& bb, const StingGrid& p, std::string& err) {
   size_t nseg = bb.seg_len.size();
   double ln = bb.nose_length();
   if (!(p.x_up > 0.0 && p.x_down > bb.aft_length() && nseg >= 1 && ln > 0.0 && p.dx_tip > 0.0))
@@ -208,6 +214,15 @@ inline bool large_domain_grid(const Body& bb, const StingGrid& p, size_t& ni, si
   for (size_t k = 0; k < nseg; ++k)
     if (!(bb.seg_len[k] > 0.0) || p.n_seg[k] < 1) return err = "segments need a positive length and >= 1 cell", false;
   if (!(p.n_up >= 1 && p.n_nose >= 2 && p.n_ext >= 1 && p.nj >= 1 && p.dr_wall > 0.0 && p.r_far > 0.0)) return err = "cell counts", false;
+  return true;
+}
+
+// body_grid.rs:160-231
+inline bool large_domain_grid(const Body& bb, const StingGrid& p, size_t& ni, size_t& nj, std::vector<double>& x, std::vector<double>& r,
+                              std::string& err) {
+  size_t nseg = bb.seg_len.size();
+  double ln = bb.nose_length();
+  if (!large_grid_check(bb, p, err)) return false;
   std::vector<double> nose = two_sided_nodes(ln, p.n_nose, p.dx_tip);
   double d_tip = nose[1] - nose[0], d_sh = nose[p.n_nose] - nose[p.n_nose - 1];
   std::vector<double> xs, up = geometric_offsets(d_tip, p.x_up, p.n_up);

@@ -262,6 +262,29 @@ int bowshock_base_domain_grid(const bowshock_body* body, const bowshock_base_gri
 /* body_grid.rs:213-231 `large_domain_grid` (sting wake). Call with x = r = NULL to get ni, nj. */
 int bowshock_large_domain_grid(const bowshock_body* body, const bowshock_sting_grid* p, uint64_t* ni, uint64_t* nj, double* x, double* r);
 
+/* ---------------------------------------------------------------------------------------------- device mesher
+ * No counterpart in the reference (its mesher is host code, one case at a time): the grids of many cases built on the
+ * GPU — the 1D node distributions with their bisections (one warp per case), the nodes (a thread per node) and the FP64
+ * metrics of every face and cell (a thread per face or cell, grid.rs:65-119). The arithmetic follows the host mesher
+ * above operation by operation without multiply-add contraction; nodes and metrics differ from it only where the
+ * device's tanh, tan, pow, acos, sin and hypot round differently from the host C library (an ulp or two). */
+typedef struct {
+  int32_t wake;               /* BOWSHOCK_WAKE_BASE: base_domain_grid; BOWSHOCK_WAKE_STING: large_domain_grid */
+  bowshock_body body;
+  bowshock_base_grid base;    /* read when wake = BOWSHOCK_WAKE_BASE */
+  bowshock_sting_grid sting;  /* read when wake = BOWSHOCK_WAKE_STING */
+} bowshock_mesh_request;
+/* FP64 words of one case's metrics: i faces [nx, nr, len, r_mid] ((ni+1) nj each), j faces [nx, nr, len, r_mid]
+ * (ni (nj+1) each), cells [area, volume per radian, xc, rc] (ni nj each), every array row-major (j, i). */
+#define BOWSHOCK_MESH_METRIC_WORDS(ni, nj) (4 * (((ni) + 1) * (nj) + (ni) * ((nj) + 1) + (ni) * (nj)))
+/* ni, nj and the solid block (zero for a sting grid) of a request, after the host mesher's argument checks (INVALID
+ * where it would refuse the request); host arithmetic only. */
+int bowshock_mesh_dims(const bowshock_mesh_request* q, uint64_t* ni, uint64_t* nj, bowshock_block* block);
+/* The grids of n requests built on the device: x, r (host, case k's (ni+1)(nj+1) nodes after those of the cases before
+ * it) and, if metrics is not NULL, BOWSHOCK_MESH_METRIC_WORDS per case in the same order; device_ms (may be NULL): the
+ * device time of the three launches. INVALID for a refused request or a non-positive cell area. */
+int bowshock_mesh_batch(uint64_t n, const bowshock_mesh_request* q, int device, double* x, double* r, double* metrics, double* device_ms);
+
 /* ---------------------------------------------------------------------------------------------- batched case arena
  * No counterpart in the reference (it runs Mach points one at a time, analysis.rs:727-797): many cases with uneven grids
  * packed into one structure-of-arrays arena, every kernel launched once per iteration for all of them, per-case
@@ -289,6 +312,11 @@ int bowshock_case_wall_distance(const bowshock_case_desc* d, double* out);
 
 typedef struct bowshock_arena bowshock_arena;
 int bowshock_arena_create(uint64_t ncases, const bowshock_case_desc* cases, int device, bowshock_arena** out);
+/* bowshock_arena_create with every case's grid built on the device from meshes[k] (body -> nodes -> metrics, the device
+ * mesher above) instead of from host nodes: cases[k].x and .r are ignored (may be NULL), cases[k].ni, .nj and the block
+ * must be those of meshes[k] (bowshock_mesh_dims). */
+int bowshock_arena_create_meshed(uint64_t ncases, const bowshock_case_desc* cases, const bowshock_mesh_request* meshes, int device,
+                                 bowshock_arena** out);
 void bowshock_arena_destroy(bowshock_arena* a);
 const char* bowshock_arena_last_error(const bowshock_arena* a);
 /* cells of all cases */

@@ -107,3 +107,19 @@ def test_limit_cycle_cd_comparison():
     ours = dict(stop_reason="mean stationary", cd_window=0.3200, cd_total=0.3210)
     assert abs(bench.cd_error(ours, dict(stop="mean stationary", cd_window=0.3199, cd_total=0.3190)) - 1e-4) < 1e-12
     assert abs(bench.cd_error(ours, dict(stop="CD stationary", cd_window=0.3199, cd_total=0.3190)) - 2e-3) < 1e-12
+
+
+def test_mesh_dims_match_the_host_mesher():
+    """bowshock_mesh_dims (the device mesher's sizes, from the cell counts) against the host mesher's grids, for every
+    sweep case; and the host mesher's argument checks refuse the same requests."""
+    from bowshock_b200 import BowshockError
+    from bowshock_b200.sweep import sweep_cases
+    for c in sweep_cases():
+        ni, nj, x, r, blk = c.grid()
+        assert c.mesh_dims() == (ni, nj, blk)
+        assert (ni, nj) == c.cells()
+    bad = sweep_cases()[0]
+    bad.grid_sting.n_nose = 1
+    bad.grid_base.n_nose = 1
+    with pytest.raises(BowshockError):
+        bad.mesh_dims()

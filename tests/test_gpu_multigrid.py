@@ -54,18 +54,16 @@ def test_implicit_multigrid_reaches_the_single_grid_fixed_point(mach, relax, sca
 
 def test_config0_implicit_multigrid_stays_bounded():
     """Config 0 (Euler, 128 x 64 -> 64 x 32 -> 32 x 16, M 1.5, base wake): the separated base flow keeps the single grid
-    in a limit cycle (residual about 6e-4); three levels with the coarse-grid correction under-relaxed by 0.5 stay
-    bounded (no divergence, residual below 1e-2 after 400 cycles) and give CD within 1e-3 of the FP64 oracle's converged
-    run (tests/golden/configs_oracle.json)."""
+    in a limit cycle (residual about 6e-4 after the first 300 iterations); three levels with the coarse-grid correction
+    under-relaxed by 0.5 do not converge either but stay bounded: over 1,000 cycles no divergence, and the last 500
+    below 1e-2 (about 1.7e-3 measured). Run to the stop rules they end at the iteration cap with CD 6.5e-4 from the
+    oracle's converged run, so the multigrid option is not offered for base-wake flows."""
     import bowshock_b200 as bk
     from tests.golden.configs import config0_case
-    ref = json.load(open(os.path.join(HERE, "golden", "configs_oracle.json")))["config0"]
     c = config0_case()
     s = c.build_solver(0)
     s.set_scheme(bk.solver.MgParams(levels=3, pre=1, post=1, implicit=c.numerics.scheme, relax=0.5))
-    r = s.run_to_stop(c.body, c.numerics, c.wake)
-    print("config0 multigrid", r["iters"], r["stop_reason"], r["cd_total"] - ref["cd_total"])
-    assert r["stop_reason"] != "non-finite residual"
-    h = np.asarray(s.run(50))
-    assert np.all(np.isfinite(h)) and h.max() < 1e-2
-    assert abs(r["cd_total"] - ref["cd_total"]) <= 1e-3
+    h = np.concatenate([np.asarray(s.run(100)) for _ in range(10)])
+    print("config0 multigrid residual every 100 cycles:", " ".join(f"{v:.1e}" for v in h[::100]))
+    assert np.all(np.isfinite(h))
+    assert h[500:].max() < 1e-2

@@ -158,8 +158,10 @@ def test_implicit_conv_matches_torch_fp32(batch, h, w, c, up, n):
 
 
 def test_implicit_conv_network_equals_im2col():
-    """The network's forward outputs and gradients are the same, bit for bit, with its convolutions as implicit GEMMs
-    and through im2col matrices: both feed the tensor cores the same K blocks in the same order."""
+    """The network's forward outputs are the same, bit for bit, with its convolutions as implicit GEMMs and through
+    im2col matrices (both feed the tensor cores the same K blocks in the same order); the loss and the weight gradients
+    to the order of their FP32 atomic sums (the loss reduction and the split-K weight-gradient GEMMs add their partial
+    sums in whatever order the blocks finish, in either form)."""
     net, L, n, pr, x, rng = _net_and_oracle()
     t = rng.standard_normal((x.shape[0], no.NET_CELLS, no.NET_OUT)).astype(np.float32) * 0.5
     outs = []
@@ -170,8 +172,11 @@ def test_implicit_conv_network_equals_im2col():
         outs.append((y, loss, g))
     (y1, l1, g1), (y0, l0, g0) = outs
     assert np.array_equal(y1, y0)
-    assert l1 == l0
-    assert np.array_equal(g1, g0)
+    assert abs(l1 - l0) <= 1e-6 * abs(l0)
+    for l in L:
+        sl = slice(l["woff"], l["boff"] + l["cout"])
+        e = np.linalg.norm(g1[sl] - g0[sl]) / (np.linalg.norm(g0[sl]) + 1e-30)
+        assert e < 1e-5, f"layer gradient differs by {e:.2e}"
 
 
 def test_net_forward_repeatable():
