@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_conv(const __grid_constant__ CU
   uint64_t* done = empty + STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   __shared__ int s_abort;
-  __shared__ int rb[BM], ry[BM], rx[BM];  // image, row and column of each output pixel of the tile (rb < 0: past M)
+  __shared__ int s_off[9][BM];  // element offset of tile row r's source pixel under tap t in cx (-1: outside the image, past M)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int nkb_total = (g.K + BK - 1) / BK;
@@ -271,12 +271,12 @@ __global__ void __launch_bounds__(128, 1) k_gemm_conv(const __grid_constant__ CU
   }
   {
     const int m = threadIdx.x, p = m0 + m;  // 128 threads, one row each
-    if (p < g.M) {
-      rx[m] = p % W;
-      ry[m] = (p / W) % H;
-      rb[m] = p / (W * H);
-    } else {
-      rb[m] = -1, ry[m] = 0, rx[m] = 0;
+    int b = -1, y = 0, x = 0;
+    if (p < g.M) x = p % W, y = (p / W) % H, b = p / (W * H);
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+      s_off[t][m] = (b >= 0 && yy >= 0 && yy < H && xx >= 0 && xx < W) ? ((b * g.cHin + (yy >> g.cup)) * g.cWin + (xx >> g.cup)) * g.cC : -1;
     }
   }
   if (warp == 0) {
@@ -315,15 +315,14 @@ __global__ void __launch_bounds__(128, 1) k_gemm_conv(const __grid_constant__ CU
         break;
       }
       const int k0 = (kb0 + i) * BK, tap = k0 / g.cC, c0 = k0 % g.cC;
-      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-      const uint32_t base = smem_u32(sa + s * A_BYTES);
-#pragma unroll 4
+      const int* offs = s_off[tap];
+      // rows r0 + 8 t share r & 7, so this thread's chunk lands at the same swizzled position in each of its rows
+      const uint32_t dst = smem_u32(sa + s * A_BYTES) + (uint32_t)(r0 * 128 + ((part ^ (r0 & 7)) << 4));
+      const bf16* cxp = g.cx + c0 + part * 8;
+#pragma unroll
       for (int t = 0; t < BM / 8; ++t) {
-        const int r = r0 + 8 * t;
-        const int b = rb[r], yy = ry[r] + dy, xx = rx[r] + dx;
-        const bool in = b >= 0 && yy >= 0 && yy < H && xx >= 0 && xx < W;
-        const bf16* src = in ? g.cx + ((((long long)b * g.cHin + (yy >> g.cup)) * g.cWin + (xx >> g.cup)) * g.cC + c0 + part * 8) : g.cx;
-        cp_async16_zfill(base + (uint32_t)(r * 128 + ((part ^ (r & 7)) << 4)), src, in ? 16u : 0u);
+        const int o = offs[r0 + 8 * t];
+        cp_async16_zfill(dst + (uint32_t)(t * 8 * 128), o >= 0 ? cxp + o : g.cx, o >= 0 ? 16u : 0u);
       }
       asm volatile("cp.async.commit_group;" ::: "memory");
       ++issued;

@@ -172,7 +172,7 @@ def test_implicit_conv_network_equals_im2col():
         outs.append((y, loss, g))
     (y1, l1, g1), (y0, l0, g0) = outs
     assert np.array_equal(y1, y0)
-    assert abs(l1 - l0) <= 1e-6 * abs(l0)
+    assert abs(l1 - l0) <= 1e-5 * abs(l0)  # 98,304 FP32 terms added atomically in any order
     for l in L:
         sl = slice(l["woff"], l["boff"] + l["cout"])
         e = np.linalg.norm(g1[sl] - g0[sl]) / (np.linalg.norm(g0[sl]) + 1e-30)
