@@ -186,8 +186,8 @@ SIGNATURES = {
     "bowshock_net_reset_optimizer": (_I, [_P]),
     "bowshock_net_train": (_I, [_P, _U, _U, _D, _U, _dp]),
     "bowshock_net_last_train_ms": (_I, [_P, _dp]),
-    "bowshock_net_set_implicit_conv": (_I, [_P, _I]),
-    "bowshock_conv3x3_bf16": (_I, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P]),
+    "bowshock_net_set_conv_mode": (_I, [_P, _I]),
+    "bowshock_conv3x3_bf16": (_I, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P, C.c_int64, _P, C.c_int32, _P, _P]),
     "bowshock_gemm_bf16": (_I, [_P, C.c_int64, _P, C.c_int64, _P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P, _P]),
 }
 

@@ -34,6 +34,7 @@ typedef __nv_bfloat16 bf16;
 using bktma::mbar_expect_tx;
 using bktma::mbar_init;
 using bktma::mbar_wait;
+using bktma::tma_load_4d;
 using bktma::smem_u32;
 using bktma::tma_load_2d;
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -115,7 +116,13 @@ __host__ __device__ constexpr int gemm_smem_bytes() {
 // D[M, N] = A[M, K] B[N, K]^T (A and B row-major BF16, K contiguous), one 128 x BN tile per CTA, the K blocks of
 // blockIdx.z's split. Warp 0 lane 0 loads (TMA), warp 1 lane 0 issues the MMAs, all four warps run the epilogue (thread t
 // owns accumulator row t: TMEM lane t).
-template <int BN>
+// CONV: A is the implicit im2col of a 3x3 'same' convolution of the NHWC activations cx [cB, cHin, cWin, cC] (cC a
+// multiple of 64, no upsampling), through a 4D tensor map over (C, W, H, B) whose box is 64 channels of 128 whole output
+// pixels (cWin x R rows x NB images): K block kb is tap kb * 64 / cC, channels (kb * 64) % cC, and its A tile is that box
+// loaded at the tile's first pixel shifted by the tap (dx, dy); the rows and columns the shift moves outside the image
+// read zeros, which is the convolution's padding. A tile of 128 output pixels is 128 / cWin whole rows of one image (or
+// whole images), so the box's smem rows are the tile's rows in order, in the 128-byte-swizzled layout the MMA reads.
+template <int BN, bool CONV>
 __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -156,7 +163,12 @@ __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtenso
         break;
       }
       mbar_expect_tx(full + s, (uint32_t)(A_BYTES + B_BYTES));
-      tma_load_2d(sa + s * A_BYTES, &ta, full + s, (kb0 + i) * BK, m0);
+      if constexpr (CONV) {
+        const int hw = g.cHin * g.cWin, k0 = (kb0 + i) * BK, tap = k0 / g.cC;
+        tma_load_4d(sa + s * A_BYTES, &ta, full + s, k0 - tap * g.cC, tap % 3 - 1, (m0 % hw) / g.cWin + tap / 3 - 1, m0 / hw);
+      } else {
+        tma_load_2d(sa + s * A_BYTES, &ta, full + s, (kb0 + i) * BK, m0);
+      }
       tma_load_2d(sb + s * B_BYTES, &tb, full + s, (kb0 + i) * BK, n0);
     }
   } else if (nkb > 0 && warp == 1 && lane == 0) {  // MMA issuer
@@ -604,11 +616,11 @@ static bool make_map(CUtensorMap* m, const void* p, long long rows, long long co
   return true;
 }
 
-template <int BN>
+template <int BN, bool CONV = false>
 static cudaError_t launch_gemm_bn(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, dim3 grid, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>());
+  cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>());
   if (e != cudaSuccess) return e;
-  k_gemm<BN><<<grid, 128, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
+  k_gemm<BN, CONV><<<grid, 128, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
   return cudaGetLastError();
 }
 
@@ -692,7 +704,69 @@ static int conv_gemm(const bf16* x, int B, int Hin, int Win, int C, int up, cons
   return 0;
 }
 
+// Whether the TMA-fed convolution (k_gemm<BN, true>) takes an H x W image: its 128-pixel tiles must be whole rows of one
+// image (H W a multiple of 128) or whole images (128 a multiple of H W), W dividing 128.
+static bool conv_tma_fits(int H, int W) { return W >= 1 && W <= 128 && 128 % W == 0 && ((H * W) % 128 == 0 || 128 % (H * W) == 0); }
+
+// The same convolution as conv_gemm (no upsampling) with both operands loaded by TMA: A through a 4D tensor map over the
+// NHWC activations x [B, H, W, C] (box: 64 channels x W x R rows x NB images = 128 pixels, 128-byte swizzle, zeros
+// outside), one box per K block at the tile's first pixel shifted by the tap.
+static int conv_gemm_tma(const bf16* x, int B, int H, int W, int C, const bf16* w, long long ldw, int N, GemmArgs g, cudaStream_t st, std::string& err) {
+  if (C % 64 || !conv_tma_fits(H, W)) {
+    err = "the TMA convolution needs a multiple of 64 channels and 128-pixel tiles of whole rows or images";
+    return BOWSHOCK_INVALID;
+  }
+  if (!get_encode(err)) return BOWSHOCK_CUDA_ERROR;
+  if (((uintptr_t)x & 15)) {
+    err = "convolution input not 16-byte aligned";
+    return BOWSHOCK_INVALID;
+  }
+  const int bn = pick_bn(N);
+  const int R = std::min(H, 128 / W), NB = 128 / (W * R);
+  CUtensorMap ta, tb;
+  cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  cuuint32_t box[4] = {(cuuint32_t)BK, (cuuint32_t)W, (cuuint32_t)R, (cuuint32_t)NB};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = g_encode(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    err = "cuTensorMapEncodeTiled (4D activations) failed (" + std::to_string((int)r) + ")";
+    return BOWSHOCK_INVALID;
+  }
+  if (!make_map(&tb, w, N, 9LL * C, ldw, bn, err)) return BOWSHOCK_INVALID;
+  const long long M = (long long)B * H * W;
+  g.M = (int)M, g.N = N, g.K = 9 * C, g.kb_per_split = (9 * C) / BK;
+  g.cx = x, g.cB = B, g.cHin = H, g.cWin = W, g.cC = C, g.cup = 0;
+  dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)((N + bn - 1) / bn), 1);
+  cudaError_t e;
+  switch (bn) {
+    case 16: e = launch_gemm_bn<16, true>(ta, tb, g, grid, st); break;
+    case 32: e = launch_gemm_bn<32, true>(ta, tb, g, grid, st); break;
+    case 64: e = launch_gemm_bn<64, true>(ta, tb, g, grid, st); break;
+    case 128: e = launch_gemm_bn<128, true>(ta, tb, g, grid, st); break;
+    default: e = launch_gemm_bn<256, true>(ta, tb, g, grid, st); break;
+  }
+  if (e != cudaSuccess) {
+    err = std::string("convolution GEMM launch: ") + cudaGetErrorString(e);
+    return BOWSHOCK_CUDA_ERROR;
+  }
+  return 0;
+}
+
 static int grid_for(long long n, int threads = 256) { return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148 * 16)); }
+
+// y [B, 2 Hin, 2 Win, C] = x [B, Hin, Win, C] repeated 2 x 2 (nearest upsampling), 8 channels (16 bytes) per thread step
+__global__ void k_upsample2x(const bf16* __restrict__ x, int B, int Hin, int Win, int C, bf16* __restrict__ y) {
+  const int H = Hin * 2, W = Win * 2, c8 = C >> 3;
+  const long long total = (long long)B * H * W * c8;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int cc = (int)(t % c8);
+    const long long p = t / c8;
+    const int xo = (int)(p % W), yo = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    reinterpret_cast<uint4*>(y)[p * c8 + cc] = reinterpret_cast<const uint4*>(x)[(((long long)b * Hin + (yo >> 1)) * Win + (xo >> 1)) * c8 + cc];
+  }
+}
 
 // ---------------------------------------------------------------------------------------------------- the network
 struct Layer {
@@ -731,7 +805,7 @@ struct Net {
   int* idx = nullptr;
   long long idx_cap = 0;
   double last_ms = 0.0;
-  bool implicit_conv = true;  // 3x3 convolutions of 64k channels as implicit GEMMs (else im2col + GEMM)
+  int conv_mode = 2;  // 3x3 convolutions of 64k channels: 0 im2col + GEMM, 1 implicit GEMM (cp.async gather), 2 implicit GEMM (TMA boxes)
 
   ~Net() {
     for (void* p : {(void*)w, (void*)gw, (void*)m1, (void*)m2, (void*)wb, (void*)x, (void*)out, (void*)col, (void*)colT, (void*)gT, (void*)wt,
@@ -865,7 +939,17 @@ struct Net {
       } else {
         g.mode = EPI_BIAS_F32, g.d = out, g.ldd = l.cout;
       }
-      if (!l.fc && implicit_conv && l.cin % 64 == 0) {  // the convolution as an implicit GEMM: no im2col matrix
+      if (!l.fc && conv_mode == 2 && l.cin % 64 == 0 && conv_tma_fits(l.H, l.W)) {  // implicit GEMM, A tiles by TMA
+        const bf16* src = in;
+        if (l.up) {  // the TMA boxes read the upsampled activations (the im2col buffer holds them)
+          k_upsample2x<<<grid_for((long long)B * l.H * l.W * (l.cin / 8)), 256, 0, stream>>>(in, B, l.H >> 1, l.W >> 1, l.cin, col);
+          src = col;
+        }
+        if ((rc = conv_gemm_tma(src, B, l.H, l.W, l.cin, wb + l.woff, l.kin, l.cout, g, stream, err))) return rc;
+        in = act[k];
+        continue;
+      }
+      if (!l.fc && conv_mode >= 1 && l.cin % 64 == 0) {  // implicit GEMM, A tiles gathered by cp.async
         if ((rc = conv_gemm(in, B, l.H >> l.up, l.W >> l.up, l.cin, l.up, wb + l.woff, l.kin, l.cout, g, stream, err))) return rc;
         in = act[k];
         continue;
@@ -929,7 +1013,9 @@ struct Net {
         k_grad_prev<<<grid_for(r * l.cin), 256, 0, stream>>>(dx, B, 1, 1, l.cin, 0, xin, BOWSHOCK_NET_SLOPE, gnext);
       } else {
         k_flip_weights<<<grid_for((long long)l.cin * 9 * l.cout), 256, 0, stream>>>(wb + l.woff, l.cin, l.cout, wt);
-        if (implicit_conv && l.cout % 64 == 0) {
+        if (conv_mode == 2 && l.cout % 64 == 0 && conv_tma_fits(l.H, l.W)) {
+          if ((rc = conv_gemm_tma(g, B, l.H, l.W, l.cout, wt, 9LL * l.cout, l.cin, gx, stream, err))) return rc;
+        } else if (conv_mode >= 1 && l.cout % 64 == 0) {
           if ((rc = conv_gemm(g, B, l.H, l.W, l.cout, 0, wt, 9LL * l.cout, l.cin, gx, stream, err))) return rc;
         } else {
           k_im2col<<<grid_for(r * 9 * (l.cout / 8)), 256, 0, stream>>>(g, B, l.H, l.W, l.cout, 0, col);
@@ -1170,18 +1256,23 @@ int bowshock_net_last_train_ms(const bowshock_net* h, double* ms) {
   return BOWSHOCK_OK;
 }
 
-int bowshock_net_set_implicit_conv(bowshock_net* h, int on) {
-  if (!h) return BOWSHOCK_INVALID;
-  h->n.implicit_conv = on != 0;
+int bowshock_net_set_conv_mode(bowshock_net* h, int mode) {
+  if (!h || mode < 0 || mode > 2) return BOWSHOCK_INVALID;
+  h->n.conv_mode = mode;
   return BOWSHOCK_OK;
 }
 
 int bowshock_conv3x3_bf16(const void* x, int64_t batch, int64_t h_in, int64_t w_in, int64_t c, int64_t up, const void* w, int64_t n, float* d,
-                          void* stream, int* err_flag) {
-  if (!x || !w || !d || !err_flag || batch <= 0 || h_in <= 0 || w_in <= 0 || c <= 0 || n <= 0 || (up != 0 && up != 1)) return BOWSHOCK_INVALID;
+                          int32_t mode, void* stream, int* err_flag) {
+  if (!x || !w || !d || !err_flag || batch <= 0 || h_in <= 0 || w_in <= 0 || c <= 0 || n <= 0 || (up != 0 && up != 1) || (mode != 1 && mode != 2) ||
+      (mode == 2 && up))
+    return BOWSHOCK_INVALID;
   std::string err;
   bknet::GemmArgs g{};
   g.mode = bknet::EPI_F32, g.d = d, g.ldd = n, g.err = err_flag;
+  if (mode == 2)
+    return bknet::conv_gemm_tma(reinterpret_cast<const bknet::bf16*>(x), (int)batch, (int)h_in, (int)w_in, (int)c,
+                                reinterpret_cast<const bknet::bf16*>(w), 9 * c, (int)n, g, reinterpret_cast<cudaStream_t>(stream), err);
   return bknet::conv_gemm(reinterpret_cast<const bknet::bf16*>(x), (int)batch, (int)h_in, (int)w_in, (int)c, (int)up,
                           reinterpret_cast<const bknet::bf16*>(w), 9 * c, (int)n, g, reinterpret_cast<cudaStream_t>(stream), err);
 }

@@ -56,6 +56,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// 4D tiled load of the box at (c0, c1, c2, c3) (c0 innermost, in elements; the outer coordinates may be negative or past
+// the extent, which reads zeros) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
+
 // cuTensorMapEncodeTiled of the installed driver, or null with a message
 inline PFN_cuTensorMapEncodeTiled_v12000 encoder(std::string& err) {
   static std::mutex mu;

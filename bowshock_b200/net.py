@@ -92,9 +92,12 @@ class Net:
         self._check(_ffi.load().bowshock_net_train(self._h, int(steps), int(batch), float(lr), int(seed), _ffi.dptr(loss)))
         return loss
 
-    def set_implicit_conv(self, on: bool):
-        """3x3 convolutions as implicit GEMMs (True, the default) or through an im2col matrix (False)."""
-        self._check(_ffi.load().bowshock_net_set_implicit_conv(self._h, int(bool(on))))
+    CONV_IM2COL, CONV_GATHER, CONV_TMA = 0, 1, 2
+
+    def set_conv_mode(self, mode: int):
+        """3x3 convolutions as implicit GEMMs fed by TMA boxes (CONV_TMA, the default), as implicit GEMMs gathered by
+        cp.async (CONV_GATHER), or through an im2col matrix (CONV_IM2COL)."""
+        self._check(_ffi.load().bowshock_net_set_conv_mode(self._h, int(mode)))
 
     def last_train_ms(self) -> float:
         ms = C.c_double()

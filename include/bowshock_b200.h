@@ -482,16 +482,19 @@ int bowshock_net_reset_optimizer(bowshock_net* n);
 int bowshock_net_train(bowshock_net* n, uint64_t steps, uint64_t batch, double lr, uint64_t seed, double* loss);
 /* device time of the last bowshock_net_train (CUDA events), milliseconds */
 int bowshock_net_last_train_ms(const bowshock_net* n, double* ms);
-/* 1 (the default): the 3x3 convolutions with a multiple of 64 input channels, forward and input gradient, run as
- * implicit GEMMs (the A tiles gathered from the NHWC activations by cp.async into the swizzled layout, no im2col
- * matrix); 0: im2col matrix + the TMA-fed GEMM. The two give the same sums in the same order. */
-int bowshock_net_set_implicit_conv(bowshock_net* n, int on);
+/* How the network runs its 3x3 convolutions with a multiple of 64 input channels (forward and input gradient): 2 (the
+ * default) implicit GEMMs whose A tiles are 4D TMA boxes of the NHWC activations shifted by the tap (zeros outside the
+ * image; an upsampling layer's input is upsampled into a buffer first), 1 implicit GEMMs whose A tiles are gathered by
+ * cp.async into the swizzled layout, 0 an im2col matrix + the TMA-fed GEMM. All three feed the tensor cores the same K
+ * blocks in the same order (the same sums). */
+int bowshock_net_set_conv_mode(bowshock_net* n, int mode);
 /* The network's implicit-GEMM convolution on caller-owned device memory: d[p][o] (FP32, p over batch x H x W output
  * pixels, H = h_in << up, W = w_in << up) = sum over the 3x3 taps and c channels of x[pixel shifted by the tap][ch]
  * w[o][tap * c + ch], x NHWC BF16 [batch][h_in][w_in][c] (c a multiple of 64, read through a nearest 2x upsampling when
- * up = 1, zeros outside the image), w BF16 [n][9 c]. */
+ * up = 1, zeros outside the image), w BF16 [n][9 c]. mode 1: A gathered by cp.async; mode 2: A by TMA boxes (up = 0, and
+ * W dividing 128 with H W a multiple or a divisor of 128). */
 int bowshock_conv3x3_bf16(const void* x, int64_t batch, int64_t h_in, int64_t w_in, int64_t c, int64_t up, const void* w, int64_t n, float* d,
-                          void* stream, int* err_flag);
+                          int32_t mode, void* stream, int* err_flag);
 /* The network's tensor-core GEMM on caller-owned device memory: d[m][n] = sum_k a[m][k] b[n][k], a and b BF16 row-major
  * (lda, ldb multiples of 8 elements, 16-byte aligned), d FP32 (ldd >= n); splits > 1 adds K slices atomically into d
  * (zeroed by the caller). stream: a cudaStream_t or NULL; err_flag: a device int set to 1 if a bounded wait gave up. */

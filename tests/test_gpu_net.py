@@ -129,21 +129,28 @@ def test_net_training_lowers_the_loss():
     assert net.last_train_ms() > 0
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("batch,h,w,c,up,n", [(2, 4, 8, 128, 0, 128), (3, 8, 16, 128, 1, 64), (2, 16, 32, 64, 1, 64),
-                                              (1, 32, 64, 64, 0, 16), (5, 7, 9, 64, 0, 200), (4, 32, 64, 64, 0, 64)])
-def test_implicit_conv_matches_torch_fp32(batch, h, w, c, up, n):
-    """The implicit-GEMM convolution (A gathered by cp.async into the swizzled tile, no im2col matrix) against torch's
-    FP32 convolution of the same BF16 input (nearest 2x upsampled when up = 1) and weights, zero padding 1."""
+                                              (1, 32, 64, 64, 0, 16), (5, 7, 9, 64, 0, 200), (4, 32, 64, 64, 0, 64),
+                                              (3, 4, 8, 64, 0, 64), (2, 8, 16, 64, 0, 256)])
+def test_implicit_conv_matches_torch_fp32(batch, h, w, c, up, n, mode):
+    """The implicit-GEMM convolution (no im2col matrix; mode 1: A gathered by cp.async into the swizzled tile, mode 2: A
+    as 4D TMA boxes of the activations shifted by the tap) against torch's FP32 convolution of the same BF16 input
+    (nearest 2x upsampled when up = 1) and weights, zero padding 1. Mode 2 takes no upsampling and needs 128-pixel
+    tiles of whole rows or images (odd-batch and ragged-image shapes included where they fit)."""
     import torch
     from bowshock_b200 import _ffi
+    H, W = h << up, w << up
+    fits = (128 % W == 0) and ((H * W) % 128 == 0 or 128 % (H * W) == 0)
+    if mode == 2 and (up or not fits):
+        pytest.skip("the TMA form takes no upsampling and needs whole-row tiles")
     g = torch.Generator(device="cuda").manual_seed(batch * 31 + h * 7 + c + n + up)
     x = torch.randn((batch, h, w, c), generator=g, device="cuda").to(torch.bfloat16)
     wt = torch.randn((n, 3, 3, c), generator=g, device="cuda").to(torch.bfloat16)
-    H, W = h << up, w << up
     d = torch.zeros((batch * H * W, n), dtype=torch.float32, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     rc = _ffi.load().bowshock_conv3x3_bf16(C.c_void_p(x.data_ptr()), batch, h, w, c, up, C.c_void_p(wt.data_ptr()), n,
-                                          C.c_void_p(d.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                          C.c_void_p(d.data_ptr()), mode, C.c_void_p(torch.cuda.current_stream().cuda_stream),
                                           C.c_void_p(err.data_ptr()))
     assert rc == 0
     torch.cuda.synchronize()
@@ -154,29 +161,31 @@ def test_implicit_conv_matches_torch_fp32(batch, h, w, c, up, n):
     ref = torch.nn.functional.conv2d(xi, wt.float().permute(0, 3, 1, 2), padding=1).permute(0, 2, 3, 1).reshape(-1, n)
     scale = ref.abs().amax(dim=1, keepdim=True) + 1e-6
     e = ((d - ref).abs() / scale).max().item()
-    assert e < 1e-4, f"conv {batch}x{h}x{w}x{c} up {up} -> {n}: max rel err {e:.2e}"
+    assert e < 1e-4, f"conv {batch}x{h}x{w}x{c} up {up} -> {n} mode {mode}: max rel err {e:.2e}"
 
 
 def test_implicit_conv_network_equals_im2col():
-    """The network's forward outputs are the same, bit for bit, with its convolutions as implicit GEMMs and through
-    im2col matrices (both feed the tensor cores the same K blocks in the same order); the loss and the weight gradients
-    to the order of their FP32 atomic sums (the loss reduction and the split-K weight-gradient GEMMs add their partial
-    sums in whatever order the blocks finish, in either form)."""
+    """The network's forward outputs are the same, bit for bit, with its convolutions as TMA-fed implicit GEMMs, as
+    gathered implicit GEMMs and through im2col matrices (all three feed the tensor cores the same K blocks in the same
+    order); the loss and the weight gradients to the order of their FP32 atomic sums (the loss reduction and the split-K
+    weight-gradient GEMMs add their partial sums in whatever order the blocks finish, in every form)."""
+    from bowshock_b200.net import Net
     net, L, n, pr, x, rng = _net_and_oracle()
     t = rng.standard_normal((x.shape[0], no.NET_CELLS, no.NET_OUT)).astype(np.float32) * 0.5
     outs = []
-    for on in (True, False):
-        net.set_implicit_conv(on)
+    for mode in (Net.CONV_TMA, Net.CONV_GATHER, Net.CONV_IM2COL):
+        net.set_conv_mode(mode)
         y = net.forward(x)
         loss, g = net.gradients(x, t)
         outs.append((y, loss, g))
-    (y1, l1, g1), (y0, l0, g0) = outs
-    assert np.array_equal(y1, y0)
-    assert abs(l1 - l0) <= 1e-5 * abs(l0)  # 98,304 FP32 terms added atomically in any order
-    for l in L:
-        sl = slice(l["woff"], l["boff"] + l["cout"])
-        e = np.linalg.norm(g1[sl] - g0[sl]) / (np.linalg.norm(g0[sl]) + 1e-30)
-        assert e < 1e-5, f"layer gradient differs by {e:.2e}"
+    y0, l0, g0 = outs[-1]
+    for y1, l1, g1 in outs[:-1]:
+        assert np.array_equal(y1, y0)
+        assert abs(l1 - l0) <= 1e-5 * abs(l0)  # 98,304 FP32 terms added atomically in any order
+        for l in L:
+            sl = slice(l["woff"], l["boff"] + l["cout"])
+            e = np.linalg.norm(g1[sl] - g0[sl]) / (np.linalg.norm(g0[sl]) + 1e-30)
+            assert e < 1e-5, f"layer gradient differs by {e:.2e}"
 
 
 def test_net_forward_repeatable():
