@@ -36,3 +36,21 @@ def test_g3_oracle_run_matches_the_reference_digits():
     r = o.run_on(c, s)
     _check(dict(iters=r.iters, stop=r.stop_reason, cd_total=r.cd_total, cd_friction=r.cd_friction, cd_base=r.cd_base,
                 cp_base=r.cp_base, y_plus_max=r.y_plus_max))
+
+
+def test_limit_cycle_spread_fixture():
+    """The oracle is deterministic (the unperturbed run of the spread fixture is the census's run of the same case, to the
+    last bit), and a limit-cycle SST case's window-mean CD, the quantity the mean-stationary rule reports
+    (engine/run.rs:150-170), moves by more than the 1e-4 parity bar when only the free-stream Mach number moves by
+    1e-12 (tests/golden/limit_cycle_spread.json, made by make_limit_cycle_spread.py): the bar sits inside the case's
+    own rounding sensitivity."""
+    import json
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spread = json.load(open(os.path.join(here, "limit_cycle_spread.json")))["cases"]
+    census = json.load(open(os.path.join(here, "sweep_census.json")))["cases"]
+    for k, s in spread.items():
+        base = [r for r in s["runs"] if r["eps"] == 0.0][0]
+        assert base["cd_window"] == census[k]["cd_window"] and base["iters"] == census[k]["iters"]
+        cds = [r["cd_window"] if r["stop"] == "mean stationary" else r["cd_total"] for r in s["runs"]]
+        assert abs(s["spread"] - (max(cds) - min(cds))) < 1e-15
+    assert spread["9"]["spread"] > 1e-4
