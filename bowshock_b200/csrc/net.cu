@@ -122,7 +122,14 @@ __host__ __device__ constexpr int gemm_smem_bytes() {
 // loaded at the tile's first pixel shifted by the tap (dx, dy); the rows and columns the shift moves outside the image
 // read zeros, which is the convolution's padding. A tile of 128 output pixels is 128 / cWin whole rows of one image (or
 // whole images), so the box's smem rows are the tile's rows in order, in the 128-byte-swizzled layout the MMA reads.
-template <int BN, bool CONV>
+// WGRAD: the weight gradient of such a convolution, D[cout, 9 cin] = sum over pixels of g[p, cout] x[p shifted by the
+// tap, cin]: A is g transposed ([cout, pixels], 2D map), B a 4D map over xs [3 cin, B, H, W], the transposed
+// activations in three copies shifted along x by dx = -1, 0, +1 (zeros past the row ends; W = 64, so a K block is one
+// image row of 64 pixels and the box's x coordinate is always 0, aligned), whose box is 64 pixels x BN channels of copy
+// dx, loaded at the image row shifted by the tap's dy (zeros above and below the image). The tap is that of the tile's
+// columns (n0 / cin; BN divides cin).
+enum { GEMM_PLAIN = 0, GEMM_CONV = 1, GEMM_WGRAD = 2 };
+template <int BN, int KIND>
 __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -163,13 +170,18 @@ __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtenso
         break;
       }
       mbar_expect_tx(full + s, (uint32_t)(A_BYTES + B_BYTES));
-      if constexpr (CONV) {
+      if constexpr (KIND == GEMM_CONV) {
         const int hw = g.cHin * g.cWin, k0 = (kb0 + i) * BK, tap = k0 / g.cC;
         tma_load_4d(sa + s * A_BYTES, &ta, full + s, k0 - tap * g.cC, tap % 3 - 1, (m0 % hw) / g.cWin + tap / 3 - 1, m0 / hw);
       } else {
         tma_load_2d(sa + s * A_BYTES, &ta, full + s, (kb0 + i) * BK, m0);
       }
-      tma_load_2d(sb + s * B_BYTES, &tb, full + s, (kb0 + i) * BK, n0);
+      if constexpr (KIND == GEMM_WGRAD) {  // K block kb: image row kb % H of image kb / H
+        const int kb = kb0 + i, tap = n0 / g.cC;
+        tma_load_4d(sb + s * B_BYTES, &tb, full + s, 0, kb % g.cHin + tap / 3 - 1, kb / g.cHin, (tap % 3) * g.cC + n0 - tap * g.cC);
+      } else {
+        tma_load_2d(sb + s * B_BYTES, &tb, full + s, (kb0 + i) * BK, n0);
+      }
     }
   } else if (nkb > 0 && warp == 1 && lane == 0) {  // MMA issuer
     for (int i = 0; i < nkb; ++i) {
@@ -616,11 +628,11 @@ static bool make_map(CUtensorMap* m, const void* p, long long rows, long long co
   return true;
 }
 
-template <int BN, bool CONV = false>
+template <int BN, int KIND = GEMM_PLAIN>
 static cudaError_t launch_gemm_bn(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, dim3 grid, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>());
+  cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>());
   if (e != cudaSuccess) return e;
-  k_gemm<BN, CONV><<<grid, 128, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
+  k_gemm<BN, KIND><<<grid, 128, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
   return cudaGetLastError();
 }
 
@@ -741,14 +753,72 @@ static int conv_gemm_tma(const bf16* x, int B, int H, int W, int C, const bf16* 
   dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)((N + bn - 1) / bn), 1);
   cudaError_t e;
   switch (bn) {
-    case 16: e = launch_gemm_bn<16, true>(ta, tb, g, grid, st); break;
-    case 32: e = launch_gemm_bn<32, true>(ta, tb, g, grid, st); break;
-    case 64: e = launch_gemm_bn<64, true>(ta, tb, g, grid, st); break;
-    case 128: e = launch_gemm_bn<128, true>(ta, tb, g, grid, st); break;
-    default: e = launch_gemm_bn<256, true>(ta, tb, g, grid, st); break;
+    case 16: e = launch_gemm_bn<16, GEMM_CONV>(ta, tb, g, grid, st); break;
+    case 32: e = launch_gemm_bn<32, GEMM_CONV>(ta, tb, g, grid, st); break;
+    case 64: e = launch_gemm_bn<64, GEMM_CONV>(ta, tb, g, grid, st); break;
+    case 128: e = launch_gemm_bn<128, GEMM_CONV>(ta, tb, g, grid, st); break;
+    default: e = launch_gemm_bn<256, GEMM_CONV>(ta, tb, g, grid, st); break;
   }
   if (e != cudaSuccess) {
     err = std::string("convolution GEMM launch: ") + cudaGetErrorString(e);
+    return BOWSHOCK_CUDA_ERROR;
+  }
+  return 0;
+}
+
+// xs [3][C][r] = the transposed activations xT [C][r] (r = B H W pixels, W = 64) shifted along x: xs[s][c][p] =
+// xT[c][p + s - 1] where the pixel's x + s - 1 lies in [0, W), else 0
+__global__ void k_shift3(const bf16* __restrict__ xT, int C, long long r, int W, bf16* __restrict__ xs) {
+  const long long total = 3LL * C * r;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long p = t % r, q = t / r;
+    const int c = (int)(q % C), sft = (int)(q / C) - 1, x = (int)(p % W) + sft;
+    xs[t] = (x >= 0 && x < W) ? xT[(long long)c * r + p + sft] : __float2bfloat16_rn(0.f);
+  }
+}
+
+// The weight gradient of a 3x3 'same' convolution of images 64 pixels wide: dw [cout, 9 cin] (FP32, accumulated
+// atomically over split-K slices; zeroed by the caller) = sum over the B x H x 64 pixels of gT[o][p] x[p shifted by the
+// tap][c], gT the output gradient transposed ([cout, pixels], BF16) and xs the layer's input transposed and shifted
+// (k_shift3: [3][cin][B][H][64]). cin a multiple of 64.
+static int wgrad_gemm_tma(const bf16* gT, const bf16* xs, int B, int H, int cin, int cout, float* dw, int* err_flag, cudaStream_t st, std::string& err) {
+  constexpr int W = 64;
+  if (cin % 64) {
+    err = "the TMA weight gradient needs a multiple of 64 input channels";
+    return BOWSHOCK_INVALID;
+  }
+  if (!get_encode(err)) return BOWSHOCK_CUDA_ERROR;
+  const int bn = cin % 128 == 0 ? 128 : 64;
+  const long long r = (long long)B * H * W;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, gT, cout, r, r, BM, err)) return BOWSHOCK_INVALID;
+  if (((uintptr_t)xs & 15)) {
+    err = "transposed activations not 16-byte aligned";
+    return BOWSHOCK_INVALID;
+  }
+  cuuint64_t dims[4] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B, 3ULL * cin};
+  cuuint64_t strides[3] = {(cuuint64_t)W * 2, (cuuint64_t)H * W * 2, (cuuint64_t)r * 2};
+  cuuint32_t box[4] = {(cuuint32_t)W, 1, 1, (cuuint32_t)bn};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult rr = g_encode(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(xs), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rr != CUDA_SUCCESS) {
+    err = "cuTensorMapEncodeTiled (4D transposed activations) failed (" + std::to_string((int)rr) + ")";
+    return BOWSHOCK_INVALID;
+  }
+  GemmArgs g{};
+  g.err = err_flag, g.mode = EPI_F32_ATOMIC, g.d = dw, g.ldd = 9LL * cin;
+  const int nkb = (int)(r / BK);  // one image row per K block
+  const int tiles = ((cout + BM - 1) / BM) * (9 * cin / bn);
+  int splits = std::max(1, std::min(nkb, 2 * 148 / tiles));
+  const int per = (nkb + splits - 1) / splits;
+  splits = (nkb + per - 1) / per;
+  g.M = cout, g.N = 9 * cin, g.K = (int)r, g.kb_per_split = per;
+  g.cHin = H, g.cWin = W, g.cC = cin;
+  dim3 grid((unsigned)((cout + BM - 1) / BM), (unsigned)(9 * cin / bn), (unsigned)splits);
+  const cudaError_t e = bn == 128 ? launch_gemm_bn<128, GEMM_WGRAD>(ta, tb, g, grid, st) : launch_gemm_bn<64, GEMM_WGRAD>(ta, tb, g, grid, st);
+  if (e != cudaSuccess) {
+    err = std::string("weight-gradient GEMM launch: ") + cudaGetErrorString(e);
     return BOWSHOCK_CUDA_ERROR;
   }
   return 0;
@@ -985,7 +1055,20 @@ struct Net {
       dim3 tg((unsigned)((l.cout + 31) / 32), (unsigned)((r + 31) / 32));
       k_transpose<<<tg, dim3(32, 8), 0, stream>>>(g, l.cout, (int)r, l.cout, gT, r);
       const bf16* XT;
-      if (l.fc) {
+      if (!l.fc && conv_mode == 2 && l.W == 64 && l.cin % 64 == 0) {
+        // the input (upsampled first where the layer upsamples) transposed into colT, its three x-shifted copies into
+        // col (3 r cin <= 9 r cin), the taps' boxes loaded from those by TMA
+        const bf16* src = xin;
+        if (l.up) {
+          k_upsample2x<<<grid_for(r * (l.cin / 8)), 256, 0, stream>>>(xin, B, l.H >> 1, l.W >> 1, l.cin, col);
+          src = col;
+        }
+        dim3 tx((unsigned)((l.cin + 31) / 32), (unsigned)((r + 31) / 32));
+        k_transpose<<<tx, dim3(32, 8), 0, stream>>>(src, l.cin, (int)r, l.cin, colT, r);
+        k_shift3<<<grid_for(3 * r * l.cin), 256, 0, stream>>>(colT, l.cin, r, l.W, col);
+        if ((rc = wgrad_gemm_tma(gT, col, B, l.H, l.cin, l.cout, gw + l.woff, d_err, stream, err))) return rc;
+        XT = nullptr;
+      } else if (l.fc) {
         dim3 tx((unsigned)((l.cin + 31) / 32), (unsigned)((r + 31) / 32));
         k_transpose<<<tx, dim3(32, 8), 0, stream>>>(xin, l.cin, (int)r, l.cin, colT, r);
         XT = colT;
@@ -999,7 +1082,7 @@ struct Net {
       gd.err = d_err, gd.mode = EPI_F32_ATOMIC, gd.d = gw + l.woff, gd.ldd = l.kin;
       const int tiles = ((l.cout + BM - 1) / BM) * (int)((l.kin + pick_bn((int)l.kin) - 1) / pick_bn((int)l.kin));
       const int splits = std::max(1, 2 * 148 / tiles);
-      if ((rc = gemm(gT, r, XT, r, l.cout, (int)l.kin, (int)r, gd, splits, stream, err))) return rc;
+      if (XT && (rc = gemm(gT, r, XT, r, l.cout, (int)l.kin, (int)r, gd, splits, stream, err))) return rc;
       k_bias_grad<<<dim3((unsigned)((l.cout + 31) / 32), (unsigned)std::min<long long>(1024, (r + 255) / 256)), dim3(32, 8), 0, stream>>>(
           g, r, l.cout, gw + l.boff);
       if (k == 0) break;
