@@ -112,3 +112,33 @@ def test_converged_normal_force_matches_oracle():  # run3.rs stop rules on both,
     assert rg["stop_reason"] in ("residual drop", "CN stationary"), rg
     assert abs(rg["cn"] - rc["cn"]) <= 2e-3 * abs(rc["cn"]) + 1e-4, (rg, rc)
     assert abs(rg["x_cp"] - rc["x_cp"]) <= 2e-2, (rg, rc)
+
+
+def test_converged_normal_force_matches_oracle_at_96x32x32():
+    """The lift-sweep body at 96 x 32 x 32 cells (98,304; the largest the 3D oracle finishes in minutes on the host) at
+    M 1.2 and M 2.5, 4 degrees: the batch's converged CN and centre of pressure against the oracle's
+    (tests/golden/lift3_oracle.json, make_lift3_fixture.py), both to run3.rs's stop rules. Tolerances as for the small
+    case: the CN-stationary rule holds CN to 0.2 % over its window on either side."""
+    import json
+    import os
+    import bowshock_b200.euler3 as e3
+    fx = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lift3_oracle.json")))
+    ni, nj, nk = fx["grid"]
+    cfgs, x_base = [], None
+    machs = sorted(fx["cases"], key=float)
+    grid = None
+    for m in machs:
+        c, ni2, nj2, x2, r2 = _grid(ni, nj, nk, float(m), fx["alpha_deg"])
+        cfgs.append(e3.Config3(float(m), math.radians(fx["alpha_deg"]), 0.5, o.MINMOD, fx["first_order"], False, e3.ImplicitParams(cfl_max=10.0)))
+        grid = (ni2, nj2, x2, r2, c.case2.grid_sting.n_up)
+        x_base = c.body.x_base()
+    ni2, nj2, x2, r2, axis = grid
+    x, y, z = e3.revolve(x2, r2, nk)
+    gpu = e3.Batch3(ni2, nj2, nk, x, y, z, axis, cfgs)
+    res = gpu.solve(x_base, max_iter=fx["max_iter"])
+    for m, rg in zip(machs, res):
+        rc = fx["cases"][m]
+        print(m, rg["iterations"], rg["stop_reason"], rg["cn"], rc["cn"], rg["x_cp"], rc["x_cp"])
+        assert rg["stop_reason"] in ("residual drop", "CN stationary"), rg
+        assert abs(rg["cn"] - rc["cn"]) <= 2e-3 * abs(rc["cn"]) + 1e-4, (m, rg, rc)
+        assert abs(rg["x_cp"] - rc["x_cp"]) <= 2e-2, (m, rg, rc)
