@@ -25,6 +25,7 @@ Metric: converged cases per hour on one B200 at |dCD| <= 1e-4 against the FP64 o
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -490,7 +491,8 @@ def measure_multigrid(device):
     """Single-grid line-implicit against 3-level FAS with the line-implicit smoother, each to the reference's stop rules
     (wall clock of GpuSolver.run_to_stop): a sting-mounted ogive + cylinder at M 2.0 (attached flow, the coarse-grid
     correction under-relaxed by 0.5, coarse CFL halved per level) and config 0 (Euler, 128 x 64, M 1.5, separated base
-    flow, correction under-relaxed by 0.5; CD against the FP64 oracle's converged run); and the transfer kernels' model
+    flow, correction under-relaxed by 0.5, capped at 4,000 cycles: it does not converge there; CD against the FP64
+    oracle's converged run); and the transfer kernels' model
     bytes over their CUDA-event time (grids this small stay in the L2 cache)."""
     import bowshock_b200 as bk
     from bowshock_b200.case import Body, Case, NOSE_TANGENT_OGIVE, WAKE_STING
@@ -506,10 +508,13 @@ def measure_multigrid(device):
         for name, levels in (("single_grid", 1), ("multigrid3", 3)):
             c = make()
             s = c.build_solver(device)
+            numerics = c.numerics
             if levels > 1:
                 s.set_scheme(bk.solver.MgParams(levels=levels, pre=1, post=1, implicit=c.numerics.scheme, relax=relax, cfl_scale=scale))
+                if key == "config0":  # it does not converge there (a bounded limit cycle): capped at 4,000 cycles
+                    numerics = dataclasses.replace(numerics, max_iter=4000)
             t0 = time.perf_counter()
-            r = s.run_to_stop(c.body, c.numerics, c.wake)
+            r = s.run_to_stop(c.body, numerics, c.wake)
             wall = time.perf_counter() - t0
             o[name] = {"iters": r["iters"], "stop": r["stop_reason"], "wall_s": wall, "cd_total": r["cd_total"]}
             if key == "config0":
