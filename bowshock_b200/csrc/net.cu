@@ -113,6 +113,66 @@ __host__ __device__ constexpr int gemm_smem_bytes() {
   return STAGES * (BM * BK * 2 + BN * BK * 2) + 1024 + 256;
 }
 
+// Epilogue of 16 accumulator columns nb .. nb + 15 of output row `row` (r: their FP32 bits from TMEM): bias + leaky
+// ReLU to BF16, FP32 with or without bias, or FP32 atomic adds (split-K). Whole 16-column chunks at 16-byte-aligned
+// addresses go out as two (BF16) or four (FP32) 16-byte stores; the values are the same either way.
+__device__ __forceinline__ void store16(const GemmArgs& g, int row, int nb, const uint32_t* r) {
+  const bool whole = nb + 16 <= g.N;
+  if (g.mode == EPI_BIAS_ACT_BF16) {
+    bf16* yp = g.y + (long long)row * g.ldy + nb;
+    if (whole && (reinterpret_cast<uintptr_t>(yp) & 15) == 0) {
+      uint4 o[2];
+      __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(o);
+#pragma unroll
+      for (int q = 0; q < 16; q += 2) {
+        float v0 = __uint_as_float(r[q]) + g.bias[nb + q];
+        v0 = v0 > 0.f ? v0 : g.slope * v0;
+        float v1 = __uint_as_float(r[q + 1]) + g.bias[nb + q + 1];
+        v1 = v1 > 0.f ? v1 : g.slope * v1;
+        h[q / 2] = __floats2bfloat162_rn(v0, v1);
+      }
+      reinterpret_cast<uint4*>(yp)[0] = o[0];
+      reinterpret_cast<uint4*>(yp)[1] = o[1];
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q += 2) {
+      if (nb + q >= g.N) break;
+      float v0 = __uint_as_float(r[q]) + g.bias[nb + q];
+      v0 = v0 > 0.f ? v0 : g.slope * v0;
+      if (nb + q + 1 < g.N) {
+        float v1 = __uint_as_float(r[q + 1]) + g.bias[nb + q + 1];
+        v1 = v1 > 0.f ? v1 : g.slope * v1;
+        *reinterpret_cast<__nv_bfloat162*>(yp + q) = __floats2bfloat162_rn(v0, v1);
+      } else {
+        yp[q] = __float2bfloat16_rn(v0);
+      }
+    }
+    return;
+  }
+  float* dp = g.d + (long long)row * g.ldd + nb;
+  if (g.mode != EPI_F32_ATOMIC && whole && (reinterpret_cast<uintptr_t>(dp) & 15) == 0) {
+#pragma unroll
+    for (int q = 0; q < 16; q += 4) {
+      float4 v = make_float4(__uint_as_float(r[q]), __uint_as_float(r[q + 1]), __uint_as_float(r[q + 2]), __uint_as_float(r[q + 3]));
+      if (g.mode == EPI_BIAS_F32) v.x += g.bias[nb + q], v.y += g.bias[nb + q + 1], v.z += g.bias[nb + q + 2], v.w += g.bias[nb + q + 3];
+      *reinterpret_cast<float4*>(dp + q) = v;
+    }
+    return;
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    if (nb + q >= g.N) break;
+    float v = __uint_as_float(r[q]);
+    if (g.mode == EPI_F32_ATOMIC)
+      atomicAdd(dp + q, v);
+    else if (g.mode == EPI_BIAS_F32)
+      dp[q] = v + g.bias[nb + q];
+    else
+      dp[q] = v;
+  }
+}
+
 // D[M, N] = A[M, K] B[N, K]^T (A and B row-major BF16, K contiguous), one 128 x BN tile per CTA, the K blocks of
 // blockIdx.z's split. Warp 0 lane 0 loads (TMA), warp 1 lane 0 issues the MMAs, all four warps run the epilogue (thread t
 // owns accumulator row t: TMEM lane t).
@@ -214,35 +274,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm(const __grid_constant__ CUtenso
       tmem_ld_wait();
       if (row >= g.M) continue;
       const int nb = n0 + c;
-      if (g.mode == EPI_BIAS_ACT_BF16) {
-        bf16* yp = g.y + (long long)row * g.ldy + nb;
-#pragma unroll
-        for (int q = 0; q < 16; q += 2) {
-          if (nb + q >= g.N) break;
-          float v0 = __uint_as_float(r[q]) + g.bias[nb + q];
-          v0 = v0 > 0.f ? v0 : g.slope * v0;
-          if (nb + q + 1 < g.N) {
-            float v1 = __uint_as_float(r[q + 1]) + g.bias[nb + q + 1];
-            v1 = v1 > 0.f ? v1 : g.slope * v1;
-            *reinterpret_cast<__nv_bfloat162*>(yp + q) = __floats2bfloat162_rn(v0, v1);
-          } else {
-            yp[q] = __float2bfloat16_rn(v0);
-          }
-        }
-      } else {
-        float* dp = g.d + (long long)row * g.ldd + nb;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          if (nb + q >= g.N) break;
-          float v = __uint_as_float(r[q]);
-          if (g.mode == EPI_F32_ATOMIC)
-            atomicAdd(dp + q, v);
-          else if (g.mode == EPI_BIAS_F32)
-            dp[q] = v + g.bias[nb + q];
-          else
-            dp[q] = v;
-        }
-      }
+      store16(g, row, nb, r);
     }
   }
   tc_fence_before();
@@ -390,35 +422,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_conv(const __grid_constant__ CU
       tmem_ld_wait();
       if (row >= g.M) continue;
       const int nb = n0 + c;
-      if (g.mode == EPI_BIAS_ACT_BF16) {
-        bf16* yp = g.y + (long long)row * g.ldy + nb;
-#pragma unroll
-        for (int q = 0; q < 16; q += 2) {
-          if (nb + q >= g.N) break;
-          float v0 = __uint_as_float(r[q]) + g.bias[nb + q];
-          v0 = v0 > 0.f ? v0 : g.slope * v0;
-          if (nb + q + 1 < g.N) {
-            float v1 = __uint_as_float(r[q + 1]) + g.bias[nb + q + 1];
-            v1 = v1 > 0.f ? v1 : g.slope * v1;
-            *reinterpret_cast<__nv_bfloat162*>(yp + q) = __floats2bfloat162_rn(v0, v1);
-          } else {
-            yp[q] = __float2bfloat16_rn(v0);
-          }
-        }
-      } else {
-        float* dp = g.d + (long long)row * g.ldd + nb;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          if (nb + q >= g.N) break;
-          float v = __uint_as_float(r[q]);
-          if (g.mode == EPI_F32_ATOMIC)
-            atomicAdd(dp + q, v);
-          else if (g.mode == EPI_BIAS_F32)
-            dp[q] = v + g.bias[nb + q];
-          else
-            dp[q] = v;
-        }
-      }
+      store16(g, row, nb, r);
     }
   }
   tc_fence_before();
