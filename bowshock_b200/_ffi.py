@@ -187,6 +187,7 @@ SIGNATURES = {
     "bowshock_net_train": (_I, [_P, _U, _U, _D, _U, _dp]),
     "bowshock_net_last_train_ms": (_I, [_P, _dp]),
     "bowshock_net_set_conv_mode": (_I, [_P, _I]),
+    "bowshock_gemm_set_persistent": (_I, [_I]),
     "bowshock_conv3x3_bf16": (_I, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P, C.c_int64, _P, C.c_int32, _P, _P]),
     "bowshock_gemm_bf16": (_I, [_P, C.c_int64, _P, C.c_int64, _P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P, _P]),
 }

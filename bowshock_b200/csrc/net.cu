@@ -605,8 +605,135 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
   }
 }
 
+// Persistent form of k_gemm for GEMMs without a K split: a grid of at most (SMs x resident CTAs) CTAs of 192 threads,
+// each looping over the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (tile t: rows (t % M tiles) x 128, columns
+// (t / M tiles) x BN). Warp 0 lane 0 streams the A and B stages of all its tiles through the STAGES ring (TMA; A as in
+// k_gemm<BN, KIND>), warp 1 lane 0 issues each tile's MMAs into one of two TMEM accumulators (alternating tiles), and
+// warps 2-5 (each owning the TMEM lane quarter warp % 4) run the epilogue of one accumulator while the MMAs fill the
+// other, so the loads, the MMAs and the epilogue of consecutive tiles overlap. Barriers: full / empty per stage,
+// acc_full[2] (tcgen05.commit after a tile's last MMA), acc_empty[2] (one arrival per epilogue warp once its lanes are
+// read). The MMAs and the K order of every tile are k_gemm's, so D is the same bit for bit. Every wait is bounded; a
+// wait that gives up ends that role and sets the error flag.
+template <int BN, int KIND>
+__global__ void __launch_bounds__(192, 1) k_gemm_p(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, TC = tmem_cols<BN>();
+  uint8_t* sa = smem;
+  uint8_t* sb = smem + STAGES * A_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sb + STAGES * B_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
+  uint64_t* acc_empty = acc_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  __shared__ int s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mtiles = (g.M + BM - 1) / BM, tiles = mtiles * ((g.N + BN - 1) / BN);
+  const int nkb = (g.K + BK - 1) / BK;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < STAGES; ++q) mbar_init(full + q, 1), mbar_init(empty + q, 1);
+    for (int q = 0; q < 2; ++q) mbar_init(acc_full + q, 1), mbar_init(acc_empty + q, 4);
+    bktma::mbar_init_fence();
+    s_abort = 0;
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 2 * TC);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  constexpr uint32_t IDESC = idesc_bf16(BM, BN);
+  if (warp == 0 && lane == 0) {  // producer
+    int it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; ok && t < tiles; t += gridDim.x) {
+      const int m0 = (t % mtiles) * BM, n0 = (t / mtiles) * BN;
+      for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const int q = it % STAGES;
+        const uint32_t ph = (uint32_t)((it / STAGES) & 1);
+        if (it >= STAGES && !mbar_wait(empty + q, ph ^ 1u)) {
+          s_abort = 1;
+          ok = false;
+          break;
+        }
+        mbar_expect_tx(full + q, (uint32_t)(A_BYTES + B_BYTES));
+        if constexpr (KIND == GEMM_CONV) {
+          const int hw = g.cHin * g.cWin, k0 = kb * BK, tap = k0 / g.cC;
+          tma_load_4d(sa + q * A_BYTES, &ta, full + q, k0 - tap * g.cC, tap % 3 - 1, (m0 % hw) / g.cWin + tap / 3 - 1, m0 / hw);
+        } else {
+          tma_load_2d(sa + q * A_BYTES, &ta, full + q, kb * BK, m0);
+        }
+        tma_load_2d(sb + q * B_BYTES, &tb, full + q, kb * BK, n0);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {  // MMA issuer
+    int it = 0, tl = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; ok && t < tiles; t += gridDim.x, ++tl) {
+      const int buf = tl & 1;
+      if (tl >= 2 && !mbar_wait(acc_empty + buf, (uint32_t)(((tl >> 1) & 1) ^ 1))) {
+        s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d = tmem + (uint32_t)(buf * TC);
+      for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const int q = it % STAGES;
+        const uint32_t ph = (uint32_t)((it / STAGES) & 1);
+        if (!mbar_wait(full + q, ph)) {
+          s_abort = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t ad = sw128_desc(sa + q * A_BYTES), bd = sw128_desc(sb + q * B_BYTES);
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) mma_bf16(d, ad + 2ull * kk, bd + 2ull * kk, IDESC, (kb | kk) != 0);
+        mma_commit(empty + q);
+      }
+      if (ok) mma_commit(acc_full + buf);
+    }
+  } else if (warp >= 2) {  // epilogue
+    const int quarter = warp & 3;
+    int tl = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+      const int buf = tl & 1;
+      bool ok = mbar_wait(acc_full + buf, (uint32_t)((tl >> 1) & 1));
+      ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
+      if (!ok) {
+        if (lane == 0) s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+      const int m0 = (t % mtiles) * BM, n0 = (t / mtiles) * BN;
+      const int row = m0 + quarter * 32 + lane;
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 16) {
+        uint32_t r[16];
+        tmem_ld16(tmem + (uint32_t)(buf * TC) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
+        tmem_ld_wait();
+        if (row < g.M) store16(g, row, n0 + c, r);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty + buf);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (s_abort && threadIdx.x == 0) atomicExch(g.err, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 2 * TC);
+  }
+}
+
 // ------------------------------------------------------------------------------------------------ host side
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+// GEMMs without a K split run the persistent kernel (k_gemm_p); false: one CTA per tile (k_gemm). Same results.
+static bool persistent_gemm = true;
 static bool get_encode(std::string& err) {
   if (!g_encode) g_encode = bktma::encoder(err);
   return g_encode != nullptr;
@@ -634,8 +761,26 @@ static bool make_map(CUtensorMap* m, const void* p, long long rows, long long co
 
 template <int BN, int KIND = GEMM_PLAIN>
 static cudaError_t launch_gemm_bn(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, dim3 grid, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>());
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  if constexpr (KIND != GEMM_WGRAD) {
+    if (grid.z == 1 && persistent_gemm) {  // one K split: the persistent kernel over the grid.x x grid.y tiles
+      static int resident = 0, sms = 0;    // CTAs of k_gemm_p<BN, KIND> per SM, SMs of the device
+      if ((e = cudaFuncSetAttribute(k_gemm_p<BN, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>())) != cudaSuccess)
+        return e;
+      if (!resident) {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_gemm_p<BN, KIND>, 192, gemm_smem_bytes<BN>())) != cudaSuccess)
+          return e;
+        resident = std::max(resident, 1);
+      }
+      const long long tiles = (long long)grid.x * grid.y;
+      const unsigned ctas = (unsigned)std::min<long long>(tiles, (long long)sms * resident);
+      k_gemm_p<BN, KIND><<<ctas, 192, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
+      return cudaGetLastError();
+    }
+  }
+  if ((e = cudaFuncSetAttribute(k_gemm<BN, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>())) != cudaSuccess) return e;
   k_gemm<BN, KIND><<<grid, 128, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
   return cudaGetLastError();
 }
@@ -1362,6 +1507,12 @@ int bowshock_conv3x3_bf16(const void* x, int64_t batch, int64_t h_in, int64_t w_
                                 reinterpret_cast<const bknet::bf16*>(w), 9 * c, (int)n, g, reinterpret_cast<cudaStream_t>(stream), err);
   return bknet::conv_gemm(reinterpret_cast<const bknet::bf16*>(x), (int)batch, (int)h_in, (int)w_in, (int)c, (int)up,
                           reinterpret_cast<const bknet::bf16*>(w), 9 * c, (int)n, g, reinterpret_cast<cudaStream_t>(stream), err);
+}
+
+int bowshock_gemm_set_persistent(int on) {
+  const int was = bknet::persistent_gemm ? 1 : 0;
+  bknet::persistent_gemm = on != 0;
+  return was;
 }
 
 int bowshock_gemm_bf16(const void* a, int64_t lda, const void* b, int64_t ldb, float* d, int64_t ldd, int64_t m, int64_t n, int64_t k, int64_t splits,

@@ -495,6 +495,11 @@ int bowshock_net_set_conv_mode(bowshock_net* n, int mode);
  * W dividing 128 with H W a multiple or a divisor of 128). */
 int bowshock_conv3x3_bf16(const void* x, int64_t batch, int64_t h_in, int64_t w_in, int64_t c, int64_t up, const void* w, int64_t n, float* d,
                           int32_t mode, void* stream, int* err_flag);
+/* 1 (the default): GEMMs without a K split (the network's forward and input-gradient GEMMs, bowshock_gemm_bf16 with
+ * splits = 1) run the persistent kernel (at most SMs x resident CTAs, each looping over tiles with two TMEM
+ * accumulators so that one tile's epilogue overlaps the next tile's MMAs); 0: one CTA per tile. Same results.
+ * Process-wide; returns the previous setting. */
+int bowshock_gemm_set_persistent(int on);
 /* The network's tensor-core GEMM on caller-owned device memory: d[m][n] = sum_k a[m][k] b[n][k], a and b BF16 row-major
  * (lda, ldb multiples of 8 elements, 16-byte aligned), d FP32 (ldd >= n); splits > 1 adds K slices atomically into d
  * (zeroed by the caller). stream: a cudaStream_t or NULL; err_flag: a device int set to 1 if a bounded wait gave up. */

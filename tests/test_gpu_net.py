@@ -49,6 +49,28 @@ def test_gemm_matches_torch_fp32(m, n, k, splits):
     assert err < 1e-4, f"{m}x{n}x{k} splits {splits}: max rel err {err:.2e}"
 
 
+@pytest.mark.parametrize("m,n,k", [(131072, 64, 576), (1000, 256, 1024), (300, 200, 136), (64, 16, 16), (4096, 4096, 256)])
+def test_persistent_gemm_equals_per_tile_gemm(m, n, k):
+    """The persistent GEMM (CTAs looping over tiles, two TMEM accumulators, epilogue overlapped with the next tile's
+    MMAs) gives the per-tile kernel's output bit for bit: the same MMAs in the same K order for every tile."""
+    import torch
+    from bowshock_b200 import _ffi
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    a = torch.randn((m, k), generator=g, device="cuda").to(torch.bfloat16)
+    b = torch.randn((n, k), generator=g, device="cuda").to(torch.bfloat16)
+    lib = _ffi.load()
+    was = lib.bowshock_gemm_set_persistent(1)
+    try:
+        d1 = _gemm(a, b)
+        lib.bowshock_gemm_set_persistent(0)
+        d0 = _gemm(a, b)
+    finally:
+        lib.bowshock_gemm_set_persistent(was)
+    assert torch.equal(d1, d0)
+    ref = a.float() @ b.float().T
+    assert ((d1 - ref).abs() / (ref.abs().amax(dim=1, keepdim=True) + 1e-6)).max().item() < 1e-4
+
+
 def _net_and_oracle(batch=8, seed=5):
     from bowshock_b200.net import Net
     L, n = no.layers()
