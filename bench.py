@@ -53,6 +53,15 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def bf16_peak():
+    """(dense BF16 TFLOP/s burst peak, 'measured' | 'fallback')."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 class Clocks:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -579,8 +588,10 @@ def run_kernels(args):
             if key == "tma":
                 torch.cuda.profiler.stop()
             ms = net.last_train_ms() / args.steps
-            out[key] = {"ms_per_step": ms, "tflops": fl / (ms / 1000.0) / 1e12}
+            tf = fl / (ms / 1000.0) / 1e12
+            out[key] = {"ms_per_step": ms, "tflops": tf, "frac_of_bf16_peak": tf / bf16_peak()[0]}
         out["ms_per_step"] = out["tma"]["ms_per_step"]
+        out["bf16_peak_kind"] = bf16_peak()[1]
         return out
     if args.workload == "lift3":
         import bowshock_b200.euler3 as e3
