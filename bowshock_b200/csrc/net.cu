@@ -915,21 +915,33 @@ static int conv_gemm_tma(const bf16* x, int B, int H, int W, int C, const bf16* 
   return 0;
 }
 
-// xs [3][C][r] = the transposed activations xT [C][r] (r = B H W pixels, W = 64) shifted along x: xs[s][c][p] =
-// xT[c][p + s - 1] where the pixel's x + s - 1 lies in [0, W), else 0
-__global__ void k_shift3(const bf16* __restrict__ xT, int C, long long r, int W, bf16* __restrict__ xs) {
-  const long long total = 3LL * C * r;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const long long p = t % r, q = t / r;
-    const int c = (int)(q % C), sft = (int)(q / C) - 1, x = (int)(p % W) + sft;
-    xs[t] = (x >= 0 && x < W) ? xT[(long long)c * r + p + sft] : __float2bfloat16_rn(0.f);
+// The weight-gradient operand of a 64-pixel-wide layer: x [r][C] (r = B H 64 pixels) transposed into three copies
+// shifted along x, xs[s][c][p] = x[p + s - 1][c] where the pixel's x + s - 1 lies in [0, 64), else 0. One image row
+// (64 pixels) x 32 channels per block through shared memory: coalesced 64-byte reads of the pixels' channels, 128-byte
+// rows of each shifted copy written as BF16 pairs. C a multiple of 32.
+__global__ void __launch_bounds__(256) k_transpose_shift3(const bf16* __restrict__ x, int C, long long r, bf16* __restrict__ xs) {
+  constexpr int W = 64;
+  __shared__ bf16 t[32][W + 2];
+  const int c0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
+  const long long p0 = (long long)blockIdx.y * W;
+#pragma unroll
+  for (int q = ty; q < W; q += 8) t[tx][q] = x[(p0 + q) * C + c0 + tx];
+  __syncthreads();
+  const bf16 z = __float2bfloat16_rn(0.f);
+#pragma unroll 1
+  for (int row = ty; row < 3 * 32; row += 8) {
+    const int sft = row / 32 - 1, c = row % 32, a = 2 * tx + sft, b = a + 1;
+    __nv_bfloat162 v;
+    v.x = (a >= 0 && a < W) ? t[c][a] : z;
+    v.y = (b >= 0 && b < W) ? t[c][b] : z;
+    reinterpret_cast<__nv_bfloat162*>(xs + ((long long)(sft + 1) * C + c0 + c) * r + p0)[tx] = v;
   }
 }
 
 // The weight gradient of a 3x3 'same' convolution of images 64 pixels wide: dw [cout, 9 cin] (FP32, accumulated
 // atomically over split-K slices; zeroed by the caller) = sum over the B x H x 64 pixels of gT[o][p] x[p shifted by the
 // tap][c], gT the output gradient transposed ([cout, pixels], BF16) and xs the layer's input transposed and shifted
-// (k_shift3: [3][cin][B][H][64]). cin a multiple of 64.
+// (k_transpose_shift3: [3][cin][B][H][64]). cin a multiple of 64.
 static int wgrad_gemm_tma(const bf16* gT, const bf16* xs, int B, int H, int cin, int cout, float* dw, int* err_flag, cudaStream_t st, std::string& err) {
   constexpr int W = 64;
   if (cin % 64) {
@@ -1205,17 +1217,16 @@ struct Net {
       k_transpose<<<tg, dim3(32, 8), 0, stream>>>(g, l.cout, (int)r, l.cout, gT, r);
       const bf16* XT;
       if (!l.fc && conv_mode == 2 && l.W == 64 && l.cin % 64 == 0) {
-        // the input (upsampled first where the layer upsamples) transposed into colT, its three x-shifted copies into
-        // col (3 r cin <= 9 r cin), the taps' boxes loaded from those by TMA
+        // the input (upsampled first where the layer upsamples) transposed with its three x-shifted copies into one of
+        // the im2col buffers (3 r cin <= 9 r cin), the taps' boxes loaded from those by TMA
         const bf16* src = xin;
         if (l.up) {
           k_upsample2x<<<grid_for(r * (l.cin / 8)), 256, 0, stream>>>(xin, B, l.H >> 1, l.W >> 1, l.cin, col);
           src = col;
         }
-        dim3 tx((unsigned)((l.cin + 31) / 32), (unsigned)((r + 31) / 32));
-        k_transpose<<<tx, dim3(32, 8), 0, stream>>>(src, l.cin, (int)r, l.cin, colT, r);
-        k_shift3<<<grid_for(3 * r * l.cin), 256, 0, stream>>>(colT, l.cin, r, l.W, col);
-        if ((rc = wgrad_gemm_tma(gT, col, B, l.H, l.cin, l.cout, gw + l.woff, d_err, stream, err))) return rc;
+        bf16* xs = src == col ? colT : col;  // the shifted copies go to whichever buffer does not hold the input
+        k_transpose_shift3<<<dim3((unsigned)(l.cin / 32), (unsigned)(r / 64)), dim3(32, 8), 0, stream>>>(src, l.cin, r, xs);
+        if ((rc = wgrad_gemm_tma(gT, xs, B, l.H, l.cin, l.cout, gw + l.woff, d_err, stream, err))) return rc;
         XT = nullptr;
       } else if (l.fc) {
         dim3 tx((unsigned)((l.cin + 31) / 32), (unsigned)((r + 31) / 32));
