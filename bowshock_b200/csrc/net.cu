@@ -915,33 +915,36 @@ static int conv_gemm_tma(const bf16* x, int B, int H, int W, int C, const bf16* 
   return 0;
 }
 
-// The weight-gradient operand of a 64-pixel-wide layer: x [r][C] (r = B H 64 pixels) transposed into three copies
-// shifted along x, xs[s][c][p] = x[p + s - 1][c] where the pixel's x + s - 1 lies in [0, 64), else 0. One image row
-// (64 pixels) x 32 channels per block through shared memory: coalesced 64-byte reads of the pixels' channels, 128-byte
-// rows of each shifted copy written as BF16 pairs. C a multiple of 32.
-__global__ void __launch_bounds__(256) k_transpose_shift3(const bf16* __restrict__ x, int C, long long r, bf16* __restrict__ xs) {
-  constexpr int W = 64;
-  __shared__ bf16 t[32][W + 2];
-  const int c0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
-  const long long p0 = (long long)blockIdx.y * W;
-#pragma unroll
-  for (int q = ty; q < W; q += 8) t[tx][q] = x[(p0 + q) * C + c0 + tx];
-  __syncthreads();
+// The weight-gradient operands of a layer W <= 64 pixels wide (W dividing 64), on a row pitch of 64 pixels: x [rows W]
+// [C] (rows = B H image rows) -> out [C][rows 64], out[c][row 64 + x] = x[row W + x][c] for x < W and 0 for the padding
+// x >= W; with SHIFT3, three such planes shifted along x, out[s][c][row 64 + x] = x[row W + x + s - 1][c] where both x
+// and x + s - 1 lie in [0, W), else 0. One image row (blockIdx.x) x 32 channels (blockIdx.y) per block through shared memory: coalesced reads of
+// the pixels' channels, 128-byte rows written as BF16 pairs. C a multiple of 32.
+template <bool SHIFT3>
+__global__ void __launch_bounds__(256) k_transpose_rows(const bf16* __restrict__ x, int C, int W, long long rows, bf16* __restrict__ out) {
+  constexpr int P64 = 64, NS = SHIFT3 ? 3 : 1;
+  __shared__ bf16 t[32][P64 + 2];
+  const int c0 = blockIdx.y * 32, tx = threadIdx.x, ty = threadIdx.y;
+  const long long row = blockIdx.x, pitch = rows * P64;
   const bf16 z = __float2bfloat16_rn(0.f);
+#pragma unroll
+  for (int q = ty; q < P64; q += 8) t[tx][q] = q < W ? x[(row * W + q) * C + c0 + tx] : z;
+  __syncthreads();
 #pragma unroll 1
-  for (int row = ty; row < 3 * 32; row += 8) {
-    const int sft = row / 32 - 1, c = row % 32, a = 2 * tx + sft, b = a + 1;
+  for (int idx = ty; idx < NS * 32; idx += 8) {
+    const int sft = SHIFT3 ? idx / 32 - 1 : 0, c = idx % 32, xa = 2 * tx, a = xa + sft, b = a + 1;
     __nv_bfloat162 v;
-    v.x = (a >= 0 && a < W) ? t[c][a] : z;
-    v.y = (b >= 0 && b < W) ? t[c][b] : z;
-    reinterpret_cast<__nv_bfloat162*>(xs + ((long long)(sft + 1) * C + c0 + c) * r + p0)[tx] = v;
+    v.x = (xa < W && a >= 0 && a < W) ? t[c][a] : z;
+    v.y = (xa + 1 < W && b >= 0 && b < W) ? t[c][b] : z;
+    reinterpret_cast<__nv_bfloat162*>(out + ((long long)(SHIFT3 ? sft + 1 : 0) * C + c0 + c) * pitch + row * P64)[tx] = v;
   }
 }
 
-// The weight gradient of a 3x3 'same' convolution of images 64 pixels wide: dw [cout, 9 cin] (FP32, accumulated
-// atomically over split-K slices; zeroed by the caller) = sum over the B x H x 64 pixels of gT[o][p] x[p shifted by the
-// tap][c], gT the output gradient transposed ([cout, pixels], BF16) and xs the layer's input transposed and shifted
-// (k_transpose_shift3: [3][cin][B][H][64]). cin a multiple of 64.
+// The weight gradient of a 3x3 'same' convolution: dw [cout, 9 cin] (FP32, accumulated atomically over split-K slices;
+// zeroed by the caller) = sum over the pixels of gT[o][p] x[p shifted by the tap][c], gT the output gradient and xs
+// the layer's input, both transposed onto a row pitch of 64 pixels (k_transpose_rows: gT [cout][B H 64], xs [3][cin]
+// [B][H][64] with the shifted copies; the padding pixels are zeros on both sides, so they add nothing). cin a multiple
+// of 64.
 static int wgrad_gemm_tma(const bf16* gT, const bf16* xs, int B, int H, int cin, int cout, float* dw, int* err_flag, cudaStream_t st, std::string& err) {
   constexpr int W = 64;
   if (cin % 64) {
@@ -1036,6 +1039,7 @@ struct Net {
   int* idx = nullptr;
   long long idx_cap = 0;
   double last_ms = 0.0;
+  long long cap_col = 0, cap_rows = 0;  // elements of col / colT and of gT / g0 / g1
   int conv_mode = 2;  // 3x3 convolutions of 64k channels: 0 im2col + GEMM, 1 implicit GEMM (cp.async gather), 2 implicit GEMM (TMA boxes)
 
   ~Net() {
@@ -1095,7 +1099,7 @@ struct Net {
     NCK(cudaMemsetAsync(wb, 0, nparam * 2, stream));
     NCK(cudaMalloc(&x, (size_t)maxB * BOWSHOCK_NET_IN * 2));
     act.assign(L.size(), nullptr);
-    long long max_col = 0, max_rows_c = 0;
+    long long max_col = 0, max_rows_c = 0;  // elements of the im2col buffers and of the gradient buffers
     for (size_t k = 0; k < L.size(); ++k) {
       const Layer& l = L[k];
       const long long r = rows(l, maxB);
@@ -1106,6 +1110,7 @@ struct Net {
     }
     const Layer& lo = L.back();
     NCK(cudaMalloc(&out, rows(lo, maxB) * lo.cout * 4));
+    cap_col = max_col, cap_rows = max_rows_c;
     NCK(cudaMalloc(&col, max_col * 2));
     NCK(cudaMalloc(&colT, max_col * 2));
     NCK(cudaMalloc(&gT, max_rows_c * 2));
@@ -1212,20 +1217,28 @@ struct Net {
       const Layer& l = L[k];
       const long long r = rows(l, B);
       const bf16* xin = k > 0 ? act[k - 1] : x;
-      // dW [cout, kin] = g^T X: K = rows
-      dim3 tg((unsigned)((l.cout + 31) / 32), (unsigned)((r + 31) / 32));
-      k_transpose<<<tg, dim3(32, 8), 0, stream>>>(g, l.cout, (int)r, l.cout, gT, r);
+      // dW [cout, kin] = g^T X: K = rows. A convolution up to 64 pixels wide runs the TMA weight gradient: g and the
+      // input transposed onto a row pitch of 64 pixels (zero padding), the input also in its three x-shifted copies
+      const long long rows64 = (long long)B * l.H * 64;
+      const bool wg = !l.fc && conv_mode == 2 && l.W <= 64 && 64 % l.W == 0 && l.cin % 64 == 0 && l.cout % 32 == 0 &&
+                      (long long)l.cout * rows64 <= cap_rows && 3LL * l.cin * rows64 <= cap_col;
+      if (wg) {
+        k_transpose_rows<false><<<dim3((unsigned)(B * l.H), (unsigned)(l.cout / 32)), dim3(32, 8), 0, stream>>>(g, l.cout, l.W, (long long)B * l.H, gT);
+      } else {
+        dim3 tg((unsigned)((l.cout + 31) / 32), (unsigned)((r + 31) / 32));
+        k_transpose<<<tg, dim3(32, 8), 0, stream>>>(g, l.cout, (int)r, l.cout, gT, r);
+      }
       const bf16* XT;
-      if (!l.fc && conv_mode == 2 && l.W == 64 && l.cin % 64 == 0) {
-        // the input (upsampled first where the layer upsamples) transposed with its three x-shifted copies into one of
-        // the im2col buffers (3 r cin <= 9 r cin), the taps' boxes loaded from those by TMA
+      if (wg) {
+        // the input (upsampled first where the layer upsamples) into one of the im2col buffers, its shifted copies
+        // into the other, the taps' boxes loaded from those by TMA
         const bf16* src = xin;
         if (l.up) {
           k_upsample2x<<<grid_for(r * (l.cin / 8)), 256, 0, stream>>>(xin, B, l.H >> 1, l.W >> 1, l.cin, col);
           src = col;
         }
-        bf16* xs = src == col ? colT : col;  // the shifted copies go to whichever buffer does not hold the input
-        k_transpose_shift3<<<dim3((unsigned)(l.cin / 32), (unsigned)(r / 64)), dim3(32, 8), 0, stream>>>(src, l.cin, r, xs);
+        bf16* xs = src == col ? colT : col;
+        k_transpose_rows<true><<<dim3((unsigned)(B * l.H), (unsigned)(l.cin / 32)), dim3(32, 8), 0, stream>>>(src, l.cin, l.W, (long long)B * l.H, xs);
         if ((rc = wgrad_gemm_tma(gT, xs, B, l.H, l.cin, l.cout, gw + l.woff, d_err, stream, err))) return rc;
         XT = nullptr;
       } else if (l.fc) {
