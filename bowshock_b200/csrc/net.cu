@@ -919,7 +919,7 @@ static int conv_gemm_tma(const bf16* x, int B, int H, int W, int C, const bf16* 
 // [C] (rows = B H image rows) -> out [C][rows 64], out[c][row 64 + x] = x[row W + x][c] for x < W and 0 for the padding
 // x >= W; with SHIFT3, three such planes shifted along x, out[s][c][row 64 + x] = x[row W + x + s - 1][c] where both x
 // and x + s - 1 lie in [0, W), else 0. One image row (blockIdx.x) x 32 channels (blockIdx.y) per block through shared memory: coalesced reads of
-// the pixels' channels, 128-byte rows written as BF16 pairs. C a multiple of 32.
+// the pixels' channels, 128-byte rows written as BF16 pairs (the last channel block may be partial).
 template <bool SHIFT3>
 __global__ void __launch_bounds__(256) k_transpose_rows(const bf16* __restrict__ x, int C, int W, long long rows, bf16* __restrict__ out) {
   constexpr int P64 = 64, NS = SHIFT3 ? 3 : 1;
@@ -928,11 +928,12 @@ __global__ void __launch_bounds__(256) k_transpose_rows(const bf16* __restrict__
   const long long row = blockIdx.x, pitch = rows * P64;
   const bf16 z = __float2bfloat16_rn(0.f);
 #pragma unroll
-  for (int q = ty; q < P64; q += 8) t[tx][q] = q < W ? x[(row * W + q) * C + c0 + tx] : z;
+  for (int q = ty; q < P64; q += 8) t[tx][q] = (q < W && c0 + tx < C) ? x[(row * W + q) * C + c0 + tx] : z;
   __syncthreads();
 #pragma unroll 1
   for (int idx = ty; idx < NS * 32; idx += 8) {
     const int sft = SHIFT3 ? idx / 32 - 1 : 0, c = idx % 32, xa = 2 * tx, a = xa + sft, b = a + 1;
+    if (c0 + c >= C) continue;
     __nv_bfloat162 v;
     v.x = (xa < W && a >= 0 && a < W) ? t[c][a] : z;
     v.y = (xa + 1 < W && b >= 0 && b < W) ? t[c][b] : z;
@@ -1220,10 +1221,10 @@ struct Net {
       // dW [cout, kin] = g^T X: K = rows. A convolution up to 64 pixels wide runs the TMA weight gradient: g and the
       // input transposed onto a row pitch of 64 pixels (zero padding), the input also in its three x-shifted copies
       const long long rows64 = (long long)B * l.H * 64;
-      const bool wg = !l.fc && conv_mode == 2 && l.W <= 64 && 64 % l.W == 0 && l.cin % 64 == 0 && l.cout % 32 == 0 &&
+      const bool wg = !l.fc && conv_mode == 2 && l.W <= 64 && 64 % l.W == 0 && l.cin % 64 == 0 && l.cout % 8 == 0 &&
                       (long long)l.cout * rows64 <= cap_rows && 3LL * l.cin * rows64 <= cap_col;
       if (wg) {
-        k_transpose_rows<false><<<dim3((unsigned)(B * l.H), (unsigned)(l.cout / 32)), dim3(32, 8), 0, stream>>>(g, l.cout, l.W, (long long)B * l.H, gT);
+        k_transpose_rows<false><<<dim3((unsigned)(B * l.H), (unsigned)((l.cout + 31) / 32)), dim3(32, 8), 0, stream>>>(g, l.cout, l.W, (long long)B * l.H, gT);
       } else {
         dim3 tg((unsigned)((l.cout + 31) / 32), (unsigned)((r + 31) / 32));
         k_transpose<<<tg, dim3(32, 8), 0, stream>>>(g, l.cout, (int)r, l.cout, gT, r);
