@@ -144,6 +144,7 @@ SIGNATURES = {
                                        C.POINTER(Block)]),
     "bowshock_large_domain_grid": (_I, [C.POINTER(BowshockBody), C.POINTER(StingGridC), C.POINTER(_U), C.POINTER(_U), _dp, _dp]),
     "bowshock_arena_create": (_I, [_U, C.POINTER(CaseDesc), _I, C.POINTER(_P)]),
+    "bowshock_arena_set_case_groups": (_I, [_P, _I]),
     "bowshock_arena_create_meshed": (_I, [_U, C.POINTER(CaseDesc), C.POINTER(MeshRequest), _I, C.POINTER(_P)]),
     "bowshock_mesh_dims": (_I, [C.POINTER(MeshRequest), C.POINTER(_U), C.POINTER(_U), C.POINTER(Block)]),
     "bowshock_mesh_batch": (_I, [_U, C.POINTER(MeshRequest), _I, _dp, _dp, _dp, _dp]),

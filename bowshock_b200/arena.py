@@ -109,6 +109,10 @@ class Arena:
         t = _ffi.LineTuning(*[int(cur[n]) for n, _ in _ffi.LineTuning._fields_])
         self._check(_ffi.load().bowshock_arena_set_tuning(self._h, C.byref(t)))
 
+    def set_case_groups(self, groups: int):
+        """Split the active cases into `groups` (1 to 4) independent chains of the chunk's graph (same results)."""
+        self._check(_ffi.load().bowshock_arena_set_case_groups(self._h, int(groups)))
+
     def solve(self, progress=None):
         """Cold-start every case and iterate each to its stop rule (converged cases are masked out)."""
         res = (_ffi.PointResult * self.ncases)()

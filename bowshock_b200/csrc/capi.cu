@@ -769,6 +769,16 @@ int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out) {
   return BOWSHOCK_OK;
 }
 
+int bowshock_arena_set_case_groups(bowshock_arena* a, int groups) {
+  if (!a || groups < 1 || groups > ArenaHost::MAX_GROUPS) return BOWSHOCK_INVALID;
+  a->ar.groups_req = groups;
+  if (a->ar.compact_lists()) {
+    a->last_error = a->ar.err;
+    return BOWSHOCK_CUDA_ERROR;
+  }
+  return BOWSHOCK_OK;
+}
+
 int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) {
   if (!a || !t) return BOWSHOCK_INVALID;
   auto w4 = [](int32_t w) { return w == 1 || w == 2 || w == 4; };

@@ -349,6 +349,21 @@ struct ArenaHost {
   int graph_len = 0;
   bool graph_dirty = false;  // `graph` is stale but has the topology of the next capture
   std::vector<int> h_active;
+  // Case groups of the captured chunk: with groups_req > 1 the active cases are split into up to groups_req groups of
+  // about equal cells, and each group's iterations are captured on a stream of its own, so the chunk's graph holds one
+  // independent chain of iterations per group and the groups' kernels run side by side. Every kernel of an iteration
+  // touches only its own cases' data (per-case counters, residual slots, records), so the states are the ones of the
+  // ungrouped graph bit for bit; what changes is how many warps are in flight when few cases are left.
+  struct Group {
+    cudaStream_t st = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ends = nullptr, ev_done = nullptr;
+    int *d_act = nullptr, *d_tl = nullptr, *d_pb = nullptr, *d_il = nullptr, *d_jl = nullptr;
+    int n_tl = 0, n_pb = 0, n_il = 0, n_jl = 0;
+  };
+  static constexpr int MAX_GROUPS = 4;
+  std::vector<Group> grp;
+  int groups_req = 1, ngroups = 1;
+  cudaEvent_t ev_split = nullptr;
 
   ~ArenaHost() { release(); }
 
@@ -375,6 +390,17 @@ struct ArenaHost {
     if (ev_fork) cudaEventDestroy(ev_fork), ev_fork = nullptr;
     if (ev_join) cudaEventDestroy(ev_join), ev_join = nullptr;
     if (ev_ends) cudaEventDestroy(ev_ends), ev_ends = nullptr;
+    for (Group& q : grp) {
+      for (cudaStream_t t : {q.st, q.side})
+        if (t) cudaStreamDestroy(t);
+      for (cudaEvent_t e : {q.ev_fork, q.ev_join, q.ev_ends, q.ev_done})
+        if (e) cudaEventDestroy(e);
+      for (int* p : {q.d_act, q.d_tl, q.d_pb, q.d_il, q.d_jl})
+        if (p) cudaFree(p);
+    }
+    grp.clear();
+    ngroups = 1;
+    if (ev_split) cudaEventDestroy(ev_split), ev_split = nullptr;
     ready = false;
   }
 
@@ -843,7 +869,77 @@ struct ArenaHost {
     A.jline_list = lists ? d_jllist : nullptr;
     A.n_tl = (int)tl.size(), A.n_pb = (int)pb.size(), A.n_il = (int)il.size(), A.n_jl = (int)jl.size();
     graph_dirty = true;  // same kernels, new grids and lists: the next capture updates the instantiated graph
+    ngroups = 1;
+    if (lists && groups_req > 1 && n_act >= 2) return group_lists(std::min(groups_req, n_act));
     return 0;
+  }
+  // The lists and masks of G case groups (Group): the active cases, largest first, each to the group with the fewest
+  // cells so far; per group the tile, padded-block and line lists (lines longest first) and the per-case mask.
+  int group_lists(int G) {
+    const int nc = (int)cases.size();
+    if (!ev_split) BK_CUDA(cudaEventCreateWithFlags(&ev_split, cudaEventDisableTiming));
+    while ((int)grp.size() < G) {
+      grp.emplace_back();
+      Group& q = grp.back();
+      BK_CUDA(cudaStreamCreateWithFlags(&q.st, cudaStreamNonBlocking));
+      BK_CUDA(cudaStreamCreateWithFlags(&q.side, cudaStreamNonBlocking));
+      for (cudaEvent_t* e : {&q.ev_fork, &q.ev_join, &q.ev_ends, &q.ev_done}) BK_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+      int rc;
+      if ((rc = dalloc(&q.d_act, nc, err)) || (rc = dalloc(&q.d_tl, ntiles, err)) || (rc = dalloc(&q.d_pb, npblk, err)) ||
+          (rc = dalloc(&q.d_il, nil, err)) || (rc = dalloc(&q.d_jl, njl, err)))
+        return rc;
+    }
+    std::vector<int> order;
+    for (int k = 0; k < nc; ++k)
+      if (h_active[k]) order.push_back(k);
+    auto cells = [&](int k) { return (long long)cases[k].ni * cases[k].nj; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells(a) > cells(b); });
+    std::vector<std::vector<int>> members(G);
+    std::vector<long long> load(G, 0);
+    for (int k : order) {
+      const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      members[g].push_back(k);
+      load[g] += cells(k);
+    }
+    for (int g = 0; g < G; ++g) {
+      Group& q = grp[g];
+      std::vector<int> act(nc, 0), tl, pb, il, jl;
+      std::vector<std::pair<int, int>> li, lj;
+      for (int k : members[g]) {
+        act[k] = 1;
+        const CaseDev& c = desc[k];
+        const HostCase& h = cases[k];
+        const int nt = c.ntx * c.nty, nb = (int)(((long long)(h.ni + 4) * (h.nj + 4) + 255) / 256);
+        for (int t = 0; t < nt; ++t) tl.push_back(c.tile_off + t);
+        for (int t = 0; t < nb; ++t) pb.push_back(c.pblk_off + t);
+        for (int t = 0; t < h.nj; ++t) li.push_back({-(h.ni - h.row_start(t)), c.iline_off + t});
+        for (int t = 0; t < h.ni; ++t) lj.push_back({-(h.nj - h.col_start(t)), c.jline_off + t});
+      }
+      std::sort(tl.begin(), tl.end());
+      std::sort(pb.begin(), pb.end());
+      std::stable_sort(li.begin(), li.end());
+      std::stable_sort(lj.begin(), lj.end());
+      for (auto& p : li) il.push_back(p.second);
+      for (auto& p : lj) jl.push_back(p.second);
+      BK_CUDA(copy_sync(stream, q.d_act, act.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, q.d_tl, tl.data(), tl.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, q.d_pb, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, q.d_il, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
+      BK_CUDA(copy_sync(stream, q.d_jl, jl.data(), jl.size() * sizeof(int), cudaMemcpyHostToDevice));
+      q.n_tl = (int)tl.size(), q.n_pb = (int)pb.size(), q.n_il = (int)il.size(), q.n_jl = (int)jl.size();
+    }
+    ngroups = G;
+    return 0;
+  }
+  // Point the launch state (A with the group's lists and mask, the streams and fork/join events) at group g, or back
+  // (the same call again restores it).
+  void swap_group(Group& q, Arena& saved) {
+    std::swap(stream, q.st);
+    std::swap(side, q.side);
+    std::swap(ev_fork, q.ev_fork);
+    std::swap(ev_join, q.ev_join);
+    std::swap(ev_ends, q.ev_ends);
+    std::swap(A, saved);
   }
 
   // ---------------------------------------------------------------- FAS multigrid (multigrid.rs:72-112)
@@ -1229,7 +1325,23 @@ struct ArenaHost {
       cudaMemsetAsync(A.rsum, 0, (size_t)chunk * nc * sizeof(double), stream);
       if (any_sst) cudaMemsetAsync(A.tsum, 0, (size_t)chunk * nc * sizeof(double), stream);
       capturing = true;
-      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      if (ngroups > 1) {  // one independent chain of iterations per case group, forked from and joined into `stream`
+        cudaEventRecord(ev_split, stream);
+        for (int g = 0; g < ngroups; ++g) {
+          Group& q = grp[g];
+          cudaStreamWaitEvent(q.st, ev_split, 0);
+          Arena ga = A;
+          ga.active = q.d_act, ga.tile_list = q.d_tl, ga.pblk_list = q.d_pb, ga.iline_list = q.d_il, ga.jline_list = q.d_jl;
+          ga.n_tl = q.n_tl, ga.n_pb = q.n_pb, ga.n_il = q.n_il, ga.n_jl = q.n_jl;
+          swap_group(q, ga);
+          for (int k = 0; k < chunk; ++k) launch_iteration(k);
+          swap_group(q, ga);
+          cudaEventRecord(q.ev_done, q.st);
+          cudaStreamWaitEvent(stream, q.ev_done, 0);
+        }
+      } else {
+        for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      }
       capturing = false;
       cudaError_t le = cudaGetLastError();
       BK_CUDA(cudaStreamEndCapture(stream, &g));

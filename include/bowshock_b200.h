@@ -394,6 +394,11 @@ int bowshock_arena_tuning(const bowshock_arena* a, bowshock_line_tuning* out);
  * rounding in the line solves, not their fixed point; the other fields change nothing in the results). Values out of
  * their ranges above give INVALID. No counterpart in the reference. */
 int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t);
+/* No counterpart in the reference. groups (1 to 4, default 1): the active cases are split into that many groups of
+ * about equal cells and each group's iterations form an independent chain in the chunk's CUDA graph, so the groups'
+ * kernels run side by side; the states are those of one group bit for bit (every kernel touches only its own cases),
+ * what changes is how many warps are in flight when few cases are left. */
+int bowshock_arena_set_case_groups(bowshock_arena* a, int groups);
 
 /* ---------------------------------------------------------------------------------------------- 3D Euler
  * The stability path (crates/bowshock-cfd/src/solver3.rs + implicit3.rs behind `GpuSolver3`, gpu/mod.rs:442-560, driven
