@@ -421,8 +421,18 @@ def main():
     ap.add_argument("--report", default=None)
     ap.add_argument("--dataset", default=None, help="an .npz of (X, T) to train on instead of generating")
     ap.add_argument("--save-dataset", default=None)
+    ap.add_argument("--eval-only", action="store_true", help="evaluate the committed network (--out) on the held-out cases, no training")
     args = ap.parse_args()
     rep = {}
+    if args.eval_only:
+        model = WarmStart.load(args.out)
+        ev = evaluate(model, args.eval_cases, HELD_OUT_SEED, args.eval_max_iter)
+        rep["held_out"] = ev
+        print(json.dumps({k: v for k, v in ev.items() if k != "per_case"}), flush=True)
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(rep, f, indent=1)
+        return
     t0 = time.perf_counter()
     if args.dataset:
         z = np.load(args.dataset)
