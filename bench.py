@@ -593,14 +593,14 @@ def run_kernels(args):
         out["ms_per_step"] = out["tma"]["ms_per_step"]
         out["bf16_peak_kind"] = bf16_peak()[1]
         return out
-    if args.workload == "lift3":
+    if args.workload in ("lift3", "lift3s"):  # lift3s: 3 of the 15 cases (4 deg at each Mach), for full ncu captures
         import bowshock_b200.euler3 as e3
-        b, _ = e3.batch_of(e3.lift_sweep_cases())
+        b, _ = e3.batch_of(e3.lift_sweep_cases((4.0,)) if args.workload == "lift3s" else e3.lift_sweep_cases())
         b.run(max(args.warmup, 1))
         torch.cuda.profiler.start()
         b.run(args.steps)
         torch.cuda.profiler.stop()
-        return {"kernels_only": True, "workload": "lift3", "cells": b.nc * b.nb, "steps": args.steps, "ms_per_step": b.ms_per_iter()}
+        return {"kernels_only": True, "workload": args.workload, "cells": b.nc * b.nb, "steps": args.steps, "ms_per_step": b.ms_per_iter()}
     from bowshock_b200.arena import Arena
     cases = build_cases()
     arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
@@ -628,7 +628,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kernels-only", action="store_true", help="only the timed arena iterations (for ncu captures)")
-    ap.add_argument("--workload", default="sweep32", choices=["sweep32", "tail6", "lift3", "net"], help="workload of --kernels-only")
+    ap.add_argument("--workload", default="sweep32", choices=["sweep32", "tail6", "lift3", "lift3s", "net"], help="workload of --kernels-only")
     ap.add_argument("--groups", type=int, default=1, help="case groups of the arena's graph in --kernels-only (1-4)")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
