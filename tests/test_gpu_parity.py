@@ -234,3 +234,32 @@ def test_multigrid_with_smoothed_smoother_matches_oracle():  # MgParams::irs: th
     rg = gpu.run(30)
     assert cases.state_diff(gpu.state_f64(), cpu.u) < 1e-5
     assert cases.residual_diff(rg[:10], rc[:10]) < 1e-3
+
+
+# The same check on every grid of the 32-case sweep (96 x 48 to 320 x 160 cells; cone, ogive and von Karman noses,
+# boattails, sting and base wakes, Euler and RANS SST, M 0.36 to 2.91), from 40 oracle iterations of each case's own
+# numerics (the oracle case of the sweep census, tests/golden/sweep_oracle.py).
+@pytest.mark.parametrize("k", range(32))
+def test_residual_per_cell_on_sweep_grids(k):
+    from bowshock_b200.sweep import sweep_cases
+    from tests.golden.sweep_oracle import oracle_case
+    c = sweep_cases()[k]
+    tol = 2e-5 if c.viscous is None else 1e-4
+    spec = cases.from_case(oracle_case(c), f"sweep case {k}")
+    dev = cases.oracle_solver(spec)
+    dev.steps(40)
+    spec.u0 = dev.u.copy()
+    spec.first_order_iters = 0
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    if spec.viscous is not None:
+        cpu.turb, cpu.mu_t = dev.turb.copy(), dev.mu_t.copy()
+        gpu.set_turb(dev.turb, dev.mu_t)
+    cpu.eval_residual(True)
+    rc, dc = cpu.res, cpu.dt
+    rg, dg, dens = gpu.eval_residual(True)
+    errs = [np.max(np.abs(rg[:, q] - rc[:, q])) / (np.max(np.abs(rc[:, q])) + 1e-30) for q in range(4)]
+    assert max(errs) < tol, f"sweep case {k}: residual max rel err {max(errs):.3e}"
+    fluid = dc > 0
+    assert np.max(np.abs(dg[fluid] - dc[fluid]) / dc[fluid]) < 1e-5
+    assert abs(dens - cpu.density_residual()) / cpu.density_residual() < 1e-4
