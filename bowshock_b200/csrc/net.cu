@@ -764,18 +764,14 @@ static cudaError_t launch_gemm_bn(const CUtensorMap& ta, const CUtensorMap& tb, 
   cudaError_t e;
   if constexpr (KIND != GEMM_WGRAD) {
     if (grid.z == 1 && persistent_gemm) {  // one K split: the persistent kernel over the grid.x x grid.y tiles
-      static int resident = 0, sms = 0;    // CTAs of k_gemm_p<BN, KIND> per SM, SMs of the device
       if ((e = cudaFuncSetAttribute(k_gemm_p<BN, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>())) != cudaSuccess)
         return e;
-      if (!resident) {
-        int dev = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_gemm_p<BN, KIND>, 192, gemm_smem_bytes<BN>())) != cudaSuccess)
-          return e;
-        resident = std::max(resident, 1);
-      }
+      int dev = 0, sms = 0, resident = 0;  // SMs of the device, CTAs of k_gemm_p<BN, KIND> per SM
+      if ((e = cudaGetDevice(&dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+          (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_gemm_p<BN, KIND>, 192, gemm_smem_bytes<BN>())) != cudaSuccess)
+        return e;
       const long long tiles = (long long)grid.x * grid.y;
-      const unsigned ctas = (unsigned)std::min<long long>(tiles, (long long)sms * resident);
+      const unsigned ctas = (unsigned)std::min<long long>(tiles, (long long)sms * std::max(resident, 1));
       k_gemm_p<BN, KIND><<<ctas, 192, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
       return cudaGetLastError();
     }
