@@ -766,12 +766,19 @@ static cudaError_t launch_gemm_bn(const CUtensorMap& ta, const CUtensorMap& tb, 
     if (grid.z == 1 && persistent_gemm) {  // one K split: the persistent kernel over the grid.x x grid.y tiles
       if ((e = cudaFuncSetAttribute(k_gemm_p<BN, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_bytes<BN>())) != cudaSuccess)
         return e;
-      int dev = 0, sms = 0, resident = 0;  // SMs of the device, CTAs of k_gemm_p<BN, KIND> per SM
-      if ((e = cudaGetDevice(&dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-          (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_gemm_p<BN, KIND>, 192, gemm_smem_bytes<BN>())) != cudaSuccess)
-        return e;
+      // SMs of the device x CTAs of k_gemm_p<BN, KIND> per SM, queried once (the grid only needs to be at most that; any
+      // smaller grid gives the same results)
+      static std::once_flag once;
+      static long long slots = 148;
+      std::call_once(once, [] {
+        int dev = 0, sms = 0, resident = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_gemm_p<BN, KIND>, 192, gemm_smem_bytes<BN>()) == cudaSuccess)
+          slots = (long long)sms * std::max(resident, 1);
+        (void)cudaGetLastError();
+      });
       const long long tiles = (long long)grid.x * grid.y;
-      const unsigned ctas = (unsigned)std::min<long long>(tiles, (long long)sms * std::max(resident, 1));
+      const unsigned ctas = (unsigned)std::min<long long>(tiles, slots);
       k_gemm_p<BN, KIND><<<ctas, 192, gemm_smem_bytes<BN>(), st>>>(ta, tb, g);
       return cudaGetLastError();
     }
