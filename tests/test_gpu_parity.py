@@ -263,3 +263,22 @@ def test_residual_per_cell_on_sweep_grids(k):
     fluid = dc > 0
     assert np.max(np.abs(dg[fluid] - dc[fluid]) / dc[fluid]) < 1e-5
     assert abs(dens - cpu.density_residual()) / cpu.density_residual() < 1e-4
+
+
+# The reference's implicit GPU-vs-CPU protocol (implicit.rs:11-35; viscous.rs body check for the SST cases) on sweep
+# grids: each case's own numerics from the free stream, 5 first-order iterations, 30 iterations, the state within 1e-3
+# and the first 5 residuals within 1e-3. Euler and SST, sting and base wakes, sub- and supersonic.
+@pytest.mark.parametrize("k", [0, 1, 2, 7, 13, 18, 21, 24])
+def test_implicit_protocol_on_sweep_grids(k):
+    from bowshock_b200.sweep import sweep_cases
+    from tests.golden.sweep_oracle import oracle_case
+    spec = cases.from_case(oracle_case(sweep_cases()[k]), f"sweep case {k}")
+    spec.first_order_iters = 5
+    cpu = cases.oracle_solver(spec)
+    gpu = cases.gpu_solver(spec)
+    rc = cpu.steps(30)
+    rg = gpu.run(30)
+    d = cases.state_diff(gpu.state_f64(), cpu.u)
+    assert np.all(np.isfinite(rg))
+    assert d < 1e-3, f"{spec.label}: state diff {d:.3e}"
+    assert cases.residual_diff(rg[:5], rc[:5]) < 1e-3
