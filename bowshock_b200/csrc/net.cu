@@ -552,8 +552,10 @@ __global__ void k_grad_prev(const float* __restrict__ dx, int B, int Hin, int Wi
 
 // Masked mean-squared error of the first `nout` channels of out [B*P, CO] against target [B, P, nout]; the gradient
 // 2 (out - t) mask / count into g [B*P, CO] (BF16, zero in the padding channels); the loss summed into *loss.
+// tstep (may be null): the loss goes to loss[*tstep] (a training step replayed from a CUDA graph reads its index here)
 __global__ void k_loss(const float* __restrict__ out, int CO, const float* __restrict__ target, int nout, const uint8_t* __restrict__ mask, int P,
-                       long long rows, float inv_count, bf16* __restrict__ g, float* __restrict__ loss) {
+                       long long rows, float inv_count, bf16* __restrict__ g, float* __restrict__ loss, const int* __restrict__ tstep) {
+  if (tstep) loss += *tstep;
   float acc = 0.f;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < rows * CO; t += (long long)gridDim.x * blockDim.x) {
     const int c = (int)(t % CO);
@@ -571,8 +573,10 @@ __global__ void k_loss(const float* __restrict__ out, int CO, const float* __res
 }
 
 // rows of the device dataset into a batch: x [B, nin] (BF16) and target [B, nt]
+// tstep (may be null): the batch's rows are idx[*tstep * B ..] (a training step replayed from a CUDA graph)
 __global__ void k_gather(const float* __restrict__ dsx, int nin, const float* __restrict__ dst, long long nt, const int* __restrict__ idx, int B,
-                         bf16* __restrict__ x, float* __restrict__ t) {
+                         bf16* __restrict__ x, float* __restrict__ t, const int* __restrict__ tstep) {
+  if (tstep) idx += (long long)(*tstep) * B;
   const long long total = (long long)B * nt;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
     const int b = (int)(q / nt);
@@ -587,7 +591,9 @@ __global__ void k_to_bf16(const float* __restrict__ a, long long n, bf16* __rest
 }
 
 // Adam step count and its bias-corrected learning rate, on the device so that a captured training step replays
-__global__ void k_adam_prep(int* step, float* coef, float lr, float b1, float b2) {
+// (and advances the training-step index tstep of a replayed step, when given)
+__global__ void k_adam_prep(int* step, float* coef, float lr, float b1, float b2, int* tstep) {
+  if (tstep) ++(*tstep);
   const int t = ++(*step);
   coef[0] = lr * sqrtf(1.f - powf(b2, (float)t)) / (1.f - powf(b1, (float)t));
 }
@@ -1035,6 +1041,7 @@ struct Net {
   float* loss1 = nullptr;  // one gradient evaluation
   int* d_err = nullptr;
   int* d_step = nullptr;
+  int* d_tstep = nullptr;  // index of the training step within a bowshock_net_train call (read by a replayed step)
   float* coef = nullptr;
   // dataset on the device
   float *dsx = nullptr, *dst = nullptr, *tb = nullptr;
@@ -1048,7 +1055,7 @@ struct Net {
 
   ~Net() {
     for (void* p : {(void*)w, (void*)gw, (void*)m1, (void*)m2, (void*)wb, (void*)x, (void*)out, (void*)col, (void*)colT, (void*)gT, (void*)wt,
-                    (void*)g0, (void*)g1, (void*)dx, (void*)loss, (void*)loss1, (void*)d_err, (void*)d_step, (void*)coef, (void*)dsx, (void*)dst, (void*)tb,
+                    (void*)g0, (void*)g1, (void*)dx, (void*)loss, (void*)loss1, (void*)d_err, (void*)d_step, (void*)d_tstep, (void*)coef, (void*)dsx, (void*)dst, (void*)tb,
                     (void*)mask, (void*)idx})
       if (p) cudaFree(p);
     for (bf16* a : act)
@@ -1127,6 +1134,7 @@ struct Net {
     NCK(cudaMalloc(&d_err, sizeof(int)));
     NCK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     NCK(cudaMalloc(&d_step, sizeof(int)));
+    NCK(cudaMalloc(&d_tstep, sizeof(int)));
     NCK(cudaMalloc(&coef, sizeof(float)));
     NCK(cudaMalloc(&loss1, sizeof(float)));
     NCK(cudaMalloc(&tb, (size_t)maxB * BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT * 4));
@@ -1209,13 +1217,13 @@ struct Net {
   }
 
   // gradients of the masked loss into gw (zeroed here), from the target batch in tb; loss summed into *loss_slot
-  int backward(int B, float* loss_slot) {
+  int backward(int B, float* loss_slot, const int* tstep = nullptr) {
     int rc;
     NCK(cudaMemsetAsync(gw, 0, nparam * 4, stream));
     const Layer& lo = L.back();
     const long long ro = rows(lo, B);
     const float inv = 1.f / (float)((long long)B * BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT);  // mean over every entry (masked ones are 0)
-    k_loss<<<grid_for(ro * lo.cout), 256, 0, stream>>>(out, lo.cout, tb, BOWSHOCK_NET_OUT, mask, BOWSHOCK_NET_CELLS, ro, inv, g0, loss_slot);
+    k_loss<<<grid_for(ro * lo.cout), 256, 0, stream>>>(out, lo.cout, tb, BOWSHOCK_NET_OUT, mask, BOWSHOCK_NET_CELLS, ro, inv, g0, loss_slot, tstep);
     bf16 *g = g0, *gnext = g1;
     for (int k = (int)L.size() - 1; k >= 0; --k) {
       const Layer& l = L[k];
@@ -1291,19 +1299,21 @@ struct Net {
     return 0;
   }
 
-  void adam(float lr) {
-    k_adam_prep<<<1, 1, 0, stream>>>(d_step, coef, lr, 0.9f, 0.999f);
+  void adam(float lr, int* tstep = nullptr) {
+    k_adam_prep<<<1, 1, 0, stream>>>(d_step, coef, lr, 0.9f, 0.999f, tstep);
     k_adam<<<grid_for(nparam), 256, 0, stream>>>(w, m1, m2, gw, nparam, coef, 0.9f, 0.999f, 1e-8f, wb);
   }
 
   // one training step of batch B on the dataset rows idx_dev[0..B): gather, forward, loss, backward, Adam
-  int train_step(int B, const int* idx_dev, float lr, float* loss_slot) {
+  // tstep (may be null): idx_dev and loss_slot are the bases of every step's indices and losses, offset on the device by
+  // the step index *tstep, which the step advances (so that one captured step replays as every step)
+  int train_step(int B, const int* idx_dev, float lr, float* loss_slot, int* tstep = nullptr) {
     k_gather<<<grid_for((long long)B * BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT), 256, 0, stream>>>(
-        dsx, BOWSHOCK_NET_IN, dst, (long long)BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT, idx_dev, B, x, tb);
+        dsx, BOWSHOCK_NET_IN, dst, (long long)BOWSHOCK_NET_CELLS * BOWSHOCK_NET_OUT, idx_dev, B, x, tb, tstep);
     int rc;
     if ((rc = forward(B))) return rc;
-    if ((rc = backward(B, loss_slot))) return rc;
-    adam(lr);
+    if ((rc = backward(B, loss_slot, tstep))) return rc;
+    adam(lr, tstep);
     NCK(cudaGetLastError());
     return 0;
   }
@@ -1492,10 +1502,28 @@ int bowshock_net_train(bowshock_net* h, uint64_t steps, uint64_t batch, double l
   NET_CK(h, cudaEventCreate(&e0));
   NET_CK(h, cudaEventCreate(&e1));
   int rc = 0;
+  // one step captured as a CUDA graph and replayed `steps` times (the step index, on the device, offsets each replay's
+  // batch indices and loss slot); the steps launched one by one if the capture fails
+  NET_CK(h, cudaMemsetAsync(n.d_tstep, 0, sizeof(int), n.stream));
+  cudaGraphExec_t step_graph = nullptr;
+  if (cudaStreamBeginCapture(n.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    const int crc = n.train_step(B, n.idx, (float)lr, n.loss, n.d_tstep);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(n.stream, &g);
+    if (!crc && ce == cudaSuccess && g && cudaGraphInstantiate(&step_graph, g, 0) != cudaSuccess) step_graph = nullptr;
+    if (g) cudaGraphDestroy(g);
+    (void)cudaGetLastError();  // a failed capture leaves the loop below to run (and report) the steps one by one
+    n.err.clear();
+  }
   NET_CK(h, cudaEventRecord(e0, n.stream));
-  for (uint64_t s = 0; s < steps && !rc; ++s) rc = n.train_step(B, n.idx + s * B, (float)lr, n.loss + s);
+  if (step_graph) {
+    for (uint64_t s = 0; s < steps; ++s) NET_CK(h, cudaGraphLaunch(step_graph, n.stream));
+  } else {
+    for (uint64_t s = 0; s < steps && !rc; ++s) rc = n.train_step(B, n.idx + s * B, (float)lr, n.loss + s);
+  }
   NET_CK(h, cudaEventRecord(e1, n.stream));
   NET_CK(h, cudaStreamSynchronize(n.stream));
+  if (step_graph) cudaGraphExecDestroy(step_graph);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
   n.last_ms = ms;
