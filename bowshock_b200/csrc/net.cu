@@ -1517,7 +1517,16 @@ int bowshock_net_train(bowshock_net* h, uint64_t steps, uint64_t batch, double l
   }
   NET_CK(h, cudaEventRecord(e0, n.stream));
   if (step_graph) {
-    for (uint64_t s = 0; s < steps; ++s) NET_CK(h, cudaGraphLaunch(step_graph, n.stream));
+    cudaError_t le = cudaSuccess;
+    for (uint64_t s = 0; s < steps && le == cudaSuccess; ++s) le = cudaGraphLaunch(step_graph, n.stream);
+    if (le != cudaSuccess) {
+      cudaStreamSynchronize(n.stream);
+      cudaGraphExecDestroy(step_graph);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      n.err = std::string("cudaGraphLaunch: ") + cudaGetErrorString(le);
+      return BOWSHOCK_CUDA_ERROR;
+    }
   } else {
     for (uint64_t s = 0; s < steps && !rc; ++s) rc = n.train_step(B, n.idx + s * B, (float)lr, n.loss + s);
   }
