@@ -343,6 +343,7 @@ def run_ours(args, rank, world, dist):
     learned = secondary(learned_census, all_cases, all_grids, fx, plain_cases_per_hr, device) if world == 1 else None
     lift3 = secondary(measure_lift3, args, device) if world == 1 else None
     mg0 = secondary(measure_multigrid, device) if world == 1 else None
+    mesh = secondary(measure_mesher, device) if world == 1 else None
     cpu_base = None
     if world == 1:  # the CPU baseline: the oracle on a bounded sample (3 iterations of every case), x its own iteration counts
         smp = OracleSample(all_cases)
@@ -384,6 +385,7 @@ def run_ours(args, rank, world, dist):
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "autotuned_lines_per_block": tuning,
             "lift3": lift3,
+            "device_mesher": mesh,
             "multigrid": mg0,
             "parallelism": (f"cases partitioned over {world} GPUs (longest-processing-time on cells x expected iterations), results "
                             "gathered" if world > 1 else "one GPU, one batched arena"),
@@ -541,6 +543,25 @@ def measure_multigrid(device):
             del s
         o["dcd_multigrid_vs_single"] = o["multigrid3"]["cd_total"] - o["single_grid"]["cd_total"]
     return out
+
+
+def measure_mesher(device):
+    """The grids of 2,000 SST cases of the sweep's distribution (the learned warm start's training set, seed 0x0B05_7EA1)
+    built by the device mesher (nodes and FP64 metrics, bowshock_mesh_batch: device time of its launches, and wall
+    clock with the copies back) against the host mesher (nodes only, one case at a time through the C ABI)."""
+    from bowshock_b200 import learned as lw
+    from bowshock_b200.case import mesh_batch
+    cs = [lw.sweep_case(p) for p in lw.draw_sst(2000, lw.TRAIN_SEED)]
+    mesh_batch(cs[:8], device=device)  # module load
+    t0 = time.perf_counter()
+    grids, _, dev_ms = mesh_batch(cs, device=device)
+    wall = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for c in cs:
+        c.grid()
+    host = time.perf_counter() - t0
+    nodes = sum((g[0] + 1) * (g[1] + 1) for g in grids)
+    return {"cases": len(cs), "nodes": int(nodes), "device_ms": dev_ms, "device_wall_s": wall, "host_nodes_only_s": host}
 
 
 def line_sweep_traffic():
