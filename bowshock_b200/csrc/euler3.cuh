@@ -16,6 +16,7 @@
 //   k3_stage      SSP-RK3 stage                                                       (solver3.rs:303-327)
 //   k3_forces     FP64 wall-pressure force integration: CN, CA, centre of pressure     (run3.rs:150-190)
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -592,10 +593,16 @@ __device__ __forceinline__ void damped_update3(const B3& B, int b, long long c, 
   }
 }
 
-// Line records of case b, direction dir: 130 planes of ncell floats: lo (25), d (25), up (25) assembled by k3_assemble;
-// M^-1 (25), Y = M^-1 up (25) by the factorising pass; g (5), the forward sweep of the current right-hand side.
+// Line records of case b, direction dir, in a region of 130 planes of ncell floats: the blocks lo (25), d (25), up (25)
+// assembled by k3_assemble and the factors M^-1 (25), Y = M^-1 up (25) of the factorising pass as 125 planes of ncell
+// FP16 values at the start of the region (half its first 125 float planes), and g (5 FP32 planes from plane R_G), the
+// forward sweep of the current right-hand side. FP16 halves the bytes the assembly writes and the line passes and the
+// defect read; the blocks and factors only precondition the defect correction (the fixed point is the residual's), and
+// their entries (the blocks of I - dt J at CFL <= 10, the inverse and the Y of a diagonally dominant block) lie far
+// inside FP16's range.
 constexpr int REC3 = 130, R_LO = 0, R_D = 25, R_UP = 50, R_MINV = 75, R_Y = 100, R_G = 125;
 __device__ __forceinline__ float* rec3(const B3& B, int b, int dir) { return B.scr + ((long long)b * 3 + dir) * REC3 * B.nc; }
+__device__ __forceinline__ __half* rec3h(const B3& B, int b, int dir) { return reinterpret_cast<__half*>(rec3(B, b, dir)); }
 // Index of cell (i, j, k) in the records of direction dir: the i-direction records are transposed (j fastest) so that the
 // threads of neighbouring i lines, which walk the lines side by side, read neighbouring addresses.
 __device__ __forceinline__ long long rcell(const B3& B, int dir, int i, int j, int k) {
@@ -610,6 +617,16 @@ __device__ __forceinline__ M5<float> ld5(const float* p, long long stride) {
 __device__ __forceinline__ void st5(float* p, long long stride, const M5<float>& m) {
 #pragma unroll
   for (int q = 0; q < 25; ++q) p[q * stride] = m[q];
+}
+__device__ __forceinline__ M5<float> ld5(const __half* p, long long stride) {
+  M5<float> m;
+#pragma unroll
+  for (int q = 0; q < 25; ++q) m[q] = __half2float(p[q * stride]);
+  return m;
+}
+__device__ __forceinline__ void st5(__half* p, long long stride, const M5<float>& m) {
+#pragma unroll
+  for (int q = 0; q < 25; ++q) p[q * stride] = __float2half_rn(m[q]);
 }
 
 // Blocks of every cell into the line records (thread per cell). part 0: the i direction, threads ordered j fastest so that
@@ -628,7 +645,7 @@ __global__ void __launch_bounds__(128, 4) k3_assemble(B3 B, int part) {
   for (int dir = part == 0 ? 0 : 1; dir < (part == 0 ? 1 : 3); ++dir) {
     M5<float> lo, d, up;
     blocks3(B, b, dir, i, j, k, lo, d, up);
-    float* r = rec3(B, b, dir) + rcell(B, dir, i, j, k);
+    __half* r = rec3h(B, b, dir) + rcell(B, dir, i, j, k);
     st5(r + R_LO * B.nc, B.nc, lo);
     st5(r + R_D * B.nc, B.nc, d);
     st5(r + R_UP * B.nc, B.nc, up);
@@ -679,13 +696,14 @@ __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, i
   long long c0, stride, r0, rs;
   int n;
   line3(B, dir, L, c0, stride, n, r0, rs);
-  float* R = rec3(B, b, dir) + r0;
+  float* R = rec3(B, b, dir) + r0;        // g (FP32 planes)
+  __half* H = rec3h(B, b, dir) + r0;      // blocks and factors (FP16 planes)
   const long long nc = B.nc;
   M5<float> Y = zero5();
   V5<float> g{{0, 0, 0, 0, 0}};
   for (int m = 0; m < n; ++m) {
     long long c = c0 + m * stride, rr = m * rs;
-    M5<float> d = ld5(R + R_D * nc + rr, nc);
+    M5<float> d = ld5(H + R_D * nc + rr, nc);
     V5<float> r = ldU(B, in, b, c);
     if (from_res) {
       float dtc = B.dt[(long long)b * nc + c];
@@ -693,7 +711,7 @@ __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, i
       for (int q = 0; q < 5; ++q) r[q] *= dtc;
     }
     if (m > 0) {
-      M5<float> lo = ld5(R + R_LO * nc + rr, nc);
+      M5<float> lo = ld5(H + R_LO * nc + rr, nc);
       axpy5(d, -1.f, mm5(lo, Y));
       V5<float> t = mv5(lo, g);
 #pragma unroll
@@ -701,9 +719,9 @@ __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, i
     }
     M5<float> Minv = inv5(d);
     g = mv5(Minv, r);
-    Y = mm5(Minv, ld5(R + R_UP * nc + rr, nc));
-    st5(R + R_MINV * nc + rr, nc, Minv);
-    st5(R + R_Y * nc + rr, nc, Y);
+    Y = mm5(Minv, ld5(H + R_UP * nc + rr, nc));
+    st5(H + R_MINV * nc + rr, nc, Minv);
+    st5(H + R_Y * nc + rr, nc, Y);
 #pragma unroll
     for (int q = 0; q < 5; ++q) R[(R_G + q) * nc + rr] = g[q];
   }
@@ -711,7 +729,7 @@ __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, i
   emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
   for (int m = n - 2; m >= 0; --m) {
     long long c = c0 + m * stride, rr = m * rs;
-    M5<float> Ym = ld5(R + R_Y * nc + rr, nc);
+    M5<float> Ym = ld5(H + R_Y * nc + rr, nc);
     V5<float> gm;
 #pragma unroll
     for (int q = 0; q < 5; ++q) gm[q] = R[(R_G + q) * nc + rr];
@@ -737,11 +755,12 @@ __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float
   long long c0, stride, r0, rs;
   int n;
   line3(B, dir, L, c0, stride, n, r0, rs);
-  float* R = rec3(B, b, dir) + r0;
+  float* R = rec3(B, b, dir) + r0;        // g (FP32 planes)
+  __half* H = rec3h(B, b, dir) + r0;      // blocks and factors (FP16 planes)
   const long long nc = B.nc;
   // both walks load the next cell's factors before the arithmetic of the current one (software pipelining)
   V5<float> g{{0, 0, 0, 0, 0}};
-  M5<float> lo_n = ld5(R + R_LO * nc, nc), mi_n = ld5(R + R_MINV * nc, nc);
+  M5<float> lo_n = ld5(H + R_LO * nc, nc), mi_n = ld5(H + R_MINV * nc, nc);
   V5<float> r_n = ldU(B, in, b, c0);
   for (int m = 0; m < n; ++m) {
     const long long rr = m * rs;
@@ -749,7 +768,7 @@ __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float
     V5<float> r = r_n;
     if (m + 1 < n) {
       const long long rn = (m + 1) * rs;
-      lo_n = ld5(R + R_LO * nc + rn, nc), mi_n = ld5(R + R_MINV * nc + rn, nc);
+      lo_n = ld5(H + R_LO * nc + rn, nc), mi_n = ld5(H + R_MINV * nc + rn, nc);
       r_n = ldU(B, in, b, c0 + (m + 1) * stride);
     }
     if (m > 0) {
@@ -764,7 +783,7 @@ __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float
   V5<float> xn = g;
   emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
   if (n >= 2) {
-    M5<float> y_n = ld5(R + R_Y * nc + (n - 2) * rs, nc);
+    M5<float> y_n = ld5(H + R_Y * nc + (n - 2) * rs, nc);
     V5<float> g_n;
 #pragma unroll
     for (int q = 0; q < 5; ++q) g_n[q] = R[(R_G + q) * nc + (n - 2) * rs];
@@ -774,7 +793,7 @@ __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float
       V5<float> gm = g_n;
       if (m > 0) {
         const long long rn = (m - 1) * rs;
-        y_n = ld5(R + R_Y * nc + rn, nc);
+        y_n = ld5(H + R_Y * nc + rn, nc);
 #pragma unroll
         for (int q = 0; q < 5; ++q) g_n[q] = R[(R_G + q) * nc + rn];
       }
@@ -791,17 +810,17 @@ __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float
 // A_dir du of cell (i, j, k) with the kept blocks of direction dir (implicit3.rs:384-410)
 __device__ __forceinline__ V5<float> apply3(const B3& B, int b, int dir, int i, int j, int k, long long c, const V5<float>& du) {
   const long long nc = B.nc;
-  const float* R = rec3(B, b, dir) + rcell(B, dir, i, j, k);
+  const __half* H = rec3h(B, b, dir) + rcell(B, dir, i, j, k);
   const int m = dir == 0 ? i : dir == 1 ? j : k, nl = dir == 0 ? B.ni : dir == 1 ? B.nj : B.nk;
   const long long stride = dir == 0 ? 1 : dir == 1 ? B.ni : (long long)B.ni * B.nj;
-  V5<float> v = mv5(ld5(R + R_D * nc, nc), du);
+  V5<float> v = mv5(ld5(H + R_D * nc, nc), du);
   if (m > 0) {
-    V5<float> t = mv5(ld5(R + R_LO * nc, nc), ldU(B, B.DU, b, c - stride));
+    V5<float> t = mv5(ld5(H + R_LO * nc, nc), ldU(B, B.DU, b, c - stride));
 #pragma unroll
     for (int q = 0; q < 5; ++q) v[q] += t[q];
   }
   if (m + 1 < nl) {
-    V5<float> t = mv5(ld5(R + R_UP * nc, nc), ldU(B, B.DU, b, c + stride));
+    V5<float> t = mv5(ld5(H + R_UP * nc, nc), ldU(B, B.DU, b, c + stride));
 #pragma unroll
     for (int q = 0; q < 5; ++q) v[q] += t[q];
   }
