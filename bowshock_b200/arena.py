@@ -172,6 +172,12 @@ class Arena:
         self._check(_ffi.load().bowshock_arena_residual_history(self._h, int(k), _ffi.dptr(out), n.value, C.byref(n)))
         return out
 
+    def set_sst_coupling(self, coupled: bool):
+        """SST line systems of the implicit scheme: False (default) the reference's loose coupling (mean-flow 4x4
+        lines, then the scalar k and omega lines); True the 6x6 block lines of (dU, dk, domega), solved by block
+        substitution (same residuals and fixed point, another iteration path)."""
+        self._check(_ffi.load().bowshock_arena_set_sst_coupling(self._h, int(bool(coupled))))
+
     def set_run_control(self, on_device: bool):
         """Stop rules of solve() on the device after every chunk (True, the default) or on the host (False)."""
         self._check(_ffi.load().bowshock_arena_set_run_control(self._h, int(bool(on_device))))

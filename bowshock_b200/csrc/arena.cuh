@@ -93,6 +93,9 @@ struct Arena {
   float2* trhs;    // SST right-hand side / solution per cell
   float4* grad_kw; // (k_x, k_r, omega_x, omega_r)
   float2* blend;   // (F1, X)
+  // coupled SST lines: per cell the derivatives of V R_k, V R_omega with respect to the mass fluxes of the cell's four
+  // faces and to its density, 3 per cell (null: loosely coupled, the reference's scheme)
+  float4* tcpl;
   // FP64-derived stencil of every face: (|d|, e_x, e_r, 0) between the two side positions (viscous.rs:233-250)
   const float4 *ifs, *jfs;
   // FAS multigrid: the restricted state at the start of a coarse cycle, and the user's mask the level masks derive from

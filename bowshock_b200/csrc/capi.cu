@@ -779,6 +779,15 @@ int bowshock_arena_set_case_groups(bowshock_arena* a, int groups) {
   return BOWSHOCK_OK;
 }
 
+int bowshock_arena_set_sst_coupling(bowshock_arena* a, int coupled) {
+  if (!a) return BOWSHOCK_INVALID;
+  if (a->ar.set_sst_coupled(coupled != 0)) {
+    a->last_error = a->ar.err;
+    return BOWSHOCK_CUDA_ERROR;
+  }
+  return BOWSHOCK_OK;
+}
+
 int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t) {
   if (!a || !t) return BOWSHOCK_INVALID;
   auto w4 = [](int32_t w) { return w == 1 || w == 2 || w == 4; };
@@ -986,6 +995,11 @@ extern "C" int bowshock_solver_set_run_control(bowshock_solver* s, int on_device
   if (!s) return BOWSHOCK_INVALID;
   s->ar.device_run_control = on_device != 0;
   return BOWSHOCK_OK;
+}
+
+extern "C" int bowshock_solver_set_sst_coupling(bowshock_solver* s, int coupled) {
+  if (!s) return BOWSHOCK_INVALID;
+  return from_arena(s, s->ar.set_sst_coupled(coupled != 0));
 }
 
 extern "C" int bowshock_solver_set_ramp(bowshock_solver* s, uint64_t ramp_k) {

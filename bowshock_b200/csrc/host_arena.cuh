@@ -339,6 +339,8 @@ struct ArenaHost {
   // 44 float4 per lane of every line
   size_t scratch_floats() const { return 4 * ((size_t)2 * rec_dir_stride(ncell) + (size_t)(nil + njl) * 32 * PREC); }
   bool any_viscous = false, any_sst = false, any_rough = false;
+  // coupled SST lines (k_turb_couple) instead of the reference's loose coupling; A.tcpl is allocated on the first switch
+  bool sst_coupled = false;
   // device buffers
   Arena A{};
   CaseDev* d_cases = nullptr;
@@ -377,7 +379,7 @@ struct ArenaHost {
                     A.FORCE, A.dt, (void*)A.iface, (void*)A.jface, (void*)A.cellg, (void*)A.ifc, (void*)A.jfc, A.scratch, A.rsum,
                     A.grad4, A.gradT, A.mu, A.mu_t, A.rough, A.fvi, A.fvj, A.turb, A.turb_new, A.dwall, A.mflux_i, A.mflux_j, A.tsum, A.tcoef,
                     A.trhs, A.grad_kw, A.blend, (void*)A.ifs, (void*)A.jfs, A.MG0, d_enabled, d_tlist, d_pblist, d_illist, d_jllist,
-                    A.lend, A.irs_eps, A.irs_c, (void*)A.wmaps};
+                    A.lend, A.irs_eps, A.irs_c, (void*)A.wmaps, A.tcpl};
     d_enabled = nullptr;
     d_tlist = d_pblist = d_illist = d_jllist = nullptr;
     for (void* p : ptrs)
@@ -696,6 +698,7 @@ struct ArenaHost {
       BK_CUDA(cudaMemsetAsync(A.mflux_i, 0, nif * sizeof(float), stream));
       BK_CUDA(cudaMemsetAsync(A.mflux_j, 0, njf * sizeof(float), stream));
     }
+    if (any_sst && sst_coupled && !A.tcpl) ALLOC(A.tcpl, 3 * ncell);
     if ((rc = upload_stencils())) return rc;
     BK_CUDA(copy_sync(stream, d_cases, desc.data(), desc.size() * sizeof(CaseDev), cudaMemcpyHostToDevice));
     if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
@@ -1094,8 +1097,18 @@ struct ArenaHost {
   // turbulence.rs:542-581, from this iteration's primitives, mass fluxes, gradients and time step: the SST update up to
   // its final step
   void launch_turb_chain(cudaStream_t st, int slot) {
+    launch_turb_terms(st, slot);
+    launch_turb_solves(st);
+  }
+  void launch_turb_terms(cudaStream_t st, int slot) {
     L(G_TURB, [&] { k_turb_grad<<<LT(), TI * TJ, 0, st>>>(A); });
-    L(G_TURB, [&] { k_turb_cell<<<LT(), TI * TJ, 0, st>>>(A, slot); });
+    if (sst_coupled && A.tcpl)
+      L(G_TURB, [&] { k_turb_cell<true><<<LT(), TI * TJ, 0, st>>>(A, slot); });
+    else
+      L(G_TURB, [&] { k_turb_cell<false><<<LT(), TI * TJ, 0, st>>>(A, slot); });
+  }
+  // the two scalar line systems (with the coupled lines, after k_turb_couple on the mean flow's stream)
+  void launch_turb_solves(cudaStream_t st) {
     if (max_line <= 32 * TL_MAXM) {
       L(G_TURB_LINES, [&] { launch_turb_lines(1, st); });
       L(G_TURB_LINES, [&] { launch_turb_lines(0, st); });
@@ -1193,6 +1206,16 @@ struct ArenaHost {
       L(G_VISC, [&] { k_visc_face<<<LT(), TI * TJ, 0, stream>>>(A); });
     }
   }
+  // Switches between the coupled SST lines and the reference's loosely coupled ones (for the next chunk on).
+  int set_sst_coupled(bool on) {
+    sst_coupled = on;
+    if (on && any_sst && !A.tcpl) {
+      int rc = dalloc(&A.tcpl, 3 * (size_t)ncell, err);
+      if (rc) return rc;
+    }
+    if (graph) cudaGraphExecDestroy(graph), graph = nullptr;
+    return 0;
+  }
   int scheme_of_arena() const { return desc.empty() ? 0 : desc[0].scheme; }
   int sub_iters_of_arena() const {
     int s = 1;
@@ -1225,10 +1248,14 @@ struct ArenaHost {
     // the SST chain on the graph's second branch (only the warp-per-line SST kernel: the thread-per-line one borrows
     // the line records)
     const bool fork = any_sst && capturing && !profiling && max_line <= 32 * TL_MAXM;
+    const bool coupled = any_sst && sst_coupled && A.tcpl;
     if (fork) {
       cudaEventRecord(ev_fork, stream);
       cudaStreamWaitEvent(side, ev_fork, 0);
-      launch_turb_chain(side, slot);
+      if (coupled)  // the line solves need the mean flow's increment: only the terms run beside the mean flow
+        launch_turb_terms(side, slot);
+      else
+        launch_turb_chain(side, slot);
       cudaEventRecord(ev_join, side);
     }
     L(G_ASSEMBLE, [&] {
@@ -1246,8 +1273,14 @@ struct ArenaHost {
     if (any_sst) {
       if (fork)
         cudaStreamWaitEvent(stream, ev_join, 0);
+      else if (coupled)
+        launch_turb_terms(stream, slot);
       else
         launch_turb_chain(stream, slot);
+      if (coupled) {
+        L(G_TURB, [&] { k_turb_couple<<<LT(), TI * TJ, 0, stream>>>(A); });
+        launch_turb_solves(stream);
+      }
       L(G_TURB, [&] { k_turb_update<<<LT(), TI * TJ, 0, stream>>>(A); });
     }
   }

@@ -164,6 +164,9 @@ __device__ __forceinline__ float strain2(float4 g, float v, float r) {  // turbu
 // Cell terms and line coefficients (turbulence.rs:477-519, 559-579). Coefficients per cell:
 //   tcoef[3c+0] = (lo_i k, lo_i w, up_i k, up_i w), [3c+1] = (d_i k, d_i w, lo_j k / d0k, lo_j w / d0w),
 //   [3c+2] = (up_j k / d0k, up_j w / d0w, d_j k, d_j w); trhs[c] = V R (the i-line right-hand side).
+// CPL: also store the coupling derivatives of the coupled SST lines (A.tcpl); the loosely coupled instance compiles
+// without them.
+template <bool CPL>
 __global__ void k_turb_cell(Arena A, int slot) {
   __shared__ double sred[TI * TJ / 32];
   __shared__ TFaceD sFI[TJ][TI + 1];  // the tile's face data, each face once (turbulence.rs:413-435)
@@ -203,6 +206,8 @@ __global__ void k_turb_cell(Arena A, int slot) {
       A.tcoef[3 * cc + 1] = make_float4(1.f, 1.f, 0.f, 0.f);
       A.tcoef[3 * cc + 2] = make_float4(0.f, 0.f, 1.f, 1.f);
       A.trhs[cc] = make_float2(0.f, 0.f);
+      if constexpr (CPL)
+        for (int q3 = 0; q3 < 3; ++q3) A.tcpl[3 * cc + q3] = make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
       float4 g = A.cellg[cc];
       float vol = g.x;
@@ -225,6 +230,7 @@ __global__ void k_turb_cell(Arena A, int slot) {
       bool ends_up[2] = {i == c.ni - 1, j == c.nj - 1};
       float rate0 = 0.f, rate1 = 0.f;
       float lo[2][2], dd[2][2], up[2][2];
+      float4 cpl[2] = {};
 #pragma unroll
       for (int dir = 0; dir < 2; ++dir) {
         const TFaceD& lf = fa[2 * dir];
@@ -238,6 +244,11 @@ __global__ void k_turb_cell(Arena A, int slot) {
         up[dir][1] = ends_up[dir] ? 0.f : -(a_up + uf.g1);
         dd[dir][0] = a_lo + a_up + lf.g0 + uf.g0;
         dd[dir][1] = a_lo + a_up + lf.g1 + uf.g1;
+        if constexpr (CPL) {
+          // d(rate)/d(m) of the two faces: inflow through the lower face (m > 0), through the upper face (m < 0)
+          const bool cl = !ends_lo[dir] && lf.m > 0.f, cu = !ends_up[dir] && uf.m < 0.f;
+          cpl[dir] = make_float4(cl ? lf.l.x - kw.x : 0.f, cl ? lf.l.y - kw.y : 0.f, cu ? kw.x - uf.r.x : 0.f, cu ? kw.y - uf.r.y : 0.f);
+        }
       }
       float r0 = rate0 / vol + src0, r1 = rate1 / vol + src1;
       float dtc = A.dt[cc];
@@ -246,6 +257,17 @@ __global__ void k_turb_cell(Arena A, int slot) {
       A.tcoef[3 * cc + 1] = make_float4(d00 + dd[0][0], d01 + dd[0][1], lo[1][0] / d00, lo[1][1] / d01);
       A.tcoef[3 * cc + 2] = make_float4(up[1][0] / d00, up[1][1] / d01, 1.f + dd[1][0] / d00, 1.f + dd[1][1] / d01);
       A.trhs[cc] = make_float2(vol * r0, vol * r1);
+      if constexpr (CPL) {
+        // d(V source)/d(rho) with mu_t, F1 and the strain frozen: the production limiter's branch, the destruction
+        // terms, and the cross-diffusion term (linear in rho)
+        const bool lim = mut_c * s2 > 10.f * BETA_STAR * rho * kw.x * kw.y;
+        const float dprod = lim ? 10.f * BETA_STAR * kw.x * kw.y : 0.f;
+        const float ds0 = dprod - BETA_STAR * kw.y * kw.x;
+        const float ds1 = gamma * (prod + rho * dprod) / fmaxf(mut_c, 1e-30f) - beta * kw.y * kw.y + (1.f - f1) * bl.y / rho;
+        A.tcpl[3 * cc] = cpl[0];
+        A.tcpl[3 * cc + 1] = cpl[1];
+        A.tcpl[3 * cc + 2] = make_float4(vol * ds0, vol * ds1, 0.f, 0.f);
+      }
       rr = (double)r0 * (double)r0;
     }
   }
@@ -451,6 +473,61 @@ __global__ void __launch_bounds__(32 * W) k_turb_lines_w(Arena A, int dir_i) {
       xn = x;
     }
   }
+}
+
+// Coupled SST lines (an option beside the reference's loose coupling). Unknowns per cell: the mean-flow increment dU (4)
+// and (dk, domega), so the line blocks are 6x6. The mean-flow rows do not depend on k and omega, because the mean-flow
+// operator freezes mu_t (implicit.rs: the viscous Jacobian takes mu + mu_t as given), so every 6x6 block is lower
+// block-triangular and the line system is solved exactly by block substitution: the 4x4 mean-flow lines first, then the
+// turbulence rows with their coupling to dU moved to the right-hand side,
+//   M_tt x = V R_t + (d(V R_t)/dU) dU,
+// M_tt being the reference's two scalar line systems (same approximate factorisation, i then j). The coupling block
+// holds what V R_t depends on through the mean-flow state on the line stencil: the mass flux m of each interior face
+// of the cell's convection terms (d rate / d m from k_turb_cell, m linearised as the first row of the Rusanov-split
+// flux Jacobian, dm = w/2 [n.(d(rho u)_L + d(rho u)_R) + lambda (d rho_L - d rho_R)], lambda = |u_n| + c of the face
+// average), and the cell's density in its sources. The strain's dependence on the velocity gradients (a wider stencil)
+// is left out, as the mean-flow operator leaves out its viscous cross terms. The residuals are the reference's, so the
+// fixed point is the loosely coupled scheme's; only the path to it changes.
+__device__ __forceinline__ float dmass(const Arena& A, float4 f, long long cl, long long pl, long long cr, long long pr) {
+  const float4 wl = A.W[pl], wr = A.W[pr];
+  const float4 dl = A.DU[cl], dr = A.DU[cr];
+  const float rho = 0.5f * (wl.x + wr.x), p = 0.5f * (wl.w + wr.w);
+  const float un = 0.5f * ((wl.y + wr.y) * f.x + (wl.z + wr.z) * f.y);
+  const float lam = fabsf(un) + sqrtf(1.4f * p / rho);
+  return 0.5f * f.w * (f.x * (dl.y + dr.y) + f.y * (dl.z + dr.z) + lam * (dl.x - dr.x));
+}
+
+// Adds (d(V R_t)/dU) dU to the turbulence right-hand side of every fluid cell of an SST case, after the mean-flow line
+// solves have left the full increment dU in DU and before the turbulence line solves.
+__global__ void k_turb_couple(Arena A) {
+  int t = tile_at(A);
+  int ci = A.tile_case[t];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci] || !c.sst) return;
+  int lt = t - c.tile_off;
+  int i = (lt % c.ntx) * TI + threadIdx.x % TI, j = (lt / c.ntx) * TJ + threadIdx.x / TI;
+  if (i >= c.ni || j >= c.nj || is_solid(c, i, j)) return;
+  const long long cc = cidx(c, i, j), pc = pidx(c, i, j);
+  const float4 a = A.tcpl[3 * cc], b = A.tcpl[3 * cc + 1], s = A.tcpl[3 * cc + 2];
+  float add0 = s.x * A.DU[cc].x, add1 = s.y * A.DU[cc].x;
+  if (i > row_start(c, j)) {
+    const float dm = dmass(A, A.iface[ifidx(c, i, j)], cidx(c, i - 1, j), pidx(c, i - 1, j), cc, pc);
+    add0 += a.x * dm, add1 += a.y * dm;
+  }
+  if (i < c.ni - 1) {
+    const float dm = dmass(A, A.iface[ifidx(c, i + 1, j)], cc, pc, cidx(c, i + 1, j), pidx(c, i + 1, j));
+    add0 += a.z * dm, add1 += a.w * dm;
+  }
+  if (j > col_start(c, i)) {
+    const float dm = dmass(A, A.jface[jfidx(c, i, j)], cidx(c, i, j - 1), pidx(c, i, j - 1), cc, pc);
+    add0 += b.x * dm, add1 += b.y * dm;
+  }
+  if (j < c.nj - 1) {
+    const float dm = dmass(A, A.jface[jfidx(c, i, j + 1)], cc, pc, cidx(c, i, j + 1), pidx(c, i, j + 1));
+    add0 += b.z * dm, add1 += b.w * dm;
+  }
+  const float2 x = A.trhs[cc];
+  A.trhs[cc] = make_float2(x.x + add0, x.y + add1);
 }
 
 __global__ void k_turb_update(Arena A) {  // turbulence.rs:584-603

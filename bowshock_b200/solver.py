@@ -139,6 +139,10 @@ class GpuSolver:
     def set_low_mach(self, on: bool):
         self._check(_ffi.load().bowshock_solver_set_low_mach(self._h, int(bool(on))))
 
+    def set_sst_coupling(self, coupled: bool):
+        """False (default): the reference's loosely coupled SST lines; True: the 6x6 block lines (Arena.set_sst_coupling)."""
+        self._check(_ffi.load().bowshock_solver_set_sst_coupling(self._h, int(bool(coupled))))
+
     def set_block(self, block):
         """`block`: None or (i_end, j_end, j_sting)."""
         if block is None:
