@@ -631,6 +631,8 @@ def lib3():
             "orc3_inv5": (None, [dp, dp]),
             "orc3_block_thomas5": (None, [U, dp, dp, dp, dp]),
             "orc3_reflection": (None, [dp, dp]),
+            "orc3_set_solid": (None, [P, U, C.POINTER(U)]),
+            "orc3_face_fluxes": (U, [P, I, dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -789,6 +791,18 @@ class Solver3:
 
     def set_iter(self, it, ramp=None):
         lib3().orc3_set_iter(self._h, it, it if ramp is None else ramp)
+
+    def set_solid(self, boxes):
+        """Solid boxes (grid3.rs:17-24 `SolidBox`): ((i0, i1), (j0, j1), (k0, k1)) half-open cell ranges each."""
+        a = np.ascontiguousarray([v for b in boxes for r in b for v in r], dtype=np.uint64)
+        lib3().orc3_set_solid(self._h, len(boxes), a.ctypes.data_as(C.POINTER(C.c_uint64)))
+
+    def face_fluxes(self, fam):
+        """Face fluxes (per unit area, 5 per face) of family 0 / 1 / 2 from the last residual evaluation."""
+        n = lib3().orc3_face_fluxes(self._h, fam, None)
+        out = np.zeros(n)
+        lib3().orc3_face_fluxes(self._h, fam, _dp(out))
+        return out.reshape(-1, 5)
 
     def eval_residual(self, cfl=0.5):
         return lib3().orc3_eval_residual(self._h, cfl)

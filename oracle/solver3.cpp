@@ -2,7 +2,8 @@
 //
 // f64 CPU restatement of the reference's 3D Euler path: crates/bowshock-cfd/src/{gas3,bc3,flux3,grid3,solver3,implicit3}.rs
 // and the runner / forces of crates/bowshock-core/src/engine/run3.rs (pressure forces CN, CA and the centre of pressure).
-// Bodies without fins only (no solid boxes). The oracle of the CUDA 3D path; only tests/ load it.
+// Solid boxes (fins, solver3.rs:13, grid3.rs:17-24) in the residual, time step, stages, implicit blocks and forces. The
+// oracle of the CUDA 3D path; only tests/ load it.
 #include <omp.h>
 
 #include <algorithm>
@@ -511,6 +512,9 @@ struct Solver3 {
   size_t iter = 0, ramp_k = 0, n_active = 0;
   std::vector<size_t> axis_k;
   std::vector<std::array<double, 2>> rot_i, rot_j, rot_k;
+  // solver3.rs:84-97: per cell, inside a solid box; n_active counts the fluid cells
+  std::vector<uint8_t> solid;
+  bool has_solid = false;
 
   size_t pidx(long i, long j, long k) const {
     return ((size_t)(k + NG) * (grid.nj + 2 * NG) + (size_t)(j + NG)) * (grid.ni + 2 * NG) + (size_t)(i + NG);
@@ -548,6 +552,27 @@ struct Solver3 {
     fi.assign(grid.iface.size(), C5{}), fj.assign(grid.jface.size(), C5{}), fk.assign(grid.kface.size(), C5{});
     u0.assign(nc, C5{});
     iter = ramp_k = 0;
+    solid.assign(nc, 0);
+    has_solid = false;
+  }
+  // boxes: 6 per box, half-open ranges [i0, i1) [j0, j1) [k0, k1) (grid3.rs:17-24 SolidBox)
+  void set_solid(size_t nbox, const uint64_t* boxes) {
+    size_t ni = grid.ni, nj = grid.nj, nk = grid.nk;
+    solid.assign(ni * nj * nk, 0);
+    for (size_t b = 0; b < nbox; ++b) {
+      const uint64_t* q = boxes + 6 * b;
+      for (uint64_t k = q[4]; k < std::min<uint64_t>(q[5], nk); ++k)
+        for (uint64_t j = q[2]; j < std::min<uint64_t>(q[3], nj); ++j)
+          for (uint64_t i = q[0]; i < std::min<uint64_t>(q[1], ni); ++i) solid[(k * nj + j) * ni + i] = 1;
+    }
+    n_active = 0;
+    for (uint8_t v : solid) n_active += v ? 0 : 1;
+    has_solid = n_active != solid.size();
+  }
+  // solver3.rs:343-353: out-of-range (ghost) positions are not solid
+  bool is_solid(long i, long j, long k) const {
+    return has_solid && i >= 0 && j >= 0 && k >= 0 && (size_t)i < grid.ni && (size_t)j < grid.nj && (size_t)k < grid.nk &&
+           solid[((size_t)k * grid.nj + (size_t)j) * grid.ni + (size_t)i];
   }
   double density_residual() const {  // solver3.rs:152-155
     double s = 0.0;
@@ -613,7 +638,27 @@ struct Solver3 {
           }
           long p0[3] = {(long)i, (long)j, k};
           auto at = [&](long s) { return w[pidx(p0[0] + s * e[0], p0[1] + s * e[1], p0[2] + s * e[2])]; };
-          out[fidx] = face_flux_lm3(at(-2), at(-1), at(0), at(1), lim, f.n, rots[fidx], low_mach);
+          auto sol = [&](long s) { return is_solid(p0[0] + s * e[0], p0[1] + s * e[1], p0[2] + s * e[2]); };
+          C5 wm2 = at(-2), wm1 = at(-1), wp0 = at(0), wp1 = at(1);
+          if (has_solid) {  // solver3.rs:362-405: solid cells as slip walls of their fluid neighbours
+            const size_t fstride = dir == 0 ? 1 : dir == 1 ? nfi : plane;
+            bool sm1 = sol(-1), sp0 = sol(0);
+            if (sm1 && sp0) {
+              out[fidx] = C5{};
+              continue;
+            }
+            if (sm1) {
+              wm1 = reflect3(wp0, f.n);
+              wm2 = sol(1) ? wm1 : reflect3(wp1, f.n);
+            } else if (sp0) {
+              wp0 = reflect3(wm1, f.n);
+              wp1 = sol(-2) ? wp0 : reflect3(wm2, f.n);
+            } else {
+              if (sol(-2)) wm2 = reflect3(wm1, faces[fidx - fstride].n);
+              if (sol(1)) wp1 = reflect3(wp0, faces[fidx + fstride].n);
+            }
+          }
+          out[fidx] = face_flux_lm3(wm2, wm1, wp0, wp1, lim, f.n, rots[fidx], low_mach);
         }
   }
   void eval_residual() {  // solver3.rs:222-270
@@ -632,6 +677,10 @@ struct Solver3 {
       for (size_t j = 0; j < nj; ++j)
         for (size_t i = 0; i < ni; ++i) {
           size_t c = ((size_t)k * nj + j) * ni + i;
+          if (solid[c]) {
+            res[c] = C5{};
+            continue;
+          }
           size_t il = ((size_t)k * nj + j) * (ni + 1) + i, jl = ((size_t)k * (nj + 1) + j) * ni + i;
           size_t ir = il + 1, jr = jl + ni, kr = c + ni * nj;
           double inv_v = 1.0 / grid.vol[c];
@@ -651,6 +700,10 @@ struct Solver3 {
       for (size_t j = 0; j < nj; ++j)
         for (size_t i = 0; i < ni; ++i) {
           size_t c = ((size_t)k * nj + j) * ni + i;
+          if (solid[c]) {
+            dt[c] = 0.0;
+            continue;
+          }
           const C5& wc = w[pidx((long)i, (long)j, k)];
           double cs = sound_speed3(wc);
           auto lam = [&](const Face3& f) { return (std::fabs(wc[1] * f.n[0] + wc[2] * f.n[1] + wc[3] * f.n[2]) + cs) * f.area; };
@@ -661,9 +714,10 @@ struct Solver3 {
           dt[c] = mode == orc::DT_SUM ? cfl_ * grid.vol[c] / (li + lj + lk) : cfl_ * grid.vol[c] / (3.0 * fmin_rs(fmin_rs(li, lj), lk));
         }
   }
-  void stage(double a, double b) {  // solver3.rs:317-327
+  void stage(double a, double b) {  // solver3.rs:317-327 (fluid cells)
     for (size_t c = 0; c < u.size(); ++c)
-      for (int k = 0; k < 5; ++k) u[c][k] = a * (u[c][k] + dt[c] * res[c][k]) + b * u0[c][k];
+      if (!solid[c])
+        for (int k = 0; k < 5; ++k) u[c][k] = a * (u[c][k] + dt[c] * res[c][k]) + b * u0[c][k];
   }
   double rk3_step() {  // solver3.rs:303-314
     eval_residual();
@@ -677,7 +731,8 @@ struct Solver3 {
     stage(2.0 / 3.0, 1.0 / 3.0);
     return rn;
   }
-  // implicit3.rs:274-355 (no solid cells): blocks of direction dir, ghost Jacobians folded at the line ends
+  // implicit3.rs:274-355: blocks of direction dir, ghost Jacobians folded at the line ends; a solid cell is the identity
+  // row, a fluid cell next to one along the line folds B T (T the reflection about the face) into its diagonal
   void assemble3(int dir, std::vector<M5>& LO, std::vector<M5>& D, std::vector<M5>& UP) {
     size_t ni = grid.ni, nj = grid.nj, nk = grid.nk, n = ni * nj * nk, plane = ni * nj;
     LO.assign(n, M5{}), D.assign(n, M5{}), UP.assign(n, M5{});
@@ -693,8 +748,13 @@ struct Solver3 {
       for (size_t j = 0; j < nj; ++j)
         for (size_t i = 0; i < ni; ++i) {
           size_t c = ((size_t)k * nj + j) * ni + i;
+          if (solid[c]) {
+            D[c] = eye5();
+            continue;
+          }
           size_t m = dir == 0 ? i : dir == 1 ? j : (size_t)k;
           size_t nl = dir == 0 ? ni : dir == 1 ? nj : nk;
+          const size_t stride = dir == 0 ? 1 : dir == 1 ? ni : plane;
           const C5& wk = w[pidx((long)i, (long)j, k)];
           const Face3 *fl, *fr;
           if (dir == 0) {
@@ -706,16 +766,23 @@ struct Solver3 {
           } else {
             fl = &grid.kface[c], fr = &grid.kface[c + plane];
           }
-          const C5& wm = w[pidx((long)i - e[0], (long)j - e[1], k - e[2])];
-          const C5& wp = w[pidx((long)i + e[0], (long)j + e[1], k + e[2])];
+          const bool lower_solid = m > 0 && solid[c - stride], upper_solid = m + 1 < nl && solid[c + stride];
+          const C5 wm = lower_solid ? reflect3(wk, fl->n) : w[pidx((long)i - e[0], (long)j - e[1], k - e[2])];
+          const C5 wp = upper_solid ? reflect3(wk, fr->n) : w[pidx((long)i + e[0], (long)j + e[1], k + e[2])];
           M5 l, dd, uu;
           cell_blocks3(wk, wm, wp, *fl, *fr, grid.vol[c], dt[c], ip, l, dd, uu);
           if (m == 0) {
             axpy5(dd, 1.0, mm5(l, ghost_t(true, *fl, i)));
             l = M5{};
+          } else if (lower_solid) {
+            axpy5(dd, 1.0, mm5(l, reflection3(fl->n)));
+            l = M5{};
           }
           if (m == nl - 1) {
             axpy5(dd, 1.0, mm5(uu, ghost_t(false, *fr, i)));
+            uu = M5{};
+          } else if (upper_solid) {
+            axpy5(dd, 1.0, mm5(uu, reflection3(fr->n)));
             uu = M5{};
           }
           LO[c] = l, D[c] = dd, UP[c] = uu;
@@ -794,6 +861,7 @@ struct Solver3 {
         for (int q = 0; q < 5; ++q) du[c][q] += corr[c][q];
     }
     for (size_t c = 0; c < n; ++c) {
+      if (solid[c]) continue;
       const C5& dq = du[c];
       double alpha = 1.0;
       for (int t = 0; t < 8; ++t) {
@@ -818,12 +886,14 @@ struct Solver3 {
   }
 };
 
-// ---------------------------------------------------------------- run3.rs (forces of bodies without fins)
+// ---------------------------------------------------------------- run3.rs (forces)
 struct Forces3 {
   double cn = 0, ca = 0, x_cp = NAN;
 };
-// run3.rs:150-190 (body wall part): j = 0 faces with i >= axis_cells and centroid x <= x_max; wall pressure extrapolated from
-// the first two cells, dF = (pw - p_inf) area (-n); coefficients of the half domain doubled, S_ref = pi/4.
+// run3.rs:130-212 `accumulate` summed over its parts: the j = 0 faces with i >= axis_cells over fluid cells, and every face
+// between a fluid and a solid cell (the fin sides, edges and tips); faces with centroid x <= x_max. The wall pressure is
+// extrapolated from the first fluid cell a and the fluid cell b behind it, pw = p_a + (p_a - p_b) d_a / (d_b - d_a), or p_a
+// where there is none; dF = (pw - p_inf) area n_into_body; coefficients of the half domain doubled, S_ref = pi/4.
 Forces3 forces_on(const Solver3& s, double mach, double x_max) {
   const Grid3& g = s.grid;
   size_t ni = g.ni, nj = g.nj, nk = g.nk;
@@ -833,23 +903,49 @@ Forces3 forces_on(const Solver3& s, double mach, double x_max) {
     const auto& x = g.xc[c];
     return std::sqrt(std::pow(x[0] - f.c[0], 2) + std::pow(x[1] - f.c[1], 2) + std::pow(x[2] - f.c[2], 2));
   };
+  auto sol = [&](size_t i, size_t j, size_t k) { return s.solid[g.cell(i, j, k)] != 0; };
   double fx = 0, fz = 0, mz = 0;
-  for (size_t k = 0; k < nk; ++k)
-    for (size_t i = g.axis_cells; i < ni; ++i) {
-      const Face3& f = g.jface[k * (nj + 1) * ni + i];
-      if (f.c[0] > x_max) continue;
-      size_t a = g.cell(i, 0, k);
-      double p0 = p(a), pw = p0;
-      if (nj > 1) {
-        size_t b = g.cell(i, 1, k);
-        double d0 = dist(a, f), d1 = dist(b, f);
-        pw = p0 + (p0 - p(b)) * d0 / (d1 - d0);
-      }
-      double d = (pw - p_inf) * f.area * -1.0;
-      fx += d * f.n[0];
-      fz += d * f.n[2];
-      mz += d * f.n[2] * f.c[0];
+  auto add = [&](size_t a, long b, const Face3& f, double sign) {
+    if (f.c[0] > x_max) return;
+    double p0 = p(a), pw = p0;
+    if (b >= 0) {
+      double d0 = dist(a, f), d1 = dist((size_t)b, f);
+      pw = p0 + (p0 - p((size_t)b)) * d0 / (d1 - d0);
     }
+    double d = (pw - p_inf) * f.area * sign;
+    fx += d * f.n[0];
+    fz += d * f.n[2];
+    mz += d * f.n[2] * f.c[0];
+  };
+  for (size_t k = 0; k < nk; ++k)
+    for (size_t i = g.axis_cells; i < ni; ++i)
+      if (!sol(i, 0, k)) add(g.cell(i, 0, k), nj > 1 && !sol(i, 1, k) ? (long)g.cell(i, 1, k) : -1, g.jface[k * (nj + 1) * ni + i], -1.0);
+  if (s.has_solid) {
+    for (size_t k = 0; k < nk; ++k)
+      for (size_t j = 0; j < nj; ++j)
+        for (size_t i = 1; i < ni; ++i) {
+          const Face3& f = g.iface[(k * nj + j) * (ni + 1) + i];
+          bool a = sol(i - 1, j, k), b = sol(i, j, k);
+          if (!a && b) add(g.cell(i - 1, j, k), i >= 2 && !sol(i - 2, j, k) ? (long)g.cell(i - 2, j, k) : -1, f, 1.0);
+          if (a && !b) add(g.cell(i, j, k), i + 1 < ni && !sol(i + 1, j, k) ? (long)g.cell(i + 1, j, k) : -1, f, -1.0);
+        }
+    for (size_t k = 0; k < nk; ++k)
+      for (size_t j = 1; j < nj; ++j)
+        for (size_t i = 0; i < ni; ++i) {
+          const Face3& f = g.jface[(k * (nj + 1) + j) * ni + i];
+          bool a = sol(i, j - 1, k), b = sol(i, j, k);
+          if (!a && b) add(g.cell(i, j - 1, k), j >= 2 && !sol(i, j - 2, k) ? (long)g.cell(i, j - 2, k) : -1, f, 1.0);
+          if (a && !b) add(g.cell(i, j, k), j + 1 < nj && !sol(i, j + 1, k) ? (long)g.cell(i, j + 1, k) : -1, f, -1.0);
+        }
+    for (size_t k = 1; k < nk; ++k)
+      for (size_t j = 0; j < nj; ++j)
+        for (size_t i = 0; i < ni; ++i) {
+          const Face3& f = g.kface[(k * nj + j) * ni + i];
+          bool a = sol(i, j, k - 1), b = sol(i, j, k);
+          if (!a && b) add(g.cell(i, j, k - 1), k >= 2 && !sol(i, j, k - 2) ? (long)g.cell(i, j, k - 2) : -1, f, 1.0);
+          if (a && !b) add(g.cell(i, j, k), k + 1 < nk && !sol(i, j, k + 1) ? (long)g.cell(i, j, k + 1) : -1, f, -1.0);
+        }
+  }
   double q = 0.5 * mach * mach, s_ref = M_PI / 4.0;
   double norm = 2.0 / (q * s_ref);
   Forces3 r;
@@ -895,6 +991,15 @@ void* orc3_new(uint64_t ni, uint64_t nj, const double* x2, const double* r2, uin
   return s;
 }
 void orc3_free(void* h) { delete static_cast<Solver3*>(h); }
+// solid boxes (6 per box: i0, i1, j0, j1, k0, k1, half-open), before the first step
+void orc3_set_solid(void* h, uint64_t nbox, const uint64_t* boxes) { static_cast<Solver3*>(h)->set_solid(nbox, boxes); }
+// the i / j / k face fluxes of the last residual evaluation (5 per face, flux per unit area)
+uint64_t orc3_face_fluxes(void* h, int dir, double* out) {
+  auto* s = static_cast<Solver3*>(h);
+  const std::vector<C5>& f = dir == 0 ? s->fi : dir == 1 ? s->fj : s->fk;
+  if (out) std::memcpy(out, f.data(), f.size() * 40);
+  return 5 * f.size();
+}
 void orc3_dims(void* h, uint64_t* ni, uint64_t* nj, uint64_t* nk) {
   auto* s = static_cast<Solver3*>(h);
   *ni = s->grid.ni, *nj = s->grid.nj, *nk = s->grid.nk;
