@@ -1157,6 +1157,10 @@ int bowshock3_create(uint64_t ni, uint64_t nj, uint64_t nk, const double* x, con
 void bowshock3_destroy(bowshock3_batch* b) { delete b; }
 const char* bowshock3_last_error(const bowshock3_batch* b) { return b ? b->last_error.c_str() : "null handle"; }
 int bowshock3_reset(bowshock3_batch* b) { return b ? b3from(b, b->b.reset()) : BOWSHOCK_INVALID; }
+int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes) {
+  if (!b || (nbox && !boxes)) return BOWSHOCK_INVALID;
+  return b3from(b, b->b.set_solid((size_t)nbox, boxes));
+}
 int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp) {
   return b ? b3from(b, b->b.set_counters((int)std::min<uint64_t>(iter, 1u << 30), (int)std::min<uint64_t>(ramp, 1u << 30))) : BOWSHOCK_INVALID;
 }

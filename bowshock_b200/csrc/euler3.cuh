@@ -14,7 +14,9 @@
 //   k3_lines_subst the defect-correction passes with the kept factors                  (implicit3.rs:274-382)
 //   k3_defect     dt R - (A_i du + A_j du + A_k du - 2 du) with the kept blocks         (implicit3.rs:384-455)
 //   k3_stage      SSP-RK3 stage                                                       (solver3.rs:303-327)
-//   k3_forces     FP64 wall-pressure force integration: CN, CA, centre of pressure     (run3.rs:150-190)
+//   k3_forces     FP64 wall-pressure force integration: CN, CA, centre of pressure     (run3.rs:130-212)
+// Solid boxes (fins, solver3.rs:13): cells of B.solid are never updated (zero residual and time step, identity rows of the
+// line systems) and act as slip walls of their fluid neighbours (reflected states in the flux stencils and in the blocks).
 #pragma once
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -316,6 +318,7 @@ struct B3 {
   const float4 *fi, *fj, *fk;  // (nx, ny, nz, area)
   const float2 *ri, *rj, *rk;  // face_rot (s, co)
   const float* vol;
+  const unsigned char* solid;  // per cell, inside a solid box (null: no solid cells)
   const int* axis_k;  // [i * nk + k], i < axis_cells
   const Case3Dev* cs;
   int *iter, *ramp, *active;
@@ -328,6 +331,10 @@ __device__ __forceinline__ long long pidx3(const B3& B, int i, int j, int k) {
   return ((long long)(k + 2) * (B.nj + 4) + (j + 2)) * (B.ni + 4) + (i + 2);
 }
 __device__ __forceinline__ long long cell3(const B3& B, int i, int j, int k) { return ((long long)k * B.nj + j) * B.ni + i; }
+// solver3.rs:343-353: positions outside the grid (ghosts) are not solid
+__device__ __forceinline__ bool sol3(const B3& B, int i, int j, int k) {
+  return B.solid && i >= 0 && j >= 0 && k >= 0 && i < B.ni && j < B.nj && k < B.nk && B.solid[cell3(B, i, j, k)];
+}
 __device__ __forceinline__ V5<float> ldU(const B3& B, const float* a, int b, long long c) {
   const float* p = a + (long long)b * 5 * B.nc + c;
   return V5<float>{{p[0], p[B.nc], p[2 * B.nc], p[3 * B.nc], p[4 * B.nc]}};
@@ -435,7 +442,35 @@ __global__ void k3_flux(B3 B, int dir) {
   int ei = dir == 0, ej = dir == 1, ek = dir == 2;
   auto at = [&](int s) { return f2d5(ldW(B, b, pidx3(B, i + s * ei, j + s * ej, k + s * ek))); };
   int lim = B.iter[b] < c.first_order_iters ? LIM_FIRST : c.limiter;
-  V5<double> fl = face_flux_lm3(at(-2), at(-1), at(0), at(1), lim, n.x, n.y, n.z, rot.x, rot.y, c.low_mach != 0);
+  V5<double> wm2 = at(-2), wm1 = at(-1), wp0 = at(0), wp1 = at(1);
+  if (B.solid) {  // solver3.rs:362-405: a solid cell is a slip wall of its fluid neighbour
+    auto sol = [&](int s) { return sol3(B, i + s * ei, j + s * ej, k + s * ek); };
+    const bool sm1 = sol(-1), sp0 = sol(0);
+    if (sm1 && sp0) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) out[q * nf] = 0.0;
+      return;
+    }
+    if (sm1) {
+      wm1 = reflect3<double>(wp0, n.x, n.y, n.z);
+      wm2 = sol(1) ? wm1 : reflect3<double>(wp1, n.x, n.y, n.z);
+    } else if (sp0) {
+      wp0 = reflect3<double>(wm1, n.x, n.y, n.z);
+      wp1 = sol(-2) ? wp0 : reflect3<double>(wm2, n.x, n.y, n.z);
+    } else {
+      const float4* fam = dir == 0 ? B.fi : dir == 1 ? B.fj : B.fk;
+      const long long fs = dir == 0 ? 1 : dir == 1 ? nfi : (long long)nfi * nfj;
+      if (sol(-2)) {
+        const float4 m = fam[f - fs];
+        wm2 = reflect3<double>(wm1, m.x, m.y, m.z);
+      }
+      if (sol(1)) {
+        const float4 m = fam[f + fs];
+        wp1 = reflect3<double>(wp0, m.x, m.y, m.z);
+      }
+    }
+  }
+  V5<double> fl = face_flux_lm3(wm2, wm1, wp0, wp1, lim, n.x, n.y, n.z, rot.x, rot.y, c.low_mach != 0);
   double area = n.w;
 #pragma unroll
   for (int q = 0; q < 5; ++q) out[q * nf] = fl[q] * area;
@@ -449,7 +484,10 @@ __global__ void k3_residual(B3 B, int dt_kind, int slot) {
   if (!B.active[b]) return;
   const Case3Dev& cs = B.cs[b];
   double rr = 0.0;
-  if (c < B.nc) {
+  if (c < B.nc && B.solid && B.solid[c]) {  // solver3.rs:251-254, 281-284: zero residual and time step
+    stU(B, B.R, b, c, V5<float>{{0.f, 0.f, 0.f, 0.f, 0.f}});
+    if (dt_kind) B.dt[(long long)b * B.nc + c] = 0.f;
+  } else if (c < B.nc) {
     int i = (int)(c % B.ni), j = (int)((c / B.ni) % B.nj), k = (int)(c / ((long long)B.ni * B.nj));
     long long il = ((long long)k * B.nj + j) * (B.ni + 1) + i, jl = ((long long)k * (B.nj + 1) + j) * B.ni + i, kl = c;
     long long ir = il + 1, jr = jl + B.ni, kr = c + (long long)B.ni * B.nj;
@@ -497,6 +535,7 @@ __global__ void k3_stage(B3 B, float a, float bb, int copy, int last) {
   int b = blockIdx.y;
   if (c >= B.nc || !B.active[b]) return;
   if (last && c == 0) B.iter[b] += 1;
+  if (B.solid && B.solid[c]) return;  // solver3.rs:317-327: fluid cells only
   V5<float> u = ldU(B, B.U, b, c);
   if (copy) stU(B, B.U0, b, c, u);
   V5<float> u0 = copy ? u : ldU(B, B.U0, b, c);
@@ -523,7 +562,11 @@ __device__ void blocks3(const B3& B, int b, int dir, int i, int j, int k, M5<flo
   } else {
     fl = B.fk[c], fr = B.fk[c + (long long)B.ni * B.nj];
   }
-  V5<float> wk = ldW(B, b, pidx3(B, i, j, k)), wm = ldW(B, b, pidx3(B, i - ei, j - ej, k - ek)), wp = ldW(B, b, pidx3(B, i + ei, j + ej, k + ek));
+  // implicit3.rs:329-332: a solid neighbour along the line enters as the reflection of this cell about the face
+  const bool lower_solid = m > 0 && sol3(B, i - ei, j - ej, k - ek), upper_solid = m + 1 < nl && sol3(B, i + ei, j + ej, k + ek);
+  V5<float> wk = ldW(B, b, pidx3(B, i, j, k));
+  V5<float> wm = lower_solid ? reflect3<float>(wk, fl.x, fl.y, fl.z) : ldW(B, b, pidx3(B, i - ei, j - ej, k - ek));
+  V5<float> wp = upper_solid ? reflect3<float>(wk, fr.x, fr.y, fr.z) : ldW(B, b, pidx3(B, i + ei, j + ej, k + ek));
   const float s = 0.5f * B.dt[(long long)b * B.nc + c] / B.vol[c], al = fl.w, ar = fr.w;
   M5<float> dl, dr;
   if (cs.roe) {
@@ -567,9 +610,15 @@ __device__ void blocks3(const B3& B, int b, int dir, int i, int j, int k, M5<flo
     bool refl = cs.implicit_bc && ((dir == 1 && i >= B.axis_cells) || dir == 2);
     if (refl) axpy5(d, 1.f, mm5(lo, reflection3(fl.x, fl.y, fl.z)));
     lo = zero5();
+  } else if (lower_solid) {  // implicit3.rs:338-345: B T folded into the diagonal, the line cut
+    axpy5(d, 1.f, mm5(lo, reflection3(fl.x, fl.y, fl.z)));
+    lo = zero5();
   }
   if (m == nl - 1) {
     if (cs.implicit_bc && dir == 2) axpy5(d, 1.f, mm5(up, reflection3(fr.x, fr.y, fr.z)));
+    up = zero5();
+  } else if (upper_solid) {
+    axpy5(d, 1.f, mm5(up, reflection3(fr.x, fr.y, fr.z)));
     up = zero5();
   }
 }
@@ -641,10 +690,14 @@ __global__ void __launch_bounds__(128, 4) k3_assemble(B3 B, int part) {
   } else {
     i = (int)(t % B.ni), j = (int)((t / B.ni) % B.nj), k = (int)(t / ((long long)B.ni * B.nj));
   }
+  const bool solid = B.solid && B.solid[cell3(B, i, j, k)];
 #pragma unroll 1
   for (int dir = part == 0 ? 0 : 1; dir < (part == 0 ? 1 : 3); ++dir) {
     M5<float> lo, d, up;
-    blocks3(B, b, dir, i, j, k, lo, d, up);
+    if (solid)  // implicit3.rs:311-314: the identity row
+      lo = zero5(), d = eye5(), up = zero5();
+    else
+      blocks3(B, b, dir, i, j, k, lo, d, up);
     __half* r = rec3h(B, b, dir) + rcell(B, dir, i, j, k);
     st5(r + R_LO * B.nc, B.nc, lo);
     st5(r + R_D * B.nc, B.nc, d);
@@ -682,7 +735,7 @@ __device__ __forceinline__ void emit3(const B3& B, int b, int epilogue, bool upd
     for (int q = 0; q < 5; ++q) du[q] += o[q];
   }
   stU(B, B.DU, b, c, du);
-  if (update) damped_update3(B, b, c, du);
+  if (update && !(B.solid && B.solid[c])) damped_update3(B, b, c, du);
 }
 
 // First pass of an iteration, one thread per line: block Thomas on the kept blocks (implicit3.rs:133-156), keeping M^-1,
@@ -861,31 +914,31 @@ __global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
   stU(B, B.RR, b, c, o);
 }
 
-// FP64 wall forces of every case (run3.rs:150-190, body wall without fins): one block per case.
-// wall: per j = 0 face (i >= axis_cells) n[3], area, c[3], the centroids of cells (i, 0, k) and (i, 1, k); x <= x_max.
+// FP64 wall forces of every case (run3.rs:130-212): one block per case. wall: WALL3 doubles per wall face, the j = 0 body
+// faces (i >= axis_cells, fluid cells) and every face between a fluid and a solid cell: n[3], area, c[3], the centroid of
+// the first fluid cell a and of the fluid cell b behind it, a, b (-1: none), and the sign that turns n into the body.
+constexpr int WALL3 = 16;
 __global__ void k3_forces(B3 B, const double* wall, int nwall, double x_max, double* out) {
   __shared__ double acc[3][256];
   int b = blockIdx.x;
   double p_inf = B.cs[b].fs[4];
   double fx = 0, fz = 0, mz = 0;
-  const int nw = B.ni - B.axis_cells;
   for (int q = threadIdx.x; q < nwall; q += blockDim.x) {
-    const double* w = wall + 13 * (long long)q;
+    const double* w = wall + WALL3 * (long long)q;
     if (w[4] > x_max) continue;
-    int i = B.axis_cells + q % nw, k = q / nw;
-    long long ca = cell3(B, i, 0, k);
     auto pres = [&](long long cc) {
       const float* p = B.U + (long long)b * 5 * B.nc + cc;
       double rho = p[0], u = p[B.nc] / rho, v = p[2 * B.nc] / rho, ww = p[3 * B.nc] / rho;
       return (GD - 1.0) * ((double)p[4 * B.nc] - 0.5 * rho * (u * u + v * v + ww * ww));
     };
+    const long long ca = (long long)w[13], cb = (long long)w[14];
     double p0 = pres(ca), pw = p0;
-    if (B.nj > 1) {
+    if (cb >= 0) {
       double d0 = sqrt((w[7] - w[4]) * (w[7] - w[4]) + (w[8] - w[5]) * (w[8] - w[5]) + (w[9] - w[6]) * (w[9] - w[6]));
       double d1 = sqrt((w[10] - w[4]) * (w[10] - w[4]) + (w[11] - w[5]) * (w[11] - w[5]) + (w[12] - w[6]) * (w[12] - w[6]));
-      pw = p0 + (p0 - pres(cell3(B, i, 1, k))) * d0 / (d1 - d0);
+      pw = p0 + (p0 - pres(cb)) * d0 / (d1 - d0);
     }
-    double dd = (pw - p_inf) * w[3] * -1.0;
+    double dd = (pw - p_inf) * w[3] * w[15];
     fx += dd * w[0];
     fz += dd * w[2];
     mz += dd * w[2] * w[4];

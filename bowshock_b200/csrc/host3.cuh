@@ -131,8 +131,12 @@ struct Batch3 {
   Grid3H g;
   std::vector<Case3Host> cases;
   std::vector<int> axis_k;
-  std::vector<double> wall;  // 13 per j = 0 wall face: n[3], area, c[3], centroid of (i,0,k), centroid of (i,1,k)
+  std::vector<double> wall;  // WALL3 per wall face (k3_forces)
   int nwall = 0, device = 0, slots = 64;
+  std::vector<unsigned char> solid_h;  // per cell, inside a solid box
+  long long n_active = 0;              // fluid cells: the density norm's denominator (solver3.rs:97, 152-155)
+  unsigned char* d_solid = nullptr;
+  size_t wall_cap = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms_per_iter = 0.0;
@@ -205,18 +209,10 @@ struct Batch3 {
         }
         axis_k[i * nk + k] = (int)bk;
       }
-    // wall faces for the forces
-    wall.clear();
-    for (size_t k = 0; k < nk; ++k)
-      for (size_t i = axis_cells; i < ni; ++i) {
-        const double* f = &g.fj[7 * (k * (nj + 1) * ni + i)];
-        for (int q = 0; q < 7; ++q) wall.push_back(f[q]);
-        const double* c0 = &g.xc[3 * ((k * nj) * ni + i)];
-        const double* c1 = &g.xc[3 * ((k * nj + 1) * ni + i)];
-        for (int q = 0; q < 3; ++q) wall.push_back(c0[q]);
-        for (int q = 0; q < 3; ++q) wall.push_back(c1[q]);
-      }
-    nwall = (int)(wall.size() / 13);
+    solid_h.assign((size_t)B.nc, 0);
+    n_active = B.nc;
+    build_wall();
+    wall_cap = std::max<size_t>(wall.size(), 1);
     int rc;
     float4 *fi, *fj, *fk;
     float2 *ri, *rj, *rk;
@@ -231,7 +227,7 @@ struct Batch3 {
     if ((rc = alloc(&B.U, ns)) || (rc = alloc(&B.U0, ns)) || (rc = alloc(&B.W, (size_t)nb * 5 * B.npad)) || (rc = alloc(&B.R, ns)) ||
         (rc = alloc(&B.X, ns)) || (rc = alloc(&B.DU, ns)) || (rc = alloc(&B.RR, ns)) || (rc = alloc(&B.dt, (size_t)nb * B.nc)) ||
         (rc = alloc(&B.scr, (size_t)nb * 3 * REC3 * B.nc)) || (rc = alloc(&B.FI, (size_t)nb * 5 * B.nfi)) || (rc = alloc(&B.FJ, (size_t)nb * 5 * B.nfj)) ||
-        (rc = alloc(&B.FK, (size_t)nb * 5 * B.nfk)) || (rc = alloc(&B.rsum, (size_t)slots * nb)) || (rc = alloc(&d_wall, wall.size())) ||
+        (rc = alloc(&B.FK, (size_t)nb * 5 * B.nfk)) || (rc = alloc(&B.rsum, (size_t)slots * nb)) || (rc = alloc(&d_wall, wall_cap)) ||
         (rc = alloc(&d_forces, 3 * (size_t)nb)))
       return rc;
     auto up_faces = [&](const std::vector<double>& f, long long n, float4* d4, float2* d2) -> int {
@@ -257,6 +253,85 @@ struct Batch3 {
     if ((rc = upload_cases())) return rc;
     h_active.assign(nb, 1);
     BK3_CUDA(copy_sync(stream, B.active, h_active.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    return reset();
+  }
+  // run3.rs:130-212: the wall faces that carry forces, WALL3 doubles each (k3_forces): the j = 0 faces of fluid cells with
+  // i >= axis_cells, then the faces between a fluid and a solid cell in i, j and k
+  void build_wall() {
+    const size_t ni = g.ni, nj = g.nj, nk = g.nk;
+    auto cell = [&](size_t i, size_t j, size_t k) { return (k * nj + j) * ni + i; };
+    auto sol = [&](size_t i, size_t j, size_t k) { return solid_h[cell(i, j, k)] != 0; };
+    wall.clear();
+    auto add = [&](const double* f, size_t a, long long b, double sign) {
+      for (int q = 0; q < 7; ++q) wall.push_back(f[q]);
+      for (int q = 0; q < 3; ++q) wall.push_back(g.xc[3 * a + q]);
+      for (int q = 0; q < 3; ++q) wall.push_back(b >= 0 ? g.xc[3 * (size_t)b + q] : 0.0);
+      wall.push_back((double)a), wall.push_back((double)b), wall.push_back(sign);
+    };
+    for (size_t k = 0; k < nk; ++k)
+      for (size_t i = (size_t)B.axis_cells; i < ni; ++i)
+        if (!sol(i, 0, k)) add(&g.fj[7 * (k * (nj + 1) * ni + i)], cell(i, 0, k), nj > 1 && !sol(i, 1, k) ? (long long)cell(i, 1, k) : -1, -1.0);
+    if (n_active != B.nc) {
+      for (size_t k = 0; k < nk; ++k)
+        for (size_t j = 0; j < nj; ++j)
+          for (size_t i = 1; i < ni; ++i) {
+            const double* f = &g.fi[7 * ((k * nj + j) * (ni + 1) + i)];
+            const bool a = sol(i - 1, j, k), b = sol(i, j, k);
+            if (!a && b) add(f, cell(i - 1, j, k), i >= 2 && !sol(i - 2, j, k) ? (long long)cell(i - 2, j, k) : -1, 1.0);
+            if (a && !b) add(f, cell(i, j, k), i + 1 < ni && !sol(i + 1, j, k) ? (long long)cell(i + 1, j, k) : -1, -1.0);
+          }
+      for (size_t k = 0; k < nk; ++k)
+        for (size_t j = 1; j < nj; ++j)
+          for (size_t i = 0; i < ni; ++i) {
+            const double* f = &g.fj[7 * ((k * (nj + 1) + j) * ni + i)];
+            const bool a = sol(i, j - 1, k), b = sol(i, j, k);
+            if (!a && b) add(f, cell(i, j - 1, k), j >= 2 && !sol(i, j - 2, k) ? (long long)cell(i, j - 2, k) : -1, 1.0);
+            if (a && !b) add(f, cell(i, j, k), j + 1 < nj && !sol(i, j + 1, k) ? (long long)cell(i, j + 1, k) : -1, -1.0);
+          }
+      for (size_t k = 1; k < nk; ++k)
+        for (size_t j = 0; j < nj; ++j)
+          for (size_t i = 0; i < ni; ++i) {
+            const double* f = &g.fk[7 * ((k * nj + j) * ni + i)];
+            const bool a = sol(i, j, k - 1), b = sol(i, j, k);
+            if (!a && b) add(f, cell(i, j, k - 1), k >= 2 && !sol(i, j, k - 2) ? (long long)cell(i, j, k - 2) : -1, 1.0);
+            if (a && !b) add(f, cell(i, j, k), k + 1 < nk && !sol(i, j, k + 1) ? (long long)cell(i, j, k + 1) : -1, -1.0);
+          }
+    }
+    nwall = (int)(wall.size() / WALL3);
+  }
+  // Solid boxes (grid3.rs:17-24 SolidBox; 6 per box: i0, i1, j0, j1, k0, k1, half-open cell ranges) of the shared grid:
+  // the cell mask, the fluid-cell count, the force faces; every case back to its free stream (solid cells keep it).
+  int set_solid(size_t nbox, const uint64_t* boxes) {
+    const uint64_t ext[3] = {(uint64_t)B.ni, (uint64_t)B.nj, (uint64_t)B.nk};
+    for (size_t q = 0; q < nbox; ++q)
+      for (int d = 0; d < 3; ++d)
+        if (!(boxes[6 * q + 2 * d] < boxes[6 * q + 2 * d + 1] && boxes[6 * q + 2 * d + 1] <= ext[d])) {
+          err = "solid box out of the grid or empty";
+          return 2;
+        }
+    std::fill(solid_h.begin(), solid_h.end(), 0);
+    for (size_t q = 0; q < nbox; ++q) {
+      const uint64_t* r = boxes + 6 * q;
+      for (uint64_t k = r[4]; k < r[5]; ++k)
+        for (uint64_t j = r[2]; j < r[3]; ++j)
+          for (uint64_t i = r[0]; i < r[1]; ++i) solid_h[(k * B.nj + j) * B.ni + i] = 1;
+    }
+    n_active = 0;
+    for (unsigned char v : solid_h) n_active += v ? 0 : 1;
+    if (n_active == 0) {
+      err = "every cell is solid";
+      return 2;
+    }
+    int rc;
+    if (!d_solid && (rc = alloc(&d_solid, (size_t)B.nc))) return rc;
+    BK3_CUDA(copy_sync(stream, d_solid, solid_h.data(), (size_t)B.nc, cudaMemcpyHostToDevice));
+    B.solid = n_active != B.nc ? d_solid : nullptr;
+    build_wall();
+    if (wall.size() > wall_cap) {
+      wall_cap = wall.size();
+      if ((rc = alloc(&d_wall, wall_cap))) return rc;
+    }
+    BK3_CUDA(copy_sync(stream, d_wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice));
     return reset();
   }
   int upload_cases() {
@@ -361,7 +436,6 @@ struct Batch3 {
     std::vector<double> h;
     long long done = 0;
     double ms_total = 0.0;
-    std::vector<long long> n_active(nb, B.nc);
     while (done < n) {
       int chunk = (int)std::min<long long>(n - done, slots);
       BK3_CUDA(cudaMemsetAsync(B.rsum, 0, (size_t)chunk * nb * sizeof(double), stream));
@@ -377,7 +451,7 @@ struct Batch3 {
       ms_total += ms;
       if (residual)
         for (int k = 0; k < chunk; ++k)
-          for (int b = 0; b < nb; ++b) residual[(done + k) * nb + b] = std::sqrt(h[(size_t)k * nb + b] / (double)B.nc);
+          for (int b = 0; b < nb; ++b) residual[(done + k) * nb + b] = std::sqrt(h[(size_t)k * nb + b] / (double)n_active);
       done += chunk;
     }
     last_ms_per_iter = n > 0 ? ms_total / (double)n : 0.0;
@@ -392,7 +466,7 @@ struct Batch3 {
     dens.resize(B.nb);
     BK3_CUDA(cudaMemcpyAsync(dens.data(), B.rsum, B.nb * sizeof(double), cudaMemcpyDeviceToHost, stream));
     BK3_CUDA(cudaStreamSynchronize(stream));
-    for (auto& d : dens) d = std::sqrt(d / (double)B.nc);
+    for (auto& d : dens) d = std::sqrt(d / (double)n_active);
     return 0;
   }
   int read_residual(int b, double* res, double* dt) {

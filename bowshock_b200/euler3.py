@@ -39,6 +39,7 @@ SIGNATURES3 = {
     "bowshock3_destroy": (None, [_P]),
     "bowshock3_last_error": (C.c_char_p, [_P]),
     "bowshock3_reset": (_I, [_P]),
+    "bowshock3_set_solid": (_I, [_P, _U, C.POINTER(_U)]),
     "bowshock3_set_iter": (_I, [_P, _U, _U]),
     "bowshock3_set_state": (_I, [_P, _U, _dp]),
     "bowshock3_state": (_I, [_P, _U, _dp]),
@@ -128,6 +129,12 @@ class Batch3:
 
     def reset(self):
         self._check(lib().bowshock3_reset(self._h))
+
+    def set_solid(self, boxes):
+        """Solid boxes of the shared grid (the fins; grid3.rs `SolidBox`): ((i0, i1), (j0, j1), (k0, k1)) half-open cell
+        ranges each; resets every case to its free stream."""
+        a = np.ascontiguousarray([v for bx in boxes for r in bx for v in r], dtype=np.uint64)
+        self._check(lib().bowshock3_set_solid(self._h, len(boxes), a.ctypes.data_as(C.POINTER(_U)) if len(boxes) else None))
 
     def set_iter(self, it, ramp=None):
         self._check(lib().bowshock3_set_iter(self._h, int(it), int(it if ramp is None else ramp)))

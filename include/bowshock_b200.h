@@ -412,7 +412,8 @@ int bowshock_solver_set_sst_coupling(bowshock_solver* s, int coupled);
  * The stability path (crates/bowshock-cfd/src/solver3.rs + implicit3.rs behind `GpuSolver3`, gpu/mod.rs:442-560, driven
  * by engine/run3.rs): a batch of cases (Mach number, incidence) on one shared 3D grid. Nodes (ni+1)(nj+1)(nk+1), index
  * (k*(nj+1)+j)*(ni+1)+i; j = 0 is the axis for i < axis_cells and the body wall beyond, j = nj and the i ends the far
- * field, k = 0 and k = nk symmetry planes (a half body revolved over [0, pi]). No fins. */
+ * field, k = 0 and k = nk symmetry planes (a half body revolved over [0, pi]). Fins are solid boxes of cells
+ * (bowshock3_set_solid). */
 typedef struct {
   double mach, alpha;       /* incidence [rad]: the air moves towards +z (gas3.rs:42-44) */
   double cfl;               /* CFL of the explicit scheme */
@@ -439,6 +440,12 @@ void bowshock3_destroy(bowshock3_batch* b);
 const char* bowshock3_last_error(const bowshock3_batch* b);
 /* every case back to its free stream at iteration 0 (GpuSolver3::reset) */
 int bowshock3_reset(bowshock3_batch* b);
+/* Solid boxes of the shared grid (crates/bowshock-cfd/src/grid3.rs:17-24 `SolidBox`, the fins; `Grid3::solid`, read by
+ * Solver3::new, solver3.rs:84-97): 6 per box, i0 i1 j0 j1 k0 k1, half-open cell ranges; nbox 0 removes them. Solid cells
+ * are never updated and act as slip walls (solver3.rs:362-405, implicit3.rs:14-16); the density norm runs over the fluid
+ * cells; the forces add every face between a fluid and a solid cell (run3.rs:130-212). Resets every case to its free
+ * stream. INVALID for an empty box or one outside the grid. */
+int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes);
 /* iteration counter (first-order start-up) and CFL-ramp counter of every case */
 int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp);
 /* conserved state of case k, ni*nj*nk x 5 (Solver3::u layout) */
@@ -448,7 +455,7 @@ int bowshock3_state(bowshock3_batch* b, uint64_t k, double* u);
 int bowshock3_run(bowshock3_batch* b, uint64_t n, double* residual);
 /* residual (ncell x 5) and time step of case k for the current state (no update); density residual of case k */
 int bowshock3_eval_residual(bowshock3_batch* b, uint64_t k, double* res, double* dt, double* density_residual);
-/* FP64 pressure forces of every case: (cn, ca, x_cp) x ncases (run3.rs `forces_on`, no fins) */
+/* FP64 pressure forces of every case: (cn, ca, x_cp) x ncases (run3.rs `forces_on`: body wall and fin faces) */
 int bowshock3_forces(bowshock3_batch* b, double x_max, double* out);
 /* cold start of every case, iterated to the stop rules with per-case masks (run3.rs:220-330) */
 int bowshock3_solve(bowshock3_batch* b, const bowshock3_run_params* p, bowshock3_result* out);
