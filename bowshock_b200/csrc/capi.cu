@@ -1161,6 +1161,11 @@ int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes
   if (!b || (nbox && !boxes)) return BOWSHOCK_INVALID;
   return b3from(b, b->b.set_solid((size_t)nbox, boxes));
 }
+int bowshock3_set_staging(bowshock3_batch* b, int on) {
+  if (!b) return BOWSHOCK_INVALID;
+  b->b.staged = on != 0;
+  return BOWSHOCK_OK;
+}
 int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp) {
   return b ? b3from(b, b->b.set_counters((int)std::min<uint64_t>(iter, 1u << 30), (int)std::min<uint64_t>(ramp, 1u << 30))) : BOWSHOCK_INVALID;
 }

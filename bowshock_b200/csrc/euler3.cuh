@@ -795,6 +795,128 @@ __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, i
   if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
 }
 
+// cp.async helpers of the staged line walks (16-byte chunks bypass L1; 4-byte copies for the strided right-hand sides)
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// The first pass with the walk staged through shared memory: the 32 lanes of a warp walk 32 adjacent lines, whose
+// records are adjacent in every plane, and the blocks lo, d, up (75 FP16 planes, 64 bytes per plane and step), the
+// right-hand side and the time step of step m + 2 are copied by cp.async while step m is computed. The loads of the
+// unstaged walk cannot move above the previous step's stores of M^-1 and Y, so every step of it waits a memory latency;
+// the arithmetic here is the same, in the same order, so the results are the unstaged kernel's bit for bit. The host
+// runs it when the lines of a warp are adjacent and every copy is 16-byte aligned (k3_staged_ok).
+constexpr int ST3N = 3;  // stages: the copies run two steps ahead
+struct Stage3 {
+  __half blk[75][32];  // planes R_LO .. R_UP + 24 of the warp's 32 lines
+  float r[5][32];      // right-hand side
+  float dt[32];
+};
+__global__ void __launch_bounds__(64) k3_lines_st(B3 B, int dir, const float* in, int from_res, float* out, int epilogue) {
+  __shared__ __align__(16) Stage3 S[2][ST3N];
+  const long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (L >= nlines3(B, dir) || !B.active[b]) return;  // whole warps: the host launches it for line counts in multiples of 32
+  const Case3Dev& cs = B.cs[b];
+  const bool update = epilogue != 0 && (cs.sub_iters > 1 ? cs.sub_iters : 1) == 1;
+  long long c0, stride, r0, rs;
+  int n;
+  line3(B, dir, L, c0, stride, n, r0, rs);
+  float* R = rec3(B, b, dir) + r0;
+  __half* H = rec3h(B, b, dir) + r0;
+  const long long nc = B.nc;
+  // lane 0's record and cell offsets: the lanes' records are adjacent; their cells too for the j and k lines, and nc apart
+  // ... ni apart for the i lines (the i records are transposed, the state is not)
+  const __half* Hw = rec3h(B, b, dir) + (r0 - lane);
+  const float* inb = in + (long long)b * 5 * nc;
+  const float* dtb = B.dt + (long long)b * nc;
+  auto issue = [&](int m) {
+    if (m < n) {
+      Stage3& st = S[wid][m % ST3N];
+      const long long rr = (long long)m * rs;
+      for (int t = lane; t < 75 * 4; t += 32) {
+        const int q = t >> 2, ch = t & 3;
+        cpa16(&st.blk[q][8 * ch], Hw + (long long)(R_LO + q) * nc + rr + 8 * ch);
+      }
+      const long long c = c0 + (long long)m * stride;
+      if (dir == 0) {  // strided cells: one 4-byte copy per lane and plane
+#pragma unroll
+        for (int v = 0; v < 5; ++v) cpa4(&st.r[v][lane], inb + v * nc + c);
+        if (from_res) cpa4(&st.dt[lane], dtb + c);
+      } else {
+        const long long cw = c - lane;
+        for (int t = lane; t < 5 * 8; t += 32) {
+          const int v = t >> 3, ch = t & 7;
+          cpa16(&st.r[v][4 * ch], inb + v * nc + cw + 4 * ch);
+        }
+        if (from_res && lane < 8) cpa16(&st.dt[4 * lane], dtb + cw + 4 * lane);
+      }
+    }
+    cpa_commit();
+  };
+  issue(0);
+  issue(1);
+  M5<float> Y = zero5();
+  V5<float> g{{0, 0, 0, 0, 0}};
+  for (int m = 0; m < n; ++m) {
+    cpa_wait1();  // the copies of step m are done (those of step m + 1 may still run)
+    __syncwarp();
+    issue(m + 2);  // into the stage step m - 1 used, which every lane has finished with
+    const Stage3& st = S[wid][m % ST3N];
+    const long long rr = (long long)m * rs;
+    M5<float> d;
+#pragma unroll
+    for (int q = 0; q < 25; ++q) d[q] = __half2float(st.blk[R_D + q][lane]);
+    V5<float> r;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) r[q] = st.r[q][lane];
+    if (from_res) {
+      float dtc = st.dt[lane];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) r[q] *= dtc;
+    }
+    if (m > 0) {
+      M5<float> lo;
+#pragma unroll
+      for (int q = 0; q < 25; ++q) lo[q] = __half2float(st.blk[R_LO + q][lane]);
+      axpy5(d, -1.f, mm5(lo, Y));
+      V5<float> t = mv5(lo, g);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) r[q] -= t[q];
+    }
+    M5<float> Minv = inv5(d);
+    g = mv5(Minv, r);
+    M5<float> up;
+#pragma unroll
+    for (int q = 0; q < 25; ++q) up[q] = __half2float(st.blk[R_UP + q][lane]);
+    Y = mm5(Minv, up);
+    st5(H + R_MINV * nc + rr, nc, Minv);
+    st5(H + R_Y * nc + rr, nc, Y);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) R[(R_G + q) * nc + rr] = g[q];
+  }
+  V5<float> xn = g;
+  emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
+  for (int m = n - 2; m >= 0; --m) {
+    long long c = c0 + m * stride, rr = m * rs;
+    M5<float> Ym = ld5(H + R_Y * nc + rr, nc);
+    V5<float> gm;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gm[q] = R[(R_G + q) * nc + rr];
+    V5<float> t = mv5(Ym, xn);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gm[q] -= t[q];
+    emit3(B, b, epilogue, update, out, c, gm);
+    xn = gm;
+  }
+  if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
+}
+
 // Defect-correction pass `pass` >= 1: the same line solve with the kept factors (forward g = M^-1 (r - lo g_prev),
 // backward x = g - Y x_next).
 __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float* in, float* out, int epilogue, int pass) {

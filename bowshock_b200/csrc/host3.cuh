@@ -396,6 +396,16 @@ struct Batch3 {
     k3_flux<<<grid_of(B.nfk, 128), 128, 0, stream>>>(B, 2);
   }
   bool implicit() const { return cases[0].implicit != 0; }
+  // the staged first pass (k3_lines_st): on unless pinned off; only where a warp's 32 lines are adjacent (i lines: nj a
+  // multiple of 32; j and k lines: ni a multiple of 32), which also makes every one of its 16-byte copies aligned
+  bool staged = true;
+  bool staged_ok(int dir) const { return staged && (dir == 0 ? B.nj % 32 == 0 : B.ni % 32 == 0); }
+  void launch_lines(int dir, long long nl, const float* in, int from_res, float* out, int epilogue) {
+    if (staged_ok(dir))
+      k3_lines_st<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
+    else
+      k3_lines<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
+  }
   int max_sub() const {
     int s = 1;
     for (auto& c : cases) s = std::max(s, c.sub_iters);
@@ -408,9 +418,9 @@ struct Batch3 {
       const long long li = (long long)B.nj * B.nk, lj = (long long)B.ni * B.nk, lk = (long long)B.ni * B.nj;
       k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 0);
       k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 1);
-      k3_lines<<<grid_of(li, 64), 64, 0, stream>>>(B, 0, B.R, 1, B.X, 0);
-      k3_lines<<<grid_of(lj, 64), 64, 0, stream>>>(B, 1, B.X, 0, B.X, 0);
-      k3_lines<<<grid_of(lk, 64), 64, 0, stream>>>(B, 2, B.X, 0, nullptr, 1);
+      launch_lines(0, li, B.R, 1, B.X, 0);
+      launch_lines(1, lj, B.X, 0, B.X, 0);
+      launch_lines(2, lk, B.X, 0, nullptr, 1);
       for (int p = 1; p < max_sub(); ++p) {
         k3_defect_i<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
         k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);

@@ -40,6 +40,7 @@ SIGNATURES3 = {
     "bowshock3_last_error": (C.c_char_p, [_P]),
     "bowshock3_reset": (_I, [_P]),
     "bowshock3_set_solid": (_I, [_P, _U, C.POINTER(_U)]),
+    "bowshock3_set_staging": (_I, [_P, _I]),
     "bowshock3_set_iter": (_I, [_P, _U, _U]),
     "bowshock3_set_state": (_I, [_P, _U, _dp]),
     "bowshock3_state": (_I, [_P, _U, _dp]),
@@ -135,6 +136,10 @@ class Batch3:
         ranges each; resets every case to its free stream."""
         a = np.ascontiguousarray([v for bx in boxes for r in bx for v in r], dtype=np.uint64)
         self._check(lib().bowshock3_set_solid(self._h, len(boxes), a.ctypes.data_as(C.POINTER(_U)) if len(boxes) else None))
+
+    def set_staging(self, on):
+        """The first line pass staged through shared memory where the grid allows it (default on); same results."""
+        self._check(lib().bowshock3_set_staging(self._h, int(bool(on))))
 
     def set_iter(self, it, ramp=None):
         self._check(lib().bowshock3_set_iter(self._h, int(it), int(it if ramp is None else ramp)))

@@ -446,6 +446,10 @@ int bowshock3_reset(bowshock3_batch* b);
  * cells; the forces add every face between a fluid and a solid cell (run3.rs:130-212). Resets every case to its free
  * stream. INVALID for an empty box or one outside the grid. */
 int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes);
+/* No counterpart in the reference. on (default 1): the first line pass stages its walk through shared memory where a
+ * warp's 32 lines are adjacent (i lines: nj a multiple of 32; j and k lines: ni a multiple of 32); 0 pins the unstaged
+ * walk. The results are the same bit for bit; only the speed differs. */
+int bowshock3_set_staging(bowshock3_batch* b, int on);
 /* iteration counter (first-order start-up) and CFL-ramp counter of every case */
 int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp);
 /* conserved state of case k, ni*nj*nk x 5 (Solver3::u layout) */
