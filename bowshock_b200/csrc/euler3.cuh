@@ -795,32 +795,29 @@ __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, i
   if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
 }
 
-// cp.async helpers of the staged line walks (16-byte chunks bypass L1; 4-byte copies for the strided right-hand sides)
+// cp.async helpers of the staged line walk (16-byte chunks, bypassing L1)
 __device__ __forceinline__ void cpa16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cpa4(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// The first pass with the walk staged through shared memory: the 32 lanes of a warp walk 32 adjacent lines, whose
-// records are adjacent in every plane, and the blocks lo, d, up (75 FP16 planes, 64 bytes per plane and step), the
-// right-hand side and the time step of step m + 2 are copied by cp.async while step m is computed. The loads of the
-// unstaged walk cannot move above the previous step's stores of M^-1 and Y, so every step of it waits a memory latency;
-// the arithmetic here is the same, in the same order, so the results are the unstaged kernel's bit for bit. The host
-// runs it when the lines of a warp are adjacent and every copy is 16-byte aligned (k3_staged_ok).
+// The first pass with the walk staged through shared memory: one warp per block walks 32 adjacent lines, whose records
+// are adjacent in every plane, and the blocks lo, d, up of step m + 2 (75 FP16 planes, 64 bytes per plane and step) are
+// copied by cp.async while step m is computed; the right-hand side and time step of step m + 1 are loaded into registers
+// before the arithmetic of step m (for the i lines they are strided by ni across the lanes). The loads of the unstaged
+// walk cannot move above the previous step's stores of M^-1 and Y, so every step of it waits a memory latency; the
+// arithmetic here is the same, in the same order, so the results are the unstaged kernel's bit for bit. One warp per
+// block and 14.4 KB of stages let 14 blocks share an SM, all the i lines of the 15-case sweep batch in one wave. The host
+// runs it where the lines of a warp are adjacent, which also aligns every copy to 16 bytes (Batch3::staged_ok).
 constexpr int ST3N = 3;  // stages: the copies run two steps ahead
 struct Stage3 {
   __half blk[75][32];  // planes R_LO .. R_UP + 24 of the warp's 32 lines
-  float r[5][32];      // right-hand side
-  float dt[32];
 };
-__global__ void __launch_bounds__(64) k3_lines_st(B3 B, int dir, const float* in, int from_res, float* out, int epilogue) {
-  __shared__ __align__(16) Stage3 S[2][ST3N];
+__global__ void __launch_bounds__(32) k3_lines_st(B3 B, int dir, const float* in, int from_res, float* out, int epilogue) {
+  __shared__ __align__(16) Stage3 S[ST3N];
   const long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = blockIdx.y, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int b = blockIdx.y, lane = threadIdx.x & 31;
   if (L >= nlines3(B, dir) || !B.active[b]) return;  // whole warps: the host launches it for line counts in multiples of 32
   const Case3Dev& cs = B.cs[b];
   const bool update = epilogue != 0 && (cs.sub_iters > 1 ? cs.sub_iters : 1) == 1;
@@ -830,53 +827,43 @@ __global__ void __launch_bounds__(64) k3_lines_st(B3 B, int dir, const float* in
   float* R = rec3(B, b, dir) + r0;
   __half* H = rec3h(B, b, dir) + r0;
   const long long nc = B.nc;
-  // lane 0's record and cell offsets: the lanes' records are adjacent; their cells too for the j and k lines, and nc apart
-  // ... ni apart for the i lines (the i records are transposed, the state is not)
-  const __half* Hw = rec3h(B, b, dir) + (r0 - lane);
-  const float* inb = in + (long long)b * 5 * nc;
-  const float* dtb = B.dt + (long long)b * nc;
+  const __half* Hw = rec3h(B, b, dir) + (r0 - lane);  // lane 0's records: the lanes' records are adjacent
   auto issue = [&](int m) {
     if (m < n) {
-      Stage3& st = S[wid][m % ST3N];
+      Stage3& st = S[m % ST3N];
       const long long rr = (long long)m * rs;
       for (int t = lane; t < 75 * 4; t += 32) {
         const int q = t >> 2, ch = t & 3;
         cpa16(&st.blk[q][8 * ch], Hw + (long long)(R_LO + q) * nc + rr + 8 * ch);
       }
-      const long long c = c0 + (long long)m * stride;
-      if (dir == 0) {  // strided cells: one 4-byte copy per lane and plane
-#pragma unroll
-        for (int v = 0; v < 5; ++v) cpa4(&st.r[v][lane], inb + v * nc + c);
-        if (from_res) cpa4(&st.dt[lane], dtb + c);
-      } else {
-        const long long cw = c - lane;
-        for (int t = lane; t < 5 * 8; t += 32) {
-          const int v = t >> 3, ch = t & 7;
-          cpa16(&st.r[v][4 * ch], inb + v * nc + cw + 4 * ch);
-        }
-        if (from_res && lane < 8) cpa16(&st.dt[4 * lane], dtb + cw + 4 * lane);
-      }
     }
     cpa_commit();
   };
+  auto rhs = [&](int m, V5<float>& r, float& dtc) {
+    const long long c = c0 + (long long)m * stride;
+    r = ldU(B, in, b, c);
+    dtc = from_res ? B.dt[(long long)b * nc + c] : 1.f;
+  };
   issue(0);
   issue(1);
+  V5<float> r_n;
+  float dt_n;
+  rhs(0, r_n, dt_n);
   M5<float> Y = zero5();
   V5<float> g{{0, 0, 0, 0, 0}};
   for (int m = 0; m < n; ++m) {
     cpa_wait1();  // the copies of step m are done (those of step m + 1 may still run)
     __syncwarp();
     issue(m + 2);  // into the stage step m - 1 used, which every lane has finished with
-    const Stage3& st = S[wid][m % ST3N];
+    const Stage3& st = S[m % ST3N];
     const long long rr = (long long)m * rs;
+    V5<float> r = r_n;
+    const float dtc = dt_n;
+    if (m + 1 < n) rhs(m + 1, r_n, dt_n);
     M5<float> d;
 #pragma unroll
     for (int q = 0; q < 25; ++q) d[q] = __half2float(st.blk[R_D + q][lane]);
-    V5<float> r;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) r[q] = st.r[q][lane];
     if (from_res) {
-      float dtc = st.dt[lane];
 #pragma unroll
       for (int q = 0; q < 5; ++q) r[q] *= dtc;
     }

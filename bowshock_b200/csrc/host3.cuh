@@ -402,7 +402,7 @@ struct Batch3 {
   bool staged_ok(int dir) const { return staged && (dir == 0 ? B.nj % 32 == 0 : B.ni % 32 == 0); }
   void launch_lines(int dir, long long nl, const float* in, int from_res, float* out, int epilogue) {
     if (staged_ok(dir))
-      k3_lines_st<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
+      k3_lines_st<<<grid_of(nl, 32), 32, 0, stream>>>(B, dir, in, from_res, out, epilogue);
     else
       k3_lines<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
   }
