@@ -904,6 +904,113 @@ __global__ void __launch_bounds__(32) k3_lines_st(B3 B, int dir, const float* in
   if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
 }
 
+// The defect-correction pass staged as k3_lines_st: the forward walk copies lo and M^-1 of step m + 2 (50 FP16 planes),
+// the backward walk Y of step m - 2 (25 planes), by cp.async into shared memory while it computes step m; the
+// right-hand side and g are loaded into registers one step ahead. Same arithmetic, same order: the results are
+// k3_lines_subst's bit for bit.
+struct StageS3 {
+  __half blk[50][32];  // forward: lo (0..24), M^-1 (25..49); backward: Y (0..24)
+};
+__global__ void __launch_bounds__(32) k3_lines_subst_st(B3 B, int dir, const float* in, float* out, int epilogue, int pass) {
+  __shared__ __align__(16) StageS3 S[ST3N];
+  const long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y, lane = threadIdx.x & 31;
+  if (L >= nlines3(B, dir) || !B.active[b]) return;  // whole warps
+  const Case3Dev& cs = B.cs[b];
+  const int s = cs.sub_iters > 1 ? cs.sub_iters : 1;
+  if (pass >= s) return;
+  const bool update = epilogue != 0 && pass == s - 1;
+  long long c0, stride, r0, rs;
+  int n;
+  line3(B, dir, L, c0, stride, n, r0, rs);
+  float* R = rec3(B, b, dir) + r0;
+  const long long nc = B.nc;
+  const __half* Hw = rec3h(B, b, dir) + (r0 - lane);
+  auto issue_f = [&](int m) {  // lo and M^-1 of step m
+    if (m < n) {
+      StageS3& st = S[m % ST3N];
+      const long long rr = (long long)m * rs;
+      for (int t = lane; t < 50 * 4; t += 32) {
+        const int q = t >> 2, ch = t & 3;
+        const int plane = q < 25 ? R_LO + q : R_MINV + (q - 25);
+        cpa16(&st.blk[q][8 * ch], Hw + (long long)plane * nc + rr + 8 * ch);
+      }
+    }
+    cpa_commit();
+  };
+  auto issue_b = [&](int m, int k) {  // Y of step m into stage k
+    if (m >= 0) {
+      StageS3& st = S[k % ST3N];
+      const long long rr = (long long)m * rs;
+      for (int t = lane; t < 25 * 4; t += 32) {
+        const int q = t >> 2, ch = t & 3;
+        cpa16(&st.blk[q][8 * ch], Hw + (long long)(R_Y + q) * nc + rr + 8 * ch);
+      }
+    }
+    cpa_commit();
+  };
+  issue_f(0);
+  issue_f(1);
+  V5<float> g{{0, 0, 0, 0, 0}};
+  V5<float> r_n = ldU(B, in, b, c0);
+  for (int m = 0; m < n; ++m) {
+    cpa_wait1();
+    __syncwarp();
+    issue_f(m + 2);
+    const StageS3& st = S[m % ST3N];
+    const long long rr = (long long)m * rs;
+    V5<float> r = r_n;
+    if (m + 1 < n) r_n = ldU(B, in, b, c0 + (m + 1) * stride);
+    if (m > 0) {
+      M5<float> lo;
+#pragma unroll
+      for (int q = 0; q < 25; ++q) lo[q] = __half2float(st.blk[q][lane]);
+      V5<float> t = mv5(lo, g);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) r[q] -= t[q];
+    }
+    M5<float> mi;
+#pragma unroll
+    for (int q = 0; q < 25; ++q) mi[q] = __half2float(st.blk[25 + q][lane]);
+    g = mv5(mi, r);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) R[(R_G + q) * nc + rr] = g[q];
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");  // the forward walk's trailing (empty) groups
+  __syncwarp();  // every lane's g stores and reads of the stages are done before the backward walk reuses them
+  V5<float> xn = g;
+  emit3(B, b, epilogue, update, out, c0 + (long long)(n - 1) * stride, xn);
+  if (n >= 2) {
+    // backward step k = 0, 1, ... handles cell m = n - 2 - k; its Y goes through stage k
+    issue_b(n - 2, 0);
+    issue_b(n - 3, 1);
+    V5<float> g_n;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) g_n[q] = R[(R_G + q) * nc + (n - 2) * rs];
+    for (int k = 0, m = n - 2; m >= 0; ++k, --m) {
+      cpa_wait1();
+      __syncwarp();
+      issue_b(m - 2, k + 2);
+      const StageS3& st = S[k % ST3N];
+      const long long c = c0 + m * stride;
+      M5<float> ym;
+#pragma unroll
+      for (int q = 0; q < 25; ++q) ym[q] = __half2float(st.blk[q][lane]);
+      V5<float> gm = g_n;
+      if (m > 0) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) g_n[q] = R[(R_G + q) * nc + (m - 1) * rs];
+      }
+      V5<float> t = mv5(ym, xn);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) gm[q] -= t[q];
+      emit3(B, b, epilogue, update, out, c, gm);
+      xn = gm;
+    }
+  }
+  if (update && L == 0) B.iter[b] += 1, B.ramp[b] += 1;
+}
+
 // Defect-correction pass `pass` >= 1: the same line solve with the kept factors (forward g = M^-1 (r - lo g_prev),
 // backward x = g - Y x_next).
 __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float* in, float* out, int epilogue, int pass) {

@@ -406,6 +406,12 @@ struct Batch3 {
     else
       k3_lines<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
   }
+  void launch_subst(int dir, long long nl, const float* in, float* out, int epilogue, int pass) {
+    if (staged_ok(dir))
+      k3_lines_subst_st<<<grid_of(nl, 32), 32, 0, stream>>>(B, dir, in, out, epilogue, pass);
+    else
+      k3_lines_subst<<<grid_of(nl, 128), 128, 0, stream>>>(B, dir, in, out, epilogue, pass);
+  }
   int max_sub() const {
     int s = 1;
     for (auto& c : cases) s = std::max(s, c.sub_iters);
@@ -424,9 +430,9 @@ struct Batch3 {
       for (int p = 1; p < max_sub(); ++p) {
         k3_defect_i<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
         k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
-        k3_lines_subst<<<grid_of(li, 128), 128, 0, stream>>>(B, 0, B.RR, B.X, 0, p);
-        k3_lines_subst<<<grid_of(lj, 128), 128, 0, stream>>>(B, 1, B.X, B.X, 0, p);
-        k3_lines_subst<<<grid_of(lk, 128), 128, 0, stream>>>(B, 2, B.X, nullptr, 2, p);
+        launch_subst(0, li, B.RR, B.X, 0, p);
+        launch_subst(1, lj, B.X, B.X, 0, p);
+        launch_subst(2, lk, B.X, nullptr, 2, p);
       }
     } else {  // SSP-RK3 (solver3.rs:303-314)
       launch_prep();
