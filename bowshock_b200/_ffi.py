@@ -166,6 +166,7 @@ SIGNATURES = {
     "bowshock_solver_set_run_control": (_I, [_P, _I]),
     "bowshock_arena_set_sst_coupling": (_I, [_P, _I]),
     "bowshock_solver_set_sst_coupling": (_I, [_P, _I]),
+    "bowshock_solver_set_mg_fusion": (_I, [_P, _I]),
     "bowshock_arena_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_arena_set_tuning": (_I, [_P, C.POINTER(LineTuning)]),
     "bowshock_arena_prepare": (_I, [_P, _U]),

@@ -157,6 +157,12 @@ __device__ __forceinline__ void pair_st(float4* hi, float4* lo, long long k, con
   lo[k] = make_float4((float)(q[0] - (double)h.x), (float)(q[1] - (double)h.y), (float)(q[2] - (double)h.z), (float)(q[3] - (double)h.w));
 }
 __device__ __forceinline__ V4<double> state_of(const Arena& A, long long k) { return pair_ld(A.U[k], A.Ulo[k]); }
+// q as pair_st stores it and state_of reads it back
+__device__ __forceinline__ V4<double> pair_round(const V4<double>& q) {
+  float4 h = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+  float4 l = make_float4((float)(q[0] - (double)h.x), (float)(q[1] - (double)h.y), (float)(q[2] - (double)h.z), (float)(q[3] - (double)h.w));
+  return pair_ld(h, l);
+}
 
 __device__ __forceinline__ int tile_at(const Arena& A) { return A.tile_list ? A.tile_list[blockIdx.x] : (int)blockIdx.x; }
 __device__ __forceinline__ int pblk_at(const Arena& A) { return A.pblk_list ? A.pblk_list[blockIdx.x] : (int)blockIdx.x; }

@@ -997,6 +997,13 @@ extern "C" int bowshock_solver_set_run_control(bowshock_solver* s, int on_device
   return BOWSHOCK_OK;
 }
 
+extern "C" int bowshock_solver_set_mg_fusion(bowshock_solver* s, int on) {
+  if (!s) return BOWSHOCK_INVALID;
+  s->ar.mg_fused = on != 0;
+  if (s->ar.graph) cudaGraphExecDestroy(s->ar.graph), s->ar.graph = nullptr;  // the chunk graph holds the old launches
+  return BOWSHOCK_OK;
+}
+
 extern "C" int bowshock_solver_set_sst_coupling(bowshock_solver* s, int coupled) {
   if (!s) return BOWSHOCK_INVALID;
   return from_arena(s, s->ar.set_sst_coupled(coupled != 0));

@@ -20,20 +20,16 @@
 namespace bk {
 
 __device__ __forceinline__ V4<float> Wat(const Arena& A, const CaseDev& c, int i, int j) { return from_f4(A.W[pidx(c, i, j)]); }
-__device__ __forceinline__ V4<double> prim_of(const Arena& A, const CaseDev& c, int i, int j) { return cons_to_prim(state_of(A, cidx(c, i, j))); }
 __device__ __forceinline__ V4<double> fs_of(const CaseDev& c) { return mk4<double>(c.fs[0], c.fs[1], c.fs[2], c.fs[3]); }
 
 // ==================================================================================== primitives + ghosts
-// FP64 from the state pair, stored as the pair (W, Wlo); the ghosts in FP64 as well.
-__global__ void k_prims(Arena A) {
-  int b = pblk_at(A);
-  int ci = A.pblk_case[b];
-  const CaseDev& c = A.cases[ci];
-  if (!A.active[ci]) return;
-  int p = (b - c.pblk_off) * blockDim.x + threadIdx.x;
-  int pw = c.ni + 4;
-  if (p >= pw * (c.nj + 4)) return;
-  int i = p % pw - 2, j = p / pw - 2;
+// FP64 from the state pair, stored as the pair (W, Wlo); the ghosts in FP64 as well. prims_at: the primitives of padded
+// position (i, j) of case c with both ghost layers and the block ghosts, from the conserved states `st(i, j)` of the
+// interior cells (k_prims: the stored states; the multigrid transfers of multigrid.cuh: the states after a restriction
+// or a prolongation, computed where they are read).
+template <class ST>
+__device__ __forceinline__ V4<double> prims_at(const Arena& A, const CaseDev& c, int i, int j, ST&& st) {
+  auto prim = [&](int a, int b) { return cons_to_prim(st(a, b)); };
   int ni = c.ni, nj = c.nj;
   V4<double> out;
   bool in_i = i >= 0 && i < ni, in_j = j >= 0 && j < nj;
@@ -43,9 +39,9 @@ __global__ void k_prims(Arena A) {
       // block ghost below a body / sting surface (solver.rs:457-471)
       int src = j0 + (j0 - 1 - j);
       float4 f = A.jface[jfidx(c, i, j0)];
-      out = wall_ghost<double>(prim_of(A, c, i, src), f.x, f.y, noslip_jface(c, i, j0));
+      out = wall_ghost<double>(prim(i, src), f.x, f.y, noslip_jface(c, i, j0));
     } else {
-      out = prim_of(A, c, i, j);
+      out = prim(i, j);
     }
   } else if (in_j && !in_i) {
     // i ghosts (solver.rs:429-439)
@@ -53,11 +49,11 @@ __global__ void k_prims(Arena A) {
     if (i < 0) {
       int k = -i;
       float4 f = A.iface[ifidx(c, 0, j)];
-      out = ghost_state<double>(c.bc[0], fs, prim_of(A, c, 0, j), prim_of(A, c, k - 1, j), f.x, f.y, -1.0);
+      out = ghost_state<double>(c.bc[0], fs, prim(0, j), prim(k - 1, j), f.x, f.y, -1.0);
     } else {
       int k = i - ni + 1;
       float4 f = A.iface[ifidx(c, ni, j)];
-      out = ghost_state<double>(c.bc[1], fs, prim_of(A, c, ni - 1, j), prim_of(A, c, ni - k, j), f.x, f.y, 1.0);
+      out = ghost_state<double>(c.bc[1], fs, prim(ni - 1, j), prim(ni - k, j), f.x, f.y, 1.0);
     }
   } else if (in_i && !in_j) {
     // j ghosts (solver.rs:440-451)
@@ -65,19 +61,31 @@ __global__ void k_prims(Arena A) {
     if (j < 0) {
       int k = -j;
       float4 f = A.jface[jfidx(c, i, 0)];
-      V4<double> mir = prim_of(A, c, i, k - 1);
+      V4<double> mir = prim(i, k - 1);
       if (noslip_jface(c, i, 0))
         out = wall_ghost<double>(mir, f.x, f.y, true);
       else
-        out = ghost_state<double>(c.bc[2], fs, prim_of(A, c, i, 0), mir, f.x, f.y, -1.0);
+        out = ghost_state<double>(c.bc[2], fs, prim(i, 0), mir, f.x, f.y, -1.0);
     } else {
       int k = j - nj + 1;
       float4 f = A.jface[jfidx(c, i, nj)];
-      out = ghost_state<double>(c.bc[3], fs, prim_of(A, c, i, nj - 1), prim_of(A, c, i, nj - k), f.x, f.y, 1.0);
+      out = ghost_state<double>(c.bc[3], fs, prim(i, nj - 1), prim(i, nj - k), f.x, f.y, 1.0);
     }
   } else {
     out = fs_of(c);  // corners: never read
   }
+  return out;
+}
+__global__ void k_prims(Arena A) {
+  int b = pblk_at(A);
+  int ci = A.pblk_case[b];
+  const CaseDev& c = A.cases[ci];
+  if (!A.active[ci]) return;
+  int p = (b - c.pblk_off) * blockDim.x + threadIdx.x;
+  int pw = c.ni + 4;
+  if (p >= pw * (c.nj + 4)) return;
+  int i = p % pw - 2, j = p / pw - 2;
+  V4<double> out = prims_at(A, c, i, j, [&](int a, int bb) { return state_of(A, cidx(c, a, bb)); });
   pair_st(A.W, A.Wlo, pidx(c, i, j), out);
 }
 
@@ -126,7 +134,30 @@ __device__ __forceinline__ V4<double> f2d(const float4& v) { return mk4<double>(
 // fluxes are spread over all NT, so with NT = 288 no thread computes more than two of them (three with 256); MINB blocks
 // per SM bound the registers. The arena's autotuner picks NT for the implicit iteration, with MINB = 3: the two compile to
 // the same arithmetic (checked bit for bit), whereas MINB = 2 rounds differently.
-template <int NT, int MINB>
+// FAS forcing of coarse cell (i, j) of case c (multigrid.rs:147-171): the volume-weighted mean residual of its fluid
+// children in the fine case, less its own residual as stored; nothing where every child is solid
+__device__ __forceinline__ void restrict_forcing_cell(const Arena& A, const CaseDev& c, int i, int j) {
+  const CaseDev& f = A.cases[c.fine_case];
+  double s[4] = {0, 0, 0, 0}, v = 0;
+  for (int d = 0; d < 4; ++d) {
+    int fi = 2 * i + (d & 1), fj = 2 * j + (d >> 1);
+    if (is_solid(f, fi, fj)) continue;
+    long long fc = cidx(f, fi, fj);
+    double vol = A.cellg[fc].x;
+    float4 r = A.R[fc];
+    s[0] += vol * r.x, s[1] += vol * r.y, s[2] += vol * r.z, s[3] += vol * r.w;
+    v += vol;
+  }
+  if (v > 0.0) {
+    long long cc = cidx(c, i, j);
+    float4 rc = A.R[cc];
+    A.FORCE[cc] = make_float4((float)(s[0] / v - rc.x), (float)(s[1] / v - rc.y), (float)(s[2] / v - rc.z), (float)(s[3] / v - rc.w));
+  }
+}
+
+// FORCING: the coarse level of a multigrid transfer; each cell also writes its FAS forcing from the residual it has just
+// stored (k_restrict_forcing folded into the coarse residual evaluation)
+template <int NT, int MINB, bool FORCING = false>
 __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int slot) {
   __shared__ __align__(128) float4 sW[TJ + 4][TI + 4];
   __shared__ __align__(128) float4 sWl[TJ + 4][TI + 4];
@@ -290,6 +321,7 @@ __global__ void __launch_bounds__(NT, MINB) k_residual(Arena A, int dt_kind, int
         A.dt[cc] = d;
       }
     }
+    if constexpr (FORCING) restrict_forcing_cell(A, c, i, j);
   }
   if (slot >= 0) {
 #pragma unroll

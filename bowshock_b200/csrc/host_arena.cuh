@@ -976,6 +976,9 @@ struct ArenaHost {
     else
       rk3(slot, last);
   }
+  // the multigrid restriction folded into the coarse level's primitives and residual evaluation (default), or the
+  // reference's order of separate transfer kernels (the same states bit for bit)
+  bool mg_fused = true;
   void mg_level(int l, int slot) {  // multigrid.rs:87-112
     const bool coarsest = l == mg_levels - 1;
     const int n_pre = coarsest ? mg_coarsest : mg_pre;
@@ -984,11 +987,21 @@ struct ArenaHost {
     if (coarsest) return;
     launch_mean_flow_prep();
     L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, (l == 0 && n_pre == 0) ? slot : -1); });
-    L(G_TRANSFER, [&] { k_restrict_state<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
-    set_level(l + 1);
-    launch_mean_flow_prep();
-    L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
-    L(G_TRANSFER, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+    if (mg_fused) {  // the restriction folded into the coarse level's primitives and residual (the same states)
+      set_level(l + 1);
+      L(G_TRANSFER, [&] { k_prims_restrict<<<LP(), 256, 0, stream>>>(A); });
+      if (any_viscous) {
+        L(G_VISC, [&] { k_visc_cell<<<LT(), TI * TJ, 0, stream>>>(A); });
+        L(G_VISC, [&] { k_visc_face<<<LT(), TI * TJ, 0, stream>>>(A); });
+      }
+      L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3, true><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+    } else {
+      L(G_TRANSFER, [&] { k_restrict_state<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+      set_level(l + 1);
+      launch_mean_flow_prep();
+      L(G_RESIDUAL, [&] { k_residual<TI * TJ, 3><<<ntiles, TI * TJ, 0, stream>>>(A, 0, -1); });
+      L(G_TRANSFER, [&] { k_restrict_forcing<<<ntiles, TI * TJ, 0, stream>>>(A, l + 1); });
+    }
     for (int g = 0; g < std::max(mg_gamma, 1); ++g) mg_level(l + 1, -1);
     L(G_TRANSFER, [&] { k_prolong<<<ntiles, TI * TJ, 0, stream>>>(A, l, mg_relax); });
     set_level(l);

@@ -139,6 +139,11 @@ class GpuSolver:
     def set_low_mach(self, on: bool):
         self._check(_ffi.load().bowshock_solver_set_low_mach(self._h, int(bool(on))))
 
+    def set_mg_fusion(self, on: bool):
+        """Multigrid restriction folded into the coarse level's kernels (True, the default) or as separate transfer
+        kernels in the reference's order (False); the same states."""
+        self._check(_ffi.load().bowshock_solver_set_mg_fusion(self._h, int(bool(on))))
+
     def set_sst_coupling(self, coupled: bool):
         """False (default): the reference's loosely coupled SST lines; True: the 6x6 block lines (Arena.set_sst_coupling)."""
         self._check(_ffi.load().bowshock_solver_set_sst_coupling(self._h, int(bool(coupled))))
