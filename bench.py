@@ -494,7 +494,9 @@ def measure_lift3(args, device):
 
 # algorithmic words of the FAS transfers per coarse cell (nv = 4): the restriction reads 4 fine cells x (state, defect,
 # volume) and writes the coarse state and forcing, the prolongation reads the coarse state and its start value and
-# reads and writes the 4 fine states
+# reads and writes the 4 fine states. The profile's transfer group times the restriction folded into the coarse level's
+# primitives (k_prims_restrict, which also converts the coarse states) and the prolongation; the forcing is written by the
+# coarse residual launch (timed with the residuals), so the figure is a lower bound.
 TRANSFER_WORDS = 4 * 9 + 8 + 8 + 4 * 8
 
 
