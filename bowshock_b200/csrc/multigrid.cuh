@@ -4,8 +4,7 @@
 //   k_restrict_state    U_c = sum V U / sum V over the fluid children, U_c^0 = U_c, forcing zeroed   (multigrid.rs:115-146)
 //   k_restrict_forcing  P_c = sum V R / sum V - R_c(U_c)                                            (multigrid.rs:147-171)
 // By default the restriction is folded into the coarse level's own kernels: k_prims_restrict restricts the state while
-// it converts it to primitives, and the coarse residual evaluation (k_residual<..., true>, with the local time step)
-// writes the forcing; the two stand-alone kernels remain for the unfused order (Arena::mg_fused). The prolongation stays a
+// it converts it to primitives, and the coarse residual evaluation (k_residual<..., true>) writes the forcing; the two stand-alone kernels remain for the unfused order (Arena::mg_fused). The prolongation stays a
 // kernel of its own: the fine primitives' ghost cells read states that other threads of that launch would correct.
 //   k_prolong           U += I (U_c - U_c^0): cell-centred bilinear weights 9/3/3/1 over the non-solid parents, the
 //                       correction halved up to 6 times until density and pressure stay positive    (multigrid.rs:177-218)

@@ -408,7 +408,7 @@ int bowshock_arena_set_case_groups(bowshock_arena* a, int groups);
 int bowshock_arena_set_sst_coupling(bowshock_arena* a, int coupled);
 int bowshock_solver_set_sst_coupling(bowshock_solver* s, int coupled);
 /* No counterpart in the reference. FAS multigrid transfers (multigrid.rs:115-171): on (default 1) the restriction of the
- * state is folded into the coarse level's primitives kernel and the forcing into its residual and time-step kernel; 0
+ * state is folded into the coarse level's primitives kernel and the forcing into its residual kernel; 0
  * launches the separate transfer kernels in the reference's order. The states are the same bit for bit. */
 int bowshock_solver_set_mg_fusion(bowshock_solver* s, int on);
 
