@@ -399,7 +399,7 @@ int bowshock_arena_set_tuning(bowshock_arena* a, const bowshock_line_tuning* t);
  * kernels run side by side; the states are those of one group bit for bit (every kernel touches only its own cases),
  * what changes is how many warps are in flight when few cases are left. */
 int bowshock_arena_set_case_groups(bowshock_arena* a, int groups);
-/* SST line systems (north_star (b): 6x6 SST blocks; the reference couples k and omega loosely, turbulence.rs:542-611).
+/* SST line systems (the reference couples k and omega loosely, turbulence.rs:542-611).
  * coupled = 0 (default): the reference's scheme, the mean flow's 4x4 lines and then the two scalar line systems of k and
  * omega. coupled = 1: the 6x6 block lines of (dU, dk, domega). The mean-flow operator freezes mu_t, so each 6x6 block
  * is lower block-triangular and the system is solved exactly by the 4x4 lines followed by the scalar lines with the
