@@ -157,3 +157,18 @@ def test_removing_the_boxes_restores_the_finless_batch():
         gpu.set_solid([((0, 0), (0, 1), (0, 1))])  # empty
     with pytest.raises(e3.BowshockError):
         gpu.set_solid([((0, 1), (0, 1), (0, dims[2] + 1))])  # outside the grid
+
+
+def test_fin_body_converged_forces_match_oracle():
+    """The afterbody fin box at M 2.5, 4 degrees, both sides run to run3.rs's stop rules (the density norm over the fluid
+    cells, CN sampled with the fin faces): the converged CN within 0.2 % and the centre of pressure within 2e-2 (the
+    tolerances of the finless case, the CN-stationary rule holding CN to 0.2 % over its window)."""
+    cpu, gpu, dims, boxes, c = _body_pair(2.5, 4.0, implicit=True, first_order=100)
+    x_base = c.body.x_base()
+    rc = cpu.run(x_base, max_iter=4000)
+    rg = gpu.solve(x_base, max_iter=4000)[0]
+    print("fin body", rc, rg)
+    assert rc["stop_reason"] in ("residual drop", "CN stationary"), rc
+    assert rg["stop_reason"] in ("residual drop", "CN stationary"), rg
+    assert abs(rg["cn"] - rc["cn"]) <= 2e-3 * abs(rc["cn"]) + 1e-4, (rg, rc)
+    assert abs(rg["x_cp"] - rc["x_cp"]) <= 2e-2, (rg, rc)

@@ -81,3 +81,29 @@ def test_coupled_sst_sweep_cases_match_the_oracle():
         assert r["iters"] == ref["iters"], k
         assert abs(r["cd_total"] - ref["cd_total"]) <= TOL, k
         assert abs(r["cd_total"] - r0["cd_total"]) <= 1e-5, k
+
+
+def test_coupling_touches_the_sst_cases_only():
+    """The 32-case sweep arena (16 Euler, 16 SST cases) for 200 iterations with coupled and with loose SST lines: every
+    Euler case's state is the same bit for bit (the coupling kernel and the SST line systems touch only SST cases), and
+    every SST case's mean flow differs (its turbulence rows, and through mu_t its later iterations, changed)."""
+    from bowshock_b200.arena import Arena
+    from bowshock_b200.sweep import sweep_cases
+    cs = sweep_cases()
+    states = {}
+    for coupled in (False, True):
+        a = Arena(cs)
+        a.set_sst_coupling(coupled)
+        a.run(200)
+        states[coupled] = [a.state(k) for k in range(len(cs))]
+        del a
+    n_sst = 0
+    for k, c in enumerate(cs):
+        same = np.array_equal(states[True][k], states[False][k])
+        assert np.all(np.isfinite(states[True][k]))
+        if c.viscous is None:  # Euler
+            assert same, k
+        else:
+            n_sst += 1
+            assert not same, k
+    assert n_sst == 16
