@@ -1168,6 +1168,10 @@ int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes
   if (!b || (nbox && !boxes)) return BOWSHOCK_INVALID;
   return b3from(b, b->b.set_solid((size_t)nbox, boxes));
 }
+int bowshock3_set_groups(bowshock3_batch* b, int groups) {
+  if (!b) return BOWSHOCK_INVALID;
+  return b3from(b, b->b.set_groups(groups));
+}
 int bowshock3_set_staging(bowshock3_batch* b, int on) {
   if (!b) return BOWSHOCK_INVALID;
   b->b.staged = on != 0;

@@ -314,6 +314,7 @@ struct Case3Dev {
 
 struct B3 {
   int ni, nj, nk, nb, axis_cells;
+  int b0;  // the first case of a launch: blockIdx.y + b0 is the case (a group of the batch's cases)
   long long nc, npad, nfi, nfj, nfk;
   const float4 *fi, *fj, *fk;  // (nx, ny, nz, area)
   const float2 *ri, *rj, *rk;  // face_rot (s, co)
@@ -359,7 +360,7 @@ __device__ __forceinline__ V5<double> fs3(const Case3Dev& c) { return V5<double>
 // ---------------------------------------------------------------- kernels
 __global__ void k3_prims(B3 B) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (t >= B.nc || !B.active[b]) return;
   int i = (int)(t % B.ni), j = (int)((t / B.ni) % B.nj), k = (int)(t / ((long long)B.ni * B.nj));
   V5<float> w = cons_to_prim3<float>(ldU(B, B.U, b, t));
@@ -369,7 +370,7 @@ __global__ void k3_prims(B3 B) {
 // ghosts of every boundary face column: i ends, j = 0 (axis or slip wall), j = nj, k ends (symmetry planes)
 __global__ void k3_ghosts(B3 B) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (!B.active[b]) return;
   const Case3Dev& c = B.cs[b];
   const long long njk = (long long)B.nj * B.nk, nik = (long long)B.ni * B.nk, nij = (long long)B.ni * B.nj;
@@ -425,7 +426,7 @@ __global__ void k3_ghosts(B3 B) {
 // face fluxes of direction dir (0 i, 1 j, 2 k), FP64, times the face area
 __global__ void k3_flux(B3 B, int dir) {
   long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   const long long nf = dir == 0 ? B.nfi : dir == 1 ? B.nfj : B.nfk;
   if (f >= nf || !B.active[b]) return;
   const Case3Dev& c = B.cs[b];
@@ -480,7 +481,7 @@ __global__ void k3_flux(B3 B, int dir) {
 __global__ void k3_residual(B3 B, int dt_kind, int slot) {
   __shared__ double sred[8];
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (!B.active[b]) return;
   const Case3Dev& cs = B.cs[b];
   double rr = 0.0;
@@ -532,7 +533,7 @@ __global__ void k3_residual(B3 B, int dt_kind, int slot) {
 
 __global__ void k3_stage(B3 B, float a, float bb, int copy, int last) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (c >= B.nc || !B.active[b]) return;
   if (last && c == 0) B.iter[b] += 1;
   if (B.solid && B.solid[c]) return;  // solver3.rs:317-327: fluid cells only
@@ -682,7 +683,7 @@ __device__ __forceinline__ void st5(__half* p, long long stride, const M5<float>
 // the transposed i records are written side by side; part 1: the j and k directions, threads ordered i fastest.
 __global__ void __launch_bounds__(128, 4) k3_assemble(B3 B, int part) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (t >= B.nc || !B.active[b]) return;
   int i, j, k;
   if (part == 0) {
@@ -742,7 +743,7 @@ __device__ __forceinline__ void emit3(const B3& B, int b, int epilogue, bool upd
 // Y and g for the defect-correction passes. in: the right-hand side (from_res: dt R).
 __global__ void __launch_bounds__(64) k3_lines(B3 B, int dir, const float* in, int from_res, float* out, int epilogue) {
   long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (L >= nlines3(B, dir) || !B.active[b]) return;
   const Case3Dev& cs = B.cs[b];
   const bool update = epilogue != 0 && (cs.sub_iters > 1 ? cs.sub_iters : 1) == 1;
@@ -817,7 +818,7 @@ struct Stage3 {
 __global__ void __launch_bounds__(32) k3_lines_st(B3 B, int dir, const float* in, int from_res, float* out, int epilogue) {
   __shared__ __align__(16) Stage3 S[ST3N];
   const long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = blockIdx.y, lane = threadIdx.x & 31;
+  const int b = B.b0 + (int)blockIdx.y, lane = threadIdx.x & 31;
   if (L >= nlines3(B, dir) || !B.active[b]) return;  // whole warps: the host launches it for line counts in multiples of 32
   const Case3Dev& cs = B.cs[b];
   const bool update = epilogue != 0 && (cs.sub_iters > 1 ? cs.sub_iters : 1) == 1;
@@ -914,7 +915,7 @@ struct StageS3 {
 __global__ void __launch_bounds__(32) k3_lines_subst_st(B3 B, int dir, const float* in, float* out, int epilogue, int pass) {
   __shared__ __align__(16) StageS3 S[ST3N];
   const long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = blockIdx.y, lane = threadIdx.x & 31;
+  const int b = B.b0 + (int)blockIdx.y, lane = threadIdx.x & 31;
   if (L >= nlines3(B, dir) || !B.active[b]) return;  // whole warps
   const Case3Dev& cs = B.cs[b];
   const int s = cs.sub_iters > 1 ? cs.sub_iters : 1;
@@ -1015,7 +1016,7 @@ __global__ void __launch_bounds__(32) k3_lines_subst_st(B3 B, int dir, const flo
 // backward x = g - Y x_next).
 __global__ void __launch_bounds__(128) k3_lines_subst(B3 B, int dir, const float* in, float* out, int epilogue, int pass) {
   long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (L >= nlines3(B, dir) || !B.active[b]) return;
   const Case3Dev& cs = B.cs[b];
   const int s = cs.sub_iters > 1 ? cs.sub_iters : 1;
@@ -1099,7 +1100,7 @@ __device__ __forceinline__ V5<float> apply3(const B3& B, int b, int dir, int i, 
 // the i-direction product A_i du into X (free between passes), threads ordered j fastest like the transposed i records
 __global__ void __launch_bounds__(128) k3_defect_i(B3 B, int pass) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (t >= B.nc || !B.active[b] || pass >= B.cs[b].sub_iters) return;
   int j = (int)(t % B.nj), i = (int)((t / B.nj) % B.ni), k = (int)(t / ((long long)B.ni * B.nj));
   long long c = cell3(B, i, j, k);
@@ -1109,7 +1110,7 @@ __global__ void __launch_bounds__(128) k3_defect_i(B3 B, int pass) {
 // defect of the unfactored operator (implicit3.rs:440-446): rr = dt R - (A_i du + A_j du + A_k du - 2 du), A_i du from X
 __global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b = blockIdx.y;
+  int b = B.b0 + (int)blockIdx.y;
   if (c >= B.nc || !B.active[b]) return;
   const Case3Dev& cs = B.cs[b];
   if (pass >= cs.sub_iters) return;

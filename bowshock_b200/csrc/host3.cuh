@@ -148,6 +148,10 @@ struct Batch3 {
   ~Batch3() { release(); }
   void release() {
     if (stream) cudaStreamSynchronize(stream);
+    for (cudaStream_t st : gst) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : gev) cudaEventDestroy(ev);
+    gst.clear(), gev.clear();
+    if (ev_fork3) cudaEventDestroy(ev_fork3), ev_fork3 = nullptr;
     for (void* p : owned)
       if (p) cudaFree(p);
     owned.clear();
@@ -386,7 +390,52 @@ struct Batch3 {
     return 0;
   }
 
-  dim3 grid_of(long long n, int threads) const { return dim3((unsigned)((n + threads - 1) / threads), (unsigned)B.nb); }
+  // Case groups: with groups > 1 the cases are split into that many groups of consecutive cases and each group's
+  // iterations of a chunk run on a stream of their own (the launches of a group cover its cases only: B.b0, gnb), so
+  // one group's kernels fill the SMs while another's last wave runs. Every kernel touches only its own cases, so the
+  // states are those of one group bit for bit (the norms' atomic block sums aside).
+  int groups = 1, gnb = 0;
+  std::vector<cudaStream_t> gst;
+  std::vector<cudaEvent_t> gev;
+  cudaEvent_t ev_fork3 = nullptr;
+  int set_groups(int n) {
+    if (n < 1 || n > 4 || n > B.nb) {
+      err = "case groups out of range (1 to 4, at most the case count)";
+      return 2;
+    }
+    while ((int)gst.size() < n) {
+      cudaStream_t st;
+      cudaEvent_t ev;
+      BK3_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      BK3_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      gst.push_back(st), gev.push_back(ev);
+    }
+    if (!ev_fork3) BK3_CUDA(cudaEventCreateWithFlags(&ev_fork3, cudaEventDisableTiming));
+    groups = n;
+    return 0;
+  }
+  dim3 grid_of(long long n, int threads) const { return dim3((unsigned)((n + threads - 1) / threads), (unsigned)(gnb ? gnb : B.nb)); }
+  // `chunk` iterations of every active case, per group on its own stream between a fork and a join on `stream`
+  void launch_chunk(int chunk) {
+    if (groups <= 1) {
+      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      return;
+    }
+    const cudaStream_t main = stream;
+    cudaEventRecord(ev_fork3, main);
+    for (int g = 0; g < groups; ++g) {
+      const int lo = (int)((long long)B.nb * g / groups), hi = (int)((long long)B.nb * (g + 1) / groups);
+      if (hi <= lo) continue;
+      stream = gst[g];
+      cudaStreamWaitEvent(stream, ev_fork3, 0);
+      B.b0 = lo, gnb = hi - lo;
+      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      cudaEventRecord(gev[g], stream);
+    }
+    stream = main;
+    B.b0 = 0, gnb = 0;
+    for (int g = 0; g < groups; ++g) cudaStreamWaitEvent(stream, gev[g], 0);
+  }
   void launch_prep() {
     k3_prims<<<grid_of(B.nc, 256), 256, 0, stream>>>(B);
     long long ng = 2LL * B.nj * B.nk + 2LL * B.ni * B.nk + 2LL * B.ni * B.nj;
@@ -456,7 +505,7 @@ struct Batch3 {
       int chunk = (int)std::min<long long>(n - done, slots);
       BK3_CUDA(cudaMemsetAsync(B.rsum, 0, (size_t)chunk * nb * sizeof(double), stream));
       BK3_CUDA(cudaEventRecord(ev0, stream));
-      for (int k = 0; k < chunk; ++k) launch_iteration(k);
+      launch_chunk(chunk);
       BK3_CUDA(cudaGetLastError());
       BK3_CUDA(cudaEventRecord(ev1, stream));
       h.resize((size_t)chunk * nb);

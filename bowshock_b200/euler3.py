@@ -41,6 +41,7 @@ SIGNATURES3 = {
     "bowshock3_reset": (_I, [_P]),
     "bowshock3_set_solid": (_I, [_P, _U, C.POINTER(_U)]),
     "bowshock3_set_staging": (_I, [_P, _I]),
+    "bowshock3_set_groups": (_I, [_P, _I]),
     "bowshock3_set_iter": (_I, [_P, _U, _U]),
     "bowshock3_set_state": (_I, [_P, _U, _dp]),
     "bowshock3_state": (_I, [_P, _U, _dp]),
@@ -140,6 +141,10 @@ class Batch3:
     def set_staging(self, on):
         """The first line pass staged through shared memory where the grid allows it (default on); same results."""
         self._check(lib().bowshock3_set_staging(self._h, int(bool(on))))
+
+    def set_groups(self, groups):
+        """Split the cases into 1 to 4 groups whose iterations run on streams of their own (the same states)."""
+        self._check(lib().bowshock3_set_groups(self._h, int(groups)))
 
     def set_iter(self, it, ramp=None):
         self._check(lib().bowshock3_set_iter(self._h, int(it), int(it if ramp is None else ramp)))

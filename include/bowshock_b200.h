@@ -454,6 +454,10 @@ int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes
  * warp's 32 lines are adjacent (i lines: nj a multiple of 32; j and k lines: ni a multiple of 32); 0 pins the unstaged
  * walk. The results are the same bit for bit; only the speed differs. */
 int bowshock3_set_staging(bowshock3_batch* b, int on);
+/* No counterpart in the reference. groups (1 to 4, at most the case count; default 1): the cases split into that many
+ * groups of consecutive cases whose iterations run on streams of their own, so one group's kernels fill the SMs while
+ * another's last wave runs. The states are the same bit for bit. INVALID out of range. */
+int bowshock3_set_groups(bowshock3_batch* b, int groups);
 /* iteration counter (first-order start-up) and CFL-ramp counter of every case */
 int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp);
 /* conserved state of case k, ni*nj*nk x 5 (Solver3::u layout) */

@@ -167,3 +167,26 @@ def test_staged_first_pass_is_bit_identical(dims):
         for a, c in zip(s1, s0):
             assert np.array_equal(a, c)
         assert np.max(np.abs(r1 - r0) / r0) < 1e-12
+
+
+def test_case_groups_are_bit_identical():
+    """bowshock3_set_groups: the batch's cases split into 2 or 3 groups whose iterations run on streams of their own give
+    the states of one group bit for bit (every kernel touches only its own cases) after 6 implicit iterations."""
+    import bowshock_b200.euler3 as e3
+    cases = e3.lift_sweep_cases((0.0, 4.0, 8.0), (0.8, 2.5), ni=96, nj=32, nk=32)
+    ref = None
+    for groups in (1, 2, 3):
+        b, _ = e3.batch_of(cases)
+        b.set_groups(groups)
+        r = b.run(6)
+        st = [b.state(k) for k in range(len(cases))]
+        del b
+        if ref is None:
+            ref = (r, st)
+            continue
+        for a, c in zip(st, ref[1]):
+            assert np.array_equal(a, c)
+        assert np.max(np.abs(r - ref[0]) / ref[0]) < 1e-12
+    b, _ = e3.batch_of(cases)
+    with pytest.raises(e3.BowshockError):
+        b.set_groups(5)
