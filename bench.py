@@ -627,6 +627,8 @@ def run_kernels(args):
     from bowshock_b200.arena import Arena
     cases = build_cases()
     arena = Arena(cases, device=int(os.environ.get("LOCAL_RANK", "0")))
+    if args.sst_coupled:  # the coupled 6x6 SST lines instead of the reference's loose coupling
+        arena.set_sst_coupling(True)
     arena.run(max(args.warmup, 3))
     if args.workload == "tail6":  # the census's last ~8,650 iterations: only the 6 mean-stationary SST cases left
         arena.set_active([1 if k in TAIL6 else 0 for k in range(len(cases))])
@@ -641,7 +643,7 @@ def run_kernels(args):
     ms = arena.ms_per_iter()
     prof = {g: round(v[0] / v[1], 4) for g, v in arena.profile(3).items() if v[1]} if args.steps >= 10 else None
     return {"kernels_only": True, "workload": args.workload, "cells": arena.cells, "steps": args.steps, "ms_per_step": ms, "ms_per_launch": prof,
-            "autotuned_lines_per_block": arena.tuning(), "case_groups": args.groups}
+            "autotuned_lines_per_block": arena.tuning(), "case_groups": args.groups, "sst_coupled": args.sst_coupled}
 
 
 def main():
@@ -653,6 +655,7 @@ def main():
     ap.add_argument("--kernels-only", action="store_true", help="only the timed arena iterations (for ncu captures)")
     ap.add_argument("--workload", default="sweep32", choices=["sweep32", "tail6", "lift3", "lift3s", "net"], help="workload of --kernels-only")
     ap.add_argument("--groups", type=int, default=1, help="case groups of the arena's graph in --kernels-only (1-4)")
+    ap.add_argument("--sst-coupled", action="store_true", help="coupled SST lines in the --kernels-only arena")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # one process per GPU: start the ranks here when the command was not launched by torchrun
