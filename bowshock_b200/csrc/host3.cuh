@@ -313,19 +313,21 @@ struct Batch3 {
           err = "solid box out of the grid or empty";
           return 2;
         }
-    std::fill(solid_h.begin(), solid_h.end(), 0);
+    std::vector<unsigned char> mask((size_t)B.nc, 0);
     for (size_t q = 0; q < nbox; ++q) {
       const uint64_t* r = boxes + 6 * q;
       for (uint64_t k = r[4]; k < r[5]; ++k)
         for (uint64_t j = r[2]; j < r[3]; ++j)
-          for (uint64_t i = r[0]; i < r[1]; ++i) solid_h[(k * B.nj + j) * B.ni + i] = 1;
+          for (uint64_t i = r[0]; i < r[1]; ++i) mask[(k * B.nj + j) * B.ni + i] = 1;
     }
-    n_active = 0;
-    for (unsigned char v : solid_h) n_active += v ? 0 : 1;
-    if (n_active == 0) {
+    long long fluid = 0;
+    for (unsigned char v : mask) fluid += v ? 0 : 1;
+    if (fluid == 0) {  // refused with the batch as it was
       err = "every cell is solid";
       return 2;
     }
+    solid_h.swap(mask);
+    n_active = fluid;
     int rc;
     if (!d_solid && (rc = alloc(&d_solid, (size_t)B.nc))) return rc;
     BK3_CUDA(copy_sync(stream, d_solid, solid_h.data(), (size_t)B.nc, cudaMemcpyHostToDevice));
