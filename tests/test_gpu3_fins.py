@@ -157,6 +157,10 @@ def test_removing_the_boxes_restores_the_finless_batch():
         gpu.set_solid([((0, 0), (0, 1), (0, 1))])  # empty
     with pytest.raises(e3.BowshockError):
         gpu.set_solid([((0, 1), (0, 1), (0, dims[2] + 1))])  # outside the grid
+    with pytest.raises(e3.BowshockError):
+        gpu.set_solid([((0, dims[0]), (0, dims[1]), (0, dims[2]))])  # every cell: refused, the batch as it was
+    r3 = gpu.run(2)
+    assert np.all(np.isfinite(r3)) and np.all(r3 > 0)
 
 
 def test_fin_body_converged_forces_match_oracle():
