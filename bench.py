@@ -15,6 +15,8 @@ Metric: converged cases per hour on one B200 at |dCD| <= 1e-4 against the FP64 o
                 launch), wall clock, reported as config.plain_single_case_cases_per_hr.
   cpu_baseline  the oracle (f64 C++ restatement of the reference CPU path, all host threads) timed on a bounded sample of
                 iterations of every case, times the oracle's own iteration counts to its stop rules (one GPU only).
+  secondary     (one GPU) in config: the census with the learned warm start, the census with the coupled 6x6 SST lines,
+                the 3D lift batch, multigrid against the single grid, the device mesher.
   --gpus N      one process per GPU (started here through torch.distributed.run unless launched by it): the 32 cases are
                 partitioned over the ranks (longest processing time on cells x expected iterations, bowshock_b200.shard),
                 each rank runs its share in its own arena, the point results are gathered (gloo, host objects); times
@@ -342,6 +344,7 @@ def run_ours(args, rank, world, dist):
     traffic = line_sweep_traffic()
     learned = secondary(learned_census, all_cases, all_grids, fx, plain_cases_per_hr, device) if world == 1 else None
     lift3 = secondary(measure_lift3, args, device) if world == 1 else None
+    coupled = secondary(sst_coupled_census, all_cases, all_grids, fx, results, census_dev_s, device) if world == 1 else None
     mg0 = secondary(measure_multigrid, device) if world == 1 else None
     mesh = secondary(measure_mesher, device) if world == 1 else None
     cpu_base = None
@@ -385,6 +388,7 @@ def run_ours(args, rank, world, dist):
             "kernel_profile_ms_per_launch": {g: v[0] / v[1] for g, v in groups.items()},
             "autotuned_lines_per_block": tuning,
             "lift3": lift3,
+            "sst_coupled": coupled,
             "device_mesher": mesh,
             "multigrid": mg0,
             "parallelism": (f"cases partitioned over {world} GPUs (longest-processing-time on cells x expected iterations), results "
@@ -414,6 +418,30 @@ def secondary(fn, *a):
         return fn(*a)
     except Exception as e:  # reported in the line, not fatal to the headline measurement
         return {"error": f"{type(e).__name__}: {e}"}
+
+
+def sst_coupled_census(cases, grids, fx, loose, loose_dev_s, device):
+    """The census again with the coupled 6x6 SST lines (Arena.set_sst_coupling; the default and the headline run the
+    reference's loose coupling): device time, stop iterations and CDs against the loose census and the oracle. The Euler
+    cases are untouched by the option; the CD-stationary SST cases reach the same CDs; the mean-stationary (limit-cycle)
+    SST cases' window means move with any change of the iteration path."""
+    from bowshock_b200.arena import Arena
+    a = Arena(cases, device=device, grids=grids)
+    a.set_sst_coupling(True)
+    res = a.solve()
+    dev_s = a.last_solve_ms() / 1000.0
+    del a
+    sst = [k for k, c in enumerate(cases) if c.viscous is not None]
+    cds = [k for k in sst if loose[k]["stop_reason"] == "CD stationary"]
+    euler = [k for k in range(len(cases)) if k not in sst]
+    dcd = {k: cd_error(res[k], fx[k]) for k in range(len(cases)) if k in fx}
+    return {"census_device_s": dev_s, "loose_census_device_s": loose_dev_s,
+            "converged_within_1e-4": sum(abs(d) <= 1e-4 for d in dcd.values()), "checked_against_oracle": len(dcd),
+            "euler_cd_identical": all(res[k]["cd_total"] == loose[k]["cd_total"] for k in euler),
+            "sst_same_stop_iterations": sum(res[k]["iters"] == loose[k]["iters"] for k in sst), "sst_cases": len(sst),
+            "max_dcd_vs_loose_cd_stationary": max(abs(res[k]["cd_total"] - loose[k]["cd_total"]) for k in cds) if cds else None,
+            "dcd_vs_loose_limit_cycle": {str(k): float(f"{res[k]['cd_total'] - loose[k]['cd_total']:.3e}") for k in sst if k not in cds},
+            "dcd": {str(k): float(f"{d:.3e}") for k, d in dcd.items()}}
 
 
 def learned_census(cases, grids, fx, plain_cases_per_hr, device):
