@@ -437,7 +437,9 @@ def sst_coupled_census(cases, grids, fx, loose, loose_dev_s, device):
     dcd = {k: cd_error(res[k], fx[k]) for k in range(len(cases)) if k in fx}
     return {"census_device_s": dev_s, "loose_census_device_s": loose_dev_s,
             "converged_within_1e-4": sum(abs(d) <= 1e-4 for d in dcd.values()), "checked_against_oracle": len(dcd),
-            "euler_cd_identical": all(res[k]["cd_total"] == loose[k]["cd_total"] for k in euler),
+            # the option touches no Euler case (their states are the same bit for bit over fixed iteration counts); a
+            # census stops on FP64 norms summed by atomics in no fixed order, so two solves can differ in the last bits
+            "max_dcd_vs_loose_euler": max(abs(res[k]["cd_total"] - loose[k]["cd_total"]) for k in euler) if euler else None,
             "sst_same_stop_iterations": sum(res[k]["iters"] == loose[k]["iters"] for k in sst), "sst_cases": len(sst),
             "max_dcd_vs_loose_cd_stationary": max(abs(res[k]["cd_total"] - loose[k]["cd_total"]) for k in cds) if cds else None,
             "dcd_vs_loose_limit_cycle": {str(k): float(f"{res[k]['cd_total'] - loose[k]['cd_total']:.3e}") for k in sst if k not in cds},
