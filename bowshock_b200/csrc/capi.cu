@@ -1211,6 +1211,14 @@ int bowshock3_forces(bowshock3_batch* b, double x_max, double* out) {
   std::memcpy(out, f.data(), f.size() * sizeof(double));
   return BOWSHOCK_OK;
 }
+int bowshock3_forces_parts(bowshock3_batch* b, double x_max, double x_nose, double* out) {
+  if (!b || !out) return BOWSHOCK_INVALID;
+  std::vector<double> f;
+  int rc = b->b.forces_parts(x_max, x_nose, f);
+  if (rc) return b3from(b, rc);
+  std::memcpy(out, f.data(), f.size() * sizeof(double));
+  return BOWSHOCK_OK;
+}
 int bowshock3_solve(bowshock3_batch* b, const bowshock3_run_params* p, bowshock3_result* out) {
   if (!b || !p || !out) return BOWSHOCK_INVALID;
   bk3::Batch3& B = b->b;

@@ -1133,8 +1133,62 @@ __global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
 
 // FP64 wall forces of every case (run3.rs:130-212): one block per case. wall: WALL3 doubles per wall face, the j = 0 body
 // faces (i >= axis_cells, fluid cells) and every face between a fluid and a solid cell: n[3], area, c[3], the centroid of
-// the first fluid cell a and of the fluid cell b behind it, a, b (-1: none), and the sign that turns n into the body.
-constexpr int WALL3 = 16;
+// the first fluid cell a and of the fluid cell b behind it, a, b (-1: none), the sign that turns n into the body, and the
+// part of the surface (0 body wall, 2 fin sides (k faces), 3 fin edges (i faces), 4 fin tips (j faces)).
+constexpr int WALL3 = 17;
+// the wall pressure of face record w of case b (run3.rs:150-160): extrapolated from the first two fluid cells
+__device__ __forceinline__ double wall_pressure3(const B3& B, int b, const double* w) {
+  auto pres = [&](long long cc) {
+    const float* p = B.U + (long long)b * 5 * B.nc + cc;
+    double rho = p[0], u = p[B.nc] / rho, v = p[2 * B.nc] / rho, ww = p[3 * B.nc] / rho;
+    return (GD - 1.0) * ((double)p[4 * B.nc] - 0.5 * rho * (u * u + v * v + ww * ww));
+  };
+  const long long ca = (long long)w[13], cb = (long long)w[14];
+  double p0 = pres(ca), pw = p0;
+  if (cb >= 0) {
+    double d0 = sqrt((w[7] - w[4]) * (w[7] - w[4]) + (w[8] - w[5]) * (w[8] - w[5]) + (w[9] - w[6]) * (w[9] - w[6]));
+    double d1 = sqrt((w[10] - w[4]) * (w[10] - w[4]) + (w[11] - w[5]) * (w[11] - w[5]) + (w[12] - w[6]) * (w[12] - w[6]));
+    pw = p0 + (p0 - pres(cb)) * d0 / (d1 - d0);
+  }
+  return pw;
+}
+// run3.rs:85-127 `breakdown_on`: the forces of every case split into nose (body wall with centroid x <= x_nose),
+// afterbody, fin sides, fin edges and fin tips; out: (cn, ca, x_cp) x 5 parts x cases
+__global__ void k3_forces_parts(B3 B, const double* wall, int nwall, double x_max, double x_nose, double* out) {
+  __shared__ double acc[15][128];
+  int b = blockIdx.x;
+  double p_inf = B.cs[b].fs[4];
+  double a[15];
+#pragma unroll
+  for (int q = 0; q < 15; ++q) a[q] = 0.0;
+  for (int q = threadIdx.x; q < nwall; q += blockDim.x) {
+    const double* w = wall + WALL3 * (long long)q;
+    if (w[4] > x_max) continue;
+    int part = (int)w[16];
+    if (part == 0 && w[4] > x_nose) part = 1;
+    const double dd = (wall_pressure3(B, b, w) - p_inf) * w[3] * w[15];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      if (k == part) a[3 * k] += dd * w[0], a[3 * k + 1] += dd * w[2], a[3 * k + 2] += dd * w[2] * w[4];
+  }
+#pragma unroll
+  for (int q = 0; q < 15; ++q) acc[q][threadIdx.x] = a[q];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int q = 0; q < 15; ++q) acc[q][threadIdx.x] += acc[q][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) {
+    const int k = threadIdx.x;
+    double mach = sqrt(B.cs[b].fs[1] * B.cs[b].fs[1] + B.cs[b].fs[3] * B.cs[b].fs[3]);
+    double norm = 2.0 / (0.5 * mach * mach * (M_PI / 4.0));
+    const double fx = acc[3 * k][0], fz = acc[3 * k + 1][0], mz = acc[3 * k + 2][0];
+    out[15 * b + 3 * k] = norm * fz;
+    out[15 * b + 3 * k + 1] = norm * fx;
+    out[15 * b + 3 * k + 2] = fabs(fz) < 1e-12 ? NAN : mz / fz;
+  }
+}
 __global__ void k3_forces(B3 B, const double* wall, int nwall, double x_max, double* out) {
   __shared__ double acc[3][256];
   int b = blockIdx.x;

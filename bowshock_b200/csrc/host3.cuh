@@ -142,7 +142,7 @@ struct Batch3 {
   double last_ms_per_iter = 0.0;
   std::string err;
   std::vector<void*> owned;
-  double *d_wall = nullptr, *d_forces = nullptr;
+  double *d_wall = nullptr, *d_forces = nullptr, *d_parts = nullptr;
   std::vector<int> h_active;
 
   ~Batch3() { release(); }
@@ -232,7 +232,7 @@ struct Batch3 {
         (rc = alloc(&B.X, ns)) || (rc = alloc(&B.DU, ns)) || (rc = alloc(&B.RR, ns)) || (rc = alloc(&B.dt, (size_t)nb * B.nc)) ||
         (rc = alloc(&B.scr, (size_t)nb * 3 * REC3 * B.nc)) || (rc = alloc(&B.FI, (size_t)nb * 5 * B.nfi)) || (rc = alloc(&B.FJ, (size_t)nb * 5 * B.nfj)) ||
         (rc = alloc(&B.FK, (size_t)nb * 5 * B.nfk)) || (rc = alloc(&B.rsum, (size_t)slots * nb)) || (rc = alloc(&d_wall, wall_cap)) ||
-        (rc = alloc(&d_forces, 3 * (size_t)nb)))
+        (rc = alloc(&d_forces, 3 * (size_t)nb)) || (rc = alloc(&d_parts, 15 * (size_t)nb)))
       return rc;
     auto up_faces = [&](const std::vector<double>& f, long long n, float4* d4, float2* d2) -> int {
       std::vector<float4> h4(n);
@@ -266,16 +266,18 @@ struct Batch3 {
     auto cell = [&](size_t i, size_t j, size_t k) { return (k * nj + j) * ni + i; };
     auto sol = [&](size_t i, size_t j, size_t k) { return solid_h[cell(i, j, k)] != 0; };
     wall.clear();
+    int part = 0;  // run3.rs:130-212: 0 body wall, 2 fin sides (k faces), 3 fin edges (i faces), 4 fin tips (j faces)
     auto add = [&](const double* f, size_t a, long long b, double sign) {
       for (int q = 0; q < 7; ++q) wall.push_back(f[q]);
       for (int q = 0; q < 3; ++q) wall.push_back(g.xc[3 * a + q]);
       for (int q = 0; q < 3; ++q) wall.push_back(b >= 0 ? g.xc[3 * (size_t)b + q] : 0.0);
-      wall.push_back((double)a), wall.push_back((double)b), wall.push_back(sign);
+      wall.push_back((double)a), wall.push_back((double)b), wall.push_back(sign), wall.push_back((double)part);
     };
     for (size_t k = 0; k < nk; ++k)
       for (size_t i = (size_t)B.axis_cells; i < ni; ++i)
         if (!sol(i, 0, k)) add(&g.fj[7 * (k * (nj + 1) * ni + i)], cell(i, 0, k), nj > 1 && !sol(i, 1, k) ? (long long)cell(i, 1, k) : -1, -1.0);
     if (n_active != B.nc) {
+      part = 3;
       for (size_t k = 0; k < nk; ++k)
         for (size_t j = 0; j < nj; ++j)
           for (size_t i = 1; i < ni; ++i) {
@@ -284,6 +286,7 @@ struct Batch3 {
             if (!a && b) add(f, cell(i - 1, j, k), i >= 2 && !sol(i - 2, j, k) ? (long long)cell(i - 2, j, k) : -1, 1.0);
             if (a && !b) add(f, cell(i, j, k), i + 1 < ni && !sol(i + 1, j, k) ? (long long)cell(i + 1, j, k) : -1, -1.0);
           }
+      part = 4;
       for (size_t k = 0; k < nk; ++k)
         for (size_t j = 1; j < nj; ++j)
           for (size_t i = 0; i < ni; ++i) {
@@ -292,6 +295,7 @@ struct Batch3 {
             if (!a && b) add(f, cell(i, j - 1, k), j >= 2 && !sol(i, j - 2, k) ? (long long)cell(i, j - 2, k) : -1, 1.0);
             if (a && !b) add(f, cell(i, j, k), j + 1 < nj && !sol(i, j + 1, k) ? (long long)cell(i, j + 1, k) : -1, -1.0);
           }
+      part = 2;
       for (size_t k = 1; k < nk; ++k)
         for (size_t j = 0; j < nj; ++j)
           for (size_t i = 0; i < ni; ++i) {
@@ -545,6 +549,15 @@ struct Batch3 {
         for (int v = 0; v < 5; ++v) res[5 * c + v] = h[v * B.nc + c];
       if (dt) dt[c] = hd[c];
     }
+    return 0;
+  }
+  // (cn, ca, x_cp) of the 5 parts of every case (k3_forces_parts)
+  int forces_parts(double x_max, double x_nose, std::vector<double>& out) {
+    k3_forces_parts<<<B.nb, 128, 0, stream>>>(B, d_wall, nwall, x_max, x_nose, d_parts);
+    BK3_CUDA(cudaGetLastError());
+    out.resize(15 * (size_t)B.nb);
+    BK3_CUDA(cudaMemcpyAsync(out.data(), d_parts, out.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    BK3_CUDA(cudaStreamSynchronize(stream));
     return 0;
   }
   int forces(double x_max, std::vector<double>& out) {

@@ -48,6 +48,7 @@ SIGNATURES3 = {
     "bowshock3_run": (_I, [_P, _U, _dp]),
     "bowshock3_eval_residual": (_I, [_P, _U, _dp, _dp, _dp]),
     "bowshock3_forces": (_I, [_P, _D, _dp]),
+    "bowshock3_forces_parts": (_I, [_P, _D, _D, _dp]),
     "bowshock3_solve": (_I, [_P, C.POINTER(RunParams3C), C.POINTER(Result3C)]),
     "bowshock3_last_ms_per_iter": (_I, [_P, _dp]),
 }
@@ -172,6 +173,15 @@ class Batch3:
         out = np.zeros(3 * self.nb)
         self._check(lib().bowshock3_forces(self._h, float(x_max), _p(out)))
         return [dict(cn=out[3 * k], ca=out[3 * k + 1], x_cp=out[3 * k + 2]) for k in range(self.nb)]
+
+    PARTS = ("nose", "afterbody", "fin_sides", "fin_edges", "fin_tips")
+
+    def forces_parts(self, x_max, x_nose):
+        """run3.rs `breakdown_on`: per case {part: dict(cn, ca, x_cp)} for the parts of PARTS."""
+        out = np.zeros(15 * self.nb)
+        self._check(lib().bowshock3_forces_parts(self._h, float(x_max), float(x_nose), _p(out)))
+        return [{p: dict(cn=out[15 * k + 3 * q], ca=out[15 * k + 3 * q + 1], x_cp=out[15 * k + 3 * q + 2]) for q, p in enumerate(self.PARTS)}
+                for k in range(self.nb)]
 
     def solve(self, x_max, max_iter=8000, rel_tol=0.002, window=500):
         p = RunParams3C(int(max_iter), float(rel_tol), int(window), float(x_max))

@@ -467,6 +467,10 @@ int bowshock3_state(bowshock3_batch* b, uint64_t k, double* u);
 int bowshock3_run(bowshock3_batch* b, uint64_t n, double* residual);
 /* residual (ncell x 5) and time step of case k for the current state (no update); density residual of case k */
 int bowshock3_eval_residual(bowshock3_batch* b, uint64_t k, double* res, double* dt, double* density_residual);
+/* run3.rs:85-127 `breakdown_on` / `LiftBreakdown`: the same forces split into 5 parts, nose (body wall with centroid
+ * x <= x_nose), afterbody, fin sides (k faces of the solid boxes), fin edges (i faces) and fin tips (j faces); out:
+ * (cn, ca, x_cp) x 5 parts x ncases, x_cp NaN where a part's normal force is below 1e-12 */
+int bowshock3_forces_parts(bowshock3_batch* b, double x_max, double x_nose, double* out);
 /* FP64 pressure forces of every case: (cn, ca, x_cp) x ncases (run3.rs `forces_on`: body wall and fin faces) */
 int bowshock3_forces(bowshock3_batch* b, double x_max, double* out);
 /* cold start of every case, iterated to the stop rules with per-case masks (run3.rs:220-330) */

@@ -633,6 +633,7 @@ def lib3():
             "orc3_reflection": (None, [dp, dp]),
             "orc3_set_solid": (None, [P, U, C.POINTER(U)]),
             "orc3_face_fluxes": (U, [P, I, dp]),
+            "orc3_forces_parts": (None, [P, D, D, D, dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -816,6 +817,14 @@ class Solver3:
         out = np.zeros(3)
         lib3().orc3_forces(self._h, self.mach, x_max, _dp(out))
         return dict(cn=out[0], ca=out[1], x_cp=out[2])
+
+    PARTS = ("nose", "afterbody", "fin_sides", "fin_edges", "fin_tips")
+
+    def forces_parts(self, x_max, x_nose):
+        """run3.rs `breakdown_on`: {part: dict(cn, ca, x_cp)}."""
+        out = np.zeros(15)
+        lib3().orc3_forces_parts(self._h, self.mach, x_max, x_nose, _dp(out))
+        return {p: dict(cn=out[3 * q], ca=out[3 * q + 1], x_cp=out[3 * q + 2]) for q, p in enumerate(self.PARTS)}
 
     def run(self, x_max, max_iter=8000, rel_tol=0.002, window=500):
         r = Orc3Result()

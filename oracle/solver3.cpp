@@ -955,6 +955,72 @@ Forces3 forces_on(const Solver3& s, double mach, double x_max) {
   return r;
 }
 
+// run3.rs:85-127 `breakdown_on` (the parts of `accumulate`, run3.rs:130-212): nose (body wall with centroid x <= x_nose),
+// afterbody, fin sides (k faces), fin edges (i faces), fin tips (j faces); (cn, ca, x_cp) per part
+std::array<Forces3, 5> forces_parts(const Solver3& s, double mach, double x_max, double x_nose) {
+  const Grid3& g = s.grid;
+  size_t ni = g.ni, nj = g.nj, nk = g.nk;
+  double p_inf = s.fs[4];
+  auto p = [&](size_t c) { return cons_to_prim3(s.u[c])[4]; };
+  auto dist = [&](size_t c, const Face3& f) {
+    const auto& x = g.xc[c];
+    return std::sqrt(std::pow(x[0] - f.c[0], 2) + std::pow(x[1] - f.c[1], 2) + std::pow(x[2] - f.c[2], 2));
+  };
+  auto sol = [&](size_t i, size_t j, size_t k) { return s.solid[g.cell(i, j, k)] != 0; };
+  double acc[5][3] = {};
+  auto add = [&](int part, size_t a, long b, const Face3& f, double sign) {
+    if (f.c[0] > x_max) return;
+    if (part == 0 && f.c[0] > x_nose) part = 1;
+    double p0 = p(a), pw = p0;
+    if (b >= 0) {
+      double d0 = dist(a, f), d1 = dist((size_t)b, f);
+      pw = p0 + (p0 - p((size_t)b)) * d0 / (d1 - d0);
+    }
+    double d = (pw - p_inf) * f.area * sign;
+    acc[part][0] += d * f.n[0];
+    acc[part][1] += d * f.n[2];
+    acc[part][2] += d * f.n[2] * f.c[0];
+  };
+  for (size_t k = 0; k < nk; ++k)
+    for (size_t i = g.axis_cells; i < ni; ++i)
+      if (!sol(i, 0, k)) add(0, g.cell(i, 0, k), nj > 1 && !sol(i, 1, k) ? (long)g.cell(i, 1, k) : -1, g.jface[k * (nj + 1) * ni + i], -1.0);
+  if (s.has_solid) {
+    for (size_t k = 0; k < nk; ++k)
+      for (size_t j = 0; j < nj; ++j)
+        for (size_t i = 1; i < ni; ++i) {
+          const Face3& f = g.iface[(k * nj + j) * (ni + 1) + i];
+          bool a = sol(i - 1, j, k), b = sol(i, j, k);
+          if (!a && b) add(3, g.cell(i - 1, j, k), i >= 2 && !sol(i - 2, j, k) ? (long)g.cell(i - 2, j, k) : -1, f, 1.0);
+          if (a && !b) add(3, g.cell(i, j, k), i + 1 < ni && !sol(i + 1, j, k) ? (long)g.cell(i + 1, j, k) : -1, f, -1.0);
+        }
+    for (size_t k = 0; k < nk; ++k)
+      for (size_t j = 1; j < nj; ++j)
+        for (size_t i = 0; i < ni; ++i) {
+          const Face3& f = g.jface[(k * (nj + 1) + j) * ni + i];
+          bool a = sol(i, j - 1, k), b = sol(i, j, k);
+          if (!a && b) add(4, g.cell(i, j - 1, k), j >= 2 && !sol(i, j - 2, k) ? (long)g.cell(i, j - 2, k) : -1, f, 1.0);
+          if (a && !b) add(4, g.cell(i, j, k), j + 1 < nj && !sol(i, j + 1, k) ? (long)g.cell(i, j + 1, k) : -1, f, -1.0);
+        }
+    for (size_t k = 1; k < nk; ++k)
+      for (size_t j = 0; j < nj; ++j)
+        for (size_t i = 0; i < ni; ++i) {
+          const Face3& f = g.kface[(k * nj + j) * ni + i];
+          bool a = sol(i, j, k - 1), b = sol(i, j, k);
+          if (!a && b) add(2, g.cell(i, j, k - 1), k >= 2 && !sol(i, j, k - 2) ? (long)g.cell(i, j, k - 2) : -1, f, 1.0);
+          if (a && !b) add(2, g.cell(i, j, k), k + 1 < nk && !sol(i, j, k + 1) ? (long)g.cell(i, j, k + 1) : -1, f, -1.0);
+        }
+  }
+  double q = 0.5 * mach * mach, s_ref = M_PI / 4.0;
+  double norm = 2.0 / (q * s_ref);
+  std::array<Forces3, 5> out;
+  for (int k = 0; k < 5; ++k) {
+    out[k].cn = norm * acc[k][1];
+    out[k].ca = norm * acc[k][0];
+    out[k].x_cp = std::fabs(acc[k][1]) < 1e-12 ? NAN : acc[k][2] / acc[k][1];
+  }
+  return out;
+}
+
 }  // namespace orc3
 
 // ---------------------------------------------------------------- C API
@@ -1063,6 +1129,10 @@ void orc3_steps(void* h, uint64_t n, double* residual) {
     double r = s->step();
     if (residual) residual[k] = r;
   }
+}
+void orc3_forces_parts(void* h, double mach, double x_max, double x_nose, double* out15) {
+  std::array<Forces3, 5> f = forces_parts(*static_cast<Solver3*>(h), mach, x_max, x_nose);
+  for (int k = 0; k < 5; ++k) out15[3 * k] = f[k].cn, out15[3 * k + 1] = f[k].ca, out15[3 * k + 2] = f[k].x_cp;
 }
 void orc3_forces(void* h, double mach, double x_max, double* out3) {
   Forces3 f = forces_on(*static_cast<Solver3*>(h), mach, x_max);

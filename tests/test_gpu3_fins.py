@@ -176,3 +176,21 @@ def test_fin_body_converged_forces_match_oracle():
     assert rg["stop_reason"] in ("residual drop", "CN stationary"), rg
     assert abs(rg["cn"] - rc["cn"]) <= 2e-3 * abs(rc["cn"]) + 1e-4, (rg, rc)
     assert abs(rg["x_cp"] - rc["x_cp"]) <= 2e-2, (rg, rc)
+
+
+def test_force_parts_match_oracle():
+    """run3.rs `breakdown_on` (bowshock3_forces_parts) on the afterbody fin box after 30 implicit iterations, evaluated on
+    the GPU's state by both sides: every part's CN and CA to 1e-9, and the parts add up to the totals."""
+    cpu, gpu, dims, boxes, c = _body_pair(2.5, 8.0, implicit=True, first_order=5)
+    gpu.run(30)
+    cpu.u = gpu.state(0)
+    x_base, x_nose = c.body.x_base(), c.body.nose_length()
+    pc = cpu.forces_parts(x_base, x_nose)
+    pg = gpu.forces_parts(x_base, x_nose)[0]
+    tot = gpu.forces(x_base)[0]
+    for part in pc:
+        for key in ("cn", "ca"):
+            assert abs(pg[part][key] - pc[part][key]) <= 1e-9 * max(1.0, abs(pc[part][key])), (part, key, pg[part], pc[part])
+    for key in ("cn", "ca"):
+        assert abs(sum(p[key] for p in pg.values()) - tot[key]) <= 1e-10 * max(1.0, abs(tot[key]))
+    assert abs(pg["fin_sides"]["cn"]) > 1e-6  # the fin box carries normal force at 8 degrees

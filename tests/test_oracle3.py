@@ -283,3 +283,21 @@ def test_fin_faces_carry_forces():
     norm = 2.0 / (0.5 * 2.0 * 2.0 * np.pi / 4.0)
     assert abs((f["ca"] - g["ca"]) - norm * fx) <= 1e-12 * max(1.0, abs(norm * fx)), (f["ca"], g["ca"], norm * fx)
     assert abs(norm * fx) > 1e-3
+
+
+def test_force_parts_sum_to_the_totals():
+    """run3.rs `breakdown_on`: the five parts (nose, afterbody, fin sides, edges, tips) of the fin grid's forces add up to
+    `forces_on`; the fin parts carry the solid box's faces (the k faces of a box in a uniform stream at zero incidence
+    have no axial component)."""
+    ni, nj, nk, x, r, theta, box = fin_grid()
+    s = o.Solver3(ni, nj, x, r, nk, theta, 0, 2.0, np.radians(4.0), limiter=o.VAN_ALBADA, implicit=True,
+                  params=o.implicit3_params(cfl_max=20.0))
+    s.set_solid([box])
+    s.steps(20)
+    tot = s.forces(10.0)
+    parts = s.forces_parts(10.0, 0.8)
+    norm_sum = lambda key: sum(p[key] for p in parts.values())
+    assert abs(norm_sum("cn") - tot["cn"]) <= 1e-12 * max(1.0, abs(tot["cn"]))
+    assert abs(norm_sum("ca") - tot["ca"]) <= 1e-12 * max(1.0, abs(tot["ca"]))
+    assert parts["fin_edges"]["ca"] != 0.0 and parts["fin_sides"]["ca"] == 0.0
+    assert abs(parts["fin_sides"]["cn"]) > 0.0
