@@ -1134,23 +1134,27 @@ static int b3from(bowshock3_batch* h, int rc) {
   return rc;
 }
 extern "C" {
+// a bowshock3_config as the batch's case record; BOWSHOCK_OK, UNSUPPORTED (not an explicit / implicit scheme) or INVALID
+static int case3_of(const bowshock3_config& c, bk3::Case3Host& h) {
+  if (c.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT && c.scheme.kind != BOWSHOCK_SCHEME_EXPLICIT) return BOWSHOCK_UNSUPPORTED;
+  if (!(c.mach > 0.0) || c.limiter < 0 || c.limiter > 3) return BOWSHOCK_INVALID;
+  h.mach = c.mach, h.alpha = c.alpha, h.cfl = c.cfl, h.limiter = c.limiter, h.low_mach = c.low_mach != 0;
+  h.first_order_iters = (long long)c.first_order_iters;
+  h.implicit = c.scheme.kind == BOWSHOCK_SCHEME_IMPLICIT;
+  h.cfl0 = c.scheme.cfl0, h.cfl_max = c.scheme.cfl_max, h.growth = c.scheme.growth, h.eps_fix = c.scheme.eps_fix;
+  h.dt_mode = c.scheme.dt_mode, h.sub_iters = (int)std::max<uint64_t>(c.scheme.sub_iters, 1), h.roe = c.scheme.roe != 0;
+  h.implicit_bc = c.scheme.implicit_bc != 0, h.lines = c.scheme.lines != 0;
+  return BOWSHOCK_OK;
+}
 int bowshock3_create(uint64_t ni, uint64_t nj, uint64_t nk, const double* x, const double* y, const double* z, uint64_t axis_cells,
                      uint64_t ncases, const bowshock3_config* cfg, int device, bowshock3_batch** out) {
   if (!x || !y || !z || !cfg || !out || ncases == 0) return BOWSHOCK_INVALID;
   *out = nullptr;
   std::vector<bk3::Case3Host> cs(ncases);
   for (uint64_t k = 0; k < ncases; ++k) {
-    const bowshock3_config& c = cfg[k];
-    if (c.scheme.kind != BOWSHOCK_SCHEME_IMPLICIT && c.scheme.kind != BOWSHOCK_SCHEME_EXPLICIT) return BOWSHOCK_UNSUPPORTED;
-    if (c.scheme.kind != cfg[0].scheme.kind) return BOWSHOCK_UNSUPPORTED;  // one scheme per batch
-    if (!(c.mach > 0.0) || c.limiter < 0 || c.limiter > 3) return BOWSHOCK_INVALID;
-    bk3::Case3Host& h = cs[k];
-    h.mach = c.mach, h.alpha = c.alpha, h.cfl = c.cfl, h.limiter = c.limiter, h.low_mach = c.low_mach != 0;
-    h.first_order_iters = (long long)c.first_order_iters;
-    h.implicit = c.scheme.kind == BOWSHOCK_SCHEME_IMPLICIT;
-    h.cfl0 = c.scheme.cfl0, h.cfl_max = c.scheme.cfl_max, h.growth = c.scheme.growth, h.eps_fix = c.scheme.eps_fix;
-    h.dt_mode = c.scheme.dt_mode, h.sub_iters = (int)std::max<uint64_t>(c.scheme.sub_iters, 1), h.roe = c.scheme.roe != 0;
-    h.implicit_bc = c.scheme.implicit_bc != 0, h.lines = c.scheme.lines != 0;
+    if (cfg[k].scheme.kind != cfg[0].scheme.kind) return BOWSHOCK_UNSUPPORTED;  // one scheme per batch
+    const int rc = case3_of(cfg[k], cs[k]);
+    if (rc) return rc;
   }
   auto* h = new bowshock3_batch();
   int rc = h->b.create(ni, nj, nk, x, y, z, axis_cells, cs, device);
@@ -1167,6 +1171,25 @@ int bowshock3_reset(bowshock3_batch* b) { return b ? b3from(b, b->b.reset()) : B
 int bowshock3_set_solid(bowshock3_batch* b, uint64_t nbox, const uint64_t* boxes) {
   if (!b || (nbox && !boxes)) return BOWSHOCK_INVALID;
   return b3from(b, b->b.set_solid((size_t)nbox, boxes));
+}
+int bowshock3_set_config(bowshock3_batch* b, uint64_t k, const bowshock3_config* cfg) {
+  if (!b || !cfg || k >= (uint64_t)b->b.B.nb) return BOWSHOCK_INVALID;
+  bk3::Case3Host h;
+  int rc = case3_of(*cfg, h);
+  if (rc) return rc;
+  rc = b->b.set_config((int)k, h);
+  if (rc == 1) {
+    b->last_error = b->b.err;
+    return BOWSHOCK_UNSUPPORTED;
+  }
+  return b3from(b, rc);
+}
+int bowshock3_profile(bowshock3_batch* b, uint64_t n, double* ms, uint64_t* launches) {
+  if (!b || !ms || !launches) return BOWSHOCK_INVALID;
+  unsigned long long l[bk3::Batch3::P3_N];
+  int rc = b->b.profile((long long)n, ms, l);
+  for (int g = 0; g < bk3::Batch3::P3_N; ++g) launches[g] = l[g];
+  return b3from(b, rc);
 }
 int bowshock3_set_groups(bowshock3_batch* b, int groups) {
   if (!b) return BOWSHOCK_INVALID;

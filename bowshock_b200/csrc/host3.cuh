@@ -152,6 +152,8 @@ struct Batch3 {
     for (cudaEvent_t ev : gev) cudaEventDestroy(ev);
     gst.clear(), gev.clear();
     if (ev_fork3) cudaEventDestroy(ev_fork3), ev_fork3 = nullptr;
+    if (pe0) cudaEventDestroy(pe0), pe0 = nullptr;
+    if (pe1) cudaEventDestroy(pe1), pe1 = nullptr;
     for (void* p : owned)
       if (p) cudaFree(p);
     owned.clear();
@@ -344,6 +346,27 @@ struct Batch3 {
     BK3_CUDA(copy_sync(stream, d_wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice));
     return reset();
   }
+  // GpuSolver3::set_config (gpu/mod.rs:482-487) for case b: free stream, CFL, limiter, first-order iterations and the
+  // low-Mach flag may change between runs, state and geometry untouched; a changed scheme restarts the case's CFL ramp.
+  // The batch runs one scheme: the explicit / implicit kind changes only for a batch of one case.
+  int set_config(int b, const Case3Host& h) {
+    const Case3Host& o = cases[b];
+    if (h.implicit != o.implicit && B.nb > 1) {
+      err = "one scheme per batch: the explicit / implicit kind changes only for a batch of one case";
+      return 1;
+    }
+    const bool scheme_changed = h.implicit != o.implicit || h.cfl0 != o.cfl0 || h.cfl_max != o.cfl_max || h.growth != o.growth ||
+                                h.eps_fix != o.eps_fix || h.dt_mode != o.dt_mode || h.sub_iters != o.sub_iters || h.roe != o.roe ||
+                                h.implicit_bc != o.implicit_bc || h.lines != o.lines;
+    cases[b] = h;
+    int rc;
+    if ((rc = upload_cases())) return rc;
+    if (scheme_changed) {
+      const int zero = 0;
+      BK3_CUDA(copy_sync(stream, B.ramp + b, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    }
+    return 0;
+  }
   int upload_cases() {
     std::vector<Case3Dev> h(cases.size());
     for (size_t k = 0; k < cases.size(); ++k) to_dev(cases[k], h[k]);
@@ -421,6 +444,40 @@ struct Batch3 {
     return 0;
   }
   dim3 grid_of(long long n, int threads) const { return dim3((unsigned)((n + threads - 1) / threads), (unsigned)(gnb ? gnb : B.nb)); }
+  // Per-kernel profile (GpuSolver3::profile_step / profile_replay, gpu/mod.rs:525-535): with `profiling` set every launch
+  // is bracketed by CUDA events and its time added to its group.
+  enum { P3_PRIMS = 0, P3_FLUX, P3_RESIDUAL, P3_ASSEMBLE, P3_LINES, P3_SUBST, P3_DEFECT, P3_STAGE, P3_N };
+  bool profiling = false;
+  double prof_ms[P3_N] = {0};
+  long long prof_n[P3_N] = {0};
+  cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+  template <class F>
+  void L3(int g, F&& launch) {
+    if (!profiling) {
+      launch();
+      return;
+    }
+    cudaEventRecord(pe0, stream);
+    launch();
+    cudaEventRecord(pe1, stream);
+    cudaEventSynchronize(pe1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, pe0, pe1);
+    prof_ms[g] += ms, prof_n[g] += 1;
+  }
+  int profile(long long n, double* ms, unsigned long long* launches) {
+    if (!pe0) {
+      BK3_CUDA(cudaEventCreate(&pe0));
+      BK3_CUDA(cudaEventCreate(&pe1));
+    }
+    for (int g = 0; g < P3_N; ++g) prof_ms[g] = 0.0, prof_n[g] = 0;
+    const int g0 = groups;
+    groups = 1, profiling = true;
+    int rc = run(n, nullptr);
+    profiling = false, groups = g0;
+    for (int g = 0; g < P3_N; ++g) ms[g] = prof_ms[g], launches[g] = (unsigned long long)prof_n[g];
+    return rc;
+  }
   // `chunk` iterations of every active case, per group on its own stream between a fork and a join on `stream`
   void launch_chunk(int chunk) {
     if (groups <= 1) {
@@ -443,12 +500,12 @@ struct Batch3 {
     for (int g = 0; g < groups; ++g) cudaStreamWaitEvent(stream, gev[g], 0);
   }
   void launch_prep() {
-    k3_prims<<<grid_of(B.nc, 256), 256, 0, stream>>>(B);
+    L3(P3_PRIMS, [&] { k3_prims<<<grid_of(B.nc, 256), 256, 0, stream>>>(B); });
     long long ng = 2LL * B.nj * B.nk + 2LL * B.ni * B.nk + 2LL * B.ni * B.nj;
-    k3_ghosts<<<grid_of(ng, 128), 128, 0, stream>>>(B);
-    k3_flux<<<grid_of(B.nfi, 128), 128, 0, stream>>>(B, 0);
-    k3_flux<<<grid_of(B.nfj, 128), 128, 0, stream>>>(B, 1);
-    k3_flux<<<grid_of(B.nfk, 128), 128, 0, stream>>>(B, 2);
+    L3(P3_PRIMS, [&] { k3_ghosts<<<grid_of(ng, 128), 128, 0, stream>>>(B); });
+    L3(P3_FLUX, [&] { k3_flux<<<grid_of(B.nfi, 128), 128, 0, stream>>>(B, 0); });
+    L3(P3_FLUX, [&] { k3_flux<<<grid_of(B.nfj, 128), 128, 0, stream>>>(B, 1); });
+    L3(P3_FLUX, [&] { k3_flux<<<grid_of(B.nfk, 128), 128, 0, stream>>>(B, 2); });
   }
   bool implicit() const { return cases[0].implicit != 0; }
   // the staged first pass (k3_lines_st): on unless pinned off; only where a warp's 32 lines are adjacent (i lines: nj a
@@ -456,16 +513,20 @@ struct Batch3 {
   bool staged = true;
   bool staged_ok(int dir) const { return staged && (dir == 0 ? B.nj % 32 == 0 : B.ni % 32 == 0); }
   void launch_lines(int dir, long long nl, const float* in, int from_res, float* out, int epilogue) {
-    if (staged_ok(dir))
-      k3_lines_st<<<grid_of(nl, 32), 32, 0, stream>>>(B, dir, in, from_res, out, epilogue);
-    else
-      k3_lines<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
+    L3(P3_LINES, [&] {
+      if (staged_ok(dir))
+        k3_lines_st<<<grid_of(nl, 32), 32, 0, stream>>>(B, dir, in, from_res, out, epilogue);
+      else
+        k3_lines<<<grid_of(nl, 64), 64, 0, stream>>>(B, dir, in, from_res, out, epilogue);
+    });
   }
   void launch_subst(int dir, long long nl, const float* in, float* out, int epilogue, int pass) {
-    if (staged_ok(dir))
-      k3_lines_subst_st<<<grid_of(nl, 32), 32, 0, stream>>>(B, dir, in, out, epilogue, pass);
-    else
-      k3_lines_subst<<<grid_of(nl, 128), 128, 0, stream>>>(B, dir, in, out, epilogue, pass);
+    L3(P3_SUBST, [&] {
+      if (staged_ok(dir))
+        k3_lines_subst_st<<<grid_of(nl, 32), 32, 0, stream>>>(B, dir, in, out, epilogue, pass);
+      else
+        k3_lines_subst<<<grid_of(nl, 128), 128, 0, stream>>>(B, dir, in, out, epilogue, pass);
+    });
   }
   int max_sub() const {
     int s = 1;
@@ -475,30 +536,30 @@ struct Batch3 {
   void launch_iteration(int slot) {
     if (implicit()) {
       launch_prep();
-      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2, slot);
+      L3(P3_RESIDUAL, [&] { k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2, slot); });
       const long long li = (long long)B.nj * B.nk, lj = (long long)B.ni * B.nk, lk = (long long)B.ni * B.nj;
-      k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 0);
-      k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 1);
+      L3(P3_ASSEMBLE, [&] { k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 0); });
+      L3(P3_ASSEMBLE, [&] { k3_assemble<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, 1); });
       launch_lines(0, li, B.R, 1, B.X, 0);
       launch_lines(1, lj, B.X, 0, B.X, 0);
       launch_lines(2, lk, B.X, 0, nullptr, 1);
       for (int p = 1; p < max_sub(); ++p) {
-        k3_defect_i<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
-        k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p);
+        L3(P3_DEFECT, [&] { k3_defect_i<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p); });
+        L3(P3_DEFECT, [&] { k3_defect<<<grid_of(B.nc, 128), 128, 0, stream>>>(B, p); });
         launch_subst(0, li, B.RR, B.X, 0, p);
         launch_subst(1, lj, B.X, B.X, 0, p);
         launch_subst(2, lk, B.X, nullptr, 2, p);
       }
     } else {  // SSP-RK3 (solver3.rs:303-314)
       launch_prep();
-      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 1, slot);
-      k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 1.f, 0.f, 1, 0);
+      L3(P3_RESIDUAL, [&] { k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 1, slot); });
+      L3(P3_STAGE, [&] { k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 1.f, 0.f, 1, 0); });
       launch_prep();
-      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0, -1);
-      k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0.25f, 0.75f, 0, 0);
+      L3(P3_RESIDUAL, [&] { k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0, -1); });
+      L3(P3_STAGE, [&] { k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0.25f, 0.75f, 0, 0); });
       launch_prep();
-      k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0, -1);
-      k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2.f / 3.f, 1.f / 3.f, 0, 1);
+      L3(P3_RESIDUAL, [&] { k3_residual<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 0, -1); });
+      L3(P3_STAGE, [&] { k3_stage<<<grid_of(B.nc, 256), 256, 0, stream>>>(B, 2.f / 3.f, 1.f / 3.f, 0, 1); });
     }
   }
   // n iterations; residual: n x nb (iteration-major), may be null

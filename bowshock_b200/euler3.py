@@ -42,6 +42,8 @@ SIGNATURES3 = {
     "bowshock3_set_solid": (_I, [_P, _U, C.POINTER(_U)]),
     "bowshock3_set_staging": (_I, [_P, _I]),
     "bowshock3_set_groups": (_I, [_P, _I]),
+    "bowshock3_set_config": (_I, [_P, _U, C.POINTER(Config3C)]),
+    "bowshock3_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
     "bowshock3_set_iter": (_I, [_P, _U, _U]),
     "bowshock3_set_state": (_I, [_P, _U, _dp]),
     "bowshock3_state": (_I, [_P, _U, _dp]),
@@ -142,6 +144,21 @@ class Batch3:
     def set_staging(self, on):
         """The first line pass staged through shared memory where the grid allows it (default on); same results."""
         self._check(lib().bowshock3_set_staging(self._h, int(bool(on))))
+
+    def set_config(self, k, config):
+        """GpuSolver3::set_config for case k (a Config3): the state is kept; a changed scheme restarts its CFL ramp."""
+        c = config.c()
+        self._check(lib().bowshock3_set_config(self._h, int(k), C.byref(c)))
+        self.configs[k] = config
+
+    PROFILE_GROUPS = ("prims", "flux", "residual", "assemble", "lines", "subst", "defect", "stage")
+
+    def profile(self, n):
+        """Per-kernel-group device time over n iterations launched one kernel at a time: {group: (ms, launches)}."""
+        ms = np.zeros(len(self.PROFILE_GROUPS))
+        cnt = (_U * len(self.PROFILE_GROUPS))()
+        self._check(lib().bowshock3_profile(self._h, int(n), _p(ms), cnt))
+        return {g: (float(ms[q]), int(cnt[q])) for q, g in enumerate(self.PROFILE_GROUPS)}
 
     def set_groups(self, groups):
         """Split the cases into 1 to 4 groups whose iterations run on streams of their own (the same states)."""

@@ -444,6 +444,16 @@ void bowshock3_destroy(bowshock3_batch* b);
 const char* bowshock3_last_error(const bowshock3_batch* b);
 /* every case back to its free stream at iteration 0 (GpuSolver3::reset) */
 int bowshock3_reset(bowshock3_batch* b);
+/* GpuSolver3::set_config (gpu/mod.rs:482-487) for case k: free stream (Mach, incidence), CFL, limiter, first-order
+ * iterations and the low-Mach flag may change between runs without touching the state; a changed scheme restarts the
+ * case's CFL ramp. The batch runs one scheme: the explicit / implicit kind changes only for a batch of one case
+ * (UNSUPPORTED otherwise). */
+int bowshock3_set_config(bowshock3_batch* b, uint64_t k, const bowshock3_config* cfg);
+/* Per-kernel profile (GpuSolver3::profile_step / profile_replay, gpu/mod.rs:525-535): n iterations launched one kernel
+ * at a time with CUDA events around each; per group (primitives and ghosts, face fluxes, residual, assembly, first line
+ * pass, substitution passes, defect, RK3 stage) the total milliseconds and launch counts, BOWSHOCK3_PROFILE_GROUPS each. */
+#define BOWSHOCK3_PROFILE_GROUPS 8
+int bowshock3_profile(bowshock3_batch* b, uint64_t n, double* ms, uint64_t* launches);
 /* Solid boxes of the shared grid (crates/bowshock-cfd/src/grid3.rs:17-24 `SolidBox`, the fins; `Grid3::solid`, read by
  * Solver3::new, solver3.rs:84-97): 6 per box, i0 i1 j0 j1 k0 k1, half-open cell ranges; nbox 0 removes them. Solid cells
  * are never updated and act as slip walls (solver3.rs:362-405, implicit3.rs:14-16); the density norm runs over the fluid

@@ -190,3 +190,36 @@ def test_case_groups_are_bit_identical():
     b, _ = e3.batch_of(cases)
     with pytest.raises(e3.BowshockError):
         b.set_groups(5)
+
+
+def test_set_config_changes_the_free_stream_between_runs():
+    """bowshock3_set_config (GpuSolver3::set_config): case 0's Mach number changed after 10 iterations, state and
+    counters kept; the next 10 iterations equal, bit for bit, those of a batch created with the new configuration from
+    the same state and counters."""
+    import bowshock_b200.euler3 as e3
+    cases = e3.lift_sweep_cases((4.0,), (0.8, 2.5), ni=48, nj=16, nk=8)
+    b, _ = e3.batch_of(cases)
+    b.run(10)
+    u0, u1 = b.state(0), b.state(1)
+    new = e3.lift_sweep_cases((4.0,), (1.2,), ni=48, nj=16, nk=8)[0].config()
+    b.set_config(0, new)
+    b.run(10)
+    ref, _ = e3.batch_of(e3.lift_sweep_cases((4.0,), (1.2,), ni=48, nj=16, nk=8) + cases[1:])
+    ref.set_state(0, u0)
+    ref.set_state(1, u1)
+    ref.set_iter(10, 10)
+    ref.run(10)
+    assert np.array_equal(b.state(0), ref.state(0))
+    assert np.array_equal(b.state(1), ref.state(1))
+
+
+def test_profile_groups():
+    """bowshock3_profile: every kernel group of the implicit iteration timed (the RK3 stage not launched), with the launch
+    counts of the three-factor scheme at sub_iters 2."""
+    import bowshock_b200.euler3 as e3
+    b, _ = e3.batch_of(e3.lift_sweep_cases((4.0,), (0.8, 2.5), ni=48, nj=16, nk=8))
+    b.run(3)
+    p = b.profile(4)
+    counts = {g: n for g, (ms, n) in p.items()}
+    assert counts == {"prims": 8, "flux": 12, "residual": 4, "assemble": 8, "lines": 12, "subst": 12, "defect": 8, "stage": 0}, counts
+    assert all(ms > 0 for g, (ms, n) in p.items() if n), p
