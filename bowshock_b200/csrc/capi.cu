@@ -1234,6 +1234,10 @@ int bowshock3_forces(bowshock3_batch* b, double x_max, double* out) {
   std::memcpy(out, f.data(), f.size() * sizeof(double));
   return BOWSHOCK_OK;
 }
+int bowshock3_read_boundary(bowshock3_batch* b, uint64_t k, double* u) {
+  if (!b || !u || k >= (uint64_t)b->b.B.nb) return BOWSHOCK_INVALID;
+  return b3from(b, b->b.read_boundary((int)k, u));
+}
 int bowshock3_forces_parts(bowshock3_batch* b, double x_max, double x_nose, double* out) {
   if (!b || !out) return BOWSHOCK_INVALID;
   std::vector<double> f;

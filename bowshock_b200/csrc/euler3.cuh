@@ -1131,6 +1131,15 @@ __global__ void __launch_bounds__(128) k3_defect(B3 B, int pass) {
   stU(B, B.RR, b, c, o);
 }
 
+// the conserved states of case b at the listed cells, 5 per cell in Cons3 order (GpuSolver3::read_boundary_into)
+__global__ void k3_gather(B3 B, int b, const long long* cells, int n, double* out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const V5<float> u = ldU(B, B.U, b, cells[q]);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) out[5 * (long long)q + v] = u[v];
+}
+
 // FP64 wall forces of every case (run3.rs:130-212): one block per case. wall: WALL3 doubles per wall face, the j = 0 body
 // faces (i >= axis_cells, fluid cells) and every face between a fluid and a solid cell: n[3], area, c[3], the centroid of
 // the first fluid cell a and of the fluid cell b behind it, a, b (-1: none), the sign that turns n into the body, and the

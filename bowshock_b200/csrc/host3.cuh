@@ -612,6 +612,34 @@ struct Batch3 {
     }
     return 0;
   }
+  // GpuSolver3::read_boundary_into (gpu/mod.rs:519-523): the states of case b at the cells the force integration reads
+  // (the first fluid cell of every wall face and the one behind it) into u (ncell x 5, Cons3 order); other cells untouched
+  int read_boundary(int b, double* u) {
+    std::vector<long long> cells;
+    for (int q = 0; q < nwall; ++q) {
+      const double* w = &wall[(size_t)WALL3 * q];
+      cells.push_back((long long)w[13]);
+      if (w[14] >= 0) cells.push_back((long long)w[14]);
+    }
+    std::sort(cells.begin(), cells.end());
+    cells.erase(std::unique(cells.begin(), cells.end()), cells.end());
+    const int n = (int)cells.size();
+    if (n == 0) return 0;
+    long long* dc = nullptr;
+    double* dv = nullptr;
+    BK3_CUDA(cudaMallocAsync(&dc, n * sizeof(long long), stream));
+    BK3_CUDA(cudaMallocAsync(&dv, 5 * (size_t)n * sizeof(double), stream));
+    BK3_CUDA(cudaMemcpyAsync(dc, cells.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream));
+    k3_gather<<<(n + 255) / 256, 256, 0, stream>>>(B, b, dc, n, dv);
+    std::vector<double> hv(5 * (size_t)n);
+    BK3_CUDA(cudaMemcpyAsync(hv.data(), dv, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    BK3_CUDA(cudaFreeAsync(dc, stream));
+    BK3_CUDA(cudaFreeAsync(dv, stream));
+    BK3_CUDA(cudaStreamSynchronize(stream));
+    for (int q = 0; q < n; ++q)
+      for (int v = 0; v < 5; ++v) u[5 * cells[q] + v] = hv[5 * (size_t)q + v];
+    return 0;
+  }
   // (cn, ca, x_cp) of the 5 parts of every case (k3_forces_parts)
   int forces_parts(double x_max, double x_nose, std::vector<double>& out) {
     k3_forces_parts<<<B.nb, 128, 0, stream>>>(B, d_wall, nwall, x_max, x_nose, d_parts);

@@ -43,6 +43,7 @@ SIGNATURES3 = {
     "bowshock3_set_staging": (_I, [_P, _I]),
     "bowshock3_set_groups": (_I, [_P, _I]),
     "bowshock3_set_config": (_I, [_P, _U, C.POINTER(Config3C)]),
+    "bowshock3_read_boundary": (_I, [_P, _U, _dp]),
     "bowshock3_profile": (_I, [_P, _U, _dp, C.POINTER(_U)]),
     "bowshock3_set_iter": (_I, [_P, _U, _U]),
     "bowshock3_set_state": (_I, [_P, _U, _dp]),
@@ -175,6 +176,12 @@ class Batch3:
         u = np.zeros(5 * self.nc)
         self._check(lib().bowshock3_state(self._h, int(k), _p(u)))
         return u.reshape(-1, 5)
+
+    def read_boundary_into(self, k, u):
+        """GpuSolver3::read_boundary_into: the force integration's cells of case k into u (ncell x 5), the rest untouched."""
+        if u.shape != (self.nc, 5) or u.dtype != np.float64 or not u.flags.c_contiguous:
+            raise ValueError("u must be a C-contiguous float64 array of shape (ncell, 5)")
+        self._check(lib().bowshock3_read_boundary(self._h, int(k), _p(u)))
 
     def run(self, n):
         out = np.zeros(n * self.nb)

@@ -473,6 +473,10 @@ int bowshock3_set_iter(bowshock3_batch* b, uint64_t iter, uint64_t ramp);
 /* conserved state of case k, ni*nj*nk x 5 (Solver3::u layout) */
 int bowshock3_set_state(bowshock3_batch* b, uint64_t k, const double* u);
 int bowshock3_state(bowshock3_batch* b, uint64_t k, double* u);
+/* GpuSolver3::read_boundary_into (gpu/mod.rs:519-523): only the cells the force integration reads (the first fluid cell
+ * of every wall and fin face and the one behind it) of case k into u (ncell x 5, the layout of bowshock3_state); the
+ * other entries of u are left as they are */
+int bowshock3_read_boundary(bowshock3_batch* b, uint64_t k, double* u);
 /* n iterations of every active case; residual (n x ncases, iteration-major) may be NULL (GpuSolver3::run) */
 int bowshock3_run(bowshock3_batch* b, uint64_t n, double* residual);
 /* residual (ncell x 5) and time step of case k for the current state (no update); density residual of case k */

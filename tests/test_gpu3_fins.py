@@ -194,3 +194,22 @@ def test_force_parts_match_oracle():
     for key in ("cn", "ca"):
         assert abs(sum(p[key] for p in pg.values()) - tot[key]) <= 1e-10 * max(1.0, abs(tot[key]))
     assert abs(pg["fin_sides"]["cn"]) > 1e-6  # the fin box carries normal force at 8 degrees
+
+
+def test_read_boundary_holds_what_the_forces_read():
+    """bowshock3_read_boundary (GpuSolver3::read_boundary_into): after 20 iterations of the fin body, the cells it fills
+    equal the state's, every other entry keeps its value (NaN here), and the oracle's forces (body wall and fin faces)
+    computed from that sparse state alone equal the GPU's to 1e-9."""
+    cpu, gpu, dims, boxes, c = _body_pair(2.5, 8.0, implicit=True, first_order=5)
+    gpu.run(20)
+    full = gpu.state(0)
+    u = np.full_like(full, np.nan)
+    gpu.read_boundary_into(0, u)
+    got = ~np.isnan(u[:, 0])
+    assert 0 < got.sum() < len(u)
+    assert np.array_equal(u[got], full[got])
+    cpu.u = u
+    x_base = c.body.x_base()
+    fc, fg = cpu.forces(x_base), gpu.forces(x_base)[0]
+    for key in ("cn", "ca"):
+        assert np.isfinite(fc[key]) and abs(fg[key] - fc[key]) <= 1e-9 * max(1.0, abs(fc[key])), (key, fg, fc)
